@@ -1,0 +1,437 @@
+"""DSMC particle-step benchmark (B200).
+
+One "step" is one full DSMC step (inflow injection, move with face-crossing
+tracing, cell sort, NTC collisions, 18-moment sampling) over every particle
+of the case. The metric is particle-steps/s: particles at the start of each
+step summed over the timed steps, divided by the device time (CUDA events on
+the library's stream, max over ranks). Mixed precision is the production
+path; the all-FP64 path is timed on the same case for the mixed/FP64 ratio.
+
+Multi-GPU runs are independent replicas (one case per GPU, no collective on
+the data path): value = the sum of all ranks' particle-steps / the slowest
+rank's time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload block|capsule]
+                  [--ppc P] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "dig-appolo_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+from pydsmc import case as C  # noqa: E402
+from pydsmc import mesh as M  # noqa: E402
+from pydsmc import workload as W  # noqa: E402
+
+METRIC = "DSMC particle-steps/s (mixed vs FP64 plain, 1 B200)"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+def block_workload(ppc: int):
+    """The block case: 48x32x32 hexes, central 8^3 block removed (48,640
+    cells), Ma 5, Kn 0.1 on the block edge, T_in 142.2 K, T_w 300 K, inflow
+    on x-min, outflow x-max, specular sides, AoA 0."""
+    raw = M.block_case_mesh(scale=1)
+    dm = M.build_dsmc_mesh(raw)
+    mess = C.mesh_message(dm, 5.0, 0.1, ppc=ppc, L0=0.5 / 32 * 8)
+    zones = [(3, 1, 0), (4, 2, 1), (5, 3, 0), (6, 4, 0), (7, 5, 0)]
+    return {"name": "block", "dm": dm, "mess": mess, "zones": zones, "inflow_dir": C.inflow_direction(0.0),
+            "desc": {"workload": "block-48640", "cells": dm.ncell, "ppc": ppc,
+                     "mesh": "hex box 1.0x0.5x0.5 m, 48x32x32 minus central 8^3 diffuse block",
+                     "Ma": 5.0, "Kn": 0.1, "aoa_deg": 0.0, "sides": "specular"}}
+
+
+def make_workload(name: str, ppc: int):
+    if name == "block":
+        return block_workload(ppc)
+    if name == "capsule":
+        from pydsmc import capsule
+        return capsule.capsule_workload(ppc)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def algorithmic_bytes(n_particles: float, ncell: int, ntri_per_cell: float, mixed: bool) -> dict:
+    """Algorithmic bytes of one step and of one move launch.
+
+    Per particle the state is read and written once: 32 B (mixed: x, v, Ir
+    as FP32 + cell id) or 60 B (FP64: x, v, Ir as FP64 + cell id). The move
+    launch reads each cell's triangles once (9 words + 8 B of face id/tag
+    per triangle); a step adds the per-cell collision and sampling state
+    (3 x 18 FP64 accumulators + crmax + 2 remainders, read and written)."""
+    sp = 32 if mixed else 60
+    word = 4 if mixed else 8
+    geom = ntri_per_cell * (9 * word + 8)
+    acc = 3 * 18 * 8 + 3 * 8
+    move = n_particles * 2 * sp + ncell * geom
+    step = move + ncell * 2 * acc
+    return {"move": move, "step": step, "per_particle_state": sp, "geom_per_cell": geom}
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                r = subprocess.run(["nvidia-smi", "-i", str(self.index), q, "--format=csv,noheader,nounits"],
+                                   capture_output=True, text=True, timeout=5)
+                if r.returncode == 0 and r.stdout.strip():
+                    self.samples.append([s.strip() for s in r.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, n in enumerate(names):
+                if len(s) > 3 + k and s[3 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+def run_case(wl, fill, precision, steps, warmup, seed, timing=False):
+    import torch
+    from pydsmc import gpu
+    p = gpu.default_params(precision=precision, seed=seed, zones=wl["zones"], inflow_dir=wl["inflow_dir"],
+                           nss=10 ** 9, nscheme=max(1, (steps + warmup) // 5), nrepeat=100)
+    case = gpu.Case(wl["dm"], wl["mess"], p, device=torch.cuda.current_device())
+    case.upload_particles(fill["x"], fill["v"], fill["ir"], fill["cell"])
+    case.statistic_macroPre()
+    istep = 0
+    for _ in range(warmup):
+        istep += 1
+        case.step(istep)
+    case.sync()
+    stream = torch.cuda.ExternalStream(case.lib.dsmc_stream(case.h))
+    n_before = []
+    case.set_timing(timing)
+    case.stage_ms(reset=True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    counts = []
+    # particle counts are device-resident; read them at the end from the counters
+    c0 = case.counters()
+    n0 = case.particle_count()
+    ev0.record(stream)
+    for _ in range(steps):
+        istep += 1
+        case.step(istep)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    c1 = case.counters()
+    n1 = case.particle_count()
+    stage = case.stage_ms(reset=True) if timing else None
+    case.sync()
+    res = {"ms": ms, "n0": n0, "n1": n1, "counters0": c0, "counters1": c1, "stage": stage, "istep": istep,
+           "case": case}
+    return res
+
+
+def particle_steps(res, steps):
+    # particles at the start of each timed step: n0 + injected - removed... use the
+    # inventory at both ends (the inventory drifts slowly) times the step count
+    return 0.5 * (res["n0"] + res["n1"]) * steps
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from pydsmc import gpu
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("no CUDA device")
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    gpu.load()
+    wl = make_workload(args.workload, args.ppc)
+    dm, mess = wl["dm"], wl["mess"]
+    fill = W.initial_fill(dm, mess, args.ppc, seed=rank, inflow_dir=wl["inflow_dir"])
+    nparts = len(fill["cell"])
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    peak, peak_kind = load_peaks()
+    # --- headline: mixed precision, graph replay
+    barrier()
+    with ClockSampler(local) as clk:
+        mixed = run_case(wl, fill, gpu.PRECISION_MIXED, args.steps, args.warmup, seed=1000 + rank)
+    barrier()
+    ms_mixed = max_over_ranks(mixed["ms"])
+    ps_mixed = sum_over_ranks(particle_steps(mixed, args.steps))
+    value = ps_mixed / (ms_mixed / 1e3)
+    case_m = mixed.pop("case")
+    # --- stage timing pass (events between stages, no graph) for the roofline
+    barrier()
+    tim = run_case(wl, fill, gpu.PRECISION_MIXED, max(3, args.steps // 2), 1, seed=2000 + rank, timing=True)
+    tim.pop("case").close()
+    stage_ms, tsteps = tim["stage"]
+    stage_avg = stage_ms / max(tsteps, 1)
+    # --- FP64 path on the same case
+    barrier()
+    fp64 = run_case(wl, fill, gpu.PRECISION_FP64, args.steps, args.warmup, seed=1000 + rank)
+    fp64.pop("case").close()
+    barrier()
+    ms_fp64 = max_over_ranks(fp64["ms"])
+    ps_fp64 = sum_over_ranks(particle_steps(fp64, args.steps))
+    value_fp64 = ps_fp64 / (ms_fp64 / 1e3)
+    # --- e2e through the C ABI with host buffers
+    barrier()
+    e2e = run_e2e(wl, fill, args, rank)
+    e2e_ms = max_over_ranks(e2e["ms"])
+    e2e_ps = sum_over_ranks(e2e["particle_steps"])
+    case_m.close()
+
+    ntri = dm.ncell and (sum(1 for _ in []) or None)
+    tri_per_cell = 12.0 if wl["name"] == "block" else 4.0
+    n_mean = 0.5 * (mixed["n0"] + mixed["n1"])
+    ab = algorithmic_bytes(n_mean, dm.ncell, tri_per_cell, mixed=True)
+    names = ["inject", "move", "sort", "collide_sample"]
+    dom = int(np.argmax(stage_avg))
+    dom_bytes = {"move": ab["move"]}.get(names[dom], None)
+    achieved = (ab["move"] / (stage_avg[1] / 1e3)) / 1e9 if stage_avg[1] > 0 else None
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "particle-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_mixed / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64acc",
+        "data": "synthetic (seeded freestream Maxwellian fill, generated mesh)",
+        "config": dict(wl["desc"], particles_per_gpu=nparts, parallelism=f"replicas x{world}",
+                       l2="particle state > L2 (126 MB)", precision="mixed"),
+        "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / args.steps, "dtype": "f64"},
+        "mixed_over_fp64": value / value_fp64 if value_fp64 > 0 else None,
+        "stage_ms_per_step": dict(zip(names, [float(x) for x in stage_avg])),
+        "roofline": {"bound": "hbm", "kernel": "move", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "peak_kind": peak_kind, "algorithmic_bytes_per_launch": ab["move"],
+                     "dominant_stage": names[dom]},
+        "e2e": {"value": e2e_ps / (e2e_ms / 1e3), "unit": "particle-steps/s",
+                "h2d_bytes_per_step": e2e["h2d"] / args.steps, "d2h_bytes_per_step": e2e["d2h"] / args.steps},
+        "gpu_launches": None,
+        "clocks": clk.summary(),
+        "counters": {k: mixed["counters1"][k] - mixed["counters0"][k] for k in mixed["counters1"]},
+    }
+    line["gpu_launches"] = launches_per_step(wl) * args.steps
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(wl, fill, args)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def launches_per_step(wl) -> int:
+    # inject: count, scan, generate; move; sort: rank, scan x2, scatter;
+    # cells: the warp kernel and the large-cell kernel
+    return 3 + 1 + 4 + 2
+
+
+def run_e2e(wl, fill, args, rank):
+    """The same step count through the C ABI with host buffers: upload the
+    particles from host memory, run the steps, read each step's counters
+    and the sampled fields (the GSIS hand-off, [cell][18] FP64) back."""
+    import torch
+    from pydsmc import gpu
+    p = gpu.default_params(precision=gpu.PRECISION_MIXED, seed=3000 + rank, zones=wl["zones"],
+                           inflow_dir=wl["inflow_dir"], nss=10 ** 9, nscheme=100, nrepeat=100)
+    case = gpu.Case(wl["dm"], wl["mess"], p, device=torch.cuda.current_device())
+    # warm the graph on a throwaway upload
+    case.upload_particles(fill["x"], fill["v"], fill["ir"], fill["cell"])
+    for s in range(1, args.warmup + 1):
+        case.step(s)
+    case.sync()
+    x = np.ascontiguousarray(fill["x"])
+    v = np.ascontiguousarray(fill["v"])
+    t0 = time.perf_counter()
+    case.upload_particles(x, v, fill["ir"], fill["cell"])
+    n0 = case.particle_count()
+    h2d = int(n0) * (7 * 8 + 4)
+    d2h = 0
+    total = 0
+    for s in range(args.warmup + 1, args.warmup + args.steps + 1):
+        case.step(s)
+        c = case.counters()
+        d2h += 12 * 8
+        total += n0
+    local = case.macro(gpu.MACRO_LOCAL)
+    d2h += local.nbytes
+    case.sync()
+    ms = (time.perf_counter() - t0) * 1e3
+    case.close()
+    return {"ms": ms, "particle_steps": total, "h2d": h2d, "d2h": d2h}
+
+
+def cpu_baseline(wl, fill, args):
+    """The reference's own DSMC step (oracle/_ref, one compute rank = one
+    core) on a bounded sample: the same mesh and constants with a reduced
+    particle count, a few steps."""
+    sys.path.insert(0, ROOT)
+    from oracle import harness as H
+    if not H.available():
+        return {"value": None, "unit": "particle-steps/s", "cores": 1, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/ref_harness not built"}
+    dm, mess = wl["dm"], wl["mess"]
+    ppc_s = max(2, min(args.ppc, 10))
+    sub = W.initial_fill(dm, mess, ppc_s, seed=7, inflow_dir=wl["inflow_dir"])
+    nsteps = 5
+    roles = {1: "interface", 2: "inlet", 3: "outlet", 4: "wall", 5: "none", 0: "none"}
+    r_arg = ",".join(f"{t}:{roles[r]}" for t, r, _ in wl["zones"])
+    with tempfile.TemporaryDirectory() as d:
+        cas = os.path.join(d, "case.cas")
+        M.write_cas(cas, wl["dm"].raw)
+        r = H.run(cas, mess, sub["x"], sub["v"], sub["ir"], sub["cell"], nsteps, 1, r_arg, nsteps + 1, timeout=600)
+    t = r["timing"]
+    return {"value": t["particle_steps_per_s"], "unit": "particle-steps/s", "cores": 1, "kind": "reference",
+            "sample": f"{wl['desc']['workload']} mesh, {ppc_s} particles/cell ({len(sub['cell'])} particles), "
+                      f"{nsteps} steps, {t['seconds']:.2f} s of one core"}
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, ROOT)
+    from oracle import harness as H
+    if not H.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness (the reference's DSMC "
+                          "code built against a one-rank MPI shim) is not built"}))
+        return
+    wl = make_workload(args.workload, args.ppc)
+    dm, mess = wl["dm"], wl["mess"]
+    cores = os.cpu_count() or 1
+    ppc_s = max(2, min(args.ppc, 10))
+    roles = {1: "interface", 2: "inlet", 3: "outlet", 4: "wall", 5: "none", 0: "none"}
+    r_arg = ",".join(f"{t}:{roles[r]}" for t, r, _ in wl["zones"])
+    nsteps = args.warmup + args.steps
+    with tempfile.TemporaryDirectory() as d:
+        cas = os.path.join(d, "case.cas")
+        M.write_cas(cas, dm.raw)
+        from concurrent.futures import ThreadPoolExecutor
+        fills = [W.initial_fill(dm, mess, ppc_s, seed=100 + k, inflow_dir=wl["inflow_dir"]) for k in range(cores)]
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=cores) as ex:
+            futs = [ex.submit(H.run, cas, mess, f["x"], f["v"], f["ir"], f["cell"], nsteps, 1 + k, r_arg, nsteps + 1, 3600)
+                    for k, f in enumerate(fills)]
+            res = [f.result() for f in futs]
+        wall = time.perf_counter() - t0
+    per = [r["timing"]["particle_steps_per_s"] for r in res]
+    agg = float(sum(per))
+    line = {"impl": "reference", "metric": METRIC, "value": agg, "unit": "particle-steps/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": wl["desc"],
+            "cpu_baseline": {"value": agg, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
+                             "sample": f"{cores} independent single-rank processes, {ppc_s} particles/cell each, "
+                                       f"{nsteps} steps each, {wall:.1f} s wall"},
+            "e2e": {"value": agg, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="block")
+    ap.add_argument("--ppc", type=int, default=200)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,530 @@
+// Device-side building blocks of the DSMC step: case views, Philox streams,
+// the exact FP64 ray/triangle test, the guarded FP32 test, and the particle
+// tracing loop (ParticleTransportOps::traceParticleDtleft,
+// src/ProcessDSMC.cpp:149-221, with CrossboundarySwitch, :1702-1829).
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dsmc {
+
+constexpr int kRoleNone = 0;
+constexpr int kRoleInterface = 1;
+constexpr int kRoleInlet = 2;
+constexpr int kRoleOutlet = 3;
+constexpr int kRoleWall = 4;
+constexpr int kRoleSpecular = 5;
+
+// Trace outcomes (ifout of the reference: 0 stayed, 1 moved, -1 removed).
+constexpr int kTraceStay = 0;
+constexpr int kTraceMoved = 1;
+constexpr int kTraceRemoved = -1;   // left through inlet/outlet
+constexpr int kTraceDropped = -2;   // no exit face (reference "Dropped")
+constexpr int kTraceLost = -3;      // crossing cap or bad neighbour
+
+// Slots of the counting sort (where a particle arrives from, seen from its
+// destination cell): 0 itself, 1..6 face neighbour j-1, 7 anything else
+// (multi-cell hops and newly injected particles).
+constexpr int kFarSlot = 7;
+constexpr int kSlots = 8;
+
+// Counter indices (DsmcCounters order, after `steps`).
+enum CounterIdx {
+    C_INJECTED = 0, C_REMOVED, C_DROPPED, C_LOST, C_WALL_HITS, C_CROSSINGS,
+    C_PAIRS, C_COLLISIONS, C_FALLBACKS, C_OVERFLOW, C_BIG_CELLS, C_COUNT
+};
+
+// Error bits in the device error word.
+constexpr int kErrCapacity = 1;
+constexpr int kErrBigCell = 2;
+constexpr int kErrRejectLoop = 4;
+constexpr int kErrSortIndex = 8;
+
+// Philox RNG stream purposes (third counter word).
+constexpr uint32_t kPurposeWall = 1;
+constexpr uint32_t kPurposeInject = 2;
+constexpr uint32_t kPurposeCollide = 3;
+
+struct DevMesh {
+    int ncell, nface, ntri, nwall;
+    const int* triOffset;        // [ncell+1]
+    const double* triD;          // [ntri*9] A, e1=B-A, e2=C-A (absolute FP64)
+    const int2* triFT;           // [ntri] face id, triangle tag
+    const float4* triF;          // [ntri*3] A-centre(3) e1(3) e2(3) |e1||e2| face tag (FP32)
+    const unsigned char* faceRole;
+    const int2* faceCells;       // [nface] c0, c1 (c1 >= ncell: ghost)
+    const float4* faceDelta;     // [nface] centre(c0) - centre(c1) as FP32
+    const int* faceWall;         // [nface] wall slot or -1
+    const double* wallRot;       // [nwall*2*9] rotation R(n) for tag 1 (or triangle), tag 2
+    const float* wallRotF;       // same, FP32
+    const double* cellCenter;    // [ncell*3]
+    const double* cellVolume;    // [ncell]
+    const int* cell2cell;        // [ncell*6]
+    const signed char* revSlot;  // [ncell*6] slot of this cell in neighbour j's list (or -1)
+};
+
+struct DevConsts {
+    double dtime;
+    double twall;        // Twall_ref
+    double sqrtTwall;
+    double vrms;
+    double neff;
+    double dtref;
+    double omega, eta, alpha, prelax, dr, nref;
+    double cdPrefactor;  // collisionDiameterPrefactor, src/ProcessDSMC.cpp:2626-2630
+    uint32_t seedLo, seedHi;
+    int maxCross;
+    int nss, nscheme, nevery, nrepeat;
+    int wallStats;
+};
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC 2011): counter-based, so every draw is a pure
+// function of (key, counter) and results do not depend on launch shape.
+// ---------------------------------------------------------------------------
+struct U4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// A sequential stream over counter (id, step, purpose, n), n = 0, 1, ...
+struct Stream {
+    uint32_t id, step, purpose, n;
+    uint32_t k0, k1;
+    U4 buf;
+    int avail;
+
+    __device__ __forceinline__ void init(uint32_t id_, uint32_t step_, uint32_t purpose_, uint32_t kLo, uint32_t kHi)
+    {
+        id = id_; step = step_; purpose = purpose_; n = 0; k0 = kLo; k1 = kHi; avail = 0;
+    }
+    __device__ __forceinline__ uint32_t next32()
+    {
+        if (avail == 0) {
+            buf = philox4x32_10(U4{id, step, purpose, n}, k0, k1);
+            ++n;
+            avail = 4;
+        }
+        const uint32_t r = (avail == 4) ? buf.x : (avail == 3) ? buf.y : (avail == 2) ? buf.z : buf.w;
+        --avail;
+        return r;
+    }
+    // uniform double in (0,1) with 53 random bits
+    __device__ __forceinline__ double uniform64()
+    {
+        const uint64_t a = next32();
+        const uint64_t b = next32();
+        const uint64_t k = (a << 21) ^ (b >> 11);
+        return ((double)k + 0.5) * 0x1.0p-53;
+    }
+    // uniform float in (0,1) with 24 random bits
+    __device__ __forceinline__ float uniform32()
+    {
+        return ((float)(next32() >> 8) + 0.5f) * 0x1.0p-24f;
+    }
+    template <typename Real> __device__ __forceinline__ Real uniform();
+};
+template <> __device__ __forceinline__ double Stream::uniform<double>() { return uniform64(); }
+template <> __device__ __forceinline__ float Stream::uniform<float>() { return uniform32(); }
+
+// ---------------------------------------------------------------------------
+// Exact FP64 arithmetic helpers: each operation rounded on its own, as the
+// reference's x86-64 build evaluates them (no fused multiply-add).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
+
+// intersectCachedTri, src/ProcessDSMC.cpp:1174-1197, operation for operation.
+__device__ __forceinline__ bool isect_exact(const double* __restrict__ T, const double x[3], const double v[3], double& t)
+{
+    const double ax = T[0], ay = T[1], az = T[2];
+    const double e1x = T[3], e1y = T[4], e1z = T[5];
+    const double e2x = T[6], e2y = T[7], e2z = T[8];
+    const double p0 = ds(dm(v[1], e2z), dm(v[2], e2y));
+    const double p1 = ds(dm(v[2], e2x), dm(v[0], e2z));
+    const double p2 = ds(dm(v[0], e2y), dm(v[1], e2x));
+    const double det = da(da(dm(e1x, p0), dm(e1y, p1)), dm(e1z, p2));
+    if (fabs(det) < 1e-14) return false;
+    const double inv = __ddiv_rn(1.0, det);
+    const double t0 = ds(x[0], ax), t1 = ds(x[1], ay), t2 = ds(x[2], az);
+    const double u = dm(da(da(dm(t0, p0), dm(t1, p1)), dm(t2, p2)), inv);
+    if (u < 0.0 || u > 1.0) return false;
+    const double q0 = ds(dm(t1, e1z), dm(t2, e1y));
+    const double q1 = ds(dm(t2, e1x), dm(t0, e1z));
+    const double q2 = ds(dm(t0, e1y), dm(t1, e1x));
+    const double vv = dm(da(da(dm(v[0], q0), dm(v[1], q1)), dm(v[2], q2)), inv);
+    if (vv < 0.0 || da(u, vv) > 1.0) return false;
+    t = dm(da(da(dm(e2x, q0), dm(e2y, q1)), dm(e2z, q2)), inv);
+    return t > 1e-14;
+}
+
+struct ExitHit {
+    int face;   // -2: none
+    int tri;
+    double t;
+};
+
+// tryCachedCellIntersection, src/ProcessDSMC.cpp:1210-1251. The reference's
+// uncached fallback (intersectFallbackCell, :1484-1524) repeats the same
+// products and sums on the same node coordinates, so it cannot find a hit the
+// cached test missed; a miss here is a miss there.
+__device__ __forceinline__ ExitHit find_exit_exact(const DevMesh& M, int cell, int crossf, int prevTri,
+                                                   const double x[3], const double v[3])
+{
+    ExitHit h{-2, -1, DBL_MAX};
+    const int b = M.triOffset[cell];
+    const int e = M.triOffset[cell + 1];
+    for (int k = b; k < e; ++k) {
+        const int2 ft = M.triFT[k];
+        if (ft.x == crossf) {
+            if (ft.y <= 0 || (prevTri != 1 && prevTri != 2) || ft.y == prevTri) continue;
+        }
+        double t = DBL_MAX;
+        if (isect_exact(M.triD + (size_t)k * 9, x, v, t) && t < h.t) {
+            h.t = t;
+            h.face = ft.x;
+            h.tri = ft.y;
+        }
+    }
+    if (h.face == -2) h.t = DBL_MAX;
+    return h;
+}
+
+// Guarded FP32 exit search. Positions are relative to the cell centre, so
+// x - A carries no cancellation from the domain's absolute coordinates.
+// Every decision the reference takes (|det| against 1e-14, u/v/u+v against
+// [0,1], t against 1e-14, the smallest t, t against dtleft) is taken in FP32
+// only when the FP32 value is farther from the threshold than an error bound
+// K*eps32/rel_det (rel_det = |det| / (|e1||e2||v|)); otherwise `ambiguous` is
+// set and the caller repeats the step in exact FP64.
+struct ExitHitF {
+    int face;
+    int tri;
+    float t;
+    float terr;
+    bool ambiguous;
+};
+
+constexpr float kGuardK = 256.0f * 5.9604645e-8f;   // 256 ulp(1) of FP32
+
+__device__ __forceinline__ ExitHitF find_exit_f32(const DevMesh& M, int cell, int crossf, int prevTri,
+                                                   const float x[3], const float v[3], float vnorm)
+{
+    ExitHitF h{-2, -1, FLT_MAX, 0.0f, false};
+    float second = FLT_MAX, secondErr = 0.0f;
+    const int b = M.triOffset[cell];
+    const int e = M.triOffset[cell + 1];
+    for (int k = b; k < e; ++k) {
+        const float4 r0 = M.triF[(size_t)k * 3 + 0];
+        const float4 r1 = M.triF[(size_t)k * 3 + 1];
+        const float4 r2 = M.triF[(size_t)k * 3 + 2];
+        const int face = __float_as_int(r2.z);
+        const int tag = __float_as_int(r2.w);
+        if (face == crossf) {
+            if (tag <= 0 || (prevTri != 1 && prevTri != 2) || tag == prevTri) continue;
+        }
+        const float ax = r0.x, ay = r0.y, az = r0.z;
+        const float e1x = r0.w, e1y = r1.x, e1z = r1.y;
+        const float e2x = r1.z, e2y = r1.w, e2z = r2.x;
+        const float e12 = r2.y;
+        const float p0 = v[1] * e2z - v[2] * e2y;
+        const float p1 = v[2] * e2x - v[0] * e2z;
+        const float p2 = v[0] * e2y - v[1] * e2x;
+        const float det = e1x * p0 + e1y * p1 + e1z * p2;
+        const float scale = e12 * vnorm;               // |e1||e2||v|
+        const float adet = fabsf(det);
+        if (!(adet > 1e-6f * scale) || adet < 1e-13f) {
+            // near-parallel ray, degenerate triangle or |det| near the
+            // reference's absolute 1e-14 cut: FP32 cannot decide
+            if (scale > 0.0f) h.ambiguous = true;
+            continue;
+        }
+        const float inv = 1.0f / det;
+        const float err = kGuardK * scale * fabsf(inv);  // bound on |u|,|v| errors
+        const float t0 = x[0] - ax, t1 = x[1] - ay, t2 = x[2] - az;
+        const float u = (t0 * p0 + t1 * p1 + t2 * p2) * inv;
+        if (u < -err || u > 1.0f + err) continue;      // certain miss
+        const float q0 = t1 * e1z - t2 * e1y;
+        const float q1 = t2 * e1x - t0 * e1z;
+        const float q2 = t0 * e1y - t1 * e1x;
+        const float w = (v[0] * q0 + v[1] * q1 + v[2] * q2) * inv;
+        if (w < -err || u + w > 1.0f + 2.0f * err) continue;
+        const float t = (e2x * q0 + e2y * q1 + e2z * q2) * inv;
+        // time error: relative err plus the position-scale term
+        const float tErr = err * (fabsf(t) + (fabsf(t0) + fabsf(t1) + fabsf(t2)) / fmaxf(vnorm, 1e-30f));
+        if (t < -tErr) continue;                       // certain miss (behind)
+        const bool inside = (u > err) && (u < 1.0f - err) && (w > err) && (u + w < 1.0f - 2.0f * err);
+        if (!inside || t <= fmaxf(tErr, 1e-13f)) {
+            h.ambiguous = true;
+            continue;
+        }
+        if (t < h.t) {
+            second = h.t; secondErr = h.terr;
+            h.t = t; h.terr = tErr; h.face = face; h.tri = tag;
+        } else if (t < second) {
+            second = t; secondErr = tErr;
+        }
+    }
+    if (h.face != -2 && second < FLT_MAX && second - h.t <= h.terr + secondErr) h.ambiguous = true;
+    return h;
+}
+
+// ---------------------------------------------------------------------------
+// Particle state in registers and the tracing loop.
+// ---------------------------------------------------------------------------
+template <typename Real>
+struct PRegs {
+    Real x[3];   // FP64: absolute; FP32: relative to the centre of `cell`
+    Real v[3];
+    Real ir;
+};
+
+struct TraceLog {        // optional per-particle record for the tracing check
+    int hitFace;
+    int hitTri;
+    int ncross;
+};
+
+struct WallTally {
+    double* tally;       // [nwall*6] or nullptr
+};
+
+// Diffuse re-emission at a wall (CrossboundarySwitch Wall case,
+// src/ProcessDSMC.cpp:1793-1825): Maxwellian at Twall_ref in the local frame
+// of the wall normal, rotational energy -ln(r) Tw / 2.
+template <typename Real>
+__device__ __forceinline__ void diffuse_reflect(const DevMesh& M, const DevConsts& C, int wslot, int tag,
+                                                PRegs<Real>& p, Stream& rng)
+{
+    const int which = (tag == 2) ? 1 : 0;
+    const Real r1 = rng.uniform<Real>();
+    const Real r2 = rng.uniform<Real>();
+    const Real al = rng.uniform<Real>();
+    const Real r3 = rng.uniform<Real>();
+    Real s, c;
+    if constexpr (sizeof(Real) == 8) {
+        sincospi(2.0 * al, &s, &c);
+        const double* R = M.wallRot + ((size_t)wslot * 2 + which) * 9;
+        const double st = C.sqrtTwall;
+        const double a = sqrt(-log(r2));
+        const double vxp = a * s * st;
+        const double vyp = a * c * st;
+        const double vzp = -sqrt(-log(r1)) * st;
+        p.v[0] = R[0] * vxp + R[1] * vyp + R[2] * vzp;
+        p.v[1] = R[3] * vxp + R[4] * vyp + R[5] * vzp;
+        p.v[2] = R[6] * vxp + R[7] * vyp + R[8] * vzp;
+        p.ir = -log(r3) * C.twall * 0.5;
+    } else {
+        sincospif(2.0f * al, &s, &c);
+        const float* R = M.wallRotF + ((size_t)wslot * 2 + which) * 9;
+        const float st = (float)C.sqrtTwall;
+        const float a = sqrtf(-__logf(r2));
+        const float vxp = a * s * st;
+        const float vyp = a * c * st;
+        const float vzp = -sqrtf(-__logf(r1)) * st;
+        p.v[0] = R[0] * vxp + R[1] * vyp + R[2] * vzp;
+        p.v[1] = R[3] * vxp + R[4] * vyp + R[5] * vzp;
+        p.v[2] = R[6] * vxp + R[7] * vyp + R[8] * vzp;
+        p.ir = -__logf(r3) * (float)C.twall * 0.5f;
+    }
+}
+
+// Mirror reflection about the wall normal (third column of R); no reference
+// counterpart (the reference leaves such tags unmapped).
+template <typename Real>
+__device__ __forceinline__ void specular_reflect(const DevMesh& M, int wslot, int tag, PRegs<Real>& p)
+{
+    const int which = (tag == 2) ? 1 : 0;
+    Real n0, n1, n2;
+    if constexpr (sizeof(Real) == 8) {
+        const double* R = M.wallRot + ((size_t)wslot * 2 + which) * 9;
+        n0 = R[2]; n1 = R[5]; n2 = R[8];
+    } else {
+        const float* R = M.wallRotF + ((size_t)wslot * 2 + which) * 9;
+        n0 = R[2]; n1 = R[5]; n2 = R[8];
+    }
+    const Real vn = p.v[0] * n0 + p.v[1] * n1 + p.v[2] * n2;
+    p.v[0] -= 2 * vn * n0;
+    p.v[1] -= 2 * vn * n1;
+    p.v[2] -= 2 * vn * n2;
+}
+
+// Counters accumulated per thread and flushed once per warp.
+struct TraceCounts {
+    uint32_t removed, dropped, lost, wall, cross, fallback;
+};
+
+// Trace one particle, starting in `cell` having entered through face
+// `crossf` / triangle `tag` (-1/-1 for a particle at rest in its cell), for
+// `dtleft` (updated: the time not flown when the trace stops). Returns the
+// reference's outcome and leaves the final cell in `cell`.
+template <typename Real>
+__device__ __forceinline__ void advance(PRegs<Real>& p, Real t)
+{
+    if constexpr (sizeof(Real) == 8) {
+        for (int d = 0; d < 3; ++d) p.x[d] = da(p.x[d], dm(p.v[d], t));
+    } else {
+        for (int d = 0; d < 3; ++d) p.x[d] += p.v[d] * t;
+    }
+}
+
+template <typename Real>
+__device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>& p, int& cell,
+                             int crossf, int tag, Real& dtleft, Stream& rng, int istep,
+                             double* wallTally, TraceCounts& cnt, bool stopAtWall, TraceLog* log)
+{
+    int ifout = kTraceStay;
+    int iter = 0;
+    while (dtleft > (Real)0) {
+        if (iter++ >= C.maxCross) { cnt.lost++; dtleft = 0; return kTraceLost; }
+        int face, tri;
+        Real t;
+        bool stays;
+        if constexpr (sizeof(Real) == 8) {
+            const ExitHit h = find_exit_exact(M, cell, crossf, tag, p.x, p.v);
+            if (h.face == -2 || !isfinite(h.t) || h.t <= 0.0) { cnt.dropped++; dtleft = 0; return kTraceDropped; }
+            face = h.face; tri = h.tri; t = h.t;
+            stays = t >= dtleft;
+        } else {
+            const float vnorm = sqrtf(p.v[0] * p.v[0] + p.v[1] * p.v[1] + p.v[2] * p.v[2]);
+            const ExitHitF h = find_exit_f32(M, cell, crossf, tag, p.x, p.v, vnorm);
+            bool amb = h.ambiguous;
+            if (!amb && h.face != -2 &&
+                fabsf(h.t - dtleft) <= h.terr + 4.8e-7f * (dtleft + (float)C.dtime)) amb = true;
+            if (amb) {
+                // Repeat this crossing step in exact FP64 from the same state.
+                cnt.fallback++;
+                const double* cc = M.cellCenter + (size_t)cell * 3;
+                double xa[3] = {cc[0] + (double)p.x[0], cc[1] + (double)p.x[1], cc[2] + (double)p.x[2]};
+                const double va[3] = {(double)p.v[0], (double)p.v[1], (double)p.v[2]};
+                const ExitHit he = find_exit_exact(M, cell, crossf, tag, xa, va);
+                if (he.face == -2 || !isfinite(he.t) || he.t <= 0.0) { cnt.dropped++; dtleft = 0; return kTraceDropped; }
+                face = he.face; tri = he.tri;
+                const double dl = (double)dtleft;
+                if (he.t >= dl) {
+                    for (int d = 0; d < 3; ++d) p.x[d] = (float)(da(xa[d], dm(va[d], dl)) - cc[d]);
+                    dtleft = 0;
+                    return ifout;
+                }
+                stays = false;
+                t = (float)he.t;
+                if (!(t < dtleft)) t = nextafterf(dtleft, 0.0f);
+            } else {
+                if (h.face == -2 || !(h.t > 0.0f)) { cnt.dropped++; dtleft = 0; return kTraceDropped; }
+                face = h.face; tri = h.tri; t = h.t;
+                stays = t >= dtleft;
+            }
+        }
+        if (stays) {
+            advance(p, dtleft);
+            dtleft = 0;
+            return ifout;
+        }
+        crossf = face;
+        tag = tri;
+        const int role = M.faceRole[face];
+        if (log && role != kRoleInterface && log->hitFace < 0) {
+            log->hitFace = face;
+            log->hitTri = tri;
+            if (stopAtWall && role == kRoleWall) {
+                advance(p, t);
+                if constexpr (sizeof(Real) == 8) dtleft = ds(dtleft, t); else dtleft -= t;
+                return ifout;
+            }
+        }
+        cnt.cross++;
+        if (log) log->ncross++;
+        // x += v t (scalar_product, src/ProcessDSMC.cpp:1611-1617) for every
+        // role that has a handler
+        if (role != kRoleNone) advance(p, t);
+        if (role == kRoleInterface) {
+            ifout = kTraceMoved;
+            if constexpr (sizeof(Real) == 8) dtleft = ds(dtleft, t); else dtleft -= t;
+            const int2 cc = M.faceCells[face];
+            int next;
+            if (cell == cc.x) next = cc.y;
+            else if (cell == cc.y) next = cc.x;
+            else next = cc.x;
+            if (next < 0 || next >= M.ncell) { cnt.lost++; dtleft = 0; return kTraceLost; }
+            if constexpr (sizeof(Real) == 4) {
+                const float4 dl = M.faceDelta[face];
+                const float sg = (cell == cc.x) ? 1.0f : -1.0f;
+                p.x[0] += sg * dl.x; p.x[1] += sg * dl.y; p.x[2] += sg * dl.z;
+            }
+            cell = next;
+        } else if (role == kRoleInlet || role == kRoleOutlet) {
+            cnt.removed++;
+            dtleft = 0;
+            return kTraceRemoved;
+        } else if (role == kRoleWall) {
+            if constexpr (sizeof(Real) == 8) dtleft = ds(dtleft, t); else dtleft -= t;
+            const int ws = M.faceWall[face];
+            const Real v0 = p.v[0], v1 = p.v[1], v2 = p.v[2], ir0 = p.ir;
+            diffuse_reflect<Real>(M, C, ws, tri, p, rng);
+            cnt.wall++;
+            if (wallTally && C.wallStats && istep > C.nss) {
+                double* T = wallTally + (size_t)ws * 6;
+                const double a0 = (double)p.v[0], a1 = (double)p.v[1], a2 = (double)p.v[2];
+                const double b0 = (double)v0, b1 = (double)v1, b2 = (double)v2;
+                atomicAdd(T + 0, 1.0);
+                atomicAdd(T + 1, a0 - b0);
+                atomicAdd(T + 2, a1 - b1);
+                atomicAdd(T + 3, a2 - b2);
+                atomicAdd(T + 4, 0.5 * ((a0 * a0 + a1 * a1 + a2 * a2) - (b0 * b0 + b1 * b1 + b2 * b2)));
+                atomicAdd(T + 5, (double)p.ir - (double)ir0);
+            }
+        } else if (role == kRoleSpecular) {
+            if constexpr (sizeof(Real) == 8) dtleft = ds(dtleft, t); else dtleft -= t;
+            specular_reflect<Real>(M, M.faceWall[face], tri, p);
+            cnt.wall++;
+        }
+        // kRoleNone: no handler (src/ProcessDSMC.cpp:1826-1827); the next
+        // search excludes this face and the particle is dropped.
+    }
+    return ifout;
+}
+
+// Warp-aggregated atomic claim of `n` consecutive slots in counter[key];
+// returns this lane's slot. Lanes with key < 0 take no slot. The whole warp
+// must call it together (full mask).
+__device__ __forceinline__ int warp_claim(int* counter, int key)
+{
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (key >= 0 && lane == leader) base = atomicAdd(counter + key, __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ void flush_counts(unsigned long long* ctr, const TraceCounts& c)
+{
+    uint32_t v[6] = {c.removed, c.dropped, c.lost, c.wall, c.cross, c.fallback};
+    const int idx[6] = {C_REMOVED, C_DROPPED, C_LOST, C_WALL_HITS, C_CROSSINGS, C_FALLBACKS};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        uint32_t s = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0 && s) atomicAdd(ctr + idx[k], (unsigned long long)s);
+    }
+}
+
+}  // namespace dsmc

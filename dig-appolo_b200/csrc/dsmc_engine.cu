@@ -1,0 +1,1279 @@
+// Host engine behind the C ABI (include/dsmc_gpu.h): builds the device mesh
+// caches from the reference's mesh arrays, owns all device state of one
+// case, and orchestrates the step stages on one stream (replayed as a CUDA
+// graph in production).
+#include "dsmc_gpu.h"
+#include "dsmc_kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+namespace dsmc {
+
+static_assert(sizeof(DsmcCellRec) == 120, "DsmcCell layout");
+static_assert(sizeof(DsmcEdgeRec) == 88, "DsmcEdge layout");
+static_assert(sizeof(DsmcMeshMessage) == 344, "meshMessage layout");
+
+namespace {
+
+constexpr unsigned char kSplit02 = 0;
+constexpr unsigned char kSplit13 = 1;
+
+// meshImport::decode_quad_split_tag, src/meshImport.h:309-327
+void decode_split(unsigned char tag, int t0[3], int t1[3])
+{
+    if (tag == kSplit02) {
+        t0[0] = 0; t0[1] = 1; t0[2] = 2; t1[0] = 0; t1[1] = 2; t1[2] = 3;
+    } else if (tag == kSplit13) {
+        t0[0] = 0; t0[1] = 1; t0[2] = 3; t1[0] = 1; t1[1] = 2; t1[2] = 3;
+    } else {
+        t0[0] = t0[1] = t0[2] = -1; t1[0] = t1[1] = t1[2] = -1;
+    }
+}
+
+// ProcessDSMC::normalize, src/ProcessDSMC.cpp:1564-1570
+void normalize3(double v[3])
+{
+    const double len = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    v[0] /= len;
+    v[1] /= len;
+    v[2] /= len;
+}
+
+// MeshparticalInitial::crossProduct, src/MeshparticalInitial.cpp:819-823
+void cross3(const double* a, const double* b, double* r)
+{
+    r[0] = a[1] * b[2] - a[2] * b[1];
+    r[1] = a[2] * b[0] - a[0] * b[2];
+    r[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// MeshparticalInitial::dotProduct, src/MeshparticalInitial.cpp:829-835
+double dot3(const double* a, const double* b)
+{
+    double r = 0.0;
+    for (int i = 0; i < 3; ++i) r += a[i] * b[i];
+    return r;
+}
+
+// ProcessDSMC::buildRotationMatrix, src/ProcessDSMC.cpp:1583-1603
+void rotation(const double* n, double R[9])
+{
+    double t1[3], t2[3];
+    if ((std::fabs(n[0]) <= std::fabs(n[1])) && (std::fabs(n[0]) <= std::fabs(n[2]))) {
+        t1[0] = 0.0; t1[1] = n[2]; t1[2] = -n[1];
+    } else if (std::fabs(n[1]) < std::fabs(n[2])) {
+        t1[0] = n[2]; t1[1] = 0.0; t1[2] = -n[0];
+    } else {
+        t1[0] = n[1]; t1[1] = -n[0]; t1[2] = 0.0;
+    }
+    normalize3(t1);
+    cross3(n, t1, t2);
+    normalize3(t2);
+    R[0] = t1[0]; R[1] = t2[0]; R[2] = n[0];
+    R[3] = t1[1]; R[4] = t2[1]; R[5] = n[1];
+    R[6] = t1[2]; R[7] = t2[2]; R[8] = n[2];
+}
+
+template <typename T>
+struct DevArray {
+    T* p = nullptr;
+    size_t n = 0;
+};
+
+}  // namespace
+
+struct Engine {
+    int device = 0;
+    int smCount = 148;
+    cudaStream_t stream = nullptr;
+    int precision = DSMC_PRECISION_FP64;
+    DsmcCaseParams params{};
+    DsmcMeshMessage mess{};
+    int ncell = 0, nface = 0, npoint = 0, ntri = 0, nwall = 0;
+    std::vector<DsmcCellRec> cells;
+    std::vector<DsmcEdgeRec> edges;
+    std::vector<double> points;
+    std::vector<unsigned char> split;
+    std::vector<int> faceRole;
+    std::vector<int> faceWallHost;
+    std::vector<double> cellCenterHost;
+    std::string err;
+
+    // device allocations
+    std::vector<void*> allocs;
+    DevMesh M{};
+    DevConsts C{};
+    DevPatches P{};
+    void* buf[2][8] = {};          // x,y,z,vx,vy,vz,ir (Real), cell (int)
+    int* start[2] = {nullptr, nullptr};
+    int* rank = nullptr;
+    int* idx = nullptr;
+    int* countSlot = nullptr;
+    int* scanPartial = nullptr;
+    double* crmax = nullptr;
+    double* remColl = nullptr;
+    double* remInj = nullptr;
+    double* acc = nullptr;
+    double* record = nullptr;
+    double* local = nullptr;
+    double* finalRecord = nullptr;
+    double* stepMom = nullptr;
+    unsigned char* sparseState = nullptr;
+    int* sparseAccum = nullptr;
+    double* windowSamples = nullptr;
+    char* windowValid = nullptr;
+    double* wallTally = nullptr;
+    StepCtl* ctl = nullptr;
+    unsigned long long* counters = nullptr;
+    int* bigList = nullptr;
+    int* bigCount = nullptr;
+    int* errorWord = nullptr;
+
+    int64_t capacity = 0;
+    int cur = 0;                   // which buffer holds the particles
+    bool haveParticles = false;
+    bool pendingInject = false;    // injected particles not yet sorted
+    bool localLazy = false;
+    int lastIstep = 0;             // step of the last statistic_macro
+    int curIstep = 0;              // step of the last stage call
+    uint64_t steps = 0;
+    int hostNLive = 0;
+
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool timing = false;
+    cudaEvent_t ev[5] = {};
+    double stageMs[4] = {0, 0, 0, 0};
+    int64_t timedSteps = 0;
+
+    ~Engine() { release(); }
+
+    void release()
+    {
+        if (device >= 0) cudaSetDevice(device);
+        for (auto& g : graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        for (auto& e : ev)
+            if (e) { cudaEventDestroy(e); e = nullptr; }
+        for (void* p : allocs) cudaFree(p);
+        allocs.clear();
+        if (stream) { cudaStreamDestroy(stream); stream = nullptr; }
+    }
+
+    bool fail(const std::string& m)
+    {
+        err = m;
+        return false;
+    }
+    bool cuda(cudaError_t e, const char* what)
+    {
+        if (e == cudaSuccess) return true;
+        err = std::string(what) + ": " + cudaGetErrorString(e);
+        return false;
+    }
+    template <typename T>
+    bool alloc(T*& p, size_t n, bool zero = true)
+    {
+        void* q = nullptr;
+        const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+        const cudaError_t e = cudaMalloc(&q, bytes);
+        if (e != cudaSuccess) {
+            err = std::string("cudaMalloc ") + std::to_string(bytes) + " B: " + cudaGetErrorString(e);
+            return false;
+        }
+        allocs.push_back(q);
+        p = static_cast<T*>(q);
+        if (zero) return cuda(cudaMemsetAsync(q, 0, bytes, stream), "cudaMemset");
+        return true;
+    }
+    template <typename T>
+    bool upload(T*& p, const std::vector<T>& h)
+    {
+        if (!alloc(p, h.size(), false)) return false;
+        if (h.empty()) return true;
+        return cuda(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream), "upload");
+    }
+    void freePtr(void* p)
+    {
+        if (!p) return;
+        cudaFree(p);
+        allocs.erase(std::remove(allocs.begin(), allocs.end(), p), allocs.end());
+    }
+
+    size_t realSize() const { return precision == DSMC_PRECISION_MIXED ? sizeof(float) : sizeof(double); }
+
+    int roleOfTag(int tag, bool* inject) const
+    {
+        for (int z = 0; z < params.nzones && z < DSMC_MAX_ZONES; ++z)
+            if (params.zone_tag[z] == tag) {
+                if (inject) *inject = params.zone_inject[z] != 0;
+                return params.zone_role[z];
+            }
+        if (inject) *inject = false;
+        return DSMC_ROLE_NONE;
+    }
+
+    bool loadPoint(int idx, double P3[3]) const
+    {
+        if (idx < 0 || (size_t)idx * 3 + 2 >= points.size()) return false;
+        P3[0] = points[(size_t)idx * 3];
+        P3[1] = points[(size_t)idx * 3 + 1];
+        P3[2] = points[(size_t)idx * 3 + 2];
+        return true;
+    }
+
+    // ------------------------------------------------------------------
+    bool build(const DsmcMeshDesc* md, const DsmcMeshMessage* mm, const DsmcCaseParams* pp, int dev)
+    {
+        if (!md || !mm || !pp) return fail("null argument");
+        if (md->ncell <= 0 || md->nface <= 0 || md->npoint <= 0 || !md->cells || !md->edges || !md->localPointXY)
+            return fail("empty or incomplete mesh");
+        params = *pp;
+        mess = *mm;
+        precision = params.precision;
+        if (precision != DSMC_PRECISION_FP64 && precision != DSMC_PRECISION_MIXED) return fail("bad precision");
+        if (params.nevery <= 0 || params.nrepeat <= 0 || params.nscheme <= 0) return fail("bad sampling controls");
+        if (params.max_crossings <= 0) params.max_crossings = 4096;
+        if (!(mess.dtime > 0.0) || !(mess.Neff > 0.0) || !(mess.v_rms > 0.0)) return fail("bad mesh message");
+        if (dev >= 0) {
+            if (!cuda(cudaSetDevice(dev), "cudaSetDevice")) return false;
+            device = dev;
+        } else if (!cuda(cudaGetDevice(&device), "cudaGetDevice")) {
+            return false;
+        }
+        cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, device);
+        if (!cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
+        ncell = md->ncell;
+        nface = md->nface;
+        npoint = md->npoint;
+        cells.assign(md->cells, md->cells + ncell);
+        edges.assign(md->edges, md->edges + nface);
+        points.assign(md->localPointXY, md->localPointXY + (size_t)npoint * 3);
+        split.assign((size_t)nface, 255);
+        if (md->faceSplitTag) split.assign(md->faceSplitTag, md->faceSplitTag + nface);
+
+        cellCenterHost.resize((size_t)ncell * 3);
+        for (int c = 0; c < ncell; ++c)
+            for (int d = 0; d < 3; ++d) cellCenterHost[(size_t)c * 3 + d] = cells[(size_t)c].cellXY[d];
+
+        // --- face roles (BoundaryConditionTable::byTag) -------------------------------
+        faceRole.assign((size_t)nface, DSMC_ROLE_NONE);
+        for (int f = 0; f < nface; ++f) faceRole[(size_t)f] = roleOfTag(edges[(size_t)f].faceTag, nullptr);
+
+        // --- triangle cache: rebuildFaceTraversalCache, src/ProcessDSMCGeometry.cpp:145-214
+        std::vector<int> triOffset((size_t)ncell + 1, 0);
+        std::vector<double> triD;
+        std::vector<int2> triFT;
+        std::vector<float4> triF;
+        triD.reserve((size_t)ncell * 8 * 9);
+        for (int lc = 0; lc < ncell; ++lc) {
+            triOffset[(size_t)lc] = (int)triFT.size();
+            const DsmcCellRec& cl = cells[(size_t)lc];
+            const double* cc = &cellCenterHost[(size_t)lc * 3];
+            auto appendTri = [&](int faceid, int tag, int ia, int ib, int ic) {
+                double A[3], B[3], Cc[3];
+                if (!loadPoint(ia, A) || !loadPoint(ib, B) || !loadPoint(ic, Cc)) return;
+                const double e1[3] = {B[0] - A[0], B[1] - A[1], B[2] - A[2]};
+                const double e2[3] = {Cc[0] - A[0], Cc[1] - A[1], Cc[2] - A[2]};
+                for (int d = 0; d < 3; ++d) triD.push_back(A[d]);
+                for (int d = 0; d < 3; ++d) triD.push_back(e1[d]);
+                for (int d = 0; d < 3; ++d) triD.push_back(e2[d]);
+                triFT.push_back(make_int2(faceid, tag));
+                float ar[3], f1[3], f2[3];
+                for (int d = 0; d < 3; ++d) {
+                    ar[d] = (float)(A[d] - cc[d]);
+                    f1[d] = (float)e1[d];
+                    f2[d] = (float)e2[d];
+                }
+                const double n1 = std::sqrt((double)f1[0] * f1[0] + (double)f1[1] * f1[1] + (double)f1[2] * f1[2]);
+                const double n2 = std::sqrt((double)f2[0] * f2[0] + (double)f2[1] * f2[1] + (double)f2[2] * f2[2]);
+                float fi, ti;
+                std::memcpy(&fi, &faceid, 4);
+                std::memcpy(&ti, &tag, 4);
+                triF.push_back(make_float4(ar[0], ar[1], ar[2], f1[0]));
+                triF.push_back(make_float4(f1[1], f1[2], f2[0], f2[1]));
+                triF.push_back(make_float4(f2[2], (float)(n1 * n2), fi, ti));
+            };
+            for (int m = 0; m < cl.num && m < 6; ++m) {
+                const int faceid = cl.cell2face[m];
+                if (faceid < 0 || faceid >= nface) continue;
+                const DsmcEdgeRec& face = edges[(size_t)faceid];
+                const int* ids = face.faceMap;
+                if (face.faceType == 3) {
+                    appendTri(faceid, -1, ids[0], ids[1], ids[2]);
+                    continue;
+                }
+                if (face.faceType != 4) continue;
+                int t0[3], t1[3];
+                decode_split(split[(size_t)faceid], t0, t1);
+                if (t0[0] < 0 || t1[0] < 0) decode_split(kSplit02, t0, t1);
+                appendTri(faceid, 1, ids[t0[0]], ids[t0[1]], ids[t0[2]]);
+                appendTri(faceid, 2, ids[t1[0]], ids[t1[1]], ids[t1[2]]);
+            }
+        }
+        triOffset[(size_t)ncell] = (int)triFT.size();
+        ntri = (int)triFT.size();
+
+        // --- wall / specular slots and rotations (getWallNormal +
+        //     processFacesQuadNormals + buildRotationMatrix)
+        auto quadNormals = [&](int fid, double n1[3], double n2[3]) -> bool {
+            const DsmcEdgeRec& e = edges[(size_t)fid];
+            double P4[4][3];
+            for (int k = 0; k < 4; ++k)
+                if (!loadPoint(e.faceMap[k], P4[k])) return false;
+            unsigned char tag = split[(size_t)fid];
+            int t0[3], t1[3];
+            decode_split(tag, t0, t1);
+            if (t0[0] < 0 || t1[0] < 0) decode_split(kSplit02, t0, t1);
+            auto make = [&](const int tri[3], double n[3]) {
+                const double* X = P4[tri[0]];
+                const double* Y = P4[tri[1]];
+                const double* Z = P4[tri[2]];
+                const double e1[3] = {Y[0] - X[0], Y[1] - X[1], Y[2] - X[2]};
+                const double e2[3] = {Z[0] - X[0], Z[1] - X[1], Z[2] - X[2]};
+                cross3(e1, e2, n);
+                normalize3(n);
+                if (dot3(e.edgeNormal, n) < 0.0) {
+                    n[0] *= -1.0; n[1] *= -1.0; n[2] *= -1.0;
+                }
+            };
+            make(t0, n1);
+            make(t1, n2);
+            return true;
+        };
+        faceWallHost.assign((size_t)nface, -1);
+        std::vector<double> wallRot;
+        std::vector<float> wallRotF;
+        for (int f = 0; f < nface; ++f) {
+            const int role = faceRole[(size_t)f];
+            if (role != DSMC_ROLE_WALL && role != DSMC_ROLE_SPECULAR) continue;
+            faceWallHost[(size_t)f] = nwall++;
+            const DsmcEdgeRec& e = edges[(size_t)f];
+            double nbase[3] = {e.edgeNormal[0], e.edgeNormal[1], e.edgeNormal[2]};
+            normalize3(nbase);
+            double n1[3] = {nbase[0], nbase[1], nbase[2]}, n2[3] = {nbase[0], nbase[1], nbase[2]};
+            if (e.faceType == 4) {
+                double q1[3], q2[3];
+                if (quadNormals(f, q1, q2)) {
+                    std::memcpy(n1, q1, sizeof n1);
+                    std::memcpy(n2, q2, sizeof n2);
+                }
+            }
+            double R[9];
+            rotation(n1, R);
+            for (int k = 0; k < 9; ++k) { wallRot.push_back(R[k]); wallRotF.push_back((float)R[k]); }
+            rotation(n2, R);
+            for (int k = 0; k < 9; ++k) { wallRot.push_back(R[k]); wallRotF.push_back((float)R[k]); }
+        }
+
+        // --- face cells / deltas
+        std::vector<int2> faceCells((size_t)nface);
+        std::vector<float4> faceDelta((size_t)nface, make_float4(0, 0, 0, 0));
+        std::vector<unsigned char> roleU8((size_t)nface);
+        for (int f = 0; f < nface; ++f) {
+            const int c0 = edges[(size_t)f].faceMap[4], c1 = edges[(size_t)f].faceMap[5];
+            faceCells[(size_t)f] = make_int2(c0, c1);
+            roleU8[(size_t)f] = (unsigned char)faceRole[(size_t)f];
+            if (c0 >= 0 && c0 < ncell && c1 >= 0 && c1 < ncell) {
+                faceDelta[(size_t)f] = make_float4(
+                    (float)(cellCenterHost[(size_t)c0 * 3] - cellCenterHost[(size_t)c1 * 3]),
+                    (float)(cellCenterHost[(size_t)c0 * 3 + 1] - cellCenterHost[(size_t)c1 * 3 + 1]),
+                    (float)(cellCenterHost[(size_t)c0 * 3 + 2] - cellCenterHost[(size_t)c1 * 3 + 2]), 0.0f);
+            }
+        }
+
+        // --- neighbour slots for the counting sort
+        std::vector<int> c2c((size_t)ncell * 6, -1);
+        std::vector<signed char> rev((size_t)ncell * 6, -1);
+        std::vector<double> vol((size_t)ncell);
+        for (int c = 0; c < ncell; ++c) {
+            vol[(size_t)c] = cells[(size_t)c].area;
+            for (int j = 0; j < 6 && j < cells[(size_t)c].num; ++j) c2c[(size_t)c * 6 + j] = cells[(size_t)c].cell2cell[j];
+        }
+        for (int c = 0; c < ncell; ++c) {
+            for (int j = 0; j < 6 && j < cells[(size_t)c].num; ++j) {
+                const int nb = c2c[(size_t)c * 6 + j];
+                const int f = cells[(size_t)c].cell2face[j];
+                if (nb < 0 || nb >= ncell) continue;
+                for (int p = 0; p < 6 && p < cells[(size_t)nb].num; ++p)
+                    if (cells[(size_t)nb].cell2face[p] == f) { rev[(size_t)c * 6 + j] = (signed char)p; break; }
+            }
+        }
+
+        // --- inlet emit patches: rebuildBoundaryEmitCache, src/ProcessDSMC.cpp:583-768
+        if (!buildPatches()) return false;
+
+        // --- device constants
+        C.dtime = mess.dtime;
+        C.twall = mess.Twall_ref;
+        C.sqrtTwall = std::sqrt(mess.Twall_ref);
+        C.vrms = mess.v_rms;
+        C.neff = mess.Neff;
+        C.dtref = mess.dt_ref;
+        C.omega = mess.omega;
+        C.eta = mess.eta;
+        C.alpha = mess.alpha;
+        C.prelax = mess.P_relax;
+        C.dr = mess.dr;
+        C.nref = mess.n_ref;
+        {
+            const double conDen = std::tgamma(5.0 / 2.0 - mess.omega);
+            const double dref2 = mess.d_ref * mess.d_ref;
+            C.cdPrefactor = M_PI * dref2 * std::pow(2 * mess.kB * mess.T_ref / mess.p_mass_r, mess.eta) / conDen;
+        }
+        C.seedLo = (uint32_t)(params.seed & 0xffffffffu);
+        C.seedHi = (uint32_t)(params.seed >> 32);
+        C.maxCross = params.max_crossings;
+        C.nss = params.nss;
+        C.nscheme = params.nscheme;
+        C.nevery = params.nevery;
+        C.nrepeat = params.nrepeat;
+        C.wallStats = params.wall_stats;
+
+        // --- device mesh
+        int* dTriOffset; double* dTriD; int2* dTriFT; float4* dTriF; unsigned char* dRole; int2* dFaceCells;
+        float4* dDelta; int* dFaceWall; double* dWallRot; float* dWallRotF; double* dCenter; double* dVol;
+        int* dC2c; signed char* dRev;
+        if (!upload(dTriOffset, triOffset) || !upload(dTriD, triD) || !upload(dTriFT, triFT) || !upload(dTriF, triF) ||
+            !upload(dRole, roleU8) || !upload(dFaceCells, faceCells) || !upload(dDelta, faceDelta) ||
+            !upload(dFaceWall, faceWallHost) || !upload(dWallRot, wallRot) || !upload(dWallRotF, wallRotF) ||
+            !upload(dCenter, cellCenterHost) || !upload(dVol, vol) || !upload(dC2c, c2c) || !upload(dRev, rev))
+            return false;
+        M.ncell = ncell; M.nface = nface; M.ntri = ntri; M.nwall = nwall;
+        M.triOffset = dTriOffset; M.triD = dTriD; M.triFT = dTriFT; M.triF = dTriF;
+        M.faceRole = dRole; M.faceCells = dFaceCells; M.faceDelta = dDelta; M.faceWall = dFaceWall;
+        M.wallRot = dWallRot; M.wallRotF = dWallRotF; M.cellCenter = dCenter; M.cellVolume = dVol;
+        M.cell2cell = dC2c; M.revSlot = dRev;
+
+        // --- per-cell state (Collision_constant_initial, src/MeshparticalInitial.cpp:798-810)
+        std::vector<double> crInit((size_t)ncell, 3.0);
+        if (!upload(crmax, crInit)) return false;
+        if (!alloc(remColl, (size_t)ncell) || !alloc(remInj, (size_t)ncell) || !alloc(acc, (size_t)ncell * 54) ||
+            !alloc(record, (size_t)ncell * 18) || !alloc(local, (size_t)ncell * 18) ||
+            !alloc(finalRecord, (size_t)ncell * 18) || !alloc(sparseState, (size_t)ncell) ||
+            !alloc(sparseAccum, (size_t)ncell) || !alloc(windowSamples, (size_t)ncell) ||
+            !alloc(windowValid, (size_t)ncell) || !alloc(wallTally, (size_t)std::max(nwall, 1) * 6) ||
+            !alloc(countSlot, (size_t)ncell * kSlots) || !alloc(scanPartial, kScanBlocks) ||
+            !alloc(start[0], (size_t)ncell + 1) || !alloc(start[1], (size_t)ncell + 1) || !alloc(ctl, 1) ||
+            !alloc(counters, C_COUNT) || !alloc(bigList, (size_t)ncell) || !alloc(bigCount, 1) ||
+            !alloc(errorWord, 1))
+            return false;
+        if (params.keep_step_moments && !alloc(stepMom, (size_t)ncell * 18)) return false;
+        cudaError_t pe = (precision == DSMC_PRECISION_MIXED) ? prepare_kernels<float>() : prepare_kernels<double>();
+        if (!cuda(pe, "kernel attributes")) return false;
+        for (auto& e : ev)
+            if (!cuda(cudaEventCreate(&e), "cudaEventCreate")) return false;
+        if (params.capacity > 0 && !ensureCapacity(params.capacity)) return false;
+        return cuda(cudaStreamSynchronize(stream), "create sync");
+    }
+
+    bool buildPatches()
+    {
+        struct Patch {
+            int cell, edge, tag;
+            double geom[9], rot[9], gas[8], addBase;
+        };
+        std::vector<Patch> patches;
+        const double gamma = mess.gamma;
+        for (int f = 0; f < nface; ++f) {
+            bool inject = false;
+            const int role = roleOfTag(edges[(size_t)f].faceTag, &inject);
+            if (role != DSMC_ROLE_INLET || !inject) continue;
+            const DsmcEdgeRec& edge = edges[(size_t)f];
+            const int g1 = edge.faceMap[4], g2 = edge.faceMap[5];
+            int cellLocal = -1;
+            if (g1 >= 0 && g1 < ncell) cellLocal = g1;
+            if (cellLocal < 0 && g2 >= 0 && g2 < ncell) cellLocal = g2;
+            if (cellLocal < 0) continue;
+            const int faceType = edge.faceType;
+            if (faceType != 3 && faceType != 4) continue;
+            const int nodeCount = faceType == 4 ? 4 : 3;
+            double pts[4][3];
+            bool ok = true;
+            for (int k = 0; k < nodeCount && ok; ++k) ok = loadPoint(edge.faceMap[k], pts[k]);
+            if (!ok) continue;
+            int tri[2][3] = {{0, 1, 2}, {-1, -1, -1}};
+            int nTris = 1;
+            double qn[2][3] = {};
+            if (faceType == 4) {
+                int t0[3], t1[3];
+                decode_split(split[(size_t)f], t0, t1);
+                if (t0[0] < 0 || t1[0] < 0) decode_split(kSplit02, t0, t1);
+                for (int k = 0; k < 3; ++k) { tri[0][k] = t0[k]; tri[1][k] = t1[k]; }
+                nTris = 2;
+                // wallMap normals (processFacesQuadNormals over inletVisMove)
+                for (int s = 0; s < 2; ++s) {
+                    const int* tt = tri[s];
+                    const double* X = pts[tt[0]];
+                    const double* Y = pts[tt[1]];
+                    const double* Z = pts[tt[2]];
+                    const double e1[3] = {Y[0] - X[0], Y[1] - X[1], Y[2] - X[2]};
+                    const double e2[3] = {Z[0] - X[0], Z[1] - X[1], Z[2] - X[2]};
+                    cross3(e1, e2, qn[s]);
+                    normalize3(qn[s]);
+                    if (dot3(edge.edgeNormal, qn[s]) < 0.0) {
+                        qn[s][0] *= -1.0; qn[s][1] *= -1.0; qn[s][2] *= -1.0;
+                    }
+                }
+            }
+            for (int tagTri = 1; tagTri <= nTris; ++tagTri) {
+                const int slot = faceType == 4 ? tagTri - 1 : 0;
+                double norm[3];
+                if (faceType == 4) {
+                    for (int d = 0; d < 3; ++d) norm[d] = qn[slot][d];
+                } else {
+                    for (int d = 0; d < 3; ++d) norm[d] = edge.edgeNormal[d];
+                    const double len = std::sqrt(norm[0] * norm[0] + norm[1] * norm[1] + norm[2] * norm[2]);
+                    if (len > 0.0 && std::isfinite(len)) { norm[0] /= len; norm[1] /= len; norm[2] /= len; }
+                }
+                const double* P0 = pts[tri[slot][0]];
+                const double* P1 = pts[tri[slot][1]];
+                const double* P2 = pts[tri[slot][2]];
+                Patch pt{};
+                pt.cell = cellLocal;
+                pt.edge = f;
+                pt.tag = faceType == 3 ? -1 : tagTri;
+                for (int d = 0; d < 3; ++d) {
+                    pt.geom[d] = P0[d];
+                    pt.geom[3 + d] = P1[d] - P0[d];
+                    pt.geom[6 + d] = P2[d] - P0[d];
+                }
+                // triangleArea, src/ProcessDSMC.cpp:601-614
+                const double ax = P1[0] - P0[0], ay = P1[1] - P0[1], az = P1[2] - P0[2];
+                const double bx = P2[0] - P0[0], by = P2[1] - P0[1], bz = P2[2] - P0[2];
+                const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+                const double area = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+                const double nmag = std::sqrt(norm[0] * norm[0] + norm[1] * norm[1] + norm[2] * norm[2]);
+                if (!(area > 0.0) || !std::isfinite(area) || !(nmag > 0.0) || !std::isfinite(nmag)) continue;
+                double neg[3] = {-norm[0], -norm[1], -norm[2]};
+                double R[9];
+                rotation(neg, R);
+                for (int k = 0; k < 9; ++k) pt.rot[k] = R[k];
+                // computeBoundaryGasState, src/ProcessDSMC.cpp:2318-2367 (FreestreamInlet)
+                const double base = 1.0 * mess.Ma * std::sqrt(gamma / 2.0) * mess.v_in / mess.v_rms;
+                const double uxN = base * params.inflow_dir[0];
+                const double uyN = base * params.inflow_dir[1];
+                const double uzN = 0.0;
+                const double tN = mess.T_in / mess.T_ref;
+                const double rhoP = 1.0 * mess.n_ref;
+                const double uxP = uxN * mess.v_rms, uyP = uyN * mess.v_rms, uzP = uzN * mess.v_rms;
+                const double tP = tN * mess.T_ref;
+                const double beta = 1.0 / std::sqrt(2 * mess.kB / mess.p_mass * tP);
+                const double sx = uxP * beta, sy = uyP * beta, sz = uzP * beta;
+                // rotation[i][j] = R[3i+j]
+                const double stp1 = R[0] * sx + R[3] * sy + R[6] * sz;
+                const double stp2 = R[1] * sx + R[4] * sy + R[7] * sz;
+                const double snp = R[2] * sx + R[5] * sy + R[8] * sz;
+                const double fs1 = snp + std::sqrt(snp * snp + 2.0);
+                const double fs2 = 0.5 * (1.0 + snp * (2.0 * snp - fs1));
+                double QA = 3.0;
+                if (std::fabs(snp) > 3.0) QA = std::fabs(snp) + 1.0;
+                pt.gas[0] = snp; pt.gas[1] = fs1; pt.gas[2] = fs2; pt.gas[3] = stp1; pt.gas[4] = stp2;
+                pt.gas[5] = tN; pt.gas[6] = std::sqrt(tN); pt.gas[7] = QA;
+                // computeBoundaryInsertCount, src/ProcessDSMC.cpp:2380-2403
+                double cosTheta = 0.0;
+                const double Umag = std::sqrt(uxP * uxP + uyP * uyP + uzP * uzP);
+                if (Umag > 0.0 && nmag > 0.0)
+                    cosTheta = -((uxP * norm[0] + uyP * norm[1] + uzP * norm[2]) / (Umag * nmag));
+                const double s = beta * Umag;
+                const double scos = s * cosTheta;
+                double addNum = mess.dtime * area * rhoP / 2.0 / std::sqrt(M_PI) * std::sqrt(tP / mess.T_ref) *
+                                (std::exp(-(scos * scos)) + std::sqrt(M_PI) * scos * (1.0 + std::erf(scos)));
+                pt.addBase = addNum / mess.Neff;
+                if (!std::isfinite(pt.addBase) || pt.addBase < 0.0 || pt.addBase > 1.0e8)
+                    return fail("inflow patch count out of range");
+                patches.push_back(pt);
+            }
+        }
+        // group patches by cell, keeping their order within a cell
+        std::stable_sort(patches.begin(), patches.end(), [](const Patch& a, const Patch& b) { return a.cell < b.cell; });
+        const int np = (int)patches.size();
+        std::vector<int> groupStart;
+        std::vector<int> pc(np), pe(np), ptg(np);
+        std::vector<double> geom((size_t)np * 9), rot((size_t)np * 9), gas((size_t)np * 8), addBase(np);
+        for (int i = 0; i < np; ++i) {
+            if (i == 0 || patches[(size_t)i].cell != patches[(size_t)i - 1].cell) groupStart.push_back(i);
+            pc[(size_t)i] = patches[(size_t)i].cell;
+            pe[(size_t)i] = patches[(size_t)i].edge;
+            ptg[(size_t)i] = patches[(size_t)i].tag;
+            std::memcpy(&geom[(size_t)i * 9], patches[(size_t)i].geom, 9 * sizeof(double));
+            std::memcpy(&rot[(size_t)i * 9], patches[(size_t)i].rot, 9 * sizeof(double));
+            std::memcpy(&gas[(size_t)i * 8], patches[(size_t)i].gas, 8 * sizeof(double));
+            addBase[(size_t)i] = patches[(size_t)i].addBase;
+        }
+        const int ngroup = (int)groupStart.size();
+        groupStart.push_back(np);
+        int *dG, *dC, *dE, *dT, *dCount, *dStart;
+        double *dGeom, *dRot, *dGas, *dAdd;
+        if (!upload(dG, groupStart) || !upload(dC, pc) || !upload(dE, pe) || !upload(dT, ptg) || !upload(dGeom, geom) ||
+            !upload(dRot, rot) || !upload(dGas, gas) || !upload(dAdd, addBase) || !alloc(dCount, (size_t)np) ||
+            !alloc(dStart, (size_t)np))
+            return false;
+        P.npatch = np; P.ngroup = ngroup; P.groupStart = dG; P.cell = dC; P.edge = dE; P.triTag = dT;
+        P.geom = dGeom; P.rot = dRot; P.gas = dGas; P.addBase = dAdd; P.count = dCount; P.start = dStart;
+        return true;
+    }
+
+    bool ensureCapacity(int64_t need)
+    {
+        if (need <= capacity) return true;
+        if (need > (int64_t)0x7fffffff - 1) return fail("capacity above 2^31 particles");
+        // keep existing particles
+        std::vector<std::vector<char>> keep;
+        const size_t rs = realSize();
+        int n = haveParticles ? hostNLive : 0;
+        if (n > 0) {
+            keep.resize(8);
+            for (int k = 0; k < 8; ++k) {
+                const size_t es = (k == 7) ? sizeof(int) : rs;
+                keep[(size_t)k].resize((size_t)n * es);
+                if (!cuda(cudaMemcpyAsync(keep[(size_t)k].data(), buf[cur][k], (size_t)n * es, cudaMemcpyDeviceToHost, stream), "keep"))
+                    return false;
+            }
+            if (!cuda(cudaStreamSynchronize(stream), "keep sync")) return false;
+        }
+        for (int b = 0; b < 2; ++b)
+            for (int k = 0; k < 8; ++k) { freePtr(buf[b][k]); buf[b][k] = nullptr; }
+        freePtr(rank); freePtr(idx);
+        rank = nullptr; idx = nullptr;
+        for (auto& g : graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        const int64_t cap = need;
+        for (int b = 0; b < 2; ++b)
+            for (int k = 0; k < 8; ++k) {
+                char* p = nullptr;
+                const size_t es = (k == 7) ? sizeof(int) : rs;
+                if (!alloc(p, (size_t)cap * es, false)) return false;
+                buf[b][k] = p;
+            }
+        if (!alloc(rank, (size_t)cap, false) || !alloc(idx, (size_t)cap, true)) return false;
+        capacity = cap;
+        for (int k = 0; k < 8 && n > 0; ++k) {
+            const size_t es = (k == 7) ? sizeof(int) : rs;
+            if (!cuda(cudaMemcpyAsync(buf[cur][k], keep[(size_t)k].data(), (size_t)n * es, cudaMemcpyHostToDevice, stream), "restore"))
+                return false;
+        }
+        StepCtl h{};
+        h.nLive = n;
+        h.capacity = (int)capacity;
+        if (!cuda(cudaMemcpyAsync(ctl, &h, sizeof h, cudaMemcpyHostToDevice, stream), "ctl")) return false;
+        return cuda(cudaStreamSynchronize(stream), "capacity sync");
+    }
+
+    template <typename Real>
+    StepArgs<Real> args() const
+    {
+        StepArgs<Real> a{};
+        a.M = M; a.C = C; a.P = P;
+        const int o = cur ^ 1;
+        for (int d = 0; d < 3; ++d) {
+            a.A.x[d] = (Real*)buf[cur][d];
+            a.A.v[d] = (Real*)buf[cur][3 + d];
+            a.B.x[d] = (Real*)buf[o][d];
+            a.B.v[d] = (Real*)buf[o][3 + d];
+        }
+        a.A.ir = (Real*)buf[cur][6]; a.A.cell = (int*)buf[cur][7];
+        a.B.ir = (Real*)buf[o][6]; a.B.cell = (int*)buf[o][7];
+        a.startA = start[cur]; a.startB = start[o];
+        a.rank = rank; a.idx = idx; a.countSlot = countSlot; a.scanPartial = scanPartial;
+        a.crmax = crmax; a.remColl = remColl; a.remInj = remInj; a.acc = acc; a.record = record;
+        a.local = local; a.finalRecord = finalRecord; a.stepMom = stepMom;
+        a.sparseState = sparseState; a.sparseAccum = sparseAccum; a.windowSamples = windowSamples;
+        a.windowValid = windowValid; a.wallTally = wallTally; a.ctl = ctl; a.counters = counters;
+        a.bigList = bigList; a.bigCount = bigCount; a.errorWord = errorWord;
+        return a;
+    }
+
+    bool setIstep(int istep)
+    {
+        return cuda(cudaMemcpyAsync(&ctl->istep, &istep, sizeof(int), cudaMemcpyHostToDevice, stream), "istep");
+    }
+
+    // Enqueue the selected stages. Returns with `cur` flipped if a sort ran.
+    template <typename Real>
+    void enqueue(uint32_t stages, bool events)
+    {
+        const StepArgs<Real> a = args<Real>();
+        if (events) cudaEventRecord(ev[0], stream);
+        if (stages & DSMC_STAGE_INJECT) launch_inject<Real>(a, smCount, stream);
+        if (events) cudaEventRecord(ev[1], stream);
+        if (stages & DSMC_STAGE_MOVE) launch_move<Real>(a, smCount, stream);
+        if (events) cudaEventRecord(ev[2], stream);
+        const bool sort = (stages & DSMC_STAGE_SORT) != 0;
+        const bool coll = (stages & DSMC_STAGE_COLLIDE) != 0;
+        const bool samp = (stages & DSMC_STAGE_SAMPLE) != 0;
+        if (sort) launch_sort<Real>(a, smCount, stream);
+        if (events) cudaEventRecord(ev[3], stream);
+        if (sort && coll && samp) {
+            launch_cells<Real>(a, kModeStep, smCount, stream);
+        } else {
+            if (sort) launch_cells<Real>(a, kModeGather, smCount, stream);
+        }
+        if (sort) {
+            cudaMemcpyAsync(&ctl->nLive, &ctl->nNext, sizeof(int), cudaMemcpyDeviceToDevice, stream);
+            cudaMemsetAsync(&ctl->nInj, 0, sizeof(int), stream);
+        }
+        if (!(sort && coll && samp)) {
+            // stages that act in place on the (now) current buffer
+            StepArgs<Real> b = a;
+            if (sort) {
+                // after the sort the current buffer is the former B
+                b.A = a.B; b.B = a.A; b.startA = a.startB; b.startB = const_cast<int*>(a.startA);
+            }
+            if (coll) launch_cells<Real>(b, kModeCollide, smCount, stream);
+            if (samp) launch_cells<Real>(b, kModeSample, smCount, stream);
+        }
+        if (events) cudaEventRecord(ev[4], stream);
+    }
+
+    template <typename Real>
+    bool stepT(int istep, uint32_t stages)
+    {
+        if (!haveParticles) return fail("no particles uploaded");
+        if (stages & ~DSMC_STAGE_ALL) return fail("unknown stage flags");
+        if (!setIstep(istep)) return false;
+        curIstep = istep;
+        const bool full = stages == DSMC_STAGE_ALL;
+        if (full && !timing && std::getenv("DSMC_NO_GRAPH") == nullptr) {
+            if (!graph[cur]) {
+                cudaGraph_t g = nullptr;
+                if (!cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture")) return false;
+                enqueue<Real>(stages, false);
+                if (!cuda(cudaStreamEndCapture(stream, &g), "end capture")) return false;
+                const cudaError_t ie = cudaGraphInstantiate(&graph[cur], g, 0);
+                cudaGraphDestroy(g);
+                if (!cuda(ie, "graph instantiate")) return false;
+            }
+            if (!cuda(cudaGraphLaunch(graph[cur], stream), "graph launch")) return false;
+        } else {
+            enqueue<Real>(stages, timing);
+            if (!cuda(cudaGetLastError(), "kernel launch")) return false;
+            if (timing) {
+                if (!cuda(cudaEventSynchronize(ev[4]), "timing sync")) return false;
+                for (int k = 0; k < 4; ++k) {
+                    float ms = 0.0f;
+                    cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+                    stageMs[k] += ms;
+                }
+                ++timedSteps;
+            }
+        }
+        if (stages & DSMC_STAGE_INJECT) pendingInject = true;
+        if (stages & DSMC_STAGE_SORT) {
+            cur ^= 1;
+            pendingInject = false;
+        }
+        if (stages & DSMC_STAGE_SAMPLE) {
+            localLazy = true;
+            lastIstep = istep;
+        }
+        if (stages & DSMC_STAGE_MOVE) ++steps;
+        return true;
+    }
+
+    bool step(int istep, uint32_t stages)
+    {
+        return precision == DSMC_PRECISION_MIXED ? stepT<float>(istep, stages) : stepT<double>(istep, stages);
+    }
+
+    bool macroPre()
+    {
+        if (!haveParticles) return fail("no particles uploaded");
+        if (precision == DSMC_PRECISION_MIXED) launch_cells<float>(args<float>(), kModePre, smCount, stream);
+        else launch_cells<double>(args<double>(), kModePre, smCount, stream);
+        localLazy = false;
+        return cuda(cudaGetLastError(), "statistic_macroPre");
+    }
+
+    bool nLiveHost(int& n)
+    {
+        if (!cuda(cudaMemcpyAsync(&n, &ctl->nLive, sizeof(int), cudaMemcpyDeviceToHost, stream), "nLive")) return false;
+        if (!cuda(cudaStreamSynchronize(stream), "sync")) return false;
+        hostNLive = n;
+        return true;
+    }
+
+    bool checkDeviceErrors()
+    {
+        int e = 0;
+        if (!cuda(cudaMemcpyAsync(&e, errorWord, sizeof(int), cudaMemcpyDeviceToHost, stream), "error word")) return false;
+        if (!cuda(cudaStreamSynchronize(stream), "sync")) return false;
+        if (e & kErrRejectLoop) return fail("inflow sampling rejection loop exceeded its bound");
+        if (e & kErrSortIndex) return fail("device self-check: inconsistent sort index (error word 8)");
+        if (e & kErrBigCell) return fail("device self-check: a cell above 4096 particles kept arrival order");
+        return true;
+    }
+
+    bool uploadParticles(int64_t n, const double* px, const double* py, const double* pz, const double* vx,
+                         const double* vy, const double* vz, const double* ir, const int32_t* cell)
+    {
+        if (n < 0) return fail("negative particle count");
+        if (n > 0 && (!px || !py || !pz || !vx || !vy || !vz || !ir || !cell)) return fail("null particle array");
+        for (int64_t i = 0; i < n; ++i)
+            if (cell[i] < 0 || cell[i] >= ncell) return fail("particle cell id out of range");
+        // order: cell-major, input order within a cell
+        std::vector<int> cnt((size_t)ncell + 1, 0);
+        for (int64_t i = 0; i < n; ++i) cnt[(size_t)cell[i] + 1]++;
+        for (int c = 0; c < ncell; ++c) cnt[(size_t)c + 1] += cnt[(size_t)c];
+        std::vector<int> st(cnt.begin(), cnt.end());
+        std::vector<int64_t> order((size_t)n);
+        {
+            std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+            for (int64_t i = 0; i < n; ++i) order[(size_t)fill[(size_t)cell[i]]++] = i;
+        }
+        int64_t need = params.capacity > 0 ? params.capacity : std::max<int64_t>(n + n / 2 + (1 << 16), 1 << 20);
+        if (n > need) return fail("more particles than the configured capacity");
+        haveParticles = false;
+        if (!ensureCapacity(need)) return false;
+        const bool mixed = precision == DSMC_PRECISION_MIXED;
+        const double* src[7] = {px, py, pz, vx, vy, vz, ir};
+        std::vector<char> hb((size_t)n * 8);
+        for (int k = 0; k < 7; ++k) {
+            if (mixed) {
+                float* f = reinterpret_cast<float*>(hb.data());
+                for (int64_t j = 0; j < n; ++j) {
+                    const int64_t i = order[(size_t)j];
+                    double v = src[k][i];
+                    if (k < 3) v = v - cellCenterHost[(size_t)cell[i] * 3 + k];
+                    f[j] = (float)v;
+                }
+            } else {
+                double* d = reinterpret_cast<double*>(hb.data());
+                for (int64_t j = 0; j < n; ++j) d[j] = src[k][order[(size_t)j]];
+            }
+            if (n > 0 && (!cuda(cudaMemcpyAsync(buf[cur][k], hb.data(), (size_t)n * realSize(), cudaMemcpyHostToDevice, stream), "upload particles") ||
+                          !cuda(cudaStreamSynchronize(stream), "sync")))
+                return false;
+        }
+        std::vector<int> hc((size_t)n);
+        for (int64_t j = 0; j < n; ++j) hc[(size_t)j] = cell[order[(size_t)j]];
+        if (n > 0 && !cuda(cudaMemcpyAsync(buf[cur][7], hc.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, stream), "upload cells"))
+            return false;
+        if (!cuda(cudaMemcpyAsync(start[cur], st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice, stream), "upload start"))
+            return false;
+        StepCtl h{};
+        h.nLive = (int)n;
+        h.capacity = (int)capacity;
+        if (!cuda(cudaMemcpyAsync(ctl, &h, sizeof h, cudaMemcpyHostToDevice, stream), "ctl")) return false;
+        if (!cuda(cudaMemsetAsync(countSlot, 0, (size_t)ncell * kSlots * sizeof(int), stream), "countSlot")) return false;
+        if (!cuda(cudaStreamSynchronize(stream), "upload sync")) return false;
+        hostNLive = (int)n;
+        haveParticles = true;
+        pendingInject = false;
+        return true;
+    }
+
+    bool downloadParticles(int64_t n, double* px, double* py, double* pz, double* vx, double* vy, double* vz,
+                           double* ir, int32_t* cellOut, uint32_t* pid)
+    {
+        int nl = 0;
+        if (!nLiveHost(nl)) return false;
+        if (n != nl) return fail("particle count mismatch: call dsmc_particle_count first");
+        std::vector<int> hc((size_t)n);
+        if (n > 0 && !cuda(cudaMemcpy(hc.data(), buf[cur][7], (size_t)n * sizeof(int), cudaMemcpyDeviceToHost), "cells"))
+            return false;
+        double* dst[7] = {px, py, pz, vx, vy, vz, ir};
+        const bool mixed = precision == DSMC_PRECISION_MIXED;
+        std::vector<char> hb((size_t)n * 8);
+        for (int k = 0; k < 7; ++k) {
+            if (!dst[k] || n == 0) continue;
+            if (!cuda(cudaMemcpy(hb.data(), buf[cur][k], (size_t)n * realSize(), cudaMemcpyDeviceToHost), "particles"))
+                return false;
+            for (int64_t j = 0; j < n; ++j) {
+                double v = mixed ? (double)reinterpret_cast<float*>(hb.data())[j] : reinterpret_cast<double*>(hb.data())[j];
+                if (mixed && k < 3) v = cellCenterHost[(size_t)hc[(size_t)j] * 3 + k] + v;
+                dst[k][j] = v;
+            }
+        }
+        if (cellOut) std::memcpy(cellOut, hc.data(), (size_t)n * sizeof(int));
+        if (pid) for (int64_t j = 0; j < n; ++j) pid[j] = (uint32_t)j;
+        return true;
+    }
+
+    bool downloadMacro(int which, double* out)
+    {
+        if (!out) return fail("null output");
+        double* src = nullptr;
+        if (which == DSMC_MACRO_LOCAL) {
+            if (localLazy) launch_macro(M, C, acc, 0, (double)params.nscheme, local, ncell, stream);
+            src = local;
+        } else if (which == DSMC_MACRO_RECORD) {
+            src = record;
+        } else if (which == DSMC_MACRO_FINAL_RECORD) {
+            if (lastIstep > params.nss)
+                launch_macro(M, C, acc, 1, (double)(lastIstep - params.nss), finalRecord, ncell, stream);
+            src = finalRecord;
+        } else {
+            return fail("unknown macro target");
+        }
+        if (!cuda(cudaMemcpyAsync(out, src, (size_t)ncell * 18 * sizeof(double), cudaMemcpyDeviceToHost, stream), "macro"))
+            return false;
+        return cuda(cudaStreamSynchronize(stream), "macro sync");
+    }
+};
+
+}  // namespace dsmc
+
+struct DsmcHandle {
+    dsmc::Engine e;
+};
+
+static thread_local std::string g_createError;
+
+#define DSMC_GUARD(h)                                                   \
+    do {                                                                \
+        if (!(h)) return DSMC_E_INVALID;                                \
+        if ((h)->e.device >= 0) cudaSetDevice((h)->e.device);           \
+    } while (0)
+
+static int status_of(dsmc::Engine& e, bool ok)
+{
+    if (ok) return DSMC_OK;
+    if (e.err.find("cudaMalloc") != std::string::npos) return DSMC_E_NOMEM;
+    if (e.err.find("capacity") != std::string::npos) return DSMC_E_CAPACITY;
+    if (e.err.find(": ") != std::string::npos && e.err.find("cuda") != std::string::npos) return DSMC_E_CUDA;
+    if (e.err.find("rejection loop") != std::string::npos) return DSMC_E_DEVICE_FAULT;
+    if (e.err.find("self-check") != std::string::npos) return DSMC_E_DEVICE_FAULT;
+    if (e.err.find("no particles") != std::string::npos) return DSMC_E_STATE;
+    return DSMC_E_INVALID;
+}
+
+extern "C" {
+
+void dsmc_default_params(DsmcCaseParams* p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->precision = DSMC_PRECISION_FP64;
+    p->nss = 5000;       // src/meshImport.h:48
+    p->nscheme = 2000;   // src/meshImport.h:56
+    p->nevery = 1;       // src/meshImport.h:52
+    p->nrepeat = 100;    // src/meshImport.h:53
+    p->wall_stats = 0;   // src/meshImport.h:50
+    p->inflow_dir[0] = std::sqrt(3.0) / 2.0;   // src/ProcessDSMC.cpp:2330-2331
+    p->inflow_dir[1] = 0.5;
+    // BoundaryConditionTable::loadDefaults, src/BoundaryCondition.h:79-117
+    p->nzones = 4;
+    p->zone_tag[0] = 3; p->zone_role[0] = DSMC_ROLE_INTERFACE; p->zone_inject[0] = 0;
+    p->zone_tag[1] = 4; p->zone_role[1] = DSMC_ROLE_INLET; p->zone_inject[1] = 1;
+    p->zone_tag[2] = 5; p->zone_role[2] = DSMC_ROLE_OUTLET; p->zone_inject[2] = 0;
+    p->zone_tag[3] = 6; p->zone_role[3] = DSMC_ROLE_WALL; p->zone_inject[3] = 0;
+    p->capacity = 0;
+    p->seed = 0;
+    p->max_crossings = 4096;
+    p->keep_step_moments = 0;
+}
+
+int dsmc_create(const DsmcMeshDesc* mesh, const DsmcMeshMessage* mess, const DsmcCaseParams* params, int device,
+                DsmcHandle** out)
+{
+    if (!out) return DSMC_E_INVALID;
+    *out = nullptr;
+    DsmcHandle* h = new (std::nothrow) DsmcHandle();
+    if (!h) return DSMC_E_NOMEM;
+    if (!h->e.build(mesh, mess, params, device)) {
+        g_createError = h->e.err;
+        const int st = status_of(h->e, false);
+        delete h;
+        return st;
+    }
+    *out = h;
+    return DSMC_OK;
+}
+
+void dsmc_destroy(DsmcHandle* h) { delete h; }
+
+const char* dsmc_last_error(const DsmcHandle* h) { return h ? h->e.err.c_str() : g_createError.c_str(); }
+
+int dsmc_upload_particles(DsmcHandle* h, int64_t n, const double* px, const double* py, const double* pz,
+                          const double* vx, const double* vy, const double* vz, const double* ir, const int32_t* cell)
+{
+    DSMC_GUARD(h);
+    return status_of(h->e, h->e.uploadParticles(n, px, py, pz, vx, vy, vz, ir, cell));
+}
+
+int dsmc_particle_count(DsmcHandle* h, int64_t* n)
+{
+    DSMC_GUARD(h);
+    if (!n) return DSMC_E_INVALID;
+    int nl = 0;
+    if (!h->e.haveParticles) { *n = 0; return DSMC_OK; }
+    const bool ok = h->e.nLiveHost(nl);
+    *n = nl;
+    return status_of(h->e, ok);
+}
+
+int dsmc_download_particles(DsmcHandle* h, int64_t n, double* px, double* py, double* pz, double* vx, double* vy,
+                            double* vz, double* ir, int32_t* cell, uint32_t* pid)
+{
+    DSMC_GUARD(h);
+    if (!h->e.haveParticles) return n == 0 ? DSMC_OK : DSMC_E_STATE;
+    return status_of(h->e, h->e.downloadParticles(n, px, py, pz, vx, vy, vz, ir, cell, pid));
+}
+
+int dsmc_step(DsmcHandle* h, int32_t istep, uint32_t stages)
+{
+    DSMC_GUARD(h);
+    return status_of(h->e, h->e.step(istep, stages));
+}
+
+int dsmc_preprocesseffquad(DsmcHandle* h, int32_t istep) { return dsmc_step(h, istep, DSMC_STAGE_INJECT); }
+int dsmc_advection(DsmcHandle* h, int32_t istep) { return dsmc_step(h, istep, DSMC_STAGE_MOVE); }
+int dsmc_cache2chain(DsmcHandle* h)
+{
+    DSMC_GUARD(h);
+    return status_of(h->e, h->e.step(h->e.curIstep, DSMC_STAGE_SORT));
+}
+int dsmc_collisionDSMC(DsmcHandle* h)
+{
+    DSMC_GUARD(h);
+    // the collision stream is keyed by the step of the preceding stage calls
+    return status_of(h->e, h->e.step(h->e.curIstep, DSMC_STAGE_COLLIDE));
+}
+int dsmc_statistic_macro(DsmcHandle* h, int32_t istep) { return dsmc_step(h, istep, DSMC_STAGE_SAMPLE); }
+int dsmc_statistic_macroPre(DsmcHandle* h)
+{
+    DSMC_GUARD(h);
+    return status_of(h->e, h->e.macroPre());
+}
+
+int dsmc_download_macro(DsmcHandle* h, int32_t which, double* out)
+{
+    DSMC_GUARD(h);
+    return status_of(h->e, h->e.downloadMacro(which, out));
+}
+
+int dsmc_download_counts(DsmcHandle* h, int32_t* ppc, double* window_samples, char* window_valid,
+                         unsigned char* sparse_state, double* stepinter_rho, double* steady_rho)
+{
+    DSMC_GUARD(h);
+    dsmc::Engine& e = h->e;
+    const size_t nc = (size_t)e.ncell;
+    bool ok = true;
+    if (ppc) {
+        std::vector<int> st(nc + 1, 0);
+        if (e.haveParticles)
+            ok = ok && e.cuda(cudaMemcpyAsync(st.data(), e.start[e.cur], (nc + 1) * sizeof(int), cudaMemcpyDeviceToHost, e.stream), "start");
+        ok = ok && e.cuda(cudaStreamSynchronize(e.stream), "sync");
+        for (size_t c = 0; c < nc && ok; ++c) ppc[c] = st[c + 1] - st[c];
+    }
+    if (ok && window_samples) ok = e.cuda(cudaMemcpyAsync(window_samples, e.windowSamples, nc * sizeof(double), cudaMemcpyDeviceToHost, e.stream), "ws");
+    if (ok && window_valid) ok = e.cuda(cudaMemcpyAsync(window_valid, e.windowValid, nc, cudaMemcpyDeviceToHost, e.stream), "wv");
+    if (ok && sparse_state) ok = e.cuda(cudaMemcpyAsync(sparse_state, e.sparseState, nc, cudaMemcpyDeviceToHost, e.stream), "ss");
+    if (ok && stepinter_rho)
+        ok = e.cuda(cudaMemcpy2DAsync(stepinter_rho, sizeof(double), e.acc + 36, 54 * sizeof(double), sizeof(double), nc,
+                                      cudaMemcpyDeviceToHost, e.stream), "stepinter");
+    if (ok && steady_rho)
+        ok = e.cuda(cudaMemcpy2DAsync(steady_rho, sizeof(double), e.acc + 18, 54 * sizeof(double), sizeof(double), nc,
+                                      cudaMemcpyDeviceToHost, e.stream), "steady");
+    ok = ok && e.cuda(cudaStreamSynchronize(e.stream), "sync");
+    return status_of(e, ok);
+}
+
+int dsmc_download_step_moments(DsmcHandle* h, double* out)
+{
+    DSMC_GUARD(h);
+    dsmc::Engine& e = h->e;
+    if (!e.stepMom) { e.err = "step moments not kept (params.keep_step_moments)"; return DSMC_E_STATE; }
+    bool ok = e.cuda(cudaMemcpyAsync(out, e.stepMom, (size_t)e.ncell * 18 * sizeof(double), cudaMemcpyDeviceToHost, e.stream), "moments");
+    ok = ok && e.cuda(cudaStreamSynchronize(e.stream), "sync");
+    return status_of(e, ok);
+}
+
+int dsmc_download_wall(DsmcHandle* h, double* tally)
+{
+    DSMC_GUARD(h);
+    dsmc::Engine& e = h->e;
+    if (!tally) return DSMC_E_INVALID;
+    std::vector<double> w((size_t)std::max(e.nwall, 1) * 6);
+    bool ok = e.cuda(cudaMemcpyAsync(w.data(), e.wallTally, w.size() * sizeof(double), cudaMemcpyDeviceToHost, e.stream), "wall");
+    ok = ok && e.cuda(cudaStreamSynchronize(e.stream), "sync");
+    if (!ok) return status_of(e, false);
+    std::memset(tally, 0, (size_t)e.nface * 6 * sizeof(double));
+    for (int f = 0; f < e.nface; ++f) {
+        const int s = e.faceWallHost[(size_t)f];
+        if (s >= 0 && e.faceRole[(size_t)f] == DSMC_ROLE_WALL)
+            for (int k = 0; k < 6; ++k) tally[(size_t)f * 6 + k] = w[(size_t)s * 6 + k];
+    }
+    return DSMC_OK;
+}
+
+int dsmc_download_cell_state(DsmcHandle* h, double* crmax, double* rem_coll, double* rem_inj)
+{
+    DSMC_GUARD(h);
+    dsmc::Engine& e = h->e;
+    const size_t b = (size_t)e.ncell * sizeof(double);
+    bool ok = true;
+    if (crmax) ok = ok && e.cuda(cudaMemcpyAsync(crmax, e.crmax, b, cudaMemcpyDeviceToHost, e.stream), "crmax");
+    if (rem_coll) ok = ok && e.cuda(cudaMemcpyAsync(rem_coll, e.remColl, b, cudaMemcpyDeviceToHost, e.stream), "remcoll");
+    if (rem_inj) ok = ok && e.cuda(cudaMemcpyAsync(rem_inj, e.remInj, b, cudaMemcpyDeviceToHost, e.stream), "reminj");
+    ok = ok && e.cuda(cudaStreamSynchronize(e.stream), "sync");
+    return status_of(e, ok);
+}
+
+int dsmc_upload_cell_state(DsmcHandle* h, const double* crmax, const double* rem_coll, const double* rem_inj)
+{
+    DSMC_GUARD(h);
+    dsmc::Engine& e = h->e;
+    const size_t b = (size_t)e.ncell * sizeof(double);
+    bool ok = true;
+    if (crmax) ok = ok && e.cuda(cudaMemcpyAsync(e.crmax, crmax, b, cudaMemcpyHostToDevice, e.stream), "crmax");
+    if (rem_coll) ok = ok && e.cuda(cudaMemcpyAsync(e.remColl, rem_coll, b, cudaMemcpyHostToDevice, e.stream), "remcoll");
+    if (rem_inj) ok = ok && e.cuda(cudaMemcpyAsync(e.remInj, rem_inj, b, cudaMemcpyHostToDevice, e.stream), "reminj");
+    ok = ok && e.cuda(cudaStreamSynchronize(e.stream), "sync");
+    return status_of(e, ok);
+}
+
+int dsmc_get_counters(DsmcHandle* h, DsmcCounters* out)
+{
+    DSMC_GUARD(h);
+    if (!out) return DSMC_E_INVALID;
+    dsmc::Engine& e = h->e;
+    unsigned long long c[dsmc::C_COUNT];
+    bool ok = e.cuda(cudaMemcpyAsync(c, e.counters, sizeof c, cudaMemcpyDeviceToHost, e.stream), "counters");
+    ok = ok && e.cuda(cudaStreamSynchronize(e.stream), "sync");
+    if (!ok) return status_of(e, false);
+    out->steps = e.steps;
+    out->injected = c[dsmc::C_INJECTED];
+    out->removed = c[dsmc::C_REMOVED];
+    out->dropped = c[dsmc::C_DROPPED];
+    out->lost = c[dsmc::C_LOST];
+    out->wall_hits = c[dsmc::C_WALL_HITS];
+    out->crossings = c[dsmc::C_CROSSINGS];
+    out->candidate_pairs = c[dsmc::C_PAIRS];
+    out->collisions = c[dsmc::C_COLLISIONS];
+    out->fp64_fallbacks = c[dsmc::C_FALLBACKS];
+    out->overflow = c[dsmc::C_OVERFLOW];
+    out->big_cells = c[dsmc::C_BIG_CELLS];
+    return DSMC_OK;
+}
+
+int dsmc_trace(DsmcHandle* h, int64_t n, const double* px, const double* py, const double* pz, const double* vx,
+               const double* vy, const double* vz, const double* dt, const int32_t* cell, int32_t stop_at_wall,
+               int32_t* out_cell, int32_t* out_ifout, int32_t* out_face, int32_t* out_tri, int32_t* out_ncross,
+               double* out_px, double* out_py, double* out_pz, double* out_vx, double* out_vy, double* out_vz,
+               double* out_dt)
+{
+    DSMC_GUARD(h);
+    dsmc::Engine& e = h->e;
+    if (n < 0 || n > 0x7fffffff) return DSMC_E_INVALID;
+    if (n == 0) return DSMC_OK;
+    if (!px || !py || !pz || !vx || !vy || !vz || !dt || !cell) return DSMC_E_INVALID;
+    for (int64_t i = 0; i < n; ++i)
+        if (cell[i] < 0 || cell[i] >= e.ncell) { e.err = "trace: cell id out of range"; return DSMC_E_INVALID; }
+    const bool mixed = e.precision == DSMC_PRECISION_MIXED;
+    const size_t rs = mixed ? 4 : 8;
+    std::vector<void*> tmp;
+    auto dal = [&](size_t bytes) -> void* {
+        void* p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(bytes, 1)) != cudaSuccess) return nullptr;
+        tmp.push_back(p);
+        return p;
+    };
+    auto cleanup = [&]() { for (void* p : tmp) cudaFree(p); };
+    void* dIn[6];
+    void* dOut[6];
+    for (int k = 0; k < 6; ++k) {
+        dIn[k] = dal((size_t)n * rs);
+        dOut[k] = dal((size_t)n * rs);
+    }
+    double* dDt = (double*)dal((size_t)n * 8);
+    double* dODt = (double*)dal((size_t)n * 8);
+    int* dCell = (int*)dal((size_t)n * 4);
+    int* dI[6];
+    for (int k = 0; k < 6; ++k) dI[k] = (int*)dal((size_t)n * 4);
+    for (void* p : tmp)
+        if (!p) { cleanup(); e.err = "trace: device allocation failed"; return DSMC_E_NOMEM; }
+    const double* src[6] = {px, py, pz, vx, vy, vz};
+    std::vector<char> hb((size_t)n * 8);
+    bool ok = true;
+    for (int k = 0; k < 6 && ok; ++k) {
+        for (int64_t i = 0; i < n; ++i) {
+            double v = src[k][i];
+            if (mixed) {
+                if (k < 3) v -= e.cellCenterHost[(size_t)cell[i] * 3 + k];
+                reinterpret_cast<float*>(hb.data())[i] = (float)v;
+            } else {
+                reinterpret_cast<double*>(hb.data())[i] = v;
+            }
+        }
+        ok = e.cuda(cudaMemcpy(dIn[k], hb.data(), (size_t)n * rs, cudaMemcpyHostToDevice), "trace upload");
+    }
+    ok = ok && e.cuda(cudaMemcpy(dDt, dt, (size_t)n * 8, cudaMemcpyHostToDevice), "trace dt");
+    ok = ok && e.cuda(cudaMemcpy(dCell, cell, (size_t)n * 4, cudaMemcpyHostToDevice), "trace cells");
+    if (ok) {
+        if (mixed)
+            dsmc::launch_trace_check<float>(e.M, e.C, (int)n, (float*)dIn[0], (float*)dIn[1], (float*)dIn[2],
+                                            (float*)dIn[3], (float*)dIn[4], (float*)dIn[5], dDt, dCell, stop_at_wall,
+                                            dI[0], dI[1], dI[2], dI[3], dI[4], dI[5], (float*)dOut[0], (float*)dOut[1],
+                                            (float*)dOut[2], (float*)dOut[3], (float*)dOut[4], (float*)dOut[5], dODt,
+                                            e.counters, e.stream);
+        else
+            dsmc::launch_trace_check<double>(e.M, e.C, (int)n, (double*)dIn[0], (double*)dIn[1], (double*)dIn[2],
+                                             (double*)dIn[3], (double*)dIn[4], (double*)dIn[5], dDt, dCell,
+                                             stop_at_wall, dI[0], dI[1], dI[2], dI[3], dI[4], dI[5], (double*)dOut[0],
+                                             (double*)dOut[1], (double*)dOut[2], (double*)dOut[3], (double*)dOut[4],
+                                             (double*)dOut[5], dODt, e.counters, e.stream);
+        ok = e.cuda(cudaGetLastError(), "trace launch") && e.cuda(cudaStreamSynchronize(e.stream), "trace sync");
+    }
+    std::vector<int> last((size_t)n);
+    int32_t* iout[5] = {out_cell, out_ifout, out_face, out_tri, out_ncross};
+    for (int k = 0; k < 5 && ok; ++k)
+        if (iout[k]) ok = e.cuda(cudaMemcpy(iout[k], dI[k], (size_t)n * 4, cudaMemcpyDeviceToHost), "trace out");
+    ok = ok && e.cuda(cudaMemcpy(last.data(), dI[5], (size_t)n * 4, cudaMemcpyDeviceToHost), "trace last");
+    double* fout[6] = {out_px, out_py, out_pz, out_vx, out_vy, out_vz};
+    for (int k = 0; k < 6 && ok; ++k) {
+        if (!fout[k]) continue;
+        ok = e.cuda(cudaMemcpy(hb.data(), dOut[k], (size_t)n * rs, cudaMemcpyDeviceToHost), "trace out");
+        for (int64_t i = 0; i < n && ok; ++i) {
+            double v = mixed ? (double)reinterpret_cast<float*>(hb.data())[i] : reinterpret_cast<double*>(hb.data())[i];
+            if (mixed && k < 3) v = e.cellCenterHost[(size_t)last[(size_t)i] * 3 + k] + v;
+            fout[k][i] = v;
+        }
+    }
+    if (ok && out_dt) ok = e.cuda(cudaMemcpy(out_dt, dODt, (size_t)n * 8, cudaMemcpyDeviceToHost), "trace dt out");
+    cleanup();
+    return status_of(e, ok);
+}
+
+int dsmc_set_timing(DsmcHandle* h, int32_t on)
+{
+    DSMC_GUARD(h);
+    h->e.timing = on != 0;
+    return DSMC_OK;
+}
+
+int dsmc_stage_ms(DsmcHandle* h, double* ms4, int64_t* nsteps, int32_t reset)
+{
+    DSMC_GUARD(h);
+    if (ms4)
+        for (int k = 0; k < 4; ++k) ms4[k] = h->e.stageMs[k];
+    if (nsteps) *nsteps = h->e.timedSteps;
+    if (reset) {
+        for (double& v : h->e.stageMs) v = 0.0;
+        h->e.timedSteps = 0;
+    }
+    return DSMC_OK;
+}
+
+void* dsmc_stream(DsmcHandle* h) { return h ? (void*)h->e.stream : nullptr; }
+
+int dsmc_sync(DsmcHandle* h)
+{
+    DSMC_GUARD(h);
+    dsmc::Engine& e = h->e;
+    bool ok = e.cuda(cudaStreamSynchronize(e.stream), "sync") && e.checkDeviceErrors();
+    return status_of(e, ok);
+}
+
+}  // extern "C"

@@ -1,0 +1,1067 @@
+// The DSMC step kernels.
+//
+//   inject   preprocesseffquad (src/ProcessDSMC.cpp:2556-2570): per-cell
+//            inflow counts with the reference's remainder carry, scan,
+//            per-patch particle generation + trace for r*dt.
+//   move     advection (src/ProcessDSMC.cpp:1946-2017): one thread per
+//            particle traces dtime through the mesh.
+//   sort     cache2chain (src/ProcessDSMC.cpp:2030-2135): deterministic
+//            counting sort. rank (warp per source cell: arrival slot and rank
+//            from warp ballots; multi-hop and injected arrivals through
+//            warp-aggregated atomics), scan, scatter of source indices.
+//   cells    warp per destination cell: gather into the sorted buffer,
+//            canonical order, NTC collisions (collisionDSMC,
+//            src/ProcessDSMC.cpp:2621-2744) with pairs run in parallel
+//            waves that keep the sequential result, and the 18-moment
+//            sampling (statistic_macro, src/ProcessDSMC.cpp:2757-2861).
+#include "dsmc_kernels.cuh"
+#include "dsmc_macro.cuh"
+
+namespace dsmc {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+template <typename Real> struct CellCap;
+template <> struct CellCap<float> { static constexpr int value = 512; };
+template <> struct CellCap<double> { static constexpr int value = 288; };
+
+// ===========================================================================
+// inject
+// ===========================================================================
+__global__ void inject_count_kernel(DevPatches P, double* remInj)
+{
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < P.ngroup; g += gridDim.x * blockDim.x) {
+        const int b = P.groupStart[g];
+        const int e = P.groupStart[g + 1];
+        const int cell = P.cell[b];
+        double rem = remInj[cell];
+        // computeBoundaryInsertCount, src/ProcessDSMC.cpp:2398-2402
+        for (int p = b; p < e; ++p) {
+            const double addNum = da(P.addBase[p], rem);
+            const double fl = floor(addNum);
+            const int n = (int)fl;
+            rem = ds(addNum, (double)n);
+            P.count[p] = n;
+        }
+        remInj[cell] = rem;
+    }
+}
+
+__global__ void __launch_bounds__(1024) inject_scan_kernel(DevPatches P, StepCtl* ctl, unsigned long long* counters)
+{
+    __shared__ int warpSum[32];
+    __shared__ int carry;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, wid = tid >> 5;
+    const int room = ctl->capacity - ctl->nLive;
+    if (tid == 0) carry = 0;
+    long long over = 0;
+    __syncthreads();
+    for (int base = 0; base < P.npatch; base += blockDim.x) {
+        const int i = base + tid;
+        const int v = (i < P.npatch) ? P.count[i] : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warpSum[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int w = (lane < (int)(blockDim.x >> 5)) ? warpSum[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(kFull, w, o);
+                if (lane >= o) w += y;
+            }
+            warpSum[lane] = w;
+        }
+        __syncthreads();
+        const int incl = x + (wid > 0 ? warpSum[wid - 1] : 0);
+        const int start = carry + incl - v;
+        if (i < P.npatch) {
+            P.start[i] = start;
+            int allowed = room - start;
+            allowed = allowed < 0 ? 0 : (allowed > v ? v : allowed);
+            if (allowed < v) {
+                over += v - allowed;
+                P.count[i] = allowed;
+            }
+        }
+        __syncthreads();
+        if (tid == blockDim.x - 1) carry += incl;
+        __syncthreads();
+    }
+    if (over) atomicAdd(counters + C_OVERFLOW, (unsigned long long)over);
+    __syncthreads();
+    if (tid == 0) {
+        const int m = carry < room ? carry : (room > 0 ? room : 0);
+        ctl->nInj = m;
+        atomicAdd(counters + C_INJECTED, (unsigned long long)m);
+    }
+}
+
+// sampleBoundaryParticle, src/ProcessDSMC.cpp:2416-2458: normal speed by
+// acceptance-rejection against the fs1/fs2 envelope, tangential components by
+// Box-Muller, rotational energy -ln(r) T / 2, all in the patch frame.
+__device__ __forceinline__ void sample_inflow_velocity(const double* gas, const double* R, Stream& rs,
+                                                       double v[3], double& ir, int* errorWord)
+{
+    const double snp = gas[0], fs1 = gas[1], fs2 = gas[2], stp1 = gas[3], stp2 = gas[4];
+    const double tN = gas[5], sq = gas[6], QA = gas[7];
+    double vzr = 0.0, vza = 0.0;
+    for (int outer = 0;; ++outer) {
+        for (int inner = 0;; ++inner) {
+            const double r = rs.uniform64();
+            vzr = (-QA + 2.0 * QA * r) * sq;
+            vza = vzr / sq + snp;
+            if (vza > 0) break;
+            if (inner > (1 << 20)) { atomicOr(errorWord, kErrRejectLoop); vza = 1e-3; break; }
+        }
+        const double vzn = vzr / sq;
+        const double pp = (2.0 * vza / fs1) * exp(fs2 - vzn * vzn);
+        if (rs.uniform64() < pp) break;
+        if (outer > (1 << 20)) { atomicOr(errorWord, kErrRejectLoop); break; }
+    }
+    const double r = rs.uniform64();
+    const double th = rs.uniform64();
+    double s, c;
+    sincospi(2.0 * th, &s, &c);
+    const double a = sqrt(-log(r));
+    const double vxa = (a * s + stp1) * sq;
+    const double vya = (a * c + stp2) * sq;
+    vza *= sq;
+    v[0] = R[0] * vxa + R[1] * vya + R[2] * vza;
+    v[1] = R[3] * vxa + R[4] * vya + R[5] * vza;
+    v[2] = R[6] * vxa + R[7] * vya + R[8] * vza;
+    ir = -log(rs.uniform64()) * tN * 0.5;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(128) inject_gen_kernel(StepArgs<Real> a)
+{
+    const int istep = a.ctl->istep;
+    const int nLive = a.ctl->nLive;
+    TraceCounts cnt{};
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.P.npatch; p += gridDim.x * blockDim.x) {
+        const int np = a.P.count[p];
+        if (np <= 0) continue;
+        const int first = a.P.start[p];
+        const int pcell = a.P.cell[p];
+        const int pedge = a.P.edge[p];
+        const int ptag = a.P.triTag[p];
+        const double* G = a.P.geom + (size_t)p * 9;
+        const double* R = a.P.rot + (size_t)p * 9;
+        const double* gas = a.P.gas + (size_t)p * 8;
+        for (int k = 0; k < np; ++k) {
+            const int gi = nLive + first + k;
+            Stream rs;
+            rs.init((uint32_t)gi, (uint32_t)istep, kPurposeInject, a.C.seedLo, a.C.seedHi);
+            double u = rs.uniform64(), w = rs.uniform64();
+            if (u + w > 1.0) { u = 1.0 - u; w = 1.0 - w; }
+            double pos[3];
+            // p0 + u e10 + v e20 (src/ProcessDSMC.cpp:2524-2526), unfused
+            for (int d = 0; d < 3; ++d) pos[d] = da(da(G[d], dm(u, G[3 + d])), dm(w, G[6 + d]));
+            double vel[3], irv;
+            sample_inflow_velocity(gas, R, rs, vel, irv, a.errorWord);
+            const double dtl = rs.uniform64() * a.C.dtime;
+            PRegs<Real> pr;
+            int cell = pcell;
+            if constexpr (sizeof(Real) == 8) {
+                for (int d = 0; d < 3; ++d) pr.x[d] = pos[d];
+            } else {
+                const double* cc = a.M.cellCenter + (size_t)cell * 3;
+                for (int d = 0; d < 3; ++d) pr.x[d] = (float)(pos[d] - cc[d]);
+            }
+            for (int d = 0; d < 3; ++d) pr.v[d] = (Real)vel[d];
+            pr.ir = (Real)irv;
+            Real dtleft = (Real)dtl;
+            const int out = trace_particle<Real>(a.M, a.C, pr, cell, pedge, ptag, dtleft, rs, istep,
+                                                 a.wallTally, cnt, false, nullptr);
+            a.A.x[0][gi] = pr.x[0]; a.A.x[1][gi] = pr.x[1]; a.A.x[2][gi] = pr.x[2];
+            a.A.v[0][gi] = pr.v[0]; a.A.v[1][gi] = pr.v[1]; a.A.v[2][gi] = pr.v[2];
+            a.A.ir[gi] = pr.ir;
+            a.A.cell[gi] = (out >= 0) ? cell : -1;
+        }
+    }
+    flush_counts(a.counters, cnt);
+}
+
+template <typename Real>
+void launch_inject(const StepArgs<Real>& a, int smCount, cudaStream_t s)
+{
+    if (a.P.npatch == 0) {
+        cudaMemsetAsync(&a.ctl->nInj, 0, sizeof(int), s);
+        return;
+    }
+    const int gCount = (a.P.ngroup + 127) / 128;
+    inject_count_kernel<<<gCount > 0 ? gCount : 1, 128, 0, s>>>(a.P, a.remInj);
+    inject_scan_kernel<<<1, 1024, 0, s>>>(a.P, a.ctl, a.counters);
+    int g = (a.P.npatch + 127) / 128;
+    if (g > smCount * 8) g = smCount * 8;
+    inject_gen_kernel<Real><<<g, 128, 0, s>>>(a);
+}
+
+// ===========================================================================
+// move
+// ===========================================================================
+template <typename Real>
+__global__ void __launch_bounds__(256) move_kernel(StepArgs<Real> a)
+{
+    const int istep = a.ctl->istep;
+    const int n = a.ctl->nLive;
+    TraceCounts cnt{};
+    const Real dt0 = (Real)a.C.dtime;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        PRegs<Real> p;
+        p.x[0] = a.A.x[0][i]; p.x[1] = a.A.x[1][i]; p.x[2] = a.A.x[2][i];
+        p.v[0] = a.A.v[0][i]; p.v[1] = a.A.v[1][i]; p.v[2] = a.A.v[2][i];
+        p.ir = a.A.ir[i];
+        int cell = a.A.cell[i];
+        Stream rs;
+        rs.init((uint32_t)i, (uint32_t)istep, kPurposeWall, a.C.seedLo, a.C.seedHi);
+        Real dtleft = dt0;
+        const uint32_t wallBefore = cnt.wall;
+        const int out = trace_particle<Real>(a.M, a.C, p, cell, -1, -1, dtleft, rs, istep, a.wallTally,
+                                             cnt, false, nullptr);
+        if (out >= 0) {
+            a.A.x[0][i] = p.x[0]; a.A.x[1][i] = p.x[1]; a.A.x[2][i] = p.x[2];
+            if (cnt.wall != wallBefore) {
+                a.A.v[0][i] = p.v[0]; a.A.v[1][i] = p.v[1]; a.A.v[2][i] = p.v[2];
+                a.A.ir[i] = p.ir;
+            }
+            a.A.cell[i] = cell;
+        } else {
+            a.A.cell[i] = -1;
+        }
+    }
+    flush_counts(a.counters, cnt);
+}
+
+template <typename Real>
+void launch_move(const StepArgs<Real>& a, int smCount, cudaStream_t s)
+{
+    move_kernel<Real><<<smCount * 8, 256, 0, s>>>(a);
+}
+
+// ===========================================================================
+// sort: rank, scan, scatter
+// ===========================================================================
+template <typename Real>
+__global__ void __launch_bounds__(256) rank_kernel(StepArgs<Real> a)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int ncell = a.M.ncell;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int s = warp; s < ncell; s += nwarps) {
+        const int b = a.startA[s];
+        const int e = a.startA[s + 1];
+        const int nbL = (lane < 6) ? a.M.cell2cell[(size_t)s * 6 + lane] : -1;
+        const int rvL = (lane < 6) ? (int)a.M.revSlot[(size_t)s * 6 + lane] : -1;
+        int nbr[6], slotQ[7], runQ[7];
+        slotQ[0] = 0;
+        runQ[0] = 0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            nbr[j] = __shfl_sync(kFull, nbL, j);
+            slotQ[j + 1] = __shfl_sync(kFull, rvL, j) + 1;
+            runQ[j + 1] = 0;
+        }
+        for (int base = b; base < e; base += 32) {
+            const int i = base + lane;
+            const bool valid = i < e;
+            const int d = valid ? a.A.cell[i] : -1;
+            int q = -1;
+            if (d >= 0) {
+                if (d == s) q = 0;
+                else {
+#pragma unroll
+                    for (int j = 5; j >= 0; --j)
+                        if (d == nbr[j]) q = j + 1;
+                }
+            }
+            int packed = -1;
+#pragma unroll
+            for (int qq = 0; qq < 7; ++qq) {
+                const unsigned m = __ballot_sync(kFull, q == qq);
+                if (q == qq) packed = (slotQ[qq] << 24) | (runQ[qq] + __popc(m & lt));
+                runQ[qq] += __popc(m);
+            }
+            const int key = (d >= 0 && q < 0) ? d * kSlots + kFarSlot : -1;
+            const int r = warp_claim(a.countSlot, key);
+            if (key >= 0) packed = (kFarSlot << 24) | r;
+            if (valid) a.rank[i] = packed;
+        }
+        int myRun = 0;
+#pragma unroll
+        for (int qq = 0; qq < 7; ++qq)
+            if (lane == qq) myRun = runQ[qq];
+        const int nbPrev = __shfl_up_sync(kFull, nbL, 1);
+        const int rvPrev = __shfl_up_sync(kFull, rvL, 1);
+        if (lane == 0) {
+            a.countSlot[(size_t)s * kSlots] = myRun;
+        } else if (lane <= 6) {
+            if (nbPrev >= 0 && nbPrev < ncell && rvPrev >= 0) a.countSlot[(size_t)nbPrev * kSlots + rvPrev + 1] = myRun;
+        }
+    }
+    // injected particles: all arrive through the far slot
+    const int nLive = a.ctl->nLive;
+    const int nTot = nLive + a.ctl->nInj;
+    for (int base = nLive + warp * 32; base < nTot; base += nwarps * 32) {
+        const int i = base + lane;
+        const int d = (i < nTot) ? a.A.cell[i] : -1;
+        const int key = d >= 0 ? d * kSlots + kFarSlot : -1;
+        const int r = warp_claim(a.countSlot, key);
+        if (i < nTot && d >= 0) a.rank[i] = (kFarSlot << 24) | r;
+    }
+}
+
+__device__ __forceinline__ int row_total(const int* countSlot, int c)
+{
+    const int4 lo = *reinterpret_cast<const int4*>(countSlot + (size_t)c * kSlots);
+    const int4 hi = *reinterpret_cast<const int4*>(countSlot + (size_t)c * kSlots + 4);
+    return lo.x + lo.y + lo.z + lo.w + hi.x + hi.y + hi.z + hi.w;
+}
+
+__device__ __forceinline__ int block_sum(int v, int* sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    int t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    __syncthreads();
+    if (threadIdx.x == 0) sh[0] = t;
+    __syncthreads();
+    const int r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(256) scan_partial_kernel(const int* countSlot, int ncell, int* partial)
+{
+    __shared__ int sh[32];
+    const int chunk = (ncell + gridDim.x - 1) / gridDim.x;
+    const int b = blockIdx.x * chunk;
+    const int e = min(ncell, b + chunk);
+    int s = 0;
+    for (int c = b + threadIdx.x; c < e; c += blockDim.x) s += row_total(countSlot, c);
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(256) scan_final_kernel(const int* countSlot, int ncell, const int* partial,
+                                                         int* start, StepCtl* ctl)
+{
+    __shared__ int sh[32];
+    __shared__ int warpSum[8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int pre = 0;
+    for (int k = threadIdx.x; k < (int)blockIdx.x; k += blockDim.x) pre += partial[k];
+    int carry = block_sum(pre, sh);
+    const int chunk = (ncell + gridDim.x - 1) / gridDim.x;
+    const int b = blockIdx.x * chunk;
+    const int e = min(ncell, b + chunk);
+    for (int base = b; base < e; base += blockDim.x) {
+        const int c = base + threadIdx.x;
+        const int v = (c < e) ? row_total(countSlot, c) : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warpSum[wid] = x;
+        __syncthreads();
+        int off = 0;
+        for (int w = 0; w < wid; ++w) off += warpSum[w];
+        int tileTotal = 0;
+        for (int w = 0; w < 8; ++w) tileTotal += warpSum[w];
+        if (c < e) start[c] = carry + off + x - v;
+        __syncthreads();
+        carry += tileTotal;
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+        start[ncell] = carry;
+        ctl->nNext = carry;
+    }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(256) scatter_kernel(StepArgs<Real> a)
+{
+    const int nTot = a.ctl->nLive + a.ctl->nInj;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nTot; i += gridDim.x * blockDim.x) {
+        const int d = a.A.cell[i];
+        if (d < 0) continue;
+        const int packed = a.rank[i];
+        const int slot = packed >> 24;
+        const int r = packed & 0xFFFFFF;
+        const int4 lo = *reinterpret_cast<const int4*>(a.countSlot + (size_t)d * kSlots);
+        const int4 hi = *reinterpret_cast<const int4*>(a.countSlot + (size_t)d * kSlots + 4);
+        int base = a.startB[d] + r;
+        if (slot > 0) base += lo.x;
+        if (slot > 1) base += lo.y;
+        if (slot > 2) base += lo.z;
+        if (slot > 3) base += lo.w;
+        if (slot > 4) base += hi.x;
+        if (slot > 5) base += hi.y;
+        if (slot > 6) base += hi.z;
+        if (base < a.startB[d] || base >= a.startB[d + 1]) {   // self-check: slot counts inconsistent
+            atomicOr(a.errorWord, kErrSortIndex);
+            continue;
+        }
+        a.idx[base] = i;
+    }
+}
+
+template <typename Real>
+void launch_sort(const StepArgs<Real>& a, int smCount, cudaStream_t s)
+{
+    rank_kernel<Real><<<smCount * 8, 256, 0, s>>>(a);
+    scan_partial_kernel<<<kScanBlocks, 256, 0, s>>>(a.countSlot, a.M.ncell, a.scanPartial);
+    scan_final_kernel<<<kScanBlocks, 256, 0, s>>>(a.countSlot, a.M.ncell, a.scanPartial, a.startB, a.ctl);
+    scatter_kernel<Real><<<smCount * 8, 256, 0, s>>>(a);
+}
+
+// ===========================================================================
+// cells: gather + collide + sample
+// ===========================================================================
+
+// Ascending bitonic sort of 32*K keys held K per lane (element e of lane l is
+// position e*32 + l). Unused slots hold 0xffffffff.
+template <int K>
+__device__ __forceinline__ void warp_bitonic(uint32_t (&a)[K])
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32 * K; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+                const int je = j >> 5;
+#pragma unroll
+                for (int e = 0; e < K; ++e) {
+                    const int e2 = e ^ je;
+                    if (e2 > e) {
+                        const bool asc = (((e << 5) | lane) & k) == 0;
+                        const uint32_t lo = min(a[e], a[e2]), hi = max(a[e], a[e2]);
+                        a[e] = asc ? lo : hi;
+                        a[e2] = asc ? hi : lo;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < K; ++e) {
+                    const uint32_t o = __shfl_xor_sync(kFull, a[e], j);
+                    const bool asc = (((e << 5) | lane) & k) == 0;
+                    const bool lower = (lane & j) == 0;
+                    a[e] = (lower == asc) ? min(a[e], o) : max(a[e], o);
+                }
+            }
+        }
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void sort_far_warp(int* seg, int m)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t v[K];
+#pragma unroll
+    for (int e = 0; e < K; ++e) {
+        const int p = e * 32 + lane;
+        v[e] = (p < m) ? (uint32_t)seg[p] : 0xffffffffu;
+    }
+    warp_bitonic<K>(v);
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < K; ++e) {
+        const int p = e * 32 + lane;
+        if (p < m) seg[p] = (int)v[e];
+    }
+    __syncwarp();
+}
+
+// collision_diameter, src/ProcessDSMC.cpp:2603-2608
+__device__ __forceinline__ double collision_diameter(double cr, double prefactor, double eta)
+{
+    const double cr2 = cr * cr;
+    return cr * prefactor * pow(1.0 / cr2, eta);
+}
+
+// collisionVelocity, src/ProcessDSMC.cpp:2679-2744, on one candidate pair.
+template <typename Real>
+__device__ __forceinline__ void collide_pair(Real* vx, Real* vy, Real* vz, Real* ir, int k1, int k2, Stream& rs,
+                                             const DevConsts& C, double consCrm, Real crm0, Real& crmLocal,
+                                             uint32_t& colls)
+{
+    const Real v1x = vx[k1], v1y = vy[k1], v1z = vz[k1];
+    const Real v2x = vx[k2], v2y = vy[k2], v2z = vz[k2];
+    const Real vr0 = v1x - v2x, vr1 = v1y - v2y, vr2 = v1z - v2z;
+    const Real cr2 = vr0 * vr0 + vr1 * vr1 + vr2 * vr2;
+    const Real cr = sqrt(cr2);
+    Real preErt = (Real)0.25 * cr2;
+    if (cr > crmLocal) crmLocal = cr;
+    Real accept;
+    if constexpr (sizeof(Real) == 8) {
+        accept = collision_diameter(cr * C.vrms, C.cdPrefactor, C.eta) / consCrm;
+    } else {
+        // ratio of the VHS sigma*c at cr and at crmax: (cr/crmax)^(1-2 eta)
+        accept = exp2f((float)(1.0 - 2.0 * C.eta) * __log2f(cr / crm0));
+    }
+    if (rs.uniform<Real>() >= accept) return;
+    const Real expLB = (Real)(1.0 / (2.5 - C.omega));
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        Real* irp = (h == 0) ? &ir[k1] : &ir[k2];
+        if (rs.uniform<Real>() <= (Real)C.prelax) {
+            const Real preEr = *irp;
+            const Real r = rs.uniform<Real>();
+            Real pw;
+            if constexpr (sizeof(Real) == 8) pw = pow(r, expLB); else pw = exp2f(expLB * __log2f(r));
+            const Real postEr = (preErt + preEr) * ((Real)1 - pw);
+            *irp = postEr;
+            preErt = preErt + preEr - postEr;
+        }
+    }
+    const Real postVr = sqrt((Real)2 * preErt / (Real)0.5);
+    const Real vc0 = (Real)0.5 * (v1x + v2x);
+    const Real vc1 = (Real)0.5 * (v1y + v2y);
+    const Real vc2 = (Real)0.5 * (v1z + v2z);
+    const Real r = rs.uniform<Real>();
+    Real cosChi;
+    if constexpr (sizeof(Real) == 8) cosChi = 2.0 * pow(r, 1.0 / C.alpha) - 1.0;
+    else cosChi = (C.alpha == 1.0) ? 2.0f * r - 1.0f : 2.0f * exp2f((float)(1.0 / C.alpha) * __log2f(r)) - 1.0f;
+    const Real sinChi = sqrt((Real)1 - cosChi * cosChi);
+    const Real th = rs.uniform<Real>();
+    Real sth, cth;
+    if constexpr (sizeof(Real) == 8) sincospi(2.0 * th, &sth, &cth); else sincospif(2.0f * th, &sth, &cth);
+    const Real vrp = sqrt(vr1 * vr1 + vr2 * vr2);
+    const Real tiny = (sizeof(Real) == 8) ? (Real)1.0e-300 : (Real)1.0e-30f;
+    const Real scale = postVr / (cr > tiny ? cr : tiny);
+    const Real vrpc = vrp > tiny ? vrp : tiny;
+    Real ref1 = scale * (cosChi * vr0 + sinChi * sth * vrp);
+    Real ref2 = scale * (cosChi * vr1 + sinChi * (cr * vr2 * cth - vr0 * vr1 * sth) / vrpc);
+    Real ref3 = scale * (cosChi * vr2 - sinChi * (cr * vr1 * cth + vr0 * vr2 * sth) / vrpc);
+    if (vrp < (Real)1e-6) {
+        ref1 = scale * cosChi * vr0;
+        ref2 = scale * sinChi * vr0 * cth;
+        ref3 = scale * sinChi * vr0 * sth;
+    }
+    vx[k1] = vc0 + (Real)0.5 * ref1; vy[k1] = vc1 + (Real)0.5 * ref2; vz[k1] = vc2 + (Real)0.5 * ref3;
+    vx[k2] = vc0 - (Real)0.5 * ref1; vy[k2] = vc1 - (Real)0.5 * ref2; vz[k2] = vc2 - (Real)0.5 * ref3;
+    ++colls;
+}
+
+// NTC collisions of one cell by one warp (collisionDSMC,
+// src/ProcessDSMC.cpp:2631-2665). Candidate pairs are drawn from a stream
+// keyed by (cell, step, pair index). Pairs run in waves: a pair goes once it
+// is the lowest unfinished pair of the batch on both its particles, so every
+// particle sees its pairs in pair order and the result equals processing the
+// pairs one after another. claim == nullptr runs them one at a time.
+template <typename Real>
+__device__ void collide_cell(Real* vx, Real* vy, Real* vz, Real* ir, int* claim, int n, int c,
+                             const StepArgs<Real>& a, int istep, uint32_t& pairsOut, uint32_t& collOut)
+{
+    const int lane = threadIdx.x & 31;
+    if (n <= 1) return;
+    double consCrm = 0.0, crm0 = 0.0;
+    int npairs = 0;
+    if (lane == 0) {
+        crm0 = a.crmax[c];
+        const double S = a.M.cellVolume[c];
+        consCrm = collision_diameter(crm0 * a.C.vrms, a.C.cdPrefactor, a.C.eta);
+        const double pairs = 0.5 * n * (n - 1) * a.C.neff * consCrm * a.C.dtime * a.C.dtref / S + a.remColl[c];
+        npairs = (int)floor(pairs);
+        a.remColl[c] = pairs - npairs;
+        pairsOut += (uint32_t)npairs;
+    }
+    npairs = __shfl_sync(kFull, npairs, 0);
+    consCrm = __shfl_sync(kFull, consCrm, 0);
+    crm0 = __shfl_sync(kFull, crm0, 0);
+    if (!(consCrm > 0.0) || npairs <= 0) return;
+    Real crmLocal = (Real)0;
+    const Real crm0r = (Real)crm0;
+    if (claim) {
+        for (int k = lane; k < n; k += 32) claim[k] = 64;
+        __syncwarp();
+    }
+    for (int base = 0; base < npairs; base += 32) {
+        const int j = base + lane;
+        const bool active = j < npairs;
+        int k1 = 0, k2 = 0;
+        Stream rs;
+        rs.init((uint32_t)c, (uint32_t)istep, kPurposeCollide | ((uint32_t)j << 4), a.C.seedLo, a.C.seedHi);
+        if (active) {
+            k1 = (int)__umulhi(rs.next32(), (uint32_t)n);
+            k2 = k1 + 1 + (int)__umulhi(rs.next32(), (uint32_t)(n - 1));
+            if (k2 >= n) k2 -= n;
+        }
+        if (!claim) {
+            for (int l = 0; l < 32; ++l) {
+                if (lane == l && active) collide_pair<Real>(vx, vy, vz, ir, k1, k2, rs, a.C, consCrm, crm0r, crmLocal, collOut);
+                __syncwarp();
+            }
+            continue;
+        }
+        bool done = !active;
+        for (int round = 0; round < 40; ++round) {
+            if (__all_sync(kFull, done)) break;
+            if (!done) {
+                atomicMin(&claim[k1], lane);
+                atomicMin(&claim[k2], lane);
+            }
+            __syncwarp();
+            const bool go = !done && claim[k1] == lane && claim[k2] == lane;
+            __syncwarp();
+            if (go) {
+                collide_pair<Real>(vx, vy, vz, ir, k1, k2, rs, a.C, consCrm, crm0r, crmLocal, collOut);
+                claim[k1] = 64;
+                claim[k2] = 64;
+                done = true;
+            }
+            __syncwarp();
+        }
+    }
+    Real m = crmLocal;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const Real y = __shfl_xor_sync(kFull, m, o);
+        m = y > m ? y : m;
+    }
+    if (lane == 0 && (double)m > crm0) a.crmax[c] = (double)m;
+}
+
+template <typename Real>
+__device__ __forceinline__ void moment_partial(const Real* vx, const Real* vy, const Real* vz, const Real* ir,
+                                               int n, int tid, int nt, double m[18])
+{
+#pragma unroll
+    for (int k = 0; k < 18; ++k) m[k] = 0.0;
+    for (int k = tid; k < n; k += nt) {
+        const double x = (double)vx[k], y = (double)vy[k], z = (double)vz[k], I = (double)ir[k];
+        const double v2 = x * x + y * y + z * z;
+        m[0] += 1.0; m[1] += x; m[2] += y; m[3] += z; m[4] += v2;
+        m[5] += x * x; m[6] += x * y; m[7] += y * y; m[8] += y * z; m[9] += z * z; m[10] += z * x;
+        m[11] += x * v2; m[12] += y * v2; m[13] += z * v2;
+        m[14] += I; m[15] += x * I; m[16] += y * I; m[17] += z * I;
+    }
+}
+
+__device__ __forceinline__ void warp_reduce18(double m[18])
+{
+#pragma unroll
+    for (int k = 0; k < 18; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m[k] += __shfl_down_sync(kFull, m[k], o);
+    }
+}
+
+// Fold one step's moments (mom[18] in shared memory) into the per-cell
+// accumulators: statistic_macro, src/ProcessDSMC.cpp:2784-2859. Called by a
+// whole warp.
+template <typename Real>
+__device__ void sample_update(const StepArgs<Real>& a, int c, const double* mom, int istep, bool pre)
+{
+    const int lane = threadIdx.x & 31;
+    const double S = a.M.cellVolume[c];
+    if (a.stepMom && lane < 18) a.stepMom[(size_t)c * 18 + lane] = mom[lane];
+    if (pre) {
+        // statistic_macroPre, src/ProcessDSMC.cpp:3312-3326
+        if (lane == 0) {
+            double out[18];
+            local_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
+            for (int k = 0; k < 18; ++k) a.local[(size_t)c * 18 + k] = out[k];
+            record_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
+            for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
+        }
+        return;
+    }
+    double* acc = a.acc + (size_t)c * 54;
+    const bool every = (istep % a.C.nevery) == 0;
+    if (lane < 18) {
+        const double v = mom[lane];
+        // updateStepWindowMoments, :3106-3113
+        const double na = (double)a.C.nscheme;
+        const double w = (istep <= a.C.nscheme) ? 1.0 : dd(ds(na, 1.0), na);
+        double s = acc[lane];
+        s = (w == 1.0) ? da(s, v) : da(dm(w, s), v);
+        acc[lane] = s;
+        if (istep > a.C.nss) acc[18 + lane] = da(acc[18 + lane], v);
+        if (every) acc[36 + lane] = da(acc[36 + lane], v);
+    }
+    __syncwarp();
+    const int ngsis = a.C.nevery * a.C.nrepeat;
+    int clear = 0;
+    if (lane == 0) {
+        unsigned char st = a.sparseState[c];
+        int accum = a.sparseAccum[c];
+        if (every && (st == 1 || st == 2)) {
+            if (accum < 0) accum = 0;
+            ++accum;
+        }
+        if (ngsis > 0 && istep % ngsis == 0) {
+            const double* inter = acc + 36;
+            const double ws = inter[0];
+            const bool finite = isfinite(ws);
+            bool sparse = (st == 1 || st == 2);
+            if (!sparse && finite && ws < 3.0) {
+                st = 1;
+                accum = a.C.nrepeat > 1 ? a.C.nrepeat : 1;
+                sparse = true;
+            }
+            const bool valid = (ws >= 3.0) && finite;
+            a.windowSamples[c] = ws;
+            a.windowValid[c] = valid ? 1 : 0;
+            double out[18];
+            if (sparse) {
+                averaged_macro(inter, (double)(accum > 1 ? accum : 1), S, a.C.neff, a.C.nref, a.C.dr, out);
+                for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
+            } else if (valid) {
+                averaged_macro(inter, (double)a.C.nrepeat, S, a.C.neff, a.C.nref, a.C.dr, out);
+                for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
+            }
+            clear = sparse ? 0 : 1;
+        }
+        a.sparseState[c] = st;
+        a.sparseAccum[c] = accum;
+    }
+    clear = __shfl_sync(kFull, clear, 0);
+    if (clear && lane < 18) acc[36 + lane] = 0.0;
+}
+
+template <typename Real>
+struct WarpSmem {
+    Real vx[CellCap<Real>::value];
+    Real vy[CellCap<Real>::value];
+    Real vz[CellCap<Real>::value];
+    Real ir[CellCap<Real>::value];
+    int claim[CellCap<Real>::value];
+    double mom[18];
+};
+
+template <typename Real, int MODE>
+__global__ void __launch_bounds__(128) cell_kernel(StepArgs<Real> a)
+{
+    constexpr int CAP = CellCap<Real>::value;
+    __shared__ WarpSmem<Real> smem[4];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    WarpSmem<Real>& S = smem[wib];
+    const int gw = blockIdx.x * 4 + wib;
+    const int nw = gridDim.x * 4;
+    const int istep = a.ctl->istep;
+    constexpr bool gather = (MODE == kModeStep || MODE == kModeGather);
+    constexpr bool collide = (MODE == kModeStep || MODE == kModeCollide);
+    constexpr bool sample = (MODE == kModeStep || MODE == kModeSample || MODE == kModePre);
+    const PBuf<Real> dst = gather ? a.B : a.A;
+    const int* start = gather ? a.startB : a.startA;
+    uint32_t pairs = 0, colls = 0, big = 0;
+    for (int c = gw; c < a.M.ncell; c += nw) {
+        const int s0 = start[c];
+        const int n = start[c + 1] - s0;
+        if (n > CAP) {
+            if (lane == 0) {
+                const int k = atomicAdd(a.bigCount, 1);
+                a.bigList[k] = c;
+                ++big;
+            }
+            continue;
+        }
+        if constexpr (gather) {
+            const int far = a.countSlot[(size_t)c * kSlots + kFarSlot];
+            __syncwarp();
+            if (lane == 0) a.countSlot[(size_t)c * kSlots + kFarSlot] = 0;
+            if (far > 32) sort_far_warp<16>(a.idx + s0 + n - far, far);
+            else if (far > 1) sort_far_warp<1>(a.idx + s0 + n - far, far);
+            const int nSrc = a.ctl->nLive + a.ctl->nInj;
+            for (int k = lane; k < n; k += 32) {
+                int i = a.idx[s0 + k];
+                if ((unsigned)i >= (unsigned)nSrc) {   // self-check: never index outside the source
+                    atomicOr(a.errorWord, kErrSortIndex);
+                    i = 0;
+                }
+                const int o = s0 + k;
+                dst.x[0][o] = a.A.x[0][i]; dst.x[1][o] = a.A.x[1][i]; dst.x[2][o] = a.A.x[2][i];
+                dst.cell[o] = c;
+                S.vx[k] = a.A.v[0][i]; S.vy[k] = a.A.v[1][i]; S.vz[k] = a.A.v[2][i];
+                S.ir[k] = a.A.ir[i];
+            }
+        } else {
+            for (int k = lane; k < n; k += 32) {
+                const int o = s0 + k;
+                S.vx[k] = a.A.v[0][o]; S.vy[k] = a.A.v[1][o]; S.vz[k] = a.A.v[2][o];
+                S.ir[k] = a.A.ir[o];
+            }
+        }
+        __syncwarp();
+        if constexpr (collide) collide_cell<Real>(S.vx, S.vy, S.vz, S.ir, S.claim, n, c, a, istep, pairs, colls);
+        __syncwarp();
+        if constexpr (gather || collide) {
+            for (int k = lane; k < n; k += 32) {
+                const int o = s0 + k;
+                dst.v[0][o] = S.vx[k]; dst.v[1][o] = S.vy[k]; dst.v[2][o] = S.vz[k];
+                dst.ir[o] = S.ir[k];
+            }
+        }
+        if constexpr (sample) {
+            double m[18];
+            moment_partial<Real>(S.vx, S.vy, S.vz, S.ir, n, lane, 32, m);
+            warp_reduce18(m);
+            if (lane == 0)
+                for (int k = 0; k < 18; ++k) S.mom[k] = m[k];
+            __syncwarp();
+            sample_update<Real>(a, c, S.mom, istep, MODE == kModePre);
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        if (pairs) atomicAdd(a.counters + C_PAIRS, (unsigned long long)pairs);
+        if (colls) atomicAdd(a.counters + C_COLLISIONS, (unsigned long long)colls);
+        if (big) atomicAdd(a.counters + C_BIG_CELLS, (unsigned long long)big);
+    }
+}
+
+// Cells with more particles than a warp stages: one 256-thread block per
+// cell, particles staged in dynamic shared memory up to kBlockCap, pairs run
+// by warp 0. Beyond kBlockCap the cell is processed in the output buffer in
+// global memory with pairs one at a time and its far segment left in arrival
+// order (flagged in the error word).
+template <typename Real, int MODE>
+__global__ void __launch_bounds__(256) big_cell_kernel(StepArgs<Real> a)
+{
+    extern __shared__ __align__(16) unsigned char dyn[];
+    Real* sv = reinterpret_cast<Real*>(dyn);
+    Real* svx = sv;
+    Real* svy = sv + kBlockCap;
+    Real* svz = sv + 2 * kBlockCap;
+    Real* sir = sv + 3 * kBlockCap;
+    int* claim = reinterpret_cast<int*>(sv + 4 * kBlockCap);
+    __shared__ double red[8][18];
+    __shared__ double mom[18];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, wid = tid >> 5;
+    const int istep = a.ctl->istep;
+    constexpr bool gather = (MODE == kModeStep || MODE == kModeGather);
+    constexpr bool collide = (MODE == kModeStep || MODE == kModeCollide);
+    constexpr bool sample = (MODE == kModeStep || MODE == kModeSample || MODE == kModePre);
+    const PBuf<Real> dst = gather ? a.B : a.A;
+    const int* start = gather ? a.startB : a.startA;
+    const int nBig = *a.bigCount;
+    uint32_t pairs = 0, colls = 0;
+    for (int bi = blockIdx.x; bi < nBig; bi += gridDim.x) {
+        const int c = a.bigList[bi];
+        const int s0 = start[c];
+        const int n = start[c + 1] - s0;
+        const bool staged = n <= kBlockCap;
+        if constexpr (gather) {
+            const int far = a.countSlot[(size_t)c * kSlots + kFarSlot];
+            __syncthreads();
+            if (tid == 0) a.countSlot[(size_t)c * kSlots + kFarSlot] = 0;
+            int* seg = a.idx + s0 + n - far;
+            if (far > 1 && far <= kBlockCap) {
+                // rank of each far entry among the far entries (distinct values)
+                for (int e = tid; e < far; e += blockDim.x) {
+                    const int v = seg[e];
+                    int r = 0;
+                    for (int f = 0; f < far; ++f) r += seg[f] < v;
+                    claim[r] = v;
+                }
+                __syncthreads();
+                for (int e = tid; e < far; e += blockDim.x) seg[e] = claim[e];
+                __syncthreads();
+            } else if (far > kBlockCap && tid == 0) {
+                atomicOr(a.errorWord, kErrBigCell);
+            }
+            const int nSrc = a.ctl->nLive + a.ctl->nInj;
+            for (int k = tid; k < n; k += blockDim.x) {
+                int i = a.idx[s0 + k];
+                if ((unsigned)i >= (unsigned)nSrc) {
+                    atomicOr(a.errorWord, kErrSortIndex);
+                    i = 0;
+                }
+                const int o = s0 + k;
+                dst.x[0][o] = a.A.x[0][i]; dst.x[1][o] = a.A.x[1][i]; dst.x[2][o] = a.A.x[2][i];
+                dst.cell[o] = c;
+                if (staged) {
+                    svx[k] = a.A.v[0][i]; svy[k] = a.A.v[1][i]; svz[k] = a.A.v[2][i]; sir[k] = a.A.ir[i];
+                } else {
+                    dst.v[0][o] = a.A.v[0][i]; dst.v[1][o] = a.A.v[1][i]; dst.v[2][o] = a.A.v[2][i];
+                    dst.ir[o] = a.A.ir[i];
+                }
+            }
+        } else if (staged) {
+            for (int k = tid; k < n; k += blockDim.x) {
+                const int o = s0 + k;
+                svx[k] = a.A.v[0][o]; svy[k] = a.A.v[1][o]; svz[k] = a.A.v[2][o]; sir[k] = a.A.ir[o];
+            }
+        }
+        __syncthreads();
+        Real* vx = staged ? svx : dst.v[0] + s0;
+        Real* vy = staged ? svy : dst.v[1] + s0;
+        Real* vz = staged ? svz : dst.v[2] + s0;
+        Real* ir = staged ? sir : dst.ir + s0;
+        if constexpr (collide) {
+            if (wid == 0) collide_cell<Real>(vx, vy, vz, ir, staged ? claim : nullptr, n, c, a, istep, pairs, colls);
+        }
+        __syncthreads();
+        if (staged && (gather || collide)) {
+            for (int k = tid; k < n; k += blockDim.x) {
+                const int o = s0 + k;
+                dst.v[0][o] = svx[k]; dst.v[1][o] = svy[k]; dst.v[2][o] = svz[k]; dst.ir[o] = sir[k];
+            }
+        }
+        if constexpr (sample) {
+            double m[18];
+            moment_partial<Real>(vx, vy, vz, ir, n, tid, blockDim.x, m);
+            warp_reduce18(m);
+            if (lane == 0)
+                for (int k = 0; k < 18; ++k) red[wid][k] = m[k];
+            __syncthreads();
+            if (tid < 18) {
+                double s = 0.0;
+                for (int w = 0; w < 8; ++w) s += red[w][tid];
+                mom[tid] = s;
+            }
+            __syncthreads();
+            if (wid == 0) sample_update<Real>(a, c, mom, istep, MODE == kModePre);
+        }
+        __syncthreads();
+    }
+    if (lane == 0) {
+        if (pairs) atomicAdd(a.counters + C_PAIRS, (unsigned long long)pairs);
+        if (colls) atomicAdd(a.counters + C_COLLISIONS, (unsigned long long)colls);
+    }
+}
+
+template <typename Real, int MODE>
+static void launch_cells_mode(const StepArgs<Real>& a, int smCount, cudaStream_t s)
+{
+    cudaMemsetAsync(a.bigCount, 0, sizeof(int), s);
+    int g = (a.M.ncell + 3) / 4;
+    if (g > smCount * 16) g = smCount * 16;
+    cell_kernel<Real, MODE><<<g, 128, 0, s>>>(a);
+    const size_t dyn = (size_t)kBlockCap * (4 * sizeof(Real) + sizeof(int));
+    big_cell_kernel<Real, MODE><<<smCount, 256, dyn, s>>>(a);
+}
+
+template <typename Real>
+cudaError_t prepare_kernels()
+{
+    const int dyn = (int)((size_t)kBlockCap * (4 * sizeof(Real) + sizeof(int)));
+    cudaError_t e = cudaSuccess;
+    const void* fns[5] = {(const void*)big_cell_kernel<Real, kModeStep>, (const void*)big_cell_kernel<Real, kModeGather>,
+                          (const void*)big_cell_kernel<Real, kModeCollide>, (const void*)big_cell_kernel<Real, kModeSample>,
+                          (const void*)big_cell_kernel<Real, kModePre>};
+    for (const void* f : fns) {
+        const cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        if (r != cudaSuccess) e = r;
+    }
+    return e;
+}
+
+template <typename Real>
+void launch_cells(const StepArgs<Real>& a, int mode, int smCount, cudaStream_t s)
+{
+    switch (mode) {
+        case kModeStep: launch_cells_mode<Real, kModeStep>(a, smCount, s); break;
+        case kModeGather: launch_cells_mode<Real, kModeGather>(a, smCount, s); break;
+        case kModeCollide: launch_cells_mode<Real, kModeCollide>(a, smCount, s); break;
+        case kModeSample: launch_cells_mode<Real, kModeSample>(a, smCount, s); break;
+        default: launch_cells_mode<Real, kModePre>(a, smCount, s); break;
+    }
+}
+
+// ===========================================================================
+// macro fields on demand (local from the exponential window, final_record
+// from the steady sum): writeAveragedMacro, src/ProcessDSMC.cpp:2790-2820
+// ===========================================================================
+__global__ void macro_kernel(DevMesh M, DevConsts C, const double* acc, int set, double count, double* out)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < M.ncell; c += gridDim.x * blockDim.x) {
+        double m[18];
+        for (int k = 0; k < 18; ++k) m[k] = acc[(size_t)c * 54 + set * 18 + k];
+        double o[18];
+        averaged_macro(m, count, M.cellVolume[c], C.neff, C.nref, C.dr, o);
+        for (int k = 0; k < 18; ++k) out[(size_t)c * 18 + k] = o[k];
+    }
+}
+
+void launch_macro(const DevMesh& M, const DevConsts& C, const double* acc, int set, double count, double* out,
+                  int ncell, cudaStream_t s)
+{
+    int g = (ncell + 255) / 256;
+    if (g > 2048) g = 2048;
+    macro_kernel<<<g > 0 ? g : 1, 256, 0, s>>>(M, C, acc, set, count, out);
+}
+
+// ===========================================================================
+// tracing check (dsmc_trace)
+// ===========================================================================
+template <typename Real>
+__global__ void trace_check_kernel(DevMesh M, DevConsts C, int n, const Real* px, const Real* py, const Real* pz,
+                                   const Real* vx, const Real* vy, const Real* vz, const double* dt,
+                                   const int* cell, int stopAtWall, int* oCell, int* oIfout, int* oFace,
+                                   int* oTri, int* oNcross, int* oLast, Real* ox, Real* oy, Real* oz, Real* ovx,
+                                   Real* ovy, Real* ovz, double* odt, unsigned long long* counters)
+{
+    TraceCounts cnt{};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        PRegs<Real> p;
+        p.x[0] = px[i]; p.x[1] = py[i]; p.x[2] = pz[i];
+        p.v[0] = vx[i]; p.v[1] = vy[i]; p.v[2] = vz[i];
+        p.ir = (Real)0;
+        int c = cell[i];
+        Stream rs;
+        rs.init((uint32_t)i, 0u, kPurposeWall, C.seedLo, C.seedHi);
+        Real dtleft = (Real)dt[i];
+        TraceLog log{-1, 0, 0};
+        const int out = trace_particle<Real>(M, C, p, c, -1, -1, dtleft, rs, 0, nullptr, cnt, stopAtWall != 0, &log);
+        oCell[i] = (out == kTraceRemoved) ? -1 : c;
+        oIfout[i] = (out >= 0) ? out : -1;
+        oFace[i] = log.hitFace;
+        oTri[i] = log.hitTri;
+        oNcross[i] = log.ncross;
+        ox[i] = p.x[0]; oy[i] = p.x[1]; oz[i] = p.x[2];
+        ovx[i] = p.v[0]; ovy[i] = p.v[1]; ovz[i] = p.v[2];
+        odt[i] = (double)dtleft;
+        oLast[i] = c;   // cell the position is relative to (mixed precision)
+    }
+    flush_counts(counters, cnt);
+}
+
+template <typename Real>
+void launch_trace_check(const DevMesh& M, const DevConsts& C, int n, const Real* px, const Real* py, const Real* pz,
+                        const Real* vx, const Real* vy, const Real* vz, const double* dt, const int* cell,
+                        int stopAtWall, int* oCell, int* oIfout, int* oFace, int* oTri, int* oNcross, int* oLast,
+                        Real* ox, Real* oy, Real* oz, Real* ovx, Real* ovy, Real* ovz, double* odt,
+                        unsigned long long* counters, cudaStream_t s)
+{
+    int g = (n + 255) / 256;
+    if (g > 4096) g = 4096;
+    trace_check_kernel<Real><<<g > 0 ? g : 1, 256, 0, s>>>(M, C, n, px, py, pz, vx, vy, vz, dt, cell, stopAtWall,
+                                                           oCell, oIfout, oFace, oTri, oNcross, oLast, ox, oy, oz,
+                                                           ovx, ovy, ovz, odt, counters);
+}
+
+#define DSMC_INSTANTIATE(Real)                                                                                   \
+    template void launch_inject<Real>(const StepArgs<Real>&, int, cudaStream_t);                                 \
+    template void launch_move<Real>(const StepArgs<Real>&, int, cudaStream_t);                                   \
+    template void launch_sort<Real>(const StepArgs<Real>&, int, cudaStream_t);                                   \
+    template void launch_cells<Real>(const StepArgs<Real>&, int, int, cudaStream_t);                             \
+    template cudaError_t prepare_kernels<Real>();                                                                \
+    template void launch_trace_check<Real>(const DevMesh&, const DevConsts&, int, const Real*, const Real*,       \
+                                           const Real*, const Real*, const Real*, const Real*, const double*,    \
+                                           const int*, int, int*, int*, int*, int*, int*, int*, Real*, Real*,    \
+                                           Real*, Real*, Real*, Real*, double*, unsigned long long*, cudaStream_t);
+DSMC_INSTANTIATE(float)
+DSMC_INSTANTIATE(double)
+
+}  // namespace dsmc

@@ -1,0 +1,100 @@
+// Kernel argument blocks and launch wrappers shared by the engine.
+#pragma once
+
+#include "dsmc_device.cuh"
+
+namespace dsmc {
+
+template <typename Real>
+struct PBuf {
+    Real* x[3];
+    Real* v[3];
+    Real* ir;
+    int* cell;
+};
+
+// Device-resident step control (read by kernels, so captured graphs replay
+// with the current values).
+struct StepCtl {
+    int istep;
+    int nLive;        // particles in the current buffer
+    int nInj;         // particles injected this step (appended after nLive)
+    int nNext;        // particles after the sort
+    int capacity;
+    int pad[3];
+};
+
+struct DevPatches {
+    int npatch, ngroup;
+    const int* groupStart;     // [ngroup+1] into patch arrays (patches grouped by cell)
+    const int* cell;           // [npatch]
+    const int* edge;           // [npatch]
+    const int* triTag;         // [npatch]
+    const double* geom;        // [npatch*9] p0, e10, e20
+    const double* rot;         // [npatch*9] rotation of -normal
+    const double* gas;         // [npatch*8] snp, fs1, fs2, stp1, stp2, tN, sqrt(tN), QA
+    const double* addBase;     // [npatch]
+    int* count;                // [npatch] this step
+    int* start;                // [npatch] exclusive scan
+};
+
+template <typename Real>
+struct StepArgs {
+    DevMesh M;
+    DevConsts C;
+    DevPatches P;
+    PBuf<Real> A;             // current buffer (source of the step)
+    PBuf<Real> B;             // next buffer (sorted output)
+    const int* startA;        // [ncell+1] layout of A
+    int* startB;              // [ncell+1] layout of B
+    int* rank;                // [cap] packed slot<<24 | rank
+    int* idx;                 // [cap] sorted source indices
+    int* countSlot;           // [ncell*8]
+    int* scanPartial;         // [kScanBlocks]
+    double* crmax;            // [ncell]
+    double* remColl;          // [ncell]
+    double* remInj;           // [ncell]
+    double* acc;              // [ncell*54]: stepsum, steady, stepinter (18 each)
+    double* record;           // [ncell*18]
+    double* local;            // [ncell*18]
+    double* finalRecord;      // [ncell*18]
+    double* stepMom;          // [ncell*18] or nullptr
+    unsigned char* sparseState;
+    int* sparseAccum;
+    double* windowSamples;
+    char* windowValid;
+    double* wallTally;        // [nwall*6]
+    StepCtl* ctl;
+    unsigned long long* counters;
+    int* bigList;
+    int* bigCount;
+    int* errorWord;
+};
+
+constexpr int kScanBlocks = 296;
+constexpr int kWarpCap = 256;      // particles a warp stages in shared memory
+constexpr int kBlockCap = 4096;    // particles the large-cell block stages
+
+// cell-kernel modes
+constexpr int kModeStep = 0;       // gather A->B + collide + sample (fused step)
+constexpr int kModeGather = 1;     // gather only (cache2chain)
+constexpr int kModeCollide = 2;    // collide in place on A
+constexpr int kModeSample = 3;     // sample in place on A
+constexpr int kModePre = 4;        // statistic_macroPre on A
+
+template <typename Real> void launch_inject(const StepArgs<Real>& a, int smCount, cudaStream_t s);
+template <typename Real> void launch_move(const StepArgs<Real>& a, int smCount, cudaStream_t s);
+template <typename Real> void launch_sort(const StepArgs<Real>& a, int smCount, cudaStream_t s);
+template <typename Real> void launch_cells(const StepArgs<Real>& a, int mode, int smCount, cudaStream_t s);
+template <typename Real> cudaError_t prepare_kernels();
+void launch_macro(const DevMesh& M, const DevConsts& C, const double* acc, int set, double count,
+                  double* out, int ncell, cudaStream_t s);
+template <typename Real>
+void launch_trace_check(const DevMesh& M, const DevConsts& C, int n, const Real* px, const Real* py,
+                        const Real* pz, const Real* vx, const Real* vy, const Real* vz,
+                        const double* dt, const int* cell, int stopAtWall, int* oCell, int* oIfout,
+                        int* oFace, int* oTri, int* oNcross, int* oLast, Real* ox, Real* oy, Real* oz,
+                        Real* ovx, Real* ovy, Real* ovz, double* odt, unsigned long long* counters,
+                        cudaStream_t s);
+
+}  // namespace dsmc

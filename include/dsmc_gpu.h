@@ -1,0 +1,284 @@
+/*
+ * dsmc_gpu.h — C ABI of the B200 DSMC particle step.
+ *
+ * Drop-in boundary for the DSMC member functions that the reference's driver
+ * (src/meshImportTest.cpp:171-234), dynamicDSMC and ProcessGSIS call on
+ * ProcessDSMC (src/ProcessDSMC.h:441-492). The host keeps the mesh import and
+ * the macroscopic GSIS / NS-G13 step; one handle holds one case (mesh,
+ * particles, per-cell collision and sampling state) resident on one GPU.
+ *
+ * Conventions
+ *   - Every entry point returns 0 on success or a negative DSMC_E_* code; no
+ *     C++ exception crosses this boundary. dsmc_last_error() gives the text.
+ *   - Host buffers are owned by the caller and only accessed during the call.
+ *   - Array layouts are the reference's: per-cell macro fields are
+ *     [cell][18] doubles in MacroIndex order (src/ProcessDSMC.h:28-49), the
+ *     mesh arrays are DsmcCell[] / DsmcEdge[] / localPointXY[3*npoint] /
+ *     faceSplitTag[nface] (src/meshImport.h:168-189), case constants are a
+ *     meshMessage image (src/meshImport.h:192-208).
+ *   - One domain: local cell id == global cell id, one compute "rank".
+ *   - A handle is used by one host thread at a time (or externally
+ *     serialised); its work runs on one CUDA stream it owns.
+ */
+#ifndef DSMC_GPU_H
+#define DSMC_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define DSMC_OK              0
+#define DSMC_E_INVALID      -1   /* bad argument / inconsistent mesh        */
+#define DSMC_E_CUDA         -2   /* CUDA runtime error                      */
+#define DSMC_E_NOMEM        -3   /* device allocation failed                */
+#define DSMC_E_CAPACITY     -4   /* particle store overflow                 */
+#define DSMC_E_DEVICE_FAULT -5   /* kernel-reported error (see counters)    */
+#define DSMC_E_STATE        -6   /* call out of order                       */
+
+/* ---- mesh records: byte layout of the reference's structs --------------- */
+/* DsmcCell, src/meshImport.h:168-178 (120 bytes) */
+typedef struct DsmcCellRec {
+    int32_t num;
+    int32_t fluentCellType;
+    int32_t cell2face[6];
+    int32_t cell2cell[6];
+    int32_t cell2face_sgn[6];
+    double  area;             /* cell VOLUME (src/meshImport.cpp:719) */
+    int32_t no;
+    double  cellXY[3];
+} DsmcCellRec;
+
+/* DsmcEdge, src/meshImport.h:180-189 (88 bytes); faceMap[4..5] = c0, c1 */
+typedef struct DsmcEdgeRec {
+    int32_t faceTag;
+    int32_t faceType;
+    double  length;           /* face area */
+    int32_t faceMap[6];
+    double  edgeNormal[3];    /* unit, from c0 to c1 */
+    double  edgeCenter[3];
+} DsmcEdgeRec;
+
+/* meshMessage, src/meshImport.h:192-208 (344 bytes) */
+typedef struct DsmcMeshMessage {
+    int32_t Ncell, Nface, Npoint, Nk, bcnumber, Nghost;
+    double Area;
+    double Ma, Kn, cfl;
+    double gamma, dr, dv, zr, zv, omega;
+    int32_t var, qn;
+    double f_tra, f_rot;
+    double delta_rp, delta_sm, omeag0, omeag1;
+    double cfl_ns, pr, cp, cv;
+    double kB, p_mass, p_mass_r, T_ref, n_ref, miu_ref, Twall_ref, p_ref, d_ref;
+    double alpha, v_rms, eta, P_relax, dt_ref;
+    double T_in, v_in;
+    int32_t eNface, iNface;
+    double Neff;
+    double dtime;
+} DsmcMeshMessage;
+
+typedef struct DsmcMeshDesc {
+    int32_t ncell;
+    int32_t nface;
+    int32_t npoint;
+    const DsmcCellRec* cells;          /* [ncell] */
+    const DsmcEdgeRec* edges;          /* [nface] */
+    const double* localPointXY;        /* [3*npoint] */
+    const unsigned char* faceSplitTag; /* [nface], FACE_SPLIT_02/13/255 */
+} DsmcMeshDesc;
+
+/* DSMC role of a Fluent zone tag (BoundaryRole, src/BoundaryCondition.h:10-24;
+ * SPECULAR is this library's addition: mirror reflection, no reference
+ * counterpart, where the reference leaves the tag unmapped). */
+enum DsmcRole {
+    DSMC_ROLE_NONE = 0,
+    DSMC_ROLE_INTERFACE = 1,
+    DSMC_ROLE_INLET = 2,
+    DSMC_ROLE_OUTLET = 3,
+    DSMC_ROLE_WALL = 4,
+    DSMC_ROLE_SPECULAR = 5
+};
+
+enum DsmcPrecision {
+    DSMC_PRECISION_FP64 = 0,   /* all-FP64 state and arithmetic (reference) */
+    DSMC_PRECISION_MIXED = 1   /* FP32 state/trace/collide, FP64 fallback
+                                  and FP64 accumulators */
+};
+
+#define DSMC_MAX_ZONES 16
+
+/* Controls that are compile-time constants or hard-coded values in the
+ * reference (src/meshImport.h:45-58, src/ProcessDSMC.cpp:2330-2331,
+ * src/BoundaryCondition.h:79-117). dsmc_default_params() fills the
+ * reference's values. */
+typedef struct DsmcCaseParams {
+    int32_t precision;            /* DsmcPrecision */
+    int32_t nss;                  /* NSS: steady sampling starts after it   */
+    int32_t nscheme;              /* NSCHEME: exponential-average window    */
+    int32_t nevery;               /* Nevery                                 */
+    int32_t nrepeat;              /* Nrepeat (NGSIS = nevery*nrepeat)       */
+    int32_t wall_stats;           /* EnableBoundaryStressHeatStatistic      */
+    double  inflow_dir[2];        /* drift direction (x,y); reference 30 deg */
+    int32_t nzones;
+    int32_t zone_tag[DSMC_MAX_ZONES];
+    int32_t zone_role[DSMC_MAX_ZONES];   /* DsmcRole */
+    int32_t zone_inject[DSMC_MAX_ZONES]; /* inlet zones that emit particles */
+    int64_t capacity;             /* particle store size; 0 = automatic      */
+    uint64_t seed;                /* Philox key                              */
+    int32_t max_crossings;        /* per particle per step; lost beyond it   */
+    int32_t keep_step_moments;    /* keep last step's raw moments on device  */
+} DsmcCaseParams;
+
+/* Stage flags of dsmc_step, in the reference's step order
+ * (src/meshImportTest.cpp:207-234). */
+#define DSMC_STAGE_INJECT   0x1u   /* preprocesseffquad */
+#define DSMC_STAGE_MOVE     0x2u   /* advection         */
+#define DSMC_STAGE_SORT     0x4u   /* cache2chain       */
+#define DSMC_STAGE_COLLIDE  0x8u   /* collisionDSMC     */
+#define DSMC_STAGE_SAMPLE   0x10u  /* statistic_macro   */
+#define DSMC_STAGE_ALL      0x1Fu
+
+/* dsmc_download_macro targets (ProcessDSMC::local/record/final_record) */
+#define DSMC_MACRO_LOCAL        0
+#define DSMC_MACRO_RECORD       1
+#define DSMC_MACRO_FINAL_RECORD 2
+#define DSMC_MACRO_WIDTH        18
+
+/* cumulative device counters, dsmc_get_counters() */
+typedef struct DsmcCounters {
+    uint64_t steps;
+    uint64_t injected;          /* particles emitted by inlet patches        */
+    uint64_t removed;           /* left through an inlet / outlet face       */
+    uint64_t dropped;           /* no exit face found (reference "Dropped")  */
+    uint64_t lost;              /* crossing cap hit or bad neighbour         */
+    uint64_t wall_hits;
+    uint64_t crossings;         /* face crossings of all kinds               */
+    uint64_t candidate_pairs;   /* NTC pairs (tol_collision_pairs)           */
+    uint64_t collisions;        /* accepted pairs (tol_collision_times)      */
+    uint64_t fp64_fallbacks;    /* mixed path: crossing steps redone in FP64 */
+    uint64_t overflow;          /* particles not stored: capacity exceeded   */
+    uint64_t big_cells;         /* cells handled by the large-cell path      */
+} DsmcCounters;
+
+typedef struct DsmcHandle DsmcHandle;
+
+/* Fill *p with the reference's compile-time values. Replaces the constants
+ * at src/meshImport.h:45-58 and the boundary table of
+ * src/BoundaryCondition.h:79-117. */
+void dsmc_default_params(DsmcCaseParams* p);
+
+/* Build a case: copies the mesh, builds the per-cell triangle cache
+ * (rebuildFaceTraversalCache, src/ProcessDSMCGeometry.cpp:145-214), the
+ * face-cross cache (src/ProcessDSMCGeometry.cpp:114-136), wall normals
+ * (processFacesQuadNormals, src/ProcessDSMC.cpp:1054-1127) and inlet emit
+ * patches (rebuildBoundaryEmitCache, src/ProcessDSMC.cpp:583-768), and
+ * allocates all device state. Replaces ProcessDSMC::ProcessDSMC
+ * (src/ProcessDSMC.cpp:271-288) plus Collision_constant_initial
+ * (src/MeshparticalInitial.cpp:798-810). device < 0 uses the current one. */
+int dsmc_create(const DsmcMeshDesc* mesh, const DsmcMeshMessage* mess,
+                const DsmcCaseParams* params, int device, DsmcHandle** out);
+
+void dsmc_destroy(DsmcHandle* h);
+
+/* Text of the last error on this handle (or of the last failed create when
+ * h is NULL). */
+const char* dsmc_last_error(const DsmcHandle* h);
+
+/* Replace all particles (the buckets cell_particles_curr,
+ * src/MeshparticalInitial.h:229) with n particles given as SoA host arrays.
+ * cell[] are local cell ids. Particles are binned and canonically ordered on
+ * the device. */
+int dsmc_upload_particles(DsmcHandle* h, int64_t n,
+                          const double* px, const double* py, const double* pz,
+                          const double* vx, const double* vy, const double* vz,
+                          const double* ir, const int32_t* cell);
+
+/* Particle count (sum of bucket sizes). */
+int dsmc_particle_count(DsmcHandle* h, int64_t* n);
+
+/* Copy all particles back (cell-major, within a cell by particle id). Any
+ * pointer may be NULL to skip that array. pid[] are the device particle ids. */
+int dsmc_download_particles(DsmcHandle* h, int64_t n,
+                            double* px, double* py, double* pz,
+                            double* vx, double* vy, double* vz,
+                            double* ir, int32_t* cell, uint32_t* pid);
+
+/* One DSMC step, stages selected by DSMC_STAGE_* flags, in reference order.
+ * DSMC_STAGE_ALL is the fused production path (one CUDA graph). */
+int dsmc_step(DsmcHandle* h, int32_t istep, uint32_t stages);
+
+/* Stage entry points with the reference's member names and arguments
+ * (src/ProcessDSMC.h:459-488). Calling the five in order equals
+ * dsmc_step(h, istep, DSMC_STAGE_ALL). */
+int dsmc_preprocesseffquad(DsmcHandle* h, int32_t istep); /* ProcessDSMC.cpp:2556 */
+int dsmc_advection(DsmcHandle* h, int32_t istep);         /* ProcessDSMC.cpp:1946 */
+int dsmc_cache2chain(DsmcHandle* h);                      /* ProcessDSMC.cpp:2030 */
+int dsmc_collisionDSMC(DsmcHandle* h);                    /* ProcessDSMC.cpp:2621 */
+int dsmc_statistic_macro(DsmcHandle* h, int32_t istep);   /* ProcessDSMC.cpp:2757 */
+int dsmc_statistic_macroPre(DsmcHandle* h);               /* ProcessDSMC.cpp:3312 */
+
+/* Per-cell macro fields [ncell][18] (local / record / final_record). */
+int dsmc_download_macro(DsmcHandle* h, int32_t which, double* out);
+
+/* Per-cell state read by ProcessGSIS::DSMC2NS (src/ProcessGSIS.cpp:1569-1656).
+ * Any pointer may be NULL. ppc = particles per cell. */
+int dsmc_download_counts(DsmcHandle* h, int32_t* ppc, double* window_samples,
+                         char* window_valid, unsigned char* sparse_state,
+                         double* stepinter_rho, double* steady_rho);
+
+/* Raw per-cell moment sums [ncell][18] of the last sampled step (requires
+ * params.keep_step_moments) in the order
+ * N, Σv(3), Σv², Σvv(xx,xy,yy,yz,zz,zx), Σv v²(3), ΣIr, Σv Ir(3). */
+int dsmc_download_step_moments(DsmcHandle* h, double* out);
+
+/* Wall surface tallies [nface][6]: hits, Δmomentum(3), ΔE_tr, ΔE_rot
+ * (recordBoundaryStressHeat, src/ProcessDSMC.cpp:1659-1689); zero rows for
+ * non-wall faces. */
+int dsmc_download_wall(DsmcHandle* h, double* tally);
+
+/* Per-cell collision state: crmax, remainderincoll (src/MeshparticalInitial.h:
+ * 233-235) and per-cell inflow remainder remainderinpre. Any may be NULL. */
+int dsmc_download_cell_state(DsmcHandle* h, double* crmax, double* rem_coll, double* rem_inj);
+int dsmc_upload_cell_state(DsmcHandle* h, const double* crmax, const double* rem_coll, const double* rem_inj);
+
+int dsmc_get_counters(DsmcHandle* h, DsmcCounters* out);
+
+/* Tracing check entry (the move kernel's trace on caller-given particles,
+ * no state change): each particle i starts in cell[i] at (p*, v*) with
+ * dt[i] to fly, exactly as ParticleTransportOps::traceParticleDtleft
+ * (src/ProcessDSMC.cpp:149-221) with a fresh crossing state. With
+ * stop_at_wall != 0 a particle stops at its first wall hit instead of being
+ * re-emitted. Outputs (any may be NULL): final cell (-1 removed/dropped),
+ * ifout (0 stayed, 1 crossed, -1 removed/dropped), first non-interface face
+ * and its triangle tag (-1/0 if none), number of crossings, final position,
+ * velocity and remaining dt. Runs at the handle's precision. */
+int dsmc_trace(DsmcHandle* h, int64_t n,
+               const double* px, const double* py, const double* pz,
+               const double* vx, const double* vy, const double* vz,
+               const double* dt, const int32_t* cell, int32_t stop_at_wall,
+               int32_t* out_cell, int32_t* out_ifout, int32_t* out_face,
+               int32_t* out_tri, int32_t* out_ncross,
+               double* out_px, double* out_py, double* out_pz,
+               double* out_vx, double* out_vy, double* out_vz, double* out_dt);
+
+/* Stage timing: with on != 0, dsmc_step runs its kernels without a CUDA
+ * graph and records CUDA events between the stages; dsmc_stage_ms then
+ * returns the device time of [inject, move, sort, collide+sample] summed
+ * over the timed steps since the last reset (reset != 0 clears the sums
+ * after reading). Off (the default) replays one captured graph per step. */
+int dsmc_set_timing(DsmcHandle* h, int32_t on);
+int dsmc_stage_ms(DsmcHandle* h, double* ms4, int64_t* nsteps, int32_t reset);
+
+/* The CUDA stream the handle's work runs on (a cudaStream_t). */
+void* dsmc_stream(DsmcHandle* h);
+
+/* Synchronise the handle's stream and report kernel-side errors. */
+int dsmc_sync(DsmcHandle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DSMC_GPU_H */

@@ -1,0 +1,118 @@
+"""Runner for oracle/_ref/ref_harness, the reference's own DSMC code built
+from its sources (ORACLE TEST INFRASTRUCTURE: used by tests/, the golden
+fixture generator and bench.py's reference arm only).
+
+Build recipe: ``make -C oracle ref`` (needs the reference sources; the built
+binary is self-contained and travels with the repository snapshot).
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BIN = os.path.join(HERE, "_ref", "ref_harness")
+
+
+def available() -> bool:
+    return os.path.exists(BIN) and os.access(BIN, os.X_OK)
+
+
+def _run(args, timeout=3600):
+    r = subprocess.run([BIN, *map(str, args)], capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"ref_harness {args[0]} failed ({r.returncode}): {r.stderr[-2000:]}")
+    return r.stdout
+
+
+def dump_mesh(cas: str, Ma: float, Kn: float, cell_dtype, edge_dtype, mess_dtype) -> dict:
+    with tempfile.TemporaryDirectory() as d:
+        _run(["mesh", cas, d, Ma, Kn])
+        return {
+            "cells": np.fromfile(os.path.join(d, "cells.bin"), dtype=cell_dtype),
+            "edges": np.fromfile(os.path.join(d, "edges.bin"), dtype=edge_dtype),
+            "points": np.fromfile(os.path.join(d, "points.bin"), dtype=np.float64),
+            "split": np.fromfile(os.path.join(d, "split.bin"), dtype=np.uint8),
+            "mess": np.fromfile(os.path.join(d, "mess.bin"), dtype=mess_dtype)[0],
+        }
+
+
+def _write_particles(path, x, v, ir, dt, cell):
+    n = int(np.asarray(cell).shape[0])
+    with open(path, "wb") as f:
+        f.write(np.int64(n).tobytes())
+        for k in range(3):
+            f.write(np.ascontiguousarray(x[:, k], dtype=np.float64).tobytes())
+        for k in range(3):
+            f.write(np.ascontiguousarray(v[:, k], dtype=np.float64).tobytes())
+        f.write(np.ascontiguousarray(ir, dtype=np.float64).tobytes())
+        f.write(np.ascontiguousarray(dt, dtype=np.float64).tobytes())
+        f.write(np.ascontiguousarray(cell, dtype=np.int32).tobytes())
+
+
+def _read_particles(path) -> dict:
+    b = np.fromfile(path, dtype=np.uint8)
+    n = int(b[:8].view(np.int64)[0])
+    d = b[8:8 + n * 64].view(np.float64).reshape(8, n)
+    cell = b[8 + n * 64:8 + n * 68].view(np.int32)
+    return {"x": d[0:3].T.copy(), "v": d[3:6].T.copy(), "ir": d[6].copy(), "dt": d[7].copy(), "cell": cell.copy()}
+
+
+def _write_mess(path, mess):
+    np.asarray(mess).reshape(()).tofile(path)
+
+
+def trace(cas: str, mess, x, v, dt, cell, stop_at_wall: bool = True) -> dict:
+    """The reference's tracing loop on the given particles."""
+    n = int(np.asarray(cell).shape[0])
+    with tempfile.TemporaryDirectory() as d:
+        pm, pp, po = (os.path.join(d, k) for k in ("mess.bin", "parts.bin", "out.bin"))
+        _write_mess(pm, mess)
+        _write_particles(pp, x, v, np.zeros(n), dt, cell)
+        _run(["trace", cas, pm, pp, po, int(stop_at_wall)])
+        b = np.fromfile(po, dtype=np.uint8)
+        m = int(b[:8].view(np.int64)[0])
+        ints = b[8:8 + 20 * m].view(np.int32).reshape(5, m)
+        dbl = b[8 + 20 * m:].view(np.float64).reshape(7, m)
+        return {"cell": ints[0].copy(), "ifout": ints[1].copy(), "face": ints[2].copy(), "tri": ints[3].copy(),
+                "ncross": ints[4].copy(), "x": dbl[0:3].T.copy(), "v": dbl[3:6].T.copy(), "dt": dbl[6].copy()}
+
+
+def advect(cas: str, mess, x, v, ir, cell, istep: int = 1, roles: str = "-") -> dict:
+    """The reference's advection(istep) + cache2chain(); buckets in order."""
+    n = int(np.asarray(cell).shape[0])
+    with tempfile.TemporaryDirectory() as d:
+        pm, pp, po = (os.path.join(d, k) for k in ("mess.bin", "parts.bin", "out.bin"))
+        _write_mess(pm, mess)
+        _write_particles(pp, x, v, ir, np.zeros(n), cell)
+        _run(["advect", cas, pm, pp, po, istep, roles])
+        return _read_particles(po)
+
+
+def run(cas: str, mess, x, v, ir, cell, nsteps: int, seed: int, roles: str = "-", avg_from: int = 1,
+        timeout: int = 3600) -> dict:
+    """The reference's five-call step loop for nsteps; returns its dumps and
+    the timing line."""
+    n = int(np.asarray(cell).shape[0])
+    ncell = None
+    with tempfile.TemporaryDirectory() as d:
+        pm, pp = os.path.join(d, "mess.bin"), os.path.join(d, "parts.bin")
+        _write_mess(pm, mess)
+        _write_particles(pp, x, v, ir, np.zeros(n), cell)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        txt = _run(["run", cas, pm, pp, out, nsteps, seed, roles, avg_from], timeout=timeout)
+        res = {"timing": json.loads(txt.strip().splitlines()[-1])}
+        res["steps"] = np.fromfile(os.path.join(out, "steps.bin"), dtype=np.int64).reshape(nsteps, 4)
+        for k in ("moments", "local", "record", "final_record"):
+            a = np.fromfile(os.path.join(out, k + ".bin"), dtype=np.float64)
+            res[k] = a.reshape(-1, 18)
+        for k in ("crmax", "remcoll", "reminj", "window_samples"):
+            res[k] = np.fromfile(os.path.join(out, k + ".bin"), dtype=np.float64)
+        res["sparse_state"] = np.fromfile(os.path.join(out, "sparse_state.bin"), dtype=np.uint8)
+        res["particles"] = _read_particles(os.path.join(out, "particles.bin"))
+        return res

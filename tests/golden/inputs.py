@@ -1,0 +1,102 @@
+"""Deterministic inputs shared by the golden-fixture generator and the tests.
+
+Inputs are rebuilt from seeds with numpy's legacy RandomState (MT19937),
+whose streams numpy keeps fixed across versions, so the fixtures only need
+to store the reference's outputs.
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "dig-appolo_b200"))
+
+from pydsmc import case as C  # noqa: E402
+from pydsmc import mesh as M  # noqa: E402
+
+# the block case, 1/4 resolution: 12x8x8 hexes minus the central 2x2x2 block
+BLOCK_SCALE = 4
+BLOCK_MA = 5.0
+BLOCK_KN = 0.1
+BLOCK_L0 = 0.125          # edge of the removed block in y/z (8 cells of 0.5/32 m)
+AOA_DEG = 30.0            # the reference's hard-coded angle of attack
+# reference boundary table (src/BoundaryCondition.h:79-117); tag 7 unmapped
+REF_ZONES = [(3, 1, 0), (4, 2, 1), (5, 3, 0), (6, 4, 0)]
+# the same with the wall zone as an outlet: advection without random draws
+NOWALL_ZONES = [(3, 1, 0), (4, 2, 1), (5, 3, 0), (6, 3, 0)]
+
+
+def block_mesh(scale: int = BLOCK_SCALE):
+    raw = M.block_case_mesh(scale=scale)
+    return raw, M.build_dsmc_mesh(raw)
+
+
+def block_mess(dm, ppc: int):
+    return C.mesh_message(dm, BLOCK_MA, BLOCK_KN, ppc=ppc, L0=BLOCK_L0)
+
+
+def inflow_dir():
+    return C.inflow_direction(AOA_DEG)
+
+
+def _cell_boxes(dm):
+    P = dm.points.reshape(-1, 3)
+    fm = dm.edges["faceMap"]
+    lo = np.full((dm.ncell, 3), np.inf)
+    hi = np.full((dm.ncell, 3), -np.inf)
+    for m in range(6):
+        f = dm.cells["cell2face"][:, m]
+        for q in range(4):
+            pts = P[fm[f, q]]
+            lo = np.minimum(lo, pts)
+            hi = np.maximum(hi, pts)
+    return lo, hi
+
+
+def freestream(mess):
+    d = inflow_dir()
+    base = 1.0 * float(mess["Ma"]) * math.sqrt(float(mess["gamma"]) / 2.0) * float(mess["v_in"]) / float(mess["v_rms"])
+    u = np.array([base * d[0], base * d[1], 0.0])
+    tN = float(mess["T_in"]) / float(mess["T_ref"])
+    return u, math.sqrt(tN / 2.0), tN
+
+
+def trace_inputs(dm, mess, n: int, seed: int):
+    """Uniform random hex cells, uniform positions, isotropic velocities with
+    mean speed 3x the freestream speed, one dt."""
+    rs = np.random.RandomState(seed)
+    cells = rs.randint(0, dm.ncell, size=n).astype(np.int32)
+    lo, hi = _cell_boxes(dm)
+    x = lo[cells] + (hi[cells] - lo[cells]) * rs.random_sample((n, 3))
+    u, _, _ = freestream(mess)
+    sigma = 3.0 * float(np.linalg.norm(u)) / math.sqrt(8.0 / math.pi)
+    v = sigma * rs.standard_normal((n, 3))
+    dt = np.full(n, float(mess["dtime"]))
+    return x, v, dt, cells
+
+
+def fill_inputs(dm, mess, ppc: int, seed: int):
+    """ppc particles per cell from the freestream Maxwellian."""
+    rs = np.random.RandomState(seed)
+    cells = np.repeat(np.arange(dm.ncell, dtype=np.int32), ppc)
+    lo, hi = _cell_boxes(dm)
+    x = lo[cells] + (hi[cells] - lo[cells]) * rs.random_sample((cells.shape[0], 3))
+    u, sig, tN = freestream(mess)
+    v = u[None, :] + sig * rs.standard_normal((cells.shape[0], 3))
+    ir = -np.log(1.0 - rs.random_sample(cells.shape[0])) * tN * 0.5
+    return x, v, ir, cells
+
+
+def fields_from_moments(mom_sum: np.ndarray, nsteps: int, dm, mess) -> np.ndarray:
+    """Time-averaged rho (per step), u (3), T and Tr from summed raw moments."""
+    N = mom_sum[:, 0]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rho = float(mess["Neff"]) / dm.cells["area"] * N / nsteps / float(mess["n_ref"])
+        u = mom_sum[:, 1:4] / N[:, None]
+        T = 2.0 / 3.0 * (mom_sum[:, 4] / N - (u * u).sum(1))
+        Tr = 4.0 / float(mess["dr"]) * mom_sum[:, 14] / N
+    return np.column_stack([rho, u, T, Tr])

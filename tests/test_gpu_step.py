@@ -1,0 +1,145 @@
+"""Full-step parity on the B200 through the C ABI.
+
+- Deterministic parts against the reference's own outputs: advection +
+  cache2chain on the wall-free block case (tests/golden/advect_pin.npz),
+  per-cell inflow remainders after 60 steps (inflow_pin.npz).
+- The whole FP64 step against the oracle, which runs the same algorithm with
+  the same Philox streams and canonical particle order: particle counts per
+  cell exact, particle states and per-cell accumulators equal to a relative
+  1e-9 (the GPU's and libm's transcendental functions differ in the last
+  bits).
+- Determinism: a repeated run, the graph and non-graph launches and the
+  stage-by-stage entry points give bit-identical results.
+"""
+import numpy as np
+import pytest
+
+import inputs as I
+from conftest import golden
+from gpu_util import make_case, make_oracle, rel_close
+from pydsmc import gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def test_advection_matches_reference(block):
+    raw, dm, mess = block
+    g = golden("advect_pin.npz")
+    x, v, ir, cell = I.fill_inputs(dm, mess, 10, seed=2)
+    with make_case(dm, mess, zones=I.NOWALL_ZONES) as case:
+        case.upload_particles(x, v, ir, cell)
+        case.advection(1)
+        case.cache2chain()
+        xg, vg, irg, cg = case.download_particles()
+    assert np.array_equal(np.bincount(cg, minlength=dm.ncell), g["ppc"])
+    order = np.lexsort((vg[:, 2], vg[:, 1], vg[:, 0]))
+    assert np.array_equal(vg[order], g["v"])
+    assert np.array_equal(cg[order], g["cell"])
+    assert np.array_equal(xg[order], g["x"])
+
+
+def test_inflow_remainders_match_reference(block):
+    raw, dm, mess = block
+    g = golden("inflow_pin.npz")
+    x, v, ir, cell = I.fill_inputs(dm, mess, 20, seed=3)
+    with make_case(dm, mess, seed=5) as case:
+        case.upload_particles(x, v, ir, cell)
+        for s in range(1, int(g["steps"]) + 1):
+            case.step(s)
+        _, _, rem = case.cell_state()
+    assert np.array_equal(rem, g["reminj"])
+
+
+def _run_gpu(dm, mess, x, v, ir, cell, nsteps, seed, stagewise=False, graph=True, precision=gpu.PRECISION_FP64,
+             zones=None):
+    import os
+    old = os.environ.pop("DSMC_NO_GRAPH", None)
+    if not graph:
+        os.environ["DSMC_NO_GRAPH"] = "1"
+    try:
+        with make_case(dm, mess, zones=zones, seed=seed, precision=precision, keep_step_moments=1) as case:
+            case.upload_particles(x, v, ir, cell)
+            case.statistic_macroPre()
+            for s in range(1, nsteps + 1):
+                if stagewise:
+                    case.preprocesseffquad(s)
+                    case.advection(s)
+                    case.cache2chain()
+                    case.collisionDSMC()
+                    case.statistic_macro(s)
+                else:
+                    case.step(s)
+            case.sync()
+            out = {
+                "particles": case.download_particles(),
+                "cell_state": case.cell_state(),
+                "moments": case.step_moments(),
+                "local": case.macro(gpu.MACRO_LOCAL),
+                "record": case.macro(gpu.MACRO_RECORD),
+                "counts": case.counts(),
+                "counters": case.counters(),
+            }
+    finally:
+        os.environ.pop("DSMC_NO_GRAPH", None)
+        if old is not None:
+            os.environ["DSMC_NO_GRAPH"] = old
+    return out
+
+
+def test_fp64_step_matches_oracle(block):
+    raw, dm, mess = block
+    x, v, ir, cell = I.fill_inputs(dm, mess, 20, seed=3)
+    nsteps = 3
+    g = _run_gpu(dm, mess, x, v, ir, cell, nsteps, seed=9)
+    o = make_oracle(dm, mess, seed=9)
+    o.set_particles(x, v, ir, cell)
+    o.macro_pre()
+    for s in range(1, nsteps + 1):
+        o.step(s)
+    xo, vo, iro, co = o.particles()
+    xg, vg, irg, cg = g["particles"]
+    assert np.array_equal(np.bincount(cg, minlength=dm.ncell), np.bincount(co, minlength=dm.ncell))
+    assert np.array_equal(cg, co)
+    for a, b in ((xg, xo), (vg, vo), (irg, iro)):
+        ok = rel_close(a, b, 1e-9, 1e-12)
+        assert ok.mean() >= 0.999, ok.mean()
+    cs_g, cs_o = g["cell_state"], o.cell_state()
+    assert np.array_equal(cs_g[2], cs_o[2])                    # inflow remainders exact
+    assert np.all(rel_close(cs_g[1], cs_o[1], 1e-9, 1e-9).mean() >= 0.99)
+    assert np.all(rel_close(cs_g[0], cs_o[0], 1e-9).mean() >= 0.99)
+    assert np.all(rel_close(g["moments"], o.step_moments(), 1e-9, 1e-9).mean() >= 0.999)
+    cg_, co_ = g["counters"], o.counters()
+    for k in ("injected", "candidate_pairs"):
+        assert cg_[k] == co_[k], k
+    for k in ("removed", "wall_hits", "collisions", "crossings"):
+        assert abs(cg_[k] - co_[k]) <= max(2, 1e-3 * co_[k]), k
+
+
+def test_repeat_graph_and_stagewise_are_bit_identical(block):
+    raw, dm, mess = block
+    x, v, ir, cell = I.fill_inputs(dm, mess, 20, seed=4)
+    a = _run_gpu(dm, mess, x, v, ir, cell, 4, seed=21)
+    b = _run_gpu(dm, mess, x, v, ir, cell, 4, seed=21)
+    c = _run_gpu(dm, mess, x, v, ir, cell, 4, seed=21, graph=False)
+    d = _run_gpu(dm, mess, x, v, ir, cell, 4, seed=21, stagewise=True)
+    for other in (b, c, d):
+        for pa, pb in zip(a["particles"], other["particles"]):
+            assert np.array_equal(pa, pb)
+        for sa, sb in zip(a["cell_state"], other["cell_state"]):
+            assert np.array_equal(sa, sb)
+        assert np.array_equal(a["moments"], other["moments"])
+        assert np.array_equal(a["local"], other["local"])
+
+
+def test_mixed_step_runs_and_conserves(block):
+    raw, dm, mess = block
+    x, v, ir, cell = I.fill_inputs(dm, mess, 20, seed=4)
+    a = _run_gpu(dm, mess, x, v, ir, cell, 20, seed=3, precision=gpu.PRECISION_MIXED)
+    b = _run_gpu(dm, mess, x, v, ir, cell, 20, seed=3, precision=gpu.PRECISION_MIXED)
+    for pa, pb in zip(a["particles"], b["particles"]):
+        assert np.array_equal(pa, pb)
+    c = a["counters"]
+    assert c["lost"] == 0 and c["overflow"] == 0 and c["dropped"] < 1e-4 * c["crossings"] + 5
+    assert c["collisions"] > 0 and c["injected"] > 0
+    n = len(a["particles"][3])
+    assert n == int(a["counts"]["ppc"].sum())

@@ -1,0 +1,74 @@
+"""Host-side logic: synthetic meshes, the CAS format, case constants and the
+seeded workloads (CPU only)."""
+import os
+import tempfile
+
+import numpy as np
+
+import inputs as I
+from pydsmc import case as C
+from pydsmc import mesh as M
+from pydsmc import workload as W
+
+
+def test_block_case_mesh_sizes():
+    raw = M.block_case_mesh(scale=1)
+    assert raw.ncell == 48 * 32 * 32 - 8 ** 3 == 48640
+    dm = M.build_dsmc_mesh(raw)
+    # volumes sum to the box minus the block
+    assert abs(dm.area_sum - (0.5 * 0.5 * 1.0 - (8 / 48) * (8 / 32) * (8 / 32) * 0.5 * 0.5)) < 1e-12
+    # each hex has 6 faces; face normals point from c0 to c1
+    assert np.all(dm.cells["num"] == 6)
+    z = raw.zone
+    assert (z == M.ZONE_WALL).sum() == 6 * 8 * 8
+    assert (z == M.ZONE_INLET).sum() == 32 * 32 and (z == M.ZONE_OUTLET).sum() == 32 * 32
+
+
+def test_normals_point_from_c0_to_c1():
+    raw, dm = I.block_mesh()
+    e = dm.edges
+    c0, c1 = e["faceMap"][:, 4], e["faceMap"][:, 5]
+    inner = c1 < dm.ncell
+    d = dm.cells["cellXY"][c1[inner]] - dm.cells["cellXY"][c0[inner]]
+    assert np.all((d * e["edgeNormal"][inner]).sum(1) > 0)
+    # boundary normals point out of the gas
+    bc = ~inner
+    out = e["edgeCenter"][bc] - dm.cells["cellXY"][c0[bc]]
+    assert np.all((out * e["edgeNormal"][bc]).sum(1) > 0)
+
+
+def test_cas_writer_format():
+    raw, dm = I.block_mesh(scale=8)
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "m.cas")
+        M.write_cas(p, raw)
+        txt = open(p).read()
+    assert txt.count("(13 (") == 1 + 5       # declaration + 5 face zones
+    assert f"(12 (0 1 {raw.ncell:x} 0))" in txt
+    assert "(13 (3 1 " in txt and "(13 (6 " in txt
+
+
+def test_mesh_message_free_constants():
+    raw, dm = I.block_mesh()
+    a = C.mesh_message(dm, 5.0, 0.1, ppc=20, L0=0.125)
+    b = C.mesh_message(dm, 5.0, 0.1, ppc=40, L0=0.125)
+    assert a["Neff"] == 2 * b["Neff"]
+    assert a["dtime"] == 0.2 * dm.min_edge
+    c = C.mesh_message(dm, 5.0, 0.05, ppc=20, L0=0.125)
+    assert c["n_ref"] > a["n_ref"]          # smaller Kn, denser gas
+    assert C.inflow_direction(30.0) == (np.sqrt(3.0) / 2.0, 0.5)
+    assert C.inflow_direction(0.0) == (1.0, 0.0)
+
+
+def test_workload_generators():
+    raw, dm = I.block_mesh()
+    mess = I.block_mess(dm, 20)
+    f = W.initial_fill(dm, mess, 5, 0, C.inflow_direction(30.0))
+    assert f["x"].shape == (5 * dm.ncell, 3)
+    lo = np.array([0.0, 0.0, 0.0])
+    hi = np.array([1.0, 0.5, 0.5])
+    assert np.all(f["x"] >= lo) and np.all(f["x"] <= hi)
+    u, sig, tN = W.freestream(mess, C.inflow_direction(30.0))
+    assert np.allclose(f["v"].mean(0), u, atol=5 * sig / np.sqrt(len(f["v"])))
+    t = W.trace_particles(dm, mess, 1000, 1, C.inflow_direction(30.0))
+    assert t["cell"].min() >= 0 and t["cell"].max() < dm.ncell
