@@ -138,52 +138,58 @@ __device__ __forceinline__ void sample_inflow_velocity(const double* gas, const 
     ir = -log(rs.uniform64()) * tN * 0.5;
 }
 
+// One thread per injected particle; its patch is found by binary search in
+// the exclusive scan of the per-patch counts (slots of one patch are
+// consecutive, so a warp mostly works on one patch).
 template <typename Real>
 __global__ void __launch_bounds__(128) inject_gen_kernel(StepArgs<Real> a)
 {
     const int istep = a.ctl->istep;
     const int nLive = a.ctl->nLive;
+    const int m = a.ctl->nInj;
+    const int np = a.P.npatch;
     TraceCounts cnt{};
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.P.npatch; p += gridDim.x * blockDim.x) {
-        const int np = a.P.count[p];
-        if (np <= 0) continue;
-        const int first = a.P.start[p];
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < m; slot += gridDim.x * blockDim.x) {
+        int lo = 0, hi = np - 1;          // last patch with start <= slot
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.P.start[mid] <= slot) lo = mid; else hi = mid - 1;
+        }
+        const int p = lo;
         const int pcell = a.P.cell[p];
         const int pedge = a.P.edge[p];
         const int ptag = a.P.triTag[p];
         const double* G = a.P.geom + (size_t)p * 9;
         const double* R = a.P.rot + (size_t)p * 9;
         const double* gas = a.P.gas + (size_t)p * 8;
-        for (int k = 0; k < np; ++k) {
-            const int gi = nLive + first + k;
-            Stream rs;
-            rs.init((uint32_t)gi, (uint32_t)istep, kPurposeInject, a.C.seedLo, a.C.seedHi);
-            double u = rs.uniform64(), w = rs.uniform64();
-            if (u + w > 1.0) { u = 1.0 - u; w = 1.0 - w; }
-            double pos[3];
-            // p0 + u e10 + v e20 (src/ProcessDSMC.cpp:2524-2526), unfused
-            for (int d = 0; d < 3; ++d) pos[d] = da(da(G[d], dm(u, G[3 + d])), dm(w, G[6 + d]));
-            double vel[3], irv;
-            sample_inflow_velocity(gas, R, rs, vel, irv, a.errorWord);
-            const double dtl = rs.uniform64() * a.C.dtime;
-            PRegs<Real> pr;
-            int cell = pcell;
-            if constexpr (sizeof(Real) == 8) {
-                for (int d = 0; d < 3; ++d) pr.x[d] = pos[d];
-            } else {
-                const double* cc = a.M.cellCenter + (size_t)cell * 3;
-                for (int d = 0; d < 3; ++d) pr.x[d] = (float)(pos[d] - cc[d]);
-            }
-            for (int d = 0; d < 3; ++d) pr.v[d] = (Real)vel[d];
-            pr.ir = (Real)irv;
-            Real dtleft = (Real)dtl;
-            const int out = trace_particle<Real>(a.M, a.C, pr, cell, pedge, ptag, dtleft, rs, istep,
-                                                 a.wallTally, cnt, false, nullptr);
-            a.A.x[0][gi] = pr.x[0]; a.A.x[1][gi] = pr.x[1]; a.A.x[2][gi] = pr.x[2];
-            a.A.v[0][gi] = pr.v[0]; a.A.v[1][gi] = pr.v[1]; a.A.v[2][gi] = pr.v[2];
-            a.A.ir[gi] = pr.ir;
-            a.A.cell[gi] = (out >= 0) ? cell : -1;
+        const int gi = nLive + slot;
+        Stream rs;
+        rs.init((uint32_t)gi, (uint32_t)istep, kPurposeInject, a.C.seedLo, a.C.seedHi);
+        double u = rs.uniform64(), w = rs.uniform64();
+        if (u + w > 1.0) { u = 1.0 - u; w = 1.0 - w; }
+        double pos[3];
+        // p0 + u e10 + v e20 (src/ProcessDSMC.cpp:2524-2526), unfused
+        for (int d = 0; d < 3; ++d) pos[d] = da(da(G[d], dm(u, G[3 + d])), dm(w, G[6 + d]));
+        double vel[3], irv;
+        sample_inflow_velocity(gas, R, rs, vel, irv, a.errorWord);
+        const double dtl = rs.uniform64() * a.C.dtime;
+        PRegs<Real> pr;
+        int cell = pcell;
+        if constexpr (sizeof(Real) == 8) {
+            for (int d = 0; d < 3; ++d) pr.x[d] = pos[d];
+        } else {
+            const double* cc = a.M.cellCenter + (size_t)cell * 3;
+            for (int d = 0; d < 3; ++d) pr.x[d] = (float)(pos[d] - cc[d]);
         }
+        for (int d = 0; d < 3; ++d) pr.v[d] = (Real)vel[d];
+        pr.ir = (Real)irv;
+        Real dtleft = (Real)dtl;
+        const int out = trace_particle<Real>(a.M, a.C, pr, cell, pedge, ptag, dtleft, rs, istep,
+                                             a.wallTally, cnt, false, nullptr);
+        a.A.x[0][gi] = pr.x[0]; a.A.x[1][gi] = pr.x[1]; a.A.x[2][gi] = pr.x[2];
+        a.A.v[0][gi] = pr.v[0]; a.A.v[1][gi] = pr.v[1]; a.A.v[2][gi] = pr.v[2];
+        a.A.ir[gi] = pr.ir;
+        a.A.cell[gi] = (out >= 0) ? cell : -1;
     }
     flush_counts(a.counters, cnt);
 }
@@ -198,9 +204,7 @@ void launch_inject(const StepArgs<Real>& a, int smCount, cudaStream_t s)
     const int gCount = (a.P.ngroup + 127) / 128;
     inject_count_kernel<<<gCount > 0 ? gCount : 1, 128, 0, s>>>(a.P, a.remInj);
     inject_scan_kernel<<<1, 1024, 0, s>>>(a.P, a.ctl, a.counters);
-    int g = (a.P.npatch + 127) / 128;
-    if (g > smCount * 8) g = smCount * 8;
-    inject_gen_kernel<Real><<<g, 128, 0, s>>>(a);
+    inject_gen_kernel<Real><<<smCount * 8, 128, 0, s>>>(a);
 }
 
 // ===========================================================================
@@ -822,6 +826,12 @@ __global__ void __launch_bounds__(128) cell_kernel(StepArgs<Real> a)
         }
         __syncwarp();
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        pairs += __shfl_xor_sync(kFull, pairs, o);
+        colls += __shfl_xor_sync(kFull, colls, o);
+        big += __shfl_xor_sync(kFull, big, o);
+    }
     if (lane == 0) {
         if (pairs) atomicAdd(a.counters + C_PAIRS, (unsigned long long)pairs);
         if (colls) atomicAdd(a.counters + C_COLLISIONS, (unsigned long long)colls);
@@ -934,6 +944,11 @@ __global__ void __launch_bounds__(256) big_cell_kernel(StepArgs<Real> a)
             if (wid == 0) sample_update<Real>(a, c, mom, istep, MODE == kModePre);
         }
         __syncthreads();
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        pairs += __shfl_xor_sync(kFull, pairs, o);
+        colls += __shfl_xor_sync(kFull, colls, o);
     }
     if (lane == 0) {
         if (pairs) atomicAdd(a.counters + C_PAIRS, (unsigned long long)pairs);

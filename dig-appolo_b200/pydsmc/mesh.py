@@ -348,22 +348,27 @@ def build_dsmc_mesh(raw: RawMesh) -> DsmcMesh:
     c1[bmask] = ncell + np.arange(int(bmask.sum()))
     bc_faces = np.nonzero(bmask)[0]
 
-    # cell2face / cell2cell / sgn in face order (setFaceCellNew, :671-687)
+    # cell2face / cell2cell / sgn in face order (setFaceCellNew, :671-687):
+    # each cell lists its faces in ascending face index
+    f_all = np.arange(nf, dtype=np.int64)
+    inner = c1 < ncell
+    cell_k = np.concatenate([c0, c1[inner]])
+    face_k = np.concatenate([f_all, f_all[inner]])
+    other = np.concatenate([c1, c0[inner]])
+    sg = np.concatenate([np.ones(nf, dtype=np.int64), -np.ones(int(inner.sum()), dtype=np.int64)])
+    order = np.lexsort((face_k, cell_k))
+    cell_k, face_k, other, sg = cell_k[order], face_k[order], other[order], sg[order]
+    tag = np.bincount(cell_k, minlength=ncell).astype(np.int64)
+    first = np.concatenate([[0], np.cumsum(tag)[:-1]])
+    slot = np.arange(cell_k.shape[0]) - first[cell_k]
+    if slot.max(initial=0) >= 6:
+        raise ValueError("a cell has more than 6 faces")
     cell2face = -np.ones((ncell, 6), dtype=np.int32)
     cell2cell = -np.ones((ncell, 6), dtype=np.int32)
     sgn = -np.ones((ncell, 6), dtype=np.int32)
-    tag = np.zeros(ncell, dtype=np.int64)
-    for f in range(nf):
-        a, b = c0[f], c1[f]
-        if b < ncell:
-            cell2cell[b, tag[b]] = a
-            cell2face[b, tag[b]] = f
-            sgn[b, tag[b]] = -1
-            tag[b] += 1
-        cell2cell[a, tag[a]] = b
-        cell2face[a, tag[a]] = f
-        sgn[a, tag[a]] = 1
-        tag[a] += 1
+    cell2face[cell_k, slot] = face_k
+    cell2cell[cell_k, slot] = other
+    sgn[cell_k, slot] = sg
 
     # cell volumes and centroids (:688-723)
     T = tag.astype(np.float64)

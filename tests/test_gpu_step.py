@@ -131,11 +131,15 @@ def test_repeat_graph_and_stagewise_are_bit_identical(block):
         assert np.array_equal(a["local"], other["local"])
 
 
+SPECULAR_ZONES = I.REF_ZONES + [(7, gpu.ROLE_SPECULAR, 0)]
+
+
 def test_mixed_step_runs_and_conserves(block):
+    # specular side planes: nothing leaves except through inlet/outlet faces
     raw, dm, mess = block
     x, v, ir, cell = I.fill_inputs(dm, mess, 20, seed=4)
-    a = _run_gpu(dm, mess, x, v, ir, cell, 20, seed=3, precision=gpu.PRECISION_MIXED)
-    b = _run_gpu(dm, mess, x, v, ir, cell, 20, seed=3, precision=gpu.PRECISION_MIXED)
+    a = _run_gpu(dm, mess, x, v, ir, cell, 20, seed=3, precision=gpu.PRECISION_MIXED, zones=SPECULAR_ZONES)
+    b = _run_gpu(dm, mess, x, v, ir, cell, 20, seed=3, precision=gpu.PRECISION_MIXED, zones=SPECULAR_ZONES)
     for pa, pb in zip(a["particles"], b["particles"]):
         assert np.array_equal(pa, pb)
     c = a["counters"]
