@@ -184,8 +184,15 @@ struct ExitHit {
 // uncached fallback (intersectFallbackCell, :1484-1524) repeats the same
 // products and sums on the same node coordinates, so it cannot find a hit the
 // cached test missed; a miss here is a miss there.
+//
+// entryFace / posTol serve the mixed path only: its positions carry FP32
+// rounding, so a particle sitting on the face it entered through can see
+// that face again at a tiny positive t that the reference, with exact
+// positions, rejects through its 1e-14 cut. Hits on entryFace closer than
+// posTol / |v.n| are therefore treated as on the face (no hit).
 __device__ __forceinline__ ExitHit find_exit_exact(const DevMesh& M, int cell, int crossf, int prevTri,
-                                                   const double x[3], const double v[3])
+                                                   const double x[3], const double v[3],
+                                                   int entryFace = -1, double posTol = 0.0)
 {
     ExitHit h{-2, -1, DBL_MAX};
     const int b = M.triOffset[cell];
@@ -195,8 +202,16 @@ __device__ __forceinline__ ExitHit find_exit_exact(const DevMesh& M, int cell, i
         if (ft.x == crossf) {
             if (ft.y <= 0 || (prevTri != 1 && prevTri != 2) || ft.y == prevTri) continue;
         }
+        const double* T = M.triD + (size_t)k * 9;
         double t = DBL_MAX;
-        if (isect_exact(M.triD + (size_t)k * 9, x, v, t) && t < h.t) {
+        if (isect_exact(T, x, v, t) && t < h.t) {
+            if (ft.x == entryFace) {
+                const double nx = T[4] * T[8] - T[5] * T[7];
+                const double ny = T[5] * T[6] - T[3] * T[8];
+                const double nz = T[3] * T[7] - T[4] * T[6];
+                const double vn = fabs(v[0] * nx + v[1] * ny + v[2] * nz) / sqrt(nx * nx + ny * ny + nz * nz);
+                if (t * vn <= posTol) continue;
+            }
             h.t = t;
             h.face = ft.x;
             h.tri = ft.y;
@@ -224,7 +239,8 @@ struct ExitHitF {
 constexpr float kGuardK = 256.0f * 5.9604645e-8f;   // 256 ulp(1) of FP32
 
 __device__ __forceinline__ ExitHitF find_exit_f32(const DevMesh& M, int cell, int crossf, int prevTri,
-                                                   const float x[3], const float v[3], float vnorm)
+                                                   const float x[3], const float v[3], float vnorm,
+                                                   int entryFace, float posTol)
 {
     ExitHitF h{-2, -1, FLT_MAX, 0.0f, false};
     float second = FLT_MAX, secondErr = 0.0f;
@@ -269,6 +285,8 @@ __device__ __forceinline__ ExitHitF find_exit_f32(const DevMesh& M, int cell, in
         // time error: relative err plus the position-scale term
         const float tErr = err * (fabsf(t) + (fabsf(t0) + fabsf(t1) + fabsf(t2)) / fmaxf(vnorm, 1e-30f));
         if (t < -tErr) continue;                       // certain miss (behind)
+        // on the entry face: |t| <= posTol/|v.n| <= posTol*|e1||e2|/|det|
+        if (face == entryFace && t <= 2.0f * posTol * e12 * fabsf(inv)) continue;
         const bool inside = (u > err) && (u < 1.0f - err) && (w > err) && (u + w < 1.0f - 2.0f * err);
         if (!inside || t <= fmaxf(tErr, 1e-13f)) {
             h.ambiguous = true;
@@ -391,6 +409,7 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
 {
     int ifout = kTraceStay;
     int iter = 0;
+    int entryFace = crossf;   // the face the particle sits on (mixed path)
     while (dtleft > (Real)0) {
         if (iter++ >= C.maxCross) { cnt.lost++; dtleft = 0; return kTraceLost; }
         int face, tri;
@@ -403,7 +422,9 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
             stays = t >= dtleft;
         } else {
             const float vnorm = sqrtf(p.v[0] * p.v[0] + p.v[1] * p.v[1] + p.v[2] * p.v[2]);
-            const ExitHitF h = find_exit_f32(M, cell, crossf, tag, p.x, p.v, vnorm);
+            // absolute uncertainty of the FP32 cell-relative position
+            const float posTol = 64.0f * 5.9604645e-8f * (fabsf(p.x[0]) + fabsf(p.x[1]) + fabsf(p.x[2]));
+            const ExitHitF h = find_exit_f32(M, cell, crossf, tag, p.x, p.v, vnorm, entryFace, posTol);
             bool amb = h.ambiguous;
             if (!amb && h.face != -2 &&
                 fabsf(h.t - dtleft) <= h.terr + 4.8e-7f * (dtleft + (float)C.dtime)) amb = true;
@@ -413,7 +434,7 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
                 const double* cc = M.cellCenter + (size_t)cell * 3;
                 double xa[3] = {cc[0] + (double)p.x[0], cc[1] + (double)p.x[1], cc[2] + (double)p.x[2]};
                 const double va[3] = {(double)p.v[0], (double)p.v[1], (double)p.v[2]};
-                const ExitHit he = find_exit_exact(M, cell, crossf, tag, xa, va);
+                const ExitHit he = find_exit_exact(M, cell, crossf, tag, xa, va, entryFace, (double)posTol);
                 if (he.face == -2 || !isfinite(he.t) || he.t <= 0.0) { cnt.dropped++; dtleft = 0; return kTraceDropped; }
                 face = he.face; tri = he.tri;
                 const double dl = (double)dtleft;
@@ -468,6 +489,7 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
                 p.x[0] += sg * dl.x; p.x[1] += sg * dl.y; p.x[2] += sg * dl.z;
             }
             cell = next;
+            entryFace = face;
         } else if (role == kRoleInlet || role == kRoleOutlet) {
             cnt.removed++;
             dtleft = 0;
@@ -478,6 +500,7 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
             const Real v0 = p.v[0], v1 = p.v[1], v2 = p.v[2], ir0 = p.ir;
             diffuse_reflect<Real>(M, C, ws, tri, p, rng);
             cnt.wall++;
+            entryFace = face;
             if (wallTally && C.wallStats && istep > C.nss) {
                 double* T = wallTally + (size_t)ws * 6;
                 const double a0 = (double)p.v[0], a1 = (double)p.v[1], a2 = (double)p.v[2];
@@ -493,6 +516,7 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
             if constexpr (sizeof(Real) == 8) dtleft = ds(dtleft, t); else dtleft -= t;
             specular_reflect<Real>(M, M.faceWall[face], tri, p);
             cnt.wall++;
+            entryFace = face;
         }
         // kRoleNone: no handler (src/ProcessDSMC.cpp:1826-1827); the next
         // search excludes this face and the particle is dropped.
