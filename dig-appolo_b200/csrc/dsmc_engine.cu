@@ -1277,3 +1277,15 @@ int dsmc_sync(DsmcHandle* h)
 }
 
 }  // extern "C"
+
+// Read-only views of a handle for the no-allocation entry point
+// (dsmc_noalloc.cu).
+namespace dsmc {
+DevMesh engine_mesh(const DsmcHandle* h) { return h->e.M; }
+DevConsts engine_consts(const DsmcHandle* h) { return h->e.C; }
+int engine_precision(const DsmcHandle* h) { return h->e.precision; }
+int engine_device(const DsmcHandle* h) { return h->e.device; }
+cudaStream_t engine_stream(const DsmcHandle* h) { return h->e.stream; }
+unsigned long long* engine_counters(const DsmcHandle* h) { return h->e.counters; }
+void engine_set_error(DsmcHandle* h, const char* msg) { h->e.err = msg; }
+}  // namespace dsmc

@@ -31,6 +31,7 @@ STAGE_ALL = 31
 MACRO_LOCAL, MACRO_RECORD, MACRO_FINAL_RECORD = 0, 1, 2
 
 MAX_ZONES = 16
+NOALLOC_MAX_TRACE = 32768
 
 
 class CaseParams(C.Structure):
@@ -85,6 +86,7 @@ _SIGS = [
     ("dsmc_upload_cell_state", C.c_int, [_P, _P, _P, _P]),
     ("dsmc_get_counters", C.c_int, [_P, _P]),
     ("dsmc_trace", C.c_int, [_P, C.c_int64] + [_P] * 8 + [C.c_int32] + [_P] * 12),
+    ("dsmc_trace_noalloc", C.c_int, [_P, C.c_int64] + [_P] * 8 + [C.c_int32] + [_P] * 12),
     ("dsmc_set_timing", C.c_int, [_P, C.c_int32]),
     ("dsmc_stage_ms", C.c_int, [_P, _P, C.POINTER(C.c_int64), C.c_int32]),
     ("dsmc_stream", C.c_void_p, [_P]),
@@ -292,8 +294,9 @@ class Case:
         self._check(self.lib.dsmc_stage_ms(self.h, _ptr(ms), C.byref(n), int(reset)), "dsmc_stage_ms")
         return ms, int(n.value)
 
-    def trace(self, x, v, dt, cell, stop_at_wall: bool = True):
-        """The move kernel's trace on given particles (dsmc_trace)."""
+    def trace(self, x, v, dt, cell, stop_at_wall: bool = True, noalloc: bool = False):
+        """The move kernel's trace on given particles (dsmc_trace, or
+        dsmc_trace_noalloc with noalloc=True)."""
         x = np.ascontiguousarray(x, dtype=np.float64)
         v = np.ascontiguousarray(v, dtype=np.float64)
         dt = np.ascontiguousarray(dt, dtype=np.float64)
@@ -302,7 +305,9 @@ class Case:
         cols = [np.ascontiguousarray(x[:, k]) for k in range(3)] + [np.ascontiguousarray(v[:, k]) for k in range(3)]
         oi = [np.empty(n, dtype=np.int32) for _ in range(5)]
         of = [np.empty(n) for _ in range(7)]
-        self._check(self.lib.dsmc_trace(self.h, n, *[_ptr(c) for c in cols], _ptr(dt), _ptr(cell), int(stop_at_wall),
-                                        *[_ptr(a) for a in oi], *[_ptr(a) for a in of]), "dsmc_trace")
+        fn = self.lib.dsmc_trace_noalloc if noalloc else self.lib.dsmc_trace
+        self._check(fn(self.h, n, *[_ptr(c) for c in cols], _ptr(dt), _ptr(cell), int(stop_at_wall),
+                       *[_ptr(a) for a in oi], *[_ptr(a) for a in of]),
+                    "dsmc_trace_noalloc" if noalloc else "dsmc_trace")
         return {"cell": oi[0], "ifout": oi[1], "face": oi[2], "tri": oi[3], "ncross": oi[4],
                 "x": np.stack(of[:3], 1), "v": np.stack(of[3:6], 1), "dt": of[6]}

@@ -264,6 +264,32 @@ int dsmc_trace(DsmcHandle* h, int64_t n,
                double* out_px, double* out_py, double* out_pz,
                double* out_vx, double* out_vy, double* out_vz, double* out_dt);
 
+/* Tracing check for callers that cannot allocate device memory: a caller
+ * recording its work into a CUDA graph (allocation is not allowed during a
+ * stream capture), or a solver that reserved the whole device for its own
+ * memory pool, or a coupling loop that forbids allocation after start-up.
+ * Same arguments and results as dsmc_trace, but the host arrays are staged
+ * in one static device array of the library instead of in buffers
+ * allocated per call: no cudaMalloc, cudaFree or other allocation happens in
+ * the call. Limits and caveats:
+ *   - n <= DSMC_NOALLOC_MAX_TRACE particles per call (larger n is rejected
+ *     with DSMC_E_INVALID); the array takes about 7.3 MB on every GPU that
+ *     loads the library, until the process exits.
+ *   - The first call on a device looks up the array's device address (with
+ *     that device current); make that first call before any stream capture.
+ *   - All calls on a device share the array: calls whose work overlaps on the
+ *     GPU (other streams, other host threads) race; serialise them.
+ * No counterpart in the reference: it is an addition of this library. */
+#define DSMC_NOALLOC_MAX_TRACE 32768
+int dsmc_trace_noalloc(DsmcHandle* h, int64_t n,
+                       const double* px, const double* py, const double* pz,
+                       const double* vx, const double* vy, const double* vz,
+                       const double* dt, const int32_t* cell, int32_t stop_at_wall,
+                       int32_t* out_cell, int32_t* out_ifout, int32_t* out_face,
+                       int32_t* out_tri, int32_t* out_ncross,
+                       double* out_px, double* out_py, double* out_pz,
+                       double* out_vx, double* out_vy, double* out_vz, double* out_dt);
+
 /* Stage timing: with on != 0, dsmc_step runs its kernels without a CUDA
  * graph and records CUDA events between the stages; dsmc_stage_ms then
  * returns the device time of [inject, move, sort, collide+sample] summed
