@@ -63,6 +63,13 @@ struct DevMesh {
     const double* cellVolume;    // [ncell]
     const int* cell2cell;        // [ncell*6]
     const signed char* revSlot;  // [ncell*6] slot of this cell in neighbour j's list (or -1)
+    // face planes (cells with convex[c] != 0): records faceOff[c]..faceOff[c+1]
+    const int* faceOff;          // [ncell+1]
+    const int4* faceRec;         // face id, index of its first triangle, node count (3/4)
+    const float4* planeF;        // outward unit normal, offset relative to the cell centre
+    const float4* diagF;         // quads: in-plane normal of the diagonal, offset (relative)
+    const double* planeD;        // [nrec*8] n(3), d, m(3), md, absolute
+    const unsigned char* convex; // [ncell]
 };
 
 struct DevConsts {
@@ -304,6 +311,104 @@ __device__ __forceinline__ ExitHitF find_exit_f32(const DevMesh& M, int cell, in
 }
 
 // ---------------------------------------------------------------------------
+// Plane-based exit search for cells that are convex with planar faces.
+//
+// The exit of a ray from inside a convex cell is the face plane it reaches
+// first among those it moves towards: t_f = (d_f - n_f.x) / (v.n_f) for
+// v.n_f > 0. That takes one dot-product pair per face instead of a full
+// triangle test per triangle. The result is only trusted when it is clear of
+// every tie the triangle tests could resolve differently: a second plane
+// reached within the error bound (edge or vertex), a tiny or negative t, a
+// plane grazed while the particle sits on it, a position outside a face
+// plane, and for quads a hit point within the bound of the split diagonal
+// (which sub-triangle). Otherwise `ambiguous` is set and the caller runs the
+// triangle search. The entry face (crossf) is never the exit: the particle
+// sits on it and moves away from it.
+// ---------------------------------------------------------------------------
+template <typename Real>
+struct PlaneHit {
+    int face;
+    int tri;       // -1 triangle face, 1/2 quad half
+    int triIdx;    // index of that triangle in the cell's triangle list
+    Real t;
+    Real terr;
+    bool ambiguous;
+};
+
+template <typename Real>
+__device__ __forceinline__ PlaneHit<Real> find_exit_planes(const DevMesh& M, int cell, int crossf, const Real x[3],
+                                                           const Real v[3])
+{
+    constexpr Real eps = (sizeof(Real) == 8) ? (Real)1.1102230246251565e-16 : (Real)5.9604645e-8f;
+    constexpr Real K = (sizeof(Real) == 8) ? (Real)64 : (Real)32;
+    PlaneHit<Real> h{-2, -1, -1, (Real)0, (Real)0, false};
+    const Real vnorm = fabs(v[0]) + fabs(v[1]) + fabs(v[2]);
+    const Real xnorm = fabs(x[0]) + fabs(x[1]) + fabs(x[2]);
+    Real best = (sizeof(Real) == 8) ? (Real)DBL_MAX : (Real)FLT_MAX;
+    Real second = best, bestErr = 0, secondErr = 0;
+    int bi = -1;
+    bool amb = false;
+    const int b = M.faceOff[cell];
+    const int e = M.faceOff[cell + 1];
+    for (int k = b; k < e; ++k) {
+        const int4 rec = M.faceRec[k];
+        if (rec.x == crossf) continue;
+        Real nx, ny, nz, d;
+        if constexpr (sizeof(Real) == 8) {
+            const double* pd = M.planeD + (size_t)k * 8;
+            nx = pd[0]; ny = pd[1]; nz = pd[2]; d = pd[3];
+        } else {
+            const float4 pl = M.planeF[k];
+            nx = pl.x; ny = pl.y; nz = pl.z; d = pl.w;
+        }
+        const Real vn = v[0] * nx + v[1] * ny + v[2] * nz;
+        const Real num = d - (x[0] * nx + x[1] * ny + x[2] * nz);
+        const Real dErr = K * eps * (fabs(d) + xnorm);
+        const Real vErr = K * eps * vnorm;
+        if (num < -dErr) amb = true;                    // outside this face plane
+        if (vn <= vErr) {
+            if (vn > -vErr && num <= dErr) amb = true;  // grazing the plane it sits on
+            continue;
+        }
+        const Real t = num / vn;
+        const Real tErr = (dErr + fabs(t) * vErr) / vn;
+        if (t < best) {
+            second = best; secondErr = bestErr;
+            best = t; bestErr = tErr; bi = k;
+        } else if (t < second) {
+            second = t; secondErr = tErr;
+        }
+    }
+    if (bi < 0) { h.ambiguous = true; return h; }
+    if (best <= bestErr) amb = true;
+    if (second - best <= bestErr + secondErr) amb = true;
+    const int4 rec = M.faceRec[bi];
+    h.face = rec.x;
+    h.t = best;
+    h.terr = bestErr;
+    h.tri = -1;
+    h.triIdx = rec.y;
+    if (rec.z == 4) {
+        Real mx, my, mz, md;
+        if constexpr (sizeof(Real) == 8) {
+            const double* pd = M.planeD + (size_t)bi * 8;
+            mx = pd[4]; my = pd[5]; mz = pd[6]; md = pd[7];
+        } else {
+            const float4 dg = M.diagF[bi];
+            mx = dg.x; my = dg.y; mz = dg.z; md = dg.w;
+        }
+        const Real px = x[0] + v[0] * best, py = x[1] + v[1] * best, pz = x[2] + v[2] * best;
+        const Real side = mx * px + my * py + mz * pz - md;
+        const Real sErr = K * eps * (fabs(md) + fabs(px) + fabs(py) + fabs(pz)) + vnorm * bestErr;
+        if (fabs(side) <= sErr) amb = true;
+        h.tri = side > (Real)0 ? 1 : 2;
+        h.triIdx = rec.y + (h.tri == 2 ? 1 : 0);
+    }
+    h.ambiguous = amb;
+    return h;
+}
+
+// ---------------------------------------------------------------------------
 // Particle state in registers and the tracing loop.
 // ---------------------------------------------------------------------------
 template <typename Real>
@@ -410,21 +515,52 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
     int ifout = kTraceStay;
     int iter = 0;
     int entryFace = crossf;   // the face the particle sits on (mixed path)
+    bool afterNone = false;   // the last hit had no handler: use the triangle search
     while (dtleft > (Real)0) {
         if (iter++ >= C.maxCross) { cnt.lost++; dtleft = 0; return kTraceLost; }
         int face, tri;
         Real t;
         bool stays;
         if constexpr (sizeof(Real) == 8) {
-            const ExitHit h = find_exit_exact(M, cell, crossf, tag, p.x, p.v);
-            if (h.face == -2 || !isfinite(h.t) || h.t <= 0.0) { cnt.dropped++; dtleft = 0; return kTraceDropped; }
-            face = h.face; tri = h.tri; t = h.t;
+            bool decided = false;
+            if (M.convex[cell] && !afterNone) {
+                // plane decision, then the reference's exact test on that one
+                // triangle for the bit-exact t; any doubt runs the full search
+                const PlaneHit<double> ph = find_exit_planes<double>(M, cell, crossf, p.x, p.v);
+                double te = DBL_MAX;
+                if (!ph.ambiguous && isect_exact(M.triD + (size_t)ph.triIdx * 9, p.x, p.v, te)) {
+                    face = ph.face; tri = ph.tri; t = te;
+                    decided = true;
+                    // the other half of a quad entry face stays eligible in
+                    // the reference's skip rule (src/ProcessDSMC.cpp:1229-1233)
+                    if (crossf >= 0 && (tag == 1 || tag == 2)) {
+                        const int b0 = M.triOffset[cell], e0 = M.triOffset[cell + 1];
+                        for (int k = b0; k < e0; ++k) {
+                            const int2 ft = M.triFT[k];
+                            if (ft.x != crossf || ft.y == tag || ft.y <= 0) continue;
+                            double t2 = DBL_MAX;
+                            if (isect_exact(M.triD + (size_t)k * 9, p.x, p.v, t2) && t2 < t) decided = false;
+                        }
+                    }
+                }
+            }
+            if (!decided) {
+                const ExitHit h = find_exit_exact(M, cell, crossf, tag, p.x, p.v);
+                if (h.face == -2 || !isfinite(h.t) || h.t <= 0.0) { cnt.dropped++; dtleft = 0; return kTraceDropped; }
+                face = h.face; tri = h.tri; t = h.t;
+            }
             stays = t >= dtleft;
         } else {
             const float vnorm = sqrtf(p.v[0] * p.v[0] + p.v[1] * p.v[1] + p.v[2] * p.v[2]);
             // absolute uncertainty of the FP32 cell-relative position
             const float posTol = 64.0f * 5.9604645e-8f * (fabsf(p.x[0]) + fabsf(p.x[1]) + fabsf(p.x[2]));
-            const ExitHitF h = find_exit_f32(M, cell, crossf, tag, p.x, p.v, vnorm, entryFace, posTol);
+            ExitHitF h;
+            if (M.convex[cell] && !afterNone) {
+                const PlaneHit<float> ph = find_exit_planes<float>(M, cell, crossf, p.x, p.v);
+                h = ExitHitF{ph.face, ph.tri, ph.t, ph.terr, ph.ambiguous};
+            } else {
+                h = find_exit_f32(M, cell, crossf, tag, p.x, p.v, vnorm, entryFace, posTol);
+            }
             bool amb = h.ambiguous;
             if (!amb && h.face != -2 &&
                 fabsf(h.t - dtleft) <= h.terr + 4.8e-7f * (dtleft + (float)C.dtime)) amb = true;
@@ -520,6 +656,7 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
         }
         // kRoleNone: no handler (src/ProcessDSMC.cpp:1826-1827); the next
         // search excludes this face and the particle is dropped.
+        afterNone = (role == kRoleNone);
     }
     return ifout;
 }

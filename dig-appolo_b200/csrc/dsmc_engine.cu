@@ -100,7 +100,7 @@ struct Engine {
     int precision = DSMC_PRECISION_FP64;
     DsmcCaseParams params{};
     DsmcMeshMessage mess{};
-    int ncell = 0, nface = 0, npoint = 0, ntri = 0, nwall = 0;
+    int ncell = 0, nface = 0, npoint = 0, ntri = 0, nwall = 0, nconvex = 0;
     std::vector<DsmcCellRec> cells;
     std::vector<DsmcEdgeRec> edges;
     std::vector<double> points;
@@ -324,6 +324,113 @@ struct Engine {
         triOffset[(size_t)ncell] = (int)triFT.size();
         ntri = (int)triFT.size();
 
+        // --- face planes for the plane-based exit search: per cell, its faces
+        //     in cell2face order with outward unit normal and offset, the
+        //     quad diagonal side test, and a flag for cells that are convex
+        //     with planar faces (only those take the plane path)
+        std::vector<int> faceOff((size_t)ncell + 1, 0);
+        std::vector<int4> faceRec;
+        std::vector<float4> planeF, diagF;
+        std::vector<double> planeD;
+        std::vector<unsigned char> convex((size_t)ncell, 0);
+        for (int lc = 0; lc < ncell; ++lc) {
+            faceOff[(size_t)lc] = (int)faceRec.size();
+            const DsmcCellRec& cl = cells[(size_t)lc];
+            const double* cc = &cellCenterHost[(size_t)lc * 3];
+            bool ok = cl.num > 0 && cl.num <= 6;
+            int triIdx = triOffset[(size_t)lc];
+            std::vector<double> cellNodes;
+            for (int m = 0; m < cl.num && m < 6 && ok; ++m) {
+                const int f = cl.cell2face[m];
+                if (f < 0 || f >= nface) { ok = false; break; }
+                const DsmcEdgeRec& e = edges[(size_t)f];
+                for (int q = 0; q < e.faceType && q < 4; ++q) {
+                    double P3[3];
+                    if (!loadPoint(e.faceMap[q], P3)) { ok = false; break; }
+                    cellNodes.insert(cellNodes.end(), P3, P3 + 3);
+                }
+            }
+            double Lc = 0.0;
+            for (size_t q = 0; q + 2 < cellNodes.size(); q += 3)
+                for (int d = 0; d < 3; ++d) Lc = std::max(Lc, std::fabs(cellNodes[q + d] - cc[d]));
+            for (int m = 0; m < cl.num && m < 6 && ok; ++m) {
+                const int f = cl.cell2face[m];
+                const DsmcEdgeRec& e = edges[(size_t)f];
+                const int type = e.faceType;
+                if (type != 3 && type != 4) { ok = false; break; }
+                double Pn[4][3];
+                for (int q = 0; q < type; ++q) loadPoint(e.faceMap[q], Pn[q]);
+                int t0[3] = {0, 1, 2}, t1[3] = {0, 2, 3};
+                if (type == 4) {
+                    decode_split(split[(size_t)f], t0, t1);
+                    if (t0[0] < 0 || t1[0] < 0) decode_split(kSplit02, t0, t1);
+                }
+                const double* A = Pn[t0[0]];
+                const double a1[3] = {Pn[t0[1]][0] - A[0], Pn[t0[1]][1] - A[1], Pn[t0[1]][2] - A[2]};
+                const double a2[3] = {Pn[t0[2]][0] - A[0], Pn[t0[2]][1] - A[1], Pn[t0[2]][2] - A[2]};
+                double n[3];
+                cross3(a1, a2, n);
+                const double nl = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+                if (!(nl > 0.0)) { ok = false; break; }
+                for (int d = 0; d < 3; ++d) n[d] /= nl;
+                double fc[3] = {0, 0, 0};
+                for (int q = 0; q < type; ++q)
+                    for (int d = 0; d < 3; ++d) fc[d] += Pn[q][d] / type;
+                if ((fc[0] - cc[0]) * n[0] + (fc[1] - cc[1]) * n[1] + (fc[2] - cc[2]) * n[2] < 0.0)
+                    for (double& x : n) x = -x;
+                const double dAbs = n[0] * A[0] + n[1] * A[1] + n[2] * A[2];
+                // planarity and convexity (every node of the cell on the inner side)
+                const double tol = 1e-9 * std::max(Lc, 1e-300);
+                for (int q = 0; q < type && ok; ++q)
+                    if (std::fabs(n[0] * Pn[q][0] + n[1] * Pn[q][1] + n[2] * Pn[q][2] - dAbs) > tol) ok = false;
+                for (size_t q = 0; q + 2 < cellNodes.size() && ok; q += 3)
+                    if (n[0] * cellNodes[q] + n[1] * cellNodes[q + 1] + n[2] * cellNodes[q + 2] - dAbs > tol) ok = false;
+                double mv[3] = {0, 0, 0}, md = 0.0;
+                if (type == 4) {
+                    // diagonal of the split and the in-plane normal to it,
+                    // oriented so that the first triangle's side is positive
+                    const int dA = t0[0] == t1[0] ? t0[0] : t1[0];   // split 02: 0; split 13: 1
+                    const int dB = t0[0] == t1[0] ? t0[2] : t1[2];   // split 02: 2; split 13: 3
+                    const double dv[3] = {Pn[dB][0] - Pn[dA][0], Pn[dB][1] - Pn[dA][1], Pn[dB][2] - Pn[dA][2]};
+                    cross3(n, dv, mv);
+                    const double ml = std::sqrt(mv[0] * mv[0] + mv[1] * mv[1] + mv[2] * mv[2]);
+                    if (!(ml > 0.0)) { ok = false; break; }
+                    for (double& x : mv) x /= ml;
+                    int only0 = -1;   // a node of the first triangle off the diagonal
+                    for (int q = 0; q < 3; ++q)
+                        if (t0[q] != dA && t0[q] != dB) only0 = t0[q];
+                    const double* Q = Pn[only0];
+                    if (mv[0] * (Q[0] - Pn[dA][0]) + mv[1] * (Q[1] - Pn[dA][1]) + mv[2] * (Q[2] - Pn[dA][2]) < 0.0)
+                        for (double& x : mv) x = -x;
+                    md = mv[0] * Pn[dA][0] + mv[1] * Pn[dA][1] + mv[2] * Pn[dA][2];
+                }
+                faceRec.push_back(make_int4(f, triIdx, type, 0));
+                triIdx += (type == 4) ? 2 : 1;
+                const double dRel = n[0] * (A[0] - cc[0]) + n[1] * (A[1] - cc[1]) + n[2] * (A[2] - cc[2]);
+                double mdRel = 0.0;
+                if (type == 4) {
+                    const double mcc = mv[0] * cc[0] + mv[1] * cc[1] + mv[2] * cc[2];
+                    mdRel = md - mcc;
+                }
+                planeF.push_back(make_float4((float)n[0], (float)n[1], (float)n[2], (float)dRel));
+                diagF.push_back(make_float4((float)mv[0], (float)mv[1], (float)mv[2], (float)mdRel));
+                const double rec[8] = {n[0], n[1], n[2], dAbs, mv[0], mv[1], mv[2], md};
+                planeD.insert(planeD.end(), rec, rec + 8);
+            }
+            if (ok && triIdx != triOffset[(size_t)lc + 1]) ok = false;
+            if (!ok) {
+                // the tri path serves this cell; drop any partial records
+                faceRec.resize((size_t)faceOff[(size_t)lc]);
+                planeF.resize((size_t)faceOff[(size_t)lc]);
+                diagF.resize((size_t)faceOff[(size_t)lc]);
+                planeD.resize((size_t)faceOff[(size_t)lc] * 8);
+            }
+            convex[(size_t)lc] = ok ? 1 : 0;
+        }
+        faceOff[(size_t)ncell] = (int)faceRec.size();
+        nconvex = 0;
+        for (unsigned char c : convex) nconvex += c;
+
         // --- wall / specular slots and rotations (getWallNormal +
         //     processFacesQuadNormals + buildRotationMatrix)
         auto quadNormals = [&](int fid, double n1[3], double n2[3]) -> bool {
@@ -444,6 +551,12 @@ struct Engine {
         int* dTriOffset; double* dTriD; int2* dTriFT; float4* dTriF; unsigned char* dRole; int2* dFaceCells;
         float4* dDelta; int* dFaceWall; double* dWallRot; float* dWallRotF; double* dCenter; double* dVol;
         int* dC2c; signed char* dRev;
+        int *dFaceOff; int4* dFaceRec; float4 *dPlaneF, *dDiagF; double* dPlaneD; unsigned char* dConvex;
+        if (!upload(dFaceOff, faceOff) || !upload(dFaceRec, faceRec) || !upload(dPlaneF, planeF) ||
+            !upload(dDiagF, diagF) || !upload(dPlaneD, planeD) || !upload(dConvex, convex))
+            return false;
+        M.faceOff = dFaceOff; M.faceRec = dFaceRec; M.planeF = dPlaneF; M.diagF = dDiagF; M.planeD = dPlaneD;
+        M.convex = dConvex;
         if (!upload(dTriOffset, triOffset) || !upload(dTriD, triD) || !upload(dTriFT, triFT) || !upload(dTriF, triF) ||
             !upload(dRole, roleU8) || !upload(dFaceCells, faceCells) || !upload(dDelta, faceDelta) ||
             !upload(dFaceWall, faceWallHost) || !upload(dWallRot, wallRot) || !upload(dWallRotF, wallRotF) ||

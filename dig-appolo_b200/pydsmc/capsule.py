@@ -89,7 +89,8 @@ def _lattice(lo, hi, h, rng, jitter=0.2):
     return P
 
 
-def capsule_mesh(h_fine: float = 0.215, h_coarse: float = 0.62, seed: int = 0, aoa_deg: float = 30.0) -> RawMesh:
+def capsule_mesh(h_fine: float = 0.215, h_coarse: float = 0.60, seed: int = 0, aoa_deg: float = 30.0,
+                 r_fine: float = 4.2) -> RawMesh:
     from scipy.spatial import Delaunay
 
     rng = np.random.default_rng(seed)
@@ -97,7 +98,6 @@ def capsule_mesh(h_fine: float = 0.215, h_coarse: float = 0.62, seed: int = 0, a
     box_hi = np.array([6 * L0, 4 * L0, 4 * L0])
     shape = CapsuleShape(x0=2.0 * L0, yc=2.0 * L0, zc=2.0 * L0)
     body_c = np.array([shape.x0 + 0.5 * (shape.cap_depth + shape.cone_len), shape.yc, shape.zc])
-    r_fine = 4.2
     coarse = _lattice(box_lo, box_hi, h_coarse, rng)
     flo = np.maximum(box_lo, body_c - r_fine)
     fhi = np.minimum(box_hi, body_c + r_fine)

@@ -413,7 +413,8 @@ def build_dsmc_mesh(raw: RawMesh) -> DsmcMesh:
         a, b = P[p1], P[p2]
         dd = np.sqrt((a[:, 0] - b[:, 0]) * (a[:, 0] - b[:, 0]) + (a[:, 1] - b[:, 1]) * (a[:, 1] - b[:, 1])
                      + (a[:, 2] - b[:, 2]) * (a[:, 2] - b[:, 2]))
-        mins.append(dd.min())
+        if dd.size:
+            mins.append(dd.min())
     min_edge = float(min(mins))
 
     cells = np.zeros(ncell, dtype=DSMC_CELL_DTYPE)

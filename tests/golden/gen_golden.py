@@ -14,6 +14,8 @@ outputs:
   inflow_pin.npz per-cell inflow remainders after 60 full steps
   stats_band.npz time-averaged rho, u, T, Tr per cell over steps 101-200 of
                  8 independently seeded reference runs (20 per cell)
+  tet_trace_pin.npz tracing-check outputs on the coarse capsule tet mesh
+                 (16,000 particles, stop at the first wall hit)
 
 Usage: python tests/golden/gen_golden.py
 """
@@ -103,6 +105,19 @@ def main():
         # remainders after 60 steps
         r60 = H.run(cas, mess, xs, vs, irs, cs, 60, 5, "-", 61)
         np.savez_compressed(os.path.join(HERE, "inflow_pin.npz"), reminj=r60["reminj"], steps=60)
+
+        # -- tetrahedral trace pin (coarse capsule)
+        rawc, dmc, messc = I.capsule_small()
+        casc = os.path.join(d, "cap.cas")
+        M.write_cas(casc, rawc)
+        refc = H.dump_mesh(casc, 5.0, 0.01, M.DSMC_CELL_DTYPE, M.DSMC_EDGE_DTYPE, C.MESH_MESSAGE_DTYPE)
+        for f in M.DSMC_EDGE_DTYPE.names:
+            if not np.array_equal(refc["edges"][f], dmc.edges[f]):
+                raise SystemExit(f"capsule mesh differs from the reference's parse in edges.{f}")
+        xt, vt, dtt, ct = I.tet_trace_inputs(dmc, messc, TRACE_N, seed=4)
+        r = H.trace(casc, messc, xt, vt, dtt, ct, True)
+        np.savez_compressed(os.path.join(HERE, "tet_trace_pin.npz"), ncell=dmc.ncell,
+                            **{k: r[k] for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt")})
     print("fixtures written to", HERE)
 
 

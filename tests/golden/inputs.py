@@ -91,6 +91,41 @@ def fill_inputs(dm, mess, ppc: int, seed: int):
     return x, v, ir, cells
 
 
+# the capsule case, coarse: a tetrahedral test mesh (10,729 tets)
+CAPSULE_SMALL = dict(h_fine=0.7, h_coarse=2.0, r_fine=4.2, seed=0)
+
+
+def capsule_small():
+    from pydsmc import capsule
+    raw = capsule.capsule_mesh(**CAPSULE_SMALL)
+    dm = M.build_dsmc_mesh(raw)
+    mess = C.mesh_message(dm, 5.0, 0.01, ppc=20, L0=capsule.L0)
+    return raw, dm, mess
+
+
+def tet_trace_inputs(dm, mess, n: int, seed: int):
+    """Uniform random tetrahedra, uniform barycentric positions, isotropic
+    velocities with mean speed 3x the freestream speed, one dt."""
+    rs = np.random.RandomState(seed)
+    cells = rs.randint(0, dm.ncell, size=n).astype(np.int32)
+    P = dm.points.reshape(-1, 3)
+    fm = dm.edges["faceMap"]
+    f = dm.cells["cell2face"][cells, :2]
+    a = fm[f[:, 0], :3]
+    b = fm[f[:, 1], :3]
+    in_a = (b[:, :, None] == a[:, None, :]).any(-1)
+    extra = np.where(~in_a, b, -1).max(axis=1)
+    verts = np.concatenate([a, extra[:, None]], axis=1)
+    w = -np.log(rs.random_sample((n, 4)))
+    w /= w.sum(1, keepdims=True)
+    x = np.einsum("nk,nkd->nd", w, P[verts])
+    u, _, _ = freestream(mess)
+    sigma = 3.0 * float(np.linalg.norm(u)) / math.sqrt(8.0 / math.pi)
+    v = sigma * rs.standard_normal((n, 3))
+    dt = np.full(n, float(mess["dtime"]))
+    return x, v, dt, cells
+
+
 def fields_from_moments(mom_sum: np.ndarray, nsteps: int, dm, mess) -> np.ndarray:
     """Time-averaged rho (per step), u (3), T and Tr from summed raw moments."""
     N = mom_sum[:, 0]

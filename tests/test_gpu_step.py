@@ -147,3 +147,23 @@ def test_mixed_step_runs_and_conserves(block):
     assert c["collisions"] > 0 and c["injected"] > 0
     n = len(a["particles"][3])
     assert n == int(a["counts"]["ppc"].sum())
+
+
+def test_fp64_tet_step_matches_oracle():
+    raw, dm, mess = I.capsule_small()
+    from pydsmc import workload as W
+    fill = W.initial_fill(dm, mess, 20, 5, I.inflow_dir())
+    x, v, ir, cell = fill["x"], fill["v"], fill["ir"], fill["cell"]
+    g = _run_gpu(dm, mess, x, v, ir, cell, 2, seed=13)
+    o = make_oracle(dm, mess, seed=13)
+    o.set_particles(x, v, ir, cell)
+    o.macro_pre()
+    for s in range(1, 3):
+        o.step(s)
+    xo, vo, iro, co = o.particles()
+    xg, vg, irg, cg = g["particles"]
+    assert np.array_equal(cg, co)
+    for a, b in ((xg, xo), (vg, vo), (irg, iro)):
+        assert rel_close(a, b, 1e-9, 1e-12).mean() >= 0.999
+    assert np.array_equal(g["cell_state"][2], o.cell_state()[2])
+    assert rel_close(g["moments"], o.step_moments(), 1e-9, 1e-9).mean() >= 0.999

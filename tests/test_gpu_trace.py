@@ -68,3 +68,39 @@ def test_mixed_trace_matches_fp64(block):
     # positions agree to FP32 rounding relative to the cell size
     assert np.max(np.abs(r["x"][same] - ro["x"][same])) < 1e-4
     assert c["fp64_fallbacks"] > 0
+
+
+@pytest.fixture(scope="module")
+def capsule_small():
+    return I.capsule_small()
+
+
+def test_fp64_tet_trace_bit_exact_vs_reference(capsule_small):
+    raw, dm, mess = capsule_small
+    g = golden("tet_trace_pin.npz")
+    x, v, dt, cell = I.tet_trace_inputs(dm, mess, len(g["cell"]), seed=4)
+    with make_case(dm, mess) as case:
+        r = case.trace(x, v, dt, cell, stop_at_wall=True)
+    for k in ("cell", "ifout", "face", "tri", "ncross"):
+        assert np.array_equal(r[k], g[k]), k
+    assert np.array_equal(r["x"], g["x"])
+    assert np.array_equal(r["dt"], g["dt"])
+
+
+def test_tet_trace_large_fp64_exact_mixed_close(capsule_small):
+    raw, dm, mess = capsule_small
+    x, v, dt, cell = I.tet_trace_inputs(dm, mess, 200_000, seed=9)
+    cc = dm.cells["cellXY"][cell]
+    x32 = cc + (x - cc).astype(np.float32).astype(np.float64)
+    v32 = v.astype(np.float32).astype(np.float64)
+    o = make_oracle(dm, mess)
+    ro = o.trace(x32, v32, dt, cell, stop_at_wall=True)
+    with make_case(dm, mess) as case:
+        r64 = case.trace(x32, v32, dt, cell, stop_at_wall=True)
+    for k in ("cell", "ifout", "face", "tri", "ncross"):
+        assert np.array_equal(r64[k], ro[k]), k
+    assert np.array_equal(r64["x"], ro["x"])
+    with make_case(dm, mess, precision=gpu.PRECISION_MIXED) as case:
+        r = case.trace(x32, v32, dt, cell, stop_at_wall=True)
+    assert np.mean(r["cell"] != ro["cell"]) <= 1e-4
+    assert np.mean(r["face"] != ro["face"]) <= 1e-4

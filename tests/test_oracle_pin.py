@@ -131,3 +131,17 @@ def test_oracle_statistics_within_reference_band(block, oracle_lib):
     ref_n = g["nparticles"].astype(float)
     lo, hi = ref_n.min(0) * 0.97, ref_n.max(0) * 1.03
     assert np.all((np.array(counts) >= lo) & (np.array(counts) <= hi))
+
+
+def test_oracle_tet_trace_bit_exact_vs_reference(oracle_lib):
+    g = golden("tet_trace_pin.npz")
+    raw, dm, mess = I.capsule_small()
+    assert dm.ncell == int(g["ncell"])
+    x, v, dt, cell = I.tet_trace_inputs(dm, mess, len(g["cell"]), seed=4)
+    o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir()))
+    r = o.trace(x, v, dt, cell, stop_at_wall=True)
+    for k in ("cell", "ifout", "face", "tri", "ncross"):
+        assert np.array_equal(r[k], g[k]), k
+    assert np.array_equal(r["x"], g["x"])
+    assert np.array_equal(r["dt"], g["dt"])
+    assert (g["face"] >= 0).sum() > 50      # wall and farfield hits are covered
