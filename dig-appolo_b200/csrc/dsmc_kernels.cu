@@ -9,11 +9,13 @@
 //            counting sort. rank (warp per source cell: arrival slot and rank
 //            from warp ballots; multi-hop and injected arrivals through
 //            warp-aggregated atomics), scan, scatter of source indices.
-//   cells    warp per destination cell: gather into the sorted buffer,
-//            canonical order, NTC collisions (collisionDSMC,
-//            src/ProcessDSMC.cpp:2621-2744) with pairs run in parallel
-//            waves that keep the sequential result, and the 18-moment
-//            sampling (statistic_macro, src/ProcessDSMC.cpp:2757-2861).
+//   cells    a warp per 32 destination cells: gather into the sorted
+//            buffer in canonical order, NTC collisions (collisionDSMC,
+//            src/ProcessDSMC.cpp:2621-2744) one cell per lane with the
+//            pairs in sequence, and the 18-moment sampling
+//            (statistic_macro, src/ProcessDSMC.cpp:2757-2861).
+#include <climits>
+
 #include "dsmc_kernels.cuh"
 #include "dsmc_macro.cuh"
 
@@ -21,9 +23,6 @@ namespace dsmc {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-template <typename Real> struct CellCap;
-template <> struct CellCap<float> { static constexpr int value = 512; };
-template <> struct CellCap<double> { static constexpr int value = 288; };
 
 // ===========================================================================
 // inject
@@ -500,6 +499,11 @@ __device__ __forceinline__ double collision_diameter(double cr, double prefactor
     return cr * prefactor * pow(1.0 / cr2, eta);
 }
 
+// Division: IEEE in FP64 (the oracle's rounding), the fast reciprocal form
+// in the FP32 path (operands here are far from the range limits).
+__device__ __forceinline__ double qdiv(double x, double y) { return x / y; }
+__device__ __forceinline__ float qdiv(float x, float y) { return __fdividef(x, y); }
+
 // collisionVelocity, src/ProcessDSMC.cpp:2679-2744, on one candidate pair.
 template <typename Real>
 __device__ __forceinline__ void collide_pair(Real* vx, Real* vy, Real* vz, Real* ir, int k1, int k2, Stream& rs,
@@ -549,11 +553,11 @@ __device__ __forceinline__ void collide_pair(Real* vx, Real* vy, Real* vz, Real*
     if constexpr (sizeof(Real) == 8) sincospi(2.0 * th, &sth, &cth); else sincospif(2.0f * th, &sth, &cth);
     const Real vrp = sqrt(vr1 * vr1 + vr2 * vr2);
     const Real tiny = (sizeof(Real) == 8) ? (Real)1.0e-300 : (Real)1.0e-30f;
-    const Real scale = postVr / (cr > tiny ? cr : tiny);
+    const Real scale = qdiv(postVr, cr > tiny ? cr : tiny);
     const Real vrpc = vrp > tiny ? vrp : tiny;
     Real ref1 = scale * (cosChi * vr0 + sinChi * sth * vrp);
-    Real ref2 = scale * (cosChi * vr1 + sinChi * (cr * vr2 * cth - vr0 * vr1 * sth) / vrpc);
-    Real ref3 = scale * (cosChi * vr2 - sinChi * (cr * vr1 * cth + vr0 * vr2 * sth) / vrpc);
+    Real ref2 = scale * (cosChi * vr1 + qdiv(sinChi * (cr * vr2 * cth - vr0 * vr1 * sth), vrpc));
+    Real ref3 = scale * (cosChi * vr2 - qdiv(sinChi * (cr * vr1 * cth + vr0 * vr2 * sth), vrpc));
     if (vrp < (Real)1e-6) {
         ref1 = scale * cosChi * vr0;
         ref2 = scale * sinChi * vr0 * cth;
@@ -565,11 +569,19 @@ __device__ __forceinline__ void collide_pair(Real* vx, Real* vy, Real* vz, Real*
 }
 
 // NTC collisions of one cell by one warp (collisionDSMC,
-// src/ProcessDSMC.cpp:2631-2665). Candidate pairs are drawn from a stream
-// keyed by (cell, step, pair index). Pairs run in waves: a pair goes once it
-// is the lowest unfinished pair of the batch on both its particles, so every
-// particle sees its pairs in pair order and the result equals processing the
-// pairs one after another. claim == nullptr runs them one at a time.
+// src/ProcessDSMC.cpp:2631-2665): the pair count from the majorant with the
+// carried remainder, then candidate pairs j = 0, 1, ... each drawn from a
+// Philox stream keyed by (cell, step, j).
+//
+// The pairs run as a sliding window: every lane holds one pending pair and
+// claims both its particles with the pair index (atomicMin); a pair whose
+// index is the lowest claim on both particles goes, and its lane takes the
+// next unassigned pair. Pairs are handed out in increasing order, so a pair
+// goes only after every lower pair that shares a particle with it, and the
+// result equals running the pairs one after another. The lowest pending
+// pair always goes, so the loop ends after at most npairs rounds.
+// claim holds n ints (shared memory, or the output buffer's cell-id slots
+// of the cell for large cells; the caller restores those).
 template <typename Real>
 __device__ void collide_cell(Real* vx, Real* vy, Real* vz, Real* ir, int* claim, int n, int c,
                              const StepArgs<Real>& a, int istep, uint32_t& pairsOut, uint32_t& collOut)
@@ -591,48 +603,43 @@ __device__ void collide_cell(Real* vx, Real* vy, Real* vz, Real* ir, int* claim,
     consCrm = __shfl_sync(kFull, consCrm, 0);
     crm0 = __shfl_sync(kFull, crm0, 0);
     if (!(consCrm > 0.0) || npairs <= 0) return;
+    for (int k = lane; k < n; k += 32) claim[k] = INT_MAX;
+    __syncwarp();
     Real crmLocal = (Real)0;
     const Real crm0r = (Real)crm0;
-    if (claim) {
-        for (int k = lane; k < n; k += 32) claim[k] = 64;
+    const unsigned below = (1u << lane) - 1u;
+    int next = 0;     // first pair not yet handed out (same in every lane)
+    int j = -1;       // this lane's pending pair
+    int k1 = 0, k2 = 0;
+    Stream rs;
+    for (;;) {
+        const unsigned idle = __ballot_sync(kFull, j < 0);
+        if (j < 0) {
+            const int jj = next + __popc(idle & below);
+            if (jj < npairs) {
+                j = jj;
+                rs.init((uint32_t)c, (uint32_t)istep, kPurposeCollide | ((uint32_t)j << 4), a.C.seedLo, a.C.seedHi);
+                k1 = (int)__umulhi(rs.next32(), (uint32_t)n);
+                k2 = k1 + 1 + (int)__umulhi(rs.next32(), (uint32_t)(n - 1));
+                if (k2 >= n) k2 -= n;
+            }
+        }
+        next = min(npairs, next + __popc(idle));
+        if (__ballot_sync(kFull, j >= 0) == 0u) break;
+        if (j >= 0) {
+            atomicMin(&claim[k1], j);
+            atomicMin(&claim[k2], j);
+        }
         __syncwarp();
-    }
-    for (int base = 0; base < npairs; base += 32) {
-        const int j = base + lane;
-        const bool active = j < npairs;
-        int k1 = 0, k2 = 0;
-        Stream rs;
-        rs.init((uint32_t)c, (uint32_t)istep, kPurposeCollide | ((uint32_t)j << 4), a.C.seedLo, a.C.seedHi);
-        if (active) {
-            k1 = (int)__umulhi(rs.next32(), (uint32_t)n);
-            k2 = k1 + 1 + (int)__umulhi(rs.next32(), (uint32_t)(n - 1));
-            if (k2 >= n) k2 -= n;
+        const bool go = j >= 0 && claim[k1] == j && claim[k2] == j;
+        __syncwarp();
+        if (go) {
+            collide_pair<Real>(vx, vy, vz, ir, k1, k2, rs, a.C, consCrm, crm0r, crmLocal, collOut);
+            claim[k1] = INT_MAX;
+            claim[k2] = INT_MAX;
+            j = -1;
         }
-        if (!claim) {
-            for (int l = 0; l < 32; ++l) {
-                if (lane == l && active) collide_pair<Real>(vx, vy, vz, ir, k1, k2, rs, a.C, consCrm, crm0r, crmLocal, collOut);
-                __syncwarp();
-            }
-            continue;
-        }
-        bool done = !active;
-        for (int round = 0; round < 40; ++round) {
-            if (__all_sync(kFull, done)) break;
-            if (!done) {
-                atomicMin(&claim[k1], lane);
-                atomicMin(&claim[k2], lane);
-            }
-            __syncwarp();
-            const bool go = !done && claim[k1] == lane && claim[k2] == lane;
-            __syncwarp();
-            if (go) {
-                collide_pair<Real>(vx, vy, vz, ir, k1, k2, rs, a.C, consCrm, crm0r, crmLocal, collOut);
-                claim[k1] = 64;
-                claim[k2] = 64;
-                done = true;
-            }
-            __syncwarp();
-        }
+        __syncwarp();
     }
     Real m = crmLocal;
 #pragma unroll
@@ -641,6 +648,31 @@ __device__ void collide_cell(Real* vx, Real* vy, Real* vz, Real* ir, int* claim,
         m = y > m ? y : m;
     }
     if (lane == 0 && (double)m > crm0) a.crmax[c] = (double)m;
+}
+
+// Canonical order of a cell's far-slot arrivals: ascending source index.
+// tmp is a scratch range of the same length (the output buffer's cell ids
+// at those positions, written later by the gather).
+__device__ void sort_far(int* seg, int m, int* tmp)
+{
+    const int lane = threadIdx.x & 31;
+    if (m <= 1) return;
+    if (m <= 32) {
+        sort_far_warp<1>(seg, m);
+    } else if (m <= 512) {
+        sort_far_warp<16>(seg, m);
+    } else {
+        // rank counting: O(m^2 / 32), for the rare very large far segments
+        for (int e = lane; e < m; e += 32) tmp[e] = seg[e];
+        __syncwarp();
+        for (int e = lane; e < m; e += 32) {
+            const int v = tmp[e];
+            int r = 0;
+            for (int f = 0; f < m; ++f) r += tmp[f] < v;
+            seg[r] = v;
+        }
+        __syncwarp();
+    }
 }
 
 template <typename Real>
@@ -741,51 +773,52 @@ __device__ void sample_update(const StepArgs<Real>& a, int c, const double* mom,
     if (clear && lane < 18) acc[36 + lane] = 0.0;
 }
 
+// The cell pass, one warp per cell: gather the cell's particles into the
+// sorted output buffer in canonical order, run its collisions, sample it.
+// Up to kStage particles of a cell keep their velocities and internal
+// energies in shared memory from the gather to the write-back, so the
+// collision rounds touch no global memory.
+constexpr int kCellWarps = 4;
+constexpr int kStage = 512;
+
 template <typename Real>
-struct WarpSmem {
-    Real vx[CellCap<Real>::value];
-    Real vy[CellCap<Real>::value];
-    Real vz[CellCap<Real>::value];
-    Real ir[CellCap<Real>::value];
-    int claim[CellCap<Real>::value];
-    double mom[18];
-};
+constexpr size_t cell_smem_bytes()
+{
+    return (size_t)kCellWarps * kStage * (4 * sizeof(Real) + sizeof(int));
+}
 
 template <typename Real, int MODE>
-__global__ void __launch_bounds__(128) cell_kernel(StepArgs<Real> a)
+__global__ void __launch_bounds__(kCellWarps * 32) cell_kernel(StepArgs<Real> a)
 {
-    constexpr int CAP = CellCap<Real>::value;
-    __shared__ WarpSmem<Real> smem[4];
+    extern __shared__ __align__(16) unsigned char cellSmem[];
+    __shared__ double momS[kCellWarps][18];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    WarpSmem<Real>& S = smem[wib];
-    const int gw = blockIdx.x * 4 + wib;
-    const int nw = gridDim.x * 4;
+    Real* sv = reinterpret_cast<Real*>(cellSmem) + (size_t)wib * 4 * kStage;
+    int* sclaim = reinterpret_cast<int*>(cellSmem + (size_t)kCellWarps * 4 * kStage * sizeof(Real)) + wib * kStage;
+    const int gw = blockIdx.x * kCellWarps + wib;
+    const int nw = gridDim.x * kCellWarps;
     const int istep = a.ctl->istep;
     constexpr bool gather = (MODE == kModeStep || MODE == kModeGather);
     constexpr bool collide = (MODE == kModeStep || MODE == kModeCollide);
     constexpr bool sample = (MODE == kModeStep || MODE == kModeSample || MODE == kModePre);
     const PBuf<Real> dst = gather ? a.B : a.A;
     const int* start = gather ? a.startB : a.startA;
+    const int ncell = a.M.ncell;
+    const int nSrc = a.ctl->nLive + a.ctl->nInj;
     uint32_t pairs = 0, colls = 0, big = 0;
-    for (int c = gw; c < a.M.ncell; c += nw) {
+    for (int c = gw; c < ncell; c += nw) {
         const int s0 = start[c];
         const int n = start[c + 1] - s0;
-        if (n > CAP) {
-            if (lane == 0) {
-                const int k = atomicAdd(a.bigCount, 1);
-                a.bigList[k] = c;
-                ++big;
-            }
-            continue;
-        }
+        const bool staged = collide && n <= kStage;
+        Real* vx = staged ? sv : dst.v[0] + s0;
+        Real* vy = staged ? sv + kStage : dst.v[1] + s0;
+        Real* vz = staged ? sv + 2 * kStage : dst.v[2] + s0;
+        Real* ri = staged ? sv + 3 * kStage : dst.ir + s0;
         if constexpr (gather) {
             const int far = a.countSlot[(size_t)c * kSlots + kFarSlot];
-            __syncwarp();
             if (lane == 0) a.countSlot[(size_t)c * kSlots + kFarSlot] = 0;
-            if (far > 32) sort_far_warp<16>(a.idx + s0 + n - far, far);
-            else if (far > 1) sort_far_warp<1>(a.idx + s0 + n - far, far);
-            const int nSrc = a.ctl->nLive + a.ctl->nInj;
+            if (far > 1) sort_far(a.idx + s0 + n - far, far, dst.cell + s0 + n - far);
             for (int k = lane; k < n; k += 32) {
                 int i = a.idx[s0 + k];
                 if ((unsigned)i >= (unsigned)nSrc) {   // self-check: never index outside the source
@@ -794,35 +827,39 @@ __global__ void __launch_bounds__(128) cell_kernel(StepArgs<Real> a)
                 }
                 const int o = s0 + k;
                 dst.x[0][o] = a.A.x[0][i]; dst.x[1][o] = a.A.x[1][i]; dst.x[2][o] = a.A.x[2][i];
+                vx[k] = a.A.v[0][i]; vy[k] = a.A.v[1][i]; vz[k] = a.A.v[2][i];
+                ri[k] = a.A.ir[i];
                 dst.cell[o] = c;
-                S.vx[k] = a.A.v[0][i]; S.vy[k] = a.A.v[1][i]; S.vz[k] = a.A.v[2][i];
-                S.ir[k] = a.A.ir[i];
             }
-        } else {
+            if (lane == 0 && n > kStage) ++big;
+        } else if (staged) {
             for (int k = lane; k < n; k += 32) {
-                const int o = s0 + k;
-                S.vx[k] = a.A.v[0][o]; S.vy[k] = a.A.v[1][o]; S.vz[k] = a.A.v[2][o];
-                S.ir[k] = a.A.ir[o];
+                vx[k] = dst.v[0][s0 + k]; vy[k] = dst.v[1][s0 + k]; vz[k] = dst.v[2][s0 + k];
+                ri[k] = dst.ir[s0 + k];
             }
         }
         __syncwarp();
-        if constexpr (collide) collide_cell<Real>(S.vx, S.vy, S.vz, S.ir, S.claim, n, c, a, istep, pairs, colls);
-        __syncwarp();
-        if constexpr (gather || collide) {
-            for (int k = lane; k < n; k += 32) {
-                const int o = s0 + k;
-                dst.v[0][o] = S.vx[k]; dst.v[1][o] = S.vy[k]; dst.v[2][o] = S.vz[k];
-                dst.ir[o] = S.ir[k];
-            }
+        if constexpr (collide) {
+            int* claim = staged ? sclaim : dst.cell + s0;
+            collide_cell<Real>(vx, vy, vz, ri, claim, n, c, a, istep, pairs, colls);
+            __syncwarp();
+            if (!staged && n > 1)
+                for (int k = lane; k < n; k += 32) dst.cell[s0 + k] = c;
         }
         if constexpr (sample) {
             double m[18];
-            moment_partial<Real>(S.vx, S.vy, S.vz, S.ir, n, lane, 32, m);
+            moment_partial<Real>(vx, vy, vz, ri, n, lane, 32, m);
             warp_reduce18(m);
             if (lane == 0)
-                for (int k = 0; k < 18; ++k) S.mom[k] = m[k];
+                for (int k = 0; k < 18; ++k) momS[wib][k] = m[k];
             __syncwarp();
-            sample_update<Real>(a, c, S.mom, istep, MODE == kModePre);
+            sample_update<Real>(a, c, momS[wib], istep, MODE == kModePre);
+        }
+        if (staged) {
+            for (int k = lane; k < n; k += 32) {
+                dst.v[0][s0 + k] = vx[k]; dst.v[1][s0 + k] = vy[k]; dst.v[2][s0 + k] = vz[k];
+                dst.ir[s0 + k] = ri[k];
+            }
         }
         __syncwarp();
     }
@@ -839,147 +876,46 @@ __global__ void __launch_bounds__(128) cell_kernel(StepArgs<Real> a)
     }
 }
 
-// Cells with more particles than a warp stages: one 256-thread block per
-// cell, particles staged in dynamic shared memory up to kBlockCap, pairs run
-// by warp 0. Beyond kBlockCap the cell is processed in the output buffer in
-// global memory with pairs one at a time and its far segment left in arrival
-// order (flagged in the error word).
+// resident blocks per SM of each cell-kernel variant, set by prepare_kernels
 template <typename Real, int MODE>
-__global__ void __launch_bounds__(256) big_cell_kernel(StepArgs<Real> a)
+struct CellOcc {
+    static int blocks;
+};
+template <typename Real, int MODE>
+int CellOcc<Real, MODE>::blocks = 1;
+
+template <typename Real, int MODE>
+static cudaError_t prepare_cell_mode()
 {
-    extern __shared__ __align__(16) unsigned char dyn[];
-    Real* sv = reinterpret_cast<Real*>(dyn);
-    Real* svx = sv;
-    Real* svy = sv + kBlockCap;
-    Real* svz = sv + 2 * kBlockCap;
-    Real* sir = sv + 3 * kBlockCap;
-    int* claim = reinterpret_cast<int*>(sv + 4 * kBlockCap);
-    __shared__ double red[8][18];
-    __shared__ double mom[18];
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, wid = tid >> 5;
-    const int istep = a.ctl->istep;
-    constexpr bool gather = (MODE == kModeStep || MODE == kModeGather);
-    constexpr bool collide = (MODE == kModeStep || MODE == kModeCollide);
-    constexpr bool sample = (MODE == kModeStep || MODE == kModeSample || MODE == kModePre);
-    const PBuf<Real> dst = gather ? a.B : a.A;
-    const int* start = gather ? a.startB : a.startA;
-    const int nBig = *a.bigCount;
-    uint32_t pairs = 0, colls = 0;
-    for (int bi = blockIdx.x; bi < nBig; bi += gridDim.x) {
-        const int c = a.bigList[bi];
-        const int s0 = start[c];
-        const int n = start[c + 1] - s0;
-        const bool staged = n <= kBlockCap;
-        if constexpr (gather) {
-            const int far = a.countSlot[(size_t)c * kSlots + kFarSlot];
-            __syncthreads();
-            if (tid == 0) a.countSlot[(size_t)c * kSlots + kFarSlot] = 0;
-            int* seg = a.idx + s0 + n - far;
-            if (far > 1 && far <= kBlockCap) {
-                // rank of each far entry among the far entries (distinct values)
-                for (int e = tid; e < far; e += blockDim.x) {
-                    const int v = seg[e];
-                    int r = 0;
-                    for (int f = 0; f < far; ++f) r += seg[f] < v;
-                    claim[r] = v;
-                }
-                __syncthreads();
-                for (int e = tid; e < far; e += blockDim.x) seg[e] = claim[e];
-                __syncthreads();
-            } else if (far > kBlockCap && tid == 0) {
-                atomicOr(a.errorWord, kErrBigCell);
-            }
-            const int nSrc = a.ctl->nLive + a.ctl->nInj;
-            for (int k = tid; k < n; k += blockDim.x) {
-                int i = a.idx[s0 + k];
-                if ((unsigned)i >= (unsigned)nSrc) {
-                    atomicOr(a.errorWord, kErrSortIndex);
-                    i = 0;
-                }
-                const int o = s0 + k;
-                dst.x[0][o] = a.A.x[0][i]; dst.x[1][o] = a.A.x[1][i]; dst.x[2][o] = a.A.x[2][i];
-                dst.cell[o] = c;
-                if (staged) {
-                    svx[k] = a.A.v[0][i]; svy[k] = a.A.v[1][i]; svz[k] = a.A.v[2][i]; sir[k] = a.A.ir[i];
-                } else {
-                    dst.v[0][o] = a.A.v[0][i]; dst.v[1][o] = a.A.v[1][i]; dst.v[2][o] = a.A.v[2][i];
-                    dst.ir[o] = a.A.ir[i];
-                }
-            }
-        } else if (staged) {
-            for (int k = tid; k < n; k += blockDim.x) {
-                const int o = s0 + k;
-                svx[k] = a.A.v[0][o]; svy[k] = a.A.v[1][o]; svz[k] = a.A.v[2][o]; sir[k] = a.A.ir[o];
-            }
-        }
-        __syncthreads();
-        Real* vx = staged ? svx : dst.v[0] + s0;
-        Real* vy = staged ? svy : dst.v[1] + s0;
-        Real* vz = staged ? svz : dst.v[2] + s0;
-        Real* ir = staged ? sir : dst.ir + s0;
-        if constexpr (collide) {
-            if (wid == 0) collide_cell<Real>(vx, vy, vz, ir, staged ? claim : nullptr, n, c, a, istep, pairs, colls);
-        }
-        __syncthreads();
-        if (staged && (gather || collide)) {
-            for (int k = tid; k < n; k += blockDim.x) {
-                const int o = s0 + k;
-                dst.v[0][o] = svx[k]; dst.v[1][o] = svy[k]; dst.v[2][o] = svz[k]; dst.ir[o] = sir[k];
-            }
-        }
-        if constexpr (sample) {
-            double m[18];
-            moment_partial<Real>(vx, vy, vz, ir, n, tid, blockDim.x, m);
-            warp_reduce18(m);
-            if (lane == 0)
-                for (int k = 0; k < 18; ++k) red[wid][k] = m[k];
-            __syncthreads();
-            if (tid < 18) {
-                double s = 0.0;
-                for (int w = 0; w < 8; ++w) s += red[w][tid];
-                mom[tid] = s;
-            }
-            __syncthreads();
-            if (wid == 0) sample_update<Real>(a, c, mom, istep, MODE == kModePre);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        pairs += __shfl_xor_sync(kFull, pairs, o);
-        colls += __shfl_xor_sync(kFull, colls, o);
-    }
-    if (lane == 0) {
-        if (pairs) atomicAdd(a.counters + C_PAIRS, (unsigned long long)pairs);
-        if (colls) atomicAdd(a.counters + C_COLLISIONS, (unsigned long long)colls);
-    }
+    cudaError_t e = cudaFuncSetAttribute(cell_kernel<Real, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)cell_smem_bytes<Real>());
+    if (e != cudaSuccess) return e;
+    int nb = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, cell_kernel<Real, MODE>, kCellWarps * 32,
+                                                      cell_smem_bytes<Real>());
+    if (e != cudaSuccess) return e;
+    CellOcc<Real, MODE>::blocks = nb > 0 ? nb : 1;
+    return cudaSuccess;
 }
 
 template <typename Real, int MODE>
 static void launch_cells_mode(const StepArgs<Real>& a, int smCount, cudaStream_t s)
 {
-    cudaMemsetAsync(a.bigCount, 0, sizeof(int), s);
-    int g = (a.M.ncell + 3) / 4;
-    if (g > smCount * 16) g = smCount * 16;
-    cell_kernel<Real, MODE><<<g, 128, 0, s>>>(a);
-    const size_t dyn = (size_t)kBlockCap * (4 * sizeof(Real) + sizeof(int));
-    big_cell_kernel<Real, MODE><<<smCount, 256, dyn, s>>>(a);
+    int g = (a.M.ncell + kCellWarps - 1) / kCellWarps;
+    const int cap = smCount * CellOcc<Real, MODE>::blocks;
+    if (g > cap) g = cap;
+    cell_kernel<Real, MODE><<<g > 0 ? g : 1, kCellWarps * 32, cell_smem_bytes<Real>(), s>>>(a);
 }
 
 template <typename Real>
 cudaError_t prepare_kernels()
 {
-    const int dyn = (int)((size_t)kBlockCap * (4 * sizeof(Real) + sizeof(int)));
-    cudaError_t e = cudaSuccess;
-    const void* fns[5] = {(const void*)big_cell_kernel<Real, kModeStep>, (const void*)big_cell_kernel<Real, kModeGather>,
-                          (const void*)big_cell_kernel<Real, kModeCollide>, (const void*)big_cell_kernel<Real, kModeSample>,
-                          (const void*)big_cell_kernel<Real, kModePre>};
-    for (const void* f : fns) {
-        const cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-        if (r != cudaSuccess) e = r;
-    }
-    return e;
+    cudaError_t e;
+    if ((e = prepare_cell_mode<Real, kModeStep>()) != cudaSuccess) return e;
+    if ((e = prepare_cell_mode<Real, kModeGather>()) != cudaSuccess) return e;
+    if ((e = prepare_cell_mode<Real, kModeCollide>()) != cudaSuccess) return e;
+    if ((e = prepare_cell_mode<Real, kModeSample>()) != cudaSuccess) return e;
+    return prepare_cell_mode<Real, kModePre>();
 }
 
 template <typename Real>

@@ -72,8 +72,6 @@ struct StepArgs {
 };
 
 constexpr int kScanBlocks = 296;
-constexpr int kWarpCap = 256;      // particles a warp stages in shared memory
-constexpr int kBlockCap = 4096;    // particles the large-cell block stages
 
 // cell-kernel modes
 constexpr int kModeStep = 0;       // gather A->B + collide + sample (fused step)

@@ -160,7 +160,7 @@ typedef struct DsmcCounters {
     uint64_t collisions;        /* accepted pairs (tol_collision_times)      */
     uint64_t fp64_fallbacks;    /* mixed path: crossing steps redone in FP64 */
     uint64_t overflow;          /* particles not stored: capacity exceeded   */
-    uint64_t big_cells;         /* cells handled by the large-cell path      */
+    uint64_t big_cells;         /* cells sorted with more than 512 particles */
 } DsmcCounters;
 
 typedef struct DsmcHandle DsmcHandle;
