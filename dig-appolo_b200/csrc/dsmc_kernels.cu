@@ -505,11 +505,14 @@ __device__ __forceinline__ double qdiv(double x, double y) { return x / y; }
 __device__ __forceinline__ float qdiv(float x, float y) { return __fdividef(x, y); }
 
 // collisionVelocity, src/ProcessDSMC.cpp:2679-2744, on one candidate pair.
+// Particle k of the cell is at vx[k * stride] (and likewise vy, vz, ir).
 template <typename Real>
-__device__ __forceinline__ void collide_pair(Real* vx, Real* vy, Real* vz, Real* ir, int k1, int k2, Stream& rs,
-                                             const DevConsts& C, double consCrm, Real crm0, Real& crmLocal,
-                                             uint32_t& colls)
+__device__ __forceinline__ void collide_pair(Real* vx, Real* vy, Real* vz, Real* ir, int stride, int k1, int k2,
+                                             Stream& rs, const DevConsts& C, double consCrm, Real crm0,
+                                             Real& crmLocal, uint32_t& colls)
 {
+    k1 *= stride;
+    k2 *= stride;
     const Real v1x = vx[k1], v1y = vy[k1], v1z = vz[k1];
     const Real v2x = vx[k2], v2y = vy[k2], v2z = vz[k2];
     const Real vr0 = v1x - v2x, vr1 = v1y - v2y, vr2 = v1z - v2z;
@@ -568,6 +571,44 @@ __device__ __forceinline__ void collide_pair(Real* vx, Real* vy, Real* vz, Real*
     ++colls;
 }
 
+// Candidate pair count of a cell from the majorant, with the carried
+// remainder (collisionDSMC, src/ProcessDSMC.cpp:2631-2645).
+template <typename Real>
+__device__ __forceinline__ int pair_count(const StepArgs<Real>& a, int c, int n, double& consCrm, double& crm0)
+{
+    crm0 = a.crmax[c];
+    const double S = a.M.cellVolume[c];
+    consCrm = collision_diameter(crm0 * a.C.vrms, a.C.cdPrefactor, a.C.eta);
+    const double pairs = 0.5 * n * (n - 1) * a.C.neff * consCrm * a.C.dtime * a.C.dtref / S + a.remColl[c];
+    const int npairs = (int)floor(pairs);
+    a.remColl[c] = pairs - npairs;
+    return npairs;
+}
+
+// NTC collisions of one small cell by one thread: the candidate pairs one
+// after another, particle k at v[k * stride].
+template <typename Real>
+__device__ void collide_cell_serial(Real* vx, Real* vy, Real* vz, Real* ir, int stride, int n, int c,
+                                    const StepArgs<Real>& a, int istep, uint32_t& pairsOut, uint32_t& collOut)
+{
+    if (n <= 1) return;
+    double consCrm, crm0;
+    const int npairs = pair_count(a, c, n, consCrm, crm0);
+    pairsOut += (uint32_t)npairs;
+    if (!(consCrm > 0.0) || npairs <= 0) return;
+    Real crmLocal = (Real)0;
+    const Real crm0r = (Real)crm0;
+    for (int j = 0; j < npairs; ++j) {
+        Stream rs;
+        rs.init((uint32_t)c, (uint32_t)istep, kPurposeCollide | ((uint32_t)j << 4), a.C.seedLo, a.C.seedHi);
+        const int k1 = (int)__umulhi(rs.next32(), (uint32_t)n);
+        int k2 = k1 + 1 + (int)__umulhi(rs.next32(), (uint32_t)(n - 1));
+        if (k2 >= n) k2 -= n;
+        collide_pair<Real>(vx, vy, vz, ir, stride, k1, k2, rs, a.C, consCrm, crm0r, crmLocal, collOut);
+    }
+    if ((double)crmLocal > crm0) a.crmax[c] = (double)crmLocal;
+}
+
 // NTC collisions of one cell by one warp (collisionDSMC,
 // src/ProcessDSMC.cpp:2631-2665): the pair count from the majorant with the
 // carried remainder, then candidate pairs j = 0, 1, ... each drawn from a
@@ -591,12 +632,7 @@ __device__ void collide_cell(Real* vx, Real* vy, Real* vz, Real* ir, int* claim,
     double consCrm = 0.0, crm0 = 0.0;
     int npairs = 0;
     if (lane == 0) {
-        crm0 = a.crmax[c];
-        const double S = a.M.cellVolume[c];
-        consCrm = collision_diameter(crm0 * a.C.vrms, a.C.cdPrefactor, a.C.eta);
-        const double pairs = 0.5 * n * (n - 1) * a.C.neff * consCrm * a.C.dtime * a.C.dtref / S + a.remColl[c];
-        npairs = (int)floor(pairs);
-        a.remColl[c] = pairs - npairs;
+        npairs = pair_count(a, c, n, consCrm, crm0);
         pairsOut += (uint32_t)npairs;
     }
     npairs = __shfl_sync(kFull, npairs, 0);
@@ -634,7 +670,7 @@ __device__ void collide_cell(Real* vx, Real* vy, Real* vz, Real* ir, int* claim,
         const bool go = j >= 0 && claim[k1] == j && claim[k2] == j;
         __syncwarp();
         if (go) {
-            collide_pair<Real>(vx, vy, vz, ir, k1, k2, rs, a.C, consCrm, crm0r, crmLocal, collOut);
+            collide_pair<Real>(vx, vy, vz, ir, 1, k1, k2, rs, a.C, consCrm, crm0r, crmLocal, collOut);
             claim[k1] = INT_MAX;
             claim[k2] = INT_MAX;
             j = -1;
@@ -675,14 +711,17 @@ __device__ void sort_far(int* seg, int m, int* tmp)
     }
 }
 
+// Raw moments of particles k = tid, tid + nt, ... below n; particle k at
+// v[k * stride].
 template <typename Real>
 __device__ __forceinline__ void moment_partial(const Real* vx, const Real* vy, const Real* vz, const Real* ir,
-                                               int n, int tid, int nt, double m[18])
+                                               int stride, int n, int tid, int nt, double m[18])
 {
 #pragma unroll
     for (int k = 0; k < 18; ++k) m[k] = 0.0;
     for (int k = tid; k < n; k += nt) {
-        const double x = (double)vx[k], y = (double)vy[k], z = (double)vz[k], I = (double)ir[k];
+        const int e = k * stride;
+        const double x = (double)vx[e], y = (double)vy[e], z = (double)vz[e], I = (double)ir[e];
         const double v2 = x * x + y * y + z * z;
         m[0] += 1.0; m[1] += x; m[2] += y; m[3] += z; m[4] += v2;
         m[5] += x * x; m[6] += x * y; m[7] += y * y; m[8] += y * z; m[9] += z * z; m[10] += z * x;
@@ -700,86 +739,86 @@ __device__ __forceinline__ void warp_reduce18(double m[18])
     }
 }
 
-// Fold one step's moments (mom[18] in shared memory) into the per-cell
-// accumulators: statistic_macro, src/ProcessDSMC.cpp:2784-2859. Called by a
-// whole warp.
+// Fold one step's moments of cell c into its accumulators, by one thread:
+// statistic_macro, src/ProcessDSMC.cpp:2784-2859 (statistic_macroPre,
+// :3312-3326, when pre).
 template <typename Real>
-__device__ void sample_update(const StepArgs<Real>& a, int c, const double* mom, int istep, bool pre)
+__device__ void sample_cell(const StepArgs<Real>& a, int c, const double* mom, int istep, bool pre)
 {
-    const int lane = threadIdx.x & 31;
     const double S = a.M.cellVolume[c];
-    if (a.stepMom && lane < 18) a.stepMom[(size_t)c * 18 + lane] = mom[lane];
+    if (a.stepMom)
+        for (int k = 0; k < 18; ++k) a.stepMom[(size_t)c * 18 + k] = mom[k];
     if (pre) {
-        // statistic_macroPre, src/ProcessDSMC.cpp:3312-3326
-        if (lane == 0) {
-            double out[18];
-            local_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
-            for (int k = 0; k < 18; ++k) a.local[(size_t)c * 18 + k] = out[k];
-            record_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
-            for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
-        }
+        double out[18];
+        local_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
+        for (int k = 0; k < 18; ++k) a.local[(size_t)c * 18 + k] = out[k];
+        record_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
+        for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
         return;
     }
     double* acc = a.acc + (size_t)c * 54;
     const bool every = (istep % a.C.nevery) == 0;
-    if (lane < 18) {
-        const double v = mom[lane];
-        // updateStepWindowMoments, :3106-3113
-        const double na = (double)a.C.nscheme;
-        const double w = (istep <= a.C.nscheme) ? 1.0 : dd(ds(na, 1.0), na);
-        double s = acc[lane];
-        s = (w == 1.0) ? da(s, v) : da(dm(w, s), v);
-        acc[lane] = s;
-        if (istep > a.C.nss) acc[18 + lane] = da(acc[18 + lane], v);
-        if (every) acc[36 + lane] = da(acc[36 + lane], v);
+    // updateStepWindowMoments, :3106-3113
+    const double na = (double)a.C.nscheme;
+    const double w = (istep <= a.C.nscheme) ? 1.0 : dd(ds(na, 1.0), na);
+    const bool steady = istep > a.C.nss;
+    for (int k = 0; k < 18; ++k) {
+        const double v = mom[k];
+        const double s = acc[k];
+        acc[k] = (w == 1.0) ? da(s, v) : da(dm(w, s), v);
+        if (steady) acc[18 + k] = da(acc[18 + k], v);
+        if (every) acc[36 + k] = da(acc[36 + k], v);
     }
-    __syncwarp();
     const int ngsis = a.C.nevery * a.C.nrepeat;
-    int clear = 0;
-    if (lane == 0) {
-        unsigned char st = a.sparseState[c];
-        int accum = a.sparseAccum[c];
-        if (every && (st == 1 || st == 2)) {
-            if (accum < 0) accum = 0;
-            ++accum;
-        }
-        if (ngsis > 0 && istep % ngsis == 0) {
-            const double* inter = acc + 36;
-            const double ws = inter[0];
-            const bool finite = isfinite(ws);
-            bool sparse = (st == 1 || st == 2);
-            if (!sparse && finite && ws < 3.0) {
-                st = 1;
-                accum = a.C.nrepeat > 1 ? a.C.nrepeat : 1;
-                sparse = true;
-            }
-            const bool valid = (ws >= 3.0) && finite;
-            a.windowSamples[c] = ws;
-            a.windowValid[c] = valid ? 1 : 0;
-            double out[18];
-            if (sparse) {
-                averaged_macro(inter, (double)(accum > 1 ? accum : 1), S, a.C.neff, a.C.nref, a.C.dr, out);
-                for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
-            } else if (valid) {
-                averaged_macro(inter, (double)a.C.nrepeat, S, a.C.neff, a.C.nref, a.C.dr, out);
-                for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
-            }
-            clear = sparse ? 0 : 1;
-        }
-        a.sparseState[c] = st;
-        a.sparseAccum[c] = accum;
+    unsigned char st = a.sparseState[c];
+    int accum = a.sparseAccum[c];
+    if (every && (st == 1 || st == 2)) {
+        if (accum < 0) accum = 0;
+        ++accum;
     }
-    clear = __shfl_sync(kFull, clear, 0);
-    if (clear && lane < 18) acc[36 + lane] = 0.0;
+    if (ngsis > 0 && istep % ngsis == 0) {
+        const double* inter = acc + 36;
+        const double ws = inter[0];
+        const bool finite = isfinite(ws);
+        bool sparse = (st == 1 || st == 2);
+        if (!sparse && finite && ws < 3.0) {
+            st = 1;
+            accum = a.C.nrepeat > 1 ? a.C.nrepeat : 1;
+            sparse = true;
+        }
+        const bool valid = (ws >= 3.0) && finite;
+        a.windowSamples[c] = ws;
+        a.windowValid[c] = valid ? 1 : 0;
+        double out[18];
+        if (sparse) {
+            averaged_macro(inter, (double)(accum > 1 ? accum : 1), S, a.C.neff, a.C.nref, a.C.dr, out);
+            for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
+        } else if (valid) {
+            averaged_macro(inter, (double)a.C.nrepeat, S, a.C.neff, a.C.nref, a.C.dr, out);
+            for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
+        }
+        if (!sparse)
+            for (int k = 0; k < 18; ++k) acc[36 + k] = 0.0;
+    }
+    a.sparseState[c] = st;
+    a.sparseAccum[c] = accum;
 }
 
-// The cell pass, one warp per cell: gather the cell's particles into the
-// sorted output buffer in canonical order, run its collisions, sample it.
-// Up to kStage particles of a cell keep their velocities and internal
-// energies in shared memory from the gather to the write-back, so the
-// collision rounds touch no global memory.
+// The cell pass. A warp takes 32 consecutive cells at a time; for each
+// cell it gathers the particles into the sorted output buffer in canonical
+// order, runs the collisions and samples the cell.
+// - Cells of at most kSmallMax particles: lane l owns cell c0 + l and runs
+//   its pairs and its moment sums alone, with the particles' velocities and
+//   internal energies in shared memory at slot k * 32 + l (lane l's slots
+//   sit in bank l, so the lanes never conflict).
+// - Larger cells: one at a time by the whole warp (collide_cell), staged in
+//   shared memory up to kStage particles, in place in the output buffer
+//   beyond.
+// A cell's moments are summed in the same order in every mode, so the fused
+// step and the stage-by-stage entry points give the same bits.
 constexpr int kCellWarps = 4;
 constexpr int kStage = 512;
+constexpr int kSmallMax = kStage / 32;
 
 template <typename Real>
 constexpr size_t cell_smem_bytes()
@@ -787,81 +826,151 @@ constexpr size_t cell_smem_bytes()
     return (size_t)kCellWarps * kStage * (4 * sizeof(Real) + sizeof(int));
 }
 
+// gather cell c's particles (source indices idx[s0 .. s0+n), far-slot tail
+// put in source order first) into dst; velocities and internal energies go
+// to v[comp][k * stride]
+template <typename Real>
+__device__ __forceinline__ void gather_cell(const StepArgs<Real>& a, const PBuf<Real>& dst, int c, int s0, int n,
+                                            int nSrc, Real* const (&v)[4], int stride)
+{
+    const int lane = threadIdx.x & 31;
+    const int far = a.countSlot[(size_t)c * kSlots + kFarSlot];
+    if (far > 1) sort_far(a.idx + s0 + n - far, far, dst.cell + s0 + n - far);
+    for (int k = lane; k < n; k += 32) {
+        int i = a.idx[s0 + k];
+        if ((unsigned)i >= (unsigned)nSrc) {   // self-check: never index outside the source
+            atomicOr(a.errorWord, kErrSortIndex);
+            i = 0;
+        }
+        const int o = s0 + k;
+        dst.x[0][o] = a.A.x[0][i]; dst.x[1][o] = a.A.x[1][i]; dst.x[2][o] = a.A.x[2][i];
+        const int e = k * stride;
+        v[0][e] = a.A.v[0][i]; v[1][e] = a.A.v[1][i]; v[2][e] = a.A.v[2][i];
+        v[3][e] = a.A.ir[i];
+        dst.cell[o] = c;
+    }
+    __syncwarp();
+    if (lane == 0) a.countSlot[(size_t)c * kSlots + kFarSlot] = 0;
+}
+
+// copy a cell's velocities and internal energies between the buffer (at s0)
+// and v[comp][k * stride], whole warp
+template <typename Real, bool kToBuffer>
+__device__ __forceinline__ void copy_cell(const PBuf<Real>& buf, int s0, int n, Real* const (&v)[4], int stride)
+{
+    const int lane = threadIdx.x & 31;
+    Real* b[4] = {buf.v[0] + s0, buf.v[1] + s0, buf.v[2] + s0, buf.ir + s0};
+    for (int k = lane; k < n; k += 32)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (kToBuffer) b[q][k] = v[q][k * stride];
+            else v[q][k * stride] = b[q][k];
+        }
+}
+
 template <typename Real, int MODE>
-__global__ void __launch_bounds__(kCellWarps * 32) cell_kernel(StepArgs<Real> a)
+__global__ void __launch_bounds__(kCellWarps * 32, 4) cell_kernel(StepArgs<Real> a)
 {
     extern __shared__ __align__(16) unsigned char cellSmem[];
-    __shared__ double momS[kCellWarps][18];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     Real* sv = reinterpret_cast<Real*>(cellSmem) + (size_t)wib * 4 * kStage;
     int* sclaim = reinterpret_cast<int*>(cellSmem + (size_t)kCellWarps * 4 * kStage * sizeof(Real)) + wib * kStage;
+    Real* const stage[4] = {sv, sv + kStage, sv + 2 * kStage, sv + 3 * kStage};
     const int gw = blockIdx.x * kCellWarps + wib;
     const int nw = gridDim.x * kCellWarps;
     const int istep = a.ctl->istep;
     constexpr bool gather = (MODE == kModeStep || MODE == kModeGather);
     constexpr bool collide = (MODE == kModeStep || MODE == kModeCollide);
     constexpr bool sample = (MODE == kModeStep || MODE == kModeSample || MODE == kModePre);
+    constexpr bool pre = (MODE == kModePre);
     const PBuf<Real> dst = gather ? a.B : a.A;
     const int* start = gather ? a.startB : a.startA;
     const int ncell = a.M.ncell;
     const int nSrc = a.ctl->nLive + a.ctl->nInj;
     uint32_t pairs = 0, colls = 0, big = 0;
-    for (int c = gw; c < ncell; c += nw) {
-        const int s0 = start[c];
-        const int n = start[c + 1] - s0;
-        const bool staged = collide && n <= kStage;
-        Real* vx = staged ? sv : dst.v[0] + s0;
-        Real* vy = staged ? sv + kStage : dst.v[1] + s0;
-        Real* vz = staged ? sv + 2 * kStage : dst.v[2] + s0;
-        Real* ri = staged ? sv + 3 * kStage : dst.ir + s0;
-        if constexpr (gather) {
-            const int far = a.countSlot[(size_t)c * kSlots + kFarSlot];
-            if (lane == 0) a.countSlot[(size_t)c * kSlots + kFarSlot] = 0;
-            if (far > 1) sort_far(a.idx + s0 + n - far, far, dst.cell + s0 + n - far);
-            for (int k = lane; k < n; k += 32) {
-                int i = a.idx[s0 + k];
-                if ((unsigned)i >= (unsigned)nSrc) {   // self-check: never index outside the source
-                    atomicOr(a.errorWord, kErrSortIndex);
-                    i = 0;
+    for (int c0 = gw * 32; c0 < ncell; c0 += nw * 32) {
+        const int myc = c0 + lane;
+        const bool valid = myc < ncell;
+        const int ms0 = valid ? start[myc] : 0;
+        const int mn = valid ? start[myc + 1] - ms0 : 0;
+        const unsigned smallMask = __ballot_sync(kFull, valid && mn <= kSmallMax);
+        const unsigned largeMask = __ballot_sync(kFull, valid && mn > kSmallMax);
+
+        // ---- small cells, one lane each
+        if (smallMask) {
+            constexpr bool stagedSmall = collide;     // gather-only and sample-only work on the buffer
+            for (unsigned m = smallMask; m; m &= m - 1) {
+                const int l = __ffs(m) - 1;
+                const int s0 = __shfl_sync(kFull, ms0, l);
+                const int n = __shfl_sync(kFull, mn, l);
+                Real* const to[4] = {stagedSmall ? stage[0] + l : dst.v[0] + s0,
+                                     stagedSmall ? stage[1] + l : dst.v[1] + s0,
+                                     stagedSmall ? stage[2] + l : dst.v[2] + s0,
+                                     stagedSmall ? stage[3] + l : dst.ir + s0};
+                if constexpr (gather) gather_cell<Real>(a, dst, c0 + l, s0, n, nSrc, to, stagedSmall ? 32 : 1);
+                else if constexpr (stagedSmall) copy_cell<Real, false>(dst, s0, n, to, 32);
+            }
+            __syncwarp();
+            const bool mine = (smallMask >> lane) & 1u;
+            Real* const own[4] = {stagedSmall ? stage[0] + lane : dst.v[0] + ms0,
+                                  stagedSmall ? stage[1] + lane : dst.v[1] + ms0,
+                                  stagedSmall ? stage[2] + lane : dst.v[2] + ms0,
+                                  stagedSmall ? stage[3] + lane : dst.ir + ms0};
+            const int ownStride = stagedSmall ? 32 : 1;
+            if constexpr (collide)
+                if (mine) collide_cell_serial<Real>(own[0], own[1], own[2], own[3], ownStride, mn, myc, a, istep, pairs,
+                                                    colls);
+            if constexpr (sample) {
+                if (mine) {
+                    double mom[18];
+                    moment_partial<Real>(own[0], own[1], own[2], own[3], ownStride, mn, 0, 1, mom);
+                    sample_cell<Real>(a, myc, mom, istep, pre);
                 }
-                const int o = s0 + k;
-                dst.x[0][o] = a.A.x[0][i]; dst.x[1][o] = a.A.x[1][i]; dst.x[2][o] = a.A.x[2][i];
-                vx[k] = a.A.v[0][i]; vy[k] = a.A.v[1][i]; vz[k] = a.A.v[2][i];
-                ri[k] = a.A.ir[i];
-                dst.cell[o] = c;
             }
-            if (lane == 0 && n > kStage) ++big;
-        } else if (staged) {
-            for (int k = lane; k < n; k += 32) {
-                vx[k] = dst.v[0][s0 + k]; vy[k] = dst.v[1][s0 + k]; vz[k] = dst.v[2][s0 + k];
-                ri[k] = dst.ir[s0 + k];
-            }
-        }
-        __syncwarp();
-        if constexpr (collide) {
-            int* claim = staged ? sclaim : dst.cell + s0;
-            collide_cell<Real>(vx, vy, vz, ri, claim, n, c, a, istep, pairs, colls);
             __syncwarp();
-            if (!staged && n > 1)
-                for (int k = lane; k < n; k += 32) dst.cell[s0 + k] = c;
-        }
-        if constexpr (sample) {
-            double m[18];
-            moment_partial<Real>(vx, vy, vz, ri, n, lane, 32, m);
-            warp_reduce18(m);
-            if (lane == 0)
-                for (int k = 0; k < 18; ++k) momS[wib][k] = m[k];
-            __syncwarp();
-            sample_update<Real>(a, c, momS[wib], istep, MODE == kModePre);
-        }
-        if (staged) {
-            for (int k = lane; k < n; k += 32) {
-                dst.v[0][s0 + k] = vx[k]; dst.v[1][s0 + k] = vy[k]; dst.v[2][s0 + k] = vz[k];
-                dst.ir[s0 + k] = ri[k];
+            if constexpr (stagedSmall) {
+                for (unsigned m = smallMask; m; m &= m - 1) {
+                    const int l = __ffs(m) - 1;
+                    Real* const from[4] = {stage[0] + l, stage[1] + l, stage[2] + l, stage[3] + l};
+                    copy_cell<Real, true>(dst, __shfl_sync(kFull, ms0, l), __shfl_sync(kFull, mn, l), from, 32);
+                }
+                __syncwarp();
             }
         }
-        __syncwarp();
+
+        // ---- larger cells, one at a time by the whole warp
+        for (unsigned m = largeMask; m; m &= m - 1) {
+            const int l = __ffs(m) - 1;
+            const int c = c0 + l;
+            const int s0 = __shfl_sync(kFull, ms0, l);
+            const int n = __shfl_sync(kFull, mn, l);
+            const bool staged = collide && n <= kStage;
+            Real* const v[4] = {staged ? stage[0] : dst.v[0] + s0, staged ? stage[1] : dst.v[1] + s0,
+                                staged ? stage[2] : dst.v[2] + s0, staged ? stage[3] : dst.ir + s0};
+            if constexpr (gather) {
+                gather_cell<Real>(a, dst, c, s0, n, nSrc, v, 1);
+                if (lane == 0 && n > kStage) ++big;
+            } else if (staged) {
+                copy_cell<Real, false>(dst, s0, n, v, 1);
+            }
+            __syncwarp();
+            if constexpr (collide) {
+                int* claim = staged ? sclaim : dst.cell + s0;
+                collide_cell<Real>(v[0], v[1], v[2], v[3], claim, n, c, a, istep, pairs, colls);
+                __syncwarp();
+                if (!staged)
+                    for (int k = lane; k < n; k += 32) dst.cell[s0 + k] = c;
+            }
+            if constexpr (sample) {
+                double mom[18];
+                moment_partial<Real>(v[0], v[1], v[2], v[3], 1, n, lane, 32, mom);
+                warp_reduce18(mom);
+                if (lane == 0) sample_cell<Real>(a, c, mom, istep, pre);
+            }
+            if (staged) copy_cell<Real, true>(dst, s0, n, v, 1);
+            __syncwarp();
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -901,7 +1010,7 @@ static cudaError_t prepare_cell_mode()
 template <typename Real, int MODE>
 static void launch_cells_mode(const StepArgs<Real>& a, int smCount, cudaStream_t s)
 {
-    int g = (a.M.ncell + kCellWarps - 1) / kCellWarps;
+    int g = (a.M.ncell + 32 * kCellWarps - 1) / (32 * kCellWarps);
     const int cap = smCount * CellOcc<Real, MODE>::blocks;
     if (g > cap) g = cap;
     cell_kernel<Real, MODE><<<g > 0 ? g : 1, kCellWarps * 32, cell_smem_bytes<Real>(), s>>>(a);
