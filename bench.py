@@ -308,7 +308,7 @@ def run_ours(args):
 
 def launches_per_step(wl) -> int:
     # inject: count, scan, generate; move; sort: rank, scan x2, scatter;
-    # cells: the warp kernel and the large-cell kernel
+    # cells: classify and the cell kernel
     return 3 + 1 + 4 + 2
 
 

@@ -38,7 +38,7 @@ enum CounterIdx {
 
 // Error bits in the device error word.
 constexpr int kErrCapacity = 1;
-constexpr int kErrBigCell = 2;
+constexpr int kErrStageCell = 2;   // a cell larger than the stage reached the staged path
 constexpr int kErrRejectLoop = 4;
 constexpr int kErrSortIndex = 8;
 
@@ -81,6 +81,7 @@ struct DevConsts {
     double dtref;
     double omega, eta, alpha, prelax, dr, nref;
     double cdPrefactor;  // collisionDiameterPrefactor, src/ProcessDSMC.cpp:2626-2630
+    float vhsExpF;       // 1 - 2 eta: exponent of the VHS sigma*c ratio (FP32 path)
     uint32_t seedLo, seedHi;
     int maxCross;
     int nss, nscheme, nevery, nrepeat;
@@ -109,6 +110,15 @@ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1)
     return c;
 }
 
+// Uniform variates from raw Philox words: a double in (0,1) with 53 random
+// bits from two words, a float in (0,1) with 24 random bits from one.
+__device__ __forceinline__ double unit64(uint32_t a, uint32_t b)
+{
+    const uint64_t k = ((uint64_t)a << 21) ^ ((uint64_t)b >> 11);
+    return ((double)k + 0.5) * 0x1.0p-53;
+}
+__device__ __forceinline__ float unit32(uint32_t a) { return ((float)(a >> 8) + 0.5f) * 0x1.0p-24f; }
+
 // A sequential stream over counter (id, step, purpose, n), n = 0, 1, ...
 struct Stream {
     uint32_t id, step, purpose, n;
@@ -134,16 +144,12 @@ struct Stream {
     // uniform double in (0,1) with 53 random bits
     __device__ __forceinline__ double uniform64()
     {
-        const uint64_t a = next32();
-        const uint64_t b = next32();
-        const uint64_t k = (a << 21) ^ (b >> 11);
-        return ((double)k + 0.5) * 0x1.0p-53;
+        const uint32_t a = next32();
+        const uint32_t b = next32();
+        return unit64(a, b);
     }
     // uniform float in (0,1) with 24 random bits
-    __device__ __forceinline__ float uniform32()
-    {
-        return ((float)(next32() >> 8) + 0.5f) * 0x1.0p-24f;
-    }
+    __device__ __forceinline__ float uniform32() { return unit32(next32()); }
     template <typename Real> __device__ __forceinline__ Real uniform();
 };
 template <> __device__ __forceinline__ double Stream::uniform<double>() { return uniform64(); }

@@ -136,8 +136,8 @@ struct Engine {
     double* wallTally = nullptr;
     StepCtl* ctl = nullptr;
     unsigned long long* counters = nullptr;
-    int* bigList = nullptr;
-    int* bigCount = nullptr;
+    int* cellList = nullptr;
+    int* cellWork = nullptr;
     int* errorWord = nullptr;
 
     int64_t capacity = 0;
@@ -529,6 +529,7 @@ struct Engine {
         C.dtref = mess.dt_ref;
         C.omega = mess.omega;
         C.eta = mess.eta;
+        C.vhsExpF = (float)(1.0 - 2.0 * mess.eta);
         C.alpha = mess.alpha;
         C.prelax = mess.P_relax;
         C.dr = mess.dr;
@@ -578,7 +579,7 @@ struct Engine {
             !alloc(windowValid, (size_t)ncell) || !alloc(wallTally, (size_t)std::max(nwall, 1) * 6) ||
             !alloc(countSlot, (size_t)ncell * kSlots) || !alloc(scanPartial, kScanBlocks) ||
             !alloc(start[0], (size_t)ncell + 1) || !alloc(start[1], (size_t)ncell + 1) || !alloc(ctl, 1) ||
-            !alloc(counters, C_COUNT) || !alloc(bigList, (size_t)ncell) || !alloc(bigCount, 1) ||
+            !alloc(counters, C_COUNT) || !alloc(cellList, (size_t)ncell * 2) || !alloc(cellWork, 8) ||
             !alloc(errorWord, 1))
             return false;
         if (params.keep_step_moments && !alloc(stepMom, (size_t)ncell * 18)) return false;
@@ -803,7 +804,7 @@ struct Engine {
         a.local = local; a.finalRecord = finalRecord; a.stepMom = stepMom;
         a.sparseState = sparseState; a.sparseAccum = sparseAccum; a.windowSamples = windowSamples;
         a.windowValid = windowValid; a.wallTally = wallTally; a.ctl = ctl; a.counters = counters;
-        a.bigList = bigList; a.bigCount = bigCount; a.errorWord = errorWord;
+        a.cellList = cellList; a.cellWork = cellWork; a.errorWord = errorWord;
         return a;
     }
 
@@ -923,6 +924,7 @@ struct Engine {
         if (!cuda(cudaStreamSynchronize(stream), "sync")) return false;
         if (e & kErrRejectLoop) return fail("inflow sampling rejection loop exceeded its bound");
         if (e & kErrSortIndex) return fail("device self-check: inconsistent sort index (error word 8)");
+        if (e & kErrStageCell) return fail("device self-check: a cell larger than the shared stage (error word 2)");
 
         return true;
     }

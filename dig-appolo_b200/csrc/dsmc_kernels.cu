@@ -504,12 +504,66 @@ __device__ __forceinline__ double collision_diameter(double cr, double prefactor
 __device__ __forceinline__ double qdiv(double x, double y) { return x / y; }
 __device__ __forceinline__ float qdiv(float x, float y) { return __fdividef(x, y); }
 
-// collisionVelocity, src/ProcessDSMC.cpp:2679-2744, on one candidate pair.
-// Particle k of the cell is at vx[k * stride] (and likewise vy, vz, ir).
+// The random words of candidate pair j of cell c at step istep: Philox
+// blocks n = 0, 1, ... of counter (c, istep, kPurposeCollide | j << 4),
+// read in order as one stream. Block 0 is drawn when the pair is handed out
+// (k1, k2, the acceptance variate; in FP32 also the first relaxation test);
+// the rest only for accepted pairs. An accepted pair always reads the same
+// positions (both variates of each particle's relaxation are drawn whether
+// or not it relaxes), so the lanes of a warp draw their blocks together.
+struct PairDraw {
+    U4 b0;
+    uint32_t c, istep, purpose;
+    __device__ __forceinline__ U4 block(uint32_t n, const DevConsts& C) const
+    {
+        return philox4x32_10(U4{c, istep, purpose, n}, C.seedLo, C.seedHi);
+    }
+};
+
+__device__ __forceinline__ PairDraw pair_draw(int c, int istep, int j, int n, const DevConsts& C, int& k1, int& k2)
+{
+    PairDraw d;
+    d.c = (uint32_t)c; d.istep = (uint32_t)istep; d.purpose = kPurposeCollide | ((uint32_t)j << 4);
+    d.b0 = d.block(0, C);
+    k1 = (int)__umulhi(d.b0.x, (uint32_t)n);
+    k2 = k1 + 1 + (int)__umulhi(d.b0.y, (uint32_t)(n - 1));
+    if (k2 >= n) k2 -= n;
+    return d;
+}
+
+// collisionVelocity, src/ProcessDSMC.cpp:2679-2744, on one candidate pair,
+// in two halves: the acceptance test (pair_accept) and, for an accepted
+// pair, the post-collision state (pair_execute). pair_execute recomputes the
+// relative velocity from the same stored velocities, so the halves give the
+// bits of the one-piece test-and-collide. Particle k of the cell is at
+// vx[k * stride] (and likewise vy, vz, ir). w2, w3: words 2 and 3 of the
+// pair's block 0.
 template <typename Real>
-__device__ __forceinline__ void collide_pair(Real* vx, Real* vy, Real* vz, Real* ir, int stride, int k1, int k2,
-                                             Stream& rs, const DevConsts& C, double consCrm, Real crm0,
-                                             Real& crmLocal, uint32_t& colls)
+__device__ __forceinline__ bool pair_accept(const Real* vx, const Real* vy, const Real* vz, int stride, int k1,
+                                            int k2, uint32_t w2, uint32_t w3, const DevConsts& C, double consCrm,
+                                            Real crm0, Real& crmLocal)
+{
+    k1 *= stride;
+    k2 *= stride;
+    const Real vr0 = vx[k1] - vx[k2], vr1 = vy[k1] - vy[k2], vr2 = vz[k1] - vz[k2];
+    const Real cr2 = vr0 * vr0 + vr1 * vr1 + vr2 * vr2;
+    const Real cr = sqrt(cr2);
+    if (cr > crmLocal) crmLocal = cr;
+    Real accept, uAcc;
+    if constexpr (sizeof(Real) == 8) {
+        accept = collision_diameter(cr * C.vrms, C.cdPrefactor, C.eta) / consCrm;
+        uAcc = unit64(w2, w3);
+    } else {
+        // ratio of the VHS sigma*c at cr and at crmax: (cr/crmax)^(1-2 eta)
+        accept = exp2f(C.vhsExpF * __log2f(__fdividef(cr, crm0)));
+        uAcc = unit32(w2);
+    }
+    return uAcc < accept;
+}
+
+template <typename Real>
+__device__ __forceinline__ void pair_execute(Real* vx, Real* vy, Real* vz, Real* ir, int stride, int k1, int k2,
+                                             int c, int istep, int j, uint32_t w3, const DevConsts& C)
 {
     k1 *= stride;
     k2 *= stride;
@@ -519,22 +573,27 @@ __device__ __forceinline__ void collide_pair(Real* vx, Real* vy, Real* vz, Real*
     const Real cr2 = vr0 * vr0 + vr1 * vr1 + vr2 * vr2;
     const Real cr = sqrt(cr2);
     Real preErt = (Real)0.25 * cr2;
-    if (cr > crmLocal) crmLocal = cr;
-    Real accept;
+    PairDraw d;
+    d.c = (uint32_t)c; d.istep = (uint32_t)istep; d.purpose = kPurposeCollide | ((uint32_t)j << 4);
+    Real uRel[2], rRel[2], rChi, th;
     if constexpr (sizeof(Real) == 8) {
-        accept = collision_diameter(cr * C.vrms, C.cdPrefactor, C.eta) / consCrm;
+        const U4 b1 = d.block(1, C), b2 = d.block(2, C), b3 = d.block(3, C);
+        uRel[0] = unit64(b1.x, b1.y); rRel[0] = unit64(b1.z, b1.w);
+        uRel[1] = unit64(b2.x, b2.y); rRel[1] = unit64(b2.z, b2.w);
+        rChi = unit64(b3.x, b3.y); th = unit64(b3.z, b3.w);
     } else {
-        // ratio of the VHS sigma*c at cr and at crmax: (cr/crmax)^(1-2 eta)
-        accept = exp2f((float)(1.0 - 2.0 * C.eta) * __log2f(cr / crm0));
+        const U4 b1 = d.block(1, C), b2 = d.block(2, C);
+        uRel[0] = unit32(w3); rRel[0] = unit32(b1.x);
+        uRel[1] = unit32(b1.y); rRel[1] = unit32(b1.z);
+        rChi = unit32(b1.w); th = unit32(b2.x);
     }
-    if (rs.uniform<Real>() >= accept) return;
     const Real expLB = (Real)(1.0 / (2.5 - C.omega));
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         Real* irp = (h == 0) ? &ir[k1] : &ir[k2];
-        if (rs.uniform<Real>() <= (Real)C.prelax) {
+        if (uRel[h] <= (Real)C.prelax) {
             const Real preEr = *irp;
-            const Real r = rs.uniform<Real>();
+            const Real r = rRel[h];
             Real pw;
             if constexpr (sizeof(Real) == 8) pw = pow(r, expLB); else pw = exp2f(expLB * __log2f(r));
             const Real postEr = (preErt + preEr) * ((Real)1 - pw);
@@ -546,12 +605,11 @@ __device__ __forceinline__ void collide_pair(Real* vx, Real* vy, Real* vz, Real*
     const Real vc0 = (Real)0.5 * (v1x + v2x);
     const Real vc1 = (Real)0.5 * (v1y + v2y);
     const Real vc2 = (Real)0.5 * (v1z + v2z);
-    const Real r = rs.uniform<Real>();
+    const Real r = rChi;
     Real cosChi;
     if constexpr (sizeof(Real) == 8) cosChi = 2.0 * pow(r, 1.0 / C.alpha) - 1.0;
     else cosChi = (C.alpha == 1.0) ? 2.0f * r - 1.0f : 2.0f * exp2f((float)(1.0 / C.alpha) * __log2f(r)) - 1.0f;
     const Real sinChi = sqrt((Real)1 - cosChi * cosChi);
-    const Real th = rs.uniform<Real>();
     Real sth, cth;
     if constexpr (sizeof(Real) == 8) sincospi(2.0 * th, &sth, &cth); else sincospif(2.0f * th, &sth, &cth);
     const Real vrp = sqrt(vr1 * vr1 + vr2 * vr2);
@@ -568,7 +626,6 @@ __device__ __forceinline__ void collide_pair(Real* vx, Real* vy, Real* vz, Real*
     }
     vx[k1] = vc0 + (Real)0.5 * ref1; vy[k1] = vc1 + (Real)0.5 * ref2; vz[k1] = vc2 + (Real)0.5 * ref3;
     vx[k2] = vc0 - (Real)0.5 * ref1; vy[k2] = vc1 - (Real)0.5 * ref2; vz[k2] = vc2 - (Real)0.5 * ref3;
-    ++colls;
 }
 
 // Candidate pair count of a cell from the majorant, with the carried
@@ -599,12 +656,12 @@ __device__ void collide_cell_serial(Real* vx, Real* vy, Real* vz, Real* ir, int 
     Real crmLocal = (Real)0;
     const Real crm0r = (Real)crm0;
     for (int j = 0; j < npairs; ++j) {
-        Stream rs;
-        rs.init((uint32_t)c, (uint32_t)istep, kPurposeCollide | ((uint32_t)j << 4), a.C.seedLo, a.C.seedHi);
-        const int k1 = (int)__umulhi(rs.next32(), (uint32_t)n);
-        int k2 = k1 + 1 + (int)__umulhi(rs.next32(), (uint32_t)(n - 1));
-        if (k2 >= n) k2 -= n;
-        collide_pair<Real>(vx, vy, vz, ir, stride, k1, k2, rs, a.C, consCrm, crm0r, crmLocal, collOut);
+        int k1, k2;
+        const PairDraw d = pair_draw(c, istep, j, n, a.C, k1, k2);
+        if (pair_accept<Real>(vx, vy, vz, stride, k1, k2, d.b0.z, d.b0.w, a.C, consCrm, crm0r, crmLocal)) {
+            pair_execute<Real>(vx, vy, vz, ir, stride, k1, k2, c, istep, j, d.b0.w, a.C);
+            ++collOut;
+        }
     }
     if ((double)crmLocal > crm0) a.crmax[c] = (double)crmLocal;
 }
@@ -647,17 +704,14 @@ __device__ void collide_cell(Real* vx, Real* vy, Real* vz, Real* ir, int* claim,
     int next = 0;     // first pair not yet handed out (same in every lane)
     int j = -1;       // this lane's pending pair
     int k1 = 0, k2 = 0;
-    Stream rs;
+    PairDraw d;
     for (;;) {
         const unsigned idle = __ballot_sync(kFull, j < 0);
         if (j < 0) {
             const int jj = next + __popc(idle & below);
             if (jj < npairs) {
                 j = jj;
-                rs.init((uint32_t)c, (uint32_t)istep, kPurposeCollide | ((uint32_t)j << 4), a.C.seedLo, a.C.seedHi);
-                k1 = (int)__umulhi(rs.next32(), (uint32_t)n);
-                k2 = k1 + 1 + (int)__umulhi(rs.next32(), (uint32_t)(n - 1));
-                if (k2 >= n) k2 -= n;
+                d = pair_draw(c, istep, j, n, a.C, k1, k2);
             }
         }
         next = min(npairs, next + __popc(idle));
@@ -670,7 +724,10 @@ __device__ void collide_cell(Real* vx, Real* vy, Real* vz, Real* ir, int* claim,
         const bool go = j >= 0 && claim[k1] == j && claim[k2] == j;
         __syncwarp();
         if (go) {
-            collide_pair<Real>(vx, vy, vz, ir, 1, k1, k2, rs, a.C, consCrm, crm0r, crmLocal, collOut);
+            if (pair_accept<Real>(vx, vy, vz, 1, k1, k2, d.b0.z, d.b0.w, a.C, consCrm, crm0r, crmLocal)) {
+                pair_execute<Real>(vx, vy, vz, ir, 1, k1, k2, c, istep, j, d.b0.w, a.C);
+                ++collOut;
+            }
             claim[k1] = INT_MAX;
             claim[k2] = INT_MAX;
             j = -1;
@@ -804,26 +861,66 @@ __device__ void sample_cell(const StepArgs<Real>& a, int c, const double* mom, i
     a.sparseAccum[c] = accum;
 }
 
-// The cell pass. A warp takes 32 consecutive cells at a time; for each
-// cell it gathers the particles into the sorted output buffer in canonical
-// order, runs the collisions and samples the cell.
-// - Cells of at most kSmallMax particles: lane l owns cell c0 + l and runs
-//   its pairs and its moment sums alone, with the particles' velocities and
-//   internal energies in shared memory at slot k * 32 + l (lane l's slots
-//   sit in bank l, so the lanes never conflict).
-// - Larger cells: one at a time by the whole warp (collide_cell), staged in
-//   shared memory up to kStage particles, in place in the output buffer
-//   beyond.
-// A cell's moments are summed in the same order in every mode, so the fused
-// step and the stage-by-stage entry points give the same bits.
-constexpr int kCellWarps = 4;
-constexpr int kStage = 512;
-constexpr int kSmallMax = kStage / 32;
+// The cell pass. For each cell: gather its particles into the sorted output
+// buffer in canonical order, run its collisions, sample it. Cells are
+// classified first (classify_kernel) and handed out dynamically, largest
+// first:
+// - huge cells (more than Stage<Real> particles): one at a time by a whole
+//   warp (collide_cell), in place in the output buffer;
+// - large cells: two at a time per warp (collide_two_channels), staged in
+//   shared memory;
+// - small cells (at most kSmallMax particles): 32 at a time per warp, lane
+//   l owning one cell and running its pairs and its moment sums alone, with
+//   the particles' velocities and internal energies in shared memory at slot
+//   k * 32 + l (lane l's slots sit in bank l, so the lanes never conflict).
+// A cell's results do not depend on which warp takes it or when, and its
+// moments are summed in the same order in every mode, so the fused step
+// and the stage-by-stage entry points give the same bits.
+constexpr int kCellWarps = 2;
+constexpr int kSmallMax = 16;
+constexpr int kSmallSlots = 32 * kSmallMax;
+template <typename Real> struct Stage { static constexpr int N = sizeof(Real) == 4 ? 512 : 384; };
 
+// per-warp shared memory: Real stage[2][4][N]; int claim[2][N]; int4 queue[64]
 template <typename Real>
-constexpr size_t cell_smem_bytes()
+__host__ __device__ constexpr size_t warp_smem_bytes()
 {
-    return (size_t)kCellWarps * kStage * (4 * sizeof(Real) + sizeof(int));
+    return (size_t)2 * Stage<Real>::N * (4 * sizeof(Real) + sizeof(int)) + 64 * sizeof(int4);
+}
+template <typename Real>
+__host__ __device__ constexpr size_t cell_smem_bytes()
+{
+    return (size_t)kCellWarps * warp_smem_bytes<Real>();
+}
+static_assert(8 * Stage<double>::N >= 4 * kSmallSlots, "small-cell slots must fit in the two stages");
+
+// cellWork: [0] huge count, [1] large count, [2] small count,
+//           [3] next huge/large item, [4] next small item
+// cellList: huge cells from the front of [0, ncell), large cells from its
+//           back, small cells from the front of [ncell, 2 ncell)
+__global__ void classify_kernel(const int* start, int ncell, int stageMax, int* list, int* work)
+{
+    const int lane = threadIdx.x & 31;
+    for (int base = blockIdx.x * blockDim.x; base < ncell; base += gridDim.x * blockDim.x) {
+        const int c = base + threadIdx.x;
+        const int n = c < ncell ? start[c + 1] - start[c] : -1;
+        const int cls = n < 0 ? -1 : (n > stageMax ? 0 : (n > kSmallMax ? 1 : 2));
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const unsigned m = __ballot_sync(kFull, cls == k);
+            if (!m) continue;
+            const int leader = __ffs(m) - 1;
+            int b = 0;
+            if (lane == leader) b = atomicAdd(work + k, __popc(m));
+            b = __shfl_sync(kFull, b, leader);
+            if (cls == k) {
+                const int pos = b + __popc(m & ((1u << lane) - 1u));
+                if (k == 0) list[pos] = c;
+                else if (k == 1) list[ncell - 1 - pos] = c;
+                else list[ncell + pos] = c;
+            }
+        }
+    }
 }
 
 // gather cell c's particles (source indices idx[s0 .. s0+n), far-slot tail
@@ -868,17 +965,188 @@ __device__ __forceinline__ void copy_cell(const PBuf<Real>& buf, int s0, int n, 
         }
 }
 
-template <typename Real, int MODE>
-__global__ void __launch_bounds__(kCellWarps * 32, 4) cell_kernel(StepArgs<Real> a)
+// moments of a cell by the whole warp (strided partial sums, fixed-order
+// tree), folded into the accumulators by lane 0
+template <typename Real>
+__device__ __forceinline__ void sample_cell_warp(const StepArgs<Real>& a, int c, Real* const (&v)[4], int n, int istep,
+                                                 bool pre)
 {
+    const int lane = threadIdx.x & 31;
+    double mom[18];
+    moment_partial<Real>(v[0], v[1], v[2], v[3], 1, n, lane, 32, mom);
+    warp_reduce18(mom);
+    if (lane == 0) sample_cell<Real>(a, c, mom, istep, pre);
+}
+
+// Collisions of staged large cells, two cells per warp at a time. Each
+// channel runs the sliding window of collide_cell (one pending pair per lane,
+// claims by pair index); the pairs that go in a round are tested for
+// acceptance by their own lanes, and the accepted ones, from both channels,
+// are queued in shared memory and carried out by consecutive lanes, so the
+// costly half of a collision runs once per round with most lanes busy. A
+// channel whose cell is finished (sampled and written back) takes the next
+// cell. *item holds a cell item already taken from the list, or -1.
+template <typename Real, int MODE>
+__device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& dst, const int* start, Real* sv,
+                                     int* sclaim, int4* queue, int nItems, int nHuge, int istep, int nSrc, int& item,
+                                     uint32_t& pairs, uint32_t& colls)
+{
+    constexpr int N = Stage<Real>::N;
+    constexpr bool gather = (MODE == kModeStep);
+    constexpr bool sample = (MODE == kModeStep);
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const int ncell = a.M.ncell;
+    int cc[2] = {-1, -1}, cs0[2] = {0, 0}, cn[2] = {0, 0}, cnp[2] = {0, 0}, cnext[2] = {0, 0};
+    double ccons[2] = {0.0, 0.0}, ccrm[2] = {0.0, 0.0};
+    Real crmL[2] = {(Real)0, (Real)0};
+    int sj[2] = {-1, -1}, sk1[2] = {0, 0}, sk2[2] = {0, 0};
+    uint32_t sw2[2] = {0u, 0u}, sw3[2] = {0u, 0u};
+    bool more = true;
+    for (;;) {
+#pragma unroll
+        for (int ch = 0; ch < 2; ++ch) {
+            Real* const v[4] = {sv + (ch * 4 + 0) * N, sv + (ch * 4 + 1) * N, sv + (ch * 4 + 2) * N,
+                                sv + (ch * 4 + 3) * N};
+            int* claim = sclaim + ch * N;
+            while (cc[ch] < 0 && more) {
+                int it = item;
+                if (it < 0) {
+                    if (lane == 0) it = atomicAdd(a.cellWork + 3, 1);
+                    it = __shfl_sync(kFull, it, 0);
+                }
+                item = -1;
+                if (it >= nItems) {
+                    more = false;
+                    break;
+                }
+                const int c = it < nHuge ? a.cellList[it] : a.cellList[ncell - 1 - (it - nHuge)];
+                const int s0 = start[c];
+                const int n = start[c + 1] - s0;
+                if (n > N) {   // never reached (huge items precede these): flag rather than overflow the stage
+                    if (lane == 0) atomicOr(a.errorWord, kErrStageCell);
+                    continue;
+                }
+                if constexpr (gather) gather_cell<Real>(a, dst, c, s0, n, nSrc, v, 1);
+                else copy_cell<Real, false>(dst, s0, n, v, 1);
+                __syncwarp();
+                double consCrm = 0.0, crm0 = 0.0;
+                int np = 0;
+                if (lane == 0 && n > 1) {
+                    np = pair_count(a, c, n, consCrm, crm0);
+                    pairs += (uint32_t)np;
+                }
+                np = __shfl_sync(kFull, np, 0);
+                consCrm = __shfl_sync(kFull, consCrm, 0);
+                crm0 = __shfl_sync(kFull, crm0, 0);
+                if (!(consCrm > 0.0) || np <= 0) {
+                    if constexpr (sample) sample_cell_warp<Real>(a, c, v, n, istep, false);
+                    copy_cell<Real, true>(dst, s0, n, v, 1);
+                    __syncwarp();
+                    continue;
+                }
+                for (int k = lane; k < n; k += 32) claim[k] = INT_MAX;
+                __syncwarp();
+                cc[ch] = c; cs0[ch] = s0; cn[ch] = n; cnp[ch] = np; cnext[ch] = 0;
+                ccons[ch] = consCrm; ccrm[ch] = crm0; crmL[ch] = (Real)0;
+            }
+        }
+        if (cc[0] < 0 && cc[1] < 0) break;
+        // hand out the next pairs to idle lanes
+#pragma unroll
+        for (int ch = 0; ch < 2; ++ch) {
+            if (cc[ch] < 0) continue;
+            const unsigned idle = __ballot_sync(kFull, sj[ch] < 0);
+            if (sj[ch] < 0) {
+                const int jj = cnext[ch] + __popc(idle & below);
+                if (jj < cnp[ch]) {
+                    sj[ch] = jj;
+                    const PairDraw d = pair_draw(cc[ch], istep, jj, cn[ch], a.C, sk1[ch], sk2[ch]);
+                    sw2[ch] = d.b0.z;
+                    sw3[ch] = d.b0.w;
+                }
+            }
+            cnext[ch] = min(cnp[ch], cnext[ch] + __popc(idle));
+        }
+        // claim both particles with the pair index; the lowest claim goes
+#pragma unroll
+        for (int ch = 0; ch < 2; ++ch)
+            if (sj[ch] >= 0) {
+                atomicMin(&sclaim[ch * N + sk1[ch]], sj[ch]);
+                atomicMin(&sclaim[ch * N + sk2[ch]], sj[ch]);
+            }
+        __syncwarp();
+        bool go[2], acc[2];
+#pragma unroll
+        for (int ch = 0; ch < 2; ++ch)
+            go[ch] = sj[ch] >= 0 && sclaim[ch * N + sk1[ch]] == sj[ch] && sclaim[ch * N + sk2[ch]] == sj[ch];
+        __syncwarp();
+#pragma unroll
+        for (int ch = 0; ch < 2; ++ch) {
+            acc[ch] = false;
+            if (go[ch]) {
+                const Real* base = sv + ch * 4 * N;
+                acc[ch] = pair_accept<Real>(base, base + N, base + 2 * N, 1, sk1[ch], sk2[ch], sw2[ch], sw3[ch], a.C,
+                                            ccons[ch], (Real)ccrm[ch], crmL[ch]);
+            }
+        }
+        const unsigned m0 = __ballot_sync(kFull, acc[0]);
+        const unsigned m1 = __ballot_sync(kFull, acc[1]);
+        if (acc[0]) queue[__popc(m0 & below)] = make_int4(sk1[0], sk2[0], sj[0], (int)sw3[0]);
+        if (acc[1]) queue[__popc(m0) + __popc(m1 & below)] = make_int4(sk1[1], sk2[1], sj[1] | (1 << 30), (int)sw3[1]);
+        __syncwarp();
+        const int total = __popc(m0) + __popc(m1);
+        for (int e = lane; e < total; e += 32) {
+            const int4 q = queue[e];
+            const int ch = q.z >> 30;
+            Real* base = sv + ch * 4 * N;
+            pair_execute<Real>(base, base + N, base + 2 * N, base + 3 * N, 1, q.x, q.y, ch ? cc[1] : cc[0], istep,
+                               q.z & 0x3fffffff, (uint32_t)q.w, a.C);
+        }
+        if (lane == 0) colls += (uint32_t)total;
+        __syncwarp();
+#pragma unroll
+        for (int ch = 0; ch < 2; ++ch)
+            if (go[ch]) {
+                sclaim[ch * N + sk1[ch]] = INT_MAX;
+                sclaim[ch * N + sk2[ch]] = INT_MAX;
+                sj[ch] = -1;
+            }
+        __syncwarp();
+        // a channel whose pairs are all done finishes its cell
+#pragma unroll
+        for (int ch = 0; ch < 2; ++ch) {
+            if (cc[ch] < 0) continue;
+            if (__ballot_sync(kFull, sj[ch] >= 0) != 0u || cnext[ch] < cnp[ch]) continue;
+            Real m = crmL[ch];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const Real y = __shfl_xor_sync(kFull, m, o);
+                m = y > m ? y : m;
+            }
+            if (lane == 0 && (double)m > ccrm[ch]) a.crmax[cc[ch]] = (double)m;
+            Real* const v[4] = {sv + (ch * 4 + 0) * N, sv + (ch * 4 + 1) * N, sv + (ch * 4 + 2) * N,
+                                sv + (ch * 4 + 3) * N};
+            if constexpr (sample) sample_cell_warp<Real>(a, cc[ch], v, cn[ch], istep, false);
+            copy_cell<Real, true>(dst, cs0[ch], cn[ch], v, 1);
+            __syncwarp();
+            cc[ch] = -1;
+        }
+    }
+}
+
+template <typename Real, int MODE>
+__global__ void __launch_bounds__(kCellWarps * 32, 5) cell_kernel(StepArgs<Real> a)
+{
+    constexpr int N = Stage<Real>::N;
     extern __shared__ __align__(16) unsigned char cellSmem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    Real* sv = reinterpret_cast<Real*>(cellSmem) + (size_t)wib * 4 * kStage;
-    int* sclaim = reinterpret_cast<int*>(cellSmem + (size_t)kCellWarps * 4 * kStage * sizeof(Real)) + wib * kStage;
-    Real* const stage[4] = {sv, sv + kStage, sv + 2 * kStage, sv + 3 * kStage};
-    const int gw = blockIdx.x * kCellWarps + wib;
-    const int nw = gridDim.x * kCellWarps;
+    unsigned char* wsm = cellSmem + (size_t)wib * warp_smem_bytes<Real>();
+    Real* sv = reinterpret_cast<Real*>(wsm);
+    int* sclaim = reinterpret_cast<int*>(wsm + (size_t)2 * 4 * N * sizeof(Real));
+    int4* queue = reinterpret_cast<int4*>(wsm + (size_t)2 * N * (4 * sizeof(Real) + sizeof(int)));
+    Real* const stage[4] = {sv, sv + kSmallSlots, sv + 2 * kSmallSlots, sv + 3 * kSmallSlots};
     const int istep = a.ctl->istep;
     constexpr bool gather = (MODE == kModeStep || MODE == kModeGather);
     constexpr bool collide = (MODE == kModeStep || MODE == kModeCollide);
@@ -888,87 +1156,91 @@ __global__ void __launch_bounds__(kCellWarps * 32, 4) cell_kernel(StepArgs<Real>
     const int* start = gather ? a.startB : a.startA;
     const int ncell = a.M.ncell;
     const int nSrc = a.ctl->nLive + a.ctl->nInj;
+    const int nHuge = a.cellWork[0], nLarge = a.cellWork[1], nSmall = a.cellWork[2];
     uint32_t pairs = 0, colls = 0, big = 0;
-    for (int c0 = gw * 32; c0 < ncell; c0 += nw * 32) {
-        const int myc = c0 + lane;
-        const bool valid = myc < ncell;
-        const int ms0 = valid ? start[myc] : 0;
-        const int mn = valid ? start[myc + 1] - ms0 : 0;
-        const unsigned smallMask = __ballot_sync(kFull, valid && mn <= kSmallMax);
-        const unsigned largeMask = __ballot_sync(kFull, valid && mn > kSmallMax);
 
-        // ---- small cells, one lane each
-        if (smallMask) {
-            constexpr bool stagedSmall = collide;     // gather-only and sample-only work on the buffer
-            for (unsigned m = smallMask; m; m &= m - 1) {
-                const int l = __ffs(m) - 1;
-                const int s0 = __shfl_sync(kFull, ms0, l);
-                const int n = __shfl_sync(kFull, mn, l);
-                Real* const to[4] = {stagedSmall ? stage[0] + l : dst.v[0] + s0,
-                                     stagedSmall ? stage[1] + l : dst.v[1] + s0,
-                                     stagedSmall ? stage[2] + l : dst.v[2] + s0,
-                                     stagedSmall ? stage[3] + l : dst.ir + s0};
-                if constexpr (gather) gather_cell<Real>(a, dst, c0 + l, s0, n, nSrc, to, stagedSmall ? 32 : 1);
-                else if constexpr (stagedSmall) copy_cell<Real, false>(dst, s0, n, to, 32);
-            }
-            __syncwarp();
-            const bool mine = (smallMask >> lane) & 1u;
-            Real* const own[4] = {stagedSmall ? stage[0] + lane : dst.v[0] + ms0,
-                                  stagedSmall ? stage[1] + lane : dst.v[1] + ms0,
-                                  stagedSmall ? stage[2] + lane : dst.v[2] + ms0,
-                                  stagedSmall ? stage[3] + lane : dst.ir + ms0};
-            const int ownStride = stagedSmall ? 32 : 1;
-            if constexpr (collide)
-                if (mine) collide_cell_serial<Real>(own[0], own[1], own[2], own[3], ownStride, mn, myc, a, istep, pairs,
-                                                    colls);
-            if constexpr (sample) {
-                if (mine) {
-                    double mom[18];
-                    moment_partial<Real>(own[0], own[1], own[2], own[3], ownStride, mn, 0, 1, mom);
-                    sample_cell<Real>(a, myc, mom, istep, pre);
-                }
-            }
-            __syncwarp();
-            if constexpr (stagedSmall) {
-                for (unsigned m = smallMask; m; m &= m - 1) {
-                    const int l = __ffs(m) - 1;
-                    Real* const from[4] = {stage[0] + l, stage[1] + l, stage[2] + l, stage[3] + l};
-                    copy_cell<Real, true>(dst, __shfl_sync(kFull, ms0, l), __shfl_sync(kFull, mn, l), from, 32);
-                }
-                __syncwarp();
-            }
+    // ---- huge cells (and, without collisions, large cells), one at a time by the whole warp
+    int item = -1;
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(a.cellWork + 3, 1);
+        it = __shfl_sync(kFull, it, 0);
+        if (it >= nHuge + nLarge) break;
+        if (collide && it >= nHuge) {   // a large cell: the two-channel loop takes it
+            item = it;
+            break;
         }
+        const int c = it < nHuge ? a.cellList[it] : a.cellList[ncell - 1 - (it - nHuge)];
+        const int s0 = start[c];
+        const int n = start[c + 1] - s0;
+        Real* const v[4] = {dst.v[0] + s0, dst.v[1] + s0, dst.v[2] + s0, dst.ir + s0};
+        if constexpr (gather) {
+            gather_cell<Real>(a, dst, c, s0, n, nSrc, v, 1);
+            if (lane == 0 && it < nHuge) ++big;
+        }
+        __syncwarp();
+        if constexpr (collide) {
+            collide_cell<Real>(v[0], v[1], v[2], v[3], dst.cell + s0, n, c, a, istep, pairs, colls);
+            __syncwarp();
+            for (int k = lane; k < n; k += 32) dst.cell[s0 + k] = c;
+        }
+        if constexpr (sample) sample_cell_warp<Real>(a, c, v, n, istep, pre);
+        __syncwarp();
+    }
 
-        // ---- larger cells, one at a time by the whole warp
-        for (unsigned m = largeMask; m; m &= m - 1) {
+    // ---- large cells, two at a time
+    if constexpr (collide)
+        if (item >= 0)
+            collide_two_channels<Real, MODE>(a, dst, start, sv, sclaim, queue, nHuge + nLarge, nHuge, istep, nSrc, item,
+                                             pairs, colls);
+
+    // ---- small cells, 32 per warp, one lane each
+    constexpr bool stagedSmall = collide;     // gather-only and sample-only work on the buffer
+    for (;;) {
+        int g = 0;
+        if (lane == 0) g = atomicAdd(a.cellWork + 4, 32);
+        g = __shfl_sync(kFull, g, 0);
+        if (g >= nSmall) break;
+        const bool mine = g + lane < nSmall;
+        const int myc = mine ? a.cellList[ncell + g + lane] : 0;
+        const int ms0 = mine ? start[myc] : 0;
+        const int mn = mine ? start[myc + 1] - ms0 : 0;
+        const unsigned mask = __ballot_sync(kFull, mine);
+        for (unsigned m = mask; m; m &= m - 1) {
             const int l = __ffs(m) - 1;
-            const int c = c0 + l;
             const int s0 = __shfl_sync(kFull, ms0, l);
             const int n = __shfl_sync(kFull, mn, l);
-            const bool staged = collide && n <= kStage;
-            Real* const v[4] = {staged ? stage[0] : dst.v[0] + s0, staged ? stage[1] : dst.v[1] + s0,
-                                staged ? stage[2] : dst.v[2] + s0, staged ? stage[3] : dst.ir + s0};
-            if constexpr (gather) {
-                gather_cell<Real>(a, dst, c, s0, n, nSrc, v, 1);
-                if (lane == 0 && n > kStage) ++big;
-            } else if (staged) {
-                copy_cell<Real, false>(dst, s0, n, v, 1);
-            }
-            __syncwarp();
-            if constexpr (collide) {
-                int* claim = staged ? sclaim : dst.cell + s0;
-                collide_cell<Real>(v[0], v[1], v[2], v[3], claim, n, c, a, istep, pairs, colls);
-                __syncwarp();
-                if (!staged)
-                    for (int k = lane; k < n; k += 32) dst.cell[s0 + k] = c;
-            }
-            if constexpr (sample) {
+            const int c = __shfl_sync(kFull, myc, l);
+            Real* const to[4] = {stagedSmall ? stage[0] + l : dst.v[0] + s0,
+                                 stagedSmall ? stage[1] + l : dst.v[1] + s0,
+                                 stagedSmall ? stage[2] + l : dst.v[2] + s0,
+                                 stagedSmall ? stage[3] + l : dst.ir + s0};
+            if constexpr (gather) gather_cell<Real>(a, dst, c, s0, n, nSrc, to, stagedSmall ? 32 : 1);
+            else if constexpr (stagedSmall) copy_cell<Real, false>(dst, s0, n, to, 32);
+        }
+        __syncwarp();
+        Real* const own[4] = {stagedSmall ? stage[0] + lane : dst.v[0] + ms0,
+                              stagedSmall ? stage[1] + lane : dst.v[1] + ms0,
+                              stagedSmall ? stage[2] + lane : dst.v[2] + ms0,
+                              stagedSmall ? stage[3] + lane : dst.ir + ms0};
+        const int ownStride = stagedSmall ? 32 : 1;
+        if constexpr (collide)
+            if (mine) collide_cell_serial<Real>(own[0], own[1], own[2], own[3], ownStride, mn, myc, a, istep, pairs,
+                                                colls);
+        if constexpr (sample) {
+            if (mine) {
                 double mom[18];
-                moment_partial<Real>(v[0], v[1], v[2], v[3], 1, n, lane, 32, mom);
-                warp_reduce18(mom);
-                if (lane == 0) sample_cell<Real>(a, c, mom, istep, pre);
+                moment_partial<Real>(own[0], own[1], own[2], own[3], ownStride, mn, 0, 1, mom);
+                sample_cell<Real>(a, myc, mom, istep, pre);
             }
-            if (staged) copy_cell<Real, true>(dst, s0, n, v, 1);
+        }
+        __syncwarp();
+        if constexpr (stagedSmall) {
+            for (unsigned m = mask; m; m &= m - 1) {
+                const int l = __ffs(m) - 1;
+                Real* const from[4] = {stage[0] + l, stage[1] + l, stage[2] + l, stage[3] + l};
+                copy_cell<Real, true>(dst, __shfl_sync(kFull, ms0, l), __shfl_sync(kFull, mn, l), from, 32);
+            }
             __syncwarp();
         }
     }
@@ -1010,7 +1282,13 @@ static cudaError_t prepare_cell_mode()
 template <typename Real, int MODE>
 static void launch_cells_mode(const StepArgs<Real>& a, int smCount, cudaStream_t s)
 {
-    int g = (a.M.ncell + 32 * kCellWarps - 1) / (32 * kCellWarps);
+    const int ncell = a.M.ncell;
+    const int* start = (MODE == kModeStep || MODE == kModeGather) ? a.startB : a.startA;
+    cudaMemsetAsync(a.cellWork, 0, 8 * sizeof(int), s);
+    int gc = (ncell + 255) / 256;
+    if (gc > smCount * 8) gc = smCount * 8;
+    classify_kernel<<<gc > 0 ? gc : 1, 256, 0, s>>>(start, ncell, Stage<Real>::N, a.cellList, a.cellWork);
+    int g = (ncell + kCellWarps - 1) / kCellWarps;
     const int cap = smCount * CellOcc<Real, MODE>::blocks;
     if (g > cap) g = cap;
     cell_kernel<Real, MODE><<<g > 0 ? g : 1, kCellWarps * 32, cell_smem_bytes<Real>(), s>>>(a);

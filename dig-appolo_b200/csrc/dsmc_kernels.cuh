@@ -66,8 +66,8 @@ struct StepArgs {
     double* wallTally;        // [nwall*6]
     StepCtl* ctl;
     unsigned long long* counters;
-    int* bigList;
-    int* bigCount;
+    int* cellList;            // [2*ncell] work lists of the cell pass
+    int* cellWork;            // [8] list lengths and hand-out counters of the cell pass
     int* errorWord;
 };
 

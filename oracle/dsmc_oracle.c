@@ -830,11 +830,15 @@ static void collide(OracleCase* o, int istep)
             if (cr > crm) crm = cr;
             const double accept = collision_diameter(o, cr * o->m.v_rms) / consCrm;
             if (st_u64(&rs) >= accept) continue;
+            /* the relaxation test's variate and the energy fraction's are
+             * both drawn for each particle whether or not it relaxes, so an
+             * accepted pair always reads the same stream positions */
             for (int h = 0; h < 2; ++h) {
                 double* irp = h == 0 ? &ir[k1] : &ir[k2];
-                if (st_u64(&rs) <= o->m.P_relax) {
+                const double u = st_u64(&rs);
+                const double r = st_u64(&rs);
+                if (u <= o->m.P_relax) {
                     const double preEr = *irp;
-                    const double r = st_u64(&rs);
                     const double postEr = (preErt + preEr) * (1.0 - pow(r, expLB));
                     *irp = postEr;
                     preErt = preErt + preEr - postEr;
