@@ -81,7 +81,11 @@ struct DevConsts {
     double dtref;
     double omega, eta, alpha, prelax, dr, nref;
     double cdPrefactor;  // collisionDiameterPrefactor, src/ProcessDSMC.cpp:2626-2630
+    double expLB;        // 1 / (2.5 - omega): Larsen-Borgnakke energy-fraction exponent
+    double invAlpha;     // 1 / alpha: VSS scattering exponent
     float vhsExpF;       // 1 - 2 eta: exponent of the VHS sigma*c ratio (FP32 path)
+    float prelaxF;       // P_relax (FP32 path)
+    float invPrelaxF;    // 1 / P_relax, 0 when P_relax is 0 (FP32 path)
     uint32_t seedLo, seedHi;
     int maxCross;
     int nss, nscheme, nevery, nrepeat;

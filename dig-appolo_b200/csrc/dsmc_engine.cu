@@ -530,6 +530,10 @@ struct Engine {
         C.omega = mess.omega;
         C.eta = mess.eta;
         C.vhsExpF = (float)(1.0 - 2.0 * mess.eta);
+        C.expLB = 1.0 / (2.5 - mess.omega);
+        C.invAlpha = 1.0 / mess.alpha;
+        C.prelaxF = (float)mess.P_relax;
+        C.invPrelaxF = mess.P_relax > 0.0 ? (float)(1.0 / mess.P_relax) : 0.0f;
         C.alpha = mess.alpha;
         C.prelax = mess.P_relax;
         C.dr = mess.dr;

@@ -507,10 +507,16 @@ __device__ __forceinline__ float qdiv(float x, float y) { return __fdividef(x, y
 // The random words of candidate pair j of cell c at step istep: Philox
 // blocks n = 0, 1, ... of counter (c, istep, kPurposeCollide | j << 4),
 // read in order as one stream. Block 0 is drawn when the pair is handed out
-// (k1, k2, the acceptance variate; in FP32 also the first relaxation test);
-// the rest only for accepted pairs. An accepted pair always reads the same
-// positions (both variates of each particle's relaxation are drawn whether
-// or not it relaxes), so the lanes of a warp draw their blocks together.
+// (words 0, 1: the two particles; word 2 and in FP64 word 3: the acceptance
+// variate); the rest only for accepted pairs, always at the same positions,
+// so the lanes of a warp draw their blocks together.
+// FP64 (the oracle's layout): block 1 = relaxation test and energy fraction
+// of the first particle, block 2 the same for the second, block 3 = the
+// deflection and azimuth variates, 53-bit uniforms from word pairs.
+// FP32: word 3 of block 0 and word 0 of block 1 are the two relaxation
+// tests, words 1 and 2 of block 1 the deflection and azimuth variates; a
+// particle that relaxes (u <= P) takes u / P as its energy fraction, which
+// given u <= P is again uniform on (0, 1], so one block less is drawn.
 struct PairDraw {
     U4 b0;
     uint32_t c, istep, purpose;
@@ -531,6 +537,11 @@ __device__ __forceinline__ PairDraw pair_draw(int c, int istep, int j, int n, co
     return d;
 }
 
+// Square root: IEEE in FP64; in the FP32 path from the hardware reciprocal
+// square root (a few ulp; the argument is a sum of squares, >= 0).
+__device__ __forceinline__ double psqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float psqrt(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+
 // collisionVelocity, src/ProcessDSMC.cpp:2679-2744, on one candidate pair,
 // in two halves: the acceptance test (pair_accept) and, for an accepted
 // pair, the post-collision state (pair_execute). pair_execute recomputes the
@@ -547,7 +558,7 @@ __device__ __forceinline__ bool pair_accept(const Real* vx, const Real* vy, cons
     k2 *= stride;
     const Real vr0 = vx[k1] - vx[k2], vr1 = vy[k1] - vy[k2], vr2 = vz[k1] - vz[k2];
     const Real cr2 = vr0 * vr0 + vr1 * vr1 + vr2 * vr2;
-    const Real cr = sqrt(cr2);
+    const Real cr = psqrt(cr2);
     if (cr > crmLocal) crmLocal = cr;
     Real accept, uAcc;
     if constexpr (sizeof(Real) == 8) {
@@ -571,7 +582,7 @@ __device__ __forceinline__ void pair_execute(Real* vx, Real* vy, Real* vz, Real*
     const Real v2x = vx[k2], v2y = vy[k2], v2z = vz[k2];
     const Real vr0 = v1x - v2x, vr1 = v1y - v2y, vr2 = v1z - v2z;
     const Real cr2 = vr0 * vr0 + vr1 * vr1 + vr2 * vr2;
-    const Real cr = sqrt(cr2);
+    const Real cr = psqrt(cr2);
     Real preErt = (Real)0.25 * cr2;
     PairDraw d;
     d.c = (uint32_t)c; d.istep = (uint32_t)istep; d.purpose = kPurposeCollide | ((uint32_t)j << 4);
@@ -582,37 +593,46 @@ __device__ __forceinline__ void pair_execute(Real* vx, Real* vy, Real* vz, Real*
         uRel[1] = unit64(b2.x, b2.y); rRel[1] = unit64(b2.z, b2.w);
         rChi = unit64(b3.x, b3.y); th = unit64(b3.z, b3.w);
     } else {
-        const U4 b1 = d.block(1, C), b2 = d.block(2, C);
-        uRel[0] = unit32(w3); rRel[0] = unit32(b1.x);
-        uRel[1] = unit32(b1.y); rRel[1] = unit32(b1.z);
-        rChi = unit32(b1.w); th = unit32(b2.x);
+        const U4 b1 = d.block(1, C);
+        uRel[0] = unit32(w3); uRel[1] = unit32(b1.x);
+        rRel[0] = fminf(uRel[0] * C.invPrelaxF, 1.0f);
+        rRel[1] = fminf(uRel[1] * C.invPrelaxF, 1.0f);
+        rChi = unit32(b1.y); th = unit32(b1.z);
     }
-    const Real expLB = (Real)(1.0 / (2.5 - C.omega));
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         Real* irp = (h == 0) ? &ir[k1] : &ir[k2];
-        if (uRel[h] <= (Real)C.prelax) {
+        bool relax;
+        if constexpr (sizeof(Real) == 8) relax = uRel[h] <= C.prelax; else relax = uRel[h] <= C.prelaxF;
+        if (relax) {
             const Real preEr = *irp;
             const Real r = rRel[h];
             Real pw;
-            if constexpr (sizeof(Real) == 8) pw = pow(r, expLB); else pw = exp2f(expLB * __log2f(r));
+            if constexpr (sizeof(Real) == 8) pw = pow(r, C.expLB); else pw = exp2f((float)C.expLB * __log2f(r));
             const Real postEr = (preErt + preEr) * ((Real)1 - pw);
             *irp = postEr;
             preErt = preErt + preEr - postEr;
         }
     }
-    const Real postVr = sqrt((Real)2 * preErt / (Real)0.5);
     const Real vc0 = (Real)0.5 * (v1x + v2x);
     const Real vc1 = (Real)0.5 * (v1y + v2y);
     const Real vc2 = (Real)0.5 * (v1z + v2z);
-    const Real r = rChi;
-    Real cosChi;
-    if constexpr (sizeof(Real) == 8) cosChi = 2.0 * pow(r, 1.0 / C.alpha) - 1.0;
-    else cosChi = (C.alpha == 1.0) ? 2.0f * r - 1.0f : 2.0f * exp2f((float)(1.0 / C.alpha) * __log2f(r)) - 1.0f;
-    const Real sinChi = sqrt((Real)1 - cosChi * cosChi);
-    Real sth, cth;
-    if constexpr (sizeof(Real) == 8) sincospi(2.0 * th, &sth, &cth); else sincospif(2.0f * th, &sth, &cth);
-    const Real vrp = sqrt(vr1 * vr1 + vr2 * vr2);
+    Real postVr, cosChi, sinChi, sth, cth;
+    if constexpr (sizeof(Real) == 8) {
+        postVr = sqrt(2.0 * preErt / 0.5);
+        cosChi = 2.0 * pow(rChi, C.invAlpha) - 1.0;
+        sinChi = sqrt(1.0 - cosChi * cosChi);
+        sincospi(2.0 * th, &sth, &cth);
+    } else {
+        postVr = 2.0f * psqrt(preErt);
+        cosChi = (C.alpha == 1.0) ? 2.0f * rChi - 1.0f : 2.0f * exp2f((float)C.invAlpha * __log2f(rChi)) - 1.0f;
+        sinChi = psqrt(1.0f - cosChi * cosChi);
+        // azimuth 2 pi th: sin and cos of 2 pi (th - 1/2) in [-pi, pi), negated
+        const float ang = 6.283185307179586f * (th - 0.5f);
+        sth = -__sinf(ang);
+        cth = -__cosf(ang);
+    }
+    const Real vrp = psqrt(vr1 * vr1 + vr2 * vr2);
     const Real tiny = (sizeof(Real) == 8) ? (Real)1.0e-300 : (Real)1.0e-30f;
     const Real scale = qdiv(postVr, cr > tiny ? cr : tiny);
     const Real vrpc = vrp > tiny ? vrp : tiny;
@@ -878,21 +898,22 @@ __device__ void sample_cell(const StepArgs<Real>& a, int c, const double* mom, i
 // and the stage-by-stage entry points give the same bits.
 constexpr int kCellWarps = 2;
 constexpr int kSmallMax = 16;
+constexpr int kArena = 512;                   // staged particles per warp
 constexpr int kSmallSlots = 32 * kSmallMax;
-template <typename Real> struct Stage { static constexpr int N = sizeof(Real) == 4 ? 512 : 384; };
+static_assert(kSmallSlots <= kArena, "small-cell slots must fit in the arena");
+template <typename Real> struct Stage { static constexpr int N = kArena; };
 
-// per-warp shared memory: Real stage[2][4][N]; int claim[2][N]; int4 queue[64]
+// per-warp shared memory: Real arena[4][kArena]; int claim[kArena]; int4 queue[64]
 template <typename Real>
 __host__ __device__ constexpr size_t warp_smem_bytes()
 {
-    return (size_t)2 * Stage<Real>::N * (4 * sizeof(Real) + sizeof(int)) + 64 * sizeof(int4);
+    return (size_t)kArena * (4 * sizeof(Real) + sizeof(int)) + 64 * sizeof(int4);
 }
 template <typename Real>
 __host__ __device__ constexpr size_t cell_smem_bytes()
 {
     return (size_t)kCellWarps * warp_smem_bytes<Real>();
 }
-static_assert(8 * Stage<double>::N >= 4 * kSmallSlots, "small-cell slots must fit in the two stages");
 
 // cellWork: [0] huge count, [1] large count, [2] small count,
 //           [3] next huge/large item, [4] next small item
@@ -978,44 +999,45 @@ __device__ __forceinline__ void sample_cell_warp(const StepArgs<Real>& a, int c,
     if (lane == 0) sample_cell<Real>(a, c, mom, istep, pre);
 }
 
-// Collisions of staged large cells, two cells per warp at a time. Each
-// channel runs the sliding window of collide_cell (one pending pair per lane,
-// claims by pair index); the pairs that go in a round are tested for
-// acceptance by their own lanes, and the accepted ones, from both channels,
-// are queued in shared memory and carried out by consecutive lanes, so the
-// costly half of a collision runs once per round with most lanes busy. A
-// channel whose cell is finished (sampled and written back) takes the next
-// cell. *item holds a cell item already taken from the list, or -1.
+// Collisions of staged large cells, two cells per warp at a time, both in
+// the warp's arena: channel 0's cell at slots [0, n0), channel 1's at
+// [kArena - n1, kArena); a cell that does not fit beside the other channel's
+// waits until that one is done. Each channel runs the sliding window of
+// collide_cell (one pending pair per lane, claims by pair index); the pairs
+// that go in a round are tested for acceptance by their own lanes, and the
+// accepted ones, from both channels, are queued in shared memory and carried
+// out by consecutive lanes, so the costly half of a collision runs once per
+// round with most lanes busy. A channel whose pairs are done finishes its
+// cell (sampled, written back) and takes the next. *item holds a cell item
+// already taken from the list, or -1.
 template <typename Real, int MODE>
-__device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& dst, const int* start, Real* sv,
-                                     int* sclaim, int4* queue, int nItems, int nHuge, int istep, int nSrc, int& item,
+__device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& dst, const int* start, Real* arena,
+                                     int* sclaim, int4* queue, int nItems, int nHuge, int istep, int nSrc, int item,
                                      uint32_t& pairs, uint32_t& colls)
 {
-    constexpr int N = Stage<Real>::N;
+    constexpr int N = kArena;
     constexpr bool gather = (MODE == kModeStep);
     constexpr bool sample = (MODE == kModeStep);
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const int ncell = a.M.ncell;
-    int cc[2] = {-1, -1}, cs0[2] = {0, 0}, cn[2] = {0, 0}, cnp[2] = {0, 0}, cnext[2] = {0, 0};
+    int cc[2] = {-1, -1}, cbase[2] = {0, 0}, cs0[2] = {0, 0}, cn[2] = {0, 0}, cnp[2] = {0, 0}, cnext[2] = {0, 0};
     double ccons[2] = {0.0, 0.0}, ccrm[2] = {0.0, 0.0};
     Real crmL[2] = {(Real)0, (Real)0};
     int sj[2] = {-1, -1}, sk1[2] = {0, 0}, sk2[2] = {0, 0};
     uint32_t sw2[2] = {0u, 0u}, sw3[2] = {0u, 0u};
+    int held = item;      // an item taken but not yet placed
     bool more = true;
     for (;;) {
 #pragma unroll
         for (int ch = 0; ch < 2; ++ch) {
-            Real* const v[4] = {sv + (ch * 4 + 0) * N, sv + (ch * 4 + 1) * N, sv + (ch * 4 + 2) * N,
-                                sv + (ch * 4 + 3) * N};
-            int* claim = sclaim + ch * N;
-            while (cc[ch] < 0 && more) {
-                int it = item;
+            while (cc[ch] < 0 && (more || held >= 0)) {
+                int it = held;
                 if (it < 0) {
                     if (lane == 0) it = atomicAdd(a.cellWork + 3, 1);
                     it = __shfl_sync(kFull, it, 0);
                 }
-                item = -1;
+                held = -1;
                 if (it >= nItems) {
                     more = false;
                     break;
@@ -1023,10 +1045,16 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
                 const int c = it < nHuge ? a.cellList[it] : a.cellList[ncell - 1 - (it - nHuge)];
                 const int s0 = start[c];
                 const int n = start[c + 1] - s0;
-                if (n > N) {   // never reached (huge items precede these): flag rather than overflow the stage
+                if (n > N) {   // never reached (huge items precede these): flag rather than overflow the arena
                     if (lane == 0) atomicOr(a.errorWord, kErrStageCell);
                     continue;
                 }
+                if (n > N - (cc[ch ^ 1] >= 0 ? cn[ch ^ 1] : 0)) {   // wait for the other channel
+                    held = it;
+                    break;
+                }
+                const int base = ch == 0 ? 0 : N - n;
+                Real* const v[4] = {arena + base, arena + N + base, arena + 2 * N + base, arena + 3 * N + base};
                 if constexpr (gather) gather_cell<Real>(a, dst, c, s0, n, nSrc, v, 1);
                 else copy_cell<Real, false>(dst, s0, n, v, 1);
                 __syncwarp();
@@ -1045,9 +1073,9 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
                     __syncwarp();
                     continue;
                 }
-                for (int k = lane; k < n; k += 32) claim[k] = INT_MAX;
+                for (int k = lane; k < n; k += 32) sclaim[base + k] = INT_MAX;
                 __syncwarp();
-                cc[ch] = c; cs0[ch] = s0; cn[ch] = n; cnp[ch] = np; cnext[ch] = 0;
+                cc[ch] = c; cbase[ch] = base; cs0[ch] = s0; cn[ch] = n; cnp[ch] = np; cnext[ch] = 0;
                 ccons[ch] = consCrm; ccrm[ch] = crm0; crmL[ch] = (Real)0;
             }
         }
@@ -1061,7 +1089,10 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
                 const int jj = cnext[ch] + __popc(idle & below);
                 if (jj < cnp[ch]) {
                     sj[ch] = jj;
-                    const PairDraw d = pair_draw(cc[ch], istep, jj, cn[ch], a.C, sk1[ch], sk2[ch]);
+                    int k1, k2;
+                    const PairDraw d = pair_draw(cc[ch], istep, jj, cn[ch], a.C, k1, k2);
+                    sk1[ch] = cbase[ch] + k1;
+                    sk2[ch] = cbase[ch] + k2;
                     sw2[ch] = d.b0.z;
                     sw3[ch] = d.b0.w;
                 }
@@ -1072,35 +1103,35 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
 #pragma unroll
         for (int ch = 0; ch < 2; ++ch)
             if (sj[ch] >= 0) {
-                atomicMin(&sclaim[ch * N + sk1[ch]], sj[ch]);
-                atomicMin(&sclaim[ch * N + sk2[ch]], sj[ch]);
+                atomicMin(&sclaim[sk1[ch]], sj[ch]);
+                atomicMin(&sclaim[sk2[ch]], sj[ch]);
             }
         __syncwarp();
         bool go[2], acc[2];
 #pragma unroll
-        for (int ch = 0; ch < 2; ++ch)
-            go[ch] = sj[ch] >= 0 && sclaim[ch * N + sk1[ch]] == sj[ch] && sclaim[ch * N + sk2[ch]] == sj[ch];
+        for (int ch = 0; ch < 2; ++ch) go[ch] = sj[ch] >= 0 && sclaim[sk1[ch]] == sj[ch] && sclaim[sk2[ch]] == sj[ch];
         __syncwarp();
 #pragma unroll
         for (int ch = 0; ch < 2; ++ch) {
             acc[ch] = false;
-            if (go[ch]) {
-                const Real* base = sv + ch * 4 * N;
-                acc[ch] = pair_accept<Real>(base, base + N, base + 2 * N, 1, sk1[ch], sk2[ch], sw2[ch], sw3[ch], a.C,
+            if (go[ch])
+                acc[ch] = pair_accept<Real>(arena, arena + N, arena + 2 * N, 1, sk1[ch], sk2[ch], sw2[ch], sw3[ch], a.C,
                                             ccons[ch], (Real)ccrm[ch], crmL[ch]);
-            }
         }
         const unsigned m0 = __ballot_sync(kFull, acc[0]);
         const unsigned m1 = __ballot_sync(kFull, acc[1]);
-        if (acc[0]) queue[__popc(m0 & below)] = make_int4(sk1[0], sk2[0], sj[0], (int)sw3[0]);
-        if (acc[1]) queue[__popc(m0) + __popc(m1 & below)] = make_int4(sk1[1], sk2[1], sj[1] | (1 << 30), (int)sw3[1]);
+        if (acc[0]) queue[__popc(m0 & below)] = make_int4(sk1[0] - cbase[0], sk2[0] - cbase[0], sj[0], (int)sw3[0]);
+        if (acc[1])
+            queue[__popc(m0) + __popc(m1 & below)] =
+                make_int4(sk1[1] - cbase[1], sk2[1] - cbase[1], sj[1] | (1 << 30), (int)sw3[1]);
         __syncwarp();
         const int total = __popc(m0) + __popc(m1);
         for (int e = lane; e < total; e += 32) {
             const int4 q = queue[e];
             const int ch = q.z >> 30;
-            Real* base = sv + ch * 4 * N;
-            pair_execute<Real>(base, base + N, base + 2 * N, base + 3 * N, 1, q.x, q.y, ch ? cc[1] : cc[0], istep,
+            const int base = ch ? cbase[1] : cbase[0];
+            Real* b = arena + base;
+            pair_execute<Real>(b, b + N, b + 2 * N, b + 3 * N, 1, q.x, q.y, ch ? cc[1] : cc[0], istep,
                                q.z & 0x3fffffff, (uint32_t)q.w, a.C);
         }
         if (lane == 0) colls += (uint32_t)total;
@@ -1108,8 +1139,8 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
 #pragma unroll
         for (int ch = 0; ch < 2; ++ch)
             if (go[ch]) {
-                sclaim[ch * N + sk1[ch]] = INT_MAX;
-                sclaim[ch * N + sk2[ch]] = INT_MAX;
+                sclaim[sk1[ch]] = INT_MAX;
+                sclaim[sk2[ch]] = INT_MAX;
                 sj[ch] = -1;
             }
         __syncwarp();
@@ -1125,8 +1156,8 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
                 m = y > m ? y : m;
             }
             if (lane == 0 && (double)m > ccrm[ch]) a.crmax[cc[ch]] = (double)m;
-            Real* const v[4] = {sv + (ch * 4 + 0) * N, sv + (ch * 4 + 1) * N, sv + (ch * 4 + 2) * N,
-                                sv + (ch * 4 + 3) * N};
+            const int base = cbase[ch];
+            Real* const v[4] = {arena + base, arena + N + base, arena + 2 * N + base, arena + 3 * N + base};
             if constexpr (sample) sample_cell_warp<Real>(a, cc[ch], v, cn[ch], istep, false);
             copy_cell<Real, true>(dst, cs0[ch], cn[ch], v, 1);
             __syncwarp();
@@ -1136,16 +1167,15 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
 }
 
 template <typename Real, int MODE>
-__global__ void __launch_bounds__(kCellWarps * 32, 5) cell_kernel(StepArgs<Real> a)
+__global__ void __launch_bounds__(kCellWarps * 32, 8) cell_kernel(StepArgs<Real> a)
 {
-    constexpr int N = Stage<Real>::N;
     extern __shared__ __align__(16) unsigned char cellSmem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     unsigned char* wsm = cellSmem + (size_t)wib * warp_smem_bytes<Real>();
     Real* sv = reinterpret_cast<Real*>(wsm);
-    int* sclaim = reinterpret_cast<int*>(wsm + (size_t)2 * 4 * N * sizeof(Real));
-    int4* queue = reinterpret_cast<int4*>(wsm + (size_t)2 * N * (4 * sizeof(Real) + sizeof(int)));
+    int* sclaim = reinterpret_cast<int*>(wsm + (size_t)4 * kArena * sizeof(Real));
+    int4* queue = reinterpret_cast<int4*>(wsm + (size_t)kArena * (4 * sizeof(Real) + sizeof(int)));
     Real* const stage[4] = {sv, sv + kSmallSlots, sv + 2 * kSmallSlots, sv + 3 * kSmallSlots};
     const int istep = a.ctl->istep;
     constexpr bool gather = (MODE == kModeStep || MODE == kModeGather);
