@@ -766,7 +766,7 @@ __device__ void collide_cell(Real* vx, Real* vy, Real* vz, Real* ir, int* claim,
 // Canonical order of a cell's far-slot arrivals: ascending source index.
 // tmp is a scratch range of the same length (the output buffer's cell ids
 // at those positions, written later by the gather).
-__device__ void sort_far(int* seg, int m, int* tmp)
+__device__ __noinline__ void sort_far(int* seg, int m, int* tmp)
 {
     const int lane = threadIdx.x & 31;
     if (m <= 1) return;
@@ -820,7 +820,7 @@ __device__ __forceinline__ void warp_reduce18(double m[18])
 // statistic_macro, src/ProcessDSMC.cpp:2784-2859 (statistic_macroPre,
 // :3312-3326, when pre).
 template <typename Real>
-__device__ void sample_cell(const StepArgs<Real>& a, int c, const double* mom, int istep, bool pre)
+__device__ __noinline__ void sample_cell(const StepArgs<Real>& a, int c, const double* mom, int istep, bool pre)
 {
     const double S = a.M.cellVolume[c];
     if (a.stepMom)
@@ -948,7 +948,7 @@ __global__ void classify_kernel(const int* start, int ncell, int stageMax, int* 
 // put in source order first) into dst; velocities and internal energies go
 // to v[comp][k * stride]
 template <typename Real>
-__device__ __forceinline__ void gather_cell(const StepArgs<Real>& a, const PBuf<Real>& dst, int c, int s0, int n,
+__device__ __noinline__ void gather_cell(const StepArgs<Real>& a, const PBuf<Real>& dst, int c, int s0, int n,
                                             int nSrc, Real* const (&v)[4], int stride)
 {
     const int lane = threadIdx.x & 31;
@@ -989,7 +989,7 @@ __device__ __forceinline__ void copy_cell(const PBuf<Real>& buf, int s0, int n, 
 // moments of a cell by the whole warp (strided partial sums, fixed-order
 // tree), folded into the accumulators by lane 0
 template <typename Real>
-__device__ __forceinline__ void sample_cell_warp(const StepArgs<Real>& a, int c, Real* const (&v)[4], int n, int istep,
+__device__ __noinline__ void sample_cell_warp(const StepArgs<Real>& a, int c, Real* const (&v)[4], int n, int istep,
                                                  bool pre)
 {
     const int lane = threadIdx.x & 31;
@@ -1011,7 +1011,8 @@ __device__ __forceinline__ void sample_cell_warp(const StepArgs<Real>& a, int c,
 // cell (sampled, written back) and takes the next. *item holds a cell item
 // already taken from the list, or -1.
 template <typename Real, int MODE>
-__device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& dst, const int* start, Real* arena,
+__device__ void collide_two_channels(const StepArgs<Real>& a, const StepArgs<Real>& sa, const PBuf<Real>& dst,
+                                     const int* start, Real* arena,
                                      int* sclaim, int4* queue, int nItems, int nHuge, int istep, int nSrc, int item,
                                      uint32_t& pairs, uint32_t& colls)
 {
@@ -1055,7 +1056,7 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
                 }
                 const int base = ch == 0 ? 0 : N - n;
                 Real* const v[4] = {arena + base, arena + N + base, arena + 2 * N + base, arena + 3 * N + base};
-                if constexpr (gather) gather_cell<Real>(a, dst, c, s0, n, nSrc, v, 1);
+                if constexpr (gather) gather_cell<Real>(sa, dst, c, s0, n, nSrc, v, 1);
                 else copy_cell<Real, false>(dst, s0, n, v, 1);
                 __syncwarp();
                 double consCrm = 0.0, crm0 = 0.0;
@@ -1068,7 +1069,7 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
                 consCrm = __shfl_sync(kFull, consCrm, 0);
                 crm0 = __shfl_sync(kFull, crm0, 0);
                 if (!(consCrm > 0.0) || np <= 0) {
-                    if constexpr (sample) sample_cell_warp<Real>(a, c, v, n, istep, false);
+                    if constexpr (sample) sample_cell_warp<Real>(sa, c, v, n, istep, false);
                     copy_cell<Real, true>(dst, s0, n, v, 1);
                     __syncwarp();
                     continue;
@@ -1158,7 +1159,7 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
             if (lane == 0 && (double)m > ccrm[ch]) a.crmax[cc[ch]] = (double)m;
             const int base = cbase[ch];
             Real* const v[4] = {arena + base, arena + N + base, arena + 2 * N + base, arena + 3 * N + base};
-            if constexpr (sample) sample_cell_warp<Real>(a, cc[ch], v, cn[ch], istep, false);
+            if constexpr (sample) sample_cell_warp<Real>(sa, cc[ch], v, cn[ch], istep, false);
             copy_cell<Real, true>(dst, cs0[ch], cn[ch], v, 1);
             __syncwarp();
             cc[ch] = -1;
@@ -1170,6 +1171,12 @@ template <typename Real, int MODE>
 __global__ void __launch_bounds__(kCellWarps * 32, 8) cell_kernel(StepArgs<Real> a)
 {
     extern __shared__ __align__(16) unsigned char cellSmem[];
+    // the arguments, in shared memory for the out-of-line per-cell helpers
+    // (a reference to the kernel parameter would make a per-thread copy)
+    __shared__ StepArgs<Real> sArgs;
+    if (threadIdx.x == 0) sArgs = a;
+    __syncthreads();
+    const StepArgs<Real>& sa = sArgs;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     unsigned char* wsm = cellSmem + (size_t)wib * warp_smem_bytes<Real>();
@@ -1205,7 +1212,7 @@ __global__ void __launch_bounds__(kCellWarps * 32, 8) cell_kernel(StepArgs<Real>
         const int n = start[c + 1] - s0;
         Real* const v[4] = {dst.v[0] + s0, dst.v[1] + s0, dst.v[2] + s0, dst.ir + s0};
         if constexpr (gather) {
-            gather_cell<Real>(a, dst, c, s0, n, nSrc, v, 1);
+            gather_cell<Real>(sa, dst, c, s0, n, nSrc, v, 1);
             if (lane == 0 && it < nHuge) ++big;
         }
         __syncwarp();
@@ -1214,14 +1221,14 @@ __global__ void __launch_bounds__(kCellWarps * 32, 8) cell_kernel(StepArgs<Real>
             __syncwarp();
             for (int k = lane; k < n; k += 32) dst.cell[s0 + k] = c;
         }
-        if constexpr (sample) sample_cell_warp<Real>(a, c, v, n, istep, pre);
+        if constexpr (sample) sample_cell_warp<Real>(sa, c, v, n, istep, pre);
         __syncwarp();
     }
 
     // ---- large cells, two at a time
     if constexpr (collide)
         if (item >= 0)
-            collide_two_channels<Real, MODE>(a, dst, start, sv, sclaim, queue, nHuge + nLarge, nHuge, istep, nSrc, item,
+            collide_two_channels<Real, MODE>(a, sa, dst, start, sv, sclaim, queue, nHuge + nLarge, nHuge, istep, nSrc, item,
                                              pairs, colls);
 
     // ---- small cells, 32 per warp, one lane each
@@ -1245,7 +1252,7 @@ __global__ void __launch_bounds__(kCellWarps * 32, 8) cell_kernel(StepArgs<Real>
                                  stagedSmall ? stage[1] + l : dst.v[1] + s0,
                                  stagedSmall ? stage[2] + l : dst.v[2] + s0,
                                  stagedSmall ? stage[3] + l : dst.ir + s0};
-            if constexpr (gather) gather_cell<Real>(a, dst, c, s0, n, nSrc, to, stagedSmall ? 32 : 1);
+            if constexpr (gather) gather_cell<Real>(sa, dst, c, s0, n, nSrc, to, stagedSmall ? 32 : 1);
             else if constexpr (stagedSmall) copy_cell<Real, false>(dst, s0, n, to, 32);
         }
         __syncwarp();
@@ -1261,7 +1268,7 @@ __global__ void __launch_bounds__(kCellWarps * 32, 8) cell_kernel(StepArgs<Real>
             if (mine) {
                 double mom[18];
                 moment_partial<Real>(own[0], own[1], own[2], own[3], ownStride, mn, 0, 1, mom);
-                sample_cell<Real>(a, myc, mom, istep, pre);
+                sample_cell<Real>(sa, myc, mom, istep, pre);
             }
         }
         __syncwarp();
