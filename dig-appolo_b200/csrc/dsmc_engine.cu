@@ -830,27 +830,20 @@ struct Engine {
         const bool sort = (stages & DSMC_STAGE_SORT) != 0;
         const bool coll = (stages & DSMC_STAGE_COLLIDE) != 0;
         const bool samp = (stages & DSMC_STAGE_SAMPLE) != 0;
-        if (sort) launch_sort<Real>(a, smCount, stream);
-        if (events) cudaEventRecord(ev[3], stream);
-        if (sort && coll && samp) {
-            launch_cells<Real>(a, kModeStep, smCount, stream);
-        } else {
-            if (sort) launch_cells<Real>(a, kModeGather, smCount, stream);
-        }
         if (sort) {
+            // rank, scan, scatter, far-slot order, gather into B
+            launch_sort<Real>(a, smCount, stream);
             cudaMemcpyAsync(&ctl->nLive, &ctl->nNext, sizeof(int), cudaMemcpyDeviceToDevice, stream);
             cudaMemsetAsync(&ctl->nInj, 0, sizeof(int), stream);
         }
-        if (!(sort && coll && samp)) {
-            // stages that act in place on the (now) current buffer
-            StepArgs<Real> b = a;
-            if (sort) {
-                // after the sort the current buffer is the former B
-                b.A = a.B; b.B = a.A; b.startA = a.startB; b.startB = const_cast<int*>(a.startA);
-            }
-            if (coll) launch_cells<Real>(b, kModeCollide, smCount, stream);
-            if (samp) launch_cells<Real>(b, kModeSample, smCount, stream);
+        if (events) cudaEventRecord(ev[3], stream);
+        // collisions and sampling act in place on the (now) current buffer
+        StepArgs<Real> b = a;
+        if (sort) {
+            b.A = a.B; b.B = a.A; b.startA = a.startB; b.startB = const_cast<int*>(a.startA);
         }
+        if (coll) launch_collide<Real>(b, smCount, stream);
+        if (samp) launch_sample<Real>(b, false, smCount, stream);
         if (events) cudaEventRecord(ev[4], stream);
     }
 
@@ -907,8 +900,8 @@ struct Engine {
     bool macroPre()
     {
         if (!haveParticles) return fail("no particles uploaded");
-        if (precision == DSMC_PRECISION_MIXED) launch_cells<float>(args<float>(), kModePre, smCount, stream);
-        else launch_cells<double>(args<double>(), kModePre, smCount, stream);
+        if (precision == DSMC_PRECISION_MIXED) launch_sample<float>(args<float>(), true, smCount, stream);
+        else launch_sample<double>(args<double>(), true, smCount, stream);
         localLazy = false;
         return cuda(cudaGetLastError(), "statistic_macroPre");
     }

@@ -421,21 +421,9 @@ __global__ void __launch_bounds__(256) scatter_kernel(StepArgs<Real> a)
             continue;
         }
         a.idx[base] = i;
+        a.B.cell[base] = d;
     }
 }
-
-template <typename Real>
-void launch_sort(const StepArgs<Real>& a, int smCount, cudaStream_t s)
-{
-    rank_kernel<Real><<<smCount * 8, 256, 0, s>>>(a);
-    scan_partial_kernel<<<kScanBlocks, 256, 0, s>>>(a.countSlot, a.M.ncell, a.scanPartial);
-    scan_final_kernel<<<kScanBlocks, 256, 0, s>>>(a.countSlot, a.M.ncell, a.scanPartial, a.startB, a.ctl);
-    scatter_kernel<Real><<<smCount * 8, 256, 0, s>>>(a);
-}
-
-// ===========================================================================
-// cells: gather + collide + sample
-// ===========================================================================
 
 // Ascending bitonic sort of 32*K keys held K per lane (element e of lane l is
 // position e*32 + l). Unused slots hold 0xffffffff.
@@ -492,11 +480,106 @@ __device__ __forceinline__ void sort_far_warp(int* seg, int m)
     __syncwarp();
 }
 
-// collision_diameter, src/ProcessDSMC.cpp:2603-2608
+// Canonical order of a cell's far-slot arrivals: ascending source index.
+// tmp is a scratch range of the same length (the output buffer's cell ids
+// at those positions, written later by the gather).
+__device__ void sort_far(int* seg, int m, int* tmp)
+{
+    const int lane = threadIdx.x & 31;
+    if (m <= 1) return;
+    if (m <= 32) {
+        sort_far_warp<1>(seg, m);
+    } else if (m <= 512) {
+        sort_far_warp<16>(seg, m);
+    } else {
+        // rank counting: O(m^2 / 32), for the rare very large far segments
+        for (int e = lane; e < m; e += 32) tmp[e] = seg[e];
+        __syncwarp();
+        for (int e = lane; e < m; e += 32) {
+            const int v = tmp[e];
+            int r = 0;
+            for (int f = 0; f < m; ++f) r += tmp[f] < v;
+            seg[r] = v;
+        }
+        __syncwarp();
+    }
+}
+
+// Raw moments of particles k = tid, tid + nt, ... below n; particle k at
+// v[k * stride].
+// Canonical order of every cell's far-slot arrivals (ascending source
+// index); the far counts are cleared for the next step's rank pass. A warp
+// reads the counts of 32 cells and sorts the segments that need it; the
+// output buffer's cell ids of a segment serve as scratch for very long
+// ones and are restored.
+__global__ void __launch_bounds__(256) farsort_kernel(int* countSlot, const int* startB, int* idx, int* cellB,
+                                                      int ncell)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int base = warp * 32; base < ncell; base += nwarps * 32) {
+        const int c = base + lane;
+        int far = 0;
+        if (c < ncell) {
+            far = countSlot[(size_t)c * kSlots + kFarSlot];
+            if (far) countSlot[(size_t)c * kSlots + kFarSlot] = 0;
+        }
+        for (unsigned m = __ballot_sync(kFull, far > 1); m; m &= m - 1) {
+            const int l = __ffs(m) - 1;
+            const int cl = base + l;
+            const int f = __shfl_sync(kFull, far, l);
+            const int e = startB[cl + 1];
+            sort_far(idx + e - f, f, cellB + e - f);
+            if (f > 512) {
+                for (int k = lane; k < f; k += 32) cellB[e - f + k] = cl;
+                __syncwarp();
+            }
+        }
+    }
+}
+
+// cache2chain's data move (src/ProcessDSMC.cpp:2030-2135): output slot o
+// takes source particle idx[o]. Coalesced writes; the reads follow the
+// source order of each arrival group.
+template <typename Real>
+__global__ void __launch_bounds__(256) gather_kernel(StepArgs<Real> a)
+{
+    const int n = a.ctl->nNext;
+    const int nSrc = a.ctl->nLive + a.ctl->nInj;
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n; o += gridDim.x * blockDim.x) {
+        const int i = a.idx[o];
+        if ((unsigned)i >= (unsigned)nSrc) {   // self-check: never index outside the source
+            atomicOr(a.errorWord, kErrSortIndex);
+            continue;
+        }
+        a.B.x[0][o] = a.A.x[0][i]; a.B.x[1][o] = a.A.x[1][i]; a.B.x[2][o] = a.A.x[2][i];
+        a.B.v[0][o] = a.A.v[0][i]; a.B.v[1][o] = a.A.v[1][i]; a.B.v[2][o] = a.A.v[2][i];
+        a.B.ir[o] = a.A.ir[i];
+    }
+}
+
+template <typename Real>
+void launch_sort(const StepArgs<Real>& a, int smCount, cudaStream_t s)
+{
+    rank_kernel<Real><<<smCount * 8, 256, 0, s>>>(a);
+    scan_partial_kernel<<<kScanBlocks, 256, 0, s>>>(a.countSlot, a.M.ncell, a.scanPartial);
+    scan_final_kernel<<<kScanBlocks, 256, 0, s>>>(a.countSlot, a.M.ncell, a.scanPartial, a.startB, a.ctl);
+    scatter_kernel<Real><<<smCount * 8, 256, 0, s>>>(a);
+    farsort_kernel<<<smCount * 4, 256, 0, s>>>(a.countSlot, a.startB, a.idx, a.B.cell, a.M.ncell);
+    gather_kernel<Real><<<smCount * 8, 256, 0, s>>>(a);
+}
+
+// ===========================================================================
+// collisions
+// ===========================================================================
+
+// collision_diameter, src/ProcessDSMC.cpp:2603-2608 (each operation rounded
+// on its own, as the oracle and the reference's x86-64 build evaluate it)
 __device__ __forceinline__ double collision_diameter(double cr, double prefactor, double eta)
 {
-    const double cr2 = cr * cr;
-    return cr * prefactor * pow(1.0 / cr2, eta);
+    const double cr2 = dm(cr, cr);
+    return dm(dm(cr, prefactor), pow(dd(1.0, cr2), eta));
 }
 
 // Division: IEEE in FP64 (the oracle's rounding), the fast reciprocal form
@@ -548,7 +631,8 @@ __device__ __forceinline__ float psqrt(float x) { return x > 0.0f ? x * rsqrtf(x
 // relative velocity from the same stored velocities, so the halves give the
 // bits of the one-piece test-and-collide. Particle k of the cell is at
 // vx[k * stride] (and likewise vy, vz, ir). w2, w3: words 2 and 3 of the
-// pair's block 0.
+// pair's block 0. The FP64 branch rounds each operation on its own in the
+// reference's evaluation order; the FP32 branch lets the compiler fuse.
 template <typename Real>
 __device__ __forceinline__ bool pair_accept(const Real* vx, const Real* vy, const Real* vz, int stride, int k1,
                                             int k2, uint32_t w2, uint32_t w3, const DevConsts& C, double consCrm,
@@ -556,109 +640,145 @@ __device__ __forceinline__ bool pair_accept(const Real* vx, const Real* vy, cons
 {
     k1 *= stride;
     k2 *= stride;
-    const Real vr0 = vx[k1] - vx[k2], vr1 = vy[k1] - vy[k2], vr2 = vz[k1] - vz[k2];
-    const Real cr2 = vr0 * vr0 + vr1 * vr1 + vr2 * vr2;
-    const Real cr = psqrt(cr2);
-    if (cr > crmLocal) crmLocal = cr;
-    Real accept, uAcc;
     if constexpr (sizeof(Real) == 8) {
-        accept = collision_diameter(cr * C.vrms, C.cdPrefactor, C.eta) / consCrm;
-        uAcc = unit64(w2, w3);
+        const double vr0 = ds(vx[k1], vx[k2]), vr1 = ds(vy[k1], vy[k2]), vr2 = ds(vz[k1], vz[k2]);
+        const double cr = sqrt(da(da(dm(vr0, vr0), dm(vr1, vr1)), dm(vr2, vr2)));
+        if (cr > crmLocal) crmLocal = cr;
+        const double accept = dd(collision_diameter(dm(cr, C.vrms), C.cdPrefactor, C.eta), consCrm);
+        return unit64(w2, w3) < accept;
     } else {
+        const float vr0 = vx[k1] - vx[k2], vr1 = vy[k1] - vy[k2], vr2 = vz[k1] - vz[k2];
+        const float cr = psqrt(vr0 * vr0 + vr1 * vr1 + vr2 * vr2);
+        if (cr > crmLocal) crmLocal = cr;
         // ratio of the VHS sigma*c at cr and at crmax: (cr/crmax)^(1-2 eta)
-        accept = exp2f(C.vhsExpF * __log2f(__fdividef(cr, crm0)));
-        uAcc = unit32(w2);
+        const float accept = exp2f(C.vhsExpF * __log2f(__fdividef(cr, crm0)));
+        return unit32(w2) < accept;
     }
-    return uAcc < accept;
+}
+
+__device__ __forceinline__ void pair_execute_fp64(double* vx, double* vy, double* vz, double* ir, int k1, int k2,
+                                                  const PairDraw& d, const DevConsts& C)
+{
+    const double v1x = vx[k1], v1y = vy[k1], v1z = vz[k1];
+    const double v2x = vx[k2], v2y = vy[k2], v2z = vz[k2];
+    const double vr0 = ds(v1x, v2x), vr1 = ds(v1y, v2y), vr2 = ds(v1z, v2z);
+    const double cr2 = da(da(dm(vr0, vr0), dm(vr1, vr1)), dm(vr2, vr2));
+    const double cr = sqrt(cr2);
+    double preErt = dm(0.25, cr2);
+    const U4 b1 = d.block(1, C), b2 = d.block(2, C), b3 = d.block(3, C);
+    const double uRel[2] = {unit64(b1.x, b1.y), unit64(b2.x, b2.y)};
+    const double rRel[2] = {unit64(b1.z, b1.w), unit64(b2.z, b2.w)};
+    const double rChi = unit64(b3.x, b3.y), th = unit64(b3.z, b3.w);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        double* irp = (h == 0) ? &ir[k1] : &ir[k2];
+        if (uRel[h] <= C.prelax) {
+            const double preEr = *irp;
+            const double postEr = dm(da(preErt, preEr), ds(1.0, pow(rRel[h], C.expLB)));
+            *irp = postEr;
+            preErt = ds(da(preErt, preEr), postEr);
+        }
+    }
+    const double postVr = sqrt(dd(dm(2.0, preErt), 0.5));
+    const double vc0 = dm(0.5, da(v1x, v2x)), vc1 = dm(0.5, da(v1y, v2y)), vc2 = dm(0.5, da(v1z, v2z));
+    const double cosChi = ds(dm(2.0, pow(rChi, C.invAlpha)), 1.0);
+    const double sinChi = sqrt(ds(1.0, dm(cosChi, cosChi)));
+    const double ang = dm(6.283185307179586, th);   // 2 pi th
+    const double sth = sin(ang), cth = cos(ang);
+    const double vrp = sqrt(da(dm(vr1, vr1), dm(vr2, vr2)));
+    const double scale = dd(postVr, cr > 1.0e-300 ? cr : 1.0e-300);
+    const double vrpc = vrp > 1.0e-300 ? vrp : 1.0e-300;
+    double r1, r2, r3;
+    if (vrp < 1e-6) {
+        r1 = dm(dm(scale, cosChi), vr0);
+        r2 = dm(dm(dm(scale, sinChi), vr0), cth);
+        r3 = dm(dm(dm(scale, sinChi), vr0), sth);
+    } else {
+        r1 = dm(scale, da(dm(cosChi, vr0), dm(dm(sinChi, sth), vrp)));
+        r2 = dm(scale, da(dm(cosChi, vr1), dd(dm(sinChi, ds(dm(dm(cr, vr2), cth), dm(dm(vr0, vr1), sth))), vrpc)));
+        r3 = dm(scale, ds(dm(cosChi, vr2), dd(dm(sinChi, da(dm(dm(cr, vr1), cth), dm(dm(vr0, vr2), sth))), vrpc)));
+    }
+    vx[k1] = da(vc0, dm(0.5, r1)); vy[k1] = da(vc1, dm(0.5, r2)); vz[k1] = da(vc2, dm(0.5, r3));
+    vx[k2] = ds(vc0, dm(0.5, r1)); vy[k2] = ds(vc1, dm(0.5, r2)); vz[k2] = ds(vc2, dm(0.5, r3));
+}
+
+__device__ __forceinline__ void pair_execute_fp32(float* vx, float* vy, float* vz, float* ir, int k1, int k2,
+                                                  const PairDraw& d, uint32_t w3, const DevConsts& C)
+{
+    const float v1x = vx[k1], v1y = vy[k1], v1z = vz[k1];
+    const float v2x = vx[k2], v2y = vy[k2], v2z = vz[k2];
+    const float vr0 = v1x - v2x, vr1 = v1y - v2y, vr2 = v1z - v2z;
+    const float cr2 = vr0 * vr0 + vr1 * vr1 + vr2 * vr2;
+    const float cr = psqrt(cr2);
+    float preErt = 0.25f * cr2;
+    const U4 b1 = d.block(1, C);
+    const float uRel[2] = {unit32(w3), unit32(b1.x)};
+    const float rChi = unit32(b1.y), th = unit32(b1.z);
+    const float expLB = (float)C.expLB;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        float* irp = (h == 0) ? &ir[k1] : &ir[k2];
+        if (uRel[h] <= C.prelaxF) {
+            const float r = fminf(uRel[h] * C.invPrelaxF, 1.0f);
+            const float preEr = *irp;
+            const float postEr = (preErt + preEr) * (1.0f - exp2f(expLB * __log2f(r)));
+            *irp = postEr;
+            preErt = preErt + preEr - postEr;
+        }
+    }
+    const float postVr = 2.0f * psqrt(preErt);
+    const float vc0 = 0.5f * (v1x + v2x), vc1 = 0.5f * (v1y + v2y), vc2 = 0.5f * (v1z + v2z);
+    const float cosChi =
+        (C.alpha == 1.0) ? 2.0f * rChi - 1.0f : 2.0f * exp2f((float)C.invAlpha * __log2f(rChi)) - 1.0f;
+    const float sinChi = psqrt(1.0f - cosChi * cosChi);
+    // azimuth 2 pi th: sin and cos of 2 pi (th - 1/2) in [-pi, pi), negated
+    const float ang = 6.283185307179586f * (th - 0.5f);
+    const float sth = -__sinf(ang), cth = -__cosf(ang);
+    const float vrp = psqrt(vr1 * vr1 + vr2 * vr2);
+    const float scale = __fdividef(postVr, cr > 1.0e-30f ? cr : 1.0e-30f);
+    const float vrpc = vrp > 1.0e-30f ? vrp : 1.0e-30f;
+    float r1, r2, r3;
+    if (vrp < 1e-6f) {
+        r1 = scale * cosChi * vr0;
+        r2 = scale * sinChi * vr0 * cth;
+        r3 = scale * sinChi * vr0 * sth;
+    } else {
+        r1 = scale * (cosChi * vr0 + sinChi * sth * vrp);
+        r2 = scale * (cosChi * vr1 + __fdividef(sinChi * (cr * vr2 * cth - vr0 * vr1 * sth), vrpc));
+        r3 = scale * (cosChi * vr2 - __fdividef(sinChi * (cr * vr1 * cth + vr0 * vr2 * sth), vrpc));
+    }
+    vx[k1] = vc0 + 0.5f * r1; vy[k1] = vc1 + 0.5f * r2; vz[k1] = vc2 + 0.5f * r3;
+    vx[k2] = vc0 - 0.5f * r1; vy[k2] = vc1 - 0.5f * r2; vz[k2] = vc2 - 0.5f * r3;
 }
 
 template <typename Real>
 __device__ __forceinline__ void pair_execute(Real* vx, Real* vy, Real* vz, Real* ir, int stride, int k1, int k2,
                                              int c, int istep, int j, uint32_t w3, const DevConsts& C)
 {
-    k1 *= stride;
-    k2 *= stride;
-    const Real v1x = vx[k1], v1y = vy[k1], v1z = vz[k1];
-    const Real v2x = vx[k2], v2y = vy[k2], v2z = vz[k2];
-    const Real vr0 = v1x - v2x, vr1 = v1y - v2y, vr2 = v1z - v2z;
-    const Real cr2 = vr0 * vr0 + vr1 * vr1 + vr2 * vr2;
-    const Real cr = psqrt(cr2);
-    Real preErt = (Real)0.25 * cr2;
     PairDraw d;
     d.c = (uint32_t)c; d.istep = (uint32_t)istep; d.purpose = kPurposeCollide | ((uint32_t)j << 4);
-    Real uRel[2], rRel[2], rChi, th;
-    if constexpr (sizeof(Real) == 8) {
-        const U4 b1 = d.block(1, C), b2 = d.block(2, C), b3 = d.block(3, C);
-        uRel[0] = unit64(b1.x, b1.y); rRel[0] = unit64(b1.z, b1.w);
-        uRel[1] = unit64(b2.x, b2.y); rRel[1] = unit64(b2.z, b2.w);
-        rChi = unit64(b3.x, b3.y); th = unit64(b3.z, b3.w);
-    } else {
-        const U4 b1 = d.block(1, C);
-        uRel[0] = unit32(w3); uRel[1] = unit32(b1.x);
-        rRel[0] = fminf(uRel[0] * C.invPrelaxF, 1.0f);
-        rRel[1] = fminf(uRel[1] * C.invPrelaxF, 1.0f);
-        rChi = unit32(b1.y); th = unit32(b1.z);
-    }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        Real* irp = (h == 0) ? &ir[k1] : &ir[k2];
-        bool relax;
-        if constexpr (sizeof(Real) == 8) relax = uRel[h] <= C.prelax; else relax = uRel[h] <= C.prelaxF;
-        if (relax) {
-            const Real preEr = *irp;
-            const Real r = rRel[h];
-            Real pw;
-            if constexpr (sizeof(Real) == 8) pw = pow(r, C.expLB); else pw = exp2f((float)C.expLB * __log2f(r));
-            const Real postEr = (preErt + preEr) * ((Real)1 - pw);
-            *irp = postEr;
-            preErt = preErt + preEr - postEr;
-        }
-    }
-    const Real vc0 = (Real)0.5 * (v1x + v2x);
-    const Real vc1 = (Real)0.5 * (v1y + v2y);
-    const Real vc2 = (Real)0.5 * (v1z + v2z);
-    Real postVr, cosChi, sinChi, sth, cth;
-    if constexpr (sizeof(Real) == 8) {
-        postVr = sqrt(2.0 * preErt / 0.5);
-        cosChi = 2.0 * pow(rChi, C.invAlpha) - 1.0;
-        sinChi = sqrt(1.0 - cosChi * cosChi);
-        sincospi(2.0 * th, &sth, &cth);
-    } else {
-        postVr = 2.0f * psqrt(preErt);
-        cosChi = (C.alpha == 1.0) ? 2.0f * rChi - 1.0f : 2.0f * exp2f((float)C.invAlpha * __log2f(rChi)) - 1.0f;
-        sinChi = psqrt(1.0f - cosChi * cosChi);
-        // azimuth 2 pi th: sin and cos of 2 pi (th - 1/2) in [-pi, pi), negated
-        const float ang = 6.283185307179586f * (th - 0.5f);
-        sth = -__sinf(ang);
-        cth = -__cosf(ang);
-    }
-    const Real vrp = psqrt(vr1 * vr1 + vr2 * vr2);
-    const Real tiny = (sizeof(Real) == 8) ? (Real)1.0e-300 : (Real)1.0e-30f;
-    const Real scale = qdiv(postVr, cr > tiny ? cr : tiny);
-    const Real vrpc = vrp > tiny ? vrp : tiny;
-    Real ref1 = scale * (cosChi * vr0 + sinChi * sth * vrp);
-    Real ref2 = scale * (cosChi * vr1 + qdiv(sinChi * (cr * vr2 * cth - vr0 * vr1 * sth), vrpc));
-    Real ref3 = scale * (cosChi * vr2 - qdiv(sinChi * (cr * vr1 * cth + vr0 * vr2 * sth), vrpc));
-    if (vrp < (Real)1e-6) {
-        ref1 = scale * cosChi * vr0;
-        ref2 = scale * sinChi * vr0 * cth;
-        ref3 = scale * sinChi * vr0 * sth;
-    }
-    vx[k1] = vc0 + (Real)0.5 * ref1; vy[k1] = vc1 + (Real)0.5 * ref2; vz[k1] = vc2 + (Real)0.5 * ref3;
-    vx[k2] = vc0 - (Real)0.5 * ref1; vy[k2] = vc1 - (Real)0.5 * ref2; vz[k2] = vc2 - (Real)0.5 * ref3;
+    if constexpr (sizeof(Real) == 8) pair_execute_fp64(vx, vy, vz, ir, k1 * stride, k2 * stride, d, C);
+    else pair_execute_fp32(vx, vy, vz, ir, k1 * stride, k2 * stride, d, w3, C);
 }
 
 // Candidate pair count of a cell from the majorant, with the carried
-// remainder (collisionDSMC, src/ProcessDSMC.cpp:2631-2645).
+// remainder (collisionDSMC, src/ProcessDSMC.cpp:2631-2645), in the
+// reference's evaluation order.
 template <typename Real>
 __device__ __forceinline__ int pair_count(const StepArgs<Real>& a, int c, int n, double& consCrm, double& crm0)
 {
     crm0 = a.crmax[c];
     const double S = a.M.cellVolume[c];
-    consCrm = collision_diameter(crm0 * a.C.vrms, a.C.cdPrefactor, a.C.eta);
-    const double pairs = 0.5 * n * (n - 1) * a.C.neff * consCrm * a.C.dtime * a.C.dtref / S + a.remColl[c];
+    consCrm = collision_diameter(dm(crm0, a.C.vrms), a.C.cdPrefactor, a.C.eta);
+    double t = dm(0.5, (double)n);
+    t = dm(t, (double)(n - 1));
+    t = dm(t, a.C.neff);
+    t = dm(t, consCrm);
+    t = dm(t, a.C.dtime);
+    t = dm(t, a.C.dtref);
+    const double pairs = da(dd(t, S), a.remColl[c]);
     const int npairs = (int)floor(pairs);
-    a.remColl[c] = pairs - npairs;
+    a.remColl[c] = ds(pairs, (double)npairs);
     return npairs;
 }
 
@@ -763,145 +883,24 @@ __device__ void collide_cell(Real* vx, Real* vy, Real* vz, Real* ir, int* claim,
     if (lane == 0 && (double)m > crm0) a.crmax[c] = (double)m;
 }
 
-// Canonical order of a cell's far-slot arrivals: ascending source index.
-// tmp is a scratch range of the same length (the output buffer's cell ids
-// at those positions, written later by the gather).
-__device__ __noinline__ void sort_far(int* seg, int m, int* tmp)
-{
-    const int lane = threadIdx.x & 31;
-    if (m <= 1) return;
-    if (m <= 32) {
-        sort_far_warp<1>(seg, m);
-    } else if (m <= 512) {
-        sort_far_warp<16>(seg, m);
-    } else {
-        // rank counting: O(m^2 / 32), for the rare very large far segments
-        for (int e = lane; e < m; e += 32) tmp[e] = seg[e];
-        __syncwarp();
-        for (int e = lane; e < m; e += 32) {
-            const int v = tmp[e];
-            int r = 0;
-            for (int f = 0; f < m; ++f) r += tmp[f] < v;
-            seg[r] = v;
-        }
-        __syncwarp();
-    }
-}
-
-// Raw moments of particles k = tid, tid + nt, ... below n; particle k at
-// v[k * stride].
-template <typename Real>
-__device__ __forceinline__ void moment_partial(const Real* vx, const Real* vy, const Real* vz, const Real* ir,
-                                               int stride, int n, int tid, int nt, double m[18])
-{
-#pragma unroll
-    for (int k = 0; k < 18; ++k) m[k] = 0.0;
-    for (int k = tid; k < n; k += nt) {
-        const int e = k * stride;
-        const double x = (double)vx[e], y = (double)vy[e], z = (double)vz[e], I = (double)ir[e];
-        const double v2 = x * x + y * y + z * z;
-        m[0] += 1.0; m[1] += x; m[2] += y; m[3] += z; m[4] += v2;
-        m[5] += x * x; m[6] += x * y; m[7] += y * y; m[8] += y * z; m[9] += z * z; m[10] += z * x;
-        m[11] += x * v2; m[12] += y * v2; m[13] += z * v2;
-        m[14] += I; m[15] += x * I; m[16] += y * I; m[17] += z * I;
-    }
-}
-
-__device__ __forceinline__ void warp_reduce18(double m[18])
-{
-#pragma unroll
-    for (int k = 0; k < 18; ++k) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) m[k] += __shfl_down_sync(kFull, m[k], o);
-    }
-}
-
-// Fold one step's moments of cell c into its accumulators, by one thread:
-// statistic_macro, src/ProcessDSMC.cpp:2784-2859 (statistic_macroPre,
-// :3312-3326, when pre).
-template <typename Real>
-__device__ __noinline__ void sample_cell(const StepArgs<Real>& a, int c, const double* mom, int istep, bool pre)
-{
-    const double S = a.M.cellVolume[c];
-    if (a.stepMom)
-        for (int k = 0; k < 18; ++k) a.stepMom[(size_t)c * 18 + k] = mom[k];
-    if (pre) {
-        double out[18];
-        local_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
-        for (int k = 0; k < 18; ++k) a.local[(size_t)c * 18 + k] = out[k];
-        record_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
-        for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
-        return;
-    }
-    double* acc = a.acc + (size_t)c * 54;
-    const bool every = (istep % a.C.nevery) == 0;
-    // updateStepWindowMoments, :3106-3113
-    const double na = (double)a.C.nscheme;
-    const double w = (istep <= a.C.nscheme) ? 1.0 : dd(ds(na, 1.0), na);
-    const bool steady = istep > a.C.nss;
-    for (int k = 0; k < 18; ++k) {
-        const double v = mom[k];
-        const double s = acc[k];
-        acc[k] = (w == 1.0) ? da(s, v) : da(dm(w, s), v);
-        if (steady) acc[18 + k] = da(acc[18 + k], v);
-        if (every) acc[36 + k] = da(acc[36 + k], v);
-    }
-    const int ngsis = a.C.nevery * a.C.nrepeat;
-    unsigned char st = a.sparseState[c];
-    int accum = a.sparseAccum[c];
-    if (every && (st == 1 || st == 2)) {
-        if (accum < 0) accum = 0;
-        ++accum;
-    }
-    if (ngsis > 0 && istep % ngsis == 0) {
-        const double* inter = acc + 36;
-        const double ws = inter[0];
-        const bool finite = isfinite(ws);
-        bool sparse = (st == 1 || st == 2);
-        if (!sparse && finite && ws < 3.0) {
-            st = 1;
-            accum = a.C.nrepeat > 1 ? a.C.nrepeat : 1;
-            sparse = true;
-        }
-        const bool valid = (ws >= 3.0) && finite;
-        a.windowSamples[c] = ws;
-        a.windowValid[c] = valid ? 1 : 0;
-        double out[18];
-        if (sparse) {
-            averaged_macro(inter, (double)(accum > 1 ? accum : 1), S, a.C.neff, a.C.nref, a.C.dr, out);
-            for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
-        } else if (valid) {
-            averaged_macro(inter, (double)a.C.nrepeat, S, a.C.neff, a.C.nref, a.C.dr, out);
-            for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
-        }
-        if (!sparse)
-            for (int k = 0; k < 18; ++k) acc[36 + k] = 0.0;
-    }
-    a.sparseState[c] = st;
-    a.sparseAccum[c] = accum;
-}
-
-// The cell pass. For each cell: gather its particles into the sorted output
-// buffer in canonical order, run its collisions, sample it. Cells are
-// classified first (classify_kernel) and handed out dynamically, largest
-// first:
-// - huge cells (more than Stage<Real> particles): one at a time by a whole
-//   warp (collide_cell), in place in the output buffer;
+// The collision pass over the sorted buffer (collisionDSMC,
+// src/ProcessDSMC.cpp:2621-2665). Cells are classified first
+// (classify_kernel) and handed out dynamically, largest first:
+// - huge cells (more than kArena particles): one at a time by a whole warp
+//   (collide_cell), in place in the buffer;
 // - large cells: two at a time per warp (collide_two_channels), staged in
 //   shared memory;
 // - small cells (at most kSmallMax particles): 32 at a time per warp, lane
-//   l owning one cell and running its pairs and its moment sums alone, with
-//   the particles' velocities and internal energies in shared memory at slot
-//   k * 32 + l (lane l's slots sit in bank l, so the lanes never conflict).
-// A cell's results do not depend on which warp takes it or when, and its
-// moments are summed in the same order in every mode, so the fused step
-// and the stage-by-stage entry points give the same bits.
+//   l owning one cell and running its pairs alone, with the particles'
+//   velocities and internal energies in shared memory at slot k * 32 + l
+//   (lane l's slots sit in bank l, so the lanes never conflict).
+// A cell's result depends on nothing but the cell, so neither the warp that
+// takes it nor the order matters.
 constexpr int kCellWarps = 2;
 constexpr int kSmallMax = 16;
 constexpr int kArena = 512;                   // staged particles per warp
 constexpr int kSmallSlots = 32 * kSmallMax;
 static_assert(kSmallSlots <= kArena, "small-cell slots must fit in the arena");
-template <typename Real> struct Stage { static constexpr int N = kArena; };
 
 // per-warp shared memory: Real arena[4][kArena]; int claim[kArena]; int4 queue[64]
 template <typename Real>
@@ -944,33 +943,6 @@ __global__ void classify_kernel(const int* start, int ncell, int stageMax, int* 
     }
 }
 
-// gather cell c's particles (source indices idx[s0 .. s0+n), far-slot tail
-// put in source order first) into dst; velocities and internal energies go
-// to v[comp][k * stride]
-template <typename Real>
-__device__ __noinline__ void gather_cell(const StepArgs<Real>& a, const PBuf<Real>& dst, int c, int s0, int n,
-                                            int nSrc, Real* const (&v)[4], int stride)
-{
-    const int lane = threadIdx.x & 31;
-    const int far = a.countSlot[(size_t)c * kSlots + kFarSlot];
-    if (far > 1) sort_far(a.idx + s0 + n - far, far, dst.cell + s0 + n - far);
-    for (int k = lane; k < n; k += 32) {
-        int i = a.idx[s0 + k];
-        if ((unsigned)i >= (unsigned)nSrc) {   // self-check: never index outside the source
-            atomicOr(a.errorWord, kErrSortIndex);
-            i = 0;
-        }
-        const int o = s0 + k;
-        dst.x[0][o] = a.A.x[0][i]; dst.x[1][o] = a.A.x[1][i]; dst.x[2][o] = a.A.x[2][i];
-        const int e = k * stride;
-        v[0][e] = a.A.v[0][i]; v[1][e] = a.A.v[1][i]; v[2][e] = a.A.v[2][i];
-        v[3][e] = a.A.ir[i];
-        dst.cell[o] = c;
-    }
-    __syncwarp();
-    if (lane == 0) a.countSlot[(size_t)c * kSlots + kFarSlot] = 0;
-}
-
 // copy a cell's velocities and internal energies between the buffer (at s0)
 // and v[comp][k * stride], whole warp
 template <typename Real, bool kToBuffer>
@@ -986,19 +958,6 @@ __device__ __forceinline__ void copy_cell(const PBuf<Real>& buf, int s0, int n, 
         }
 }
 
-// moments of a cell by the whole warp (strided partial sums, fixed-order
-// tree), folded into the accumulators by lane 0
-template <typename Real>
-__device__ __noinline__ void sample_cell_warp(const StepArgs<Real>& a, int c, Real* const (&v)[4], int n, int istep,
-                                                 bool pre)
-{
-    const int lane = threadIdx.x & 31;
-    double mom[18];
-    moment_partial<Real>(v[0], v[1], v[2], v[3], 1, n, lane, 32, mom);
-    warp_reduce18(mom);
-    if (lane == 0) sample_cell<Real>(a, c, mom, istep, pre);
-}
-
 // Collisions of staged large cells, two cells per warp at a time, both in
 // the warp's arena: channel 0's cell at slots [0, n0), channel 1's at
 // [kArena - n1, kArena); a cell that does not fit beside the other channel's
@@ -1007,18 +966,15 @@ __device__ __noinline__ void sample_cell_warp(const StepArgs<Real>& a, int c, Re
 // that go in a round are tested for acceptance by their own lanes, and the
 // accepted ones, from both channels, are queued in shared memory and carried
 // out by consecutive lanes, so the costly half of a collision runs once per
-// round with most lanes busy. A channel whose pairs are done finishes its
-// cell (sampled, written back) and takes the next. *item holds a cell item
+// round with most lanes busy. A channel whose pairs are done writes its
+// cell back and takes the next. *item holds a cell item
 // already taken from the list, or -1.
-template <typename Real, int MODE>
-__device__ void collide_two_channels(const StepArgs<Real>& a, const StepArgs<Real>& sa, const PBuf<Real>& dst,
-                                     const int* start, Real* arena,
-                                     int* sclaim, int4* queue, int nItems, int nHuge, int istep, int nSrc, int item,
+template <typename Real>
+__device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& dst, const int* start, Real* arena,
+                                     int* sclaim, int4* queue, int nItems, int nHuge, int istep, int item,
                                      uint32_t& pairs, uint32_t& colls)
 {
     constexpr int N = kArena;
-    constexpr bool gather = (MODE == kModeStep);
-    constexpr bool sample = (MODE == kModeStep);
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const int ncell = a.M.ncell;
@@ -1056,8 +1012,7 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const StepArgs<Rea
                 }
                 const int base = ch == 0 ? 0 : N - n;
                 Real* const v[4] = {arena + base, arena + N + base, arena + 2 * N + base, arena + 3 * N + base};
-                if constexpr (gather) gather_cell<Real>(sa, dst, c, s0, n, nSrc, v, 1);
-                else copy_cell<Real, false>(dst, s0, n, v, 1);
+                copy_cell<Real, false>(dst, s0, n, v, 1);
                 __syncwarp();
                 double consCrm = 0.0, crm0 = 0.0;
                 int np = 0;
@@ -1068,9 +1023,7 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const StepArgs<Rea
                 np = __shfl_sync(kFull, np, 0);
                 consCrm = __shfl_sync(kFull, consCrm, 0);
                 crm0 = __shfl_sync(kFull, crm0, 0);
-                if (!(consCrm > 0.0) || np <= 0) {
-                    if constexpr (sample) sample_cell_warp<Real>(sa, c, v, n, istep, false);
-                    copy_cell<Real, true>(dst, s0, n, v, 1);
+                if (!(consCrm > 0.0) || np <= 0) {   // nothing changes: no write-back
                     __syncwarp();
                     continue;
                 }
@@ -1159,7 +1112,6 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const StepArgs<Rea
             if (lane == 0 && (double)m > ccrm[ch]) a.crmax[cc[ch]] = (double)m;
             const int base = cbase[ch];
             Real* const v[4] = {arena + base, arena + N + base, arena + 2 * N + base, arena + 3 * N + base};
-            if constexpr (sample) sample_cell_warp<Real>(sa, cc[ch], v, cn[ch], istep, false);
             copy_cell<Real, true>(dst, cs0[ch], cn[ch], v, 1);
             __syncwarp();
             cc[ch] = -1;
@@ -1167,16 +1119,10 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const StepArgs<Rea
     }
 }
 
-template <typename Real, int MODE>
-__global__ void __launch_bounds__(kCellWarps * 32, 8) cell_kernel(StepArgs<Real> a)
+template <typename Real>
+__global__ void __launch_bounds__(kCellWarps * 32, 8) collide_kernel(StepArgs<Real> a)
 {
     extern __shared__ __align__(16) unsigned char cellSmem[];
-    // the arguments, in shared memory for the out-of-line per-cell helpers
-    // (a reference to the kernel parameter would make a per-thread copy)
-    __shared__ StepArgs<Real> sArgs;
-    if (threadIdx.x == 0) sArgs = a;
-    __syncthreads();
-    const StepArgs<Real>& sa = sArgs;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     unsigned char* wsm = cellSmem + (size_t)wib * warp_smem_bytes<Real>();
@@ -1185,54 +1131,39 @@ __global__ void __launch_bounds__(kCellWarps * 32, 8) cell_kernel(StepArgs<Real>
     int4* queue = reinterpret_cast<int4*>(wsm + (size_t)kArena * (4 * sizeof(Real) + sizeof(int)));
     Real* const stage[4] = {sv, sv + kSmallSlots, sv + 2 * kSmallSlots, sv + 3 * kSmallSlots};
     const int istep = a.ctl->istep;
-    constexpr bool gather = (MODE == kModeStep || MODE == kModeGather);
-    constexpr bool collide = (MODE == kModeStep || MODE == kModeCollide);
-    constexpr bool sample = (MODE == kModeStep || MODE == kModeSample || MODE == kModePre);
-    constexpr bool pre = (MODE == kModePre);
-    const PBuf<Real> dst = gather ? a.B : a.A;
-    const int* start = gather ? a.startB : a.startA;
+    const PBuf<Real> buf = a.A;
+    const int* start = a.startA;
     const int ncell = a.M.ncell;
-    const int nSrc = a.ctl->nLive + a.ctl->nInj;
     const int nHuge = a.cellWork[0], nLarge = a.cellWork[1], nSmall = a.cellWork[2];
     uint32_t pairs = 0, colls = 0, big = 0;
 
-    // ---- huge cells (and, without collisions, large cells), one at a time by the whole warp
+    // ---- huge cells, one at a time by the whole warp, in place
     int item = -1;
     for (;;) {
         int it = 0;
         if (lane == 0) it = atomicAdd(a.cellWork + 3, 1);
         it = __shfl_sync(kFull, it, 0);
         if (it >= nHuge + nLarge) break;
-        if (collide && it >= nHuge) {   // a large cell: the two-channel loop takes it
+        if (it >= nHuge) {   // a large cell: the two-channel loop takes it
             item = it;
             break;
         }
-        const int c = it < nHuge ? a.cellList[it] : a.cellList[ncell - 1 - (it - nHuge)];
+        const int c = a.cellList[it];
         const int s0 = start[c];
         const int n = start[c + 1] - s0;
-        Real* const v[4] = {dst.v[0] + s0, dst.v[1] + s0, dst.v[2] + s0, dst.ir + s0};
-        if constexpr (gather) {
-            gather_cell<Real>(sa, dst, c, s0, n, nSrc, v, 1);
-            if (lane == 0 && it < nHuge) ++big;
-        }
+        if (lane == 0) ++big;
+        collide_cell<Real>(buf.v[0] + s0, buf.v[1] + s0, buf.v[2] + s0, buf.ir + s0, buf.cell + s0, n, c, a, istep,
+                           pairs, colls);
         __syncwarp();
-        if constexpr (collide) {
-            collide_cell<Real>(v[0], v[1], v[2], v[3], dst.cell + s0, n, c, a, istep, pairs, colls);
-            __syncwarp();
-            for (int k = lane; k < n; k += 32) dst.cell[s0 + k] = c;
-        }
-        if constexpr (sample) sample_cell_warp<Real>(sa, c, v, n, istep, pre);
+        for (int k = lane; k < n; k += 32) buf.cell[s0 + k] = c;   // the claims used the cell ids
         __syncwarp();
     }
 
     // ---- large cells, two at a time
-    if constexpr (collide)
-        if (item >= 0)
-            collide_two_channels<Real, MODE>(a, sa, dst, start, sv, sclaim, queue, nHuge + nLarge, nHuge, istep, nSrc, item,
-                                             pairs, colls);
+    if (item >= 0)
+        collide_two_channels<Real>(a, buf, start, sv, sclaim, queue, nHuge + nLarge, nHuge, istep, item, pairs, colls);
 
     // ---- small cells, 32 per warp, one lane each
-    constexpr bool stagedSmall = collide;     // gather-only and sample-only work on the buffer
     for (;;) {
         int g = 0;
         if (lane == 0) g = atomicAdd(a.cellWork + 4, 32);
@@ -1242,44 +1173,23 @@ __global__ void __launch_bounds__(kCellWarps * 32, 8) cell_kernel(StepArgs<Real>
         const int myc = mine ? a.cellList[ncell + g + lane] : 0;
         const int ms0 = mine ? start[myc] : 0;
         const int mn = mine ? start[myc + 1] - ms0 : 0;
-        const unsigned mask = __ballot_sync(kFull, mine);
+        const unsigned mask = __ballot_sync(kFull, mine && mn > 1);
         for (unsigned m = mask; m; m &= m - 1) {
             const int l = __ffs(m) - 1;
-            const int s0 = __shfl_sync(kFull, ms0, l);
-            const int n = __shfl_sync(kFull, mn, l);
-            const int c = __shfl_sync(kFull, myc, l);
-            Real* const to[4] = {stagedSmall ? stage[0] + l : dst.v[0] + s0,
-                                 stagedSmall ? stage[1] + l : dst.v[1] + s0,
-                                 stagedSmall ? stage[2] + l : dst.v[2] + s0,
-                                 stagedSmall ? stage[3] + l : dst.ir + s0};
-            if constexpr (gather) gather_cell<Real>(sa, dst, c, s0, n, nSrc, to, stagedSmall ? 32 : 1);
-            else if constexpr (stagedSmall) copy_cell<Real, false>(dst, s0, n, to, 32);
+            Real* const to[4] = {stage[0] + l, stage[1] + l, stage[2] + l, stage[3] + l};
+            copy_cell<Real, false>(buf, __shfl_sync(kFull, ms0, l), __shfl_sync(kFull, mn, l), to, 32);
         }
         __syncwarp();
-        Real* const own[4] = {stagedSmall ? stage[0] + lane : dst.v[0] + ms0,
-                              stagedSmall ? stage[1] + lane : dst.v[1] + ms0,
-                              stagedSmall ? stage[2] + lane : dst.v[2] + ms0,
-                              stagedSmall ? stage[3] + lane : dst.ir + ms0};
-        const int ownStride = stagedSmall ? 32 : 1;
-        if constexpr (collide)
-            if (mine) collide_cell_serial<Real>(own[0], own[1], own[2], own[3], ownStride, mn, myc, a, istep, pairs,
-                                                colls);
-        if constexpr (sample) {
-            if (mine) {
-                double mom[18];
-                moment_partial<Real>(own[0], own[1], own[2], own[3], ownStride, mn, 0, 1, mom);
-                sample_cell<Real>(sa, myc, mom, istep, pre);
-            }
+        if ((mask >> lane) & 1u)
+            collide_cell_serial<Real>(stage[0] + lane, stage[1] + lane, stage[2] + lane, stage[3] + lane, 32, mn, myc,
+                                      a, istep, pairs, colls);
+        __syncwarp();
+        for (unsigned m = mask; m; m &= m - 1) {
+            const int l = __ffs(m) - 1;
+            Real* const from[4] = {stage[0] + l, stage[1] + l, stage[2] + l, stage[3] + l};
+            copy_cell<Real, true>(buf, __shfl_sync(kFull, ms0, l), __shfl_sync(kFull, mn, l), from, 32);
         }
         __syncwarp();
-        if constexpr (stagedSmall) {
-            for (unsigned m = mask; m; m &= m - 1) {
-                const int l = __ffs(m) - 1;
-                Real* const from[4] = {stage[0] + l, stage[1] + l, stage[2] + l, stage[3] + l};
-                copy_cell<Real, true>(dst, __shfl_sync(kFull, ms0, l), __shfl_sync(kFull, mn, l), from, 32);
-            }
-            __syncwarp();
-        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -1295,63 +1205,148 @@ __global__ void __launch_bounds__(kCellWarps * 32, 8) cell_kernel(StepArgs<Real>
 }
 
 // resident blocks per SM of each cell-kernel variant, set by prepare_kernels
-template <typename Real, int MODE>
+template <typename Real>
 struct CellOcc {
     static int blocks;
 };
-template <typename Real, int MODE>
-int CellOcc<Real, MODE>::blocks = 1;
-
-template <typename Real, int MODE>
-static cudaError_t prepare_cell_mode()
-{
-    cudaError_t e = cudaFuncSetAttribute(cell_kernel<Real, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)cell_smem_bytes<Real>());
-    if (e != cudaSuccess) return e;
-    int nb = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, cell_kernel<Real, MODE>, kCellWarps * 32,
-                                                      cell_smem_bytes<Real>());
-    if (e != cudaSuccess) return e;
-    CellOcc<Real, MODE>::blocks = nb > 0 ? nb : 1;
-    return cudaSuccess;
-}
-
-template <typename Real, int MODE>
-static void launch_cells_mode(const StepArgs<Real>& a, int smCount, cudaStream_t s)
-{
-    const int ncell = a.M.ncell;
-    const int* start = (MODE == kModeStep || MODE == kModeGather) ? a.startB : a.startA;
-    cudaMemsetAsync(a.cellWork, 0, 8 * sizeof(int), s);
-    int gc = (ncell + 255) / 256;
-    if (gc > smCount * 8) gc = smCount * 8;
-    classify_kernel<<<gc > 0 ? gc : 1, 256, 0, s>>>(start, ncell, Stage<Real>::N, a.cellList, a.cellWork);
-    int g = (ncell + kCellWarps - 1) / kCellWarps;
-    const int cap = smCount * CellOcc<Real, MODE>::blocks;
-    if (g > cap) g = cap;
-    cell_kernel<Real, MODE><<<g > 0 ? g : 1, kCellWarps * 32, cell_smem_bytes<Real>(), s>>>(a);
-}
+template <typename Real>
+int CellOcc<Real>::blocks = 1;
 
 template <typename Real>
 cudaError_t prepare_kernels()
 {
-    cudaError_t e;
-    if ((e = prepare_cell_mode<Real, kModeStep>()) != cudaSuccess) return e;
-    if ((e = prepare_cell_mode<Real, kModeGather>()) != cudaSuccess) return e;
-    if ((e = prepare_cell_mode<Real, kModeCollide>()) != cudaSuccess) return e;
-    if ((e = prepare_cell_mode<Real, kModeSample>()) != cudaSuccess) return e;
-    return prepare_cell_mode<Real, kModePre>();
+    cudaError_t e = cudaFuncSetAttribute(collide_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)cell_smem_bytes<Real>());
+    if (e != cudaSuccess) return e;
+    int nb = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, collide_kernel<Real>, kCellWarps * 32,
+                                                      cell_smem_bytes<Real>());
+    if (e != cudaSuccess) return e;
+    CellOcc<Real>::blocks = nb > 0 ? nb : 1;
+    return cudaSuccess;
 }
 
 template <typename Real>
-void launch_cells(const StepArgs<Real>& a, int mode, int smCount, cudaStream_t s)
+void launch_collide(const StepArgs<Real>& a, int smCount, cudaStream_t s)
 {
-    switch (mode) {
-        case kModeStep: launch_cells_mode<Real, kModeStep>(a, smCount, s); break;
-        case kModeGather: launch_cells_mode<Real, kModeGather>(a, smCount, s); break;
-        case kModeCollide: launch_cells_mode<Real, kModeCollide>(a, smCount, s); break;
-        case kModeSample: launch_cells_mode<Real, kModeSample>(a, smCount, s); break;
-        default: launch_cells_mode<Real, kModePre>(a, smCount, s); break;
+    const int ncell = a.M.ncell;
+    cudaMemsetAsync(a.cellWork, 0, 8 * sizeof(int), s);
+    int gc = (ncell + 255) / 256;
+    if (gc > smCount * 8) gc = smCount * 8;
+    classify_kernel<<<gc > 0 ? gc : 1, 256, 0, s>>>(a.startA, ncell, kArena, a.cellList, a.cellWork);
+    int g = (ncell + kCellWarps - 1) / kCellWarps;
+    const int cap = smCount * CellOcc<Real>::blocks;
+    if (g > cap) g = cap;
+    collide_kernel<Real><<<g > 0 ? g : 1, kCellWarps * 32, cell_smem_bytes<Real>(), s>>>(a);
+}
+
+// ===========================================================================
+// sampling
+// ===========================================================================
+
+// Raw moments of one cell's particles, summed in particle order with each
+// operation rounded on its own (the oracle's order and rounding).
+template <typename Real>
+__device__ __forceinline__ void cell_moments(const PBuf<Real>& b, int s0, int n, double m[18])
+{
+#pragma unroll
+    for (int k = 0; k < 18; ++k) m[k] = 0.0;
+    for (int k = s0; k < s0 + n; ++k) {
+        const double x = (double)b.v[0][k], y = (double)b.v[1][k], z = (double)b.v[2][k], I = (double)b.ir[k];
+        const double v2 = da(da(dm(x, x), dm(y, y)), dm(z, z));
+        m[0] = da(m[0], 1.0); m[1] = da(m[1], x); m[2] = da(m[2], y); m[3] = da(m[3], z); m[4] = da(m[4], v2);
+        m[5] = da(m[5], dm(x, x)); m[6] = da(m[6], dm(x, y)); m[7] = da(m[7], dm(y, y));
+        m[8] = da(m[8], dm(y, z)); m[9] = da(m[9], dm(z, z)); m[10] = da(m[10], dm(z, x));
+        m[11] = da(m[11], dm(x, v2)); m[12] = da(m[12], dm(y, v2)); m[13] = da(m[13], dm(z, v2));
+        m[14] = da(m[14], I); m[15] = da(m[15], dm(x, I)); m[16] = da(m[16], dm(y, I)); m[17] = da(m[17], dm(z, I));
     }
+}
+
+// Fold one step's moments of cell c into its accumulators, by one thread:
+// statistic_macro, src/ProcessDSMC.cpp:2784-2859 (statistic_macroPre,
+// :3312-3326, when pre).
+template <typename Real>
+__device__ __forceinline__ void sample_cell(const StepArgs<Real>& a, int c, const double* mom, int istep, bool pre)
+{
+    const double S = a.M.cellVolume[c];
+    if (a.stepMom)
+        for (int k = 0; k < 18; ++k) a.stepMom[(size_t)c * 18 + k] = mom[k];
+    if (pre) {
+        double out[18];
+        local_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
+        for (int k = 0; k < 18; ++k) a.local[(size_t)c * 18 + k] = out[k];
+        record_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
+        for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
+        return;
+    }
+    double* acc = a.acc + (size_t)c * 54;
+    const bool every = (istep % a.C.nevery) == 0;
+    // updateStepWindowMoments, :3106-3113
+    const double na = (double)a.C.nscheme;
+    const double w = (istep <= a.C.nscheme) ? 1.0 : dd(ds(na, 1.0), na);
+    const bool steady = istep > a.C.nss;
+    for (int k = 0; k < 18; ++k) {
+        const double v = mom[k];
+        const double s = acc[k];
+        acc[k] = (w == 1.0) ? da(s, v) : da(dm(w, s), v);
+        if (steady) acc[18 + k] = da(acc[18 + k], v);
+        if (every) acc[36 + k] = da(acc[36 + k], v);
+    }
+    const int ngsis = a.C.nevery * a.C.nrepeat;
+    unsigned char st = a.sparseState[c];
+    int accum = a.sparseAccum[c];
+    if (every && (st == 1 || st == 2)) {
+        if (accum < 0) accum = 0;
+        ++accum;
+    }
+    if (ngsis > 0 && istep % ngsis == 0) {
+        const double* inter = acc + 36;
+        const double ws = inter[0];
+        const bool finite = isfinite(ws);
+        bool sparse = (st == 1 || st == 2);
+        if (!sparse && finite && ws < 3.0) {
+            st = 1;
+            accum = a.C.nrepeat > 1 ? a.C.nrepeat : 1;
+            sparse = true;
+        }
+        const bool valid = (ws >= 3.0) && finite;
+        a.windowSamples[c] = ws;
+        a.windowValid[c] = valid ? 1 : 0;
+        double out[18];
+        if (sparse) {
+            averaged_macro(inter, (double)(accum > 1 ? accum : 1), S, a.C.neff, a.C.nref, a.C.dr, out);
+            for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
+        } else if (valid) {
+            averaged_macro(inter, (double)a.C.nrepeat, S, a.C.neff, a.C.nref, a.C.dr, out);
+            for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
+        }
+        if (!sparse)
+            for (int k = 0; k < 18; ++k) acc[36 + k] = 0.0;
+    }
+    a.sparseState[c] = st;
+    a.sparseAccum[c] = accum;
+}
+
+// statistic_macro / statistic_macroPre over the sorted buffer: one thread
+// per cell.
+template <typename Real>
+__global__ void __launch_bounds__(128) sample_kernel(StepArgs<Real> a, int pre)
+{
+    const int istep = a.ctl->istep;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < a.M.ncell; c += gridDim.x * blockDim.x) {
+        const int s0 = a.startA[c];
+        double mom[18];
+        cell_moments<Real>(a.A, s0, a.startA[c + 1] - s0, mom);
+        sample_cell<Real>(a, c, mom, istep, pre != 0);
+    }
+}
+
+template <typename Real>
+void launch_sample(const StepArgs<Real>& a, bool pre, int smCount, cudaStream_t s)
+{
+    int g = (a.M.ncell + 127) / 128;
+    if (g > smCount * 16) g = smCount * 16;
+    sample_kernel<Real><<<g > 0 ? g : 1, 128, 0, s>>>(a, pre ? 1 : 0);
 }
 
 // ===========================================================================
@@ -1430,7 +1425,8 @@ void launch_trace_check(const DevMesh& M, const DevConsts& C, int n, const Real*
     template void launch_inject<Real>(const StepArgs<Real>&, int, cudaStream_t);                                 \
     template void launch_move<Real>(const StepArgs<Real>&, int, cudaStream_t);                                   \
     template void launch_sort<Real>(const StepArgs<Real>&, int, cudaStream_t);                                   \
-    template void launch_cells<Real>(const StepArgs<Real>&, int, int, cudaStream_t);                             \
+    template void launch_collide<Real>(const StepArgs<Real>&, int, cudaStream_t);                                \
+    template void launch_sample<Real>(const StepArgs<Real>&, bool, int, cudaStream_t);                           \
     template cudaError_t prepare_kernels<Real>();                                                                \
     template void launch_trace_check<Real>(const DevMesh&, const DevConsts&, int, const Real*, const Real*,       \
                                            const Real*, const Real*, const Real*, const Real*, const double*,    \

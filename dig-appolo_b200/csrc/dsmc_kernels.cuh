@@ -73,17 +73,11 @@ struct StepArgs {
 
 constexpr int kScanBlocks = 296;
 
-// cell-kernel modes
-constexpr int kModeStep = 0;       // gather A->B + collide + sample (fused step)
-constexpr int kModeGather = 1;     // gather only (cache2chain)
-constexpr int kModeCollide = 2;    // collide in place on A
-constexpr int kModeSample = 3;     // sample in place on A
-constexpr int kModePre = 4;        // statistic_macroPre on A
-
 template <typename Real> void launch_inject(const StepArgs<Real>& a, int smCount, cudaStream_t s);
 template <typename Real> void launch_move(const StepArgs<Real>& a, int smCount, cudaStream_t s);
 template <typename Real> void launch_sort(const StepArgs<Real>& a, int smCount, cudaStream_t s);
-template <typename Real> void launch_cells(const StepArgs<Real>& a, int mode, int smCount, cudaStream_t s);
+template <typename Real> void launch_collide(const StepArgs<Real>& a, int smCount, cudaStream_t s);
+template <typename Real> void launch_sample(const StepArgs<Real>& a, bool pre, int smCount, cudaStream_t s);
 template <typename Real> cudaError_t prepare_kernels();
 void launch_macro(const DevMesh& M, const DevConsts& C, const double* acc, int set, double count,
                   double* out, int ncell, cudaStream_t s);
