@@ -7,12 +7,17 @@ step summed over the timed steps, divided by the device time (CUDA events on
 the library's stream, max over ranks). Mixed precision is the production
 path; the all-FP64 path is timed on the same case for the mixed/FP64 ratio.
 
+Default workload: the capsule case (Ma 5, Kn 0.01, AoA 30 deg) on the
+generated 371,214-tet mesh at 100 particles per cell (37.1M particles);
+--workload block runs the 48,640-hex block case (200 particles per cell by
+default).
+
 Multi-GPU runs are independent replicas (one case per GPU, no collective on
 the data path): value = the sum of all ranks' particle-steps / the slowest
 rank's time.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload block|capsule]
-                  [--ppc P] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload capsule|block]
+                  [--ppc P] [--impl ours|reference] [--no-cpu-baseline]
 """
 from __future__ import annotations
 
@@ -78,20 +83,49 @@ def make_workload(name: str, ppc: int):
 
 
 def algorithmic_bytes(n_particles: float, ncell: int, ntri_per_cell: float, mixed: bool) -> dict:
-    """Algorithmic bytes of one step and of one move launch.
+    """Algorithmic bytes of one step and of one launch of each stage's main
+    kernel.
 
-    Per particle the state is read and written once: 32 B (mixed: x, v, Ir
-    as FP32 + cell id) or 60 B (FP64: x, v, Ir as FP64 + cell id). The move
-    launch reads each cell's triangles once (9 words + 8 B of face id/tag
-    per triangle); a step adds the per-cell collision and sampling state
-    (3 x 18 FP64 accumulators + crmax + 2 remainders, read and written)."""
+    - step: each particle's state read and written once, 32 B (mixed: x, v,
+      Ir as FP32 + cell id) or 60 B (FP64: x, v, Ir as FP64 + cell id); each
+      cell's triangles read once (9 words + 8 B of face id/tag per
+      triangle); the per-cell collision and sampling state (3 x 18 FP64
+      accumulators + crmax + 2 remainders) read and written.
+    - move: the particle state read and written, the triangles read.
+    - collide: velocities and internal energy read and written (16 B mixed,
+      32 B FP64 per particle); crmax and the collision remainder read and
+      written, the cell volume and the cell's start read.
+    - sample: velocities and internal energy read; the accumulators read and
+      written and the record fields written (18 FP64) per cell.
+    - sort (gather): the state read from the source and written to the
+      sorted slot, plus the source index."""
     sp = 32 if mixed else 60
     word = 4 if mixed else 8
+    vi = 4 * word
     geom = ntri_per_cell * (9 * word + 8)
     acc = 3 * 18 * 8 + 3 * 8
     move = n_particles * 2 * sp + ncell * geom
     step = move + ncell * 2 * acc
-    return {"move": move, "step": step, "per_particle_state": sp, "geom_per_cell": geom}
+    collide = n_particles * 2 * vi + ncell * (2 * 8 + 2 * 8 + 8 + 4)
+    sample = n_particles * vi + ncell * (2 * 54 * 8 + 18 * 8 + 4)
+    sort = n_particles * (2 * sp + 4)
+    return {"step": step, "move": move, "collide": collide, "sample": sample, "sort": sort, "inject": None,
+            "per_particle_state": sp, "geom_per_cell": geom}
+
+
+def measured_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of a kernel on this workload from the committed
+    ncu summary (profiles/<kernel>_<workload>.md, line
+    'dram_bytes_per_launch: N'), or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.strip().startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].strip().split()[0]), os.path.relpath(path, ROOT)
+    except OSError:
+        pass
+    return None, None
 
 
 # ---------------------------------------------------------------------------
@@ -260,14 +294,18 @@ def run_ours(args):
     e2e_ps = sum_over_ranks(e2e["particle_steps"])
     case_m.close()
 
-    ntri = dm.ncell and (sum(1 for _ in []) or None)
     tri_per_cell = 12.0 if wl["name"] == "block" else 4.0
     n_mean = 0.5 * (mixed["n0"] + mixed["n1"])
     ab = algorithmic_bytes(n_mean, dm.ncell, tri_per_cell, mixed=True)
-    names = ["inject", "move", "sort", "collide_sample"]
-    dom = int(np.argmax(stage_avg))
-    dom_bytes = {"move": ab["move"]}.get(names[dom], None)
-    achieved = (ab["move"] / (stage_avg[1] / 1e3)) / 1e9 if stage_avg[1] > 0 else None
+    names = ["inject", "move", "sort", "collide", "sample"]
+    kernels = {"inject": "inject_gen_kernel", "move": "move_kernel", "sort": "gather_kernel",
+               "collide": "collide_kernel", "sample": "sample_kernel"}
+    dom = names[int(np.argmax(stage_avg))]
+    dom_ms = float(stage_avg[names.index(dom)])
+    dom_bytes = ab.get(dom)
+    achieved = (dom_bytes / (dom_ms / 1e3)) / 1e9 if (dom_bytes and dom_ms > 0) else None
+    traffic, traffic_src = measured_traffic(kernels[dom], wl["desc"]["workload"] + f"_ppc{args.ppc}")
+    step_achieved = (ab["step"] / (ms_mixed / args.steps / 1e3)) / 1e9
     line = {
         "metric": METRIC,
         "value": value,
@@ -286,10 +324,12 @@ def run_ours(args):
         "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / args.steps, "dtype": "f64"},
         "mixed_over_fp64": value / value_fp64 if value_fp64 > 0 else None,
         "stage_ms_per_step": dict(zip(names, [float(x) for x in stage_avg])),
-        "roofline": {"bound": "hbm", "kernel": "move", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
-                     "peak_kind": peak_kind, "algorithmic_bytes_per_launch": ab["move"],
-                     "dominant_stage": names[dom]},
+        "roofline": {"bound": "hbm", "kernel": kernels[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "traffic_source": traffic_src, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
+                     "step": {"algorithmic_bytes": ab["step"], "achieved": step_achieved,
+                              "frac": step_achieved / peak}},
         "e2e": {"value": e2e_ps / (e2e_ms / 1e3), "unit": "particle-steps/s",
                 "h2d_bytes_per_step": e2e["h2d"] / args.steps, "d2h_bytes_per_step": e2e["d2h"] / args.steps},
         "gpu_launches": None,
@@ -307,9 +347,9 @@ def run_ours(args):
 
 
 def launches_per_step(wl) -> int:
-    # inject: count, scan, generate; move; sort: rank, scan x2, scatter;
-    # cells: classify and the cell kernel
-    return 3 + 1 + 4 + 2
+    # inject: count, scan, generate; move; sort: rank, scan x2, scatter,
+    # far-slot order, gather; collide: classify, collide; sample
+    return 3 + 1 + 6 + 2 + 1
 
 
 def run_e2e(wl, fill, args, rank):
@@ -420,13 +460,15 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="block")
-    ap.add_argument("--ppc", type=int, default=200)
+    ap.add_argument("--workload", default="capsule")
+    ap.add_argument("--ppc", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.ppc is None:
+        args.ppc = 100 if args.workload == "capsule" else 200
     if args.impl == "reference":
         run_reference(args)
     else:

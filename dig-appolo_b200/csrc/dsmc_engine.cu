@@ -152,8 +152,8 @@ struct Engine {
 
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool timing = false;
-    cudaEvent_t ev[5] = {};
-    double stageMs[4] = {0, 0, 0, 0};
+    cudaEvent_t ev[6] = {};
+    double stageMs[5] = {0, 0, 0, 0, 0};
     int64_t timedSteps = 0;
 
     ~Engine() { release(); }
@@ -843,8 +843,9 @@ struct Engine {
             b.A = a.B; b.B = a.A; b.startA = a.startB; b.startB = const_cast<int*>(a.startA);
         }
         if (coll) launch_collide<Real>(b, smCount, stream);
-        if (samp) launch_sample<Real>(b, false, smCount, stream);
         if (events) cudaEventRecord(ev[4], stream);
+        if (samp) launch_sample<Real>(b, false, smCount, stream);
+        if (events) cudaEventRecord(ev[5], stream);
     }
 
     template <typename Real>
@@ -870,8 +871,8 @@ struct Engine {
             enqueue<Real>(stages, timing);
             if (!cuda(cudaGetLastError(), "kernel launch")) return false;
             if (timing) {
-                if (!cuda(cudaEventSynchronize(ev[4]), "timing sync")) return false;
-                for (int k = 0; k < 4; ++k) {
+                if (!cuda(cudaEventSynchronize(ev[5]), "timing sync")) return false;
+                for (int k = 0; k < 5; ++k) {
                     float ms = 0.0f;
                     cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
                     stageMs[k] += ms;
@@ -1365,11 +1366,11 @@ int dsmc_set_timing(DsmcHandle* h, int32_t on)
     return DSMC_OK;
 }
 
-int dsmc_stage_ms(DsmcHandle* h, double* ms4, int64_t* nsteps, int32_t reset)
+int dsmc_stage_ms(DsmcHandle* h, double* ms5, int64_t* nsteps, int32_t reset)
 {
     DSMC_GUARD(h);
-    if (ms4)
-        for (int k = 0; k < 4; ++k) ms4[k] = h->e.stageMs[k];
+    if (ms5)
+        for (int k = 0; k < 5; ++k) ms5[k] = h->e.stageMs[k];
     if (nsteps) *nsteps = h->e.timedSteps;
     if (reset) {
         for (double& v : h->e.stageMs) v = 0.0;

@@ -289,7 +289,7 @@ class Case:
         self._check(self.lib.dsmc_set_timing(self.h, int(on)), "dsmc_set_timing")
 
     def stage_ms(self, reset: bool = False):
-        ms = np.zeros(4)
+        ms = np.zeros(5)
         n = C.c_int64()
         self._check(self.lib.dsmc_stage_ms(self.h, _ptr(ms), C.byref(n), int(reset)), "dsmc_stage_ms")
         return ms, int(n.value)

@@ -292,11 +292,12 @@ int dsmc_trace_noalloc(DsmcHandle* h, int64_t n,
 
 /* Stage timing: with on != 0, dsmc_step runs its kernels without a CUDA
  * graph and records CUDA events between the stages; dsmc_stage_ms then
- * returns the device time of [inject, move, sort, collide+sample] summed
- * over the timed steps since the last reset (reset != 0 clears the sums
- * after reading). Off (the default) replays one captured graph per step. */
+ * returns the device time of [inject, move, sort, collide, sample] (ms5[5])
+ * summed over the timed steps since the last reset (reset != 0 clears the
+ * sums after reading). Off (the default) replays one captured graph per
+ * step. */
 int dsmc_set_timing(DsmcHandle* h, int32_t on);
-int dsmc_stage_ms(DsmcHandle* h, double* ms4, int64_t* nsteps, int32_t reset);
+int dsmc_stage_ms(DsmcHandle* h, double* ms5, int64_t* nsteps, int32_t reset);
 
 /* The CUDA stream the handle's work runs on (a cudaStream_t). */
 void* dsmc_stream(DsmcHandle* h);
