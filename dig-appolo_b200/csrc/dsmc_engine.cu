@@ -243,6 +243,10 @@ struct Engine {
         precision = params.precision;
         if (precision != DSMC_PRECISION_FP64 && precision != DSMC_PRECISION_MIXED) return fail("bad precision");
         if (params.nevery <= 0 || params.nrepeat <= 0 || params.nscheme <= 0) return fail("bad sampling controls");
+        if (params.nzones < 0 || params.nzones > DSMC_MAX_ZONES) return fail("nzones outside [0, DSMC_MAX_ZONES]");
+        for (int z = 0; z < params.nzones; ++z)
+            if (params.zone_role[z] < DSMC_ROLE_NONE || params.zone_role[z] > DSMC_ROLE_SPECULAR)
+                return fail("unknown zone role");
         if (params.max_crossings <= 0) params.max_crossings = 4096;
         if (!(mess.dtime > 0.0) || !(mess.Neff > 0.0) || !(mess.v_rms > 0.0)) return fail("bad mesh message");
         if (dev >= 0) {

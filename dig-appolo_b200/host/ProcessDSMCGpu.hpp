@@ -1,0 +1,275 @@
+// ProcessDSMCGpu: the reference's ProcessDSMC interface for the DSMC
+// particle step (src/ProcessDSMC.h:441-492), on the B200 library's C-ABI
+// (include/dsmc_gpu.h). Header only, C++17; link with -ldsmcgpu.
+//
+// Same member names and argument meaning as the reference:
+//   preprocesseffquad(istep), advection(istep), cache2chain(),
+//   collisionDSMC(), statistic_macro(istep), statistic_macroPre(),
+//   out2dat(istep), outBoundaryStressHeat(istep)
+// and the per-cell fields the host GSIS step reads (local, record,
+// final_record, [ncell][18] in MacroIndex order). One object owns one
+// device-resident case (all cells of the mesh: one domain).
+//
+// Errors: the reference prints and aborts (e.g. src/ProcessDSMC.cpp:874);
+// here a failed call throws DsmcError carrying the library's message
+// (dsmc_last_error), and the object stays usable where the library allows.
+#pragma once
+
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <fstream>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "dsmc_gpu.h"
+
+namespace dsmc_b200 {
+
+class DsmcError : public std::runtime_error {
+public:
+    explicit DsmcError(const std::string& m) : std::runtime_error(m) {}
+};
+
+// Particles as structure-of-arrays host vectors (cell_particles_curr
+// flattened; src/MeshparticalInitial.h:229).
+struct Particles {
+    std::vector<double> x, y, z, vx, vy, vz, ir;
+    std::vector<int32_t> cell;
+    size_t size() const { return cell.size(); }
+};
+
+// One wall face of outBoundaryStressHeat's output
+// (src/ProcessDSMC.cpp:3498-3550): normal (outward), pressure, shear
+// vector, stress vector, translational / rotational / total heat flux,
+// normalised by n_ref like the reference's Fluent sections.
+struct WallFaceFields {
+    int face = -1;
+    double normal[3] = {0.0, 0.0, 0.0};
+    double pressure = 0.0;
+    double shear[3] = {0.0, 0.0, 0.0};
+    double stress[3] = {0.0, 0.0, 0.0};
+    double qTrans = 0.0, qRot = 0.0, qTotal = 0.0;
+};
+
+class ProcessDSMCGpu {
+public:
+    static constexpr int Madata = DSMC_MACRO_WIDTH;   // MacroIndex count (src/ProcessDSMC.h:28-49)
+
+    // The mesh arrays are the reference's own (DsmcCell, DsmcEdge,
+    // localPointXY, faceSplitTag after rootCaptureGlobalDsmcAndReleaseMesh);
+    // they are copied at construction.
+    ProcessDSMCGpu(const DsmcMeshDesc& mesh, const DsmcMeshMessage& mess, const DsmcCaseParams& params,
+                   int device = 0)
+        : mess_(mess), params_(params), ncell_(mesh.ncell), nface_(mesh.nface),
+          edges_(mesh.edges, mesh.edges + mesh.nface)
+    {
+        if (dsmc_create(&mesh, &mess, &params, device, &h_) != DSMC_OK)
+            throw DsmcError(std::string("dsmc_create: ") + dsmc_last_error(nullptr));
+    }
+    ~ProcessDSMCGpu()
+    {
+        if (h_) dsmc_destroy(h_);
+    }
+    ProcessDSMCGpu(const ProcessDSMCGpu&) = delete;
+    ProcessDSMCGpu& operator=(const ProcessDSMCGpu&) = delete;
+    ProcessDSMCGpu(ProcessDSMCGpu&& o) noexcept { *this = std::move(o); }
+    ProcessDSMCGpu& operator=(ProcessDSMCGpu&& o) noexcept
+    {
+        if (this != &o) {
+            if (h_) dsmc_destroy(h_);
+            h_ = o.h_; o.h_ = nullptr;
+            mess_ = o.mess_; params_ = o.params_; ncell_ = o.ncell_; nface_ = o.nface_;
+            edges_ = std::move(o.edges_);
+        }
+        return *this;
+    }
+
+    // ---- particles
+    void uploadParticles(const Particles& p)
+    {
+        check(dsmc_upload_particles(h_, (int64_t)p.size(), p.x.data(), p.y.data(), p.z.data(), p.vx.data(),
+                                    p.vy.data(), p.vz.data(), p.ir.data(), p.cell.data()),
+              "dsmc_upload_particles");
+    }
+    int64_t particleCount() const
+    {
+        int64_t n = 0;
+        check(dsmc_particle_count(h_, &n), "dsmc_particle_count");
+        return n;
+    }
+    Particles downloadParticles() const
+    {
+        const int64_t n = particleCount();
+        Particles p;
+        for (auto* v : {&p.x, &p.y, &p.z, &p.vx, &p.vy, &p.vz, &p.ir}) v->resize((size_t)n);
+        p.cell.resize((size_t)n);
+        check(dsmc_download_particles(h_, n, p.x.data(), p.y.data(), p.z.data(), p.vx.data(), p.vy.data(),
+                                      p.vz.data(), p.ir.data(), p.cell.data(), nullptr),
+              "dsmc_download_particles");
+        return p;
+    }
+
+    // ---- the reference's step (src/meshImportTest.cpp:207-234)
+    void preprocesseffquad(int istep) { check(dsmc_preprocesseffquad(h_, istep), "preprocesseffquad"); }
+    void advection(int istep) { check(dsmc_advection(h_, istep), "advection"); }
+    void cache2chain() { check(dsmc_cache2chain(h_), "cache2chain"); }
+    void collisionDSMC() { check(dsmc_collisionDSMC(h_), "collisionDSMC"); }
+    void statistic_macro(int istep) { check(dsmc_statistic_macro(h_, istep), "statistic_macro"); }
+    void statistic_macroPre() { check(dsmc_statistic_macroPre(h_), "statistic_macroPre"); }
+    // the five calls above as one CUDA-graph replay (same kernels, same bits)
+    void step(int istep) { check(dsmc_step(h_, istep, DSMC_STAGE_ALL), "dsmc_step"); }
+
+    // ---- fields for the host GSIS step, [ncell][18] FP64 in MacroIndex order
+    std::vector<double> local() const { return macro(DSMC_MACRO_LOCAL); }
+    std::vector<double> record() const { return macro(DSMC_MACRO_RECORD); }
+    std::vector<double> final_record() const { return macro(DSMC_MACRO_FINAL_RECORD); }
+    std::vector<int32_t> particlesPerCell() const
+    {
+        std::vector<int32_t> ppc((size_t)ncell_);
+        check(dsmc_download_counts(h_, ppc.data(), nullptr, nullptr, nullptr, nullptr, nullptr), "counts");
+        return ppc;
+    }
+    std::vector<unsigned char> sparseState() const
+    {
+        std::vector<unsigned char> st((size_t)ncell_);
+        check(dsmc_download_counts(h_, nullptr, nullptr, nullptr, st.data(), nullptr, nullptr), "counts");
+        return st;
+    }
+
+    // The field set out2dat writes (src/ProcessDSMC.cpp:3338-3377): record
+    // up to NSS and for sparse cells (states 1, 2), final_record after.
+    std::vector<double> out2datFields(int istep) const
+    {
+        std::vector<double> rec = record();
+        if (istep <= params_.nss) return rec;
+        const std::vector<double> fin = final_record();
+        const std::vector<unsigned char> st = sparseState();
+        for (int c = 0; c < ncell_; ++c) {
+            if (st[(size_t)c] == 1 || st[(size_t)c] == 2) continue;
+            for (int j = 0; j < Madata; ++j) rec[(size_t)c * Madata + j] = fin[(size_t)c * Madata + j];
+        }
+        return rec;
+    }
+
+    // out2dat (src/ProcessDSMC.cpp:3338-3438): writes the fields of
+    // out2datFields, one line per cell (cell id, 18 values). The reference
+    // writes them through meshImport::out2Fluent_dsmc as a Fluent data file;
+    // that writer is not part of this library.
+    bool out2dat(int istep, const std::string& path) const
+    {
+        const std::vector<double> w = out2datFields(istep);
+        std::ofstream f(path);
+        if (!f) return false;
+        f.precision(16);
+        for (int c = 0; c < ncell_; ++c) {
+            f << c;
+            for (int j = 0; j < Madata; ++j) f << ' ' << w[(size_t)c * Madata + j];
+            f << '\n';
+        }
+        return (bool)f;
+    }
+
+    // outBoundaryStressHeat's conversion (src/ProcessDSMC.cpp:3451-3550):
+    // steady wall tallies (hits, momentum and energy deltas, accumulated
+    // after NSS) to pressure, shear and heat flux per wall face, scaled by
+    // 2 Neff / (dt * steps) / area / n_ref. Only faces whose zone is a
+    // diffuse wall are returned.
+    std::vector<WallFaceFields> boundaryStressHeat(int istep) const
+    {
+        std::vector<double> raw((size_t)nface_ * 6);
+        check(dsmc_download_wall(h_, raw.data()), "dsmc_download_wall");
+        const bool steady = istep > params_.nss;
+        const double sampleSteps = steady ? (double)(istep - params_.nss) : 1.0;
+        const double timeScale = (mess_.dtime > 0.0 && sampleSteps > 0.0) ? mess_.Neff / (mess_.dtime * sampleSteps) : 0.0;
+        std::vector<WallFaceFields> out;
+        for (int f = 0; f < nface_; ++f) {
+            const DsmcEdgeRec& e = edges_[(size_t)f];
+            if (roleOf(e.faceTag) != DSMC_ROLE_WALL) continue;
+            WallFaceFields w;
+            w.face = f;
+            double n[3] = {e.edgeNormal[0], e.edgeNormal[1], e.edgeNormal[2]};
+            const double len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+            if (len > 0.0 && std::isfinite(len)) {
+                for (double& v : n) v /= len;
+            } else {
+                n[0] = 1.0; n[1] = 0.0; n[2] = 0.0;
+            }
+            const double ni[3] = {-n[0], -n[1], -n[2]};
+            const double* in = &raw[(size_t)f * 6];
+            const double pn = in[1] * ni[0] + in[2] * ni[1] + in[3] * ni[2];
+            const double pt[3] = {in[1] - pn * ni[0], in[2] - pn * ni[1], in[3] - pn * ni[2]};
+            const double area = (e.length > 0.0 && std::isfinite(e.length)) ? e.length : 1.0;
+            const double scale = (area > 0.0 && mess_.n_ref > 0.0) ? 2.0 * timeScale / area / mess_.n_ref : 0.0;
+            for (int d = 0; d < 3; ++d) w.normal[d] = n[d];
+            w.pressure = pn * scale;
+            for (int d = 0; d < 3; ++d) w.shear[d] = -pt[d] * scale;
+            for (int d = 0; d < 3; ++d) w.stress[d] = w.pressure * w.normal[d] + w.shear[d];
+            w.qTrans = -in[4] * scale;
+            w.qRot = -in[5] * scale;
+            w.qTotal = w.qTrans + w.qRot;
+            out.push_back(w);
+        }
+        return out;
+    }
+
+    // outBoundaryStressHeat: the fields above, one line per wall face
+    // (face id, normal, pressure, shear, stress, q_trans, q_rot, q_total).
+    // The reference writes them as Fluent 700-706 sections; that writer is
+    // not part of this library. Returns true (nothing written) when wall
+    // statistics are off, like the reference.
+    bool outBoundaryStressHeat(int istep, const std::string& path) const
+    {
+        if (!params_.wall_stats) return true;
+        const std::vector<WallFaceFields> w = boundaryStressHeat(istep);
+        std::ofstream f(path);
+        if (!f) return false;
+        f.precision(16);
+        for (const WallFaceFields& x : w) {
+            f << x.face << ' ' << x.normal[0] << ' ' << x.normal[1] << ' ' << x.normal[2] << ' ' << x.pressure;
+            for (double v : x.shear) f << ' ' << v;
+            for (double v : x.stress) f << ' ' << v;
+            f << ' ' << x.qTrans << ' ' << x.qRot << ' ' << x.qTotal << '\n';
+        }
+        return (bool)f;
+    }
+
+    DsmcCounters counters() const
+    {
+        DsmcCounters c{};
+        check(dsmc_get_counters(h_, &c), "dsmc_get_counters");
+        return c;
+    }
+    void sync() const { check(dsmc_sync(h_), "dsmc_sync"); }
+    DsmcHandle* handle() const { return h_; }
+    int ncell() const { return ncell_; }
+
+private:
+    std::vector<double> macro(int which) const
+    {
+        std::vector<double> out((size_t)ncell_ * Madata);
+        check(dsmc_download_macro(h_, which, out.data()), "dsmc_download_macro");
+        return out;
+    }
+    int roleOf(int tag) const
+    {
+        for (int k = 0; k < params_.nzones; ++k)
+            if (params_.zone_tag[k] == tag) return params_.zone_role[k];
+        return DSMC_ROLE_NONE;
+    }
+    void check(int status, const char* what) const
+    {
+        if (status != DSMC_OK) throw DsmcError(std::string(what) + ": " + dsmc_last_error(h_));
+    }
+
+    DsmcHandle* h_ = nullptr;
+    DsmcMeshMessage mess_{};
+    DsmcCaseParams params_{};
+    int ncell_ = 0, nface_ = 0;
+    std::vector<DsmcEdgeRec> edges_;
+};
+
+}  // namespace dsmc_b200

@@ -1,0 +1,132 @@
+"""The C++ host layer (dig-appolo_b200/host/ProcessDSMCGpu.hpp), the
+reference's ProcessDSMC interface over the C-ABI.
+
+CPU: the header and tests/cpp/host_driver.cpp compile with g++ and link
+against the built library.
+GPU: the driver runs the block case through the reference's stage calls
+(and through the fused step) and gives the same bits as the Python binding
+of the same C-ABI; an invalid case raises DsmcError with the library's
+message; the wall-field conversion matches outBoundaryStressHeat's formula
+(src/ProcessDSMC.cpp:3494-3550) evaluated here on the downloaded tallies.
+"""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+import inputs as I
+from gpu_util import make_case
+from pydsmc import gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_DIR = os.path.join(ROOT, "dig-appolo_b200", "lib")
+
+
+def _compile(out_dir):
+    exe = os.path.join(out_dir, "host_driver")
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror",
+           "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "dig-appolo_b200", "host"),
+           os.path.join(ROOT, "tests", "cpp", "host_driver.cpp"), "-o", exe,
+           "-L", LIB_DIR, "-ldsmcgpu", f"-Wl,-rpath,{LIB_DIR}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_host_layer_compiles_and_links(tmp_path):
+    if not shutil.which("g++"):
+        pytest.skip("no g++")
+    if not os.path.exists(os.path.join(LIB_DIR, "libdsmcgpu.so")):
+        pytest.skip("library not built")
+    exe = _compile(str(tmp_path))
+    assert os.path.exists(exe)
+
+
+def _write_case(d, dm, mess, params, x, v, ir, cell):
+    with open(os.path.join(d, "case.txt"), "w") as f:
+        f.write(f"{dm.ncell} {dm.nface} {dm.npoint} {len(cell)}\n")
+    np.ascontiguousarray(dm.cells).tofile(os.path.join(d, "cells.bin"))
+    np.ascontiguousarray(dm.edges).tofile(os.path.join(d, "edges.bin"))
+    np.ascontiguousarray(dm.points, dtype=np.float64).tofile(os.path.join(d, "points.bin"))
+    np.ascontiguousarray(dm.split, dtype=np.uint8).tofile(os.path.join(d, "split.bin"))
+    np.ascontiguousarray(mess).tofile(os.path.join(d, "mess.bin"))
+    with open(os.path.join(d, "params.bin"), "wb") as f:
+        f.write(bytes(params))
+    for k, a in (("x", x[:, 0]), ("y", x[:, 1]), ("z", x[:, 2]), ("vx", v[:, 0]), ("vy", v[:, 1]), ("vz", v[:, 2]),
+                 ("ir", ir)):
+        np.ascontiguousarray(a, dtype=np.float64).tofile(os.path.join(d, f"{k}.bin"))
+    np.ascontiguousarray(cell, dtype=np.int32).tofile(os.path.join(d, "cell.bin"))
+
+
+def _wall_fields(dm, mess, zones, tally, istep, nss):
+    """outBoundaryStressHeat's conversion, src/ProcessDSMC.cpp:3494-3550."""
+    role = {t: r for t, r, _ in zones}
+    ts = float(mess["Neff"]) / (float(mess["dtime"]) * (istep - nss if istep > nss else 1.0))
+    rows = []
+    for f in range(dm.nface):
+        e = dm.edges[f]
+        if role.get(int(e["faceTag"]), 0) != gpu.ROLE_WALL:
+            continue
+        n = np.array(e["edgeNormal"], dtype=float)
+        n = n / np.linalg.norm(n)
+        ni = -n
+        t = tally[f]
+        pn = t[1:4] @ ni
+        pt = t[1:4] - pn * ni
+        scale = 2.0 * ts / float(e["length"]) / float(mess["n_ref"])
+        p = pn * scale
+        sh = -pt * scale
+        rows.append([f, *n, p, *sh, *(p * n + sh), -t[4] * scale, -t[5] * scale, -(t[4] + t[5]) * scale])
+    return np.array(rows)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fused", [0, 1])
+def test_host_layer_matches_python_binding(block, tmp_path, fused):
+    raw, dm, mess = block
+    x, v, ir, cell = I.fill_inputs(dm, mess, 20, seed=5)
+    nsteps, nss = 6, 2
+    params = gpu.default_params(precision=gpu.PRECISION_FP64, seed=17, zones=I.REF_ZONES, inflow_dir=I.inflow_dir(),
+                                nss=nss, nscheme=3, nevery=1, nrepeat=2, wall_stats=1)
+    d = str(tmp_path)
+    _write_case(d, dm, mess, params, x, v, ir, cell)
+    exe = _compile(d)
+    r = subprocess.run([exe, d, str(nsteps), str(fused)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    with make_case(dm, mess, seed=17, nss=nss, nscheme=3, nevery=1, nrepeat=2, wall_stats=1) as case:
+        case.upload_particles(x, v, ir, cell)
+        case.statistic_macroPre()
+        for s in range(1, nsteps + 1):
+            case.step(s)
+        xg, vg, irg, cg = case.download_particles()
+        local = case.macro(gpu.MACRO_LOCAL)
+        record = case.macro(gpu.MACRO_RECORD)
+        final = case.macro(gpu.MACRO_FINAL_RECORD)
+        tally = case.wall()
+        sparse_state = case.counts()["sparse_state"]
+    n = len(cg)
+    got = {k: np.fromfile(os.path.join(d, f"out_{k}.bin"), dtype=np.float64) for k in
+           ("x", "y", "z", "vx", "vy", "vz", "ir")}
+    assert np.array_equal(np.fromfile(os.path.join(d, "out_cell.bin"), dtype=np.int32), cg)
+    assert np.array_equal(np.stack([got["x"], got["y"], got["z"]], 1), xg)
+    assert np.array_equal(np.stack([got["vx"], got["vy"], got["vz"]], 1), vg)
+    assert np.array_equal(got["ir"], irg)
+    assert len(got["x"]) == n
+    for k, ref in (("local", local), ("record", record), ("final", final)):
+        assert np.array_equal(np.fromfile(os.path.join(d, f"out_{k}.bin")).reshape(ref.shape), ref, equal_nan=True), k
+    # out2dat after NSS: final_record except for sparse cells
+    o2d = np.fromfile(os.path.join(d, "out_out2dat.bin")).reshape(final.shape)
+    sparse = (sparse_state == 1) | (sparse_state == 2)
+    assert np.array_equal(o2d[~sparse], final[~sparse], equal_nan=True)
+    assert np.array_equal(o2d[sparse], record[sparse], equal_nan=True)
+    # wall fields
+    wall = np.loadtxt(os.path.join(d, "out_wall.txt"), ndmin=2)
+    want = _wall_fields(dm, mess, I.REF_ZONES, tally, nsteps, nss)
+    assert wall.shape == want.shape
+    assert np.array_equal(wall[:, 0], want[:, 0])
+    assert np.allclose(wall[:, 1:], want[:, 1:], rtol=1e-12, atol=1e-300)
+    assert (tally[:, 0] > 0).sum() > 0
+    err = open(os.path.join(d, "out_error.txt")).read()
+    assert "nzones" in err
