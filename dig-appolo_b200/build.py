@@ -3,7 +3,9 @@
 ``libdsmcgpu.so`` is compiled by nvcc for sm_100a only (no PTX for other
 targets, no multi-arch), with the host side at ``-ffp-contract=off`` so the
 host-built mesh caches and inflow constants are evaluated in the reference's
-operation order. The result lands in ``dig-appolo_b200/lib/``.
+operation order. FP32 device arithmetic flushes subnormals (``-ftz=true``):
+the FP32 path's operands (cell-relative positions, velocities, energies) are
+far from the subnormal range, and FP64 is unaffected. The result lands in ``dig-appolo_b200/lib/``.
 """
 from __future__ import annotations
 
@@ -33,7 +35,7 @@ def nvcc() -> str:
 
 def common_flags() -> list[str]:
     return [
-        "-O3", "-std=c++17", "-lineinfo",
+        "-O3", "-std=c++17", "-lineinfo", "-ftz=true",
         "-gencode", "arch=compute_100a,code=sm_100a",
         "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
         "-I", os.path.join(ROOT, "include"), "-I", CSRC,

@@ -1119,8 +1119,11 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
     }
 }
 
+// Nine resident blocks (18 warps) per SM: the arena (22.5 KB per block plus
+// the 1 KB the runtime reserves) fits nine in 228 KB; the bound caps the
+// registers to match (113 per thread).
 template <typename Real>
-__global__ void __launch_bounds__(kCellWarps * 32, 8) collide_kernel(StepArgs<Real> a)
+__global__ void __launch_bounds__(kCellWarps * 32, 9) collide_kernel(StepArgs<Real> a)
 {
     extern __shared__ __align__(16) unsigned char cellSmem[];
     const int lane = threadIdx.x & 31;
