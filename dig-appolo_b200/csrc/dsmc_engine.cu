@@ -151,6 +151,9 @@ struct Engine {
     int hostNLive = 0;
 
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    LaunchShape shape;             // launch shapes (dsmc_set_launch_shape, dsmc_autotune)
+    int generation = 0;            // bumped whenever captured graphs become stale
+    bool devIstepValid = false;    // ctl->istep on the device equals curIstep
     bool timing = false;
     cudaEvent_t ev[6] = {};
     double stageMs[5] = {0, 0, 0, 0, 0};
@@ -256,6 +259,7 @@ struct Engine {
             return false;
         }
         cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, device);
+        shape.smCount = smCount;
         if (!cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
         ncell = md->ncell;
         nface = md->nface;
@@ -770,6 +774,7 @@ struct Engine {
         rank = nullptr; idx = nullptr;
         for (auto& g : graph)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        ++generation;
         const int64_t cap = need;
         for (int b = 0; b < 2; ++b)
             for (int k = 0; k < 8; ++k) {
@@ -827,16 +832,16 @@ struct Engine {
     {
         const StepArgs<Real> a = args<Real>();
         if (events) cudaEventRecord(ev[0], stream);
-        if (stages & DSMC_STAGE_INJECT) launch_inject<Real>(a, smCount, stream);
+        if (stages & DSMC_STAGE_INJECT) launch_inject<Real>(a, shape, stream);
         if (events) cudaEventRecord(ev[1], stream);
-        if (stages & DSMC_STAGE_MOVE) launch_move<Real>(a, smCount, stream);
+        if (stages & DSMC_STAGE_MOVE) launch_move<Real>(a, shape, stream);
         if (events) cudaEventRecord(ev[2], stream);
         const bool sort = (stages & DSMC_STAGE_SORT) != 0;
         const bool coll = (stages & DSMC_STAGE_COLLIDE) != 0;
         const bool samp = (stages & DSMC_STAGE_SAMPLE) != 0;
         if (sort) {
             // rank, scan, scatter, far-slot order, gather into B
-            launch_sort<Real>(a, smCount, stream);
+            launch_sort<Real>(a, shape, stream);
             cudaMemcpyAsync(&ctl->nLive, &ctl->nNext, sizeof(int), cudaMemcpyDeviceToDevice, stream);
             cudaMemsetAsync(&ctl->nInj, 0, sizeof(int), stream);
         }
@@ -846,9 +851,9 @@ struct Engine {
         if (sort) {
             b.A = a.B; b.B = a.A; b.startA = a.startB; b.startB = const_cast<int*>(a.startA);
         }
-        if (coll) launch_collide<Real>(b, smCount, stream);
+        if (coll) launch_collide<Real>(b, shape, stream);
         if (events) cudaEventRecord(ev[4], stream);
-        if (samp) launch_sample<Real>(b, false, smCount, stream);
+        if (samp) launch_sample<Real>(b, false, shape, stream);
         if (events) cudaEventRecord(ev[5], stream);
     }
 
@@ -859,6 +864,7 @@ struct Engine {
         if (stages & ~DSMC_STAGE_ALL) return fail("unknown stage flags");
         if (!setIstep(istep)) return false;
         curIstep = istep;
+        devIstepValid = true;
         const bool full = stages == DSMC_STAGE_ALL;
         if (full && !timing && std::getenv("DSMC_NO_GRAPH") == nullptr) {
             if (!graph[cur]) {
@@ -902,11 +908,129 @@ struct Engine {
         return precision == DSMC_PRECISION_MIXED ? stepT<float>(istep, stages) : stepT<double>(istep, stages);
     }
 
+    void dropGraphs()
+    {
+        for (auto& g : graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        ++generation;
+    }
+
+    bool setShape(const DsmcLaunchShape& s)
+    {
+        if (s.move_threads != 128 && s.move_threads != 256 && s.move_threads != 512)
+            return fail("launch shape: move_threads must be 128, 256 or 512");
+        if (s.move_blocks_per_sm < 1 || s.move_blocks_per_sm > 32 || s.sort_blocks_per_sm < 1 ||
+            s.sort_blocks_per_sm > 32 || s.collide_blocks_per_sm < 1 || s.collide_blocks_per_sm > 32)
+            return fail("launch shape: blocks per SM outside [1, 32]");
+        // work already queued keeps the shape it was launched with
+        shape.moveThreads = s.move_threads;
+        shape.moveBlocksPerSm = s.move_blocks_per_sm;
+        shape.sortBlocksPerSm = s.sort_blocks_per_sm;
+        shape.collideBlocksPerSm = s.collide_blocks_per_sm;
+        dropGraphs();
+        return true;
+    }
+
+    DsmcLaunchShape getShape() const
+    {
+        DsmcLaunchShape s;
+        s.move_threads = shape.moveThreads;
+        s.move_blocks_per_sm = shape.moveBlocksPerSm;
+        s.sort_blocks_per_sm = shape.sortBlocksPerSm;
+        s.collide_blocks_per_sm = shape.collideBlocksPerSm;
+        return s;
+    }
+
+    // The autotuner: runs full steps of this case from step `istep` on,
+    // timing each stage with events, and keeps per stage the fastest of a
+    // few launch shapes (move: block size x blocks per SM; rank / scatter /
+    // gather: blocks per SM; collide: blocks per SM). Since no kernel's
+    // result depends on its launch shape, the steps it runs are ordinary
+    // steps of the case; on return `istep` is the next step to run.
+    bool autotune(int& istep, int trialSteps)
+    {
+        if (trialSteps < 1) return fail("autotune: trial_steps < 1");
+        const bool wasTiming = timing;
+        timing = true;
+        auto trial = [&](const DsmcLaunchShape& cand, int stage, double& ms) -> bool {
+            if (!setShape(cand)) return false;
+            for (double& v : stageMs) v = 0.0;
+            timedSteps = 0;
+            for (int k = 0; k < trialSteps; ++k)
+                if (!step(istep++, DSMC_STAGE_ALL)) return false;
+            ms = stageMs[stage] / (double)trialSteps;
+            return true;
+        };
+        DsmcLaunchShape best = getShape();
+        bool ok = step(istep++, DSMC_STAGE_ALL);   // one untimed-order step to warm the caches
+        double bestMs = 0.0;
+        if (ok) ok = trial(best, 1, bestMs);
+        const int threads[3] = {128, 256, 512};
+        const int blocks[4] = {2, 4, 8, 16};
+        for (int t = 0; ok && t < 3; ++t)
+            for (int b = 0; ok && b < 4; ++b) {
+                DsmcLaunchShape c = best;
+                c.move_threads = threads[t];
+                c.move_blocks_per_sm = blocks[b] * 256 / threads[t] > 0 ? blocks[b] * 256 / threads[t] : 1;
+                if (c.move_threads == best.move_threads && c.move_blocks_per_sm == best.move_blocks_per_sm) continue;
+                double ms = 0.0;
+                ok = trial(c, 1, ms);
+                if (ok && ms < bestMs) { bestMs = ms; best = c; }
+            }
+        if (ok) ok = trial(best, 2, bestMs);
+        for (int b = 0; ok && b < 4; ++b) {
+            DsmcLaunchShape c = best;
+            c.sort_blocks_per_sm = blocks[b];
+            if (c.sort_blocks_per_sm == best.sort_blocks_per_sm) continue;
+            double ms = 0.0;
+            ok = trial(c, 2, ms);
+            if (ok && ms < bestMs) { bestMs = ms; best = c; }
+        }
+        if (ok) ok = trial(best, 3, bestMs);
+        const int cblocks[3] = {3, 6, 9};
+        for (int b = 0; ok && b < 3; ++b) {
+            DsmcLaunchShape c = best;
+            c.collide_blocks_per_sm = cblocks[b];
+            if (c.collide_blocks_per_sm == best.collide_blocks_per_sm) continue;
+            double ms = 0.0;
+            ok = trial(c, 3, ms);
+            if (ok && ms < bestMs) { bestMs = ms; best = c; }
+        }
+        timing = wasTiming;
+        for (double& v : stageMs) v = 0.0;
+        timedSteps = 0;
+        if (!ok) return false;
+        return setShape(best);
+    }
+
+    // ---- batched steps (DsmcBatch): one full step on the handle's stream,
+    // the step counter advanced on the device, recorded into the batch graph
+    template <typename Real>
+    void enqueueBatchT()
+    {
+        launch_bump_istep(ctl, stream);
+        enqueue<Real>(DSMC_STAGE_ALL, false);
+    }
+    void enqueueBatch()
+    {
+        if (precision == DSMC_PRECISION_MIXED) enqueueBatchT<float>();
+        else enqueueBatchT<double>();
+    }
+    void afterBatchStep()
+    {
+        ++curIstep;
+        cur ^= 1;
+        pendingInject = false;
+        localLazy = true;
+        lastIstep = curIstep;
+        ++steps;
+    }
+
     bool macroPre()
     {
         if (!haveParticles) return fail("no particles uploaded");
-        if (precision == DSMC_PRECISION_MIXED) launch_sample<float>(args<float>(), true, smCount, stream);
-        else launch_sample<double>(args<double>(), true, smCount, stream);
+        if (precision == DSMC_PRECISION_MIXED) launch_sample<float>(args<float>(), true, shape, stream);
+        else launch_sample<double>(args<double>(), true, shape, stream);
         localLazy = false;
         return cuda(cudaGetLastError(), "statistic_macroPre");
     }
@@ -986,6 +1110,7 @@ struct Engine {
         if (!cuda(cudaStreamSynchronize(stream), "upload sync")) return false;
         hostNLive = (int)n;
         haveParticles = true;
+        devIstepValid = false;
         pendingInject = false;
         return true;
     }
@@ -1393,10 +1518,11 @@ int dsmc_sync(DsmcHandle* h)
     return status_of(e, ok);
 }
 
-}  // extern "C"
 
 // Read-only views of a handle for the no-allocation entry point
 // (dsmc_noalloc.cu).
+}  // extern "C"
+
 namespace dsmc {
 DevMesh engine_mesh(const DsmcHandle* h) { return h->e.M; }
 DevConsts engine_consts(const DsmcHandle* h) { return h->e.C; }
@@ -1406,3 +1532,209 @@ cudaStream_t engine_stream(const DsmcHandle* h) { return h->e.stream; }
 unsigned long long* engine_counters(const DsmcHandle* h) { return h->e.counters; }
 void engine_set_error(DsmcHandle* h, const char* msg) { h->e.err = msg; }
 }  // namespace dsmc
+
+extern "C" {
+
+// ---------------------------------------------------------------------------
+// launch shapes and the autotuner
+// ---------------------------------------------------------------------------
+int dsmc_get_launch_shape(DsmcHandle* h, DsmcLaunchShape* out)
+{
+    DSMC_GUARD(h);
+    if (!out) return DSMC_E_INVALID;
+    *out = h->e.getShape();
+    return DSMC_OK;
+}
+
+int dsmc_set_launch_shape(DsmcHandle* h, const DsmcLaunchShape* shape)
+{
+    DSMC_GUARD(h);
+    if (!shape) return DSMC_E_INVALID;
+    return h->e.setShape(*shape) ? DSMC_OK : DSMC_E_INVALID;
+}
+
+int dsmc_autotune(DsmcHandle* h, int32_t first_istep, int32_t trial_steps, int32_t* next_istep,
+                  DsmcLaunchShape* chosen)
+{
+    DSMC_GUARD(h);
+    int istep = first_istep;
+    const bool ok = h->e.autotune(istep, trial_steps);
+    if (next_istep) *next_istep = istep;
+    if (chosen) *chosen = h->e.getShape();
+    return status_of(h->e, ok);
+}
+
+// ---------------------------------------------------------------------------
+// batched steps
+// ---------------------------------------------------------------------------
+struct DsmcBatch {
+    std::vector<DsmcHandle*> cases;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t done = nullptr;
+    std::vector<cudaEvent_t> join;
+    struct Cached {
+        std::vector<int> key;
+        cudaGraphExec_t exec = nullptr;
+    };
+    std::vector<Cached> graphs;
+    std::string err;
+
+    ~DsmcBatch()
+    {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        for (auto e : join)
+            if (e) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        if (done) cudaEventDestroy(done);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    bool fail(const std::string& m)
+    {
+        err = m;
+        return false;
+    }
+    bool cuda(cudaError_t e, const char* what)
+    {
+        if (e == cudaSuccess) return true;
+        return fail(std::string(what) + ": " + cudaGetErrorString(e));
+    }
+    // the graph state of every case: buffer parity and graph generation
+    std::vector<int> key() const
+    {
+        std::vector<int> k;
+        k.reserve(cases.size() * 2);
+        for (DsmcHandle* h : cases) {
+            k.push_back(h->e.cur);
+            k.push_back(h->e.generation);
+        }
+        return k;
+    }
+    bool capture(cudaGraphExec_t& exec)
+    {
+        cudaGraph_t g = nullptr;
+        if (!cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "batch capture")) return false;
+        cudaEventRecord(fork, stream);
+        for (size_t k = 0; k < cases.size(); ++k) {
+            dsmc::Engine& e = cases[k]->e;
+            cudaStreamWaitEvent(e.stream, fork, 0);
+            e.enqueueBatch();
+            cudaEventRecord(join[k], e.stream);
+            cudaStreamWaitEvent(stream, join[k], 0);
+        }
+        if (!cuda(cudaStreamEndCapture(stream, &g), "batch end capture")) return false;
+        const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        return cuda(ie, "batch graph instantiate");
+    }
+    bool step(int nsteps)
+    {
+        if (nsteps < 0) return fail("negative step count");
+        if (nsteps == 0) return true;
+        for (DsmcHandle* h : cases) {
+            dsmc::Engine& e = h->e;
+            if (!e.haveParticles) return fail("a case of the batch has no particles");
+            if (e.timing) return fail("a case of the batch is in timing mode");
+            if (!e.devIstepValid) {
+                if (!e.setIstep(e.curIstep)) return fail("istep: " + e.err);
+                e.devIstepValid = true;
+            }
+            // the batch stream starts after the work already queued on each case
+            cudaEventRecord(done, e.stream);
+            cudaStreamWaitEvent(stream, done, 0);
+        }
+        for (int s = 0; s < nsteps; ++s) {
+            const std::vector<int> k = key();
+            cudaGraphExec_t exec = nullptr;
+            for (auto& c : graphs)
+                if (c.key == k) exec = c.exec;
+            if (!exec) {
+                if (graphs.size() >= 4) {   // stale entries (a case was re-uploaded)
+                    cudaStreamSynchronize(stream);
+                    cudaGraphExecDestroy(graphs.front().exec);
+                    graphs.erase(graphs.begin());
+                }
+                if (!capture(exec)) return false;
+                graphs.push_back(Cached{k, exec});
+            }
+            if (!cuda(cudaGraphLaunch(exec, stream), "batch graph launch")) return false;
+            for (DsmcHandle* h : cases) h->e.afterBatchStep();
+        }
+        // later work on each case's own stream follows the batch
+        cudaEventRecord(done, stream);
+        for (DsmcHandle* h : cases) cudaStreamWaitEvent(h->e.stream, done, 0);
+        return cuda(cudaGetLastError(), "batch step");
+    }
+};
+
+int dsmc_batch_create(DsmcHandle* const* cases, int32_t n, DsmcBatch** out)
+{
+    if (!out) return DSMC_E_INVALID;
+    *out = nullptr;
+    if (!cases || n < 1) {
+        g_createError = "dsmc_batch_create: no cases";
+        return DSMC_E_INVALID;
+    }
+    for (int32_t k = 0; k < n; ++k) {
+        if (!cases[k]) {
+            g_createError = "dsmc_batch_create: null case handle";
+            return DSMC_E_INVALID;
+        }
+        if (cases[k]->e.device != cases[0]->e.device) {
+            g_createError = "dsmc_batch_create: cases on different devices";
+            return DSMC_E_INVALID;
+        }
+        for (int32_t j = 0; j < k; ++j)
+            if (cases[j] == cases[k]) {
+                g_createError = "dsmc_batch_create: a case appears twice";
+                return DSMC_E_INVALID;
+            }
+    }
+    DsmcBatch* b = new (std::nothrow) DsmcBatch();
+    if (!b) return DSMC_E_NOMEM;
+    b->cases.assign(cases, cases + n);
+    b->device = cases[0]->e.device;
+    cudaSetDevice(b->device);
+    bool ok = b->cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "batch stream") &&
+              b->cuda(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "batch event") &&
+              b->cuda(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "batch event");
+    b->join.assign((size_t)n, nullptr);
+    for (int32_t k = 0; ok && k < n; ++k)
+        ok = b->cuda(cudaEventCreateWithFlags(&b->join[(size_t)k], cudaEventDisableTiming), "batch event");
+    if (!ok) {
+        g_createError = b->err;
+        delete b;
+        return DSMC_E_CUDA;
+    }
+    *out = b;
+    return DSMC_OK;
+}
+
+void dsmc_batch_destroy(DsmcBatch* b) { delete b; }
+
+const char* dsmc_batch_last_error(const DsmcBatch* b) { return b ? b->err.c_str() : g_createError.c_str(); }
+
+int dsmc_batch_step(DsmcBatch* b, int32_t nsteps)
+{
+    if (!b) return DSMC_E_INVALID;
+    cudaSetDevice(b->device);
+    return b->step(nsteps) ? DSMC_OK : DSMC_E_STATE;
+}
+
+void* dsmc_batch_stream(DsmcBatch* b) { return b ? (void*)b->stream : nullptr; }
+
+int dsmc_batch_sync(DsmcBatch* b)
+{
+    if (!b) return DSMC_E_INVALID;
+    cudaSetDevice(b->device);
+    if (!b->cuda(cudaStreamSynchronize(b->stream), "batch sync")) return DSMC_E_CUDA;
+    for (DsmcHandle* h : b->cases)
+        if (!h->e.checkDeviceErrors()) return b->fail(h->e.err), status_of(h->e, false);
+    return DSMC_OK;
+}
+
+}  // extern "C"

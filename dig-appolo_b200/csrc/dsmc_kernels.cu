@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(128) inject_gen_kernel(StepArgs<Real> a)
 }
 
 template <typename Real>
-void launch_inject(const StepArgs<Real>& a, int smCount, cudaStream_t s)
+void launch_inject(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s)
 {
     if (a.P.npatch == 0) {
         cudaMemsetAsync(&a.ctl->nInj, 0, sizeof(int), s);
@@ -203,14 +203,14 @@ void launch_inject(const StepArgs<Real>& a, int smCount, cudaStream_t s)
     const int gCount = (a.P.ngroup + 127) / 128;
     inject_count_kernel<<<gCount > 0 ? gCount : 1, 128, 0, s>>>(a.P, a.remInj);
     inject_scan_kernel<<<1, 1024, 0, s>>>(a.P, a.ctl, a.counters);
-    inject_gen_kernel<Real><<<smCount * 8, 128, 0, s>>>(a);
+    inject_gen_kernel<Real><<<L.smCount * 8, 128, 0, s>>>(a);
 }
 
 // ===========================================================================
 // move
 // ===========================================================================
 template <typename Real>
-__global__ void __launch_bounds__(256) move_kernel(StepArgs<Real> a)
+__global__ void __launch_bounds__(512) move_kernel(StepArgs<Real> a)
 {
     const int istep = a.ctl->istep;
     const int n = a.ctl->nLive;
@@ -243,10 +243,16 @@ __global__ void __launch_bounds__(256) move_kernel(StepArgs<Real> a)
 }
 
 template <typename Real>
-void launch_move(const StepArgs<Real>& a, int smCount, cudaStream_t s)
+void launch_move(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s)
 {
-    move_kernel<Real><<<smCount * 8, 256, 0, s>>>(a);
+    move_kernel<Real><<<L.smCount * L.moveBlocksPerSm, L.moveThreads, 0, s>>>(a);
 }
+
+// advance the step counter on the device (batched steps, where the graph
+// carries no host-written step number)
+__global__ void bump_istep_kernel(StepCtl* ctl) { ctl->istep += 1; }
+
+void launch_bump_istep(StepCtl* ctl, cudaStream_t s) { bump_istep_kernel<<<1, 1, 0, s>>>(ctl); }
 
 // ===========================================================================
 // sort: rank, scan, scatter
@@ -560,14 +566,15 @@ __global__ void __launch_bounds__(256) gather_kernel(StepArgs<Real> a)
 }
 
 template <typename Real>
-void launch_sort(const StepArgs<Real>& a, int smCount, cudaStream_t s)
+void launch_sort(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s)
 {
-    rank_kernel<Real><<<smCount * 8, 256, 0, s>>>(a);
+    const int g = L.smCount * L.sortBlocksPerSm;
+    rank_kernel<Real><<<g, 256, 0, s>>>(a);
     scan_partial_kernel<<<kScanBlocks, 256, 0, s>>>(a.countSlot, a.M.ncell, a.scanPartial);
     scan_final_kernel<<<kScanBlocks, 256, 0, s>>>(a.countSlot, a.M.ncell, a.scanPartial, a.startB, a.ctl);
-    scatter_kernel<Real><<<smCount * 8, 256, 0, s>>>(a);
-    farsort_kernel<<<smCount * 4, 256, 0, s>>>(a.countSlot, a.startB, a.idx, a.B.cell, a.M.ncell);
-    gather_kernel<Real><<<smCount * 8, 256, 0, s>>>(a);
+    scatter_kernel<Real><<<g, 256, 0, s>>>(a);
+    farsort_kernel<<<L.smCount * 4, 256, 0, s>>>(a.countSlot, a.startB, a.idx, a.B.cell, a.M.ncell);
+    gather_kernel<Real><<<g, 256, 0, s>>>(a);
 }
 
 // ===========================================================================
@@ -1230,15 +1237,15 @@ cudaError_t prepare_kernels()
 }
 
 template <typename Real>
-void launch_collide(const StepArgs<Real>& a, int smCount, cudaStream_t s)
+void launch_collide(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s)
 {
     const int ncell = a.M.ncell;
     cudaMemsetAsync(a.cellWork, 0, 8 * sizeof(int), s);
     int gc = (ncell + 255) / 256;
-    if (gc > smCount * 8) gc = smCount * 8;
+    if (gc > L.smCount * 8) gc = L.smCount * 8;
     classify_kernel<<<gc > 0 ? gc : 1, 256, 0, s>>>(a.startA, ncell, kArena, a.cellList, a.cellWork);
     int g = (ncell + kCellWarps - 1) / kCellWarps;
-    const int cap = smCount * CellOcc<Real>::blocks;
+    const int cap = L.smCount * min(CellOcc<Real>::blocks, max(1, L.collideBlocksPerSm));
     if (g > cap) g = cap;
     collide_kernel<Real><<<g > 0 ? g : 1, kCellWarps * 32, cell_smem_bytes<Real>(), s>>>(a);
 }
@@ -1345,10 +1352,10 @@ __global__ void __launch_bounds__(128) sample_kernel(StepArgs<Real> a, int pre)
 }
 
 template <typename Real>
-void launch_sample(const StepArgs<Real>& a, bool pre, int smCount, cudaStream_t s)
+void launch_sample(const StepArgs<Real>& a, bool pre, const LaunchShape& L, cudaStream_t s)
 {
     int g = (a.M.ncell + 127) / 128;
-    if (g > smCount * 16) g = smCount * 16;
+    if (g > L.smCount * 16) g = L.smCount * 16;
     sample_kernel<Real><<<g > 0 ? g : 1, 128, 0, s>>>(a, pre ? 1 : 0);
 }
 
@@ -1425,11 +1432,11 @@ void launch_trace_check(const DevMesh& M, const DevConsts& C, int n, const Real*
 }
 
 #define DSMC_INSTANTIATE(Real)                                                                                   \
-    template void launch_inject<Real>(const StepArgs<Real>&, int, cudaStream_t);                                 \
-    template void launch_move<Real>(const StepArgs<Real>&, int, cudaStream_t);                                   \
-    template void launch_sort<Real>(const StepArgs<Real>&, int, cudaStream_t);                                   \
-    template void launch_collide<Real>(const StepArgs<Real>&, int, cudaStream_t);                                \
-    template void launch_sample<Real>(const StepArgs<Real>&, bool, int, cudaStream_t);                           \
+    template void launch_inject<Real>(const StepArgs<Real>&, const LaunchShape&, cudaStream_t);                  \
+    template void launch_move<Real>(const StepArgs<Real>&, const LaunchShape&, cudaStream_t);                    \
+    template void launch_sort<Real>(const StepArgs<Real>&, const LaunchShape&, cudaStream_t);                    \
+    template void launch_collide<Real>(const StepArgs<Real>&, const LaunchShape&, cudaStream_t);                 \
+    template void launch_sample<Real>(const StepArgs<Real>&, bool, const LaunchShape&, cudaStream_t);            \
     template cudaError_t prepare_kernels<Real>();                                                                \
     template void launch_trace_check<Real>(const DevMesh&, const DevConsts&, int, const Real*, const Real*,       \
                                            const Real*, const Real*, const Real*, const Real*, const double*,    \

@@ -73,11 +73,23 @@ struct StepArgs {
 
 constexpr int kScanBlocks = 296;
 
-template <typename Real> void launch_inject(const StepArgs<Real>& a, int smCount, cudaStream_t s);
-template <typename Real> void launch_move(const StepArgs<Real>& a, int smCount, cudaStream_t s);
-template <typename Real> void launch_sort(const StepArgs<Real>& a, int smCount, cudaStream_t s);
-template <typename Real> void launch_collide(const StepArgs<Real>& a, int smCount, cudaStream_t s);
-template <typename Real> void launch_sample(const StepArgs<Real>& a, bool pre, int smCount, cudaStream_t s);
+// Launch shapes of the step's kernels. Every kernel loops over its work
+// (grid-stride or dynamic hand-out) and draws from counter-based streams, so
+// results do not depend on these; only the speed does.
+struct LaunchShape {
+    int smCount = 148;
+    int moveThreads = 256;        // threads per block of the move kernel: 128, 256, 512
+    int moveBlocksPerSm = 8;      // move grid = smCount x this
+    int sortBlocksPerSm = 8;      // rank, scatter, gather grids = smCount x this
+    int collideBlocksPerSm = 9;   // collide grid cap per SM (at most the resident blocks)
+};
+
+template <typename Real> void launch_inject(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s);
+template <typename Real> void launch_move(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s);
+template <typename Real> void launch_sort(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s);
+template <typename Real> void launch_collide(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s);
+template <typename Real> void launch_sample(const StepArgs<Real>& a, bool pre, const LaunchShape& L, cudaStream_t s);
+void launch_bump_istep(StepCtl* ctl, cudaStream_t s);
 template <typename Real> cudaError_t prepare_kernels();
 void launch_macro(const DevMesh& M, const DevConsts& C, const double* acc, int set, double count,
                   double* out, int ncell, cudaStream_t s);

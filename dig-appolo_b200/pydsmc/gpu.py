@@ -59,6 +59,14 @@ class Counters(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in COUNTER_NAMES]
 
 
+class LaunchShape(C.Structure):
+    _fields_ = [("move_threads", C.c_int32), ("move_blocks_per_sm", C.c_int32),
+                ("sort_blocks_per_sm", C.c_int32), ("collide_blocks_per_sm", C.c_int32)]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
 _lib = None
 
 # (name, restype, argtypes) for every entry point of include/dsmc_gpu.h
@@ -91,6 +99,15 @@ _SIGS = [
     ("dsmc_stage_ms", C.c_int, [_P, _P, C.POINTER(C.c_int64), C.c_int32]),
     ("dsmc_stream", C.c_void_p, [_P]),
     ("dsmc_sync", C.c_int, [_P]),
+    ("dsmc_get_launch_shape", C.c_int, [_P, _P]),
+    ("dsmc_set_launch_shape", C.c_int, [_P, _P]),
+    ("dsmc_autotune", C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int32), _P]),
+    ("dsmc_batch_create", C.c_int, [_P, C.c_int32, C.POINTER(C.c_void_p)]),
+    ("dsmc_batch_destroy", None, [_P]),
+    ("dsmc_batch_last_error", C.c_char_p, [_P]),
+    ("dsmc_batch_step", C.c_int, [_P, C.c_int32]),
+    ("dsmc_batch_stream", C.c_void_p, [_P]),
+    ("dsmc_batch_sync", C.c_int, [_P]),
 ]
 EXPORTED = [s[0] for s in _SIGS]
 
@@ -311,3 +328,70 @@ class Case:
                     "dsmc_trace_noalloc" if noalloc else "dsmc_trace")
         return {"cell": oi[0], "ifout": oi[1], "face": oi[2], "tri": oi[3], "ncross": oi[4],
                 "x": np.stack(of[:3], 1), "v": np.stack(of[3:6], 1), "dt": of[6]}
+
+    # -- launch shapes ----------------------------------------------------------
+    def launch_shape(self) -> dict:
+        sh = LaunchShape()
+        self._check(self.lib.dsmc_get_launch_shape(self.h, C.byref(sh)), "dsmc_get_launch_shape")
+        return sh.as_dict()
+
+    def set_launch_shape(self, **kw):
+        sh = LaunchShape()
+        self._check(self.lib.dsmc_get_launch_shape(self.h, C.byref(sh)), "dsmc_get_launch_shape")
+        for k, v in kw.items():
+            setattr(sh, k, v)
+        self._check(self.lib.dsmc_set_launch_shape(self.h, C.byref(sh)), "dsmc_set_launch_shape")
+
+    def autotune(self, first_istep: int, trial_steps: int = 2):
+        """Run steps first_istep, ... while timing launch shapes; returns
+        (next step to run, shape kept)."""
+        nxt = C.c_int32()
+        sh = LaunchShape()
+        self._check(self.lib.dsmc_autotune(self.h, first_istep, trial_steps, C.byref(nxt), C.byref(sh)),
+                    "dsmc_autotune")
+        return int(nxt.value), sh.as_dict()
+
+
+class Batch:
+    """Independent cases on one device stepped together: each batch step is
+    one CUDA graph whose branches are the cases' steps (dsmc_batch_*)."""
+
+    def __init__(self, cases):
+        self.lib = load()
+        self.cases = list(cases)
+        arr = (C.c_void_p * len(self.cases))(*[c.h for c in self.cases])
+        b = C.c_void_p()
+        rc = self.lib.dsmc_batch_create(arr, len(self.cases), C.byref(b))
+        if rc != 0:
+            raise DsmcError(f"dsmc_batch_create failed ({rc}): {self.lib.dsmc_batch_last_error(None).decode()}")
+        self.b = b
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise DsmcError(f"{what} failed ({rc}): {self.lib.dsmc_batch_last_error(self.b).decode()}")
+
+    def step(self, nsteps: int = 1):
+        self._check(self.lib.dsmc_batch_step(self.b, nsteps), "dsmc_batch_step")
+
+    def sync(self):
+        self._check(self.lib.dsmc_batch_sync(self.b), "dsmc_batch_sync")
+
+    def stream(self):
+        return self.lib.dsmc_batch_stream(self.b)
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.lib.dsmc_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -305,6 +305,57 @@ void* dsmc_stream(DsmcHandle* h);
 /* Synchronise the handle's stream and report kernel-side errors. */
 int dsmc_sync(DsmcHandle* h);
 
+/* ---------------------------------------------------------------------------
+ * Launch shapes and the autotuner. No reference counterpart: the reference
+ * runs on CPU cores. Every kernel loops over its work and draws from
+ * counter-based random streams, so the shape changes the speed of a step,
+ * never its result.
+ * ------------------------------------------------------------------------- */
+typedef struct DsmcLaunchShape {
+    int32_t move_threads;          /* threads per block of the move kernel: 128, 256 or 512 */
+    int32_t move_blocks_per_sm;    /* move grid = SMs x this, 1..32 (particles per thread follow) */
+    int32_t sort_blocks_per_sm;    /* rank / scatter / gather grids = SMs x this, 1..32 */
+    int32_t collide_blocks_per_sm; /* cap on the collision grid per SM, 1..32 (at most the resident blocks) */
+} DsmcLaunchShape;
+
+int dsmc_get_launch_shape(DsmcHandle* h, DsmcLaunchShape* out);
+/* Takes effect for steps enqueued after the call (captured graphs are rebuilt). */
+int dsmc_set_launch_shape(DsmcHandle* h, const DsmcLaunchShape* shape);
+
+/* Runs full steps first_istep, first_istep+1, ... of the case, timing each
+ * stage, and keeps per stage the fastest of a few shapes (move: block size
+ * x blocks per SM; sort: blocks per SM; collide: blocks per SM). The steps
+ * are ordinary steps of the case (about 20 x trial_steps of them);
+ * *next_istep receives the next step to run, *chosen the shape kept. */
+int dsmc_autotune(DsmcHandle* h, int32_t first_istep, int32_t trial_steps, int32_t* next_istep,
+                  DsmcLaunchShape* chosen);
+
+/* ---------------------------------------------------------------------------
+ * Batched steps: many independent cases (handles on one device, each with
+ * its own mesh, constants, particles and step counter) advanced together,
+ * each step of all of them replayed as one CUDA graph whose branches run
+ * concurrently. No reference counterpart: the reference runs one case per
+ * MPI job.
+ * ------------------------------------------------------------------------- */
+typedef struct DsmcBatch DsmcBatch;
+
+/* The cases must be distinct handles on one device. The batch does not own
+ * them; destroy the batch before any of its cases. */
+int dsmc_batch_create(DsmcHandle* const* cases, int32_t n, DsmcBatch** out);
+void dsmc_batch_destroy(DsmcBatch* b);
+const char* dsmc_batch_last_error(const DsmcBatch* b);
+
+/* Advance every case by nsteps full steps; each case's steps continue its
+ * own count (the step after its last dsmc_step / stage call / batch step).
+ * Equal, bit for bit, to stepping each case on its own. Asynchronous: work
+ * queued afterwards on a case's own stream follows the batch. */
+int dsmc_batch_step(DsmcBatch* b, int32_t nsteps);
+
+/* The stream the batch graph runs on (a cudaStream_t), and a wait for it
+ * that also reports device-side errors of the cases. */
+void* dsmc_batch_stream(DsmcBatch* b);
+int dsmc_batch_sync(DsmcBatch* b);
+
 #ifdef __cplusplus
 }
 #endif
