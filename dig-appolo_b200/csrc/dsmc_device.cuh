@@ -46,6 +46,8 @@ constexpr int kErrSortIndex = 8;
 constexpr uint32_t kPurposeWall = 1;
 constexpr uint32_t kPurposeInject = 2;
 constexpr uint32_t kPurposeCollide = 3;
+constexpr uint32_t kPurposeFillCount = 4;   // initial fill: per-cell count rounding, counter (cell, 0, 4, 0)
+constexpr uint32_t kPurposeFill = 5;        // initial fill: particle k of cell c, counter (c, k, 5, block)
 
 struct DevMesh {
     int ncell, nface, ntri, nwall;
@@ -99,14 +101,23 @@ struct DevConsts {
 // ---------------------------------------------------------------------------
 struct U4 { uint32_t x, y, z, w; };
 
-__device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1)
+__host__ __device__ __forceinline__ uint32_t mulhi32(uint32_t a, uint32_t b)
+{
+#ifdef __CUDA_ARCH__
+    return __umulhi(a, b);
+#else
+    return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
+
+__host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1)
 {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
         const uint32_t lo0 = 0xD2511F53u * c.x;
-        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t hi0 = mulhi32(0xD2511F53u, c.x);
         const uint32_t lo1 = 0xCD9E8D57u * c.z;
-        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
+        const uint32_t hi1 = mulhi32(0xCD9E8D57u, c.z);
         c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
         k0 += 0x9E3779B9u;
         k1 += 0xBB67AE85u;
@@ -116,7 +127,7 @@ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1)
 
 // Uniform variates from raw Philox words: a double in (0,1) with 53 random
 // bits from two words, a float in (0,1) with 24 random bits from one.
-__device__ __forceinline__ double unit64(uint32_t a, uint32_t b)
+__host__ __device__ __forceinline__ double unit64(uint32_t a, uint32_t b)
 {
     const uint64_t k = ((uint64_t)a << 21) ^ ((uint64_t)b >> 11);
     return ((double)k + 0.5) * 0x1.0p-53;

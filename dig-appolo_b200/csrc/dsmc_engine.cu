@@ -1115,6 +1115,63 @@ struct Engine {
         return true;
     }
 
+    // Device-side initial fill. Counts follow setParticleMessage
+    // (src/meshImport.cpp:1399-1421): cell c expects Ns = V_c * Nps / V_total
+    // particles (Nps = ppcMean * ncell) and gets floor(Ns) + 1 with
+    // probability frac(Ns), else floor(Ns); the draw for cell c is Philox
+    // counter (c, 0, kPurposeFillCount, 0) under the key `seed`. Placement and
+    // velocities: fill_kernel.
+    bool fillFreestream(double ppcMean, uint64_t seed)
+    {
+        if (!(ppcMean > 0.0) || !std::isfinite(ppcMean)) return fail("fill: particles per cell must be positive");
+        const uint32_t k0 = (uint32_t)(seed & 0xffffffffu), k1 = (uint32_t)(seed >> 32);
+        double vtot = 0.0;
+        for (int c = 0; c < ncell; ++c) vtot += cells[(size_t)c].area;
+        if (!(vtot > 0.0)) return fail("fill: zero mesh volume");
+        const double nps = ppcMean * (double)ncell;
+        std::vector<int> st((size_t)ncell + 1, 0);
+        int64_t total = 0;
+        for (int c = 0; c < ncell; ++c) {
+            const double ns = cells[(size_t)c].area * nps / vtot;
+            const double fl = std::floor(ns);
+            const U4 b = philox4x32_10(U4{(uint32_t)c, 0u, kPurposeFillCount, 0u}, k0, k1);
+            const int64_t nc = (int64_t)fl + ((unit64(b.x, b.y) < ns - fl) ? 1 : 0);
+            total += nc;
+            if (total > (int64_t)0x7fffffff - 1) return fail("fill: more than 2^31 particles");
+            st[(size_t)c + 1] = (int)total;
+        }
+        const int64_t need = params.capacity > 0 ? params.capacity
+                                                 : std::max<int64_t>(total + total / 2 + (1 << 16), 1 << 20);
+        if (total > need) return fail("fill: more particles than the configured capacity");
+        haveParticles = false;
+        if (!ensureCapacity(need)) return false;
+        if (!cuda(cudaMemcpyAsync(start[cur], st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice, stream), "fill start"))
+            return false;
+        FillParams f{};
+        const double base = 1.0 * mess.Ma * std::sqrt(mess.gamma / 2.0) * mess.v_in / mess.v_rms;
+        f.u[0] = base * params.inflow_dir[0];
+        f.u[1] = base * params.inflow_dir[1];
+        f.u[2] = 0.0;
+        f.tN = mess.T_in / mess.T_ref;
+        f.sig = std::sqrt(f.tN / 2.0);
+        f.keyLo = k0;
+        f.keyHi = k1;
+        if (precision == DSMC_PRECISION_MIXED) launch_fill<float>(args<float>(), f, shape, stream);
+        else launch_fill<double>(args<double>(), f, shape, stream);
+        if (!cuda(cudaGetLastError(), "fill kernel")) return false;
+        StepCtl h{};
+        h.nLive = (int)total;
+        h.capacity = (int)capacity;
+        if (!cuda(cudaMemcpyAsync(ctl, &h, sizeof h, cudaMemcpyHostToDevice, stream), "ctl")) return false;
+        if (!cuda(cudaMemsetAsync(countSlot, 0, (size_t)ncell * kSlots * sizeof(int), stream), "countSlot")) return false;
+        if (!cuda(cudaStreamSynchronize(stream), "fill sync")) return false;
+        hostNLive = (int)total;
+        haveParticles = true;
+        devIstepValid = false;
+        pendingInject = false;
+        return true;
+    }
+
     bool downloadParticles(int64_t n, double* px, double* py, double* pz, double* vx, double* vy, double* vz,
                            double* ir, int32_t* cellOut, uint32_t* pid)
     {
@@ -1534,6 +1591,12 @@ void engine_set_error(DsmcHandle* h, const char* msg) { h->e.err = msg; }
 }  // namespace dsmc
 
 extern "C" {
+
+int dsmc_fill_freestream(DsmcHandle* h, double ppc_mean, uint64_t seed)
+{
+    DSMC_GUARD(h);
+    return status_of(h->e, h->e.fillFreestream(ppc_mean, seed));
+}
 
 // ---------------------------------------------------------------------------
 // launch shapes and the autotuner

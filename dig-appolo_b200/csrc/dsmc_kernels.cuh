@@ -90,6 +90,15 @@ template <typename Real> void launch_sort(const StepArgs<Real>& a, const LaunchS
 template <typename Real> void launch_collide(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s);
 template <typename Real> void launch_sample(const StepArgs<Real>& a, bool pre, const LaunchShape& L, cudaStream_t s);
 void launch_bump_istep(StepCtl* ctl, cudaStream_t s);
+
+// Freestream of the initial fill, normalised like the particle state.
+struct FillParams {
+    double u[3];      // drift
+    double sig;       // thermal spread per component, sqrt(T/2)
+    double tN;        // temperature (rotational energy mean tN/2)
+    uint32_t keyLo, keyHi;
+};
+template <typename Real> void launch_fill(const StepArgs<Real>& a, const FillParams& f, const LaunchShape& L, cudaStream_t s);
 template <typename Real> cudaError_t prepare_kernels();
 void launch_macro(const DevMesh& M, const DevConsts& C, const double* acc, int set, double count,
                   double* out, int ncell, cudaStream_t s);

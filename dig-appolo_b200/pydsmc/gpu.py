@@ -78,6 +78,7 @@ _SIGS = [
     ("dsmc_last_error", C.c_char_p, [_P]),
     ("dsmc_upload_particles", C.c_int, [_P, C.c_int64] + [_P] * 8),
     ("dsmc_particle_count", C.c_int, [_P, C.POINTER(C.c_int64)]),
+    ("dsmc_fill_freestream", C.c_int, [_P, C.c_double, C.c_uint64]),
     ("dsmc_download_particles", C.c_int, [_P, C.c_int64] + [_P] * 9),
     ("dsmc_step", C.c_int, [_P, C.c_int32, C.c_uint32]),
     ("dsmc_preprocesseffquad", C.c_int, [_P, C.c_int32]),
@@ -328,6 +329,10 @@ class Case:
                     "dsmc_trace_noalloc" if noalloc else "dsmc_trace")
         return {"cell": oi[0], "ifout": oi[1], "face": oi[2], "tri": oi[3], "ncross": oi[4],
                 "x": np.stack(of[:3], 1), "v": np.stack(of[3:6], 1), "dt": of[6]}
+
+    def fill_freestream(self, ppc_mean: float, seed: int = 0):
+        """Device-side initial fill (dsmc_fill_freestream)."""
+        self._check(self.lib.dsmc_fill_freestream(self.h, float(ppc_mean), int(seed)), "dsmc_fill_freestream")
 
     # -- launch shapes ----------------------------------------------------------
     def launch_shape(self) -> dict:

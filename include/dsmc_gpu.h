@@ -196,6 +196,19 @@ int dsmc_upload_particles(DsmcHandle* h, int64_t n,
                           const double* vx, const double* vy, const double* vz,
                           const double* ir, const int32_t* cell);
 
+/* Replace all particles by an initial fill made on the device (replaces
+ * Np_tri_inititial / meshfillpar / velocityLocationGenerate,
+ * src/MeshparticalInitial.cpp:481-721, with the per-cell counts of
+ * setParticleMessage, src/meshImport.cpp:1399-1421): cell c gets
+ * floor(Ns) or floor(Ns) + 1 particles (the latter with probability
+ * frac(Ns)), Ns = V_c * ppc_mean * ncell / V_total, placed uniformly in the
+ * cell (split into tetrahedra from its centroid to its face triangles, as
+ * the reference's centre-face split). Velocities: the freestream Maxwellian
+ * of the case (its inflow drift and T_in) where the reference draws a unit
+ * Maxwellian at rest that its GSIS start-up then replaces; Ir from the
+ * equilibrium distribution at T_in. seed keys the fill's random streams. */
+int dsmc_fill_freestream(DsmcHandle* h, double ppc_mean, uint64_t seed);
+
 /* Particle count (sum of bucket sizes). */
 int dsmc_particle_count(DsmcHandle* h, int64_t* n);
 
