@@ -206,7 +206,9 @@ int dsmc_upload_particles(DsmcHandle* h, int64_t n,
  * the reference's centre-face split). Velocities: the freestream Maxwellian
  * of the case (its inflow drift and T_in) where the reference draws a unit
  * Maxwellian at rest that its GSIS start-up then replaces; Ir from the
- * equilibrium distribution at T_in. seed keys the fill's random streams. */
+ * equilibrium distribution at T_in. seed keys the fill's random streams.
+ * The freestream number density corresponds to ppc_mean equal to the
+ * particles per cell the case's Neff was set for (meshMessage). */
 int dsmc_fill_freestream(DsmcHandle* h, double ppc_mean, uint64_t seed);
 
 /* Particle count (sum of bucket sizes). */
