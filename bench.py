@@ -16,8 +16,13 @@ Multi-GPU runs are independent replicas (one case per GPU, no collective on
 the data path): value = the sum of all ranks' particle-steps / the slowest
 rank's time.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload capsule|block]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload capsule|block|batch]
                   [--ppc P] [--impl ours|reference] [--no-cpu-baseline]
+                  [--cases N] [--batch-seed S] [--no-autotune]
+
+--workload batch runs the batched form instead: --cases seeded hex-box
+cases advanced together, one CUDA graph per step, against the same cases
+stepped one after another.
 """
 from __future__ import annotations
 
@@ -186,7 +191,10 @@ def run_case(wl, fill, precision, steps, warmup, seed, timing=False):
     p = gpu.default_params(precision=precision, seed=seed, zones=wl["zones"], inflow_dir=wl["inflow_dir"],
                            nss=10 ** 9, nscheme=max(1, (steps + warmup) // 5), nrepeat=100)
     case = gpu.Case(wl["dm"], wl["mess"], p, device=torch.cuda.current_device())
-    case.upload_particles(fill["x"], fill["v"], fill["ir"], fill["cell"])
+    if "device" in fill:
+        case.fill_freestream(*fill["device"])
+    else:
+        case.upload_particles(fill["x"], fill["v"], fill["ir"], fill["cell"])
     case.statistic_macroPre()
     istep = 0
     for _ in range(warmup):
@@ -241,8 +249,9 @@ def run_ours(args):
     gpu.load()
     wl = make_workload(args.workload, args.ppc)
     dm, mess = wl["dm"], wl["mess"]
-    fill = W.initial_fill(dm, mess, args.ppc, seed=rank, inflow_dir=wl["inflow_dir"])
-    nparts = len(fill["cell"])
+    # the reference's initial state: a mean of ppc particles per cell in
+    # proportion to the cell volumes, drawn on the device
+    fill = {"device": (float(args.ppc), 1000 + rank)}
 
     def barrier():
         if world > 1:
@@ -273,6 +282,7 @@ def run_ours(args):
     ps_mixed = sum_over_ranks(particle_steps(mixed, args.steps))
     value = ps_mixed / (ms_mixed / 1e3)
     case_m = mixed.pop("case")
+    nparts = int(mixed["n0"])
     # --- stage timing pass (events between stages, no graph) for the roofline
     barrier()
     tim = run_case(wl, fill, gpu.PRECISION_MIXED, max(3, args.steps // 2), 1, seed=2000 + rank, timing=True)
@@ -361,15 +371,15 @@ def run_e2e(wl, fill, args, rank):
     p = gpu.default_params(precision=gpu.PRECISION_MIXED, seed=3000 + rank, zones=wl["zones"],
                            inflow_dir=wl["inflow_dir"], nss=10 ** 9, nscheme=100, nrepeat=100)
     case = gpu.Case(wl["dm"], wl["mess"], p, device=torch.cuda.current_device())
-    # warm the graph on a throwaway upload
-    case.upload_particles(fill["x"], fill["v"], fill["ir"], fill["cell"])
+    # the same initial particles as host arrays (made on the device, read
+    # back before the timed region); the graph is warmed on them
+    case.fill_freestream(*fill["device"])
+    hx, hv, hir, hcell = case.download_particles()
     for s in range(1, args.warmup + 1):
         case.step(s)
     case.sync()
-    x = np.ascontiguousarray(fill["x"])
-    v = np.ascontiguousarray(fill["v"])
     t0 = time.perf_counter()
-    case.upload_particles(x, v, fill["ir"], fill["cell"])
+    case.upload_particles(hx, hv, hir, hcell)
     n0 = case.particle_count()
     h2d = int(n0) * (7 * 8 + 4)
     d2h = 0
@@ -398,7 +408,7 @@ def cpu_baseline(wl, fill, args):
                 "sample": "unavailable: oracle/_ref/ref_harness not built"}
     dm, mess = wl["dm"], wl["mess"]
     ppc_s = max(2, min(args.ppc, 10))
-    sub = W.initial_fill(dm, mess, ppc_s, seed=7, inflow_dir=wl["inflow_dir"])
+    sub = W.initial_fill(dm, mess, ppc_s, seed=7, inflow_dir=wl["inflow_dir"], proportional=True)
     nsteps = 5
     roles = {1: "interface", 2: "inlet", 3: "outlet", 4: "wall", 5: "none", 0: "none"}
     r_arg = ",".join(f"{t}:{roles[r]}" for t, r, _ in wl["zones"])
@@ -408,8 +418,140 @@ def cpu_baseline(wl, fill, args):
         r = H.run(cas, mess, sub["x"], sub["v"], sub["ir"], sub["cell"], nsteps, 1, r_arg, nsteps + 1, timeout=600)
     t = r["timing"]
     return {"value": t["particle_steps_per_s"], "unit": "particle-steps/s", "cores": 1, "kind": "reference",
-            "sample": f"{wl['desc']['workload']} mesh, {ppc_s} particles/cell ({len(sub['cell'])} particles), "
+            "sample": f"{wl['desc']['workload']} mesh, {ppc_s} particles/cell on average in proportion to the cell "
+                      f"volumes ({len(sub['cell'])} particles), "
                       f"{nsteps} steps, {t['seconds']:.2f} s of one core"}
+
+
+# ---------------------------------------------------------------------------
+# batched form: many independent cases in one CUDA graph per step
+# ---------------------------------------------------------------------------
+BLOCK_ZONES = [(3, 1, 0), (4, 2, 1), (5, 3, 0), (6, 4, 0), (7, 5, 0)]
+
+
+def batch_specs(n: int, seed: int):
+    """Seeded hex-box obstacle cases: cells log-uniform in 5k-80k (a box of
+    3k x 2k x 2k hexes, 1.0 x 0.5 x 0.5 m, with the central (k/2)^3 block
+    removed as a diffuse wall, k even), particles per cell uniform in
+    20-200, Ma uniform in 3-10, angle of attack uniform in 0-40 deg, Kn on
+    the block edge log-uniform in 0.01-1."""
+    rs = np.random.default_rng(seed)
+    out = []
+    for j in range(n):
+        cells = math.exp(rs.uniform(math.log(5e3), math.log(8e4)))
+        k = max(4, 2 * int(round((cells / 11.875) ** (1.0 / 3.0) / 2.0)))
+        out.append({"k": k, "ppc": float(rs.uniform(20, 200)), "Ma": float(rs.uniform(3, 10)),
+                    "aoa": float(rs.uniform(0, 40)), "Kn": float(math.exp(rs.uniform(math.log(0.01), 0.0))),
+                    "seed": j})
+    return out
+
+
+def batch_mesh(k: int):
+    h = k // 2
+    nx, ny, nz = 3 * k, 2 * k, 2 * k
+    i0, j0, k0 = (nx - h) // 2, (ny - h) // 2, (nz - h) // 2
+    raw = M.hex_box(nx, ny, nz, 1.0, 0.5, 0.5, (i0, i0 + h, j0, j0 + h, k0, k0 + h))
+    return M.build_dsmc_mesh(raw), h * 0.5 / ny
+
+
+def make_batch_cases(specs, precision, autotune=True):
+    import torch
+    from pydsmc import gpu
+    meshes = {}
+    cases, steps = [], []
+    for sp in specs:
+        if sp["k"] not in meshes:
+            meshes[sp["k"]] = batch_mesh(sp["k"])
+        dm, L0 = meshes[sp["k"]]
+        mess = C.mesh_message(dm, sp["Ma"], sp["Kn"], ppc=int(round(sp["ppc"])), L0=L0)
+        p = gpu.default_params(precision=precision, seed=7000 + sp["seed"], zones=BLOCK_ZONES,
+                               inflow_dir=C.inflow_direction(sp["aoa"]), nss=10 ** 9, nscheme=50, nrepeat=100)
+        case = gpu.Case(dm, mess, p, device=torch.cuda.current_device())
+        case.fill_freestream(sp["ppc"], 9000 + sp["seed"])
+        case.statistic_macroPre()
+        nxt = 1
+        if autotune:
+            nxt, _ = case.autotune(1, trial_steps=1)
+        cases.append(case)
+        steps.append(nxt - 1)
+    return cases, steps
+
+
+def run_batch(args):
+    """The batched form: args.cases cases (batch_specs), autotuned, advanced
+    (a) one after another, each by its own per-step graph, and (b) together,
+    one CUDA graph per step whose branches are the cases. value = total
+    particle-steps / device time of (b)."""
+    import torch
+    from pydsmc import gpu
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    gpu.load()
+    specs = batch_specs(args.cases, args.batch_seed)
+    t0 = time.perf_counter()
+    cases, steps = make_batch_cases(specs, gpu.PRECISION_MIXED, autotune=not args.no_autotune)
+    setup_s = time.perf_counter() - t0
+    K, W0 = args.steps, args.warmup
+    # (a) one after another: device time summed over the cases
+    seq_ms, seq_ps = 0.0, 0.0
+    for j, case in enumerate(cases):
+        for _ in range(W0):
+            steps[j] += 1
+            case.step(steps[j])
+        case.sync()
+        st = torch.cuda.ExternalStream(case.lib.dsmc_stream(case.h))
+        n0 = case.particle_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(K):
+            steps[j] += 1
+            case.step(steps[j])
+        e1.record(st)
+        e1.synchronize()
+        seq_ms += e0.elapsed_time(e1)
+        seq_ps += 0.5 * (n0 + case.particle_count()) * K
+    # (b) together
+    batch = gpu.Batch(cases)
+    batch.step(W0)
+    batch.sync()
+    bs = torch.cuda.ExternalStream(batch.stream())
+    n0 = sum(c.particle_count() for c in cases)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(bs)
+        batch.step(K)
+        e1.record(bs)
+        e1.synchronize()
+    b_ms = e0.elapsed_time(e1)
+    batch.sync()
+    n1 = sum(c.particle_count() for c in cases)
+    b_ps = 0.5 * (n0 + n1) * K
+    shapes = [c.launch_shape() for c in cases]
+    batch.close()
+    for c in cases:
+        c.close()
+    cells = [batch_mesh_cells(sp["k"]) for sp in specs]
+    line = {
+        "metric": f"DSMC particle-steps/s, {len(specs)}-case batch (one CUDA graph per step, 1 B200)",
+        "value": b_ps / (b_ms / 1e3), "unit": "particle-steps/s", "n_gpus": 1, "steps": K, "warmup": W0,
+        "ms_per_step": b_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64acc", "data": "synthetic (seeded cases, device freestream fill)",
+        "sequential": {"value": seq_ps / (seq_ms / 1e3), "ms_per_step": seq_ms / K,
+                       "how": "each case on its own, one after another, its own per-step graph"},
+        "batch_over_sequential": (b_ps / (b_ms / 1e3)) / (seq_ps / (seq_ms / 1e3)),
+        "config": {"workload": f"batch-{len(specs)}", "cases": len(specs), "cells_total": int(sum(cells)),
+                   "particles_total": int(n0), "cells_range": [int(min(cells)), int(max(cells))],
+                   "autotuned": not args.no_autotune, "batch_seed": args.batch_seed, "setup_s": setup_s,
+                   "move_threads_chosen": sorted({s["move_threads"] for s in shapes})},
+        "gpu_launches": None,
+        "clocks": clk.summary(),
+    }
+    line["gpu_launches"] = launches_per_step(None) * K * len(specs) + K * len(specs)
+    print(json.dumps(line), flush=True)
+
+
+def batch_mesh_cells(k: int) -> int:
+    h = k // 2
+    return 12 * k ** 3 - h ** 3
 
 
 # ---------------------------------------------------------------------------
@@ -436,7 +578,8 @@ def run_reference(args):
         cas = os.path.join(d, "case.cas")
         M.write_cas(cas, dm.raw)
         from concurrent.futures import ThreadPoolExecutor
-        fills = [W.initial_fill(dm, mess, ppc_s, seed=100 + k, inflow_dir=wl["inflow_dir"]) for k in range(cores)]
+        fills = [W.initial_fill(dm, mess, ppc_s, seed=100 + k, inflow_dir=wl["inflow_dir"], proportional=True)
+                 for k in range(cores)]
         t0 = time.perf_counter()
         with ThreadPoolExecutor(max_workers=cores) as ex:
             futs = [ex.submit(H.run, cas, mess, f["x"], f["v"], f["ir"], f["cell"], nsteps, 1 + k, r_arg, nsteps + 1, 3600)
@@ -449,7 +592,8 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": wl["desc"],
             "cpu_baseline": {"value": agg, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
-                             "sample": f"{cores} independent single-rank processes, {ppc_s} particles/cell each, "
+                             "sample": f"{cores} independent single-rank processes, {ppc_s} particles/cell on "
+                                       f"average each, "
                                        f"{nsteps} steps each, {wall:.1f} s wall"},
             "e2e": {"value": agg, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -464,6 +608,9 @@ def main():
     ap.add_argument("--ppc", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cases", type=int, default=64, help="batch workload: number of cases")
+    ap.add_argument("--batch-seed", type=int, default=0)
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -471,6 +618,8 @@ def main():
         args.ppc = 100 if args.workload == "capsule" else 200
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_ours(args)
 

@@ -74,10 +74,19 @@ def cell_boxes(dm: DsmcMesh):
     return lo, hi
 
 
-def initial_fill(dm: DsmcMesh, mess, ppc: int, seed: int, inflow_dir) -> dict:
-    """``ppc`` particles per cell from the freestream Maxwellian."""
+def initial_fill(dm: DsmcMesh, mess, ppc: int, seed: int, inflow_dir, proportional: bool = False) -> dict:
+    """Particles from the freestream Maxwellian: ``ppc`` in every cell, or
+    with ``proportional`` a mean of ``ppc`` per cell in proportion to the
+    cell volumes, each cell's count rounded up with probability equal to its
+    fraction (the reference's initial counts, src/meshImport.cpp:1399-1421)."""
     rng = np.random.default_rng(seed)
-    cells = np.repeat(np.arange(dm.ncell, dtype=np.int32), ppc)
+    if proportional:
+        vol = dm.cells["area"].astype(float)
+        ns = vol * (ppc * dm.ncell) / vol.sum()
+        n = np.floor(ns).astype(np.int64) + (rng.random(dm.ncell) < ns - np.floor(ns))
+        cells = np.repeat(np.arange(dm.ncell, dtype=np.int32), n)
+    else:
+        cells = np.repeat(np.arange(dm.ncell, dtype=np.int32), ppc)
     x = uniform_positions(dm, cells, rng)
     u, sig, tN = freestream(mess, inflow_dir)
     v = u[None, :] + sig * rng.standard_normal((cells.shape[0], 3))

@@ -72,3 +72,15 @@ def test_workload_generators():
     assert np.allclose(f["v"].mean(0), u, atol=5 * sig / np.sqrt(len(f["v"])))
     t = W.trace_particles(dm, mess, 1000, 1, C.inflow_direction(30.0))
     assert t["cell"].min() >= 0 and t["cell"].max() < dm.ncell
+
+
+def test_batch_specs_follow_the_batched_configuration():
+    import bench
+    sp = bench.batch_specs(64, 0)
+    assert sp == bench.batch_specs(64, 0)                    # seeded
+    cells = [bench.batch_mesh_cells(s["k"]) for s in sp]
+    assert min(cells) >= 4000 and max(cells) <= 90000        # log-uniform 5k-80k, rounded to even k
+    assert all(20 <= s["ppc"] <= 200 and 3 <= s["Ma"] <= 10 and 0 <= s["aoa"] <= 40 for s in sp)
+    assert all(0.01 <= s["Kn"] <= 1.0 for s in sp)
+    dm, L0 = bench.batch_mesh(8)
+    assert dm.ncell == bench.batch_mesh_cells(8)
