@@ -16,13 +16,15 @@ Multi-GPU runs are independent replicas (one case per GPU, no collective on
 the data path): value = the sum of all ranks' particle-steps / the slowest
 rank's time.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload capsule|block|batch]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload capsule|block|batch|serve]
                   [--ppc P] [--impl ours|reference] [--no-cpu-baseline]
                   [--cases N] [--batch-seed S] [--no-autotune]
 
 --workload batch runs the batched form instead: --cases seeded hex-box
 cases advanced together, one CUDA graph per step, against the same cases
-stepped one after another.
+stepped one after another. --workload serve runs the served form: --requests
+capsule cases arriving at --rate per second, served with continuous batching
+(p50/p99 time-to-result, cases/hour, particle-steps/s).
 """
 from __future__ import annotations
 
@@ -196,7 +198,10 @@ def run_case(wl, fill, precision, steps, warmup, seed, timing=False):
     else:
         case.upload_particles(fill["x"], fill["v"], fill["ir"], fill["cell"])
     case.statistic_macroPre()
-    istep = 0
+    # launch shapes picked on this case (ordinary steps; results do not
+    # depend on them), then the warm-up steps
+    istep, _ = case.autotune(1, trial_steps=1)
+    istep -= 1
     for _ in range(warmup):
         istep += 1
         case.step(istep)
@@ -328,7 +333,7 @@ def run_ours(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32+f64acc",
-        "data": "synthetic (seeded freestream Maxwellian fill, generated mesh)",
+        "data": "synthetic (generated mesh; device freestream fill, counts in proportion to cell volume)",
         "config": dict(wl["desc"], particles_per_gpu=nparts, parallelism=f"replicas x{world}",
                        l2="particle state > L2 (126 MB)", precision="mixed"),
         "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / args.steps, "dtype": "f64"},
@@ -555,6 +560,74 @@ def batch_mesh_cells(k: int) -> int:
 
 
 # ---------------------------------------------------------------------------
+# served form: continuous batching of arriving capsule cases
+# ---------------------------------------------------------------------------
+SERVE_SCALES = (2.65, 1.8, 1.4, 1.15, 1.0)   # mesh spacing factors: about 20k to 371k tets
+
+
+def serve_pool():
+    """Capsule meshes at several resolutions (the request stream resamples
+    among them)."""
+    from pydsmc import capsule
+    pool = []
+    for f in SERVE_SCALES:
+        raw = capsule.capsule_mesh(h_fine=0.215 * f, h_coarse=0.60 * f, seed=0)
+        pool.append(M.build_dsmc_mesh(raw))
+    return pool
+
+
+def run_serve(args):
+    """The served form: args.requests capsule cases arriving as a Poisson
+    stream (args.rate per second), each on a mesh drawn from the pool, with
+    10-100 particles per cell and 200-2000 steps (mixed precision, Ma 5,
+    Kn 0.01, AoA 30 deg); admission by a 160 GB device-memory budget; fields
+    handed to the host every 100 steps; sampling window 20%, steady sampling
+    from 50% of each case's steps."""
+    import torch
+    from pydsmc import capsule, gpu, serve
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    gpu.load()
+    t0 = time.perf_counter()
+    pool = serve_pool()
+    setup_s = time.perf_counter() - t0
+    rs = np.random.default_rng(args.batch_seed)
+    zones = [(3, 1, 0), (4, 2, 1), (5, 3, 0), (6, 4, 0)]
+    reqs, t = [], 0.0
+    for j in range(args.requests):
+        t += rs.exponential(1.0 / args.rate)
+        dm = pool[int(rs.integers(0, len(pool)))]
+        ppc = float(rs.uniform(10, 100))
+        steps = int(rs.integers(200, 2001))
+        mess = C.mesh_message(dm, 5.0, 0.01, ppc=int(round(ppc)), L0=capsule.L0)
+        reqs.append((t, serve.CaseRequest(dm=dm, mess=mess, zones=zones, inflow_dir=C.inflow_direction(30.0),
+                                          steps=steps, ppc=ppc, seed=j, precision=gpu.PRECISION_MIXED,
+                                          name=f"req{j}")))
+    be = serve.GpuBackend(device=torch.cuda.current_device())
+    srv = serve.Server(be, hbm_budget=160e9, max_active=64, handoff_every=100)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        start = time.perf_counter()
+        for ta, r in reqs:
+            srv.submit(r, start + ta)
+        srv.run()
+    be.close()
+    s = srv.summary()
+    line = {
+        "metric": "DSMC served capsule cases (continuous batching, 1 B200): particle-steps/s; p50/p99 time-to-result",
+        "value": s["particle_steps_per_s"], "unit": "particle-steps/s", "n_gpus": 1,
+        "p50_s": s["p50_s"], "p99_s": s["p99_s"], "cases_per_hour": s["cases_per_hour"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc",
+        "data": "synthetic (seeded Poisson request stream, generated meshes, device freestream fill)",
+        "config": {"workload": "serve-capsule", "requests": args.requests, "rate_per_s": args.rate,
+                   "mesh_cells": sorted(int(d.ncell) for d in pool), "ppc": [10, 100], "steps": [200, 2000],
+                   "hbm_budget_gb": 160, "handoff_every": 100, "max_concurrent": s["max_concurrent"],
+                   "rounds": s["rounds"], "span_s": s["span_s"], "mesh_setup_s": setup_s,
+                   "timing": "wall clock from each request's arrival to its result on the host"},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # reference arm
 # ---------------------------------------------------------------------------
 def run_reference(args):
@@ -611,6 +684,8 @@ def main():
     ap.add_argument("--cases", type=int, default=64, help="batch workload: number of cases")
     ap.add_argument("--batch-seed", type=int, default=0)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--requests", type=int, default=16, help="serve workload: number of requests")
+    ap.add_argument("--rate", type=float, default=4.0, help="serve workload: arrivals per second")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -620,6 +695,8 @@ def main():
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

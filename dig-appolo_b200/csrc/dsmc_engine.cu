@@ -917,8 +917,8 @@ struct Engine {
 
     bool setShape(const DsmcLaunchShape& s)
     {
-        if (s.move_threads != 128 && s.move_threads != 256 && s.move_threads != 512)
-            return fail("launch shape: move_threads must be 128, 256 or 512");
+        if (s.move_threads != 128 && s.move_threads != 256)
+            return fail("launch shape: move_threads must be 128 or 256");
         if (s.move_blocks_per_sm < 1 || s.move_blocks_per_sm > 32 || s.sort_blocks_per_sm < 1 ||
             s.sort_blocks_per_sm > 32 || s.collide_blocks_per_sm < 1 || s.collide_blocks_per_sm > 32)
             return fail("launch shape: blocks per SM outside [1, 32]");
@@ -965,9 +965,9 @@ struct Engine {
         bool ok = step(istep++, DSMC_STAGE_ALL);   // one untimed-order step to warm the caches
         double bestMs = 0.0;
         if (ok) ok = trial(best, 1, bestMs);
-        const int threads[3] = {128, 256, 512};
+        const int threads[2] = {128, 256};
         const int blocks[4] = {2, 4, 8, 16};
-        for (int t = 0; ok && t < 3; ++t)
+        for (int t = 0; ok && t < 2; ++t)
             for (int b = 0; ok && b < 4; ++b) {
                 DsmcLaunchShape c = best;
                 c.move_threads = threads[t];

@@ -209,8 +209,11 @@ void launch_inject(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s
 // ===========================================================================
 // move
 // ===========================================================================
+// Three resident 256-thread blocks per SM (registers capped at 85): the
+// trace is bound by dependent loads, so occupancy pays more than the few
+// registers it spills to L1.
 template <typename Real>
-__global__ void __launch_bounds__(512) move_kernel(StepArgs<Real> a)
+__global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
 {
     const int istep = a.ctl->istep;
     const int n = a.ctl->nLive;

@@ -78,7 +78,7 @@ constexpr int kScanBlocks = 296;
 // results do not depend on these; only the speed does.
 struct LaunchShape {
     int smCount = 148;
-    int moveThreads = 256;        // threads per block of the move kernel: 128, 256, 512
+    int moveThreads = 256;        // threads per block of the move kernel: 128 or 256
     int moveBlocksPerSm = 8;      // move grid = smCount x this
     int sortBlocksPerSm = 8;      // rank, scatter, gather grids = smCount x this
     int collideBlocksPerSm = 9;   // collide grid cap per SM (at most the resident blocks)

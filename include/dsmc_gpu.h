@@ -327,7 +327,7 @@ int dsmc_sync(DsmcHandle* h);
  * never its result.
  * ------------------------------------------------------------------------- */
 typedef struct DsmcLaunchShape {
-    int32_t move_threads;          /* threads per block of the move kernel: 128, 256 or 512 */
+    int32_t move_threads;          /* threads per block of the move kernel: 128 or 256 */
     int32_t move_blocks_per_sm;    /* move grid = SMs x this, 1..32 (particles per thread follow) */
     int32_t sort_blocks_per_sm;    /* rank / scatter / gather grids = SMs x this, 1..32 */
     int32_t collide_blocks_per_sm; /* cap on the collision grid per SM, 1..32 (at most the resident blocks) */

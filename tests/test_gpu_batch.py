@@ -43,7 +43,7 @@ def _same(a, b):
 
 
 SHAPES = [dict(move_threads=128, move_blocks_per_sm=3, sort_blocks_per_sm=1, collide_blocks_per_sm=1),
-          dict(move_threads=512, move_blocks_per_sm=2, sort_blocks_per_sm=16, collide_blocks_per_sm=5),
+          dict(move_threads=128, move_blocks_per_sm=2, sort_blocks_per_sm=16, collide_blocks_per_sm=5),
           dict(move_threads=256, move_blocks_per_sm=32, sort_blocks_per_sm=3, collide_blocks_per_sm=9)]
 
 
@@ -72,7 +72,7 @@ def test_autotune_runs_ordinary_steps(block):
         tuned.statistic_macroPre()
         nxt, shape = tuned.autotune(1, trial_steps=1)
         assert nxt > 10
-        assert shape["move_threads"] in (128, 256, 512)
+        assert shape["move_threads"] in (128, 256)
         assert tuned.launch_shape() == shape
         for s in range(nxt, nxt + 2):
             tuned.step(s)
