@@ -232,6 +232,19 @@ def run_case(wl, fill, precision, steps, warmup, seed, timing=False):
     return res
 
 
+def over_ranks(x: float, op: str, device: str) -> float:
+    """x reduced over the ranks of the process group (max or sum); x itself
+    without a group or with one rank. Replica runs report the slowest
+    rank's time and the sum of all ranks' particle-steps."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def particle_steps(res, steps):
     # particles at the start of each timed step: n0 + injected - removed... use the
     # inventory at both ends (the inventory drifts slowly) times the step count
@@ -264,18 +277,10 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return over_ranks(x, "max", "cuda")
 
     def sum_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return over_ranks(x, "sum", "cuda")
 
     peak, peak_kind = load_peaks()
     # --- headline: mixed precision, graph replay
