@@ -22,7 +22,7 @@ LIB_DIR = os.path.join(HERE, "lib")
 OBJ_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(LIB_DIR, "libdsmcgpu.so")
 
-SOURCES = ["dsmc_kernels.cu", "dsmc_engine.cu", "dsmc_noalloc.cu"]
+SOURCES = ["dsmc_kernels.cu", "dsmc_engine.cu", "dsmc_noalloc.cu", "dsmc_gsis.cu"]
 HEADERS = ["dsmc_device.cuh", "dsmc_kernels.cuh", "dsmc_macro.cuh"]
 
 

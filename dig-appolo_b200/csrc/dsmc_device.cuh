@@ -41,6 +41,7 @@ constexpr int kErrCapacity = 1;
 constexpr int kErrStageCell = 2;   // a cell larger than the stage reached the staged path
 constexpr int kErrRejectLoop = 4;
 constexpr int kErrSortIndex = 8;
+constexpr int kErrGsisCount = 16;  // a GSIS target count outside [0, 2^30)
 
 // Philox RNG stream purposes (third counter word).
 constexpr uint32_t kPurposeWall = 1;
@@ -48,6 +49,10 @@ constexpr uint32_t kPurposeInject = 2;
 constexpr uint32_t kPurposeCollide = 3;
 constexpr uint32_t kPurposeFillCount = 4;   // initial fill: per-cell count rounding, counter (cell, 0, 4, 0)
 constexpr uint32_t kPurposeFill = 5;        // initial fill: particle k of cell c, counter (c, k, 5, block)
+// GSIS particle update: counter (cell, j, 6 | sub << 4 | epoch << 8, block)
+// with sub 0 the count rounding, 1 deletion draws, 2 copies, 3 Maxwellian
+// samples into empty cells; epoch counts the updates of a case.
+constexpr uint32_t kPurposeGsis = 6;
 
 struct DevMesh {
     int ncell, nface, ntri, nwall;
@@ -72,6 +77,12 @@ struct DevMesh {
     const float4* diagF;         // quads: in-plane normal of the diagonal, offset (relative)
     const double* planeD;        // [nrec*8] n(3), d, m(3), md, absolute
     const unsigned char* convex; // [ncell]
+    // placement tetrahedra of each cell (buildCellInitTets): records
+    // placeOff[c]..placeOff[c+1], four vertices each (absolute FP64; the
+    // barycentric weights a, b, c, d go to them in this order) and volume
+    const int* placeOff;         // [ncell+1]
+    const double* placeV;        // [nplace*12]
+    const double* placeVol;      // [nplace]
 };
 
 struct DevConsts {
@@ -177,6 +188,57 @@ template <> __device__ __forceinline__ float Stream::uniform<float>() { return u
 __device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
+
+// ---------------------------------------------------------------------------
+// Placement of new particles (initial fill, GSIS copies and samples)
+// ---------------------------------------------------------------------------
+
+// A point of the placement tetrahedron V from four uniforms normalised by
+// their sum (randomBarycentric4, src/MeshparticalInitial.cpp:85-106 and
+// src/ProcessGSIS.cpp:513-534), out = a V0 + b V1 + c V2 + d V3 evaluated
+// left to right (velocityLocationGenerate, src/MeshparticalInitial.cpp:
+// 646-721; sampleCellLocation, src/ProcessGSIS.cpp:1000-1028).
+__device__ __forceinline__ void place_point(const double* __restrict__ V, double r0, double r1, double r2, double r3,
+                                            double out[3])
+{
+    const double sum = da(da(da(r0, r1), r2), r3);
+    double a = 0.25, b = 0.25, c = 0.25, d = 0.25;
+    if (sum > 0.0 && isfinite(sum)) {
+        a = __ddiv_rn(r0, sum);
+        b = __ddiv_rn(r1, sum);
+        c = __ddiv_rn(r2, sum);
+        d = __ddiv_rn(r3, sum);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[k] = da(da(da(dm(a, V[k]), dm(b, V[3 + k])), dm(c, V[6 + k])), dm(d, V[9 + k]));
+}
+
+// sampleCellLocation (src/ProcessGSIS.cpp:977-1029): a placement
+// tetrahedron of cell c by volume (the first whose volume is at least the
+// remaining pick, subtracting as it goes), then a point in it; the cell
+// centre when the cell has no placement tetrahedra (randomlocation's
+// fallback, src/ProcessGSIS.cpp:2478-2488).
+__device__ __forceinline__ void place_in_cell(const DevMesh& M, int c, double uPick, double r0, double r1, double r2,
+                                              double r3, double out[3])
+{
+    const int t0 = M.placeOff[c], t1 = M.placeOff[c + 1];
+    double total = 0.0;
+    for (int t = t0; t < t1; ++t) total = da(total, M.placeVol[t]);
+    if (t1 <= t0 || !(total > 0.0) || !isfinite(total)) {
+        out[0] = M.cellCenter[(size_t)c * 3 + 0];
+        out[1] = M.cellCenter[(size_t)c * 3 + 1];
+        out[2] = M.cellCenter[(size_t)c * 3 + 2];
+        return;
+    }
+    double pick = dm(uPick, total);
+    int ch = t1 - 1;
+    for (int t = t0; t < t1; ++t) {
+        const double v = M.placeVol[t];
+        if (pick <= v) { ch = t; break; }
+        pick = ds(pick, v);
+    }
+    place_point(M.placeV + (size_t)ch * 12, r0, r1, r2, r3, out);
+}
 
 // intersectCachedTri, src/ProcessDSMC.cpp:1174-1197, operation for operation.
 __device__ __forceinline__ bool isect_exact(const double* __restrict__ T, const double x[3], const double v[3], double& t)

@@ -139,6 +139,13 @@ struct Engine {
     int* cellList = nullptr;
     int* cellWork = nullptr;
     int* errorWord = nullptr;
+    int* placeFirst = nullptr;     // [nplace] cell-local first particle of each placement tetrahedron (fill)
+    // GSIS particle update (allocated on first use)
+    double* gsisNs = nullptr;
+    unsigned char* gsisAcc = nullptr;
+    int* gsisFlag = nullptr;
+    unsigned long long* gsisTally = nullptr;
+    uint32_t gsisEpoch = 0;
 
     int64_t capacity = 0;
     int cur = 0;                   // which buffer holds the particles
@@ -233,6 +240,142 @@ struct Engine {
         P3[1] = points[(size_t)idx * 3 + 1];
         P3[2] = points[(size_t)idx * 3 + 2];
         return true;
+    }
+
+    // ------------------------------------------------------------------
+    // Placement tetrahedra of every cell, as buildCellInitTets
+    // (src/MeshparticalInitial.cpp:172-355, src/ProcessGSIS.cpp:748-964):
+    // a cell with 4 distinct nodes is its own tetrahedron (nodes in order of
+    // first appearance over its faces); a cell with 5 nodes and one quad is
+    // split into the two base triangles (the quad's split tag) with the apex;
+    // any other cell into its centre with each face triangle. A tetrahedron
+    // of zero or non-finite volume rejects that decomposition; a cell that
+    // none fits gets no tetrahedra (the fill places nothing there and GSIS
+    // copies go to the cell centre).
+    std::vector<int> placeOffHost;
+    std::vector<double> placeVolHost;
+
+    void buildPlacement(std::vector<double>& V)
+    {
+        placeOffHost.assign((size_t)ncell + 1, 0);
+        placeVolHost.clear();
+        V.clear();
+        // tetAbsVolume / appendCenterFaceTet, src/ProcessGSIS.cpp:660-675, 829-870
+        auto tetVol = [](const double* P0, const double* P1, const double* P2, const double* P3) {
+            const double ax = P1[0] - P0[0], ay = P1[1] - P0[1], az = P1[2] - P0[2];
+            const double bx = P2[0] - P0[0], by = P2[1] - P0[1], bz = P2[2] - P0[2];
+            const double cx = P3[0] - P0[0], cy = P3[1] - P0[1], cz = P3[2] - P0[2];
+            const double crx = by * cz - bz * cy;
+            const double cry = bz * cx - bx * cz;
+            const double crz = bx * cy - by * cx;
+            return std::fabs(ax * crx + ay * cry + az * crz) / 6.0;
+        };
+        struct Tet { double v[12]; double vol; };
+        std::vector<Tet> tets;
+        auto vertexTet = [&](int n0, int n1, int n2, int n3) {
+            Tet t;
+            const int n[4] = {n0, n1, n2, n3};
+            for (int k = 0; k < 4; ++k)
+                if (!loadPoint(n[k], &t.v[3 * k])) return false;
+            t.vol = tetVol(&t.v[0], &t.v[3], &t.v[6], &t.v[9]);
+            if (!(t.vol > 0.0) || !std::isfinite(t.vol)) return false;
+            tets.push_back(t);
+            return true;
+        };
+        auto centerTet = [&](int c, int n0, int n1, int n2) {
+            Tet t;
+            for (int d = 0; d < 3; ++d) t.v[d] = cellCenterHost[(size_t)c * 3 + d];
+            const int n[3] = {n0, n1, n2};
+            for (int k = 0; k < 3; ++k)
+                if (!loadPoint(n[k], &t.v[3 + 3 * k])) return false;
+            t.vol = tetVol(&t.v[0], &t.v[3], &t.v[6], &t.v[9]);
+            if (!(t.vol > 0.0) || !std::isfinite(t.vol)) return false;
+            tets.push_back(t);
+            return true;
+        };
+        auto validFace = [&](int f) { return f >= 0 && f < nface; };
+        std::vector<int> uniq;
+        for (int c = 0; c < ncell; ++c) {
+            placeOffHost[(size_t)c] = (int)placeVolHost.size();
+            const DsmcCellRec& cl = cells[(size_t)c];
+            const int nf = std::min(cl.num, 6);
+            // collectCellUniqueNodes
+            bool nodesOk = true;
+            uniq.clear();
+            for (int m = 0; m < nf && nodesOk; ++m) {
+                const int f = cl.cell2face[m];
+                if (!validFace(f)) { nodesOk = false; break; }
+                const DsmcEdgeRec& e = edges[(size_t)f];
+                if (e.faceType != 3 && e.faceType != 4) { nodesOk = false; break; }
+                for (int k = 0; k < e.faceType; ++k) {
+                    const int node = e.faceMap[k];
+                    if (node < 0 || (size_t)node * 3 + 2 >= points.size()) { nodesOk = false; break; }
+                    if (std::find(uniq.begin(), uniq.end(), node) == uniq.end()) uniq.push_back(node);
+                }
+            }
+            tets.clear();
+            bool done = false;
+            // appendTetCellTets
+            if (nodesOk && uniq.size() == 4u) done = vertexTet(uniq[0], uniq[1], uniq[2], uniq[3]);
+            // appendPyramidCellTets
+            if (!done) {
+                tets.clear();
+                int quad = -1;
+                bool ok = true;
+                for (int m = 0; m < nf; ++m) {
+                    const int f = cl.cell2face[m];
+                    if (!validFace(f)) { ok = false; break; }
+                    if (edges[(size_t)f].faceType == 4) {
+                        if (quad >= 0) { ok = false; break; }
+                        quad = f;
+                    }
+                }
+                if (ok && quad >= 0 && nodesOk && uniq.size() == 5u) {
+                    const DsmcEdgeRec& base = edges[(size_t)quad];
+                    int apex = -1;
+                    for (int node : uniq) {
+                        bool onBase = false;
+                        for (int k = 0; k < 4; ++k) onBase = onBase || base.faceMap[k] == node;
+                        if (!onBase) { apex = node; break; }
+                    }
+                    if (apex >= 0) {
+                        int t0[3], t1[3];
+                        decode_split(split[(size_t)quad], t0, t1);
+                        if (t0[0] < 0 || t1[0] < 0) decode_split(kSplit02, t0, t1);
+                        done = vertexTet(base.faceMap[t0[0]], base.faceMap[t0[1]], base.faceMap[t0[2]], apex) &&
+                               vertexTet(base.faceMap[t1[0]], base.faceMap[t1[1]], base.faceMap[t1[2]], apex);
+                    }
+                }
+            }
+            // appendCenterFaceTets
+            if (!done) {
+                tets.clear();
+                bool ok = true;
+                for (int m = 0; m < nf && ok; ++m) {
+                    const int f = cl.cell2face[m];
+                    if (!validFace(f)) { ok = false; break; }
+                    const DsmcEdgeRec& e = edges[(size_t)f];
+                    if (e.faceType == 3) {
+                        ok = centerTet(c, e.faceMap[0], e.faceMap[1], e.faceMap[2]);
+                    } else if (e.faceType == 4) {
+                        int t0[3], t1[3];
+                        decode_split(split[(size_t)f], t0, t1);
+                        if (t0[0] < 0 || t1[0] < 0) decode_split(kSplit02, t0, t1);
+                        ok = centerTet(c, e.faceMap[t0[0]], e.faceMap[t0[1]], e.faceMap[t0[2]]) &&
+                             centerTet(c, e.faceMap[t1[0]], e.faceMap[t1[1]], e.faceMap[t1[2]]);
+                    } else {
+                        ok = false;
+                    }
+                }
+                done = ok && !tets.empty();
+            }
+            if (!done) continue;
+            for (const Tet& t : tets) {
+                V.insert(V.end(), t.v, t.v + 12);
+                placeVolHost.push_back(t.vol);
+            }
+        }
+        placeOffHost[(size_t)ncell] = (int)placeVolHost.size();
     }
 
     // ------------------------------------------------------------------
@@ -580,6 +723,15 @@ struct Engine {
         M.faceRole = dRole; M.faceCells = dFaceCells; M.faceDelta = dDelta; M.faceWall = dFaceWall;
         M.wallRot = dWallRot; M.wallRotF = dWallRotF; M.cellCenter = dCenter; M.cellVolume = dVol;
         M.cell2cell = dC2c; M.revSlot = dRev;
+        {
+            std::vector<double> placeV;
+            buildPlacement(placeV);
+            int* dPlaceOff; double* dPlaceV; double* dPlaceVol;
+            if (!upload(dPlaceOff, placeOffHost) || !upload(dPlaceV, placeV) || !upload(dPlaceVol, placeVolHost) ||
+                !alloc(placeFirst, placeVolHost.size()))
+                return false;
+            M.placeOff = dPlaceOff; M.placeV = dPlaceV; M.placeVol = dPlaceVol;
+        }
 
         // --- per-cell state (Collision_constant_initial, src/MeshparticalInitial.cpp:798-810)
         std::vector<double> crInit((size_t)ncell, 3.0);
@@ -1121,7 +1273,60 @@ struct Engine {
     // probability frac(Ns), else floor(Ns); the draw for cell c is Philox
     // counter (c, 0, kPurposeFillCount, 0) under the key `seed`. Placement and
     // velocities: fill_kernel.
-    bool fillFreestream(double ppcMean, uint64_t seed)
+    // Sub-tetrahedron counts of one cell (Np_tri_inititial,
+    // src/MeshparticalInitial.cpp:481-514): Iround(Np V_t / V_cell) each,
+    // then adjust_particles (src/MeshparticalInitial.cpp:752-786) moves the
+    // sum to Np by +-1 on |delta| distinct tetrahedra chosen by a partial
+    // Fisher-Yates shuffle (all of them when |delta| reaches their number)
+    // and clamps at zero. Draws: Philox (c, t, kPurposeFillCount, 1) for the
+    // rounding of tetrahedron t, (c, i, kPurposeFillCount, 2) for shuffle
+    // step i. Returns the cell's particle count.
+    static int subTetCounts(int c, int np, const double* vol, int nt, uint32_t k0, uint32_t k1, int* first)
+    {
+        if (np <= 0 || nt <= 0) {
+            for (int t = 0; t < nt; ++t) first[t] = 0;
+            return 0;
+        }
+        double sumVol = 0.0;
+        for (int t = 0; t < nt; ++t) sumVol += vol[t];
+        std::vector<double> region((size_t)nt);
+        int sumN = 0;
+        for (int t = 0; t < nt; ++t) {
+            const double x = static_cast<double>(np) * vol[t] / sumVol;
+            const double fl = std::floor(x);
+            const U4 b = philox4x32_10(U4{(uint32_t)c, (uint32_t)t, kPurposeFillCount, 1u}, k0, k1);
+            region[(size_t)t] = (unit64(b.x, b.y) < x - fl) ? fl + 1.0 : fl;
+            sumN += static_cast<int>(region[(size_t)t]);
+        }
+        const int delta = np - sumN;
+        const int absDelta = std::abs(delta);
+        const double step = delta > 0 ? 1.0 : -1.0;
+        if (absDelta >= nt) {
+            for (int t = 0; t < nt; ++t) region[(size_t)t] += step;
+        } else if (absDelta > 0) {
+            std::vector<int> ind((size_t)nt);
+            for (int t = 0; t < nt; ++t) ind[(size_t)t] = t;
+            for (int i = 0; i < absDelta; ++i) {
+                const U4 b = philox4x32_10(U4{(uint32_t)c, (uint32_t)i, kPurposeFillCount, 2u}, k0, k1);
+                int r = i + (int)(unit64(b.x, b.y) * (double)(nt - i));
+                if (r > nt - 1) r = nt - 1;
+                std::swap(ind[(size_t)i], ind[(size_t)r]);
+            }
+            for (int i = 0; i < absDelta; ++i) region[(size_t)ind[(size_t)i]] += step;
+        }
+        int n = 0;
+        for (int t = 0; t < nt; ++t) {
+            first[t] = n;
+            n += static_cast<int>(std::max(region[(size_t)t], 0.0));
+        }
+        return n;
+    }
+
+    // The initial fill (Np_tri_inititial / meshfillpar, src/MeshparticalInitial.cpp:
+    // 413-418, 481-721) with the per-cell counts of setParticleMessage
+    // (src/meshImport.cpp:1399-1421). atRest: the reference's unit Maxwellian
+    // at rest; otherwise the case's freestream.
+    bool fill(double ppcMean, uint64_t seed, bool atRest)
     {
         if (!(ppcMean > 0.0) || !std::isfinite(ppcMean)) return fail("fill: particles per cell must be positive");
         const uint32_t k0 = (uint32_t)(seed & 0xffffffffu), k1 = (uint32_t)(seed >> 32);
@@ -1130,13 +1335,16 @@ struct Engine {
         if (!(vtot > 0.0)) return fail("fill: zero mesh volume");
         const double nps = ppcMean * (double)ncell;
         std::vector<int> st((size_t)ncell + 1, 0);
+        std::vector<int> first(placeVolHost.size(), 0);
         int64_t total = 0;
         for (int c = 0; c < ncell; ++c) {
             const double ns = cells[(size_t)c].area * nps / vtot;
             const double fl = std::floor(ns);
+            if (!(fl < 1.0e9)) return fail("fill: more than 1e9 particles in a cell");
             const U4 b = philox4x32_10(U4{(uint32_t)c, 0u, kPurposeFillCount, 0u}, k0, k1);
-            const int64_t nc = (int64_t)fl + ((unit64(b.x, b.y) < ns - fl) ? 1 : 0);
-            total += nc;
+            const int np = (int)fl + ((unit64(b.x, b.y) < ns - fl) ? 1 : 0);
+            const int t0 = placeOffHost[(size_t)c], nt = placeOffHost[(size_t)c + 1] - t0;
+            total += subTetCounts(c, np, placeVolHost.data() + t0, nt, k0, k1, first.data() + t0);
             if (total > (int64_t)0x7fffffff - 1) return fail("fill: more than 2^31 particles");
             st[(size_t)c + 1] = (int)total;
         }
@@ -1147,17 +1355,26 @@ struct Engine {
         if (!ensureCapacity(need)) return false;
         if (!cuda(cudaMemcpyAsync(start[cur], st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice, stream), "fill start"))
             return false;
+        if (!first.empty() &&
+            !cuda(cudaMemcpyAsync(placeFirst, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice, stream),
+                  "fill tetrahedra"))
+            return false;
         FillParams f{};
-        const double base = 1.0 * mess.Ma * std::sqrt(mess.gamma / 2.0) * mess.v_in / mess.v_rms;
-        f.u[0] = base * params.inflow_dir[0];
-        f.u[1] = base * params.inflow_dir[1];
-        f.u[2] = 0.0;
-        f.tN = mess.T_in / mess.T_ref;
-        f.sig = std::sqrt(f.tN / 2.0);
+        if (atRest) {
+            f.sig = 1.0;
+            f.tN = 1.0;
+        } else {
+            const double base = 1.0 * mess.Ma * std::sqrt(mess.gamma / 2.0) * mess.v_in / mess.v_rms;
+            f.u[0] = base * params.inflow_dir[0];
+            f.u[1] = base * params.inflow_dir[1];
+            f.u[2] = 0.0;
+            f.tN = mess.T_in / mess.T_ref;
+            f.sig = std::sqrt(f.tN / 2.0);
+        }
         f.keyLo = k0;
         f.keyHi = k1;
-        if (precision == DSMC_PRECISION_MIXED) launch_fill<float>(args<float>(), f, shape, stream);
-        else launch_fill<double>(args<double>(), f, shape, stream);
+        if (precision == DSMC_PRECISION_MIXED) launch_fill<float>(args<float>(), f, placeFirst, shape, stream);
+        else launch_fill<double>(args<double>(), f, placeFirst, shape, stream);
         if (!cuda(cudaGetLastError(), "fill kernel")) return false;
         StepCtl h{};
         h.nLive = (int)total;
@@ -1169,6 +1386,89 @@ struct Engine {
         haveParticles = true;
         devIstepValid = false;
         pendingInject = false;
+        return true;
+    }
+
+    // GSIS particle update (molecular_velocity_change, src/ProcessGSIS.cpp:
+    // 2239-2366) between steps; see csrc/dsmc_gsis.cu.
+    bool gsisUpdate(const double* ns, const char* accepted, DsmcGsisReport* rep)
+    {
+        if (!ns) return fail("GSIS: null nsresult");
+        if (!haveParticles) return fail("GSIS: no particles");
+        if (pendingInject) return fail("GSIS: a step is in progress (injected particles not yet sorted)");
+        // the reference stops at the first gated-in cell with a NaN density or velocity
+        int firstNan = ncell;
+        for (int c = 0; c < ncell && firstNan == ncell; ++c) {
+            if (accepted && accepted[c] == 0) continue;
+            const double* r = ns + (size_t)c * 6;
+            if (std::isnan(r[0]) || std::isnan(r[1]) || std::isnan(r[2]) || std::isnan(r[3])) firstNan = c;
+        }
+        if (!gsisNs && (!alloc(gsisNs, (size_t)ncell * 6, false) || !alloc(gsisAcc, (size_t)ncell, false) ||
+                        !alloc(gsisFlag, (size_t)ncell, false) || !alloc(gsisTally, 4, false)))
+            return false;
+        if (!cuda(cudaMemcpyAsync(gsisNs, ns, (size_t)ncell * 6 * sizeof(double), cudaMemcpyHostToDevice, stream), "GSIS ns") ||
+            (accepted && !cuda(cudaMemcpyAsync(gsisAcc, accepted, (size_t)ncell, cudaMemcpyHostToDevice, stream), "GSIS gate")) ||
+            !cuda(cudaMemsetAsync(gsisTally, 0, 4 * sizeof(unsigned long long), stream), "GSIS tally"))
+            return false;
+        GsisArgs g{};
+        g.ns = gsisNs;
+        g.accepted = accepted ? gsisAcc : nullptr;
+        g.firstNan = firstNan;
+        g.keyLo = C.seedLo;
+        g.keyHi = C.seedHi;
+        g.purpose = kPurposeGsis | ((gsisEpoch & 0xffffffu) << 8);
+        g.flag = gsisFlag;
+        g.tally = gsisTally;
+        int err0 = 0;
+        if (!cuda(cudaMemcpyAsync(&err0, errorWord, sizeof(int), cudaMemcpyDeviceToHost, stream), "error word"))
+            return false;
+        if (precision == DSMC_PRECISION_MIXED) launch_gsis_count<float>(args<float>(), g, stream);
+        else launch_gsis_count<double>(args<double>(), g, stream);
+        if (!cuda(cudaGetLastError(), "GSIS count")) return false;
+        StepCtl h{};
+        int err1 = 0;
+        if (!cuda(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, stream), "ctl") ||
+            !cuda(cudaMemcpyAsync(&err1, errorWord, sizeof(int), cudaMemcpyDeviceToHost, stream), "error word") ||
+            !cuda(cudaStreamSynchronize(stream), "GSIS count sync"))
+            return false;
+        auto abandon = [&](const std::string& m) {
+            cudaMemcpyAsync(errorWord, &err0, sizeof(int), cudaMemcpyHostToDevice, stream);
+            cudaMemsetAsync(countSlot, 0, (size_t)ncell * kSlots * sizeof(int), stream);
+            cudaStreamSynchronize(stream);
+            return fail(m);
+        };
+        if ((err1 & ~err0) & kErrGsisCount)
+            return abandon("GSIS: an NS density gives a particle count outside [0, 2^30)");
+        const int64_t nNext = h.nNext;
+        if (nNext > capacity) {
+            if (params.capacity > 0) return abandon("GSIS: more particles than the configured capacity");
+            // growing keeps the particles of A; the counts and the layout of B stay valid
+            if (!ensureCapacity(std::max<int64_t>(nNext + nNext / 2 + (1 << 16), 1 << 20))) return false;
+        }
+        if (precision == DSMC_PRECISION_MIXED) launch_gsis_rebuild<float>(args<float>(), g, shape, stream);
+        else launch_gsis_rebuild<double>(args<double>(), g, shape, stream);
+        if (!cuda(cudaGetLastError(), "GSIS rebuild")) return false;
+        cur ^= 1;
+        h.nLive = (int)nNext;
+        h.nInj = 0;
+        h.capacity = (int)capacity;
+        unsigned long long tally[4] = {0, 0, 0, 0};
+        if (!cuda(cudaMemcpyAsync(ctl, &h, sizeof h, cudaMemcpyHostToDevice, stream), "ctl") ||
+            !cuda(cudaMemsetAsync(countSlot, 0, (size_t)ncell * kSlots * sizeof(int), stream), "countSlot") ||
+            !cuda(cudaMemcpyAsync(tally, gsisTally, sizeof tally, cudaMemcpyDeviceToHost, stream), "GSIS tally") ||
+            !cuda(cudaStreamSynchronize(stream), "GSIS sync"))
+            return false;
+        hostNLive = (int)nNext;
+        devIstepValid = false;
+        ++gsisEpoch;
+        if (rep) {
+            rep->nan_cell = firstNan < ncell ? firstNan : -1;
+            rep->cells_updated = (int32_t)tally[0];
+            rep->cells_skipped = (int32_t)tally[1];
+            rep->added = (int64_t)tally[2];
+            rep->removed = (int64_t)tally[3];
+            rep->particles = nNext;
+        }
         return true;
     }
 
@@ -1244,6 +1544,7 @@ static int status_of(dsmc::Engine& e, bool ok)
     if (e.err.find("rejection loop") != std::string::npos) return DSMC_E_DEVICE_FAULT;
     if (e.err.find("self-check") != std::string::npos) return DSMC_E_DEVICE_FAULT;
     if (e.err.find("no particles") != std::string::npos) return DSMC_E_STATE;
+    if (e.err.find("in progress") != std::string::npos) return DSMC_E_STATE;
     return DSMC_E_INVALID;
 }
 
@@ -1595,7 +1896,20 @@ extern "C" {
 int dsmc_fill_freestream(DsmcHandle* h, double ppc_mean, uint64_t seed)
 {
     DSMC_GUARD(h);
-    return status_of(h->e, h->e.fillFreestream(ppc_mean, seed));
+    return status_of(h->e, h->e.fill(ppc_mean, seed, false));
+}
+
+int dsmc_fill_initial(DsmcHandle* h, double ppc_mean, uint64_t seed)
+{
+    DSMC_GUARD(h);
+    return status_of(h->e, h->e.fill(ppc_mean, seed, true));
+}
+
+int dsmc_molecular_velocity_change(DsmcHandle* h, const double* nsresult, const char* accepted,
+                                   DsmcGsisReport* report)
+{
+    DSMC_GUARD(h);
+    return status_of(h->e, h->e.gsisUpdate(nsresult, accepted, report));
 }
 
 // ---------------------------------------------------------------------------

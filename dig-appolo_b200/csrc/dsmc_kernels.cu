@@ -1365,94 +1365,75 @@ void launch_sample(const StepArgs<Real>& a, bool pre, const LaunchShape& L, cuda
 // ===========================================================================
 // initial fill (Np_tri_inititial / meshfillpar / velocityLocationGenerate,
 // src/MeshparticalInitial.cpp:481-721): particles already counted per cell
-// (startA) are placed uniformly in their cell and drawn from the freestream
-// Maxwellian. A cell is split into tetrahedra (its centroid with each face
-// triangle); a particle picks one by volume and a uniform point in it from
-// Dirichlet(1,1,1,1) weights (four exponential spacings). Particle k of cell
-// c draws from the Philox counter (c, k, kPurposeFill, block).
+// (startA) and per placement tetrahedron (tetFirst: the cell-local index of
+// each tetrahedron's first particle, counted on the host) take, in
+// tetrahedron order, a point of their tetrahedron from the reference's
+// normalised-uniform weights and a velocity u + sig * (unit Box-Muller
+// triple: sqrt(-2 ln r) sin th, sqrt(-2 ln r) cos th, sqrt(-2 ln r2) sin th2)
+// with Ir = -ln(r3) tN / 2; u = 0, sig = 1, tN = 1 is the reference's own
+// unit Maxwellian at rest. Particle k of cell c draws from the Philox
+// counters (c, k, kPurposeFill, 0..4): (r, th), (r2, th2), (r3, w0),
+// (w1, w2), (w3, -).
 // ===========================================================================
 template <typename Real>
-__global__ void __launch_bounds__(256) fill_kernel(StepArgs<Real> a, FillParams f)
+__global__ void __launch_bounds__(256) fill_kernel(StepArgs<Real> a, FillParams f, const int* __restrict__ tetFirst)
 {
-    __shared__ double cumS[8][32];
     const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     constexpr bool mixed = sizeof(Real) == 4;
+    constexpr double kTwoPi = 6.283185307179586;   // 2 * M_PI
     for (int c = warp; c < a.M.ncell; c += nwarps) {
         const int s0 = a.startA[c];
         const int n = a.startA[c + 1] - s0;
-        if (n == 0) continue;
-        const int t0 = a.M.triOffset[c];
-        const int nt = min(a.M.triOffset[c + 1] - t0, 32);
+        const int t0 = a.M.placeOff[c], t1 = a.M.placeOff[c + 1];
+        if (n == 0 || t1 <= t0) continue;
         const double cx = a.M.cellCenter[(size_t)c * 3 + 0], cy = a.M.cellCenter[(size_t)c * 3 + 1],
                      cz = a.M.cellCenter[(size_t)c * 3 + 2];
-        double vol = 0.0;
-        if (lane < nt) {
-            const double* T = a.M.triD + (size_t)(t0 + lane) * 9;
-            const double ax = T[0] - cx, ay = T[1] - cy, az = T[2] - cz;
-            vol = fabs(ax * (T[4] * T[8] - T[5] * T[7]) - ay * (T[3] * T[8] - T[5] * T[6]) +
-                       az * (T[3] * T[7] - T[4] * T[6])) / 6.0;
-        }
-        double cum = vol;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const double y = __shfl_up_sync(kFull, cum, o);
-            if (lane >= o) cum += y;
-        }
-        cumS[wib][lane] = cum;
-        __syncwarp();
-        const double total = cumS[wib][31];
         for (int k = lane; k < n; k += 32) {
+            int t = t0;
+            for (int q = t0 + 1; q < t1; ++q)
+                if (tetFirst[q] <= k) t = q;
             const uint32_t cc = (uint32_t)c, kk = (uint32_t)k;
             const U4 b0 = philox4x32_10(U4{cc, kk, kPurposeFill, 0u}, f.keyLo, f.keyHi);
             const U4 b1 = philox4x32_10(U4{cc, kk, kPurposeFill, 1u}, f.keyLo, f.keyHi);
             const U4 b2 = philox4x32_10(U4{cc, kk, kPurposeFill, 2u}, f.keyLo, f.keyHi);
             const U4 b3 = philox4x32_10(U4{cc, kk, kPurposeFill, 3u}, f.keyLo, f.keyHi);
             const U4 b4 = philox4x32_10(U4{cc, kk, kPurposeFill, 4u}, f.keyLo, f.keyHi);
-            // sub-tetrahedron by volume
-            const double pick = unit64(b0.x, b0.y) * total;
-            int t = nt - 1;
-            for (int q = 0; q < nt; ++q)
-                if (pick < cumS[wib][q]) { t = q; break; }
-            const double* T = a.M.triD + (size_t)(t0 + t) * 9;
-            const double ax = T[0] - cx, ay = T[1] - cy, az = T[2] - cz;
-            const double e0 = -log(unit64(b0.z, b0.w)), e1 = -log(unit64(b1.x, b1.y));
-            const double e2 = -log(unit64(b1.z, b1.w)), e3 = -log(unit64(b2.x, b2.y));
-            const double inv = 1.0 / (e0 + e1 + e2 + e3);
-            const double wA = (e1 + e2 + e3) * inv, wB = e2 * inv, wC = e3 * inv;   // e0: the centroid's weight
-            const double rx = wA * ax + wB * T[3] + wC * T[6];
-            const double ry = wA * ay + wB * T[4] + wC * T[7];
-            const double rz = wA * az + wB * T[5] + wC * T[8];
-            // freestream Maxwellian (Box-Muller) and rotational energy
-            const double rad1 = sqrt(-2.0 * log(unit64(b2.z, b2.w)));
-            double s1, c1;
-            sincospi(2.0 * unit64(b3.x, b3.y), &s1, &c1);
-            const double rad2 = sqrt(-2.0 * log(unit64(b3.z, b3.w)));
-            double s2, c2;
-            sincospi(2.0 * unit64(b4.x, b4.y), &s2, &c2);
-            const double ir = -log(unit64(b4.z, b4.w)) * f.tN * 0.5;
+            const double rad1 = sqrt(dm(-2.0, log(unit64(b0.x, b0.y))));
+            const double th1 = dm(kTwoPi, unit64(b0.z, b0.w));
+            const double rad2 = sqrt(dm(-2.0, log(unit64(b1.x, b1.y))));
+            const double th2 = dm(kTwoPi, unit64(b1.z, b1.w));
+            const double ir = dm(dm(-log(unit64(b2.x, b2.y)), f.tN), 0.5);
+            double x[3];
+            place_point(a.M.placeV + (size_t)t * 12, unit64(b2.z, b2.w), unit64(b3.x, b3.y), unit64(b3.z, b3.w),
+                        unit64(b4.x, b4.y), x);
             const int o = s0 + k;
             if constexpr (mixed) {
-                a.A.x[0][o] = (Real)rx; a.A.x[1][o] = (Real)ry; a.A.x[2][o] = (Real)rz;
+                a.A.x[0][o] = (Real)(x[0] - cx); a.A.x[1][o] = (Real)(x[1] - cy); a.A.x[2][o] = (Real)(x[2] - cz);
             } else {
-                a.A.x[0][o] = (Real)(cx + rx); a.A.x[1][o] = (Real)(cy + ry); a.A.x[2][o] = (Real)(cz + rz);
+                a.A.x[0][o] = x[0]; a.A.x[1][o] = x[1]; a.A.x[2][o] = x[2];
             }
-            a.A.v[0][o] = (Real)(f.u[0] + f.sig * rad1 * c1);
-            a.A.v[1][o] = (Real)(f.u[1] + f.sig * rad1 * s1);
-            a.A.v[2][o] = (Real)(f.u[2] + f.sig * rad2 * c2);
+            a.A.v[0][o] = (Real)da(f.u[0], dm(f.sig, dm(rad1, sin(th1))));
+            a.A.v[1][o] = (Real)da(f.u[1], dm(f.sig, dm(rad1, cos(th1))));
+            a.A.v[2][o] = (Real)da(f.u[2], dm(f.sig, dm(rad2, sin(th2))));
             a.A.ir[o] = (Real)ir;
             a.A.cell[o] = c;
         }
-        __syncwarp();
     }
 }
 
 template <typename Real>
-void launch_fill(const StepArgs<Real>& a, const FillParams& f, const LaunchShape& L, cudaStream_t s)
+void launch_fill(const StepArgs<Real>& a, const FillParams& f, const int* tetFirst, const LaunchShape& L,
+                 cudaStream_t s)
 {
-    fill_kernel<Real><<<L.smCount * 8, 256, 0, s>>>(a, f);
+    fill_kernel<Real><<<L.smCount * 8, 256, 0, s>>>(a, f, tetFirst);
+}
+
+void launch_scan_counts(const int* countSlot, int ncell, int* partial, int* start, StepCtl* ctl, cudaStream_t s)
+{
+    scan_partial_kernel<<<kScanBlocks, 256, 0, s>>>(countSlot, ncell, partial);
+    scan_final_kernel<<<kScanBlocks, 256, 0, s>>>(countSlot, ncell, partial, start, ctl);
 }
 
 // ===========================================================================
@@ -1533,7 +1514,8 @@ void launch_trace_check(const DevMesh& M, const DevConsts& C, int n, const Real*
     template void launch_sort<Real>(const StepArgs<Real>&, const LaunchShape&, cudaStream_t);                    \
     template void launch_collide<Real>(const StepArgs<Real>&, const LaunchShape&, cudaStream_t);                 \
     template void launch_sample<Real>(const StepArgs<Real>&, bool, const LaunchShape&, cudaStream_t);            \
-    template void launch_fill<Real>(const StepArgs<Real>&, const FillParams&, const LaunchShape&, cudaStream_t); \
+    template void launch_fill<Real>(const StepArgs<Real>&, const FillParams&, const int*, const LaunchShape&,    \
+                                    cudaStream_t);                                                               \
     template cudaError_t prepare_kernels<Real>();                                                                \
     template void launch_trace_check<Real>(const DevMesh&, const DevConsts&, int, const Real*, const Real*,       \
                                            const Real*, const Real*, const Real*, const Real*, const double*,    \

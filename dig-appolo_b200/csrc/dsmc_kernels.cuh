@@ -98,7 +98,26 @@ struct FillParams {
     double tN;        // temperature (rotational energy mean tN/2)
     uint32_t keyLo, keyHi;
 };
-template <typename Real> void launch_fill(const StepArgs<Real>& a, const FillParams& f, const LaunchShape& L, cudaStream_t s);
+template <typename Real>
+void launch_fill(const StepArgs<Real>& a, const FillParams& f, const int* tetFirst, const LaunchShape& L, cudaStream_t s);
+// exclusive scan of the countSlot rows into start[0..ncell], total into ctl->nNext
+void launch_scan_counts(const int* countSlot, int ncell, int* partial, int* start, StepCtl* ctl, cudaStream_t s);
+
+// GSIS particle update (molecular_velocity_change, src/ProcessGSIS.cpp:2239-2366)
+struct GsisArgs {
+    const double* ns;                // [ncell*6] density / n_ref, u (3), T, Tr
+    const unsigned char* accepted;   // [ncell] or nullptr (acceptance gate off)
+    int firstNan;                    // cells from this one on are left untouched
+    uint32_t keyLo, keyHi;
+    uint32_t purpose;                // kPurposeGsis | epoch << 8
+    int* flag;                       // [ncell] 1: the cell is updated
+    unsigned long long* tally;       // [4] cells updated, cells skipped, particles added, removed
+};
+// target counts into the countSlot rows and their scan into startB / ctl->nNext
+template <typename Real> void launch_gsis_count(const StepArgs<Real>& a, const GsisArgs& g, cudaStream_t s);
+// B from A: kept, copied, sampled and deleted particles, then the per-cell linear map
+template <typename Real> void launch_gsis_rebuild(const StepArgs<Real>& a, const GsisArgs& g, const LaunchShape& L,
+                                                  cudaStream_t s);
 template <typename Real> cudaError_t prepare_kernels();
 void launch_macro(const DevMesh& M, const DevConsts& C, const double* acc, int set, double count,
                   double* out, int ncell, cudaStream_t s);

@@ -59,6 +59,14 @@ class Counters(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in COUNTER_NAMES]
 
 
+class GsisReport(C.Structure):
+    _fields_ = [("nan_cell", C.c_int32), ("cells_updated", C.c_int32), ("cells_skipped", C.c_int32),
+                ("pad", C.c_int32), ("added", C.c_int64), ("removed", C.c_int64), ("particles", C.c_int64)]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_ if n != "pad"}
+
+
 class LaunchShape(C.Structure):
     _fields_ = [("move_threads", C.c_int32), ("move_blocks_per_sm", C.c_int32),
                 ("sort_blocks_per_sm", C.c_int32), ("collide_blocks_per_sm", C.c_int32)]
@@ -78,7 +86,9 @@ _SIGS = [
     ("dsmc_last_error", C.c_char_p, [_P]),
     ("dsmc_upload_particles", C.c_int, [_P, C.c_int64] + [_P] * 8),
     ("dsmc_particle_count", C.c_int, [_P, C.POINTER(C.c_int64)]),
+    ("dsmc_fill_initial", C.c_int, [_P, C.c_double, C.c_uint64]),
     ("dsmc_fill_freestream", C.c_int, [_P, C.c_double, C.c_uint64]),
+    ("dsmc_molecular_velocity_change", C.c_int, [_P, _P, _P, _P]),
     ("dsmc_download_particles", C.c_int, [_P, C.c_int64] + [_P] * 9),
     ("dsmc_step", C.c_int, [_P, C.c_int32, C.c_uint32]),
     ("dsmc_preprocesseffquad", C.c_int, [_P, C.c_int32]),
@@ -330,9 +340,23 @@ class Case:
         return {"cell": oi[0], "ifout": oi[1], "face": oi[2], "tri": oi[3], "ncross": oi[4],
                 "x": np.stack(of[:3], 1), "v": np.stack(of[3:6], 1), "dt": of[6]}
 
+    def fill_initial(self, ppc_mean: float, seed: int = 0):
+        """The reference's initial fill on the device (dsmc_fill_initial)."""
+        self._check(self.lib.dsmc_fill_initial(self.h, float(ppc_mean), int(seed)), "dsmc_fill_initial")
+
     def fill_freestream(self, ppc_mean: float, seed: int = 0):
-        """Device-side initial fill (dsmc_fill_freestream)."""
+        """The initial fill with the case's freestream (dsmc_fill_freestream)."""
         self._check(self.lib.dsmc_fill_freestream(self.h, float(ppc_mean), int(seed)), "dsmc_fill_freestream")
+
+    def molecular_velocity_change(self, nsresult, accepted=None) -> dict:
+        """GSIS particle update (dsmc_molecular_velocity_change); nsresult
+        [ncell, 6], accepted [ncell] or None."""
+        ns = np.ascontiguousarray(nsresult, dtype=np.float64).reshape(-1, 6)
+        acc = None if accepted is None else np.ascontiguousarray(accepted, dtype=np.int8)
+        rep = GsisReport()
+        self._check(self.lib.dsmc_molecular_velocity_change(self.h, _ptr(ns), None if acc is None else _ptr(acc),
+                                                            C.byref(rep)), "dsmc_molecular_velocity_change")
+        return rep.as_dict()
 
     # -- launch shapes ----------------------------------------------------------
     def launch_shape(self) -> dict:

@@ -196,20 +196,72 @@ int dsmc_upload_particles(DsmcHandle* h, int64_t n,
                           const double* vx, const double* vy, const double* vz,
                           const double* ir, const int32_t* cell);
 
-/* Replace all particles by an initial fill made on the device (replaces
- * Np_tri_inititial / meshfillpar / velocityLocationGenerate,
- * src/MeshparticalInitial.cpp:481-721, with the per-cell counts of
- * setParticleMessage, src/meshImport.cpp:1399-1421): cell c gets
- * floor(Ns) or floor(Ns) + 1 particles (the latter with probability
- * frac(Ns)), Ns = V_c * ppc_mean * ncell / V_total, placed uniformly in the
- * cell (split into tetrahedra from its centroid to its face triangles, as
- * the reference's centre-face split). Velocities: the freestream Maxwellian
- * of the case (its inflow drift and T_in) where the reference draws a unit
- * Maxwellian at rest that its GSIS start-up then replaces; Ir from the
- * equilibrium distribution at T_in. seed keys the fill's random streams.
+/* Replace all particles by the reference's initial fill, made on the device
+ * (MeshparticalInitial's constructor fill: Np_tri_inititial / meshfillpar /
+ * velocityLocationGenerate, src/MeshparticalInitial.cpp:413-418, 481-721,
+ * with the per-cell counts of setParticleMessage, src/meshImport.cpp:
+ * 1399-1421). Cell c gets Np = floor(Ns) or floor(Ns) + 1 particles (the
+ * latter with probability frac(Ns)), Ns = V_c * ppc_mean * ncell / V_total.
+ * The cell is split into placement tetrahedra as buildCellInitTets does
+ * (a tetrahedral cell is one; a pyramid two, base triangles with the apex;
+ * other cells the centre with each face triangle); tetrahedron t gets
+ * Iround(Np V_t / V_cell) particles, adjusted by +-1 on randomly chosen
+ * tetrahedra to sum to Np (adjust_particles, clamped at zero). A particle
+ * is the point a V0 + b V1 + c V2 + d V3 of its tetrahedron with (a, b, c,
+ * d) four uniforms divided by their sum (randomBarycentric4; not uniform in
+ * the tetrahedron, denser towards its centroid, as in the reference), a unit
+ * Maxwellian velocity at rest (Box-Muller: sqrt(-2 ln r) sin th,
+ * sqrt(-2 ln r) cos th, sqrt(-2 ln r2) sin th2) and Ir = -ln(r3) / 2.
+ * seed keys the fill's random streams (Philox). */
+int dsmc_fill_initial(DsmcHandle* h, double ppc_mean, uint64_t seed);
+
+/* dsmc_fill_initial's counts and placement with the case's freestream
+ * instead of the unit Maxwellian at rest: drift Ma sqrt(gamma/2) v_in / v_rms
+ * along the inflow direction, thermal spread sqrt(T/2) per component and
+ * Ir = -ln(r3) T / 2, T = T_in / T_ref (computeBoundaryGasState,
+ * src/ProcessDSMC.cpp:2318-2367). This is the state the reference's coupled
+ * start-up reaches when its first GSIS update shifts the fill to a uniform
+ * freestream (dsmc_molecular_velocity_change does the same on the device).
  * The freestream number density corresponds to ppc_mean equal to the
  * particles per cell the case's Neff was set for (meshMessage). */
 int dsmc_fill_freestream(DsmcHandle* h, double ppc_mean, uint64_t seed);
+
+/* Outcome of a GSIS particle update. */
+typedef struct DsmcGsisReport {
+    int32_t nan_cell;        /* first cell with a NaN NS density or velocity (the
+                                update stops before it), -1 when there is none */
+    int32_t cells_updated;   /* cells brought to their NS state */
+    int32_t cells_skipped;   /* cells the acceptance gate left alone */
+    int32_t pad;
+    int64_t added;           /* particles copied or sampled */
+    int64_t removed;         /* particles deleted */
+    int64_t particles;       /* particles after the update */
+} DsmcGsisReport;
+
+/* The GSIS particle update between two steps, on the device
+ * (ProcessGSIS::molecular_velocity_change with replication, deletion,
+ * MaxwellianSample and randomlocation, src/ProcessGSIS.cpp:2239-2530).
+ * nsresult [ncell][6]: the NS solution per cell, density / n_ref, velocity
+ * (3), T and Tr in the particle state's normalisation. accepted [ncell] or
+ * NULL: when given (the acceptance gate is on) cells with accepted[c] == 0
+ * are left untouched. Cells are taken in order and the update stops at the
+ * first gated-in cell whose density or velocity is NaN (report->nan_cell).
+ * Each updated cell is brought to Iround(density V_c n_ref / Neff)
+ * particles, by copying particles chosen uniformly from the growing bucket
+ * to random points of the cell (sampling a Maxwellian at the NS state when
+ * the cell is empty, unless T < 0) or by deleting uniformly chosen
+ * particles (the last one fills the hole); a deletion of more particles
+ * than the cell holds (negative density) is refused, as in the reference.
+ * Then v -> k v + b and Ir -> kr Ir with k = sqrt(T_ns / T), b = u_ns - k u,
+ * kr = Tr_ns / Tr from the cell's moments (T = 2/(3N) (sum v^2 - N u^2),
+ * Tr = 4 / dr / N sum Ir), when T, T_ns and Tr are positive. Random
+ * choices come from Philox streams keyed by the case's seed, the cell and
+ * the update's sequence number on this handle. Grows the particle store
+ * when automatic (DSMC_E_CAPACITY with a fixed capacity); a density that
+ * gives a count outside [0, 2^30) leaves the particles untouched and
+ * returns DSMC_E_INVALID. report may be NULL. */
+int dsmc_molecular_velocity_change(DsmcHandle* h, const double* nsresult, const char* accepted,
+                                   DsmcGsisReport* report);
 
 /* Particle count (sum of bucket sizes). */
 int dsmc_particle_count(DsmcHandle* h, int64_t* n);

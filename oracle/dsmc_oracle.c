@@ -87,6 +87,7 @@ struct OracleCase {
     int* saccum;
     int localLazy, lastIstep;
     uint64_t ctr[8];
+    uint32_t gsisEpoch;   /* GSIS updates made so far (keys their random streams) */
 };
 
 /* ------------------------------------------------------------------------ */
@@ -1064,3 +1065,443 @@ void oracle_get_wall(const OracleCase* o, double* tally)
 }
 
 void oracle_counters(const OracleCase* o, uint64_t out[8]) { memcpy(out, o->ctr, sizeof(uint64_t) * 8); }
+
+/* ------------------------------------------------------------------------ */
+/* placement tetrahedra, initial fill and the GSIS particle update           */
+/* ------------------------------------------------------------------------ */
+static double philox_u64(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, int half)
+{
+    const uint32_t c[4] = {c0, c1, c2, c3}, k[2] = {k0, k1};
+    uint32_t out[4];
+    oracle_philox(c, k, out);
+    const uint64_t a = half ? out[2] : out[0], b = half ? out[3] : out[1];
+    const uint64_t q = (a << 21) ^ (b >> 11);
+    return ((double)q + 0.5) * 0x1.0p-53;
+}
+
+/* |(P1-P0) . ((P2-P0) x (P3-P0))| / 6: tetAbsVolume and appendCenterFaceTet,
+ * src/ProcessGSIS.cpp:660-675, 829-870 */
+static double tet_volume(const double* P0, const double* P1, const double* P2, const double* P3)
+{
+    const double ax = P1[0] - P0[0], ay = P1[1] - P0[1], az = P1[2] - P0[2];
+    const double bx = P2[0] - P0[0], by = P2[1] - P0[1], bz = P2[2] - P0[2];
+    const double cx = P3[0] - P0[0], cy = P3[1] - P0[1], cz = P3[2] - P0[2];
+    const double crx = by * cz - bz * cy, cry = bz * cx - bx * cz, crz = bx * cy - by * cx;
+    return fabs(ax * crx + ay * cry + az * crz) / 6.0;
+}
+
+static int node_ok(const OracleCase* o, int n) { return n >= 0 && n < o->npoint; }
+
+/* one tetrahedron: vertices V0 (the centre when ctr != NULL) and nodes */
+static int place_add(const OracleCase* o, const double* ctr, const int* nodes, double* V, double* vol, int* nt)
+{
+    double* v = V + (size_t)(*nt) * 12;
+    int k0 = 0;
+    if (ctr) { v[0] = ctr[0]; v[1] = ctr[1]; v[2] = ctr[2]; k0 = 1; }
+    for (int k = k0; k < 4; ++k) {
+        const int n = nodes[k - k0];
+        if (!node_ok(o, n)) return 0;
+        memcpy(v + 3 * k, o->pts + (size_t)n * 3, 3 * sizeof(double));
+    }
+    const double w = tet_volume(v, v + 3, v + 6, v + 9);
+    if (!(w > 0.0) || !isfinite(w)) return 0;
+    vol[*nt] = w;
+    ++*nt;
+    return 1;
+}
+
+/* buildCellInitTets (src/MeshparticalInitial.cpp:172-355, the same
+ * decomposition as src/ProcessGSIS.cpp:748-964) for cell c: appendTetCellTets,
+ * then appendPyramidCellTets, then appendCenterFaceTets. V gets 12 doubles
+ * and vol one per tetrahedron (room for 12). Returns the number (0: none). */
+static int place_cell(const OracleCase* o, int c, double* V, double* vol)
+{
+    const Cell* cl = &o->cells[c];
+    const int nf = cl->num < 6 ? cl->num : 6;
+    int uniq[24], nu = 0, nodesOk = 1;
+    for (int m = 0; m < nf && nodesOk; ++m) {
+        const int f = cl->cell2face[m];
+        if (f < 0 || f >= o->nface) { nodesOk = 0; break; }
+        const Edge* e = &o->edges[f];
+        if (e->faceType != 3 && e->faceType != 4) { nodesOk = 0; break; }
+        for (int k = 0; k < e->faceType; ++k) {
+            const int n = e->faceMap[k];
+            if (!node_ok(o, n)) { nodesOk = 0; break; }
+            int seen = 0;
+            for (int q = 0; q < nu; ++q) seen |= uniq[q] == n;
+            if (!seen) uniq[nu++] = n;
+        }
+    }
+    int nt = 0;
+    if (nodesOk && nu == 4 && place_add(o, NULL, uniq, V, vol, &nt)) return nt;
+    nt = 0;
+    int quad = -1, ok = 1;
+    for (int m = 0; m < nf; ++m) {
+        const int f = cl->cell2face[m];
+        if (f < 0 || f >= o->nface) { ok = 0; break; }
+        if (o->edges[f].faceType == 4) {
+            if (quad >= 0) { ok = 0; break; }
+            quad = f;
+        }
+    }
+    if (ok && quad >= 0 && nodesOk && nu == 5) {
+        const Edge* b = &o->edges[quad];
+        int apex = -1;
+        for (int q = 0; q < nu && apex < 0; ++q) {
+            int on = 0;
+            for (int k = 0; k < 4; ++k) on |= b->faceMap[k] == uniq[q];
+            if (!on) apex = uniq[q];
+        }
+        if (apex >= 0) {
+            int t0[3], t1[3];
+            decode_split(o->split ? o->split[quad] : 0, t0, t1);
+            if (t0[0] < 0 || t1[0] < 0) decode_split(0, t0, t1);
+            const int a[4] = {b->faceMap[t0[0]], b->faceMap[t0[1]], b->faceMap[t0[2]], apex};
+            const int d[4] = {b->faceMap[t1[0]], b->faceMap[t1[1]], b->faceMap[t1[2]], apex};
+            if (place_add(o, NULL, a, V, vol, &nt) && place_add(o, NULL, d, V, vol, &nt)) return nt;
+        }
+    }
+    nt = 0;
+    for (int m = 0; m < nf; ++m) {
+        const int f = cl->cell2face[m];
+        if (f < 0 || f >= o->nface) return 0;
+        const Edge* e = &o->edges[f];
+        if (e->faceType == 3) {
+            if (!place_add(o, cl->cellXY, e->faceMap, V, vol, &nt)) return 0;
+        } else if (e->faceType == 4) {
+            int t0[3], t1[3];
+            decode_split(o->split ? o->split[f] : 0, t0, t1);
+            if (t0[0] < 0 || t1[0] < 0) decode_split(0, t0, t1);
+            const int a[3] = {e->faceMap[t0[0]], e->faceMap[t0[1]], e->faceMap[t0[2]]};
+            const int d[3] = {e->faceMap[t1[0]], e->faceMap[t1[1]], e->faceMap[t1[2]]};
+            if (!place_add(o, cl->cellXY, a, V, vol, &nt) || !place_add(o, cl->cellXY, d, V, vol, &nt)) return 0;
+        } else {
+            return 0;
+        }
+    }
+    return nt;
+}
+
+int oracle_placement(const OracleCase* o, int* off, double* V, double* vol)
+{
+    double v[12 * 12], w[12];
+    int n = 0;
+    for (int c = 0; c < o->ncell; ++c) {
+        const int nt = place_cell(o, c, v, w);
+        if (off) off[c] = n;
+        if (V) memcpy(V + (size_t)n * 12, v, sizeof(double) * 12 * (size_t)nt);
+        if (vol) memcpy(vol + n, w, sizeof(double) * (size_t)nt);
+        n += nt;
+    }
+    if (off) off[o->ncell] = n;
+    return n;
+}
+
+/* randomBarycentric4 (src/MeshparticalInitial.cpp:85-106): four uniforms
+ * over their sum; the point a V0 + b V1 + c V2 + d V3 */
+static void place_point(const double* V, double r0, double r1, double r2, double r3, double out[3])
+{
+    const double sum = r0 + r1 + r2 + r3;
+    double a = 0.25, b = 0.25, c = 0.25, d = 0.25;
+    if (sum > 0.0 && isfinite(sum)) { a = r0 / sum; b = r1 / sum; c = r2 / sum; d = r3 / sum; }
+    for (int k = 0; k < 3; ++k) out[k] = a * V[k] + b * V[3 + k] + c * V[6 + k] + d * V[9 + k];
+}
+
+/* sampleCellLocation (src/ProcessGSIS.cpp:977-1029) with randomlocation's
+ * fallback to the cell centre (:2478-2488) */
+static void place_in_cell(const OracleCase* o, int c, double uPick, double r0, double r1, double r2, double r3,
+                          double out[3])
+{
+    double V[12 * 12], vol[12];
+    const int nt = place_cell(o, c, V, vol);
+    double total = 0.0;
+    for (int t = 0; t < nt; ++t) total += vol[t];
+    if (nt == 0 || !(total > 0.0) || !isfinite(total)) {
+        memcpy(out, o->cells[c].cellXY, 3 * sizeof(double));
+        return;
+    }
+    double pick = uPick * total;
+    int ch = nt - 1;
+    for (int t = 0; t < nt; ++t) {
+        if (pick <= vol[t]) { ch = t; break; }
+        pick -= vol[t];
+    }
+    place_point(V + (size_t)ch * 12, r0, r1, r2, r3, out);
+}
+
+/* Np_tri_inititial + adjust_particles (src/MeshparticalInitial.cpp:481-514,
+ * 752-786) with Philox draws (c, t, 4, 1) for tetrahedron t's rounding and
+ * (c, i, 4, 2) for shuffle step i; first[t] = the tetrahedron's first
+ * particle. Returns the cell's count. */
+static int fill_cell_counts(int c, int np, const double* vol, int nt, uint32_t k0, uint32_t k1, int* first)
+{
+    double region[12];
+    int ind[12];
+    if (np <= 0 || nt <= 0) {
+        for (int t = 0; t < nt; ++t) first[t] = 0;
+        return 0;
+    }
+    double sumVol = 0.0;
+    for (int t = 0; t < nt; ++t) sumVol += vol[t];
+    int sumN = 0;
+    for (int t = 0; t < nt; ++t) {
+        const double x = (double)np * vol[t] / sumVol;
+        const double fl = floor(x);
+        region[t] = (philox_u64((uint32_t)c, (uint32_t)t, 4u, 1u, k0, k1, 0) < x - fl) ? fl + 1.0 : fl;
+        sumN += (int)region[t];
+    }
+    const int delta = np - sumN;
+    const int ad = delta < 0 ? -delta : delta;
+    const double stepv = delta > 0 ? 1.0 : -1.0;
+    if (ad >= nt) {
+        for (int t = 0; t < nt; ++t) region[t] += stepv;
+    } else if (ad > 0) {
+        for (int t = 0; t < nt; ++t) ind[t] = t;
+        for (int i = 0; i < ad; ++i) {
+            int r = i + (int)(philox_u64((uint32_t)c, (uint32_t)i, 4u, 2u, k0, k1, 0) * (double)(nt - i));
+            if (r > nt - 1) r = nt - 1;
+            const int tmp = ind[i]; ind[i] = ind[r]; ind[r] = tmp;
+        }
+        for (int i = 0; i < ad; ++i) region[ind[i]] += stepv;
+    }
+    int n = 0;
+    for (int t = 0; t < nt; ++t) {
+        first[t] = n;
+        n += (int)(region[t] > 0.0 ? region[t] : 0.0);
+    }
+    return n;
+}
+
+int oracle_fill(OracleCase* o, double ppc_mean, uint64_t seed, int at_rest)
+{
+    const uint32_t k0 = (uint32_t)(seed & 0xffffffffu), k1 = (uint32_t)(seed >> 32);
+    double vtot = 0.0;
+    for (int c = 0; c < o->ncell; ++c) vtot += o->cells[c].area;
+    if (!(vtot > 0.0) || !(ppc_mean > 0.0)) return -1;
+    const double nps = ppc_mean * (double)o->ncell;
+    double u[3] = {0.0, 0.0, 0.0}, sig = 1.0, tN = 1.0;
+    if (!at_rest) {
+        const Mess* m = &o->m;
+        const double base = 1.0 * m->Ma * sqrt(m->gamma / 2.0) * m->v_in / m->v_rms;
+        u[0] = base * o->dirx;
+        u[1] = base * o->diry;
+        tN = m->T_in / m->T_ref;
+        sig = sqrt(tN / 2.0);
+    }
+    /* counts */
+    int* cnt = (int*)malloc(sizeof(int) * (size_t)o->ncell);
+    int* firsts = (int*)malloc(sizeof(int) * (size_t)o->ncell * 12);
+    int64_t total = 0;
+    double V[12 * 12], vol[12];
+    for (int c = 0; c < o->ncell; ++c) {
+        const double ns = o->cells[c].area * nps / vtot;
+        const double fl = floor(ns);
+        const int np = (int)fl + ((philox_u64((uint32_t)c, 0u, 4u, 0u, k0, k1, 0) < ns - fl) ? 1 : 0);
+        const int nt = place_cell(o, c, V, vol);
+        cnt[c] = fill_cell_counts(c, np, vol, nt, k0, k1, firsts + (size_t)c * 12);
+        total += cnt[c];
+    }
+    if (!reserve(o, total + 16)) { free(cnt); free(firsts); return -3; }
+    o->start[0] = 0;
+    for (int c = 0; c < o->ncell; ++c) o->start[c + 1] = o->start[c] + cnt[c];
+    for (int c = 0; c < o->ncell; ++c) {
+        const int nt = place_cell(o, c, V, vol);
+        const int* first = firsts + (size_t)c * 12;
+        for (int k = 0; k < cnt[c]; ++k) {
+            int t = 0;
+            for (int q = 1; q < nt; ++q)
+                if (first[q] <= k) t = q;
+            double r[10];
+            for (int b = 0; b < 5; ++b) {
+                r[2 * b] = philox_u64((uint32_t)c, (uint32_t)k, 5u, (uint32_t)b, k0, k1, 0);
+                r[2 * b + 1] = philox_u64((uint32_t)c, (uint32_t)k, 5u, (uint32_t)b, k0, k1, 1);
+            }
+            /* velocityLocationGenerate, src/MeshparticalInitial.cpp:646-721 */
+            const double rad1 = sqrt(-2.0 * log(r[0])), th1 = 2 * M_PI * r[1];
+            const double rad2 = sqrt(-2.0 * log(r[2])), th2 = 2 * M_PI * r[3];
+            const int64_t j = o->start[c] + k;
+            double x[3];
+            place_point(V + (size_t)t * 12, r[5], r[6], r[7], r[8], x);
+            o->px[j] = x[0]; o->py[j] = x[1]; o->pz[j] = x[2];
+            o->vx[j] = u[0] + sig * (rad1 * sin(th1));
+            o->vy[j] = u[1] + sig * (rad1 * cos(th1));
+            o->vz[j] = u[2] + sig * (rad2 * sin(th2));
+            o->ir[j] = -log(r[4]) * tN * 0.5;
+            o->pc[j] = c;
+        }
+    }
+    free(cnt);
+    free(firsts);
+    o->n = total;
+    o->nInj = 0;
+    o->sorted = 1;
+    return 0;
+}
+
+/* molecular_velocity_change with replication, deletion, MaxwellianSample and
+ * randomlocation (src/ProcessGSIS.cpp:2239-2530). The reference's mt19937
+ * and rand() draws are replaced by Philox counters (cell, j, 6 | sub << 4 |
+ * epoch << 8, block) under the case's seed: sub 0 the count rounding, 1 the
+ * deletion draws (two per block), 2 the copies (choice, pick, 4 weights),
+ * 3 the Maxwellian samples (3 x (r, th), (r, pick), 4 weights). Particles
+ * are rebuilt cell by cell in the reference's bucket order. report: nan
+ * cell (-1 none), cells updated, cells skipped, added, removed, particles.
+ * Returns -2 (particles untouched) if a count falls outside [0, 2^30). */
+int oracle_molecular_velocity_change(OracleCase* o, const double* ns, const char* accepted, int64_t report[6])
+{
+    const int ncell = o->ncell;
+    const uint32_t P = 6u | ((o->gsisEpoch & 0xffffffu) << 8);
+    int firstNan = ncell;
+    for (int c = 0; c < ncell && firstNan == ncell; ++c) {
+        if (accepted && accepted[c] == 0) continue;
+        const double* r = ns + (size_t)c * 6;
+        if (isnan(r[0]) || isnan(r[1]) || isnan(r[2]) || isnan(r[3])) firstNan = c;
+    }
+    int* target = (int*)malloc(sizeof(int) * (size_t)ncell);
+    char* upd = (char*)calloc((size_t)ncell, 1);
+    int64_t updated = 0, skipped = 0, added = 0, removed = 0, total = 0;
+    for (int c = 0; c < ncell; ++c) {
+        const int n0 = o->start[c + 1] - o->start[c];
+        target[c] = n0;
+        if (c < firstNan) {
+            if (accepted && accepted[c] == 0) {
+                ++skipped;
+            } else {
+                upd[c] = 1;
+                ++updated;
+                const double* r = ns + (size_t)c * 6;
+                /* n_ns = nsresult * (area * n_ref) / Neff, Iround
+                 * (src/MeshparticalInitial.cpp:730-742) */
+                const double x = r[0] * (o->cells[c].area * o->m.n_ref) / o->m.Neff;
+                const double fl = floor(x);
+                const double nns = (philox_u64((uint32_t)c, 0u, P, 0u, o->k0, o->k1, 0) < x - fl) ? fl + 1.0 : fl;
+                if (nns > (double)n0) {
+                    if (!(nns < 1073741824.0)) { free(target); free(upd); return -2; }
+                    if (!(n0 == 0 && r[4] < 0.0)) target[c] = (int)nns;
+                } else if (nns < (double)n0 && nns >= 0.0) {
+                    target[c] = (int)nns;
+                }
+            }
+        }
+        if (target[c] > n0) added += target[c] - n0;
+        else removed += n0 - target[c];
+        total += target[c];
+    }
+    double *nx = (double*)malloc(sizeof(double) * (size_t)(total + 1)), *ny = (double*)malloc(sizeof(double) * (size_t)(total + 1)),
+           *nz = (double*)malloc(sizeof(double) * (size_t)(total + 1)), *nvx = (double*)malloc(sizeof(double) * (size_t)(total + 1)),
+           *nvy = (double*)malloc(sizeof(double) * (size_t)(total + 1)), *nvz = (double*)malloc(sizeof(double) * (size_t)(total + 1)),
+           *nir = (double*)malloc(sizeof(double) * (size_t)(total + 1));
+    int* npc = (int*)malloc(sizeof(int) * (size_t)(total + 1));
+    int* nstart = (int*)malloc(sizeof(int) * ((size_t)ncell + 1));
+    nstart[0] = 0;
+    for (int c = 0; c < ncell; ++c) nstart[c + 1] = nstart[c] + target[c];
+    int cap = 64;
+    int* perm = (int*)malloc(sizeof(int) * (size_t)cap);
+    for (int c = 0; c < ncell; ++c) {
+        const int sA = o->start[c], n0 = o->start[c + 1] - sA;
+        const int sB = nstart[c], n1 = target[c];
+        const int need = (n0 > n1 ? n0 : n1) + 1;
+        if (need > cap) { cap = need; perm = (int*)realloc(perm, sizeof(int) * (size_t)cap); }
+        /* perm[q]: the old particle at bucket position q (copies: the original) */
+        for (int k = 0; k < n0; ++k) perm[k] = k;
+        const double* r = ns + (size_t)c * 6;
+        int sampled = 0;
+        if (n1 < n0) {
+            for (int j = 0; j < n0 - n1; ++j) {   /* deletion, src/ProcessGSIS.cpp:2490-2530 */
+                const int m = n0 - j;
+                int kp = (int)(philox_u64((uint32_t)c, (uint32_t)(j >> 1), P | (1u << 4), 0u, o->k0, o->k1, j & 1) * (double)m);
+                if (kp > m - 1) kp = m - 1;
+                perm[kp] = perm[m - 1];
+            }
+        } else if (n1 > n0 && n0 > 0) {
+            for (int j = 0; j < n1 - n0; ++j) {   /* replication, src/ProcessGSIS.cpp:2368-2441 */
+                const int m = n0 + j;
+                int kp = (int)(philox_u64((uint32_t)c, (uint32_t)j, P | (2u << 4), 0u, o->k0, o->k1, 0) * (double)m);
+                if (kp > m - 1) kp = m - 1;
+                perm[n0 + j] = perm[kp];
+            }
+        } else if (n1 > n0) {
+            sampled = 1;
+        }
+        for (int q = 0; q < n1; ++q) {
+            const int64_t to = sB + q;
+            npc[to] = c;
+            if (sampled) {   /* MaxwellianSample, src/ProcessGSIS.cpp:2443-2466 */
+                double w[12];
+                for (int b = 0; b < 6; ++b) {
+                    w[2 * b] = philox_u64((uint32_t)c, (uint32_t)q, P | (3u << 4), (uint32_t)b, o->k0, o->k1, 0);
+                    w[2 * b + 1] = philox_u64((uint32_t)c, (uint32_t)q, P | (3u << 4), (uint32_t)b, o->k0, o->k1, 1);
+                }
+                double* vv[3] = {&nvx[to], &nvy[to], &nvz[to]};
+                for (int k = 0; k < 3; ++k) {
+                    const double th = 2 * M_PI * w[2 * k + 1];
+                    *vv[k] = sqrt(r[4]) * sqrt(-log(w[2 * k])) * sin(th) + r[1 + k];
+                }
+                nir[to] = -log(w[6]) * 0.5 * r[5];
+                double x[3];
+                place_in_cell(o, c, w[7], w[8], w[9], w[10], w[11], x);
+                nx[to] = x[0]; ny[to] = x[1]; nz[to] = x[2];
+                continue;
+            }
+            const int64_t from = sA + perm[q];
+            nvx[to] = o->vx[from]; nvy[to] = o->vy[from]; nvz[to] = o->vz[from]; nir[to] = o->ir[from];
+            if (q < n0) {
+                nx[to] = o->px[from]; ny[to] = o->py[from]; nz[to] = o->pz[from];
+            } else {   /* randomlocation of copy j = q - n0 */
+                const uint32_t j = (uint32_t)(q - n0);
+                double w[6];
+                for (int b = 0; b < 3; ++b) {
+                    w[2 * b] = philox_u64((uint32_t)c, j, P | (2u << 4), (uint32_t)b, o->k0, o->k1, 0);
+                    w[2 * b + 1] = philox_u64((uint32_t)c, j, P | (2u << 4), (uint32_t)b, o->k0, o->k1, 1);
+                }
+                double x[3];
+                place_in_cell(o, c, w[1], w[2], w[3], w[4], w[5], x);
+                nx[to] = x[0]; ny[to] = x[1]; nz[to] = x[2];
+            }
+        }
+        if (!upd[c] || n1 == 0) continue;
+        /* the linear map, src/ProcessGSIS.cpp:2290-2343 */
+        double n = 0.0, u[3] = {0.0, 0.0, 0.0}, T = 0.0, Tr = 0.0;
+        for (int q = sB; q < sB + n1; ++q) {
+            n += 1.0;
+            u[0] += nvx[q]; u[1] += nvy[q]; u[2] += nvz[q];
+            T += (nvx[q] * nvx[q] + nvy[q] * nvy[q] + nvz[q] * nvz[q]);
+            Tr += nir[q];
+        }
+        const double Np = n;
+        u[0] = u[0] / Np; u[1] = u[1] / Np; u[2] = u[2] / Np;
+        const double u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+        T = 2.0 / (3.0 * Np) * (T - Np * u2);
+        Tr = 4.0 / o->m.dr / Np * Tr;
+        double k = 1.0, kr = 1.0, b[3] = {0.0, 0.0, 0.0};
+        if (T > 0 && r[4] > 0 && Tr > 0) {
+            k = sqrt(r[4] / T);
+            b[0] = r[1] - k * u[0]; b[1] = r[2] - k * u[1]; b[2] = r[3] - k * u[2];
+            kr = r[5] / Tr;
+        }
+        for (int q = sB; q < sB + n1; ++q) {
+            nvx[q] = k * nvx[q] + b[0];
+            nvy[q] = k * nvy[q] + b[1];
+            nvz[q] = k * nvz[q] + b[2];
+            nir[q] = kr * nir[q];
+        }
+    }
+    free(perm);
+    if (!reserve(o, total + 16)) return -3;
+    memcpy(o->px, nx, sizeof(double) * (size_t)total); memcpy(o->py, ny, sizeof(double) * (size_t)total);
+    memcpy(o->pz, nz, sizeof(double) * (size_t)total); memcpy(o->vx, nvx, sizeof(double) * (size_t)total);
+    memcpy(o->vy, nvy, sizeof(double) * (size_t)total); memcpy(o->vz, nvz, sizeof(double) * (size_t)total);
+    memcpy(o->ir, nir, sizeof(double) * (size_t)total); memcpy(o->pc, npc, sizeof(int) * (size_t)total);
+    memcpy(o->start, nstart, sizeof(int) * ((size_t)ncell + 1));
+    free(nx); free(ny); free(nz); free(nvx); free(nvy); free(nvz); free(nir); free(npc); free(nstart);
+    free(target); free(upd);
+    o->n = total;
+    o->nInj = 0;
+    o->sorted = 1;
+    ++o->gsisEpoch;
+    if (report) {
+        report[0] = firstNan < ncell ? firstNan : -1;
+        report[1] = updated; report[2] = skipped; report[3] = added; report[4] = removed; report[5] = total;
+    }
+    return 0;
+}

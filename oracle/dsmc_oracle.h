@@ -68,6 +68,14 @@ void oracle_get_counts(const OracleCase* o, int* ppc, double* window_samples, ch
 void oracle_get_wall(const OracleCase* o, double* tally);        /* [nface][6] */
 /* injected, removed, dropped, lost, wall_hits, crossings, pairs, collisions */
 void oracle_counters(const OracleCase* o, uint64_t out[8]);
+/* Placement tetrahedra (buildCellInitTets): off[ncell+1], V[nplace*12],
+ * vol[nplace] (any may be NULL); returns nplace. */
+int oracle_placement(const OracleCase* o, int* off, double* V, double* vol);
+/* Initial fill as dsmc_fill_initial (at_rest = 1) / dsmc_fill_freestream. */
+int oracle_fill(OracleCase* o, double ppc_mean, uint64_t seed, int at_rest);
+/* GSIS particle update as dsmc_molecular_velocity_change; report: nan cell,
+ * cells updated, cells skipped, added, removed, particles. */
+int oracle_molecular_velocity_change(OracleCase* o, const double* ns, const char* accepted, int64_t report[6]);
 
 #ifdef __cplusplus
 }

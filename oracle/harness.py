@@ -116,3 +116,36 @@ def run(cas: str, mess, x, v, ir, cell, nsteps: int, seed: int, roles: str = "-"
         res["sparse_state"] = np.fromfile(os.path.join(out, "sparse_state.bin"), dtype=np.uint8)
         res["particles"] = _read_particles(os.path.join(out, "particles.bin"))
         return res
+
+
+def gsis(cas: str, mess, x, v, ir, cell, nsresult, accepted=None, seed: int = 1, roles: str = "-") -> dict:
+    """The reference's molecular_velocity_change on the given particles and
+    NS solution; buckets in order."""
+    n = int(np.asarray(cell).shape[0])
+    with tempfile.TemporaryDirectory() as d:
+        pm, pp, pn, pa, po = (os.path.join(d, k) for k in ("mess.bin", "parts.bin", "ns.bin", "acc.bin", "out.bin"))
+        _write_mess(pm, mess)
+        _write_particles(pp, x, v, ir, np.zeros(n), cell)
+        np.ascontiguousarray(nsresult, dtype=np.float64).tofile(pn)
+        if accepted is None:
+            pa = "-"
+        else:
+            np.ascontiguousarray(accepted, dtype=np.int8).tofile(pa)
+        _run(["gsis", cas, pm, pp, pn, pa, po, seed, roles])
+        return _read_particles(po)
+
+
+def fill(cas: str, mess, counts, seed: int = 1) -> dict:
+    """The reference's initial fill of every cell with counts[c] particles
+    (Np_tri_inititial + meshfillpar); buckets in order plus the
+    per-tetrahedron counts."""
+    with tempfile.TemporaryDirectory() as d:
+        pm, pc = os.path.join(d, "mess.bin"), os.path.join(d, "counts.bin")
+        _write_mess(pm, mess)
+        np.ascontiguousarray(counts, dtype=np.int32).tofile(pc)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        _run(["fill", cas, pm, pc, out, seed])
+        res = _read_particles(os.path.join(out, "particles.bin"))
+        res["np_tri"] = np.fromfile(os.path.join(out, "np_tri.bin"), dtype=np.int32)
+        return res

@@ -43,6 +43,12 @@ def load():
         lib.oracle_get_counts.argtypes = [_P, _P, _P, _P, _P]
         lib.oracle_get_wall.argtypes = [_P, _P]
         lib.oracle_counters.argtypes = [_P, _P]
+        lib.oracle_placement.restype = C.c_int
+        lib.oracle_placement.argtypes = [_P, _P, _P, _P]
+        lib.oracle_fill.restype = C.c_int
+        lib.oracle_fill.argtypes = [_P, C.c_double, C.c_uint64, C.c_int]
+        lib.oracle_molecular_velocity_change.restype = C.c_int
+        lib.oracle_molecular_velocity_change.argtypes = [_P, _P, _P, _P]
         _lib = lib
     return _lib
 
@@ -164,3 +170,27 @@ class Oracle:
         self.lib.oracle_counters(self.h, _p(out))
         names = ["injected", "removed", "dropped", "lost", "wall_hits", "crossings", "candidate_pairs", "collisions"]
         return {k: int(v) for k, v in zip(names, out)}
+
+    def placement(self):
+        """Placement tetrahedra: offsets [ncell+1], vertices [nplace, 4, 3], volumes."""
+        off = np.empty(self.ncell + 1, dtype=np.int32)
+        n = int(self.lib.oracle_placement(self.h, _p(off), None, None))
+        V = np.empty((n, 4, 3))
+        vol = np.empty(n)
+        self.lib.oracle_placement(self.h, _p(off), _p(V), _p(vol))
+        return off, V, vol
+
+    def fill(self, ppc_mean, seed, at_rest=True):
+        rc = self.lib.oracle_fill(self.h, float(ppc_mean), int(seed), 1 if at_rest else 0)
+        if rc:
+            raise RuntimeError(f"oracle_fill failed {rc}")
+
+    def molecular_velocity_change(self, ns, accepted=None):
+        ns = np.ascontiguousarray(ns, dtype=np.float64).reshape(self.ncell, 6)
+        acc = None if accepted is None else np.ascontiguousarray(accepted, dtype=np.int8)
+        rep = np.zeros(6, dtype=np.int64)
+        rc = self.lib.oracle_molecular_velocity_change(self.h, _p(ns), None if acc is None else _p(acc), _p(rep))
+        if rc:
+            raise RuntimeError(f"oracle_molecular_velocity_change failed {rc}")
+        names = ["nan_cell", "cells_updated", "cells_skipped", "added", "removed", "particles"]
+        return {k: int(v) for k, v in zip(names, rep)}

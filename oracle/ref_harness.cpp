@@ -34,10 +34,21 @@
  *       statistic_macro) and dumps per-step counters, time-averaged per-cell
  *       step moments, local/record/final_record, crmax, remainders and the
  *       final particles. Prints wall time of the step loop.
+ *   gsis CAS MESS PARTS NS ACCEPTED OUT SEED ROLES
+ *       Fills the buckets, builds a ProcessGSIS over the rig (no NS solver),
+ *       sets its nsresult from NS ([ncell][6] doubles) and, unless ACCEPTED
+ *       is "-", its acceptance gate from ACCEPTED ([ncell] bytes), runs the
+ *       public molecular_velocity_change() and dumps every bucket.
+ *   fill CAS MESS COUNTS OUT SEED
+ *       For every cell c with COUNTS[c] > 0 ([ncell] int32), the public
+ *       Np_tri_inititial + meshfillpar of MeshparticalInitial (the initial
+ *       fill of one cell); dumps every bucket to OUT/particles.bin and the
+ *       per-tetrahedron counts, cell after cell, to OUT/np_tri.bin (int32).
  *   ROLES is "-" or a comma list tag:role with role in
  *       none,interface,inlet,outlet,wall.
  */
 #include "ProcessDSMC.h"
+#include "ProcessGSIS.h"
 #include "MeshparticalInitial.h"
 #include "MessagePassing.h"
 #include "meshImport.h"
@@ -175,7 +186,10 @@ void applyRoles(ProcessDSMC& p, const std::string& roles)
     p.rebuildBoundaryDerivedState();
 }
 
-bool buildRig(Rig& r, const char* cas, const char* messPath, const std::string& roles)
+// withProcess = false stops before ProcessDSMC, whose constructor takes the
+// mesh arrays over from MeshparticalInitial (src/ProcessDSMC.cpp:359-395):
+// the reference's own initial fill runs on MeshparticalInitial before that.
+bool buildRig(Rig& r, const char* cas, const char* messPath, const std::string& roles, bool withProcess = true)
 {
     std::vector<char> mb;
     if (!readFile(messPath, mb) || mb.size() != sizeof(meshMessage)) {
@@ -217,6 +231,7 @@ bool buildRig(Rig& r, const char* cas, const char* messPath, const std::string& 
     pi->cell_particle_reserve_hint.assign((std::size_t)ncell, 0);
     pi->Collision_constant_initial();
     r.partinit = pi;
+    if (!withProcess) return true;
     r.process = new ProcessDSMC(r.mesh, mess, pi, r.ctx);
     applyRoles(*r.process, roles);
     return true;
@@ -409,6 +424,63 @@ int cmdRun(int argc, char** argv)
     return ok ? 0 : 1;
 }
 
+int cmdGsis(int argc, char** argv)
+{
+    if (argc < 10) return 2;
+    Rig r;
+    if (!buildRig(r, argv[2], argv[3], argv[9])) return 1;
+    Particles P;
+    if (!readParticles(argv[4], P)) return 1;
+    const int ncell = r.process->iNcell;
+    std::vector<char> nsb;
+    if (!readFile(argv[5], nsb) || nsb.size() != (std::size_t)ncell * 6 * 8) {
+        std::fprintf(stderr, "bad NS file %s\n", argv[5]);
+        return 1;
+    }
+    const unsigned seed = (unsigned)std::strtoul(argv[8], nullptr, 10);
+    r.partinit->thread_rng().seed(seed);
+    std::srand(seed);
+    fillBuckets(r, P);
+    ProcessGSIS g(r.mesh, r.process, r.partinit, nullptr, r.ctx);
+    g.nsresult.resize((std::size_t)ncell * 6);
+    std::memcpy(g.nsresult.data(), nsb.data(), nsb.size());
+    const std::string acc = argv[6];
+    if (acc != "-") {
+        std::vector<char> ab;
+        if (!readFile(acc, ab) || ab.size() != (std::size_t)ncell) return 1;
+        g.dsmc2ns_macro_accepted.assign(ab.begin(), ab.end());
+        g.dsmc2ns_acceptance_ready = true;
+    }
+    g.molecular_velocity_change();
+    return writeParticles(argv[7], dumpBuckets(r)) ? 0 : 1;
+}
+
+int cmdFill(int argc, char** argv)
+{
+    if (argc < 7) return 2;
+    Rig r;
+    if (!buildRig(r, argv[2], argv[3], "-", false)) return 1;
+    const int ncell = r.partinit->my_ncell;
+    std::vector<char> cb;
+    if (!readFile(argv[4], cb) || cb.size() != (std::size_t)ncell * 4) return 1;
+    const unsigned seed = (unsigned)std::strtoul(argv[6], nullptr, 10);
+    r.partinit->thread_rng().seed(seed);
+    std::srand(seed);
+    const std::string out = argv[5];
+    std::vector<int> npTri;
+    for (int c = 0; c < ncell; ++c) {
+        int np = 0;
+        std::memcpy(&np, cb.data() + (std::size_t)c * 4, 4);
+        if (np <= 0) continue;
+        std::vector<double> tri;
+        r.partinit->Np_tri_inititial(c, tri, np);
+        for (double t : tri) npTri.push_back((int)t);
+        if (!tri.empty()) r.partinit->meshfillpar(c, tri);
+    }
+    bool ok = writeParticles(out + "/particles.bin", dumpBuckets(r));
+    return ok && writeFile(out + "/np_tri.bin", npTri.data(), npTri.size() * 4) ? 0 : 1;
+}
+
 }  // namespace
 
 int main(int argc, char** argv)
@@ -422,6 +494,8 @@ int main(int argc, char** argv)
     if (cmd == "trace") return cmdTrace(argc, argv);
     if (cmd == "advect") return cmdAdvect(argc, argv);
     if (cmd == "run") return cmdRun(argc, argv);
+    if (cmd == "gsis") return cmdGsis(argc, argv);
+    if (cmd == "fill") return cmdFill(argc, argv);
     std::fprintf(stderr, "unknown command %s\n", cmd.c_str());
     return 2;
 }

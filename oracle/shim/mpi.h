@@ -186,4 +186,16 @@ inline int MPI_Waitall(int n, MPI_Request* reqs, MPI_Status*)
 }
 inline int MPI_Wait(MPI_Request* r, MPI_Status* s) { return MPI_Waitall(1, r, s); }
 
+// Persistent requests serve only the NS solver's halo exchange between
+// ranks (src/MacroSolver.cpp, src/ProcessGSIS.cpp:1493), which a world of one
+// rank does not have; the harness compiles that code but never runs it, so
+// they do nothing.
+#define MPI_PROC_NULL (-1)
+inline int MPI_Send_init(const void*, int, MPI_Datatype, int, int, MPI_Comm, MPI_Request* req)
+{ *req = MPI_REQUEST_NULL; return MPI_SUCCESS; }
+inline int MPI_Recv_init(void*, int, MPI_Datatype, int, int, MPI_Comm, MPI_Request* req)
+{ *req = MPI_REQUEST_NULL; return MPI_SUCCESS; }
+inline int MPI_Startall(int, MPI_Request*) { return MPI_SUCCESS; }
+inline int MPI_Request_free(MPI_Request* req) { *req = MPI_REQUEST_NULL; return MPI_SUCCESS; }
+
 #endif

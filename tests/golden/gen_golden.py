@@ -16,8 +16,19 @@ outputs:
                  8 independently seeded reference runs (20 per cell)
   tet_trace_pin.npz tracing-check outputs on the coarse capsule tet mesh
                  (16,000 particles, stop at the first wall hit)
+  gsis_pin.npz   the reference's molecular_velocity_change on the 1/4 block
+                 mesh (gsis_edge_inputs: gate, NaN cell, emptied cells,
+                 negative densities): per-cell counts and moments after the
+                 update, how many particles kept their input position, whether
+                 every moved particle carries a kept particle's velocity, and
+                 the box-relative positions of the moved particles
+  fill_pin.npz   the reference's initial fill (Np_tri_inititial + meshfillpar)
+                 with the counts of the fill rule: per-tetrahedron counts and
+                 box-relative positions on the 1/4 block mesh (centre-face
+                 tetrahedra), sorted barycentric weights on the capsule tets,
+                 velocity and Ir moments
 
-Usage: python tests/golden/gen_golden.py
+Usage: python tests/golden/gen_golden.py [fixture ...]   (default: all)
 """
 from __future__ import annotations
 
@@ -49,76 +60,180 @@ def roles_arg(zones):
     return ",".join(f"{t}:{names[r]}" for t, r, _ in zones)
 
 
+GSIS_PPC = 12
+GSIS_SEED = 13
+FILL_PPC = 7
+FILL_SEED = 2024
+FILL_TET_CELLS = 3000
+FILL_TET_SAMPLE = 6000
+
+
+def fill_counts(dm, ppc, seed):
+    """Per-cell counts of the fill rule (setParticleMessage, with the
+    Philox draw (c, 0, 4, 0) of the CUDA library and the oracle)."""
+    from oracle import oracle as O
+    O.load()
+    vol = dm.cells["area"].astype(float)
+    nps = ppc * dm.ncell
+    vt = vol.sum()
+    key = [seed & 0xFFFFFFFF, seed >> 32]
+    out = np.empty(dm.ncell, dtype=np.int32)
+    for c in range(dm.ncell):
+        ns = vol[c] * nps / vt
+        fl = np.floor(ns)
+        b = O.philox([c, 0, 4, 0], key)
+        u = (((int(b[0]) << 21) ^ (int(b[1]) >> 11)) + 0.5) * 2.0 ** -53
+        out[c] = int(fl) + (1 if u < ns - fl else 0)
+    return out
+
+
+def gsis_summary(dm, before, after):
+    """Per-cell counts, moments and structure of a GSIS update's output."""
+    x0, v0, ir0, c0 = before
+    x1, v1, ir1, c1 = after
+    nc = dm.ncell
+    lo, hi = I.cell_boxes(dm)
+    kept = np.zeros(nc, np.int32)
+    dup_ok = np.ones(nc, bool)
+    rel = []
+    s0 = np.concatenate([[0], np.cumsum(np.bincount(c0, minlength=nc))])
+    s1 = np.concatenate([[0], np.cumsum(np.bincount(c1, minlength=nc))])
+    for c in range(nc):
+        X0 = x0[s0[c]:s0[c + 1]]
+        X1, V1 = x1[s1[c]:s1[c + 1]], v1[s1[c]:s1[c + 1]]
+        known = {tuple(p) for p in X0}
+        is_kept = np.array([tuple(p) in known for p in X1], dtype=bool)
+        kept[c] = int(is_kept.sum())
+        if len(X0) and (~is_kept).any():
+            vk = {tuple(p) for p in V1[is_kept]}
+            dup_ok[c] = all(tuple(p) in vk for p in V1[~is_kept])
+        if (~is_kept).any():
+            rel.append((X1[~is_kept] - lo[c]) / (hi[c] - lo[c]))
+    n = np.bincount(c1, minlength=nc).astype(float)
+    m = np.maximum(n, 1.0)
+    u = np.stack([np.bincount(c1, v1[:, k], nc) for k in range(3)], 1) / m[:, None]
+    return {"counts": n.astype(np.int32), "u": u, "kept": kept, "dup_ok": dup_ok,
+            "sums": np.stack([np.bincount(c1, (v1 * v1).sum(1), nc), np.bincount(c1, ir1, nc)], 1),
+            "rel": np.concatenate(rel) if rel else np.zeros((0, 3))}
+
+
+def sorted_barycentric(dm, x, cell):
+    P = dm.points.reshape(-1, 3)
+    V = P[I.tet_vertices(dm, cell)]
+    T = np.stack([V[:, 1] - V[:, 0], V[:, 2] - V[:, 0], V[:, 3] - V[:, 0]], axis=2)
+    lam = np.linalg.solve(T, (x - V[:, 0])[:, :, None])[:, :, 0]
+    return np.sort(np.concatenate([1.0 - lam.sum(1, keepdims=True), lam], axis=1), axis=1)
+
+
+def gen_gsis_fill(d):
+    raw, dm = I.block_mesh()
+    cas = os.path.join(d, "b4g.cas")
+    M.write_cas(cas, raw)
+    mess = I.block_mess(dm, STATS_PPC)
+    parts, ns, acc, nan_cell, empty, neg = I.gsis_edge_inputs(dm, mess, GSIS_PPC, GSIS_SEED)
+    r = H.gsis(cas, mess, *parts, ns, acc, seed=7)
+    summ = gsis_summary(dm, parts, (r["x"], r["v"], r["ir"], r["cell"]))
+    np.savez_compressed(os.path.join(HERE, "gsis_pin.npz"), ppc=GSIS_PPC, seed=GSIS_SEED, **summ)
+
+    counts = fill_counts(dm, FILL_PPC, FILL_SEED)
+    f = H.fill(cas, mess, counts, seed=8)
+    lo, hi = I.cell_boxes(dm)
+    rel = (f["x"] - lo[f["cell"]]) / (hi[f["cell"]] - lo[f["cell"]])
+    rawc, dmc, messc = I.capsule_small()
+    casc = os.path.join(d, "capg.cas")
+    M.write_cas(casc, rawc)
+    countsc = fill_counts(dmc, FILL_PPC, FILL_SEED)
+    countsc[FILL_TET_CELLS:] = 0
+    fc = H.fill(casc, messc, countsc, seed=9)
+    bary = sorted_barycentric(dmc, fc["x"], fc["cell"])[:FILL_TET_SAMPLE]
+    vv = np.concatenate([f["v"], fc["v"]])
+    irr = np.concatenate([f["ir"], fc["ir"]])
+    np.savez_compressed(os.path.join(HERE, "fill_pin.npz"), ppc=FILL_PPC, seed=FILL_SEED, counts=counts,
+                        cell_count=np.bincount(f["cell"], minlength=dm.ncell).astype(np.int32),
+                        np_tri=f["np_tri"].astype(np.int16), rel=rel, tet_cells=FILL_TET_CELLS,
+                        tet_count=np.bincount(fc["cell"], minlength=dmc.ncell).astype(np.int32), bary=bary,
+                        v_mean=vv.mean(0), v_var=vv.var(0), ir_mean=irr.mean(), n_v=len(vv))
+
+
 def main():
     if not H.available():
         raise SystemExit("oracle/_ref/ref_harness missing: make -C oracle ref")
-    out = {}
+    want = set(sys.argv[1:])
+    if want - {"gsis", "fill", "core"}:
+        raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill")
     with tempfile.TemporaryDirectory() as d:
-        # -- mesh pin (1/8 block mesh)
-        raw8, dm8 = I.block_mesh(scale=8)
-        cas8 = os.path.join(d, "b8.cas")
-        M.write_cas(cas8, raw8)
-        ref = H.dump_mesh(cas8, I.BLOCK_MA, I.BLOCK_KN, M.DSMC_CELL_DTYPE, M.DSMC_EDGE_DTYPE, C.MESH_MESSAGE_DTYPE)
-        np.savez_compressed(os.path.join(HERE, "mesh_pin.npz"), cells=ref["cells"], edges=ref["edges"],
-                            points=ref["points"], split=ref["split"], mess=np.asarray(ref["mess"]))
-
-        # -- trace pin (1/4 block mesh)
-        raw, dm = I.block_mesh()
-        cas = os.path.join(d, "b4.cas")
-        M.write_cas(cas, raw)
-        mess = I.block_mess(dm, STATS_PPC)
-        x, v, dt, cell = I.trace_inputs(dm, mess, TRACE_N, seed=1)
-        res = {}
-        for stop in (1, 0):
-            r = H.trace(cas, mess, x, v, dt, cell, bool(stop))
-            for k in ("cell", "ifout", "face", "tri", "ncross"):
-                res[f"{k}_{stop}"] = r[k]
-            if stop:
-                res["x_1"] = r["x"]
-                res["dt_1"] = r["dt"]
-        np.savez_compressed(os.path.join(HERE, "trace_pin.npz"), mess=np.asarray(mess), **res)
-
-        # -- advection pin (wall zone as outlet, deterministic)
-        xf, vf, irf, cf = I.fill_inputs(dm, mess, 10, seed=2)
-        r = H.advect(cas, mess, xf, vf, irf, cf, 1, roles_arg(I.NOWALL_ZONES))
-        order = np.lexsort((r["v"][:, 2], r["v"][:, 1], r["v"][:, 0]))
-        ppc = np.bincount(r["cell"], minlength=dm.ncell)
-        np.savez_compressed(os.path.join(HERE, "advect_pin.npz"), ppc=ppc, x=r["x"][order], v=r["v"][order],
-                            cell=r["cell"][order])
-
-        # -- inflow remainders and the statistics band (reference roles)
-        xs, vs, irs, cs = I.fill_inputs(dm, mess, STATS_PPC, seed=3)
-        fields = []
-        reminj = None
-        nper = []
-        for s in STATS_SEEDS:
-            rr = H.run(cas, mess, xs, vs, irs, cs, STATS_STEPS, s, "-", STATS_AVG_FROM)
-            if reminj is None:
-                reminj = rr["reminj"]
-            elif not np.array_equal(reminj, rr["reminj"]):
-                raise SystemExit("reference inflow remainders differ between seeds")
-            fields.append(I.fields_from_moments(rr["moments"], STATS_STEPS - STATS_AVG_FROM + 1, dm, mess))
-            nper.append(rr["steps"][:, 0])
-        fields = np.stack(fields)
-        np.savez_compressed(os.path.join(HERE, "stats_band.npz"), fields=fields, nparticles=np.stack(nper),
-                            steps=STATS_STEPS, avg_from=STATS_AVG_FROM, ppc=STATS_PPC, seeds=np.array(STATS_SEEDS))
-        # remainders after 60 steps
-        r60 = H.run(cas, mess, xs, vs, irs, cs, 60, 5, "-", 61)
-        np.savez_compressed(os.path.join(HERE, "inflow_pin.npz"), reminj=r60["reminj"], steps=60)
-
-        # -- tetrahedral trace pin (coarse capsule)
-        rawc, dmc, messc = I.capsule_small()
-        casc = os.path.join(d, "cap.cas")
-        M.write_cas(casc, rawc)
-        refc = H.dump_mesh(casc, 5.0, 0.01, M.DSMC_CELL_DTYPE, M.DSMC_EDGE_DTYPE, C.MESH_MESSAGE_DTYPE)
-        for f in M.DSMC_EDGE_DTYPE.names:
-            if not np.array_equal(refc["edges"][f], dmc.edges[f]):
-                raise SystemExit(f"capsule mesh differs from the reference's parse in edges.{f}")
-        xt, vt, dtt, ct = I.tet_trace_inputs(dmc, messc, TRACE_N, seed=4)
-        r = H.trace(casc, messc, xt, vt, dtt, ct, True)
-        np.savez_compressed(os.path.join(HERE, "tet_trace_pin.npz"), ncell=dmc.ncell,
-                            **{k: r[k] for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt")})
+        if not want or want & {"gsis", "fill"}:
+            gen_gsis_fill(d)
+        if not want or "core" in want:
+            gen_core(d)
     print("fixtures written to", HERE)
+
+
+def gen_core(d):
+    # -- mesh pin (1/8 block mesh)
+    raw8, dm8 = I.block_mesh(scale=8)
+    cas8 = os.path.join(d, "b8.cas")
+    M.write_cas(cas8, raw8)
+    ref = H.dump_mesh(cas8, I.BLOCK_MA, I.BLOCK_KN, M.DSMC_CELL_DTYPE, M.DSMC_EDGE_DTYPE, C.MESH_MESSAGE_DTYPE)
+    np.savez_compressed(os.path.join(HERE, "mesh_pin.npz"), cells=ref["cells"], edges=ref["edges"],
+                        points=ref["points"], split=ref["split"], mess=np.asarray(ref["mess"]))
+
+    # -- trace pin (1/4 block mesh)
+    raw, dm = I.block_mesh()
+    cas = os.path.join(d, "b4.cas")
+    M.write_cas(cas, raw)
+    mess = I.block_mess(dm, STATS_PPC)
+    x, v, dt, cell = I.trace_inputs(dm, mess, TRACE_N, seed=1)
+    res = {}
+    for stop in (1, 0):
+        r = H.trace(cas, mess, x, v, dt, cell, bool(stop))
+        for k in ("cell", "ifout", "face", "tri", "ncross"):
+            res[f"{k}_{stop}"] = r[k]
+        if stop:
+            res["x_1"] = r["x"]
+            res["dt_1"] = r["dt"]
+    np.savez_compressed(os.path.join(HERE, "trace_pin.npz"), mess=np.asarray(mess), **res)
+
+    # -- advection pin (wall zone as outlet, deterministic)
+    xf, vf, irf, cf = I.fill_inputs(dm, mess, 10, seed=2)
+    r = H.advect(cas, mess, xf, vf, irf, cf, 1, roles_arg(I.NOWALL_ZONES))
+    order = np.lexsort((r["v"][:, 2], r["v"][:, 1], r["v"][:, 0]))
+    ppc = np.bincount(r["cell"], minlength=dm.ncell)
+    np.savez_compressed(os.path.join(HERE, "advect_pin.npz"), ppc=ppc, x=r["x"][order], v=r["v"][order],
+                        cell=r["cell"][order])
+
+    # -- inflow remainders and the statistics band (reference roles)
+    xs, vs, irs, cs = I.fill_inputs(dm, mess, STATS_PPC, seed=3)
+    fields = []
+    reminj = None
+    nper = []
+    for s in STATS_SEEDS:
+        rr = H.run(cas, mess, xs, vs, irs, cs, STATS_STEPS, s, "-", STATS_AVG_FROM)
+        if reminj is None:
+            reminj = rr["reminj"]
+        elif not np.array_equal(reminj, rr["reminj"]):
+            raise SystemExit("reference inflow remainders differ between seeds")
+        fields.append(I.fields_from_moments(rr["moments"], STATS_STEPS - STATS_AVG_FROM + 1, dm, mess))
+        nper.append(rr["steps"][:, 0])
+    fields = np.stack(fields)
+    np.savez_compressed(os.path.join(HERE, "stats_band.npz"), fields=fields, nparticles=np.stack(nper),
+                        steps=STATS_STEPS, avg_from=STATS_AVG_FROM, ppc=STATS_PPC, seeds=np.array(STATS_SEEDS))
+    # remainders after 60 steps
+    r60 = H.run(cas, mess, xs, vs, irs, cs, 60, 5, "-", 61)
+    np.savez_compressed(os.path.join(HERE, "inflow_pin.npz"), reminj=r60["reminj"], steps=60)
+
+    # -- tetrahedral trace pin (coarse capsule)
+    rawc, dmc, messc = I.capsule_small()
+    casc = os.path.join(d, "cap.cas")
+    M.write_cas(casc, rawc)
+    refc = H.dump_mesh(casc, 5.0, 0.01, M.DSMC_CELL_DTYPE, M.DSMC_EDGE_DTYPE, C.MESH_MESSAGE_DTYPE)
+    for f in M.DSMC_EDGE_DTYPE.names:
+        if not np.array_equal(refc["edges"][f], dmc.edges[f]):
+            raise SystemExit(f"capsule mesh differs from the reference's parse in edges.{f}")
+    xt, vt, dtt, ct = I.tet_trace_inputs(dmc, messc, TRACE_N, seed=4)
+    r = H.trace(casc, messc, xt, vt, dtt, ct, True)
+    np.savez_compressed(os.path.join(HERE, "tet_trace_pin.npz"), ncell=dmc.ncell,
+                        **{k: r[k] for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt")})
 
 
 if __name__ == "__main__":

@@ -43,7 +43,7 @@ def inflow_dir():
     return C.inflow_direction(AOA_DEG)
 
 
-def _cell_boxes(dm):
+def cell_boxes(dm):
     P = dm.points.reshape(-1, 3)
     fm = dm.edges["faceMap"]
     lo = np.full((dm.ncell, 3), np.inf)
@@ -70,7 +70,7 @@ def trace_inputs(dm, mess, n: int, seed: int):
     mean speed 3x the freestream speed, one dt."""
     rs = np.random.RandomState(seed)
     cells = rs.randint(0, dm.ncell, size=n).astype(np.int32)
-    lo, hi = _cell_boxes(dm)
+    lo, hi = cell_boxes(dm)
     x = lo[cells] + (hi[cells] - lo[cells]) * rs.random_sample((n, 3))
     u, _, _ = freestream(mess)
     sigma = 3.0 * float(np.linalg.norm(u)) / math.sqrt(8.0 / math.pi)
@@ -83,7 +83,7 @@ def fill_inputs(dm, mess, ppc: int, seed: int):
     """ppc particles per cell from the freestream Maxwellian."""
     rs = np.random.RandomState(seed)
     cells = np.repeat(np.arange(dm.ncell, dtype=np.int32), ppc)
-    lo, hi = _cell_boxes(dm)
+    lo, hi = cell_boxes(dm)
     x = lo[cells] + (hi[cells] - lo[cells]) * rs.random_sample((cells.shape[0], 3))
     u, sig, tN = freestream(mess)
     v = u[None, :] + sig * rs.standard_normal((cells.shape[0], 3))
@@ -124,6 +124,72 @@ def tet_trace_inputs(dm, mess, n: int, seed: int):
     v = sigma * rs.standard_normal((n, 3))
     dt = np.full(n, float(mess["dtime"]))
     return x, v, dt, cells
+
+
+def tet_vertices(dm, cells):
+    """The 4 distinct nodes of each tetrahedral cell, from its first two faces."""
+    fm = dm.edges["faceMap"]
+    f = dm.cells["cell2face"][cells, :2]
+    a = fm[f[:, 0], :3]
+    b = fm[f[:, 1], :3]
+    in_a = (b[:, :, None] == a[:, None, :]).any(-1)
+    extra = np.where(~in_a, b, -1).max(axis=1)
+    return np.concatenate([a, extra[:, None]], axis=1)
+
+
+def fill_inputs_any(dm, mess, ppc: int, seed: int):
+    """fill_inputs for meshes of tetrahedra: uniform barycentric positions."""
+    rs = np.random.RandomState(seed)
+    cells = np.repeat(np.arange(dm.ncell, dtype=np.int32), ppc)
+    P = dm.points.reshape(-1, 3)
+    w = -np.log(rs.random_sample((cells.shape[0], 4)))
+    w /= w.sum(1, keepdims=True)
+    x = np.einsum("nk,nkd->nd", w, P[tet_vertices(dm, cells)])
+    u, sig, tN = freestream(mess)
+    v = u[None, :] + sig * rs.standard_normal((cells.shape[0], 3))
+    ir = -np.log(1.0 - rs.random_sample(cells.shape[0])) * tN * 0.5
+    return x, v, ir, cells
+
+
+def gsis_inputs(dm, mess, ppc: int, seed: int, gate: bool = True, nan: bool = True):
+    """An NS solution for the GSIS particle update: densities of 0.5x..1.6x
+    the given particles per cell, drift perturbed around the freestream,
+    T and Tr of 0.7x..1.4x T_in; with ``gate`` a 10% gated-out set, with
+    ``nan`` a NaN velocity 37 cells before the end (gated in)."""
+    rs = np.random.RandomState(seed)
+    nc = dm.ncell
+    vol = dm.cells["area"].astype(float)
+    u0, sig, tN = freestream(mess)
+    ns = np.zeros((nc, 6))
+    ns[:, 0] = rs.uniform(0.5, 1.6, nc) * ppc * float(mess["Neff"]) / (vol * float(mess["n_ref"]))
+    ns[:, 1:4] = u0 + 0.3 * rs.standard_normal((nc, 3))
+    ns[:, 4] = tN * rs.uniform(0.7, 1.4, nc)
+    ns[:, 5] = tN * rs.uniform(0.7, 1.4, nc)
+    acc = (rs.random_sample(nc) > 0.1).astype(np.int8) if gate else None
+    nan_cell = None
+    if nan:
+        nan_cell = nc - 37
+        ns[nan_cell, 2] = np.nan
+        if acc is not None:
+            acc[nan_cell] = 1
+    return ns, acc, nan_cell
+
+
+def gsis_edge_inputs(dm, mess, ppc: int, seed: int):
+    """Particles (fill_inputs) with 40 cells emptied, and an NS solution
+    (gsis_inputs, gate on, NaN cell) in which 5 of the empty cells have
+    T < 0 and 10 occupied cells a negative density."""
+    x, v, ir, cell = fill_inputs(dm, mess, ppc, seed)
+    rs = np.random.RandomState(seed + 1)
+    empty = rs.choice(dm.ncell - 40, 40, replace=False)
+    keep = ~np.isin(cell, empty)
+    ns, acc, nan_cell = gsis_inputs(dm, mess, ppc, seed + 2)
+    ns[empty[:5], 4] = -1.0
+    acc[empty] = 1
+    neg = rs.choice(np.setdiff1d(np.arange(dm.ncell - 40), empty), 10, replace=False)
+    ns[neg, 0] = -ns[neg, 0]
+    acc[neg] = 1
+    return (x[keep], v[keep], ir[keep], cell[keep]), ns, acc, nan_cell, empty, neg
 
 
 def fields_from_moments(mom_sum: np.ndarray, nsteps: int, dm, mess) -> np.ndarray:
