@@ -293,6 +293,11 @@ def run_ours(args):
     value = ps_mixed / (ms_mixed / 1e3)
     case_m = mixed.pop("case")
     nparts = int(mixed["n0"])
+    # --- the GSIS particle update on the same case (between steps): an NS
+    # state of +-10% density around the current counts, drift and
+    # temperatures perturbed around the freestream; host wall time of the
+    # call (NS upload, count pass and scan, one read-back, rebuild)
+    gsis = gsis_timing(case_m, wl, seed=3000 + rank)
     # --- stage timing pass (events between stages, no graph) for the roofline
     barrier()
     tim = run_case(wl, fill, gpu.PRECISION_MIXED, max(3, args.steps // 2), 1, seed=2000 + rank, timing=True)
@@ -338,7 +343,7 @@ def run_ours(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32+f64acc",
-        "data": "synthetic (generated mesh; device freestream fill, counts in proportion to cell volume)",
+        "data": "synthetic (generated mesh; device initial fill: the reference's per-cell counts and placement, freestream velocities)",
         "config": dict(wl["desc"], particles_per_gpu=nparts, parallelism=f"replicas x{world}",
                        l2="particle state > L2 (126 MB)", precision="mixed"),
         "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / args.steps, "dtype": "f64"},
@@ -353,6 +358,7 @@ def run_ours(args):
         "e2e": {"value": e2e_ps / (e2e_ms / 1e3), "unit": "particle-steps/s",
                 "h2d_bytes_per_step": e2e["h2d"] / args.steps, "d2h_bytes_per_step": e2e["d2h"] / args.steps},
         "gpu_launches": None,
+        "gsis_update": gsis,
         "clocks": clk.summary(),
         "counters": {k: mixed["counters1"][k] - mixed["counters0"][k] for k in mixed["counters1"]},
     }
@@ -364,6 +370,29 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def gsis_timing(case, wl, seed: int, repeats: int = 3) -> dict:
+    dm, mess = wl["dm"], wl["mess"]
+    rs = np.random.default_rng(seed)
+    n = case.counts()["ppc"].astype(float)
+    vol = dm.cells["area"].astype(float)
+    u, sig, tN = W.freestream(mess, wl["inflow_dir"])
+    ns = np.empty((dm.ncell, 6))
+    ns[:, 0] = np.maximum(n, 1.0) * rs.uniform(0.9, 1.1, dm.ncell) * float(mess["Neff"]) / (vol * float(mess["n_ref"]))
+    ns[:, 1:4] = u + 0.05 * rs.standard_normal((dm.ncell, 3))
+    ns[:, 4] = tN * rs.uniform(0.95, 1.05, dm.ncell)
+    ns[:, 5] = tN * rs.uniform(0.95, 1.05, dm.ncell)
+    case.sync()
+    ms = []
+    rep = None
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        rep = case.molecular_velocity_change(ns)
+        ms.append((time.perf_counter() - t0) * 1e3)
+    return {"ms": float(np.median(ms)), "particles": int(rep["particles"]), "cells_updated": int(rep["cells_updated"]),
+            "added": int(rep["added"]), "removed": int(rep["removed"]),
+            "note": "host wall time of dsmc_molecular_velocity_change (NS upload included), median of 3"}
 
 
 def launches_per_step(wl) -> int:
@@ -553,6 +582,7 @@ def run_batch(args):
                    "autotuned": not args.no_autotune, "batch_seed": args.batch_seed, "setup_s": setup_s,
                    "move_threads_chosen": sorted({s["move_threads"] for s in shapes})},
         "gpu_launches": None,
+        "gsis_update": gsis,
         "clocks": clk.summary(),
     }
     line["gpu_launches"] = launches_per_step(None) * K * len(specs) + K * len(specs)

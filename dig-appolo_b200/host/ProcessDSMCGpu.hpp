@@ -113,6 +113,20 @@ public:
         return p;
     }
 
+    // ---- the initial fill on the device: MeshparticalInitial's own
+    // (Np_tri_inititial / meshfillpar, src/MeshparticalInitial.cpp:413-418,
+    // 481-721: a unit Maxwellian at rest), or the same placement with the
+    // case's freestream (the state the coupled start-up's first GSIS update
+    // shifts the fill to)
+    void initialFill(double ppcMean, uint64_t seed)
+    {
+        check(dsmc_fill_initial(h_, ppcMean, seed), "dsmc_fill_initial");
+    }
+    void freestreamFill(double ppcMean, uint64_t seed)
+    {
+        check(dsmc_fill_freestream(h_, ppcMean, seed), "dsmc_fill_freestream");
+    }
+
     // ---- the reference's step (src/meshImportTest.cpp:207-234)
     void preprocesseffquad(int istep) { check(dsmc_preprocesseffquad(h_, istep), "preprocesseffquad"); }
     void advection(int istep) { check(dsmc_advection(h_, istep), "advection"); }
@@ -270,6 +284,46 @@ private:
     DsmcCaseParams params_{};
     int ncell_ = 0, nface_ = 0;
     std::vector<DsmcEdgeRec> edges_;
+};
+
+// ProcessGSISGpu: the particle side of the reference's ProcessGSIS
+// (src/ProcessGSIS.h:71-131) over a ProcessDSMCGpu: the NS solution per cell
+// (nsresult, [icell][6]: density / n_ref, u, T, Tr), the DSMC->NS acceptance
+// gate (dsmc2ns_macro_accepted, used when dsmc2ns_acceptance_ready) and
+// molecular_velocity_change() on the device. The NS solver (MacroSolver)
+// and the DSMC2NS / NS2DSMC exchanges stay with the caller, which fills
+// nsresult from its NS step and reads the DSMC fields through
+// ProcessDSMCGpu::local().
+class ProcessGSISGpu {
+public:
+    explicit ProcessGSISGpu(ProcessDSMCGpu& process)
+        : icell(process.ncell()), nsresult((size_t)process.ncell() * 6, 0.0),
+          dsmc2ns_macro_accepted((size_t)process.ncell(), 1), process_(process)
+    {
+    }
+
+    int icell;
+    std::vector<double> nsresult;
+    std::vector<char> dsmc2ns_macro_accepted;
+    bool dsmc2ns_acceptance_ready = false;
+
+    // molecular_velocity_change (src/ProcessGSIS.cpp:2239-2366). Where the
+    // reference prints "The solution from ns solver is nan, ..." the report's
+    // nan_cell is the first NaN cell (cells before it are updated, as there).
+    DsmcGsisReport molecular_velocity_change()
+    {
+        if (nsresult.size() != (size_t)icell * 6 || dsmc2ns_macro_accepted.size() != (size_t)icell)
+            throw DsmcError("molecular_velocity_change: nsresult / acceptance sizes do not match icell");
+        DsmcGsisReport rep{};
+        const char* gate = dsmc2ns_acceptance_ready ? dsmc2ns_macro_accepted.data() : nullptr;
+        const int st = dsmc_molecular_velocity_change(process_.handle(), nsresult.data(), gate, &rep);
+        if (st != DSMC_OK)
+            throw DsmcError(std::string("dsmc_molecular_velocity_change: ") + dsmc_last_error(process_.handle()));
+        return rep;
+    }
+
+private:
+    ProcessDSMCGpu& process_;
 };
 
 }  // namespace dsmc_b200

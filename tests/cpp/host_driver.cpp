@@ -5,7 +5,10 @@
 // drives ProcessDSMC (src/meshImportTest.cpp:207-234) and writes the
 // particles, the macro fields and the wall fields back for comparison.
 //
-//   host_driver <dir> <nsteps> <mode: 0 stage calls, 1 fused step>
+//   host_driver <dir> <nsteps> <mode: 0 stage calls, 1 fused step,
+//                                    2 fused steps, then a GSIS particle
+//                                    update from <dir>/ns.bin and <dir>/acc.bin
+//                                    and one more step>
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -39,7 +42,8 @@ int main(int argc, char** argv)
     }
     const std::string d = argv[1];
     const int nsteps = std::stoi(argv[2]);
-    const int fused = std::stoi(argv[3]);
+    const int mode = std::stoi(argv[3]);
+    const int fused = mode != 0;
     try {
         std::ifstream meta(d + "/case.txt");
         long ncell, nface, npoint, n;
@@ -72,6 +76,16 @@ int main(int argc, char** argv)
                 process.collisionDSMC();
                 process.statistic_macro(istep);
             }
+        }
+        if (mode == 2) {
+            dsmc_b200::ProcessGSISGpu gsis(process);
+            gsis.nsresult = load<double>(d + "/ns.bin", (size_t)ncell * 6);
+            gsis.dsmc2ns_macro_accepted = load<char>(d + "/acc.bin", (size_t)ncell);
+            gsis.dsmc2ns_acceptance_ready = true;
+            const DsmcGsisReport rep = gsis.molecular_velocity_change();
+            std::ofstream(d + "/out_gsis.txt") << rep.nan_cell << ' ' << rep.cells_updated << ' ' << rep.cells_skipped
+                                               << ' ' << rep.added << ' ' << rep.removed << ' ' << rep.particles << '\n';
+            process.step(nsteps + 1);
         }
         const dsmc_b200::Particles q = process.downloadParticles();
         for (const char* k : {"x", "y", "z", "vx", "vy", "vz", "ir"}) {

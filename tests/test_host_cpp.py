@@ -130,3 +130,36 @@ def test_host_layer_matches_python_binding(block, tmp_path, fused):
     assert (tally[:, 0] > 0).sum() > 0
     err = open(os.path.join(d, "out_error.txt")).read()
     assert "nzones" in err
+
+
+@pytest.mark.gpu
+def test_host_gsis_matches_python_binding(block, tmp_path):
+    """ProcessGSISGpu::molecular_velocity_change between steps (gate on, a
+    NaN cell) equals the Python binding's call on the same case."""
+    raw, dm, mess = block
+    x, v, ir, cell = I.fill_inputs(dm, mess, 20, seed=6)
+    nsteps = 3
+    params = gpu.default_params(precision=gpu.PRECISION_FP64, seed=23, zones=I.REF_ZONES, inflow_dir=I.inflow_dir(),
+                                nss=2, nscheme=3, nevery=1, nrepeat=2)
+    ns, acc, nan_cell = I.gsis_inputs(dm, mess, 20, seed=31)
+    d = str(tmp_path)
+    _write_case(d, dm, mess, params, x, v, ir, cell)
+    ns.tofile(os.path.join(d, "ns.bin"))
+    acc.tofile(os.path.join(d, "acc.bin"))
+    exe = _compile(d)
+    r = subprocess.run([exe, d, str(nsteps), "2"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    with make_case(dm, mess, seed=23, nss=2, nscheme=3, nevery=1, nrepeat=2) as case:
+        case.upload_particles(x, v, ir, cell)
+        case.statistic_macroPre()
+        for s in range(1, nsteps + 1):
+            case.step(s)
+        rep = case.molecular_velocity_change(ns, acc)
+        case.step(nsteps + 1)
+        xg, vg, irg, cg = case.download_particles()
+    got = [int(t) for t in open(os.path.join(d, "out_gsis.txt")).read().split()]
+    assert got == [rep[k] for k in ("nan_cell", "cells_updated", "cells_skipped", "added", "removed", "particles")]
+    assert rep["nan_cell"] == nan_cell
+    assert np.array_equal(np.fromfile(os.path.join(d, "out_cell.bin"), dtype=np.int32), cg)
+    assert np.array_equal(np.fromfile(os.path.join(d, "out_vx.bin")), vg[:, 0])
+    assert np.array_equal(np.fromfile(os.path.join(d, "out_x.bin")), xg[:, 0])
