@@ -22,7 +22,7 @@ LIB_DIR = os.path.join(HERE, "lib")
 OBJ_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(LIB_DIR, "libdsmcgpu.so")
 
-SOURCES = ["dsmc_kernels.cu", "dsmc_engine.cu", "dsmc_noalloc.cu", "dsmc_gsis.cu"]
+SOURCES = ["dsmc_kernels.cu", "dsmc_engine.cu", "dsmc_noalloc.cu", "dsmc_gsis.cu", "dsmc_meshio.cpp"]
 HEADERS = ["dsmc_device.cuh", "dsmc_kernels.cuh", "dsmc_macro.cuh"]
 
 
@@ -53,12 +53,13 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(LIB_DIR, exist_ok=True)
     os.makedirs(OBJ_DIR, exist_ok=True)
     cc = nvcc()
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "dsmc_gpu.h")]
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", h)
+                                                        for h in ("dsmc_gpu.h", "dsmc_meshio.h")]
     objs = []
     jobs = []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(OBJ_DIR, src.replace(".cu", ".o"))
+        o = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
             jobs.append([cc, *common_flags(), "-c", s, "-o", o])

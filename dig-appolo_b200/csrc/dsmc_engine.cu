@@ -3,6 +3,7 @@
 // case, and orchestrates the step stages on one stream (replayed as a CUDA
 // graph in production).
 #include "dsmc_gpu.h"
+#include "dsmc_meshio.h"
 #include "dsmc_kernels.cuh"
 
 #include <algorithm>
@@ -2112,6 +2113,49 @@ int dsmc_batch_sync(DsmcBatch* b)
     for (DsmcHandle* h : b->cases)
         if (!h->e.checkDeviceErrors()) return b->fail(h->e.err), status_of(h->e, false);
     return DSMC_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// field output (ProcessDSMC::out2dat, outBoundaryStressHeat)
+// ---------------------------------------------------------------------------
+int dsmc_out2dat(DsmcHandle* h, int32_t istep, const DsmcZone* zones, int32_t nzones, const char* path)
+{
+    DSMC_GUARD(h);
+    dsmc::Engine& e = h->e;
+    const size_t nc = (size_t)e.ncell;
+    std::vector<double> rec(nc * 18), fin(nc * 18);
+    std::vector<unsigned char> sparse(nc, 0);
+    if (!e.downloadMacro(DSMC_MACRO_RECORD, rec.data()) || !e.downloadMacro(DSMC_MACRO_FINAL_RECORD, fin.data()))
+        return status_of(e, false);
+    bool ok = e.cuda(cudaMemcpyAsync(sparse.data(), e.sparseState, nc, cudaMemcpyDeviceToHost, e.stream), "sparse") &&
+              e.cuda(cudaStreamSynchronize(e.stream), "sync");
+    if (!ok) return status_of(e, false);
+    // record up to NSS and for sparse cells (DSMC2NS_SPARSE_ACCUMULATING /
+    // RELEASED), final_record after (src/ProcessDSMC.cpp:3346-3364)
+    for (size_t c = 0; c < nc; ++c) {
+        const bool useRecord = istep <= e.params.nss || sparse[c] == 1 || sparse[c] == 2;
+        if (!useRecord) std::memcpy(&rec[c * 18], &fin[c * 18], 18 * sizeof(double));
+    }
+    const int st = dsmc_write_fluent_cells(path, &e.mess, zones, nzones, rec.data(), e.ncell);
+    if (st != DSMC_OK) e.err = dsmc_meshio_last_error();
+    return st;
+}
+
+int dsmc_out_boundary_stress_heat(DsmcHandle* h, int32_t istep, const DsmcZone* zones, int32_t nzones,
+                                  const char* path)
+{
+    DSMC_GUARD(h);
+    dsmc::Engine& e = h->e;
+    // EnableBoundaryStressHeatStatistic off: nothing to write
+    if (!e.params.wall_stats) return DSMC_OK;
+    std::vector<double> tally((size_t)e.nface * 6);
+    const int dst = dsmc_download_wall(h, tally.data());
+    if (dst != DSMC_OK) return dst;
+    const int st = dsmc_write_fluent_wall(path, &e.mess, &e.params, zones, nzones, e.edges.data(), e.nface,
+                                          tally.data(), istep);
+    if (st != DSMC_OK) e.err = dsmc_meshio_last_error();
+    return st;
 }
 
 }  // extern "C"

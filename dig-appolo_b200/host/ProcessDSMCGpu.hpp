@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "dsmc_gpu.h"
+#include "dsmc_meshio.h"
 
 namespace dsmc_b200 {
 
@@ -55,6 +56,48 @@ struct WallFaceFields {
     double qTrans = 0.0, qRot = 0.0, qTotal = 0.0;
 };
 
+// A Fluent ASCII case read by the library (meshImport's readCAS +
+// preprocess + the DSMC topology, for one partition): the arrays
+// ProcessDSMCGpu takes, the zone declarations (zonemap) and the case
+// constants (setMeshMessage / setParticleMessage).
+class MeshFile {
+public:
+    explicit MeshFile(const std::string& casPath)
+    {
+        if (dsmc_mesh_read_cas(casPath.c_str(), &m_) != DSMC_OK) throw DsmcError(dsmc_meshio_last_error());
+    }
+    ~MeshFile() { dsmc_mesh_free(m_); }
+    MeshFile(const MeshFile&) = delete;
+    MeshFile& operator=(const MeshFile&) = delete;
+
+    DsmcMeshDesc desc() const
+    {
+        DsmcMeshDesc md{};
+        dsmc_mesh_get_desc(m_, &md);
+        return md;
+    }
+    std::vector<DsmcZone> zonemap() const
+    {
+        int32_t n = 0;
+        dsmc_mesh_get_zones(m_, nullptr, 0, &n);
+        std::vector<DsmcZone> z((size_t)n);
+        dsmc_mesh_get_zones(m_, z.data(), n, &n);
+        return z;
+    }
+    // the reference's constants: L0 3.912, T_in 142.2, T_wall 300, 100 per cell
+    DsmcMeshMessage message(double Ma, double Kn, int ppc = 100, double L0 = 3.912, double T_in = 142.2,
+                            double T_wall = 300.0, double cfl = 1e2, double cfl_ns = 5.0) const
+    {
+        DsmcMeshMessage mm{};
+        if (dsmc_mesh_message(m_, Ma, Kn, ppc, L0, T_in, T_wall, cfl, cfl_ns, &mm) != DSMC_OK)
+            throw DsmcError(dsmc_meshio_last_error());
+        return mm;
+    }
+
+private:
+    DsmcMeshFile* m_ = nullptr;
+};
+
 class ProcessDSMCGpu {
 public:
     static constexpr int Madata = DSMC_MACRO_WIDTH;   // MacroIndex count (src/ProcessDSMC.h:28-49)
@@ -69,7 +112,26 @@ public:
     {
         if (dsmc_create(&mesh, &mess, &params, device, &h_) != DSMC_OK)
             throw DsmcError(std::string("dsmc_create: ") + dsmc_last_error(nullptr));
+        // zone declarations as a case file makes them: the cell zone 2 and
+        // one face zone per run of equal face tags
+        zonemap.push_back(DsmcZone{12, 2, 1, ncell_});
+        for (int f = 0; f < nface_;) {
+            int g = f;
+            while (g < nface_ && edges_[(size_t)g].faceTag == edges_[(size_t)f].faceTag) ++g;
+            zonemap.push_back(DsmcZone{13, edges_[(size_t)f].faceTag, f + 1, g});
+            f = g;
+        }
     }
+    // From a case file: its arrays and its zone declarations.
+    ProcessDSMCGpu(const MeshFile& mesh, const DsmcMeshMessage& mess, const DsmcCaseParams& params, int device = 0)
+        : ProcessDSMCGpu(mesh.desc(), mess, params, device)
+    {
+        zonemap = mesh.zonemap();
+    }
+
+    // meshImport::zonemap (src/meshImport.h:120-129): the zones out2dat and
+    // outBoundaryStressHeat write
+    std::vector<DsmcZone> zonemap;
     ~ProcessDSMCGpu()
     {
         if (h_) dsmc_destroy(h_);
@@ -84,6 +146,7 @@ public:
             h_ = o.h_; o.h_ = nullptr;
             mess_ = o.mess_; params_ = o.params_; ncell_ = o.ncell_; nface_ = o.nface_;
             edges_ = std::move(o.edges_);
+            zonemap = std::move(o.zonemap);
         }
         return *this;
     }
@@ -169,22 +232,20 @@ public:
         return rec;
     }
 
-    // out2dat (src/ProcessDSMC.cpp:3338-3438): writes the fields of
-    // out2datFields, one line per cell (cell id, 18 values). The reference
-    // writes them through meshImport::out2Fluent_dsmc as a Fluent data file;
-    // that writer is not part of this library.
+    // out2dat (src/ProcessDSMC.cpp:3338-3438): the fields of out2datFields
+    // as meshImport::out2Fluent_dsmc writes them (Fluent sections 700-712
+    // of cell zone 2). The reference's path is
+    // ./statisticResults/DSMCKn%.1f_iter%d_CELL%d.dat (defaultOut2datPath).
     bool out2dat(int istep, const std::string& path) const
     {
-        const std::vector<double> w = out2datFields(istep);
-        std::ofstream f(path);
-        if (!f) return false;
-        f.precision(16);
-        for (int c = 0; c < ncell_; ++c) {
-            f << c;
-            for (int j = 0; j < Madata; ++j) f << ' ' << w[(size_t)c * Madata + j];
-            f << '\n';
-        }
-        return (bool)f;
+        check(dsmc_out2dat(h_, istep, zonemap.data(), (int32_t)zonemap.size(), path.c_str()), "dsmc_out2dat");
+        return true;
+    }
+    std::string defaultOut2datPath(int istep) const
+    {
+        char b[200];
+        std::snprintf(b, sizeof b, "./statisticResults/DSMCKn%.1f_iter%d_CELL%d.dat", mess_.Kn, istep, mess_.Ncell);
+        return b;
     }
 
     // outBoundaryStressHeat's conversion (src/ProcessDSMC.cpp:3451-3550):
@@ -230,25 +291,16 @@ public:
         return out;
     }
 
-    // outBoundaryStressHeat: the fields above, one line per wall face
-    // (face id, normal, pressure, shear, stress, q_trans, q_rot, q_total).
-    // The reference writes them as Fluent 700-706 sections; that writer is
-    // not part of this library. Returns true (nothing written) when wall
-    // statistics are off, like the reference.
+    // outBoundaryStressHeat (src/ProcessDSMC.cpp:3451-3652): the fields
+    // above as Fluent sections 700-706 of every all-wall zone. Returns true
+    // with nothing written when wall statistics are off (the reference's
+    // build has them off) or no zone is all wall. The reference's path is
+    // ./statisticResults/BoundaryStressHeatFluentKn%.1f_iter%d.dat.
     bool outBoundaryStressHeat(int istep, const std::string& path) const
     {
-        if (!params_.wall_stats) return true;
-        const std::vector<WallFaceFields> w = boundaryStressHeat(istep);
-        std::ofstream f(path);
-        if (!f) return false;
-        f.precision(16);
-        for (const WallFaceFields& x : w) {
-            f << x.face << ' ' << x.normal[0] << ' ' << x.normal[1] << ' ' << x.normal[2] << ' ' << x.pressure;
-            for (double v : x.shear) f << ' ' << v;
-            for (double v : x.stress) f << ' ' << v;
-            f << ' ' << x.qTrans << ' ' << x.qRot << ' ' << x.qTotal << '\n';
-        }
-        return (bool)f;
+        check(dsmc_out_boundary_stress_heat(h_, istep, zonemap.data(), (int32_t)zonemap.size(), path.c_str()),
+              "dsmc_out_boundary_stress_heat");
+        return true;
     }
 
     DsmcCounters counters() const

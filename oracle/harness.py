@@ -149,3 +149,19 @@ def fill(cas: str, mess, counts, seed: int = 1) -> dict:
         res = _read_particles(os.path.join(out, "particles.bin"))
         res["np_tri"] = np.fromfile(os.path.join(out, "np_tri.bin"), dtype=np.int32)
         return res
+
+
+def fluent(cas: str, mess, fields) -> dict:
+    """The reference's out2Fluent_dsmc of fields [ncell][18] on the mesh of
+    cas; returns the file's bytes and the zone declarations (id, first, last)."""
+    with tempfile.TemporaryDirectory() as d:
+        pm, pf = os.path.join(d, "mess.bin"), os.path.join(d, "fields.bin")
+        _write_mess(pm, mess)
+        np.ascontiguousarray(fields, dtype=np.float64).tofile(pf)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        _run(["fluent", cas, pm, pf, out])
+        with open(os.path.join(out, "fields.dat"), "rb") as fh:
+            text = fh.read()
+        zones = np.fromfile(os.path.join(out, "zones.bin"), dtype=np.int32).reshape(-1, 3)
+        return {"text": text, "zones": zones}

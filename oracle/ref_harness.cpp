@@ -44,6 +44,11 @@
  *       Np_tri_inititial + meshfillpar of MeshparticalInitial (the initial
  *       fill of one cell); dumps every bucket to OUT/particles.bin and the
  *       per-tetrahedron counts, cell after cell, to OUT/np_tri.bin (int32).
+ *   fluent CAS MESS FIELDS OUT
+ *       readCAS + preprocess, then the public meshImport::out2Fluent_dsmc on
+ *       FIELDS ([ncell][18] doubles) with MESS as the case constants, into
+ *       OUT/fields.dat; the zone declarations (zonemap: id, first, last) go
+ *       to OUT/zones.bin (int32).
  *   ROLES is "-" or a comma list tag:role with role in
  *       none,interface,inlet,outlet,wall.
  */
@@ -481,6 +486,31 @@ int cmdFill(int argc, char** argv)
     return ok && writeFile(out + "/np_tri.bin", npTri.data(), npTri.size() * 4) ? 0 : 1;
 }
 
+int cmdFluent(int argc, char** argv)
+{
+    if (argc < 6) return 2;
+    std::vector<char> mb;
+    if (!readFile(argv[3], mb) || mb.size() != sizeof(meshMessage)) return 1;
+    meshMessage mess;
+    std::memcpy(&mess, mb.data(), sizeof(mess));
+    meshImport* mesh = loadMesh(argv[2], mess.Ma, mess.Kn);
+    if (!mesh) return 1;
+    mesh->mess = mess;
+    std::vector<char> wb;
+    if (!readFile(argv[4], wb) || wb.size() % (18 * 8) != 0) return 1;
+    std::vector<double> w(wb.size() / 8);
+    std::memcpy(w.data(), wb.data(), wb.size());
+    const std::string out = argv[5];
+    if (!mesh->out2Fluent_dsmc((out + "/fields.dat").c_str(), w.data())) return 1;
+    std::vector<int> z;
+    for (const ZONE& zn : mesh->zonemap) {
+        z.push_back(zn.id);
+        z.push_back(zn.firstidx);
+        z.push_back(zn.lastidx);
+    }
+    return writeFile(out + "/zones.bin", z.data(), z.size() * 4) ? 0 : 1;
+}
+
 }  // namespace
 
 int main(int argc, char** argv)
@@ -496,6 +526,7 @@ int main(int argc, char** argv)
     if (cmd == "run") return cmdRun(argc, argv);
     if (cmd == "gsis") return cmdGsis(argc, argv);
     if (cmd == "fill") return cmdFill(argc, argv);
+    if (cmd == "fluent") return cmdFluent(argc, argv);
     std::fprintf(stderr, "unknown command %s\n", cmd.c_str());
     return 2;
 }

@@ -99,7 +99,8 @@ int main(int argc, char** argv)
         save(d + "/out_record.bin", process.record());
         save(d + "/out_final.bin", process.final_record());
         save(d + "/out_out2dat.bin", process.out2datFields(nsteps));
-        if (!process.outBoundaryStressHeat(nsteps, d + "/out_wall.txt")) throw std::runtime_error("wall output");
+        if (!process.outBoundaryStressHeat(nsteps, d + "/out_wall.dat")) throw std::runtime_error("wall output");
+        if (!process.out2dat(nsteps, d + "/out_fluent.dat")) throw std::runtime_error("field output");
         // an invalid call reports through the exception, like a failed
         // reference call reports through its abort message
         bool threw = false;

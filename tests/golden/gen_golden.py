@@ -155,15 +155,37 @@ def gen_gsis_fill(d):
                         v_mean=vv.mean(0), v_var=vv.var(0), ir_mean=irr.mean(), n_v=len(vv))
 
 
+def fluent_fields(ncell, seed=17):
+    rs = np.random.RandomState(seed)
+    w = rs.standard_normal((ncell, 18)) * 10.0 ** rs.randint(-8, 8, (ncell, 18))
+    w[0, 3] = np.nan
+    w[1, 5] = 0.0
+    w[2, 7] = -1e-300
+    w[3, 0] = 1e300
+    return w
+
+
+def gen_fluent(d):
+    raw8, dm8 = I.block_mesh(scale=8)
+    cas8 = os.path.join(d, "b8f.cas")
+    M.write_cas(cas8, raw8)
+    mess = C.mesh_message(dm8, I.BLOCK_MA, I.BLOCK_KN, ppc=20, L0=I.BLOCK_L0)
+    r = H.fluent(cas8, mess, fluent_fields(dm8.ncell))
+    np.savez_compressed(os.path.join(HERE, "fluent_pin.npz"), text=np.frombuffer(r["text"], dtype=np.uint8),
+                        zones=r["zones"], mess=np.asarray(mess))
+
+
 def main():
     if not H.available():
         raise SystemExit("oracle/_ref/ref_harness missing: make -C oracle ref")
     want = set(sys.argv[1:])
-    if want - {"gsis", "fill", "core"}:
-        raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill")
+    if want - {"gsis", "fill", "fluent", "core"}:
+        raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent")
     with tempfile.TemporaryDirectory() as d:
         if not want or want & {"gsis", "fill"}:
             gen_gsis_fill(d)
+        if not want or "fluent" in want:
+            gen_fluent(d)
         if not want or "core" in want:
             gen_core(d)
     print("fixtures written to", HERE)

@@ -1,5 +1,5 @@
 """The C-ABI library builds, loads and exports every entry point that
-include/dsmc_gpu.h declares (no GPU calls)."""
+include/dsmc_gpu.h and include/dsmc_meshio.h declare (no GPU calls)."""
 import ctypes
 import os
 import re
@@ -8,13 +8,16 @@ import numpy as np
 
 from conftest import ROOT
 
-HEADER = os.path.join(ROOT, "include", "dsmc_gpu.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("dsmc_gpu.h", "dsmc_meshio.h")]
 
 
-def declared_symbols():
-    txt = open(HEADER).read()
-    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(dsmc_[a-zA-Z0-9_]+)\s*\(", txt)))
+def declared_symbols(headers=HEADERS):
+    out = set()
+    for h in headers:
+        txt = open(h).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        out |= set(re.findall(r"\b(dsmc_[a-zA-Z0-9_]+)\s*\(", txt))
+    return sorted(out)
 
 
 def test_header_declares_the_stage_entry_points():
@@ -33,8 +36,11 @@ def test_library_exports_every_declared_symbol():
     lib = ctypes.CDLL(gpu.lib_path())
     missing = [s for s in declared_symbols() if not hasattr(lib, s)]
     assert not missing, missing
-    # the Python binding covers the same set
-    assert sorted(gpu.EXPORTED) == declared_symbols()
+    # the Python bindings cover the same sets
+    from pydsmc import meshio
+    assert sorted(gpu.EXPORTED) == declared_symbols(HEADERS[:1])
+    assert sorted(meshio.EXPORTED) == declared_symbols(HEADERS[1:])
+    assert set(os.listdir(os.path.join(ROOT, "include"))) == {"dsmc_gpu.h", "dsmc_meshio.h"}
 
 
 def test_struct_layouts_match_header():

@@ -6,8 +6,12 @@ against the built library.
 GPU: the driver runs the block case through the reference's stage calls
 (and through the fused step) and gives the same bits as the Python binding
 of the same C-ABI; an invalid case raises DsmcError with the library's
-message; the wall-field conversion matches outBoundaryStressHeat's formula
-(src/ProcessDSMC.cpp:3494-3550) evaluated here on the downloaded tallies.
+message; out2dat and outBoundaryStressHeat write the Fluent files that the
+library's writers make from the Python binding's fields and tallies (with
+the zone declarations the host layer derives: cell zone 2 and one face zone
+per run of equal face tags), and the wall fields follow outBoundaryStressHeat's
+formula (src/ProcessDSMC.cpp:3494-3550) evaluated here on the downloaded
+tallies.
 """
 import os
 import shutil
@@ -121,12 +125,32 @@ def test_host_layer_matches_python_binding(block, tmp_path, fused):
     sparse = (sparse_state == 1) | (sparse_state == 2)
     assert np.array_equal(o2d[~sparse], final[~sparse], equal_nan=True)
     assert np.array_equal(o2d[sparse], record[sparse], equal_nan=True)
-    # wall fields
-    wall = np.loadtxt(os.path.join(d, "out_wall.txt"), ndmin=2)
+    # Fluent files: the library's writers on the binding's fields and tallies
+    from pydsmc import meshio as IO
+    tags = dm.edges["faceTag"]
+    runs = np.flatnonzero(np.diff(tags)) + 1
+    bounds = np.concatenate([[0], runs, [dm.nface]])
+    zones = [(12, 2, 1, dm.ncell)] + [(13, int(tags[a]), int(a) + 1, int(b)) for a, b in zip(bounds[:-1], bounds[1:])]
+    IO.write_fluent_cells(os.path.join(d, "want_fluent.dat"), mess, zones, o2d)
+    assert open(os.path.join(d, "out_fluent.dat"), "rb").read() == open(os.path.join(d, "want_fluent.dat"), "rb").read()
+    IO.write_fluent_wall(os.path.join(d, "want_wall.dat"), mess, params, zones, dm.edges, tally, nsteps)
+    # wall tallies are sums of atomic adds: two runs agree to rounding, so
+    # the section structure is compared exactly and the numbers to 1e-12
+    ga = open(os.path.join(d, "out_wall.dat")).read().splitlines()
+    wa = open(os.path.join(d, "want_wall.dat")).read().splitlines()
+    assert len(ga) == len(wa)
+    for a, b in zip(ga, wa):
+        if a.startswith("(") or a == "))":
+            assert a == b
+        else:
+            assert np.allclose(np.array(a.split(), float), np.array(b.split(), float), rtol=1e-12, atol=1e-300)
+    # the wall fields follow the reference's formula
     want = _wall_fields(dm, mess, I.REF_ZONES, tally, nsteps, nss)
-    assert wall.shape == want.shape
-    assert np.array_equal(wall[:, 0], want[:, 0])
-    assert np.allclose(wall[:, 1:], want[:, 1:], rtol=1e-12, atol=1e-300)
+    lines = open(os.path.join(d, "out_wall.dat")).read().splitlines()
+    wz = [z for z in zones if z[1] == 6][0]
+    k = lines.index(f"(300 (704 6 1 0 0 {wz[2]} {wz[3]})") + 2
+    pressure = np.array([float(lines[k + j]) for j in range(wz[3] - wz[2] + 1)])
+    assert np.allclose(pressure, want[:, 4], rtol=1e-13, atol=1e-300)
     assert (tally[:, 0] > 0).sum() > 0
     err = open(os.path.join(d, "out_error.txt")).read()
     assert "nzones" in err
