@@ -576,10 +576,7 @@ struct TraceCounts {
     uint32_t removed, dropped, lost, wall, cross, fallback;
 };
 
-// Trace one particle, starting in `cell` having entered through face
-// `crossf` / triangle `tag` (-1/-1 for a particle at rest in its cell), for
-// `dtleft` (updated: the time not flown when the trace stops). Returns the
-// reference's outcome and leaves the final cell in `cell`.
+// x += v t (scalar_product, src/ProcessDSMC.cpp:1611-1617)
 template <typename Real>
 __device__ __forceinline__ void advance(PRegs<Real>& p, Real t)
 {
@@ -590,17 +587,41 @@ __device__ __forceinline__ void advance(PRegs<Real>& p, Real t)
     }
 }
 
+// The tracing loop's state between two exit searches.
+struct TraceState {
+    int ifout;        // outcome so far
+    int iter;         // exit searches made
+    int crossf, tag;  // the face / triangle the particle entered through
+    int entryFace;    // the face the particle sits on (mixed path)
+    bool afterNone;   // the last hit had no handler: use the triangle search
+    __device__ __forceinline__ void begin(int crossf0, int tag0)
+    {
+        ifout = kTraceStay;
+        iter = 0;
+        crossf = crossf0;
+        tag = tag0;
+        entryFace = crossf0;
+        afterNone = false;
+    }
+};
+
+// One pass of the tracing loop (traceParticleDtleft, src/ProcessDSMC.cpp:
+// 149-221): an exit search from `cell` and either the advance to the end of
+// the step or the crossing with its boundary handling. Returns true when the
+// trace is over, with the outcome in st.ifout.
 template <typename Real>
-__device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>& p, int& cell,
-                             int crossf, int tag, Real& dtleft, Stream& rng, int istep,
-                             double* wallTally, TraceCounts& cnt, bool stopAtWall, TraceLog* log)
+__device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C, PRegs<Real>& p, int& cell,
+                                           Real& dtleft, TraceState& st, Stream& rng, int istep,
+                                           double* wallTally, TraceCounts& cnt, bool stopAtWall, TraceLog* log)
 {
-    int ifout = kTraceStay;
-    int iter = 0;
-    int entryFace = crossf;   // the face the particle sits on (mixed path)
-    bool afterNone = false;   // the last hit had no handler: use the triangle search
-    while (dtleft > (Real)0) {
-        if (iter++ >= C.maxCross) { cnt.lost++; dtleft = 0; return kTraceLost; }
+    int& ifout = st.ifout;
+    int& crossf = st.crossf;
+    int& tag = st.tag;
+    int& entryFace = st.entryFace;
+    bool& afterNone = st.afterNone;
+    if (!(dtleft > (Real)0)) return true;
+    {
+        if (st.iter++ >= C.maxCross) { cnt.lost++; dtleft = 0; ifout = kTraceLost; return true; }
         int face, tri;
         Real t;
         bool stays;
@@ -629,7 +650,7 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
             }
             if (!decided) {
                 const ExitHit h = find_exit_exact(M, cell, crossf, tag, p.x, p.v);
-                if (h.face == -2 || !isfinite(h.t) || h.t <= 0.0) { cnt.dropped++; dtleft = 0; return kTraceDropped; }
+                if (h.face == -2 || !isfinite(h.t) || h.t <= 0.0) { cnt.dropped++; dtleft = 0; ifout = kTraceDropped; return true; }
                 face = h.face; tri = h.tri; t = h.t;
             }
             stays = t >= dtleft;
@@ -654,19 +675,19 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
                 double xa[3] = {cc[0] + (double)p.x[0], cc[1] + (double)p.x[1], cc[2] + (double)p.x[2]};
                 const double va[3] = {(double)p.v[0], (double)p.v[1], (double)p.v[2]};
                 const ExitHit he = find_exit_exact(M, cell, crossf, tag, xa, va, entryFace, (double)posTol);
-                if (he.face == -2 || !isfinite(he.t) || he.t <= 0.0) { cnt.dropped++; dtleft = 0; return kTraceDropped; }
+                if (he.face == -2 || !isfinite(he.t) || he.t <= 0.0) { cnt.dropped++; dtleft = 0; ifout = kTraceDropped; return true; }
                 face = he.face; tri = he.tri;
                 const double dl = (double)dtleft;
                 if (he.t >= dl) {
                     for (int d = 0; d < 3; ++d) p.x[d] = (float)(da(xa[d], dm(va[d], dl)) - cc[d]);
                     dtleft = 0;
-                    return ifout;
+                    return true;
                 }
                 stays = false;
                 t = (float)he.t;
                 if (!(t < dtleft)) t = nextafterf(dtleft, 0.0f);
             } else {
-                if (h.face == -2 || !(h.t > 0.0f)) { cnt.dropped++; dtleft = 0; return kTraceDropped; }
+                if (h.face == -2 || !(h.t > 0.0f)) { cnt.dropped++; dtleft = 0; ifout = kTraceDropped; return true; }
                 face = h.face; tri = h.tri; t = h.t;
                 stays = t >= dtleft;
             }
@@ -674,7 +695,7 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
         if (stays) {
             advance(p, dtleft);
             dtleft = 0;
-            return ifout;
+            return true;
         }
         crossf = face;
         tag = tri;
@@ -685,7 +706,7 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
             if (stopAtWall && role == kRoleWall) {
                 advance(p, t);
                 if constexpr (sizeof(Real) == 8) dtleft = ds(dtleft, t); else dtleft -= t;
-                return ifout;
+                return true;
             }
         }
         cnt.cross++;
@@ -701,7 +722,7 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
             if (cell == cc.x) next = cc.y;
             else if (cell == cc.y) next = cc.x;
             else next = cc.x;
-            if (next < 0 || next >= M.ncell) { cnt.lost++; dtleft = 0; return kTraceLost; }
+            if (next < 0 || next >= M.ncell) { cnt.lost++; dtleft = 0; ifout = kTraceLost; return true; }
             if constexpr (sizeof(Real) == 4) {
                 const float4 dl = M.faceDelta[face];
                 const float sg = (cell == cc.x) ? 1.0f : -1.0f;
@@ -712,7 +733,7 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
         } else if (role == kRoleInlet || role == kRoleOutlet) {
             cnt.removed++;
             dtleft = 0;
-            return kTraceRemoved;
+            ifout = kTraceRemoved; return true;
         } else if (role == kRoleWall) {
             if constexpr (sizeof(Real) == 8) dtleft = ds(dtleft, t); else dtleft -= t;
             const int ws = M.faceWall[face];
@@ -741,7 +762,23 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
         // search excludes this face and the particle is dropped.
         afterNone = (role == kRoleNone);
     }
-    return ifout;
+    return false;
+}
+
+// Trace one particle, starting in `cell` having entered through face
+// `crossf` / triangle `tag` (-1/-1 for a particle at rest in its cell), for
+// `dtleft` (updated: the time not flown when the trace stops). Returns the
+// reference's outcome and leaves the final cell in `cell`.
+template <typename Real>
+__device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>& p, int& cell,
+                             int crossf, int tag, Real& dtleft, Stream& rng, int istep,
+                             double* wallTally, TraceCounts& cnt, bool stopAtWall, TraceLog* log)
+{
+    TraceState st;
+    st.begin(crossf, tag);
+    while (!trace_step<Real>(M, C, p, cell, dtleft, st, rng, istep, wallTally, cnt, stopAtWall, log)) {
+    }
+    return st.ifout;
 }
 
 // Warp-aggregated atomic claim of `n` consecutive slots in counter[key];

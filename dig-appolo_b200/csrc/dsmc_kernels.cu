@@ -212,34 +212,78 @@ void launch_inject(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s
 // Three resident 256-thread blocks per SM (registers capped at 85): the
 // trace is bound by dependent loads, so occupancy pays more than the few
 // registers it spills to L1.
+// Particles are handed to warps in chunks (one atomic per chunk on the
+// step's cursor) and to lanes one at a time: a lane whose particle has
+// finished its trace writes it back and takes the next particle of the
+// chunk, so the lanes of a warp keep doing exit searches instead of waiting
+// for the warp's longest trace (about a quarter of the particles cross a
+// face in a step, a few cross several). Each particle is traced by the same
+// code with its own random stream (particle index, step), so the result
+// does not depend on which lane or warp takes it.
+constexpr int kMoveChunk = 128;
+
 template <typename Real>
 __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
 {
     const int istep = a.ctl->istep;
     const int n = a.ctl->nLive;
+    const int lane = threadIdx.x & 31;
+    const unsigned lower = (1u << lane) - 1u;
     TraceCounts cnt{};
     const Real dt0 = (Real)a.C.dtime;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        PRegs<Real> p;
-        p.x[0] = a.A.x[0][i]; p.x[1] = a.A.x[1][i]; p.x[2] = a.A.x[2][i];
-        p.v[0] = a.A.v[0][i]; p.v[1] = a.A.v[1][i]; p.v[2] = a.A.v[2][i];
-        p.ir = a.A.ir[i];
-        int cell = a.A.cell[i];
-        Stream rs;
-        rs.init((uint32_t)i, (uint32_t)istep, kPurposeWall, a.C.seedLo, a.C.seedHi);
-        Real dtleft = dt0;
-        const uint32_t wallBefore = cnt.wall;
-        const int out = trace_particle<Real>(a.M, a.C, p, cell, -1, -1, dtleft, rs, istep, a.wallTally,
-                                             cnt, false, nullptr);
-        if (out >= 0) {
-            a.A.x[0][i] = p.x[0]; a.A.x[1][i] = p.x[1]; a.A.x[2][i] = p.x[2];
-            if (cnt.wall != wallBefore) {
-                a.A.v[0][i] = p.v[0]; a.A.v[1][i] = p.v[1]; a.A.v[2][i] = p.v[2];
-                a.A.ir[i] = p.ir;
+    int chunkNext = 0, chunkEnd = 0;   // this warp's chunk (warp-uniform)
+    bool exhausted = false;            // warp-uniform
+    int i = -1;                        // this lane's particle
+    PRegs<Real> p;
+    int cell = 0;
+    Real dtleft = 0;
+    TraceState st;
+    Stream rs;
+    uint32_t wallBefore = 0;
+    for (;;) {
+        unsigned want = __ballot_sync(kFull, i < 0);
+        while (want && !exhausted) {
+            if (chunkNext >= chunkEnd) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(&a.ctl->moveCursor, kMoveChunk);
+                base = __shfl_sync(kFull, base, 0);
+                if (base >= n) {
+                    exhausted = true;
+                    break;
+                }
+                chunkNext = base;
+                chunkEnd = min(base + kMoveChunk, n);
             }
-            a.A.cell[i] = cell;
-        } else {
-            a.A.cell[i] = -1;
+            const int take = min(chunkEnd - chunkNext, __popc(want));
+            const bool mine = ((want >> lane) & 1u) && __popc(want & lower) < take;
+            if (mine) {
+                i = chunkNext + __popc(want & lower);
+                p.x[0] = a.A.x[0][i]; p.x[1] = a.A.x[1][i]; p.x[2] = a.A.x[2][i];
+                p.v[0] = a.A.v[0][i]; p.v[1] = a.A.v[1][i]; p.v[2] = a.A.v[2][i];
+                p.ir = a.A.ir[i];
+                cell = a.A.cell[i];
+                rs.init((uint32_t)i, (uint32_t)istep, kPurposeWall, a.C.seedLo, a.C.seedHi);
+                dtleft = dt0;
+                st.begin(-1, -1);
+                wallBefore = cnt.wall;
+            }
+            chunkNext += take;
+            want &= ~__ballot_sync(kFull, mine);
+        }
+        const bool active = i >= 0;
+        if (!__any_sync(kFull, active)) break;
+        if (active && trace_step<Real>(a.M, a.C, p, cell, dtleft, st, rs, istep, a.wallTally, cnt, false, nullptr)) {
+            if (st.ifout >= 0) {
+                a.A.x[0][i] = p.x[0]; a.A.x[1][i] = p.x[1]; a.A.x[2][i] = p.x[2];
+                if (cnt.wall != wallBefore) {
+                    a.A.v[0][i] = p.v[0]; a.A.v[1][i] = p.v[1]; a.A.v[2][i] = p.v[2];
+                    a.A.ir[i] = p.ir;
+                }
+                a.A.cell[i] = cell;
+            } else {
+                a.A.cell[i] = -1;
+            }
+            i = -1;
         }
     }
     flush_counts(a.counters, cnt);
@@ -248,6 +292,7 @@ __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
 template <typename Real>
 void launch_move(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s)
 {
+    cudaMemsetAsync(&a.ctl->moveCursor, 0, sizeof(int), s);
     move_kernel<Real><<<L.smCount * L.moveBlocksPerSm, L.moveThreads, 0, s>>>(a);
 }
 

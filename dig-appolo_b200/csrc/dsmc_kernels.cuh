@@ -21,7 +21,8 @@ struct StepCtl {
     int nInj;         // particles injected this step (appended after nLive)
     int nNext;        // particles after the sort
     int capacity;
-    int pad[3];
+    int moveCursor;   // particles handed out by the move kernel (reset before each move)
+    int pad[2];
 };
 
 struct DevPatches {
