@@ -3,17 +3,19 @@
 //   inject   preprocesseffquad (src/ProcessDSMC.cpp:2556-2570): per-cell
 //            inflow counts with the reference's remainder carry, scan,
 //            per-patch particle generation + trace for r*dt.
-//   move     advection (src/ProcessDSMC.cpp:1946-2017): one thread per
-//            particle traces dtime through the mesh.
+//   move     advection (src/ProcessDSMC.cpp:1946-2017): lanes trace
+//            particles for dtime through the mesh, refilled from warp
+//            chunks as their particles finish.
 //   sort     cache2chain (src/ProcessDSMC.cpp:2030-2135): deterministic
 //            counting sort. rank (warp per source cell: arrival slot and rank
 //            from warp ballots; multi-hop and injected arrivals through
-//            warp-aggregated atomics), scan, scatter of source indices.
-//   cells    a warp per 32 destination cells: gather into the sorted
-//            buffer in canonical order, NTC collisions (collisionDSMC,
-//            src/ProcessDSMC.cpp:2621-2744) one cell per lane with the
-//            pairs in sequence, and the 18-moment sampling
-//            (statistic_macro, src/ProcessDSMC.cpp:2757-2861).
+//            warp-aggregated atomics), scan, scatter of source indices, the
+//            far arrivals put in source order, gather of the particles.
+//   collide  collisionDSMC (src/ProcessDSMC.cpp:2621-2744): cells classed
+//            by size; NTC candidate pairs in sequence per cell (claims keep
+//            the reference's pair order), accepted pairs run together.
+//   sample   statistic_macro (src/ProcessDSMC.cpp:2757-2861): the
+//            18-moment sums of each cell in particle order.
 #include <climits>
 
 #include "dsmc_kernels.cuh"
@@ -559,13 +561,36 @@ __device__ void sort_far(int* seg, int m, int* tmp)
     }
 }
 
-// Raw moments of particles k = tid, tid + nt, ... below n; particle k at
-// v[k * stride].
-// Canonical order of every cell's far-slot arrivals (ascending source
-// index); the far counts are cleared for the next step's rank pass. A warp
-// reads the counts of 32 cells and sorts the segments that need it; the
-// output buffer's cell ids of a segment serve as scratch for very long
-// ones and are restored.
+// Ascending sort of 16 keys in registers (bitonic network; the indices are
+// constants once unrolled).
+__device__ __forceinline__ void sort16(uint32_t (&v)[16])
+{
+#pragma unroll
+    for (int k = 2; k <= 16; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const uint32_t lo = min(v[i], v[l]), hi = max(v[i], v[l]);
+                    const bool asc = (i & k) == 0;
+                    v[i] = asc ? lo : hi;
+                    v[l] = asc ? hi : lo;
+                }
+            }
+        }
+    }
+}
+
+// Canonical order of every cell's far-slot arrivals: ascending source
+// index; the far counts are cleared for the next step's rank pass. Each
+// lane takes one cell: a segment of up to 16 arrivals (the common case:
+// multi-cell hops and injected particles are a few per cell) is sorted in
+// the lane's registers; longer ones by the whole warp, whose output cell
+// ids serve as scratch for very long ones and are restored.
+constexpr int kLaneSort = 16;
+
 __global__ void __launch_bounds__(256) farsort_kernel(int* countSlot, const int* startB, int* idx, int* cellB,
                                                       int ncell)
 {
@@ -579,7 +604,17 @@ __global__ void __launch_bounds__(256) farsort_kernel(int* countSlot, const int*
             far = countSlot[(size_t)c * kSlots + kFarSlot];
             if (far) countSlot[(size_t)c * kSlots + kFarSlot] = 0;
         }
-        for (unsigned m = __ballot_sync(kFull, far > 1); m; m &= m - 1) {
+        if (far >= 2 && far <= kLaneSort) {
+            int* seg = idx + startB[c + 1] - far;
+            uint32_t v[kLaneSort];
+#pragma unroll
+            for (int k = 0; k < kLaneSort; ++k) v[k] = k < far ? (uint32_t)seg[k] : 0xffffffffu;
+            sort16(v);
+#pragma unroll
+            for (int k = 0; k < kLaneSort; ++k)
+                if (k < far) seg[k] = (int)v[k];
+        }
+        for (unsigned m = __ballot_sync(kFull, far > kLaneSort); m; m &= m - 1) {
             const int l = __ffs(m) - 1;
             const int cl = base + l;
             const int f = __shfl_sync(kFull, far, l);
