@@ -23,6 +23,7 @@ constexpr int kTraceMoved = 1;
 constexpr int kTraceRemoved = -1;   // left through inlet/outlet
 constexpr int kTraceDropped = -2;   // no exit face (reference "Dropped")
 constexpr int kTraceLost = -3;      // crossing cap or bad neighbour
+constexpr int kNbLost = -100;       // face record: an interface face without a cell on the other side
 
 // Slots of the counting sort (where a particle arrives from, seen from its
 // destination cell): 0 itself, 1..6 face neighbour j-1, 7 anything else
@@ -72,11 +73,15 @@ struct DevMesh {
     const signed char* revSlot;  // [ncell*6] slot of this cell in neighbour j's list (or -1)
     // face planes (cells with convex[c] != 0): records faceOff[c]..faceOff[c+1]
     const int* faceOff;          // [ncell+1]
-    const int4* faceRec;         // face id, index of its first triangle, node count (3/4)
+    const int4* faceRec;         // face id, index of its first triangle, node count (3/4), and the crossing:
+                                 // the cell on the other side (interface), kNbLost, or -(role + 1)
     const float4* planeF;        // outward unit normal, offset relative to the cell centre
     const float4* diagF;         // quads: in-plane normal of the diagonal, offset (relative)
     const double* planeD;        // [nrec*8] n(3), d, m(3), md, absolute
     const unsigned char* convex; // [ncell]
+    const float4* nbDeltaF;      // [nrec] FP32 centre shift of a crossing through the record (this - other)
+    int faceStride;              // F when every cell is convex with F records (record k = cell * F + j), else 0
+    int allConvex;               // every cell takes the plane path
     // placement tetrahedra of each cell (buildCellInitTets): records
     // placeOff[c]..placeOff[c+1], four vertices each (absolute FP64; the
     // barycentric weights a, b, c, d go to them in this order) and volume
@@ -416,6 +421,8 @@ struct PlaneHit {
     Real t;
     Real terr;
     bool ambiguous;
+    int nb;        // the record's crossing: the cell on the other side, kNbLost or -(role + 1)
+    float4 delta;  // FP32 path: the record's centre shift
 };
 
 template <typename Real>
@@ -424,17 +431,20 @@ __device__ __forceinline__ PlaneHit<Real> find_exit_planes(const DevMesh& M, int
 {
     constexpr Real eps = (sizeof(Real) == 8) ? (Real)1.1102230246251565e-16 : (Real)5.9604645e-8f;
     constexpr Real K = (sizeof(Real) == 8) ? (Real)64 : (Real)32;
-    PlaneHit<Real> h{-2, -1, -1, (Real)0, (Real)0, false};
+    PlaneHit<Real> h{-2, -1, -1, (Real)0, (Real)0, false, 0, make_float4(0.f, 0.f, 0.f, 0.f)};
     const Real vnorm = fabs(v[0]) + fabs(v[1]) + fabs(v[2]);
     const Real xnorm = fabs(x[0]) + fabs(x[1]) + fabs(x[2]);
     Real best = (sizeof(Real) == 8) ? (Real)DBL_MAX : (Real)FLT_MAX;
     Real second = best, bestErr = 0, secondErr = 0;
     int bi = -1;
     bool amb = false;
-    const int b = M.faceOff[cell];
-    const int e = M.faceOff[cell + 1];
+    float4 bestDelta = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int b = M.faceStride ? cell * M.faceStride : M.faceOff[cell];
+    const int e = M.faceStride ? b + M.faceStride : M.faceOff[cell + 1];
     for (int k = b; k < e; ++k) {
         const int4 rec = M.faceRec[k];
+        float4 dk = make_float4(0.f, 0.f, 0.f, 0.f);
+        if constexpr (sizeof(Real) == 4) dk = M.nbDeltaF[k];
         if (rec.x == crossf) continue;
         Real nx, ny, nz, d;
         if constexpr (sizeof(Real) == 8) {
@@ -458,6 +468,7 @@ __device__ __forceinline__ PlaneHit<Real> find_exit_planes(const DevMesh& M, int
         if (t < best) {
             second = best; secondErr = bestErr;
             best = t; bestErr = tErr; bi = k;
+            bestDelta = dk;
         } else if (t < second) {
             second = t; secondErr = tErr;
         }
@@ -471,6 +482,8 @@ __device__ __forceinline__ PlaneHit<Real> find_exit_planes(const DevMesh& M, int
     h.terr = bestErr;
     h.tri = -1;
     h.triIdx = rec.y;
+    h.nb = rec.w;
+    h.delta = bestDelta;
     if (rec.z == 4) {
         Real mx, my, mz, md;
         if constexpr (sizeof(Real) == 8) {
@@ -625,9 +638,13 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
         int face, tri;
         Real t;
         bool stays;
+        // a face chosen by the plane search comes with its record's crossing
+        bool hint = false;
+        int hintNb = 0;
+        float4 hintDelta = make_float4(0.f, 0.f, 0.f, 0.f);
         if constexpr (sizeof(Real) == 8) {
             bool decided = false;
-            if (M.convex[cell] && !afterNone) {
+            if ((M.allConvex || M.convex[cell]) && !afterNone) {
                 // plane decision, then the reference's exact test on that one
                 // triangle for the bit-exact t; any doubt runs the full search
                 const PlaneHit<double> ph = find_exit_planes<double>(M, cell, crossf, p.x, p.v);
@@ -635,6 +652,7 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
                 if (!ph.ambiguous && isect_exact(M.triD + (size_t)ph.triIdx * 9, p.x, p.v, te)) {
                     face = ph.face; tri = ph.tri; t = te;
                     decided = true;
+                    hintNb = ph.nb;
                     // the other half of a quad entry face stays eligible in
                     // the reference's skip rule (src/ProcessDSMC.cpp:1229-1233)
                     if (crossf >= 0 && (tag == 1 || tag == 2)) {
@@ -648,6 +666,7 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
                     }
                 }
             }
+            hint = decided;
             if (!decided) {
                 const ExitHit h = find_exit_exact(M, cell, crossf, tag, p.x, p.v);
                 if (h.face == -2 || !isfinite(h.t) || h.t <= 0.0) { cnt.dropped++; dtleft = 0; ifout = kTraceDropped; return true; }
@@ -659,9 +678,13 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
             // absolute uncertainty of the FP32 cell-relative position
             const float posTol = 64.0f * 5.9604645e-8f * (fabsf(p.x[0]) + fabsf(p.x[1]) + fabsf(p.x[2]));
             ExitHitF h;
-            if (M.convex[cell] && !afterNone) {
+            bool planes = false;
+            if ((M.allConvex || M.convex[cell]) && !afterNone) {
                 const PlaneHit<float> ph = find_exit_planes<float>(M, cell, crossf, p.x, p.v);
                 h = ExitHitF{ph.face, ph.tri, ph.t, ph.terr, ph.ambiguous};
+                planes = true;
+                hintNb = ph.nb;
+                hintDelta = ph.delta;
             } else {
                 h = find_exit_f32(M, cell, crossf, tag, p.x, p.v, vnorm, entryFace, posTol);
             }
@@ -690,6 +713,7 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
                 if (h.face == -2 || !(h.t > 0.0f)) { cnt.dropped++; dtleft = 0; ifout = kTraceDropped; return true; }
                 face = h.face; tri = h.tri; t = h.t;
                 stays = t >= dtleft;
+                hint = planes;
             }
         }
         if (stays) {
@@ -699,7 +723,7 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
         }
         crossf = face;
         tag = tri;
-        const int role = M.faceRole[face];
+        const int role = !hint ? (int)M.faceRole[face] : (hintNb >= 0 || hintNb == kNbLost) ? kRoleInterface : -(hintNb + 1);
         if (log && role != kRoleInterface && log->hitFace < 0) {
             log->hitFace = face;
             log->hitTri = tri;
@@ -717,16 +741,25 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
         if (role == kRoleInterface) {
             ifout = kTraceMoved;
             if constexpr (sizeof(Real) == 8) dtleft = ds(dtleft, t); else dtleft -= t;
-            const int2 cc = M.faceCells[face];
             int next;
-            if (cell == cc.x) next = cc.y;
-            else if (cell == cc.y) next = cc.x;
-            else next = cc.x;
+            int2 cc = make_int2(0, 0);
+            if (hint) {
+                next = hintNb;
+            } else {
+                cc = M.faceCells[face];
+                if (cell == cc.x) next = cc.y;
+                else if (cell == cc.y) next = cc.x;
+                else next = cc.x;
+            }
             if (next < 0 || next >= M.ncell) { cnt.lost++; dtleft = 0; ifout = kTraceLost; return true; }
             if constexpr (sizeof(Real) == 4) {
-                const float4 dl = M.faceDelta[face];
-                const float sg = (cell == cc.x) ? 1.0f : -1.0f;
-                p.x[0] += sg * dl.x; p.x[1] += sg * dl.y; p.x[2] += sg * dl.z;
+                if (hint) {
+                    p.x[0] += hintDelta.x; p.x[1] += hintDelta.y; p.x[2] += hintDelta.z;
+                } else {
+                    const float4 dl = M.faceDelta[face];
+                    const float sg = (cell == cc.x) ? 1.0f : -1.0f;
+                    p.x[0] += sg * dl.x; p.x[1] += sg * dl.y; p.x[2] += sg * dl.z;
+                }
             }
             cell = next;
             entryFace = face;

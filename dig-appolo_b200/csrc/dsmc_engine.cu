@@ -651,6 +651,34 @@ struct Engine {
             }
         }
 
+        // --- what a crossing through each face record needs, kept with the
+        //     record so the trace reads no per-face array: the cell on the
+        //     other side (interface faces, as the trace picks it) or the
+        //     face's role, and the FP32 centre shift in the crossing's sense
+        std::vector<float4> nbDeltaF(faceRec.size(), make_float4(0, 0, 0, 0));
+        for (int lc = 0; lc < ncell; ++lc) {
+            for (int k = faceOff[(size_t)lc]; k < faceOff[(size_t)lc + 1]; ++k) {
+                const int f = faceRec[(size_t)k].x;
+                const int role = faceRole[(size_t)f];
+                int nb;
+                if (role == DSMC_ROLE_INTERFACE) {
+                    const int2 fc = faceCells[(size_t)f];
+                    const int next = (lc == fc.x) ? fc.y : (lc == fc.y) ? fc.x : fc.x;
+                    nb = (next >= 0 && next < ncell) ? next : kNbLost;
+                    const float sg = (lc == fc.x) ? 1.0f : -1.0f;
+                    const float4 dl = faceDelta[(size_t)f];
+                    nbDeltaF[(size_t)k] = make_float4(sg * dl.x, sg * dl.y, sg * dl.z, 0.0f);
+                } else {
+                    nb = -(role + 1);
+                }
+                faceRec[(size_t)k].w = nb;
+            }
+        }
+        // every cell convex with the same number of faces: records at cell * F
+        int faceStride = nconvex == ncell && ncell > 0 ? faceOff[1] - faceOff[0] : 0;
+        for (int lc = 0; lc < ncell && faceStride; ++lc)
+            if (faceOff[(size_t)lc] != lc * faceStride) faceStride = 0;
+
         // --- neighbour slots for the counting sort
         std::vector<int> c2c((size_t)ncell * 6, -1);
         std::vector<signed char> rev((size_t)ncell * 6, -1);
@@ -708,12 +736,15 @@ struct Engine {
         int* dTriOffset; double* dTriD; int2* dTriFT; float4* dTriF; unsigned char* dRole; int2* dFaceCells;
         float4* dDelta; int* dFaceWall; double* dWallRot; float* dWallRotF; double* dCenter; double* dVol;
         int* dC2c; signed char* dRev;
-        int *dFaceOff; int4* dFaceRec; float4 *dPlaneF, *dDiagF; double* dPlaneD; unsigned char* dConvex;
+        int *dFaceOff; int4* dFaceRec; float4 *dPlaneF, *dDiagF, *dNbDelta; double* dPlaneD; unsigned char* dConvex;
         if (!upload(dFaceOff, faceOff) || !upload(dFaceRec, faceRec) || !upload(dPlaneF, planeF) ||
-            !upload(dDiagF, diagF) || !upload(dPlaneD, planeD) || !upload(dConvex, convex))
+            !upload(dDiagF, diagF) || !upload(dPlaneD, planeD) || !upload(dConvex, convex) ||
+            !upload(dNbDelta, nbDeltaF))
             return false;
         M.faceOff = dFaceOff; M.faceRec = dFaceRec; M.planeF = dPlaneF; M.diagF = dDiagF; M.planeD = dPlaneD;
-        M.convex = dConvex;
+        M.convex = dConvex; M.nbDeltaF = dNbDelta;
+        M.faceStride = faceStride;
+        M.allConvex = nconvex == ncell ? 1 : 0;
         if (!upload(dTriOffset, triOffset) || !upload(dTriD, triD) || !upload(dTriFT, triFT) || !upload(dTriF, triF) ||
             !upload(dRole, roleU8) || !upload(dFaceCells, faceCells) || !upload(dDelta, faceDelta) ||
             !upload(dFaceWall, faceWallHost) || !upload(dWallRot, wallRot) || !upload(dWallRotF, wallRotF) ||
