@@ -139,6 +139,8 @@ struct Engine {
     unsigned long long* counters = nullptr;
     int* cellList = nullptr;
     int* cellWork = nullptr;
+    int* cellPairs = nullptr;
+    double* cellCons = nullptr;
     int* errorWord = nullptr;
     int* placeFirst = nullptr;     // [nplace] cell-local first particle of each placement tetrahedron (fill)
     // GSIS particle update (allocated on first use)
@@ -776,6 +778,7 @@ struct Engine {
             !alloc(countSlot, (size_t)ncell * kSlots) || !alloc(scanPartial, kScanBlocks) ||
             !alloc(start[0], (size_t)ncell + 1) || !alloc(start[1], (size_t)ncell + 1) || !alloc(ctl, 1) ||
             !alloc(counters, C_COUNT) || !alloc(cellList, (size_t)ncell * 2) || !alloc(cellWork, 8) ||
+            !alloc(cellPairs, (size_t)ncell) || !alloc(cellCons, (size_t)ncell) ||
             !alloc(errorWord, 1))
             return false;
         if (params.keep_step_moments && !alloc(stepMom, (size_t)ncell * 18)) return false;
@@ -1002,6 +1005,7 @@ struct Engine {
         a.sparseState = sparseState; a.sparseAccum = sparseAccum; a.windowSamples = windowSamples;
         a.windowValid = windowValid; a.wallTally = wallTally; a.ctl = ctl; a.counters = counters;
         a.cellList = cellList; a.cellWork = cellWork; a.errorWord = errorWord;
+        a.cellPairs = cellPairs; a.cellCons = cellCons;
         return a;
     }
 

@@ -872,6 +872,16 @@ __device__ __forceinline__ int pair_count(const StepArgs<Real>& a, int c, int n,
     return npairs;
 }
 
+// The pair count and the majorant term of cell c as the classify pass
+// computed them (pair_count), with the cell's crmax.
+template <typename Real>
+__device__ __forceinline__ int pair_fetch(const StepArgs<Real>& a, int c, double& consCrm, double& crm0)
+{
+    consCrm = a.cellCons[c];
+    crm0 = a.crmax[c];
+    return a.cellPairs[c];
+}
+
 // NTC collisions of one small cell by one thread: the candidate pairs one
 // after another, particle k at v[k * stride].
 template <typename Real>
@@ -880,7 +890,7 @@ __device__ void collide_cell_serial(Real* vx, Real* vy, Real* vz, Real* ir, int 
 {
     if (n <= 1) return;
     double consCrm, crm0;
-    const int npairs = pair_count(a, c, n, consCrm, crm0);
+    const int npairs = pair_fetch(a, c, consCrm, crm0);
     pairsOut += (uint32_t)npairs;
     if (!(consCrm > 0.0) || npairs <= 0) return;
     Real crmLocal = (Real)0;
@@ -919,7 +929,7 @@ __device__ void collide_cell(Real* vx, Real* vy, Real* vz, Real* ir, int* claim,
     double consCrm = 0.0, crm0 = 0.0;
     int npairs = 0;
     if (lane == 0) {
-        npairs = pair_count(a, c, n, consCrm, crm0);
+        npairs = pair_fetch(a, c, consCrm, crm0);
         pairsOut += (uint32_t)npairs;
     }
     npairs = __shfl_sync(kFull, npairs, 0);
@@ -1008,12 +1018,24 @@ __host__ __device__ constexpr size_t cell_smem_bytes()
 //           [3] next huge/large item, [4] next small item
 // cellList: huge cells from the front of [0, ncell), large cells from its
 //           back, small cells from the front of [ncell, 2 ncell)
-__global__ void classify_kernel(const int* start, int ncell, int stageMax, int* list, int* work)
+template <typename Real>
+__global__ void classify_kernel(StepArgs<Real> a, int stageMax)
 {
     const int lane = threadIdx.x & 31;
+    const int* start = a.startA;
+    const int ncell = a.M.ncell;
+    int* list = a.cellList;
+    int* work = a.cellWork;
     for (int base = blockIdx.x * blockDim.x; base < ncell; base += gridDim.x * blockDim.x) {
         const int c = base + threadIdx.x;
         const int n = c < ncell ? start[c + 1] - start[c] : -1;
+        // the cell's candidate pair count, one thread per cell (the
+        // collision kernels read it back with pair_fetch)
+        if (n > 1) {
+            double consCrm, crm0;
+            a.cellPairs[c] = pair_count(a, c, n, consCrm, crm0);
+            a.cellCons[c] = consCrm;
+        }
         const int cls = n < 0 ? -1 : (n > stageMax ? 0 : (n > kSmallMax ? 1 : 2));
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -1107,7 +1129,7 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
                 double consCrm = 0.0, crm0 = 0.0;
                 int np = 0;
                 if (lane == 0 && n > 1) {
-                    np = pair_count(a, c, n, consCrm, crm0);
+                    np = pair_fetch(a, c, consCrm, crm0);
                     pairs += (uint32_t)np;
                 }
                 np = __shfl_sync(kFull, np, 0);
@@ -1326,7 +1348,7 @@ void launch_collide(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t 
     cudaMemsetAsync(a.cellWork, 0, 8 * sizeof(int), s);
     int gc = (ncell + 255) / 256;
     if (gc > L.smCount * 8) gc = L.smCount * 8;
-    classify_kernel<<<gc > 0 ? gc : 1, 256, 0, s>>>(a.startA, ncell, kArena, a.cellList, a.cellWork);
+    classify_kernel<Real><<<gc > 0 ? gc : 1, 256, 0, s>>>(a, kArena);
     int g = (ncell + kCellWarps - 1) / kCellWarps;
     const int cap = L.smCount * min(CellOcc<Real>::blocks, max(1, L.collideBlocksPerSm));
     if (g > cap) g = cap;

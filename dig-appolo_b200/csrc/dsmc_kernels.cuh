@@ -67,6 +67,8 @@ struct StepArgs {
     double* wallTally;        // [nwall*6]
     StepCtl* ctl;
     unsigned long long* counters;
+    int* cellPairs;           // [ncell] candidate pair count of the step (classify pass)
+    double* cellCons;         // [ncell] majorant term of the pair count (classify pass)
     int* cellList;            // [2*ncell] work lists of the cell pass
     int* cellWork;            // [8] list lengths and hand-out counters of the cell pass
     int* errorWord;
