@@ -349,9 +349,9 @@ __global__ void __launch_bounds__(256) rank_kernel(StepArgs<Real> a)
                 if (q == qq) packed = (slotQ[qq] << 24) | (runQ[qq] + __popc(m & lt));
                 runQ[qq] += __popc(m);
             }
-            const int key = (d >= 0 && q < 0) ? d * kSlots + kFarSlot : -1;
-            const int r = warp_claim(a.countSlot, key);
-            if (key >= 0) packed = (kFarSlot << 24) | r;
+            // multi-cell hops (a few percent): a slot each; their order is
+            // made canonical after the scatter
+            if (d >= 0 && q < 0) packed = (kFarSlot << 24) | atomicAdd(a.countSlot + (size_t)d * kSlots + kFarSlot, 1);
             if (valid) a.rank[i] = packed;
         }
         int myRun = 0;
@@ -634,17 +634,41 @@ __global__ void __launch_bounds__(256) farsort_kernel(int* countSlot, const int*
 template <typename Real>
 __global__ void __launch_bounds__(256) gather_kernel(StepArgs<Real> a)
 {
+    // four output slots per thread, their loads issued before their stores
+    constexpr int U = 4;
     const int n = a.ctl->nNext;
-    const int nSrc = a.ctl->nLive + a.ctl->nInj;
-    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n; o += gridDim.x * blockDim.x) {
-        const int i = a.idx[o];
-        if ((unsigned)i >= (unsigned)nSrc) {   // self-check: never index outside the source
-            atomicOr(a.errorWord, kErrSortIndex);
-            continue;
+    const unsigned nSrc = (unsigned)(a.ctl->nLive + a.ctl->nInj);
+    const int stride = gridDim.x * blockDim.x;
+    for (int o0 = blockIdx.x * blockDim.x + threadIdx.x; o0 < n; o0 += U * stride) {
+        int src[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int o = o0 + u * stride;
+            src[u] = o < n ? a.idx[o] : -1;
         }
-        a.B.x[0][o] = a.A.x[0][i]; a.B.x[1][o] = a.A.x[1][i]; a.B.x[2][o] = a.A.x[2][i];
-        a.B.v[0][o] = a.A.v[0][i]; a.B.v[1][o] = a.A.v[1][i]; a.B.v[2][o] = a.A.v[2][i];
-        a.B.ir[o] = a.A.ir[i];
+        Real x[U], y[U], z[U], vx[U], vy[U], vz[U], ir[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int o = o0 + u * stride;
+            if (o < n && (unsigned)src[u] < nSrc) {
+                const int i = src[u];
+                x[u] = a.A.x[0][i]; y[u] = a.A.x[1][i]; z[u] = a.A.x[2][i];
+                vx[u] = a.A.v[0][i]; vy[u] = a.A.v[1][i]; vz[u] = a.A.v[2][i];
+                ir[u] = a.A.ir[i];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int o = o0 + u * stride;
+            if (o >= n) continue;
+            if ((unsigned)src[u] >= nSrc) {   // self-check: never index outside the source
+                atomicOr(a.errorWord, kErrSortIndex);
+                continue;
+            }
+            a.B.x[0][o] = x[u]; a.B.x[1][o] = y[u]; a.B.x[2][o] = z[u];
+            a.B.v[0][o] = vx[u]; a.B.v[1][o] = vy[u]; a.B.v[2][o] = vz[u];
+            a.B.ir[o] = ir[u];
+        }
     }
 }
 
