@@ -455,29 +455,47 @@ __global__ void __launch_bounds__(256) scan_final_kernel(const int* countSlot, i
 template <typename Real>
 __global__ void __launch_bounds__(256) scatter_kernel(StepArgs<Real> a)
 {
+    // four particles per thread, their loads issued before their stores
+    constexpr int U = 4;
     const int nTot = a.ctl->nLive + a.ctl->nInj;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nTot; i += gridDim.x * blockDim.x) {
-        const int d = a.A.cell[i];
-        if (d < 0) continue;
-        const int packed = a.rank[i];
-        const int slot = packed >> 24;
-        const int r = packed & 0xFFFFFF;
-        const int4 lo = *reinterpret_cast<const int4*>(a.countSlot + (size_t)d * kSlots);
-        const int4 hi = *reinterpret_cast<const int4*>(a.countSlot + (size_t)d * kSlots + 4);
-        int base = a.startB[d] + r;
-        if (slot > 0) base += lo.x;
-        if (slot > 1) base += lo.y;
-        if (slot > 2) base += lo.z;
-        if (slot > 3) base += lo.w;
-        if (slot > 4) base += hi.x;
-        if (slot > 5) base += hi.y;
-        if (slot > 6) base += hi.z;
-        if (base < a.startB[d] || base >= a.startB[d + 1]) {   // self-check: slot counts inconsistent
-            atomicOr(a.errorWord, kErrSortIndex);
-            continue;
+    const int stride = gridDim.x * blockDim.x;
+    for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < nTot; i0 += U * stride) {
+        int d[U], packed[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int i = i0 + u * stride;
+            d[u] = i < nTot ? a.A.cell[i] : -1;
+            packed[u] = i < nTot ? a.rank[i] : 0;
         }
-        a.idx[base] = i;
-        a.B.cell[base] = d;
+        int4 lo[U], hi[U];
+        int s0[U], s1[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (d[u] < 0) continue;
+            lo[u] = *reinterpret_cast<const int4*>(a.countSlot + (size_t)d[u] * kSlots);
+            hi[u] = *reinterpret_cast<const int4*>(a.countSlot + (size_t)d[u] * kSlots + 4);
+            s0[u] = a.startB[d[u]];
+            s1[u] = a.startB[d[u] + 1];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (d[u] < 0) continue;
+            const int slot = packed[u] >> 24;
+            int base = s0[u] + (packed[u] & 0xFFFFFF);
+            if (slot > 0) base += lo[u].x;
+            if (slot > 1) base += lo[u].y;
+            if (slot > 2) base += lo[u].z;
+            if (slot > 3) base += lo[u].w;
+            if (slot > 4) base += hi[u].x;
+            if (slot > 5) base += hi[u].y;
+            if (slot > 6) base += hi[u].z;
+            if (base < s0[u] || base >= s1[u]) {   // self-check: slot counts inconsistent
+                atomicOr(a.errorWord, kErrSortIndex);
+                continue;
+            }
+            a.idx[base] = i0 + u * stride;
+            a.B.cell[base] = d[u];
+        }
     }
 }
 
@@ -561,39 +579,21 @@ __device__ void sort_far(int* seg, int m, int* tmp)
     }
 }
 
-// Ascending sort of 16 keys in registers (bitonic network; the indices are
-// constants once unrolled).
-__device__ __forceinline__ void sort16(uint32_t (&v)[16])
-{
-#pragma unroll
-    for (int k = 2; k <= 16; k <<= 1) {
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const int l = i ^ j;
-                if (l > i) {
-                    const uint32_t lo = min(v[i], v[l]), hi = max(v[i], v[l]);
-                    const bool asc = (i & k) == 0;
-                    v[i] = asc ? lo : hi;
-                    v[l] = asc ? hi : lo;
-                }
-            }
-        }
-    }
-}
-
 // Canonical order of every cell's far-slot arrivals: ascending source
 // index; the far counts are cleared for the next step's rank pass. Each
-// lane takes one cell: a segment of up to 16 arrivals (the common case:
-// multi-cell hops and injected particles are a few per cell) is sorted in
-// the lane's registers; longer ones by the whole warp, whose output cell
-// ids serve as scratch for very long ones and are restored.
-constexpr int kLaneSort = 16;
+// lane takes one cell: a segment of up to kLaneSort arrivals (the common
+// case: multi-cell hops and injected particles are some tens per cell at
+// most) is insertion-sorted in the lane's own shared-memory row; longer
+// ones by the whole warp, whose output cell ids serve as scratch for very
+// long ones and are restored.
+constexpr int kLaneSort = 32;
+constexpr int kFarsortThreads = 256;
 
-__global__ void __launch_bounds__(256) farsort_kernel(int* countSlot, const int* startB, int* idx, int* cellB,
-                                                      int ncell)
+__global__ void __launch_bounds__(kFarsortThreads) farsort_kernel(int* countSlot, const int* startB, int* idx,
+                                                                  int* cellB, int ncell)
 {
+    __shared__ int rows[kFarsortThreads][kLaneSort + 1];
+    int* row = rows[threadIdx.x];
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -606,13 +606,17 @@ __global__ void __launch_bounds__(256) farsort_kernel(int* countSlot, const int*
         }
         if (far >= 2 && far <= kLaneSort) {
             int* seg = idx + startB[c + 1] - far;
-            uint32_t v[kLaneSort];
-#pragma unroll
-            for (int k = 0; k < kLaneSort; ++k) v[k] = k < far ? (uint32_t)seg[k] : 0xffffffffu;
-            sort16(v);
-#pragma unroll
-            for (int k = 0; k < kLaneSort; ++k)
-                if (k < far) seg[k] = (int)v[k];
+            for (int k = 0; k < far; ++k) row[k] = seg[k];
+            for (int k = 1; k < far; ++k) {
+                const int v = row[k];
+                int j = k - 1;
+                while (j >= 0 && row[j] > v) {
+                    row[j + 1] = row[j];
+                    --j;
+                }
+                row[j + 1] = v;
+            }
+            for (int k = 0; k < far; ++k) seg[k] = row[k];
         }
         for (unsigned m = __ballot_sync(kFull, far > kLaneSort); m; m &= m - 1) {
             const int l = __ffs(m) - 1;
@@ -680,7 +684,7 @@ void launch_sort(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s)
     scan_partial_kernel<<<kScanBlocks, 256, 0, s>>>(a.countSlot, a.M.ncell, a.scanPartial);
     scan_final_kernel<<<kScanBlocks, 256, 0, s>>>(a.countSlot, a.M.ncell, a.scanPartial, a.startB, a.ctl);
     scatter_kernel<Real><<<g, 256, 0, s>>>(a);
-    farsort_kernel<<<L.smCount * 4, 256, 0, s>>>(a.countSlot, a.startB, a.idx, a.B.cell, a.M.ncell);
+    farsort_kernel<<<L.smCount * 4, kFarsortThreads, 0, s>>>(a.countSlot, a.startB, a.idx, a.B.cell, a.M.ncell);
     gather_kernel<Real><<<g, 256, 0, s>>>(a);
 }
 
