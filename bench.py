@@ -120,18 +120,38 @@ def algorithmic_bytes(n_particles: float, ncell: int, ntri_per_cell: float, mixe
             "per_particle_state": sp, "geom_per_cell": geom}
 
 
-def measured_traffic(kernel: str, workload: str):
+def measured_traffic(kernel: str, workload: str, particles: float):
     """DRAM bytes per launch of a kernel on this workload from the committed
-    ncu summary (profiles/<kernel>_<workload>.md, line
-    'dram_bytes_per_launch: N'), or None."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
-    try:
+    ncu summaries (profiles/<kernel>_<mesh>_ppc<N>.md, lines
+    'dram_bytes_per_launch: B' and 'particles: P'): the summary of this very
+    workload if there is one, else one of the same mesh at another particle
+    count, scaled to this launch by the particle ratio (full captures are
+    taken on a smaller case). Returns (bytes or None, source note)."""
+    mesh, _, _ = workload.rpartition("_ppc")
+    pdir = os.path.join(ROOT, "profiles")
+
+    def read(path):
+        vals = {}
         with open(path) as f:
             for line in f:
-                if line.strip().startswith("dram_bytes_per_launch:"):
-                    return float(line.split(":", 1)[1].strip().split()[0]), os.path.relpath(path, ROOT)
-    except OSError:
-        pass
+                k, sep, v = line.strip().partition(":")
+                if sep and k in ("dram_bytes_per_launch", "particles"):
+                    vals[k] = float(v.strip().split()[0])
+        return vals
+
+    exact = os.path.join(pdir, f"{kernel}_{workload}.md")
+    cands = [exact] if os.path.exists(exact) else sorted(
+        os.path.join(pdir, f) for f in (os.listdir(pdir) if os.path.isdir(pdir) else [])
+        if f.startswith(f"{kernel}_{mesh}_ppc") and f.endswith(".md"))
+    for path in cands:
+        vals = read(path)
+        if "dram_bytes_per_launch" not in vals:
+            continue
+        rel = os.path.relpath(path, ROOT)
+        if path == exact or "particles" not in vals:
+            return vals["dram_bytes_per_launch"], rel
+        scale = particles / vals["particles"]
+        return vals["dram_bytes_per_launch"] * scale, f"{rel}, scaled by particles x{scale:.3f}"
     return None, None
 
 
@@ -329,7 +349,7 @@ def run_ours(args):
     dom_ms = float(stage_avg[names.index(dom)])
     dom_bytes = ab.get(dom)
     achieved = (dom_bytes / (dom_ms / 1e3)) / 1e9 if (dom_bytes and dom_ms > 0) else None
-    traffic, traffic_src = measured_traffic(kernels[dom], wl["desc"]["workload"] + f"_ppc{args.ppc}")
+    traffic, traffic_src = measured_traffic(kernels[dom], wl["desc"]["workload"] + f"_ppc{args.ppc}", n_mean)
     step_achieved = (ab["step"] / (ms_mixed / args.steps / 1e3)) / 1e9
     line = {
         "metric": METRIC,
