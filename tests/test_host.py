@@ -84,3 +84,21 @@ def test_batch_specs_follow_the_batched_configuration():
     assert all(0.01 <= s["Kn"] <= 1.0 for s in sp)
     dm, L0 = bench.batch_mesh(8)
     assert dm.ncell == bench.batch_mesh_cells(8)
+
+
+def test_bench_reads_and_scales_profile_traffic(tmp_path, monkeypatch):
+    """bench.py's roofline traffic: the summary of the benchmarked workload
+    itself, else one of the same mesh at another particle count scaled by
+    the particle ratio, else none."""
+    import bench
+    prof = tmp_path / "profiles"
+    prof.mkdir()
+    (prof / "move_kernel_meshA_ppc40.md").write_text("x\nparticles: 1000\ndram_bytes_per_launch: 5000\n")
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    b, src = bench.measured_traffic("move_kernel", "meshA_ppc100", 2500.0)
+    assert b == 12500.0 and "scaled by particles x2.500" in src
+    (prof / "move_kernel_meshA_ppc100.md").write_text("dram_bytes_per_launch: 7000\n")
+    b, src = bench.measured_traffic("move_kernel", "meshA_ppc100", 2500.0)
+    assert b == 7000.0 and src == os.path.join("profiles", "move_kernel_meshA_ppc100.md")
+    assert bench.measured_traffic("move_kernel", "meshB_ppc100", 2500.0) == (None, None)
+    assert bench.measured_traffic("collide_kernel", "meshA_ppc100", 2500.0) == (None, None)
