@@ -716,7 +716,10 @@ def run_reference(args):
         wall = time.perf_counter() - t0
     per = [r["timing"]["particle_steps_per_s"] for r in res]
     agg = float(sum(per))
-    line = {"impl": "reference", "metric": METRIC, "value": agg, "unit": "particle-steps/s", "n_gpus": 0,
+    # n_gpus: the N this arm was launched for (the reference itself runs on
+    # the host cores; "device" says so)
+    line = {"impl": "reference", "metric": METRIC, "value": agg, "unit": "particle-steps/s",
+            "n_gpus": int(os.environ.get("WORLD_SIZE", args.gpus)), "device": f"host ({cores} cores)",
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": wl["desc"],
             "cpu_baseline": {"value": agg, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
