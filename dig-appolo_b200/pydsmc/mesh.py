@@ -174,6 +174,86 @@ def hex_box(nx: int, ny: int, nz: int, lx: float, ly: float, lz: float,
                    meta={"kind": "hex_box", "n": (nx, ny, nz), "L": (lx, ly, lz), "hole": hole})
 
 
+def pyramid_box(nx: int, ny: int, nz: int, lx: float, ly: float, lz: float) -> RawMesh:
+    """Box ``[0,lx]x[0,ly]x[0,lz]`` of ``nx*ny*nz`` cubes, each split into six
+    pyramids (Fluent element type 5) with the cube's centre as apex and a
+    cube face as base: cell ``6 q + d`` is the pyramid of cube ``q`` on face
+    ``d`` (-x, +x, -y, +y, -z, +z). Base quads are shared with the
+    neighbouring cube's pyramid or lie on the boundary (x-min inlet, x-max
+    outlet, the other sides zone 7); the triangles from each cube edge to the
+    centre are shared by the two pyramids of that edge."""
+    gx = np.linspace(0.0, lx, nx + 1)
+    gy = np.linspace(0.0, ly, ny + 1)
+    gz = np.linspace(0.0, lz, nz + 1)
+    X, Y, Z = np.meshgrid(gx, gy, gz, indexing="ij")
+    grid = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    cx = 0.5 * (gx[:-1] + gx[1:])
+    cy = 0.5 * (gy[:-1] + gy[1:])
+    cz = 0.5 * (gz[:-1] + gz[1:])
+    CX, CY, CZ = np.meshgrid(cx, cy, cz, indexing="ij")
+    centres = np.stack([CX.ravel(), CY.ravel(), CZ.ravel()], axis=1)
+    points = np.concatenate([grid, centres])
+    G = grid.shape[0]
+    n = (nx, ny, nz)
+
+    def nid(i, j, k):
+        return (i * (ny + 1) + j) * (nz + 1) + k
+
+    def qid(i, j, k):
+        return (i * ny + j) * nz + k
+
+    faces, ftype, c0s, c1s, zones = [], [], [], [], []
+    # base quads, plane by plane as in hex_box
+    for axis in range(3):
+        shape = list(n)
+        shape[axis] += 1
+        for i, j, k in np.ndindex(*shape):
+            if axis == 0:
+                quad = [nid(i, j, k), nid(i, j + 1, k), nid(i, j + 1, k + 1), nid(i, j, k + 1)]
+            elif axis == 1:
+                quad = [nid(i, j, k), nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i + 1, j, k)]
+            else:
+                quad = [nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j + 1, k), nid(i, j + 1, k)]
+            p = (i, j, k)
+            lo = list(p)
+            lo[axis] -= 1
+            has_lo = lo[axis] >= 0
+            has_hi = p[axis] < n[axis]
+            a = qid(*lo) * 6 + 2 * axis + 1 if has_lo else -1     # the lower cube's +face pyramid
+            b = qid(*p) * 6 + 2 * axis if has_hi else -1          # the upper cube's -face pyramid
+            if a >= 0 and b >= 0:
+                faces.append(quad); ftype.append(4); c0s.append(a); c1s.append(b); zones.append(ZONE_INTERIOR)
+            else:
+                z = (ZONE_INLET if b >= 0 else ZONE_OUTLET) if axis == 0 else ZONE_SIDE
+                faces.append(quad); ftype.append(4); c0s.append(a if a >= 0 else b); c1s.append(-1); zones.append(z)
+    # edge triangles inside every cube
+    for i, j, k in np.ndindex(nx, ny, nz):
+        q = qid(i, j, k)
+        ctr = G + q
+        for o1 in (0, 1):
+            for o2 in (0, 1):
+                # along z at x-offset o1, y-offset o2: pyramids -/+x and -/+y
+                tri = [nid(i + o1, j + o2, k), nid(i + o1, j + o2, k + 1), ctr, -1]
+                faces.append(tri); ftype.append(3); c0s.append(q * 6 + o1); c1s.append(q * 6 + 2 + o2)
+                zones.append(ZONE_INTERIOR)
+                # along x at y-offset o1, z-offset o2: pyramids -/+y and -/+z
+                tri = [nid(i, j + o1, k + o2), nid(i + 1, j + o1, k + o2), ctr, -1]
+                faces.append(tri); ftype.append(3); c0s.append(q * 6 + 2 + o1); c1s.append(q * 6 + 4 + o2)
+                zones.append(ZONE_INTERIOR)
+                # along y at x-offset o1, z-offset o2: pyramids -/+x and -/+z
+                tri = [nid(i + o1, j, k + o2), nid(i + o1, j + 1, k + o2), ctr, -1]
+                faces.append(tri); ftype.append(3); c0s.append(q * 6 + o1); c1s.append(q * 6 + 4 + o2)
+                zones.append(ZONE_INTERIOR)
+    faces = np.asarray(faces, dtype=np.int32)
+    ftype = np.asarray(ftype, dtype=np.int32)
+    c0 = np.asarray(c0s, dtype=np.int32)
+    c1 = np.asarray(c1s, dtype=np.int32)
+    zone = np.asarray(zones, dtype=np.int32)
+    faces, ftype, c0, c1, zone = _order_by_zone(faces, ftype, c0, c1, zone)
+    return RawMesh(points, faces, ftype, c0, c1, zone, 6 * nx * ny * nz, 5,
+                   meta={"kind": "pyramid_box", "n": (nx, ny, nz), "L": (lx, ly, lz)})
+
+
 def block_case_mesh(scale: int = 1) -> RawMesh:
     """The block case: 1.0 x 0.5 x 0.5 m box of 48x32x32 hexes with the
     central 8x8x8-cell block removed (48,640 cells). ``scale`` > 1 divides

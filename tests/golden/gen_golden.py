@@ -175,17 +175,55 @@ def gen_fluent(d):
                         zones=r["zones"], mess=np.asarray(mess))
 
 
+PYR_N = (3, 2, 2)
+PYR_L = (0.6, 0.4, 0.4)
+PYR_PPC = 40
+PYR_SEED = 77
+
+
+def pyramid_case():
+    raw = M.pyramid_box(*PYR_N, *PYR_L)
+    dm = M.build_dsmc_mesh(raw)
+    mess = C.mesh_message(dm, I.BLOCK_MA, I.BLOCK_KN, ppc=PYR_PPC, L0=0.1)
+    return raw, dm, mess
+
+
+def cube_relative(x, cell):
+    """Positions relative to each pyramid's cube, in [0, 1]^3."""
+    nx, ny, nz = PYR_N
+    q = cell // 6
+    i, j, k = q // (ny * nz), (q // nz) % ny, q % nz
+    h = np.array([PYR_L[0] / nx, PYR_L[1] / ny, PYR_L[2] / nz])
+    return (x - np.stack([i, j, k], 1) * h) / h
+
+
+def gen_pyramid(d):
+    raw, dm, mess = pyramid_case()
+    cas = os.path.join(d, "pyr.cas")
+    M.write_cas(cas, raw)
+    ref = H.dump_mesh(cas, I.BLOCK_MA, I.BLOCK_KN, M.DSMC_CELL_DTYPE, M.DSMC_EDGE_DTYPE, C.MESH_MESSAGE_DTYPE)
+    counts = fill_counts(dm, PYR_PPC, PYR_SEED)
+    f = H.fill(cas, mess, counts, seed=11)
+    np.savez_compressed(os.path.join(HERE, "pyramid_pin.npz"), cells=ref["cells"], edges=ref["edges"],
+                        points=ref["points"], split=ref["split"], counts=counts,
+                        cell_count=np.bincount(f["cell"], minlength=dm.ncell).astype(np.int32),
+                        np_tri=f["np_tri"].astype(np.int16), rel=cube_relative(f["x"], f["cell"]),
+                        v_mean=f["v"].mean(0), v_var=f["v"].var(0), ir_mean=f["ir"].mean(), n_v=len(f["v"]))
+
+
 def main():
     if not H.available():
         raise SystemExit("oracle/_ref/ref_harness missing: make -C oracle ref")
     want = set(sys.argv[1:])
-    if want - {"gsis", "fill", "fluent", "core"}:
-        raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent")
+    if want - {"gsis", "fill", "fluent", "pyramid", "core"}:
+        raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent, pyramid")
     with tempfile.TemporaryDirectory() as d:
         if not want or want & {"gsis", "fill"}:
             gen_gsis_fill(d)
         if not want or "fluent" in want:
             gen_fluent(d)
+        if not want or "pyramid" in want:
+            gen_pyramid(d)
         if not want or "core" in want:
             gen_core(d)
     print("fixtures written to", HERE)
