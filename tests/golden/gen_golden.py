@@ -27,6 +27,14 @@ outputs:
                  box-relative positions on the 1/4 block mesh (centre-face
                  tetrahedra), sorted barycentric weights on the capsule tets,
                  velocity and Ir moments
+  fluent_pin.npz out2Fluent_dsmc's file for given fields on the 1/8 block
+                 mesh, with its zone list and mesh message
+  pyramid_pin.npz the reference's arrays for a box of cubes split into six
+                 pyramids each (mixed triangle / quad faces) and its initial
+                 fill there (counts per placement tetrahedron, cube-relative
+                 positions, velocity and Ir moments)
+  pyramid_trace_pin.npz tracing-check outputs on that mesh (16,000
+                 particles, dt uniform in [0, dtime])
 
 Usage: python tests/golden/gen_golden.py [fixture ...]   (default: all)
 """
@@ -209,6 +217,10 @@ def gen_pyramid(d):
                         cell_count=np.bincount(f["cell"], minlength=dm.ncell).astype(np.int32),
                         np_tri=f["np_tri"].astype(np.int16), rel=cube_relative(f["x"], f["cell"]),
                         v_mean=f["v"].mean(0), v_var=f["v"].var(0), ir_mean=f["ir"].mean(), n_v=len(f["v"]))
+    x, v, dt, cell = I.pyramid_trace_inputs(raw, mess, TRACE_N, seed=6)
+    r = H.trace(cas, mess, x, v, dt, cell, True)
+    np.savez_compressed(os.path.join(HERE, "pyramid_trace_pin.npz"), ncell=dm.ncell,
+                        **{k: r[k] for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt")})
 
 
 def main():

@@ -79,6 +79,28 @@ def trace_inputs(dm, mess, n: int, seed: int):
     return x, v, dt, cells
 
 
+def pyramid_trace_inputs(raw, mess, n: int, seed: int):
+    """Uniform random points in the cubes of a ``pydsmc.mesh.pyramid_box``
+    mesh, each in the pyramid of the cube face it is nearest to (uniform in
+    every pyramid), isotropic velocities with mean speed 3x the freestream
+    speed, dt uniform in [0, dtime]."""
+    nx, ny, nz = raw.meta["n"]
+    h = np.array(raw.meta["L"], dtype=float) / np.array([nx, ny, nz])
+    rs = np.random.RandomState(seed)
+    q = rs.randint(0, nx * ny * nz, size=n)
+    ijk = np.stack([q // (ny * nz), (q // nz) % ny, q % nz], 1)
+    r = rs.random_sample((n, 3))
+    x = (ijk + r) * h
+    axis = np.abs(r - 0.5).argmax(1)
+    side = (r[np.arange(n), axis] > 0.5).astype(np.int64)
+    cells = (6 * q + 2 * axis + side).astype(np.int32)
+    u, _, _ = freestream(mess)
+    sigma = 3.0 * float(np.linalg.norm(u)) / math.sqrt(8.0 / math.pi)
+    v = sigma * rs.standard_normal((n, 3))
+    dt = float(mess["dtime"]) * rs.random_sample(n)
+    return x, v, dt, cells
+
+
 def fill_inputs(dm, mess, ppc: int, seed: int):
     """ppc particles per cell from the freestream Maxwellian."""
     rs = np.random.RandomState(seed)

@@ -11,6 +11,9 @@ around its centre.
 - The oracle's initial fill follows the reference's on these cells: two
   per-tetrahedron counts per cell with the same rounding offsets, the same
   distribution of positions in each cube, and the unit Maxwellian moments.
+- The oracle's tracing check is bit-exact with the reference's on these
+  cells (tests/golden/pyramid_trace_pin.npz): crossings through triangles
+  and split quads, exits through the inlet, outlet and side zones.
 """
 
 import numpy as np
@@ -106,3 +109,21 @@ def test_fill_on_pyramids_follows_the_reference(pyr, oracle_lib):
     assert np.all(np.abs(v.mean(0) - g["v_mean"]) < 5 * np.sqrt(1.0 / len(v) + 1.0 / n))
     assert np.all(np.abs(v.var(0) - g["v_var"]) < 5 * np.sqrt(2.0 / len(v) + 2.0 / n))
     assert abs(ir.mean() - float(g["ir_mean"])) < 5 * np.sqrt(0.25 / len(v) + 0.25 / n)
+
+
+def test_trace_on_pyramids_is_bit_exact_vs_reference(pyr, oracle_lib):
+    raw, dm, mess = pyr
+    g = golden("pyramid_trace_pin.npz")
+    assert dm.ncell == int(g["ncell"])
+    x, v, dt, cell = I.pyramid_trace_inputs(raw, mess, len(g["cell"]), seed=6)
+    o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir()))
+    r = o.trace(x, v, dt, cell, stop_at_wall=True)
+    for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt"):
+        assert np.array_equal(r[k], g[k]), k
+    # every outcome, both face kinds and both halves of the split quads
+    assert {-1, 0, 1} <= set(np.unique(g["ifout"]).tolist())
+    assert g["ncross"].max() >= 6
+    hit = g["face"] >= 0
+    kinds = set(dm.edges["faceType"][g["face"][hit]].tolist())
+    assert kinds == {4}                      # only the box's quads are boundary faces
+    assert len(set(g["tri"][hit].tolist())) == 2
