@@ -25,6 +25,11 @@ The box is 4x4x4 hexahedra with every boundary zone specular
   exponential Ir distribution.
 - Specular reflection through axis-aligned faces flips the normal velocity
   component and keeps every speed component's magnitude bit for bit.
+- Wall statistics (recordBoundaryStressHeat, src/ProcessDSMC.cpp:1659-1689,
+  converted as outBoundaryStressHeat does, :3494-3552) in a box of diffuse
+  walls at the gas temperature: the hits per area are the one-sided flux
+  n s / sqrt(2 pi), the normal stress is p = rho T, and the shear and the
+  heat flux vanish.
 """
 import math
 
@@ -39,6 +44,7 @@ from pydsmc import case as C
 from pydsmc import mesh as M
 
 SPECULAR = [(3, 1, 0), (4, 5, 0), (5, 5, 0), (7, 5, 0)]
+DIFFUSE = [(3, 1, 0), (4, 4, 0), (5, 4, 0), (7, 4, 0)]
 STAGE_MOVE, STAGE_SORT, STAGE_COLLIDE, STAGE_ALL = 0x2, 0x4, 0x8, 0x1F
 PPC = 200
 
@@ -166,3 +172,45 @@ def test_specular_reflection_keeps_speed_components(box, oracle_lib):
     assert _inside(dm, r["x"])
     # an odd number of reflections off the x faces flips vx: some did
     assert (np.sign(r["v"][:, 0]) != np.sign(v[:, 0])).sum() > n // 10
+
+
+def test_wall_statistics_of_an_isothermal_box(box, oracle_lib):
+    raw, dm, mess = box
+    tw = float(mess["Twall_ref"])
+    o = oracle_lib.Oracle(dm, mess, OracleParams(DIFFUSE, I.inflow_dir(), seed=3, nss=0, wall_stats=1))
+    rs = np.random.RandomState(1)
+    cells = np.repeat(np.arange(dm.ncell, dtype=np.int32), 100)
+    lo, hi = I.cell_boxes(dm)
+    n = len(cells)
+    x = lo[cells] + (hi[cells] - lo[cells]) * rs.random_sample((n, 3))
+    v = math.sqrt(tw / 2) * rs.standard_normal((n, 3))           # in equilibrium with the walls
+    ir = -np.log1p(-rs.random_sample(n)) * tw / 2
+    o.set_particles(x, v, ir, cells)
+    steps = 100
+    for s in range(1, steps + 1):
+        o.step(s, STAGE_ALL)
+    assert len(o.particles()[3]) == n and o.counters()["lost"] == 0
+    t = o.wall()
+    neff, nref, dt = float(mess["Neff"]), float(mess["n_ref"]), float(mess["dtime"])
+    vol = dm.cells["area"].sum()
+    rho = n * neff / (vol * nref)
+    flux = n / vol * math.sqrt(tw / 2) / math.sqrt(2 * math.pi) * dt * steps
+    hits, p, shear, q = [], [], [], []
+    for f in np.nonzero(t[:, 0] > 0)[0]:
+        e = dm.edges[f]
+        nrm = np.array(e["edgeNormal"], dtype=float)
+        nrm /= np.linalg.norm(nrm)
+        pn = -(t[f, 1:4] * nrm).sum()
+        scale = 2.0 * neff / (dt * steps) / float(e["length"]) / nref
+        hits.append(t[f, 0] / float(e["length"]))
+        p.append(pn * scale)
+        shear.append((t[f, 1:4] + pn * nrm) * scale)
+        q.append(-(t[f, 4] + t[f, 5]) * scale)
+    nf = len(p)
+    assert nf == 6 * 16                                        # every boundary face was hit
+    se = lambda a: np.std(a, axis=0) / math.sqrt(nf)
+    assert abs(np.mean(hits) - flux) < 4 * se(hits)
+    assert abs(np.mean(p) - rho * tw) < 4 * se(p)
+    assert abs(np.mean(p) / (rho * tw) - 1.0) < 0.03
+    assert np.all(np.abs(np.mean(shear, axis=0)) < 4 * se(shear))
+    assert abs(np.mean(q)) < 4 * se(q)
