@@ -35,6 +35,9 @@ outputs:
                  positions, velocity and Ir moments)
   pyramid_trace_pin.npz tracing-check outputs on that mesh (16,000
                  particles, dt uniform in [0, dtime])
+  macro_band.npz per-cell mean and seed-to-seed spread of the time-averaged
+                 stress and heat-flux fields (writeAveragedMacro's
+                 definitions) over the same 8 reference runs as stats_band
 
 Usage: python tests/golden/gen_golden.py [fixture ...]   (default: all)
 """
@@ -223,12 +226,34 @@ def gen_pyramid(d):
                         **{k: r[k] for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt")})
 
 
+# the stress and heat-flux fields of macro_from_moments, banded like stats_band
+MACRO_BAND_FIELDS = [5, 6, 7, 8, 9, 10, 11, 12, 13, 15, 16, 17]
+
+
+def gen_band(d):
+    raw, dm = I.block_mesh()
+    cas = os.path.join(d, "b4.cas")
+    M.write_cas(cas, raw)
+    mess = I.block_mess(dm, STATS_PPC)
+    xs, vs, irs, cs = I.fill_inputs(dm, mess, STATS_PPC, seed=3)
+    fields = []
+    for s in STATS_SEEDS:
+        rr = H.run(cas, mess, xs, vs, irs, cs, STATS_STEPS, s, "-", STATS_AVG_FROM)
+        f = I.macro_from_moments(rr["moments"], STATS_STEPS - STATS_AVG_FROM + 1, dm, mess)
+        fields.append(f[:, MACRO_BAND_FIELDS])
+    fields = np.stack(fields)
+    np.savez_compressed(os.path.join(HERE, "macro_band.npz"), mean=fields.mean(0), sd=fields.std(0, ddof=1),
+                        k=len(STATS_SEEDS), columns=np.array(MACRO_BAND_FIELDS), steps=STATS_STEPS,
+                        avg_from=STATS_AVG_FROM, ppc=STATS_PPC)
+
+
 def main():
     if not H.available():
         raise SystemExit("oracle/_ref/ref_harness missing: make -C oracle ref")
     want = set(sys.argv[1:])
-    if want - {"gsis", "fill", "fluent", "pyramid", "core"}:
-        raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent, pyramid")
+    if want - {"gsis", "fill", "fluent", "pyramid", "band", "core"}:
+        raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent, pyramid, "
+                         "band")
     with tempfile.TemporaryDirectory() as d:
         if not want or want & {"gsis", "fill"}:
             gen_gsis_fill(d)
@@ -236,6 +261,8 @@ def main():
             gen_fluent(d)
         if not want or "pyramid" in want:
             gen_pyramid(d)
+        if not want or "band" in want:
+            gen_band(d)
         if not want or "core" in want:
             gen_core(d)
     print("fixtures written to", HERE)

@@ -214,6 +214,46 @@ def gsis_edge_inputs(dm, mess, ppc: int, seed: int):
     return (x[keep], v[keep], ir[keep], cell[keep]), ns, acc, nan_cell, empty, neg
 
 
+def macro_from_moments(mom_sum: np.ndarray, nsteps: int, dm, mess) -> np.ndarray:
+    """The 18 macro fields of writeAveragedMacro (src/ProcessDSMC.cpp:
+    3158-3179) from raw moment sums over nsteps steps: rho, u (3), T, the
+    deviatoric stress (xx, xy, yy, yz, zz, zx), the heat flux (3), Tr and
+    the rotational heat flux (3). Cells the reference zeroes
+    (guardInvalidMacro, :3194-3211: no particles, rho, T or Tr not positive,
+    a non-finite field) give NaN."""
+    m = mom_sum.T
+    N = m[0]
+    out = np.full((mom_sum.shape[0], 18), np.nan)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rho = float(mess["Neff"]) / dm.cells["area"] * N / nsteps / float(mess["n_ref"])
+        u = m[1:4] / N
+        ux, uy, uz = u
+        u2 = (u * u).sum(0)
+        T = 2.0 / 3.0 / N * (m[4] - N * u2)
+        c = 2.0 * rho / N
+        dev = lambda a, b, d, ua, ub, ud: c * (2.0 / 3.0 * a - b / 3.0 - d / 3.0 - 2.0 / 3.0 * N * ua * ua +
+                                              N * ub * ub / 3.0 + N * ud * ud / 3.0)
+        out[:, 0] = rho
+        out[:, 1:4] = u.T
+        out[:, 4] = T
+        out[:, 5] = dev(m[5], m[7], m[9], ux, uy, uz)
+        out[:, 6] = c * (m[6] - N * ux * uy)
+        out[:, 7] = dev(m[7], m[5], m[9], uy, ux, uz)
+        out[:, 8] = c * (m[8] - N * uy * uz)
+        out[:, 9] = dev(m[9], m[5], m[7], uz, ux, uy)
+        out[:, 10] = c * (m[10] - N * uz * ux)
+        out[:, 11] = rho / N * (m[11] - 2 * ux * m[5] - 2 * uy * m[6] - 2 * uz * m[10] + u2 * m[1]) - ux * 1.5 * T * rho
+        out[:, 12] = rho / N * (m[12] - 2 * ux * m[6] - 2 * uy * m[7] - 2 * uz * m[8] + u2 * m[2]) - uy * 1.5 * T * rho
+        out[:, 13] = rho / N * (m[13] - 2 * ux * m[10] - 2 * uy * m[8] - 2 * uz * m[9] + u2 * m[3]) - uz * 1.5 * T * rho
+        out[:, 14] = 4.0 / float(mess["dr"]) / N * m[14]
+        out[:, 15] = c * (m[15] - ux * m[14])
+        out[:, 16] = c * (m[16] - uy * m[14])
+        out[:, 17] = c * (m[17] - uz * m[14])
+    valid = (N > 1e-12) & (out[:, 0] > 0) & (out[:, 4] > 0) & (out[:, 14] > 0) & np.isfinite(out).all(1)
+    out[~valid] = np.nan
+    return out
+
+
 def fields_from_moments(mom_sum: np.ndarray, nsteps: int, dm, mess) -> np.ndarray:
     """Time-averaged rho (per step), u (3), T and Tr from summed raw moments."""
     N = mom_sum[:, 0]

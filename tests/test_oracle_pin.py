@@ -109,7 +109,10 @@ def _band_check(fields, band, min_frac=0.95):
     return frac, float(np.mean(z)), z
 
 
-def test_oracle_statistics_within_reference_band(block, oracle_lib):
+@pytest.fixture(scope="module")
+def oracle_stats_run(block, oracle_lib):
+    """The oracle on the reference band's inputs: summed step moments over
+    the averaging window and the particle count after every step."""
     raw, dm, mess = block
     g = golden("stats_band.npz")
     x, v, ir, cell = I.fill_inputs(dm, mess, int(g["ppc"]), seed=3)
@@ -123,7 +126,14 @@ def test_oracle_statistics_within_reference_band(block, oracle_lib):
         if s >= a0:
             acc += o.step_moments()
         counts.append(len(o.particles()[3]))
-    f = I.fields_from_moments(acc, steps - a0 + 1, dm, mess)
+    return acc, steps - a0 + 1, counts
+
+
+def test_oracle_statistics_within_reference_band(block, oracle_stats_run):
+    raw, dm, mess = block
+    g = golden("stats_band.npz")
+    acc, nsteps, counts = oracle_stats_run
+    f = I.fields_from_moments(acc, nsteps, dm, mess)
     frac, zbar, _ = _band_check(f, g["fields"])
     assert frac >= 0.95, frac
     assert abs(zbar) < 0.3, zbar
@@ -131,6 +141,27 @@ def test_oracle_statistics_within_reference_band(block, oracle_lib):
     ref_n = g["nparticles"].astype(float)
     lo, hi = ref_n.min(0) * 0.97, ref_n.max(0) * 1.03
     assert np.all((np.array(counts) >= lo) & (np.array(counts) <= hi))
+
+
+def test_oracle_stress_and_heat_flux_within_reference_band(block, oracle_stats_run):
+    """Deviatoric stress, heat flux and rotational heat flux as
+    writeAveragedMacro defines them, against the same 8 reference runs."""
+    raw, dm, mess = block
+    g = golden("macro_band.npz")
+    acc, nsteps, counts = oracle_stats_run
+    assert nsteps == int(g["steps"]) - int(g["avg_from"]) + 1
+    f = I.macro_from_moments(acc, nsteps, dm, mess)[:, g["columns"]]
+    K = int(g["k"])
+    sd = g["sd"] * np.sqrt(1.0 + 1.0 / K)
+    ok = np.isfinite(f) & np.isfinite(g["mean"]) & (sd > 0)
+    assert ok.mean() > 0.9
+    z = (f[ok] - g["mean"][ok]) / sd[ok]
+    assert np.mean(np.abs(z) <= 3.0) >= 0.95
+    assert abs(np.mean(z)) < 0.3
+    # each field on its own: no bias
+    for j in range(f.shape[1]):
+        zj = (f[ok[:, j], j] - g["mean"][ok[:, j], j]) / sd[ok[:, j], j]
+        assert abs(np.mean(zj)) < 0.3, (int(g["columns"][j]), float(np.mean(zj)))
 
 
 def test_oracle_tet_trace_bit_exact_vs_reference(oracle_lib):
