@@ -37,7 +37,9 @@ outputs:
                  particles, dt uniform in [0, dtime])
   macro_band.npz per-cell mean and seed-to-seed spread of the time-averaged
                  stress and heat-flux fields (writeAveragedMacro's
-                 definitions) over the same 8 reference runs as stats_band
+                 definitions) over the same 8 reference runs as stats_band,
+                 and each run's per-step particles, injected particles,
+                 candidate pairs and collisions
 
 Usage: python tests/golden/gen_golden.py [fixture ...]   (default: all)
 """
@@ -236,15 +238,17 @@ def gen_band(d):
     M.write_cas(cas, raw)
     mess = I.block_mess(dm, STATS_PPC)
     xs, vs, irs, cs = I.fill_inputs(dm, mess, STATS_PPC, seed=3)
-    fields = []
+    fields, per_step = [], []
     for s in STATS_SEEDS:
         rr = H.run(cas, mess, xs, vs, irs, cs, STATS_STEPS, s, "-", STATS_AVG_FROM)
         f = I.macro_from_moments(rr["moments"], STATS_STEPS - STATS_AVG_FROM + 1, dm, mess)
         fields.append(f[:, MACRO_BAND_FIELDS])
+        per_step.append(rr["steps"])
     fields = np.stack(fields)
     np.savez_compressed(os.path.join(HERE, "macro_band.npz"), mean=fields.mean(0), sd=fields.std(0, ddof=1),
                         k=len(STATS_SEEDS), columns=np.array(MACRO_BAND_FIELDS), steps=STATS_STEPS,
-                        avg_from=STATS_AVG_FROM, ppc=STATS_PPC)
+                        avg_from=STATS_AVG_FROM, ppc=STATS_PPC,
+                        per_step=np.stack(per_step).astype(np.int32))
 
 
 def main():

@@ -112,7 +112,8 @@ def _band_check(fields, band, min_frac=0.95):
 @pytest.fixture(scope="module")
 def oracle_stats_run(block, oracle_lib):
     """The oracle on the reference band's inputs: summed step moments over
-    the averaging window and the particle count after every step."""
+    the averaging window, the particle count after every step and the
+    candidate pairs and collisions of every step."""
     raw, dm, mess = block
     g = golden("stats_band.npz")
     x, v, ir, cell = I.fill_inputs(dm, mess, int(g["ppc"]), seed=3)
@@ -120,19 +121,23 @@ def oracle_stats_run(block, oracle_lib):
     o.set_particles(x, v, ir, cell)
     acc = np.zeros((dm.ncell, 18))
     steps, a0 = int(g["steps"]), int(g["avg_from"])
-    counts = []
+    counts, pairs, coll = [], [], []
     for s in range(1, steps + 1):
         o.step(s)
         if s >= a0:
             acc += o.step_moments()
         counts.append(len(o.particles()[3]))
-    return acc, steps - a0 + 1, counts
+        c = o.counters()
+        pairs.append(c["candidate_pairs"])
+        coll.append(c["collisions"])
+    per_step = {"pairs": np.diff(np.concatenate([[0], pairs])), "collisions": np.diff(np.concatenate([[0], coll]))}
+    return acc, steps - a0 + 1, counts, per_step
 
 
 def test_oracle_statistics_within_reference_band(block, oracle_stats_run):
     raw, dm, mess = block
     g = golden("stats_band.npz")
-    acc, nsteps, counts = oracle_stats_run
+    acc, nsteps, counts, _ = oracle_stats_run
     f = I.fields_from_moments(acc, nsteps, dm, mess)
     frac, zbar, _ = _band_check(f, g["fields"])
     assert frac >= 0.95, frac
@@ -148,7 +153,7 @@ def test_oracle_stress_and_heat_flux_within_reference_band(block, oracle_stats_r
     writeAveragedMacro defines them, against the same 8 reference runs."""
     raw, dm, mess = block
     g = golden("macro_band.npz")
-    acc, nsteps, counts = oracle_stats_run
+    acc, nsteps, counts, _ = oracle_stats_run
     assert nsteps == int(g["steps"]) - int(g["avg_from"]) + 1
     f = I.macro_from_moments(acc, nsteps, dm, mess)[:, g["columns"]]
     K = int(g["k"])
@@ -162,6 +167,33 @@ def test_oracle_stress_and_heat_flux_within_reference_band(block, oracle_stats_r
     for j in range(f.shape[1]):
         zj = (f[ok[:, j], j] - g["mean"][ok[:, j], j]) / sd[ok[:, j], j]
         assert abs(np.mean(zj)) < 0.3, (int(g["columns"][j]), float(np.mean(zj)))
+
+
+def test_oracle_collision_counts_within_reference_band(oracle_stats_run):
+    """Particles, NTC candidate pairs (tol_collision_pairs) and accepted
+    collisions (tol_collision_times, src/ProcessDSMC.cpp:2621-2666) summed
+    over the 200 steps, and the acceptance fraction, against the 8 reference
+    runs: within 4 seed-to-seed standard deviations."""
+    g = golden("macro_band.npz")
+    ref = g["per_step"].astype(float)                     # [seed, step, (particles, injected, pairs, collisions)]
+    acc, nsteps, counts, per_step = oracle_stats_run
+    K = ref.shape[0]
+    mine = {
+        "particles": float(np.sum(counts)),
+        "pairs": float(per_step["pairs"].sum()),
+        "collisions": float(per_step["collisions"].sum()),
+    }
+    mine["acceptance"] = mine["collisions"] / mine["pairs"]
+    band = {
+        "particles": ref[:, :, 0].sum(1),
+        "pairs": ref[:, :, 2].sum(1),
+        "collisions": ref[:, :, 3].sum(1),
+    }
+    band["acceptance"] = band["collisions"] / band["pairs"]
+    for k, b in band.items():
+        z = (mine[k] - b.mean()) / (b.std(ddof=1) * np.sqrt(1.0 + 1.0 / K))
+        assert abs(z) < 4.0, (k, mine[k], b.mean(), z)
+    assert mine["collisions"] > 50000
 
 
 def test_oracle_tet_trace_bit_exact_vs_reference(oracle_lib):
