@@ -254,6 +254,80 @@ def pyramid_box(nx: int, ny: int, nz: int, lx: float, ly: float, lz: float) -> R
                    meta={"kind": "pyramid_box", "n": (nx, ny, nz), "L": (lx, ly, lz)})
 
 
+def prism_box(nx: int, ny: int, nz: int, lx: float, ly: float, lz: float) -> RawMesh:
+    """Box ``[0,lx]x[0,ly]x[0,lz]`` of ``nx*ny*nz`` cubes, each split into two
+    wedges (Fluent element type 6) by the vertical plane through its xy
+    diagonal from (i, j) to (i+1, j+1): cell ``2 q`` has the triangle
+    (i,j), (i+1,j), (i+1,j+1) as cross-section (it owns the cube's -y and +x
+    faces), cell ``2 q + 1`` the triangle (i,j), (i+1,j+1), (i,j+1) (the +y
+    and -x faces). Triangles lie on the z planes, quads on the x and y planes
+    and on the diagonals. x-min is the inlet, x-max the outlet, the other
+    sides zone 7."""
+    gx = np.linspace(0.0, lx, nx + 1)
+    gy = np.linspace(0.0, ly, ny + 1)
+    gz = np.linspace(0.0, lz, nz + 1)
+    X, Y, Z = np.meshgrid(gx, gy, gz, indexing="ij")
+    points = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+
+    def nid(i, j, k):
+        return (i * (ny + 1) + j) * (nz + 1) + k
+
+    def qid(i, j, k):
+        return (i * ny + j) * nz + k
+
+    faces, ftype, c0s, c1s, zones = [], [], [], [], []
+
+    def add(nodes, a, b, zone):
+        faces.append(list(nodes) + [-1] * (4 - len(nodes)))
+        ftype.append(len(nodes))
+        c0s.append(a)
+        c1s.append(b)
+        zones.append(zone)
+
+    # x planes: the +x face of a cube is wedge 0's, the -x face wedge 1's
+    for i, j, k in np.ndindex(nx + 1, ny, nz):
+        quad = [nid(i, j, k), nid(i, j + 1, k), nid(i, j + 1, k + 1), nid(i, j, k + 1)]
+        a = 2 * qid(i - 1, j, k) if i > 0 else -1
+        b = 2 * qid(i, j, k) + 1 if i < nx else -1
+        if a >= 0 and b >= 0:
+            add(quad, a, b, ZONE_INTERIOR)
+        else:
+            add(quad, a if a >= 0 else b, -1, ZONE_INLET if b >= 0 else ZONE_OUTLET)
+    # y planes: the -y face is wedge 0's, the +y face wedge 1's
+    for i, j, k in np.ndindex(nx, ny + 1, nz):
+        quad = [nid(i, j, k), nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i + 1, j, k)]
+        a = 2 * qid(i, j - 1, k) + 1 if j > 0 else -1
+        b = 2 * qid(i, j, k) if j < ny else -1
+        if a >= 0 and b >= 0:
+            add(quad, a, b, ZONE_INTERIOR)
+        else:
+            add(quad, a if a >= 0 else b, -1, ZONE_SIDE)
+    # z planes: two triangles per cube column, shared with the wedge above
+    for i, j, k in np.ndindex(nx, ny, nz + 1):
+        tris = ([nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j + 1, k)],
+                [nid(i, j, k), nid(i + 1, j + 1, k), nid(i, j + 1, k)])
+        for t, tri in enumerate(tris):
+            a = 2 * qid(i, j, k - 1) + t if k > 0 else -1
+            b = 2 * qid(i, j, k) + t if k < nz else -1
+            if a >= 0 and b >= 0:
+                add(tri, a, b, ZONE_INTERIOR)
+            else:
+                add(tri, a if a >= 0 else b, -1, ZONE_SIDE)
+    # the diagonal quad inside every cube
+    for i, j, k in np.ndindex(nx, ny, nz):
+        q = qid(i, j, k)
+        add([nid(i, j, k), nid(i + 1, j + 1, k), nid(i + 1, j + 1, k + 1), nid(i, j, k + 1)], 2 * q, 2 * q + 1,
+            ZONE_INTERIOR)
+    faces = np.asarray(faces, dtype=np.int32)
+    ftype = np.asarray(ftype, dtype=np.int32)
+    c0 = np.asarray(c0s, dtype=np.int32)
+    c1 = np.asarray(c1s, dtype=np.int32)
+    zone = np.asarray(zones, dtype=np.int32)
+    faces, ftype, c0, c1, zone = _order_by_zone(faces, ftype, c0, c1, zone)
+    return RawMesh(points, faces, ftype, c0, c1, zone, 2 * nx * ny * nz, 6,
+                   meta={"kind": "prism_box", "n": (nx, ny, nz), "L": (lx, ly, lz)})
+
+
 def block_case_mesh(scale: int = 1) -> RawMesh:
     """The block case: 1.0 x 0.5 x 0.5 m box of 48x32x32 hexes with the
     central 8x8x8-cell block removed (48,640 cells). ``scale`` > 1 divides

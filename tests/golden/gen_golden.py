@@ -35,6 +35,9 @@ outputs:
                  positions, velocity and Ir moments)
   pyramid_trace_pin.npz tracing-check outputs on that mesh (16,000
                  particles, dt uniform in [0, dtime])
+  prism_pin.npz  the same for that box with each cube split into two wedges
+                 (two triangles and three quads per cell): arrays, fill, and
+                 tracing-check outputs (8,000 particles)
   macro_band.npz per-cell mean and seed-to-seed spread of the time-averaged
                  stress and heat-flux fields (writeAveragedMacro's
                  definitions) over the same 8 reference runs as stats_band,
@@ -192,6 +195,7 @@ PYR_N = (3, 2, 2)
 PYR_L = (0.6, 0.4, 0.4)
 PYR_PPC = 40
 PYR_SEED = 77
+PRISM_SEED = 78
 
 
 def pyramid_case():
@@ -201,31 +205,50 @@ def pyramid_case():
     return raw, dm, mess
 
 
-def cube_relative(x, cell):
-    """Positions relative to each pyramid's cube, in [0, 1]^3."""
+def prism_case():
+    """The same box as pyramid_case, each cube split into two wedges."""
+    raw = M.prism_box(*PYR_N, *PYR_L)
+    dm = M.build_dsmc_mesh(raw)
+    mess = C.mesh_message(dm, I.BLOCK_MA, I.BLOCK_KN, ppc=PYR_PPC, L0=0.1)
+    return raw, dm, mess
+
+
+def cube_relative(x, cell, per_cube=6):
+    """Positions relative to each cell's cube (per_cube cells per cube: 6
+    pyramids or 2 wedges), in [0, 1]^3."""
     nx, ny, nz = PYR_N
-    q = cell // 6
+    q = cell // per_cube
     i, j, k = q // (ny * nz), (q // nz) % ny, q % nz
     h = np.array([PYR_L[0] / nx, PYR_L[1] / ny, PYR_L[2] / nz])
     return (x - np.stack([i, j, k], 1) * h) / h
 
 
-def gen_pyramid(d):
-    raw, dm, mess = pyramid_case()
-    cas = os.path.join(d, "pyr.cas")
+def _split_box_pins(d, name, case, per_cube, fill_seed, ref_seed, trace_seed, trace_n):
+    raw, dm, mess = case()
+    cas = os.path.join(d, name + ".cas")
     M.write_cas(cas, raw)
     ref = H.dump_mesh(cas, I.BLOCK_MA, I.BLOCK_KN, M.DSMC_CELL_DTYPE, M.DSMC_EDGE_DTYPE, C.MESH_MESSAGE_DTYPE)
-    counts = fill_counts(dm, PYR_PPC, PYR_SEED)
-    f = H.fill(cas, mess, counts, seed=11)
-    np.savez_compressed(os.path.join(HERE, "pyramid_pin.npz"), cells=ref["cells"], edges=ref["edges"],
-                        points=ref["points"], split=ref["split"], counts=counts,
-                        cell_count=np.bincount(f["cell"], minlength=dm.ncell).astype(np.int32),
-                        np_tri=f["np_tri"].astype(np.int16), rel=cube_relative(f["x"], f["cell"]),
-                        v_mean=f["v"].mean(0), v_var=f["v"].var(0), ir_mean=f["ir"].mean(), n_v=len(f["v"]))
-    x, v, dt, cell = I.pyramid_trace_inputs(raw, mess, TRACE_N, seed=6)
+    counts = fill_counts(dm, PYR_PPC, fill_seed)
+    f = H.fill(cas, mess, counts, seed=ref_seed)
+    fill = dict(cells=ref["cells"], edges=ref["edges"], points=ref["points"], split=ref["split"], counts=counts,
+                cell_count=np.bincount(f["cell"], minlength=dm.ncell).astype(np.int32),
+                np_tri=f["np_tri"].astype(np.int16), rel=cube_relative(f["x"], f["cell"], per_cube),
+                v_mean=f["v"].mean(0), v_var=f["v"].var(0), ir_mean=f["ir"].mean(), n_v=len(f["v"]))
+    x, v, dt, cell = I.split_box_trace_inputs(raw, mess, trace_n, seed=trace_seed)
     r = H.trace(cas, mess, x, v, dt, cell, True)
-    np.savez_compressed(os.path.join(HERE, "pyramid_trace_pin.npz"), ncell=dm.ncell,
-                        **{k: r[k] for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt")})
+    trace = dict(ncell=dm.ncell, **{k: r[k] for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt")})
+    return fill, trace
+
+
+def gen_pyramid(d):
+    fill, trace = _split_box_pins(d, "pyr", pyramid_case, 6, PYR_SEED, 11, 6, TRACE_N)
+    np.savez_compressed(os.path.join(HERE, "pyramid_pin.npz"), **fill)
+    np.savez_compressed(os.path.join(HERE, "pyramid_trace_pin.npz"), **trace)
+
+
+def gen_prism(d):
+    fill, trace = _split_box_pins(d, "prism", prism_case, 2, PRISM_SEED, 12, 7, TRACE_N // 2)
+    np.savez_compressed(os.path.join(HERE, "prism_pin.npz"), **fill, **{"trace_" + k: v for k, v in trace.items()})
 
 
 # the stress and heat-flux fields of macro_from_moments, banded like stats_band
@@ -255,9 +278,9 @@ def main():
     if not H.available():
         raise SystemExit("oracle/_ref/ref_harness missing: make -C oracle ref")
     want = set(sys.argv[1:])
-    if want - {"gsis", "fill", "fluent", "pyramid", "band", "core"}:
+    if want - {"gsis", "fill", "fluent", "pyramid", "prism", "band", "core"}:
         raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent, pyramid, "
-                         "band")
+                         "prism, band")
     with tempfile.TemporaryDirectory() as d:
         if not want or want & {"gsis", "fill"}:
             gen_gsis_fill(d)
@@ -265,6 +288,8 @@ def main():
             gen_fluent(d)
         if not want or "pyramid" in want:
             gen_pyramid(d)
+        if not want or "prism" in want:
+            gen_prism(d)
         if not want or "band" in want:
             gen_band(d)
         if not want or "core" in want:

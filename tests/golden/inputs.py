@@ -79,11 +79,12 @@ def trace_inputs(dm, mess, n: int, seed: int):
     return x, v, dt, cells
 
 
-def pyramid_trace_inputs(raw, mess, n: int, seed: int):
-    """Uniform random points in the cubes of a ``pydsmc.mesh.pyramid_box``
-    mesh, each in the pyramid of the cube face it is nearest to (uniform in
-    every pyramid), isotropic velocities with mean speed 3x the freestream
-    speed, dt uniform in [0, dtime]."""
+def split_box_trace_inputs(raw, mess, n: int, seed: int):
+    """Uniform random points in the cubes of a ``pydsmc.mesh.pyramid_box`` or
+    ``prism_box`` mesh, each with the cell of its cube that holds it (the
+    pyramid of the nearest cube face, or the wedge on its side of the
+    diagonal), isotropic velocities with mean speed 3x the freestream speed,
+    dt uniform in [0, dtime]."""
     nx, ny, nz = raw.meta["n"]
     h = np.array(raw.meta["L"], dtype=float) / np.array([nx, ny, nz])
     rs = np.random.RandomState(seed)
@@ -91,9 +92,14 @@ def pyramid_trace_inputs(raw, mess, n: int, seed: int):
     ijk = np.stack([q // (ny * nz), (q // nz) % ny, q % nz], 1)
     r = rs.random_sample((n, 3))
     x = (ijk + r) * h
-    axis = np.abs(r - 0.5).argmax(1)
-    side = (r[np.arange(n), axis] > 0.5).astype(np.int64)
-    cells = (6 * q + 2 * axis + side).astype(np.int32)
+    if raw.meta["kind"] == "pyramid_box":
+        axis = np.abs(r - 0.5).argmax(1)
+        side = (r[np.arange(n), axis] > 0.5).astype(np.int64)
+        cells = (6 * q + 2 * axis + side).astype(np.int32)
+    elif raw.meta["kind"] == "prism_box":
+        cells = (2 * q + (r[:, 1] > r[:, 0])).astype(np.int32)
+    else:
+        raise ValueError(raw.meta["kind"])
     u, _, _ = freestream(mess)
     sigma = 3.0 * float(np.linalg.norm(u)) / math.sqrt(8.0 / math.pi)
     v = sigma * rs.standard_normal((n, 3))
