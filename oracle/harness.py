@@ -66,20 +66,30 @@ def _write_mess(path, mess):
     np.asarray(mess).reshape(()).tofile(path)
 
 
-def trace(cas: str, mess, x, v, dt, cell, stop_at_wall: bool = True) -> dict:
+def trace(cas: str, mess, x, v, dt, cell, stop_at_wall: bool = True, timeout: int = 3600) -> dict:
     """The reference's tracing loop on the given particles."""
     n = int(np.asarray(cell).shape[0])
     with tempfile.TemporaryDirectory() as d:
         pm, pp, po = (os.path.join(d, k) for k in ("mess.bin", "parts.bin", "out.bin"))
         _write_mess(pm, mess)
         _write_particles(pp, x, v, np.zeros(n), dt, cell)
-        _run(["trace", cas, pm, pp, po, int(stop_at_wall)])
+        _run(["trace", cas, pm, pp, po, int(stop_at_wall)], timeout=timeout)
         b = np.fromfile(po, dtype=np.uint8)
         m = int(b[:8].view(np.int64)[0])
         ints = b[8:8 + 20 * m].view(np.int32).reshape(5, m)
         dbl = b[8 + 20 * m:].view(np.float64).reshape(7, m)
         return {"cell": ints[0].copy(), "ifout": ints[1].copy(), "face": ints[2].copy(), "tri": ints[3].copy(),
                 "ncross": ints[4].copy(), "x": dbl[0:3].T.copy(), "v": dbl[3:6].T.copy(), "dt": dbl[6].copy()}
+
+
+def trace_finishes(cas: str, mess, x, v, dt, cell, seconds: float) -> bool:
+    """Whether the reference's tracing loop ends within the given time on
+    these particles (its loop has no iteration bound)."""
+    try:
+        trace(cas, mess, x, v, dt, cell, True, timeout=seconds)
+        return True
+    except subprocess.TimeoutExpired:
+        return False
 
 
 def advect(cas: str, mess, x, v, ir, cell, istep: int = 1, roles: str = "-") -> dict:

@@ -38,6 +38,9 @@ outputs:
   prism_pin.npz  the same for that box with each cube split into two wedges
                  (two triangles and three quads per cell): arrays, fill, and
                  tracing-check outputs (8,000 particles)
+  degenerate_trace_pin.npz tracing-check outputs for exact, degenerate
+                 paths on the 1/4 block mesh (degenerate_trace_inputs), and
+                 the particles on which the reference's loop does not return
   macro_band.npz per-cell mean and seed-to-seed spread of the time-averaged
                  stress and heat-flux fields (writeAveragedMacro's
                  definitions) over the same 8 reference runs as stats_band,
@@ -251,6 +254,51 @@ def gen_prism(d):
     np.savez_compressed(os.path.join(HERE, "prism_pin.npz"), **fill, **{"trace_" + k: v for k, v in trace.items()})
 
 
+DEGEN_CELLS = 20
+DEGEN_SEED = 9
+DEGEN_SPIN_SECONDS = 3
+
+
+def gen_degenerate(d):
+    """Degenerate tracing inputs on the 1/4 block mesh. The reference's loop
+    has no iteration bound; the particles the oracle stops at its crossing
+    bound are each given to the reference alone for DEGEN_SPIN_SECONDS (the
+    rest finish together in well under a second) and recorded as spinning
+    when it has not returned; the reference's outputs are stored for the
+    rest."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    raw, dm = I.block_mesh()
+    cas = os.path.join(d, "b4d.cas")
+    M.write_cas(cas, raw)
+    mess = I.block_mess(dm, STATS_PPC)
+    x, v, dt, cell = I.degenerate_trace_inputs(dm, mess, DEGEN_CELLS, DEGEN_SEED)
+
+    class P:                                 # DsmcCaseParams fields for the oracle
+        nzones = len(I.REF_ZONES)
+        zone_tag = [z[0] for z in I.REF_ZONES]
+        zone_role = [z[1] for z in I.REF_ZONES]
+        zone_inject = [z[2] for z in I.REF_ZONES]
+        inflow_dir = tuple(I.inflow_dir())
+        seed, nss, nscheme, nevery, nrepeat, wall_stats, max_crossings = 0, 5000, 2000, 1, 100, 0, 4096
+
+    q = O.Oracle(dm, mess, P()).trace(x, v, dt, cell, stop_at_wall=True)
+    cand = np.nonzero(q["ncross"] >= P.max_crossings)[0]
+
+    def finishes(i):
+        return H.trace_finishes(cas, mess, x[[i]], v[[i]], dt[[i]], cell[[i]], DEGEN_SPIN_SECONDS)
+
+    with ThreadPoolExecutor(8) as ex:
+        fin = list(ex.map(finishes, cand))
+    if any(fin):
+        raise SystemExit(f"the reference finished on {int(np.sum(fin))} particles the oracle bounds")
+    ok = np.setdiff1d(np.arange(len(cell)), cand)
+    r = H.trace(cas, mess, x[ok], v[ok], dt[ok], cell[ok], True, timeout=120)
+    np.savez_compressed(os.path.join(HERE, "degenerate_trace_pin.npz"), ncells=DEGEN_CELLS, seed=DEGEN_SEED,
+                        spin_seconds=DEGEN_SPIN_SECONDS, ok=ok.astype(np.int32), spins=cand.astype(np.int32),
+                        **{k: r[k] for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt")})
+
+
 # the stress and heat-flux fields of macro_from_moments, banded like stats_band
 MACRO_BAND_FIELDS = [5, 6, 7, 8, 9, 10, 11, 12, 13, 15, 16, 17]
 
@@ -278,9 +326,9 @@ def main():
     if not H.available():
         raise SystemExit("oracle/_ref/ref_harness missing: make -C oracle ref")
     want = set(sys.argv[1:])
-    if want - {"gsis", "fill", "fluent", "pyramid", "prism", "band", "core"}:
+    if want - {"gsis", "fill", "fluent", "pyramid", "prism", "band", "degenerate", "core"}:
         raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent, pyramid, "
-                         "prism, band")
+                         "prism, band, degenerate")
     with tempfile.TemporaryDirectory() as d:
         if not want or want & {"gsis", "fill"}:
             gen_gsis_fill(d)
@@ -292,6 +340,8 @@ def main():
             gen_prism(d)
         if not want or "band" in want:
             gen_band(d)
+        if not want or "degenerate" in want:
+            gen_degenerate(d)
         if not want or "core" in want:
             gen_core(d)
     print("fixtures written to", HERE)

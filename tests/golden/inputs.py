@@ -107,6 +107,38 @@ def split_box_trace_inputs(raw, mess, n: int, seed: int):
     return x, v, dt, cells
 
 
+def degenerate_trace_inputs(dm, mess, ncells: int, seed: int):
+    """Exact, degenerate paths in hexahedral cells: from the centre, a
+    corner, the opposite corner, two face centres, an edge midpoint and a
+    top-face centre of each of ncells random cells, along each of the 26
+    directions (+-1, 0) x 3 at 3x the freestream speed, so that paths meet
+    faces at their centres (on a quad's split diagonal), along edges and
+    through vertices; then, per cell, a particle at rest, one with dt = 0,
+    one with a denormal-small speed and one starting on a face and moving
+    along it. dt = dtime."""
+    lo, hi = cell_boxes(dm)
+    ctr = 0.5 * (lo + hi)
+    rs = np.random.RandomState(seed)
+    cells = rs.choice(dm.ncell, ncells, replace=False)
+    dirs = [d for d in ((a, b, c) for a in (-1, 0, 1) for b in (-1, 0, 1) for c in (-1, 0, 1)) if d != (0, 0, 0)]
+    u, _, _ = freestream(mess)
+    sp = 3.0 * float(np.linalg.norm(u))
+    dtime = float(mess["dtime"])
+    X, V, C, T = [], [], [], []
+    for c in cells:
+        L, H, M = lo[c], hi[c], ctr[c]
+        starts = [M, L, H, np.array([L[0], M[1], M[2]]), np.array([H[0], M[1], M[2]]),
+                  np.array([L[0], L[1], M[2]]), np.array([M[0], M[1], H[2]])]
+        for s0 in starts:
+            for d in dirs:
+                X.append(s0); V.append(np.array(d, float) * sp); C.append(c); T.append(dtime)
+        for x0, v0, t0 in ((M, np.zeros(3), dtime), (M, np.array([sp, 0.0, 0.0]), 0.0),
+                           (M, np.array([1e-300, 0.0, 0.0]), dtime),
+                           (np.array([L[0], M[1], M[2]]), np.array([0.0, sp, 0.3 * sp]), dtime)):
+            X.append(x0); V.append(v0); C.append(c); T.append(t0)
+    return np.array(X), np.array(V), np.array(T), np.array(C, dtype=np.int32)
+
+
 def fill_inputs(dm, mess, ppc: int, seed: int):
     """ppc particles per cell from the freestream Maxwellian."""
     rs = np.random.RandomState(seed)

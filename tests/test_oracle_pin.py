@@ -196,6 +196,39 @@ def test_oracle_collision_counts_within_reference_band(oracle_stats_run):
     assert mine["collisions"] > 50000
 
 
+def test_oracle_degenerate_trace_vs_reference(block, oracle_lib):
+    """Exact paths through face centres (on the quads' split diagonals),
+    edges and vertices, starts on faces, edges and corners, particles at
+    rest, dt = 0, a denormal speed and a path along a face: bit-exact with
+    the reference wherever its loop returns. Where it does not (it was given
+    a few seconds per particle; the rest take milliseconds together) the
+    path meets a split quad's diagonal on a face whose zone has no role in
+    the reference's table (the block's sides, zone 7): CrossboundarySwitch
+    leaves the particle where it is and the next search finds the other
+    triangle of the same quad, without end. The oracle, like the CUDA path,
+    stops such a particle at max_crossings and reports it lost; with zone 7
+    given a role no particle reaches the bound."""
+    raw, dm, mess = block
+    g = golden("degenerate_trace_pin.npz")
+    x, v, dt, cell = I.degenerate_trace_inputs(dm, mess, int(g["ncells"]), int(g["seed"]))
+    assert len(g["ok"]) + len(g["spins"]) == len(cell)
+    o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir()))
+    r = o.trace(x, v, dt, cell, stop_at_wall=True)
+    ok, spins = g["ok"], g["spins"]
+    for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt"):
+        assert np.array_equal(r[k][ok], g[k]), k
+    # every outcome, drops (no exit found from a corner or face) among them
+    assert {-1, 0, 1} <= set(np.unique(g["ifout"]).tolist())
+    assert (g["face"] >= 0).sum() > 100
+    assert len(spins) > 0
+    lost = o.counters()["lost"]
+    assert lost == len(spins) and np.all(r["ncross"][spins] == 4096)
+    assert np.all(dm.edges["faceTag"][r["face"][spins]] == 7)
+    o7 = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES + [(7, 3, 0)], I.inflow_dir()))
+    o7.trace(x, v, dt, cell, stop_at_wall=True)
+    assert o7.counters()["lost"] == 0
+
+
 def test_oracle_tet_trace_bit_exact_vs_reference(oracle_lib):
     g = golden("tet_trace_pin.npz")
     raw, dm, mess = I.capsule_small()
