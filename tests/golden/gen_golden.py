@@ -39,8 +39,9 @@ outputs:
                  (two triangles and three quads per cell): arrays, fill, and
                  tracing-check outputs (8,000 particles)
   degenerate_trace_pin.npz tracing-check outputs for exact, degenerate
-                 paths on the 1/4 block mesh (degenerate_trace_inputs), and
-                 the particles on which the reference's loop does not return
+                 paths on the 1/4 block mesh (degenerate_trace_inputs), the
+                 particles on which the reference's loop does not return, and
+                 the same on the capsule tets (degenerate_tet_trace_inputs)
   macro_band.npz per-cell mean and seed-to-seed spread of the time-averaged
                  stress and heat-flux fields (writeAveragedMacro's
                  definitions) over the same 8 reference runs as stats_band,
@@ -255,6 +256,7 @@ def gen_prism(d):
 
 
 DEGEN_CELLS = 20
+DEGEN_TET_CELLS = 12
 DEGEN_SEED = 9
 DEGEN_SPIN_SECONDS = 3
 
@@ -294,9 +296,17 @@ def gen_degenerate(d):
         raise SystemExit(f"the reference finished on {int(np.sum(fin))} particles the oracle bounds")
     ok = np.setdiff1d(np.arange(len(cell)), cand)
     r = H.trace(cas, mess, x[ok], v[ok], dt[ok], cell[ok], True, timeout=120)
+    # the same on the capsule tetrahedra (every zone has a role there)
+    rawc, dmc, messc = I.capsule_small()
+    casc = os.path.join(d, "capd.cas")
+    M.write_cas(casc, rawc)
+    xt, vt, dtt, ct = I.degenerate_tet_trace_inputs(dmc, messc, DEGEN_TET_CELLS, DEGEN_SEED)
+    rt = H.trace(casc, messc, xt, vt, dtt, ct, True, timeout=120)
     np.savez_compressed(os.path.join(HERE, "degenerate_trace_pin.npz"), ncells=DEGEN_CELLS, seed=DEGEN_SEED,
                         spin_seconds=DEGEN_SPIN_SECONDS, ok=ok.astype(np.int32), spins=cand.astype(np.int32),
-                        **{k: r[k] for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt")})
+                        tet_ncells=DEGEN_TET_CELLS,
+                        **{k: r[k] for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt")},
+                        **{"tet_" + k: rt[k] for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt")})
 
 
 # the stress and heat-flux fields of macro_from_moments, banded like stats_band

@@ -139,6 +139,34 @@ def degenerate_trace_inputs(dm, mess, ncells: int, seed: int):
     return np.array(X), np.array(V), np.array(T), np.array(C, dtype=np.int32)
 
 
+def degenerate_tet_trace_inputs(dm, mess, ncells: int, seed: int):
+    """Exact, degenerate paths in tetrahedral cells: from the centroid, the
+    4 vertices, the 6 edge midpoints and the 4 face centroids of each of
+    ncells random cells, towards and away from each other of those 15
+    points at 3x the freestream speed, so that paths run along edges and
+    faces and through vertices. dt = dtime."""
+    P = dm.points.reshape(-1, 3)
+    rs = np.random.RandomState(seed)
+    cells = rs.choice(dm.ncell, ncells, replace=False)
+    u, _, _ = freestream(mess)
+    sp = 3.0 * float(np.linalg.norm(u))
+    dtime = float(mess["dtime"])
+    X, V, C = [], [], []
+    for c, A in zip(cells, P[tet_vertices(dm, cells)]):
+        pts = ([A.mean(0)] + [A[i] for i in range(4)] +
+               [(A[i] + A[j]) / 2 for i in range(4) for j in range(i + 1, 4)] +
+               [(A.sum(0) - A[i]) / 3 for i in range(4)])
+        for s0 in pts:
+            for t0 in pts:
+                d = t0 - s0
+                n = np.linalg.norm(d)
+                if n == 0:
+                    continue
+                for sgn in (1.0, -1.0):
+                    X.append(s0); V.append(sgn * d / n * sp); C.append(c)
+    return np.array(X), np.array(V), np.full(len(C), dtime), np.array(C, dtype=np.int32)
+
+
 def fill_inputs(dm, mess, ppc: int, seed: int):
     """ppc particles per cell from the freestream Maxwellian."""
     rs = np.random.RandomState(seed)

@@ -229,6 +229,23 @@ def test_oracle_degenerate_trace_vs_reference(block, oracle_lib):
     assert o7.counters()["lost"] == 0
 
 
+def test_oracle_degenerate_tet_trace_vs_reference(oracle_lib):
+    """Paths along tetrahedron edges and faces and through vertices, from
+    vertices, edge midpoints, face centroids and centroids: bit-exact with
+    the reference on every particle (every zone of the capsule has a role,
+    so the reference's loop always returns)."""
+    g = golden("degenerate_trace_pin.npz")
+    raw, dm, mess = I.capsule_small()
+    x, v, dt, cell = I.degenerate_tet_trace_inputs(dm, mess, int(g["tet_ncells"]), int(g["seed"]))
+    o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir()))
+    r = o.trace(x, v, dt, cell, stop_at_wall=True)
+    for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt"):
+        assert np.array_equal(r[k], g["tet_" + k]), k
+    c = o.counters()
+    assert c["lost"] == 0 and c["dropped"] > len(cell) // 4 and c["crossings"] > 500
+    assert {-1, 0, 1} <= set(np.unique(g["tet_ifout"]).tolist())
+
+
 def test_oracle_tet_trace_bit_exact_vs_reference(oracle_lib):
     g = golden("tet_trace_pin.npz")
     raw, dm, mess = I.capsule_small()
