@@ -22,6 +22,10 @@ outputs:
                  update, how many particles kept their input position, whether
                  every moved particle carries a kept particle's velocity, and
                  the box-relative positions of the moved particles
+  gsis_tet_pin.npz the same on the capsule tets: counts, kept counts and
+                 copies per cell, the largest deviations of the moments from
+                 the NS values, and 8,000 of the moved particles' sorted
+                 barycentric weights
   fill_pin.npz   the reference's initial fill (Np_tri_inititial + meshfillpar)
                  with the counts of the fill rule: per-tetrahedron counts and
                  box-relative positions on the 1/4 block mesh (centre-face
@@ -107,12 +111,14 @@ def fill_counts(dm, ppc, seed):
     return out
 
 
-def gsis_summary(dm, before, after):
-    """Per-cell counts, moments and structure of a GSIS update's output."""
+def gsis_summary(dm, before, after, tets=False):
+    """Per-cell counts, moments and structure of a GSIS update's output; the
+    moved particles' positions relative to their cell's box (hexahedra) or
+    as sorted barycentric weights (tetrahedra)."""
     x0, v0, ir0, c0 = before
     x1, v1, ir1, c1 = after
     nc = dm.ncell
-    lo, hi = I.cell_boxes(dm)
+    lo, hi = (None, None) if tets else I.cell_boxes(dm)
     kept = np.zeros(nc, np.int32)
     dup_ok = np.ones(nc, bool)
     rel = []
@@ -128,13 +134,36 @@ def gsis_summary(dm, before, after):
             vk = {tuple(p) for p in V1[is_kept]}
             dup_ok[c] = all(tuple(p) in vk for p in V1[~is_kept])
         if (~is_kept).any():
-            rel.append((X1[~is_kept] - lo[c]) / (hi[c] - lo[c]))
+            moved = X1[~is_kept]
+            rel.append(sorted_barycentric(dm, moved, np.full(len(moved), c)) if tets else
+                       (moved - lo[c]) / (hi[c] - lo[c]))
     n = np.bincount(c1, minlength=nc).astype(float)
     m = np.maximum(n, 1.0)
     u = np.stack([np.bincount(c1, v1[:, k], nc) for k in range(3)], 1) / m[:, None]
     return {"counts": n.astype(np.int32), "u": u, "kept": kept, "dup_ok": dup_ok,
             "sums": np.stack([np.bincount(c1, (v1 * v1).sum(1), nc), np.bincount(c1, ir1, nc)], 1),
             "rel": np.concatenate(rel) if rel else np.zeros((0, 3))}
+
+
+GSIS_TET_REL = 8000
+
+
+def gsis_moment_errors(dm, mess, cell0, ns, acc, nan_cell, summ):
+    """How far a GSIS update's per-cell moments are from the NS values, over
+    the updated cells holding more than one particle with T > 0: the largest
+    velocity error relative to the largest |u|, the largest relative T and
+    Tr errors, and the share of such cells among the updated ones."""
+    upd = acc.astype(bool)
+    upd[nan_cell:] = False
+    n = summ["counts"].astype(float)
+    live = upd & (n > 1)
+    m = np.maximum(n, 1)
+    T = 2.0 / (3.0 * m) * (summ["sums"][:, 0] - n * (summ["u"] ** 2).sum(1))
+    Tr = 4.0 / float(mess["dr"]) / m * summ["sums"][:, 1]
+    ok = live & (T > 0)
+    return {"u_err": np.abs(summ["u"][ok] - ns[ok, 1:4]).max() / np.abs(ns[ok, 1:4]).max(),
+            "T_err": np.abs(T[ok] / ns[ok, 4] - 1).max(), "Tr_err": np.abs(Tr[ok] / ns[ok, 5] - 1).max(),
+            "ok_share": ok.sum() / max(live.sum(), 1)}
 
 
 def sorted_barycentric(dm, x, cell):
@@ -154,6 +183,18 @@ def gen_gsis_fill(d):
     r = H.gsis(cas, mess, *parts, ns, acc, seed=7)
     summ = gsis_summary(dm, parts, (r["x"], r["v"], r["ir"], r["cell"]))
     np.savez_compressed(os.path.join(HERE, "gsis_pin.npz"), ppc=GSIS_PPC, seed=GSIS_SEED, **summ)
+    # the same on the capsule tets
+    rawt, dmt, messt = I.capsule_small()
+    cast = os.path.join(d, "capgs.cas")
+    M.write_cas(cast, rawt)
+    parts, ns, acc, nan_cell, empty, neg = I.gsis_edge_inputs(dmt, messt, GSIS_PPC, GSIS_SEED, tets=True)
+    r = H.gsis(cast, messt, *parts, ns, acc, seed=7)
+    summ = gsis_summary(dmt, parts, (r["x"], r["v"], r["ir"], r["cell"]), tets=True)
+    err = gsis_moment_errors(dmt, messt, parts[3], ns, acc, nan_cell, summ)
+    sub = np.random.RandomState(1).permutation(len(summ["rel"]))[:GSIS_TET_REL]
+    np.savez_compressed(os.path.join(HERE, "gsis_tet_pin.npz"), ppc=GSIS_PPC, seed=GSIS_SEED,
+                        counts=summ["counts"], kept=summ["kept"], dup_ok=summ["dup_ok"],
+                        rel=summ["rel"][np.sort(sub)].astype(np.float32), n_rel=len(summ["rel"]), **err)
 
     counts = fill_counts(dm, FILL_PPC, FILL_SEED)
     f = H.fill(cas, mess, counts, seed=8)

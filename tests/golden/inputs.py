@@ -263,11 +263,12 @@ def gsis_inputs(dm, mess, ppc: int, seed: int, gate: bool = True, nan: bool = Tr
     return ns, acc, nan_cell
 
 
-def gsis_edge_inputs(dm, mess, ppc: int, seed: int):
-    """Particles (fill_inputs) with 40 cells emptied, and an NS solution
-    (gsis_inputs, gate on, NaN cell) in which 5 of the empty cells have
-    T < 0 and 10 occupied cells a negative density."""
-    x, v, ir, cell = fill_inputs(dm, mess, ppc, seed)
+def gsis_edge_inputs(dm, mess, ppc: int, seed: int, tets: bool = False):
+    """Particles (fill_inputs, or fill_inputs_any on tetrahedra) with 40
+    cells emptied, and an NS solution (gsis_inputs, gate on, NaN cell) in
+    which 5 of the empty cells have T < 0 and 10 occupied cells a negative
+    density."""
+    x, v, ir, cell = (fill_inputs_any if tets else fill_inputs)(dm, mess, ppc, seed)
     rs = np.random.RandomState(seed + 1)
     empty = rs.choice(dm.ncell - 40, 40, replace=False)
     keep = ~np.isin(cell, empty)

@@ -1,13 +1,15 @@
 """The oracle's initial fill and GSIS particle update, pinned against the
-reference's own code (tests/golden/gsis_pin.npz and fill_pin.npz, made by
-gen_golden.py from oracle/_ref/ref_harness on the same inputs).
+reference's own code (tests/golden/gsis_pin.npz, gsis_tet_pin.npz and
+fill_pin.npz, made by gen_golden.py from oracle/_ref/ref_harness on the same
+inputs).
 
 The reference draws from mt19937 and rand(), the oracle (and the CUDA
 library) from Philox, so the pins are the properties that do not depend on
 the draws, compared exactly, and the distributions, compared by tests:
 
-- update: every updated cell holds floor or ceil of its NS count (the ceil
-  as often as the fractional parts say), empty cells with T < 0 stay empty,
+- update (hexahedra of the block, and the capsule tets): every updated cell
+  holds floor or ceil of its NS count (the ceil as often as the fractional
+  parts say), empty cells with T < 0 stay empty,
   negative densities keep the count, gated-out cells and cells from the NaN
   cell on are untouched; the particles that kept their position number
   min(before, after); every moved particle carries a kept particle's
@@ -185,3 +187,55 @@ def test_placement_tetrahedra_fill_the_cells(block, oracle_lib):
         off, V, vol = o.placement()
         assert np.all(np.diff(off) > 0)
         assert np.abs(np.add.reduceat(vol, off[:-1]) / dm.cells["area"] - 1.0).max() < 1e-9
+
+
+@pytest.fixture(scope="module")
+def gsis_tet_case(oracle_lib):
+    raw, dm, mess = I.capsule_small()
+    g = golden("gsis_tet_pin.npz")
+    parts, ns, acc, nan_cell, empty, neg = I.gsis_edge_inputs(dm, mess, int(g["ppc"]), int(g["seed"]), tets=True)
+    o = _oracle(oracle_lib, dm, mess, seed=21)
+    o.set_particles(*parts)
+    rep = o.molecular_velocity_change(ns, acc)
+    from gen_golden import gsis_summary
+    mine = gsis_summary(dm, parts, o.particles(), tets=True)
+    return dm, mess, parts, ns, acc, nan_cell, empty, neg, g, mine, rep
+
+
+def test_update_on_tets_follows_the_reference(gsis_tet_case):
+    """The update on the capsule tets: counts, kept particles and copies as
+    on hexahedra, the moments equal to the NS values in both, and the moved
+    particles' sorted barycentric weights (four uniforms over their sum, the
+    reference's placement in a tetrahedron) with the same distribution."""
+    from gen_golden import gsis_moment_errors
+    dm, mess, parts, ns, acc, nan_cell, empty, neg, g, mine, rep = gsis_tet_case
+    nc = dm.ncell
+    n0 = np.bincount(parts[3], minlength=nc)
+    upd = acc.astype(bool)
+    upd[nan_cell:] = False
+    x = ns[:, 0] * dm.cells["area"] * float(mess["n_ref"]) / float(mess["Neff"])
+    fl = np.floor(x)
+    regular = upd & ~np.isin(np.arange(nc), empty[:5]) & ~np.isin(np.arange(nc), neg)
+    frac = (x - fl)[regular]
+    for res in (g, mine):
+        n = res["counts"]
+        assert np.array_equal(n[~upd], n0[~upd])
+        assert np.all(n[empty[:5]] == 0)
+        assert np.array_equal(n[neg], n0[neg])
+        assert np.all((n[regular] == fl[regular]) | (n[regular] == fl[regular] + 1))
+        k = (n[regular] == fl[regular] + 1).sum()
+        assert abs(k - frac.sum()) < 5 * np.sqrt((frac * (1 - frac)).sum())
+        assert np.array_equal(res["kept"], np.minimum(n0, n))
+        assert res["dup_ok"].all()
+    assert rep["nan_cell"] == nan_cell and rep["cells_updated"] == int(upd.sum())
+    err = gsis_moment_errors(dm, mess, parts[3], ns, acc, nan_cell, mine)
+    for e in (g, err):
+        assert float(e["ok_share"]) > 0.8
+        assert float(e["u_err"]) < 1e-12 and float(e["T_err"]) < 1e-11 and float(e["Tr_err"]) < 1e-11
+    a, b = g["rel"].astype(float), mine["rel"]
+    assert len(b) > 5000 and abs(len(b) / int(g["n_rel"]) - 1) < 0.1
+    assert b.min() > -1e-9 and b.max() < 1 + 1e-9
+    for k in range(4):
+        assert stats.ks_2samp(a[:, k], b[:, k]).pvalue > 1e-3
+    # not uniform in the tetrahedron (Dirichlet(1,1,1,1): mean largest weight 25/48)
+    assert a[:, 3].mean() < 0.45 and b[:, 3].mean() < 0.45
