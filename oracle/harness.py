@@ -92,6 +92,27 @@ def trace_finishes(cas: str, mess, x, v, dt, cell, seconds: float) -> bool:
         return False
 
 
+def sample(cas: str, mess, x, v, ir, cell, nsteps: int, ppc: int) -> dict:
+    """statistic_macroPre, then statistic_macro(k) for k = 1..nsteps on the
+    particles of each step (the harness's sampledAt rule over the given
+    ones, ppc per cell in input order); the macro arrays and window state
+    after the last step."""
+    n = int(np.asarray(cell).shape[0])
+    with tempfile.TemporaryDirectory() as d:
+        pm, pp = os.path.join(d, "mess.bin"), os.path.join(d, "parts.bin")
+        _write_mess(pm, mess)
+        _write_particles(pp, x, v, ir, np.zeros(n), cell)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        _run(["sample", cas, pm, pp, out, nsteps, ppc])
+        res = {k: np.fromfile(os.path.join(out, k + ".bin"), dtype=np.float64).reshape(-1, 18)
+               for k in ("local", "record", "final_record")}
+        res["window_samples"] = np.fromfile(os.path.join(out, "window_samples.bin"), dtype=np.float64)
+        res["window_valid"] = np.fromfile(os.path.join(out, "window_valid.bin"), dtype=np.float64).astype(np.int8)
+        res["sparse_state"] = np.fromfile(os.path.join(out, "sparse_state.bin"), dtype=np.uint8)
+        return res
+
+
 def advect(cas: str, mess, x, v, ir, cell, istep: int = 1, roles: str = "-") -> dict:
     """The reference's advection(istep) + cache2chain(); buckets in order."""
     n = int(np.asarray(cell).shape[0])

@@ -49,6 +49,12 @@
  *       FIELDS ([ncell][18] doubles) with MESS as the case constants, into
  *       OUT/fields.dat; the zone declarations (zonemap: id, first, last) go
  *       to OUT/zones.bin (int32).
+ *   sample CAS MESS PARTS OUT NSTEPS PPC
+ *       statistic_macroPre, then for every step k = 1..NSTEPS the buckets
+ *       are refilled with the step's particles (sampledAt: PARTS thinned
+ *       and scaled by a rule of k, PPC particles per cell in PARTS) and the
+ *       public statistic_macro(k) runs; dumps local, record, final_record,
+ *       the window samples and validity and the sparse states.
  *   ROLES is "-" or a comma list tag:role with role in
  *       none,interface,inlet,outlet,wall.
  */
@@ -486,6 +492,53 @@ int cmdFill(int argc, char** argv)
     return ok && writeFile(out + "/np_tri.bin", npTri.data(), npTri.size() * 4) ? 0 : 1;
 }
 
+// The particles sampled at step k in the "sample" command: particle i of
+// the input (cell c) is present unless c % 5 == 0 and (k % 50 != 0 or
+// i % PPC != 0) (such cells hold one particle on two steps of every
+// 100: sparse windows), or c % 5 == 1 and (k + i) % 3 == 0; velocities are
+// scaled by s = 1 + (k % 8) / 16 and Ir by s * s (both exact in binary).
+bool sampledAt(int k, std::size_t i, int c, int ppc)
+{
+    if (c % 5 == 0) return k % 50 == 0 && (int)(i % (std::size_t)ppc) == 0;
+    if (c % 5 == 1) return (k + (long long)i) % 3 != 0;
+    return true;
+}
+
+int cmdSample(int argc, char** argv)
+{
+    if (argc < 8) return 2;
+    Rig r;
+    if (!buildRig(r, argv[2], argv[3], "-")) return 1;
+    Particles P;
+    if (!readParticles(argv[4], P)) return 1;
+    const std::string out = argv[5];
+    const int nsteps = std::atoi(argv[6]);
+    const int ppc = std::atoi(argv[7]);
+    ProcessDSMC& p = *r.process;
+    p.statistic_macroPre();
+    for (int k = 1; k <= nsteps; ++k) {
+        for (auto& b : r.partinit->cell_particles_curr) b.clear();
+        const double s = 1.0 + (double)(k % 8) / 16.0;
+        Particles Q;
+        for (std::size_t i = 0; i < P.size(); ++i) {
+            if (!sampledAt(k, i, P.cell[i], ppc)) continue;
+            Q.px.push_back(P.px[i]); Q.py.push_back(P.py[i]); Q.pz.push_back(P.pz[i]);
+            Q.vx.push_back(P.vx[i] * s); Q.vy.push_back(P.vy[i] * s); Q.vz.push_back(P.vz[i] * s);
+            Q.ir.push_back(P.ir[i] * (s * s)); Q.dt.push_back(0.0); Q.cell.push_back(P.cell[i]);
+        }
+        fillBuckets(r, Q);
+        p.statistic_macro(k);
+    }
+    std::vector<double> wv(p.dsmc2ns_window_valid.begin(), p.dsmc2ns_window_valid.end());
+    bool ok = writeFile(out + "/local.bin", p.local.data(), p.local.size() * 8);
+    ok = ok && writeFile(out + "/record.bin", p.record.data(), p.record.size() * 8);
+    ok = ok && writeFile(out + "/final_record.bin", p.final_record.data(), p.final_record.size() * 8);
+    ok = ok && writeFile(out + "/window_samples.bin", p.dsmc2ns_window_samples.data(), p.dsmc2ns_window_samples.size() * 8);
+    ok = ok && writeFile(out + "/window_valid.bin", wv.data(), wv.size() * 8);
+    ok = ok && writeFile(out + "/sparse_state.bin", p.dsmc2ns_sparse_state.data(), p.dsmc2ns_sparse_state.size());
+    return ok ? 0 : 1;
+}
+
 int cmdFluent(int argc, char** argv)
 {
     if (argc < 6) return 2;
@@ -527,6 +580,7 @@ int main(int argc, char** argv)
     if (cmd == "gsis") return cmdGsis(argc, argv);
     if (cmd == "fill") return cmdFill(argc, argv);
     if (cmd == "fluent") return cmdFluent(argc, argv);
+    if (cmd == "sample") return cmdSample(argc, argv);
     std::fprintf(stderr, "unknown command %s\n", cmd.c_str());
     return 2;
 }

@@ -46,6 +46,10 @@ outputs:
                  paths on the 1/4 block mesh (degenerate_trace_inputs), the
                  particles on which the reference's loop does not return, and
                  the same on the capsule tets (degenerate_tet_trace_inputs)
+  sample_pin.npz the reference's statistic_macro over 5,200 steps of a
+                 deterministic particle sequence on the 1/8 block mesh
+                 (inputs.sampled_at): local, record, final_record, window
+                 samples and validity, sparse states
   macro_band.npz per-cell mean and seed-to-seed spread of the time-averaged
                  stress and heat-flux fields (writeAveragedMacro's
                  definitions) over the same 8 reference runs as stats_band,
@@ -296,6 +300,22 @@ def gen_prism(d):
     np.savez_compressed(os.path.join(HERE, "prism_pin.npz"), **fill, **{"trace_" + k: v for k, v in trace.items()})
 
 
+SAMPLE_PPC = 6
+SAMPLE_SEED = 31
+SAMPLE_STEPS = 5200          # past NSCHEME (2000) and NSS (5000), src/meshImport.h:48-59
+
+
+def gen_sample(d):
+    raw, dm = I.block_mesh(scale=8)
+    cas = os.path.join(d, "b8s.cas")
+    M.write_cas(cas, raw)
+    mess = I.block_mess(dm, SAMPLE_PPC)
+    x, v, ir, cell = I.fill_inputs(dm, mess, SAMPLE_PPC, SAMPLE_SEED)
+    r = H.sample(cas, mess, x, v, ir, cell, SAMPLE_STEPS, SAMPLE_PPC)
+    np.savez_compressed(os.path.join(HERE, "sample_pin.npz"), ppc=SAMPLE_PPC, seed=SAMPLE_SEED, steps=SAMPLE_STEPS,
+                        **r)
+
+
 DEGEN_CELLS = 20
 DEGEN_TET_CELLS = 12
 DEGEN_SEED = 9
@@ -377,9 +397,9 @@ def main():
     if not H.available():
         raise SystemExit("oracle/_ref/ref_harness missing: make -C oracle ref")
     want = set(sys.argv[1:])
-    if want - {"gsis", "fill", "fluent", "pyramid", "prism", "band", "degenerate", "core"}:
+    if want - {"gsis", "fill", "fluent", "pyramid", "prism", "band", "degenerate", "sample", "core"}:
         raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent, pyramid, "
-                         "prism, band, degenerate")
+                         "prism, band, degenerate, sample")
     with tempfile.TemporaryDirectory() as d:
         if not want or want & {"gsis", "fill"}:
             gen_gsis_fill(d)
@@ -393,6 +413,8 @@ def main():
             gen_band(d)
         if not want or "degenerate" in want:
             gen_degenerate(d)
+        if not want or "sample" in want:
+            gen_sample(d)
         if not want or "core" in want:
             gen_core(d)
     print("fixtures written to", HERE)

@@ -167,6 +167,22 @@ def degenerate_tet_trace_inputs(dm, mess, ncells: int, seed: int):
     return np.array(X), np.array(V), np.full(len(C), dtime), np.array(C, dtype=np.int32)
 
 
+def sampled_at(k: int, cell, ppc: int):
+    """The particles (a mask over fill_inputs' cell-major order, ppc per
+    cell) sampled at step k of the harness's "sample" command, and the
+    velocity scale s (Ir scales by s * s): cells c % 5 == 0 hold one
+    particle on two steps of every 100, cells c % 5 == 1 lose a third of
+    theirs in turn."""
+    i = np.arange(len(cell))
+    c = np.asarray(cell)
+    keep = np.ones(len(c), dtype=bool)
+    a = c % 5 == 0
+    keep[a] = (k % 50 == 0) & (i[a] % ppc == 0)
+    b = c % 5 == 1
+    keep[b] = (k + i[b]) % 3 != 0
+    return keep, 1.0 + (k % 8) / 16.0
+
+
 def fill_inputs(dm, mess, ppc: int, seed: int):
     """ppc particles per cell from the freestream Maxwellian."""
     rs = np.random.RandomState(seed)

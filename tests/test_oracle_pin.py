@@ -246,6 +246,39 @@ def test_oracle_degenerate_tet_trace_vs_reference(oracle_lib):
     assert {-1, 0, 1} <= set(np.unique(g["tet_ifout"]).tolist())
 
 
+def test_oracle_sampling_bit_exact_vs_reference(oracle_lib):
+    """statistic_macro (src/ProcessDSMC.cpp:2757-2861) over 5,200 steps of
+    a particle sequence with no random draws (inputs.sampled_at: thinned
+    and rescaled particles, cells that hold one particle on two steps of
+    each 100-step window): the step-window average with its exponential
+    weight after NSCHEME, the steady average after NSS, the GSIS window
+    samples, validity and record, and the sparse-cell state machine, all
+    bit-exact with the reference's."""
+    from pydsmc import gpu
+    g = golden("sample_pin.npz")
+    raw, dm = I.block_mesh(scale=8)
+    ppc = int(g["ppc"])
+    mess = I.block_mess(dm, ppc)
+    x, v, ir, cell = I.fill_inputs(dm, mess, ppc, int(g["seed"]))
+    o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir(), nss=5000, nscheme=2000, nevery=1,
+                                                 nrepeat=100))
+    o.macro_pre()
+    for k in range(1, int(g["steps"]) + 1):
+        keep, s = I.sampled_at(k, cell, ppc)
+        o.set_particles(x[keep], v[keep] * s, ir[keep] * (s * s), cell[keep])
+        o.step(k, 0x10)
+    for name, which in (("local", gpu.MACRO_LOCAL), ("record", gpu.MACRO_RECORD),
+                        ("final_record", gpu.MACRO_FINAL_RECORD)):
+        assert np.array_equal(o.macro(which), g[name]), name
+    cn = o.counts()
+    for k in ("window_samples", "window_valid", "sparse_state"):
+        assert np.array_equal(cn[k], g[k]), k
+    # the sequence reaches the sparse state and fills every output
+    assert (g["sparse_state"] == 1).sum() > 10 and (g["sparse_state"] == 0).sum() > 10
+    for name in ("local", "record", "final_record"):
+        assert (g[name][:, 0] > 0).all()
+
+
 def test_oracle_tet_trace_bit_exact_vs_reference(oracle_lib):
     g = golden("tet_trace_pin.npz")
     raw, dm, mess = I.capsule_small()
