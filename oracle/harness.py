@@ -113,6 +113,25 @@ def sample(cas: str, mess, x, v, ir, cell, nsteps: int, ppc: int) -> dict:
         return res
 
 
+def collide(cas: str, mess, x, v, ir, cell, seed: int = 1) -> dict:
+    """One collisionDSMC() on the given particles from the initial crmax and
+    remainders: remainders, crmax, candidate pairs, collisions and the
+    buckets after it."""
+    n = int(np.asarray(cell).shape[0])
+    with tempfile.TemporaryDirectory() as d:
+        pm, pp = os.path.join(d, "mess.bin"), os.path.join(d, "parts.bin")
+        _write_mess(pm, mess)
+        _write_particles(pp, x, v, ir, np.zeros(n), cell)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        _run(["collide", cas, pm, pp, out, seed])
+        cnt = np.fromfile(os.path.join(out, "counts.bin"), dtype=np.float64)
+        return {"remcoll": np.fromfile(os.path.join(out, "remcoll.bin"), dtype=np.float64),
+                "crmax": np.fromfile(os.path.join(out, "crmax.bin"), dtype=np.float64),
+                "pairs": int(cnt[0]), "collisions": int(cnt[1]),
+                "particles": _read_particles(os.path.join(out, "particles.bin"))}
+
+
 def advect(cas: str, mess, x, v, ir, cell, istep: int = 1, roles: str = "-") -> dict:
     """The reference's advection(istep) + cache2chain(); buckets in order."""
     n = int(np.asarray(cell).shape[0])

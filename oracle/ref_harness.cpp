@@ -55,6 +55,12 @@
  *       and scaled by a rule of k, PPC particles per cell in PARTS) and the
  *       public statistic_macro(k) runs; dumps local, record, final_record,
  *       the window samples and validity and the sparse states.
+ *   collide CAS MESS PARTS OUT SEED
+ *       Fills the buckets and runs the public collisionDSMC() once from the
+ *       initial crmax and remainders (Collision_constant_initial); dumps
+ *       the remainders, crmax, the candidate pairs and collisions
+ *       (tol_collision_pairs / tol_collision_times, two doubles) and every
+ *       bucket.
  *   ROLES is "-" or a comma list tag:role with role in
  *       none,interface,inlet,outlet,wall.
  */
@@ -539,6 +545,28 @@ int cmdSample(int argc, char** argv)
     return ok ? 0 : 1;
 }
 
+int cmdCollide(int argc, char** argv)
+{
+    if (argc < 7) return 2;
+    Rig r;
+    if (!buildRig(r, argv[2], argv[3], "-")) return 1;
+    Particles P;
+    if (!readParticles(argv[4], P)) return 1;
+    const std::string out = argv[5];
+    const unsigned seed = (unsigned)std::strtoul(argv[6], nullptr, 10);
+    r.partinit->thread_rng().seed(seed);
+    std::srand(seed);
+    fillBuckets(r, P);
+    ProcessDSMC& p = *r.process;
+    p.collisionDSMC();
+    const double counts[2] = {(double)p.tol_collision_pairs, (double)p.tol_collision_times};
+    bool ok = writeFile(out + "/remcoll.bin", r.partinit->remainderincoll.data(), r.partinit->remainderincoll.size() * 8);
+    ok = ok && writeFile(out + "/crmax.bin", r.partinit->crmax.data(), r.partinit->crmax.size() * 8);
+    ok = ok && writeFile(out + "/counts.bin", counts, sizeof counts);
+    ok = ok && writeParticles(out + "/particles.bin", dumpBuckets(r));
+    return ok ? 0 : 1;
+}
+
 int cmdFluent(int argc, char** argv)
 {
     if (argc < 6) return 2;
@@ -581,6 +609,7 @@ int main(int argc, char** argv)
     if (cmd == "fill") return cmdFill(argc, argv);
     if (cmd == "fluent") return cmdFluent(argc, argv);
     if (cmd == "sample") return cmdSample(argc, argv);
+    if (cmd == "collide") return cmdCollide(argc, argv);
     std::fprintf(stderr, "unknown command %s\n", cmd.c_str());
     return 2;
 }

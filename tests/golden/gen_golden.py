@@ -50,6 +50,10 @@ outputs:
                  deterministic particle sequence on the 1/8 block mesh
                  (inputs.sampled_at): local, record, final_record, window
                  samples and validity, sparse states
+  collide_pin.npz one collisionDSMC of the reference on ragged particle
+                 sets (block hexahedra and capsule tets): the NTC remainders,
+                 candidate pairs, collisions, how many cells raised crmax,
+                 and the largest per-cell momentum and energy changes
   macro_band.npz per-cell mean and seed-to-seed spread of the time-averaged
                  stress and heat-flux fields (writeAveragedMacro's
                  definitions) over the same 8 reference runs as stats_band,
@@ -316,6 +320,52 @@ def gen_sample(d):
                         **r)
 
 
+COLLIDE_PPC = (20, 12)        # block hexahedra, capsule tets
+COLLIDE_SEED = 41
+
+
+def collide_cases():
+    """Ragged particle sets for one collisionDSMC: the 1/4 block mesh and the
+    capsule tets."""
+    raw, dm = I.block_mesh()
+    mess = I.block_mess(dm, STATS_PPC)
+    rawc, dmc, messc = I.capsule_small()
+    out = []
+    for (r, m, ms, fill, ppc, k) in ((raw, dm, mess, I.fill_inputs, COLLIDE_PPC[0], 0),
+                                     (rawc, dmc, messc, I.fill_inputs_any, COLLIDE_PPC[1], 1)):
+        parts = I.ragged(fill(m, ms, ppc, COLLIDE_SEED + k), m.ncell, ppc, COLLIDE_SEED + 10 + k)
+        out.append((r, m, ms, parts))
+    return out
+
+
+def collision_conservation(ncell, before, after):
+    """The largest per-cell change of momentum (relative to the cell's
+    momentum scale sqrt(sum |v|^2)) and of energy sum(|v|^2 / 2 + Ir)
+    (relative) between two particle sets."""
+    def sums(p):
+        x, v, ir, c = p
+        mom = np.stack([np.bincount(c, v[:, j], ncell) for j in range(3)], 1)
+        return mom, np.bincount(c, 0.5 * (v * v).sum(1) + ir, ncell), np.sqrt(np.bincount(c, (v * v).sum(1), ncell))
+    m0, e0, s0 = sums(before)
+    m1, e1, _ = sums(after)
+    live = s0 > 0
+    return (float((np.abs(m1 - m0).max(1)[live] / s0[live]).max()),
+            float((np.abs(e1 - e0)[live] / e0[live]).max()))
+
+
+def gen_collide(d):
+    res = {}
+    for k, (raw, dm, mess, parts) in zip(("block", "tets"), collide_cases()):
+        cas = os.path.join(d, f"col_{k}.cas")
+        M.write_cas(cas, raw)
+        r = H.collide(cas, mess, *parts, seed=3)
+        after = (r["particles"]["x"], r["particles"]["v"], r["particles"]["ir"], r["particles"]["cell"])
+        dmom, den = collision_conservation(dm.ncell, parts, after)
+        res.update({f"{k}_remcoll": r["remcoll"], f"{k}_pairs": r["pairs"], f"{k}_collisions": r["collisions"],
+                    f"{k}_crmax_raised": int((r["crmax"] > 3.0).sum()), f"{k}_dmom": dmom, f"{k}_den": den})
+    np.savez_compressed(os.path.join(HERE, "collide_pin.npz"), **res)
+
+
 DEGEN_CELLS = 20
 DEGEN_TET_CELLS = 12
 DEGEN_SEED = 9
@@ -397,9 +447,9 @@ def main():
     if not H.available():
         raise SystemExit("oracle/_ref/ref_harness missing: make -C oracle ref")
     want = set(sys.argv[1:])
-    if want - {"gsis", "fill", "fluent", "pyramid", "prism", "band", "degenerate", "sample", "core"}:
+    if want - {"gsis", "fill", "fluent", "pyramid", "prism", "band", "degenerate", "sample", "collide", "core"}:
         raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent, pyramid, "
-                         "prism, band, degenerate, sample")
+                         "prism, band, degenerate, sample, collide")
     with tempfile.TemporaryDirectory() as d:
         if not want or want & {"gsis", "fill"}:
             gen_gsis_fill(d)
@@ -415,6 +465,8 @@ def main():
             gen_degenerate(d)
         if not want or "sample" in want:
             gen_sample(d)
+        if not want or "collide" in want:
+            gen_collide(d)
         if not want or "core" in want:
             gen_core(d)
     print("fixtures written to", HERE)

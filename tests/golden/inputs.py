@@ -183,6 +183,15 @@ def sampled_at(k: int, cell, ppc: int):
     return keep, 1.0 + (k % 8) / 16.0
 
 
+def ragged(parts, ncell: int, ppc: int, seed: int):
+    """Thin particles given ppc per cell in cell-major order: each cell keeps
+    a share drawn uniformly in [0, 1), so counts run from 0 to ppc."""
+    rs = np.random.RandomState(seed)
+    x, v, ir, cell = parts
+    keep = rs.random_sample(len(cell)) < np.repeat(rs.random_sample(ncell), ppc)
+    return x[keep], v[keep], ir[keep], cell[keep]
+
+
 def fill_inputs(dm, mess, ppc: int, seed: int):
     """ppc particles per cell from the freestream Maxwellian."""
     rs = np.random.RandomState(seed)

@@ -279,6 +279,34 @@ def test_oracle_sampling_bit_exact_vs_reference(oracle_lib):
         assert (g[name][:, 0] > 0).all()
 
 
+def test_oracle_ntc_pairs_bit_exact_vs_reference(oracle_lib):
+    """One collisionDSMC (src/ProcessDSMC.cpp:2621-2666) on ragged cells
+    (0 to ppc particles) of the block and the capsule tets, from the initial
+    crmax and remainders: the NTC candidate pairs of every cell and the
+    remainder each cell carries are bit-exact with the reference's (they
+    depend on no draw); the accepted collisions, which do, agree within 4
+    binomial sigma, and both conserve every cell's momentum and energy to
+    rounding."""
+    from gen_golden import collide_cases, collision_conservation
+    g = golden("collide_pin.npz")
+    for k, (raw, dm, mess, parts) in zip(("block", "tets"), collide_cases()):
+        o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir(), seed=3))
+        o.set_particles(*parts)
+        o.step(1, 0x8)
+        crmax, rem, _ = o.cell_state()
+        c = o.counters()
+        assert np.array_equal(rem, g[f"{k}_remcoll"]), k
+        assert c["candidate_pairs"] == int(g[f"{k}_pairs"]), k
+        pairs, ref = int(g[f"{k}_pairs"]), int(g[f"{k}_collisions"])
+        p = ref / pairs
+        assert abs(c["collisions"] - ref) < 4 * np.sqrt(pairs * p * (1 - p)) + 4, (k, c["collisions"], ref)
+        dmom, den = collision_conservation(dm.ncell, parts, o.particles())
+        assert dmom < 1e-13 and den < 1e-13
+        assert float(g[f"{k}_dmom"]) < 1e-13 and float(g[f"{k}_den"]) < 1e-13
+        assert (np.bincount(parts[3], minlength=dm.ncell) <= 1).sum() > 10      # empty and single cells too
+    assert int(g["tets_pairs"]) > 500000
+
+
 def test_oracle_tet_trace_bit_exact_vs_reference(oracle_lib):
     g = golden("tet_trace_pin.npz")
     raw, dm, mess = I.capsule_small()
