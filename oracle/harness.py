@@ -132,6 +132,22 @@ def collide(cas: str, mess, x, v, ir, cell, seed: int = 1) -> dict:
                 "particles": _read_particles(os.path.join(out, "particles.bin"))}
 
 
+def inject(cas: str, mess, nsteps: int, seed: int = 1) -> dict:
+    """preprocesseffquad on an empty domain for nsteps: the injected
+    particles that stayed in the domain, their count per step and the
+    inflow remainders."""
+    with tempfile.TemporaryDirectory() as d:
+        pm = os.path.join(d, "mess.bin")
+        _write_mess(pm, mess)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        _run(["inject", cas, pm, out, nsteps, seed])
+        res = _read_particles(os.path.join(out, "particles.bin"))
+        res["per_step"] = np.fromfile(os.path.join(out, "steps.bin"), dtype=np.int64)
+        res["reminj"] = np.fromfile(os.path.join(out, "reminj.bin"), dtype=np.float64)
+        return res
+
+
 def advect(cas: str, mess, x, v, ir, cell, istep: int = 1, roles: str = "-") -> dict:
     """The reference's advection(istep) + cache2chain(); buckets in order."""
     n = int(np.asarray(cell).shape[0])

@@ -61,6 +61,12 @@
  *       the remainders, crmax, the candidate pairs and collisions
  *       (tol_collision_pairs / tol_collision_times, two doubles) and every
  *       bucket.
+ *   inject CAS MESS OUT NSTEPS SEED
+ *       With no particles in the domain, the public preprocesseffquad(k)
+ *       for k = 1..NSTEPS; after each step the injected particles that
+ *       stayed in the domain (recv_cache) are collected and the cache is
+ *       cleared. Dumps them (OUT/particles.bin), their count per step and
+ *       the inflow remainders.
  *   ROLES is "-" or a comma list tag:role with role in
  *       none,interface,inlet,outlet,wall.
  */
@@ -567,6 +573,35 @@ int cmdCollide(int argc, char** argv)
     return ok ? 0 : 1;
 }
 
+int cmdInject(int argc, char** argv)
+{
+    if (argc < 6) return 2;
+    Rig r;
+    if (!buildRig(r, argv[2], argv[3], "-")) return 1;
+    const std::string out = argv[4];
+    const int nsteps = std::atoi(argv[5]);
+    const unsigned seed = (unsigned)std::strtoul(argv[6], nullptr, 10);
+    r.partinit->thread_rng().seed(seed);
+    std::srand(seed);
+    ProcessDSMC& p = *r.process;
+    Particles Q;
+    std::vector<long long> perStep((std::size_t)nsteps, 0);
+    for (int k = 1; k <= nsteps; ++k) {
+        p.preprocesseffquad(k);
+        perStep[(std::size_t)(k - 1)] = (long long)p.recv_cache.size();
+        for (const particle& q : p.recv_cache) {
+            Q.px.push_back(q.p_location[0]); Q.py.push_back(q.p_location[1]); Q.pz.push_back(q.p_location[2]);
+            Q.vx.push_back(q.p_velocity[0]); Q.vy.push_back(q.p_velocity[1]); Q.vz.push_back(q.p_velocity[2]);
+            Q.ir.push_back(q.p_Ir); Q.dt.push_back(q.dt_left); Q.cell.push_back(q.p_mesh_serial);
+        }
+        p.recv_cache.clear();
+    }
+    bool ok = writeParticles(out + "/particles.bin", Q);
+    ok = ok && writeFile(out + "/steps.bin", perStep.data(), perStep.size() * 8);
+    ok = ok && writeFile(out + "/reminj.bin", r.partinit->remainderinpre.data(), r.partinit->remainderinpre.size() * 8);
+    return ok ? 0 : 1;
+}
+
 int cmdFluent(int argc, char** argv)
 {
     if (argc < 6) return 2;
@@ -610,6 +645,7 @@ int main(int argc, char** argv)
     if (cmd == "fluent") return cmdFluent(argc, argv);
     if (cmd == "sample") return cmdSample(argc, argv);
     if (cmd == "collide") return cmdCollide(argc, argv);
+    if (cmd == "inject") return cmdInject(argc, argv);
     std::fprintf(stderr, "unknown command %s\n", cmd.c_str());
     return 2;
 }

@@ -54,6 +54,9 @@ outputs:
                  sets (block hexahedra and capsule tets): the NTC remainders,
                  candidate pairs, collisions, how many cells raised crmax,
                  and the largest per-cell momentum and energy changes
+  inject_pin.npz the reference's injection on an empty 1/4 block mesh for
+                 40 steps: particles kept per step and per cell, the inflow
+                 remainders, and 6,000 of the kept particles (float32)
   macro_band.npz per-cell mean and seed-to-seed spread of the time-averaged
                  stress and heat-flux fields (writeAveragedMacro's
                  definitions) over the same 8 reference runs as stats_band,
@@ -366,6 +369,25 @@ def gen_collide(d):
     np.savez_compressed(os.path.join(HERE, "collide_pin.npz"), **res)
 
 
+INJECT_STEPS = 40
+INJECT_SEED = 5
+INJECT_SAMPLE = 6000
+
+
+def gen_inject(d):
+    raw, dm = I.block_mesh()
+    cas = os.path.join(d, "b4i.cas")
+    M.write_cas(cas, raw)
+    mess = I.block_mess(dm, STATS_PPC)
+    r = H.inject(cas, mess, INJECT_STEPS, INJECT_SEED)
+    sub = np.sort(np.random.RandomState(2).permutation(len(r["cell"]))[:INJECT_SAMPLE])
+    np.savez_compressed(os.path.join(HERE, "inject_pin.npz"), steps=INJECT_STEPS, seed=INJECT_SEED,
+                        per_step=r["per_step"].astype(np.int32), reminj=r["reminj"],
+                        cell_count=np.bincount(r["cell"], minlength=dm.ncell).astype(np.int32),
+                        x=r["x"][sub].astype(np.float32), v=r["v"][sub].astype(np.float32),
+                        ir=r["ir"][sub].astype(np.float32))
+
+
 DEGEN_CELLS = 20
 DEGEN_TET_CELLS = 12
 DEGEN_SEED = 9
@@ -447,9 +469,10 @@ def main():
     if not H.available():
         raise SystemExit("oracle/_ref/ref_harness missing: make -C oracle ref")
     want = set(sys.argv[1:])
-    if want - {"gsis", "fill", "fluent", "pyramid", "prism", "band", "degenerate", "sample", "collide", "core"}:
+    if want - {"gsis", "fill", "fluent", "pyramid", "prism", "band", "degenerate", "sample", "collide", "inject",
+               "core"}:
         raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent, pyramid, "
-                         "prism, band, degenerate, sample, collide")
+                         "prism, band, degenerate, sample, collide, inject")
     with tempfile.TemporaryDirectory() as d:
         if not want or want & {"gsis", "fill"}:
             gen_gsis_fill(d)
@@ -467,6 +490,8 @@ def main():
             gen_sample(d)
         if not want or "collide" in want:
             gen_collide(d)
+        if not want or "inject" in want:
+            gen_inject(d)
         if not want or "core" in want:
             gen_core(d)
     print("fixtures written to", HERE)

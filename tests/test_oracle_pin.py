@@ -4,6 +4,7 @@ the reference's own code (tests/golden/, made by gen_golden.py from
 oracle/_ref/ref_harness) and against published Philox known answers."""
 import numpy as np
 import pytest
+from scipy import stats
 
 import inputs as I
 from conftest import OracleParams, golden
@@ -305,6 +306,39 @@ def test_oracle_ntc_pairs_bit_exact_vs_reference(oracle_lib):
         assert float(g[f"{k}_dmom"]) < 1e-13 and float(g[f"{k}_den"]) < 1e-13
         assert (np.bincount(parts[3], minlength=dm.ncell) <= 1).sum() > 10      # empty and single cells too
     assert int(g["tets_pairs"]) > 500000
+
+
+def test_oracle_injection_follows_the_reference(block, oracle_lib):
+    """preprocesseffquad (src/ProcessDSMC.cpp:2416-2570) on an empty domain
+    for 40 steps: the inflow remainders are bit-exact; the particles that
+    stay in the domain after their r dt trace are as many (within 4
+    binomial sigma of the share lost), spread over the inlet cells alike
+    (chi-squared), and their positions, velocities and Ir have the same
+    distributions (KS)."""
+    raw, dm, mess = block
+    g = golden("inject_pin.npz")
+    o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir(), seed=int(g["seed"])))
+    empty = np.zeros((0, 3))
+    xs, vs, irs, cs = [], [], [], []
+    for k in range(1, int(g["steps"]) + 1):
+        o.set_particles(empty, empty, np.zeros(0), np.zeros(0, np.int32))
+        o.step(k, 0x1 | 0x4)                        # inject, then merge into the cells
+        x, v, ir, c = o.particles()
+        xs.append(x); vs.append(v); irs.append(ir); cs.append(c)
+    x, v, ir, c = (np.concatenate(a) for a in (xs, vs, irs, cs))
+    _, _, rem = o.cell_state()
+    assert np.array_equal(rem, g["reminj"])
+    emitted = o.counters()["injected"]
+    kept_ref = int(g["per_step"].sum())
+    q = 1.0 - kept_ref / emitted
+    assert abs(len(c) - kept_ref) < 4 * np.sqrt(emitted * q * (1 - q)) + 4
+    cnt = np.bincount(c, minlength=dm.ncell)
+    inlet = (cnt + g["cell_count"]) > 0
+    assert stats.chi2_contingency(np.stack([cnt[inlet], g["cell_count"][inlet]])).pvalue > 1e-3
+    for k in range(3):
+        assert stats.ks_2samp(x[:, k], g["x"][:, k]).pvalue > 1e-3, ("x", k)
+        assert stats.ks_2samp(v[:, k], g["v"][:, k]).pvalue > 1e-3, ("v", k)
+    assert stats.ks_2samp(ir, g["ir"]).pvalue > 1e-3
 
 
 def test_oracle_tet_trace_bit_exact_vs_reference(oracle_lib):
