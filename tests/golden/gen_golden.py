@@ -57,6 +57,10 @@ outputs:
   inject_pin.npz the reference's injection on an empty 1/4 block mesh for
                  40 steps: particles kept per step and per cell, the inflow
                  remainders, and 6,000 of the kept particles (float32)
+  wall_pin.npz   particles traced near the block's wall (wall_trace_inputs):
+                 the reference's first non-interface face of each, and the
+                 final velocity (float32) of those whose first hit is the
+                 wall, after its diffuse re-emission
   macro_band.npz per-cell mean and seed-to-seed spread of the time-averaged
                  stress and heat-flux fields (writeAveragedMacro's
                  definitions) over the same 8 reference runs as stats_band,
@@ -388,6 +392,24 @@ def gen_inject(d):
                         ir=r["ir"][sub].astype(np.float32))
 
 
+WALL_N = 20000
+WALL_SEED = 12
+
+
+def gen_wall(d):
+    raw, dm = I.block_mesh()
+    cas = os.path.join(d, "b4w.cas")
+    M.write_cas(cas, raw)
+    mess = I.block_mess(dm, STATS_PPC)
+    x, v, dt, c = I.wall_trace_inputs(dm, mess, WALL_N, WALL_SEED)
+    first = H.trace(cas, mess, x, v, dt, c, True)
+    full = H.trace(cas, mess, x, v, dt, c, False)
+    hit = np.nonzero((first["face"] >= 0) & (dm.edges["faceTag"][np.maximum(first["face"], 0)] == 6))[0]
+    np.savez_compressed(os.path.join(HERE, "wall_pin.npz"), n=WALL_N, seed=WALL_SEED,
+                        first_face=first["face"].astype(np.int32), hit=hit.astype(np.int32),
+                        v=full["v"][hit].astype(np.float32))
+
+
 DEGEN_CELLS = 20
 DEGEN_TET_CELLS = 12
 DEGEN_SEED = 9
@@ -470,9 +492,9 @@ def main():
         raise SystemExit("oracle/_ref/ref_harness missing: make -C oracle ref")
     want = set(sys.argv[1:])
     if want - {"gsis", "fill", "fluent", "pyramid", "prism", "band", "degenerate", "sample", "collide", "inject",
-               "core"}:
+               "wall", "core"}:
         raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent, pyramid, "
-                         "prism, band, degenerate, sample, collide, inject")
+                         "prism, band, degenerate, sample, collide, inject, wall")
     with tempfile.TemporaryDirectory() as d:
         if not want or want & {"gsis", "fill"}:
             gen_gsis_fill(d)
@@ -492,6 +514,8 @@ def main():
             gen_collide(d)
         if not want or "inject" in want:
             gen_inject(d)
+        if not want or "wall" in want:
+            gen_wall(d)
         if not want or "core" in want:
             gen_core(d)
     print("fixtures written to", HERE)

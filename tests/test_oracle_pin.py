@@ -341,6 +341,35 @@ def test_oracle_injection_follows_the_reference(block, oracle_lib):
     assert stats.ks_2samp(ir, g["ir"]).pvalue > 1e-3
 
 
+def test_oracle_diffuse_wall_follows_the_reference(block, oracle_lib):
+    """Diffuse re-emission at the wall (CrossboundarySwitch's wall branch,
+    src/ProcessDSMC.cpp:1702-1829): the paths up to the first wall hit are
+    bit-exact (the first non-interface face of every particle is the
+    reference's); the velocities after the hit follow the reference's
+    (KS on the normal component, the speed and each component), with the
+    flux-weighted Maxwellian's mean normal speed sqrt(Tw / 2) sqrt(pi / 2)."""
+    raw, dm, mess = block
+    g = golden("wall_pin.npz")
+    x, v, dt, c = I.wall_trace_inputs(dm, mess, int(g["n"]), int(g["seed"]))
+    o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir(), seed=3))
+    first = o.trace(x, v, dt, c, stop_at_wall=True)
+    assert np.array_equal(first["face"], g["first_face"])
+    hit = g["hit"]
+    assert len(hit) > 3000
+    full = o.trace(x, v, dt, c, stop_at_wall=False)
+    nrm = dm.edges["edgeNormal"][g["first_face"][hit]]
+    nrm = nrm / np.linalg.norm(nrm, axis=1)[:, None]
+    mine, ref = full["v"][hit], g["v"].astype(float)
+    vn_m, vn_r = -(mine * nrm).sum(1), -(ref * nrm).sum(1)
+    assert stats.ks_2samp(vn_m, vn_r).pvalue > 1e-3
+    assert stats.ks_2samp(np.linalg.norm(mine, axis=1), np.linalg.norm(ref, axis=1)).pvalue > 1e-3
+    for k in range(3):
+        assert stats.ks_2samp(mine[:, k], ref[:, k]).pvalue > 1e-3
+    want = np.sqrt(float(mess["Twall_ref"]) / 2) * np.sqrt(np.pi / 2)
+    for vn in (vn_m, vn_r):
+        assert abs(vn.mean() / want - 1) < 0.03
+
+
 def test_oracle_tet_trace_bit_exact_vs_reference(oracle_lib):
     g = golden("tet_trace_pin.npz")
     raw, dm, mess = I.capsule_small()
