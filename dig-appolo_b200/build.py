@@ -23,7 +23,7 @@ OBJ_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(LIB_DIR, "libdsmcgpu.so")
 
 SOURCES = ["dsmc_kernels.cu", "dsmc_engine.cu", "dsmc_noalloc.cu", "dsmc_gsis.cu", "dsmc_meshio.cpp"]
-HEADERS = ["dsmc_device.cuh", "dsmc_kernels.cuh", "dsmc_macro.cuh"]
+HEADERS = ["dsmc_device.cuh", "dsmc_kernels.cuh", "dsmc_macro.cuh", "dsmc_hostpack.h"]
 
 
 def nvcc() -> str:

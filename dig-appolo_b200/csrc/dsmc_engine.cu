@@ -5,6 +5,7 @@
 #include "dsmc_gpu.h"
 #include "dsmc_meshio.h"
 #include "dsmc_kernels.cuh"
+#include "dsmc_hostpack.h"
 
 #include <algorithm>
 #include <cmath>
@@ -1248,18 +1249,12 @@ struct Engine {
     {
         if (n < 0) return fail("negative particle count");
         if (n > 0 && (!px || !py || !pz || !vx || !vy || !vz || !ir || !cell)) return fail("null particle array");
-        for (int64_t i = 0; i < n; ++i)
-            if (cell[i] < 0 || cell[i] >= ncell) return fail("particle cell id out of range");
+        const int nthreads = hostpack::threads_for(n);
+        if (!hostpack::cells_in_range(n, cell, ncell, nthreads)) return fail("particle cell id out of range");
         // order: cell-major, input order within a cell
-        std::vector<int> cnt((size_t)ncell + 1, 0);
-        for (int64_t i = 0; i < n; ++i) cnt[(size_t)cell[i] + 1]++;
-        for (int c = 0; c < ncell; ++c) cnt[(size_t)c + 1] += cnt[(size_t)c];
-        std::vector<int> st(cnt.begin(), cnt.end());
-        std::vector<int64_t> order((size_t)n);
-        {
-            std::vector<int> fill(cnt.begin(), cnt.end() - 1);
-            for (int64_t i = 0; i < n; ++i) order[(size_t)fill[(size_t)cell[i]]++] = i;
-        }
+        std::vector<int> st;
+        std::vector<int64_t> order;
+        hostpack::order_by_cell(n, cell, ncell, nthreads, st, order);
         int64_t need = params.capacity > 0 ? params.capacity : std::max<int64_t>(n + n / 2 + (1 << 16), 1 << 20);
         if (n > need) return fail("more particles than the configured capacity");
         haveParticles = false;
@@ -1268,24 +1263,18 @@ struct Engine {
         const double* src[7] = {px, py, pz, vx, vy, vz, ir};
         std::vector<char> hb((size_t)n * 8);
         for (int k = 0; k < 7; ++k) {
-            if (mixed) {
-                float* f = reinterpret_cast<float*>(hb.data());
-                for (int64_t j = 0; j < n; ++j) {
-                    const int64_t i = order[(size_t)j];
-                    double v = src[k][i];
-                    if (k < 3) v = v - cellCenterHost[(size_t)cell[i] * 3 + k];
-                    f[j] = (float)v;
-                }
-            } else {
-                double* d = reinterpret_cast<double*>(hb.data());
-                for (int64_t j = 0; j < n; ++j) d[j] = src[k][order[(size_t)j]];
-            }
+            if (mixed)
+                hostpack::gather_convert<float>(n, order.data(), src[k], cell, k < 3 ? cellCenterHost.data() : nullptr, k,
+                                                reinterpret_cast<float*>(hb.data()), nthreads);
+            else
+                hostpack::gather_convert<double>(n, order.data(), src[k], cell, nullptr, k,
+                                                 reinterpret_cast<double*>(hb.data()), nthreads);
             if (n > 0 && (!cuda(cudaMemcpyAsync(buf[cur][k], hb.data(), (size_t)n * realSize(), cudaMemcpyHostToDevice, stream), "upload particles") ||
                           !cuda(cudaStreamSynchronize(stream), "sync")))
                 return false;
         }
         std::vector<int> hc((size_t)n);
-        for (int64_t j = 0; j < n; ++j) hc[(size_t)j] = cell[order[(size_t)j]];
+        hostpack::gather_cells(n, order.data(), cell, hc.data(), nthreads);
         if (n > 0 && !cuda(cudaMemcpyAsync(buf[cur][7], hc.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, stream), "upload cells"))
             return false;
         if (!cuda(cudaMemcpyAsync(start[cur], st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice, stream), "upload start"))
@@ -1520,15 +1509,17 @@ struct Engine {
         double* dst[7] = {px, py, pz, vx, vy, vz, ir};
         const bool mixed = precision == DSMC_PRECISION_MIXED;
         std::vector<char> hb((size_t)n * 8);
+        const int nthreads = hostpack::threads_for(n);
         for (int k = 0; k < 7; ++k) {
             if (!dst[k] || n == 0) continue;
             if (!cuda(cudaMemcpy(hb.data(), buf[cur][k], (size_t)n * realSize(), cudaMemcpyDeviceToHost), "particles"))
                 return false;
-            for (int64_t j = 0; j < n; ++j) {
-                double v = mixed ? (double)reinterpret_cast<float*>(hb.data())[j] : reinterpret_cast<double*>(hb.data())[j];
-                if (mixed && k < 3) v = cellCenterHost[(size_t)hc[(size_t)j] * 3 + k] + v;
-                dst[k][j] = v;
-            }
+            if (mixed)
+                hostpack::widen<float>(n, reinterpret_cast<const float*>(hb.data()), hc.data(),
+                                       k < 3 ? cellCenterHost.data() : nullptr, k, dst[k], nthreads);
+            else
+                hostpack::widen<double>(n, reinterpret_cast<const double*>(hb.data()), hc.data(), nullptr, k, dst[k],
+                                        nthreads);
         }
         if (cellOut) std::memcpy(cellOut, hc.data(), (size_t)n * sizeof(int));
         if (pid) for (int64_t j = 0; j < n; ++j) pid[j] = (uint32_t)j;

@@ -39,6 +39,22 @@ def _compile(out_dir):
     return exe
 
 
+def test_hostpack_matches_the_serial_loops(tmp_path):
+    """The threaded host loops of the particle upload and download
+    (csrc/dsmc_hostpack.h) against serial restatements, every thread count,
+    edge cases included (tests/cpp/hostpack_test.cpp)."""
+    if not shutil.which("g++"):
+        pytest.skip("no g++")
+    exe = os.path.join(str(tmp_path), "hostpack_test")
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", "-pthread",
+           "-I", os.path.join(ROOT, "dig-appolo_b200", "csrc"),
+           os.path.join(ROOT, "tests", "cpp", "hostpack_test.cpp"), "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+
+
 def test_host_layer_compiles_and_links(tmp_path):
     if not shutil.which("g++"):
         pytest.skip("no g++")
