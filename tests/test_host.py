@@ -1,9 +1,10 @@
-"""Host-side logic: synthetic meshes, the CAS format, case constants and the
-seeded workloads (CPU only)."""
+"""Host-side logic: synthetic meshes, the CAS format, case constants, the
+seeded workloads and the Python binding's argument handling (CPU only)."""
 import os
 import tempfile
 
 import numpy as np
+import pytest
 
 import inputs as I
 from pydsmc import case as C
@@ -102,3 +103,45 @@ def test_bench_reads_and_scales_profile_traffic(tmp_path, monkeypatch):
     assert b == 7000.0 and src == os.path.join("profiles", "move_kernel_meshA_ppc100.md")
     assert bench.measured_traffic("move_kernel", "meshB_ppc100", 2500.0) == (None, None)
     assert bench.measured_traffic("collide_kernel", "meshA_ppc100", 2500.0) == (None, None)
+
+
+def test_upload_columns_passes_what_upload_particles_passes():
+    """pydsmc.gpu.Case.upload_columns (the bench's end-to-end upload) hands
+    dsmc_upload_particles the same count and data as upload_particles, passes
+    contiguous float64 columns without copying them, and refuses columns of
+    unequal length; checked against a stand-in for the library."""
+    import ctypes as C
+    from pydsmc import gpu
+
+    calls = []
+
+    class FakeLib:
+        def dsmc_upload_particles(self, h, n, *ptrs):
+            cols = [np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(n,)).copy() for p in ptrs[:7]]
+            cell = np.ctypeslib.as_array(C.cast(ptrs[7], C.POINTER(C.c_int32)), shape=(n,)).copy()
+            calls.append({"h": h, "n": n, "cols": cols, "cell": cell, "addr": [p.value for p in ptrs]})
+            return 0
+
+        def dsmc_destroy(self, h):
+            pass
+
+    case = gpu.Case.__new__(gpu.Case)
+    case.lib, case.h = FakeLib(), 7
+    rs = np.random.RandomState(0)
+    n = 1000
+    x, v = rs.standard_normal((n, 3)), rs.standard_normal((n, 3))
+    ir, cell = rs.random_sample(n), rs.randint(0, 50, n).astype(np.int32)
+    case.upload_particles(x, v, ir, cell)
+    cols = [np.ascontiguousarray(x[:, k]) for k in range(3)] + [np.ascontiguousarray(v[:, k]) for k in range(3)]
+    case.upload_columns(*cols, ir, cell)
+    case.upload_columns(*(x[:, k] for k in range(3)), *(v[:, k] for k in range(3)), ir, cell)   # strided views
+    a = calls[0]
+    for b in calls[1:]:
+        assert b["h"] == 7 and b["n"] == n
+        assert all(np.array_equal(p, q) for p, q in zip(a["cols"], b["cols"]))
+        assert np.array_equal(a["cell"], b["cell"])
+    assert calls[1]["addr"] == [c.ctypes.data for c in cols] + [ir.ctypes.data, cell.ctypes.data]
+    with pytest.raises(ValueError):
+        case.upload_columns(*cols, ir[:-1], cell)
+    assert len(calls) == 3
+    case.h = None
