@@ -1761,6 +1761,22 @@ int dsmc_upload_cell_state(DsmcHandle* h, const double* crmax, const double* rem
     return status_of(e, ok);
 }
 
+int dsmc_upload_sparse_state(DsmcHandle* h, const unsigned char* sparse_state)
+{
+    DSMC_GUARD(h);
+    dsmc::Engine& e = h->e;
+    if (!sparse_state) return DSMC_E_INVALID;
+    for (int c = 0; c < e.ncell; ++c)
+        if (sparse_state[c] > 2) {
+            e.err = "sparse state outside 0..2";
+            return DSMC_E_INVALID;
+        }
+    bool ok = e.cuda(cudaMemcpyAsync(e.sparseState, sparse_state, (size_t)e.ncell, cudaMemcpyHostToDevice, e.stream),
+                     "sparse state");
+    ok = ok && e.cuda(cudaStreamSynchronize(e.stream), "sync");
+    return status_of(e, ok);
+}
+
 int dsmc_get_counters(DsmcHandle* h, DsmcCounters* out)
 {
     DSMC_GUARD(h);

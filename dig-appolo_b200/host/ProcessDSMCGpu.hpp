@@ -216,6 +216,13 @@ public:
         check(dsmc_download_counts(h_, nullptr, nullptr, nullptr, st.data(), nullptr, nullptr), "counts");
         return st;
     }
+    // dsmc2ns_sparse_state as ProcessGSIS::DSMC2NS leaves it (1 accumulating,
+    // 2 released; src/ProcessGSIS.cpp:1660-1674), written back for the steps
+    void setSparseState(const std::vector<unsigned char>& st)
+    {
+        if ((int)st.size() != ncell_) throw DsmcError("setSparseState: one state per cell");
+        check(dsmc_upload_sparse_state(h_, st.data()), "dsmc_upload_sparse_state");
+    }
 
     // The field set out2dat writes (src/ProcessDSMC.cpp:3338-3377): record
     // up to NSS and for sparse cells (states 1, 2), final_record after.

@@ -103,6 +103,7 @@ _SIGS = [
     ("dsmc_download_wall", C.c_int, [_P, _P]),
     ("dsmc_download_cell_state", C.c_int, [_P, _P, _P, _P]),
     ("dsmc_upload_cell_state", C.c_int, [_P, _P, _P, _P]),
+    ("dsmc_upload_sparse_state", C.c_int, [_P, _P]),
     ("dsmc_get_counters", C.c_int, [_P, _P]),
     ("dsmc_trace", C.c_int, [_P, C.c_int64] + [_P] * 8 + [C.c_int32] + [_P] * 12),
     ("dsmc_trace_noalloc", C.c_int, [_P, C.c_int64] + [_P] * 8 + [C.c_int32] + [_P] * 12),
@@ -319,6 +320,14 @@ class Case:
         crmax, rem_coll, rem_inj = f(crmax), f(rem_coll), f(rem_inj)
         self._check(self.lib.dsmc_upload_cell_state(self.h, _ptr(crmax), _ptr(rem_coll), _ptr(rem_inj)),
                     "dsmc_upload_cell_state")
+
+    def set_sparse_state(self, sparse_state):
+        """Write back the per-cell sparse-sample states (0 normal, 1
+        accumulating, 2 released) the host's GSIS exchange decided."""
+        ss = np.ascontiguousarray(sparse_state, dtype=np.uint8).reshape(-1)
+        if ss.shape[0] != self.ncell:
+            raise ValueError("one sparse state per cell")
+        self._check(self.lib.dsmc_upload_sparse_state(self.h, _ptr(ss)), "dsmc_upload_sparse_state")
 
     def counters(self) -> dict:
         c = Counters()

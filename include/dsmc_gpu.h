@@ -311,6 +311,14 @@ int dsmc_download_wall(DsmcHandle* h, double* tally);
 int dsmc_download_cell_state(DsmcHandle* h, double* crmax, double* rem_coll, double* rem_inj);
 int dsmc_upload_cell_state(DsmcHandle* h, const double* crmax, const double* rem_coll, const double* rem_inj);
 
+/* Per-cell sparse-sample states [ncell] written back by the host's GSIS
+ * exchange: ProcessGSIS::DSMC2NS marks a cell accumulating (1) when its
+ * samples are too few or its cell Knudsen number is rejected, and released
+ * (2) when an accumulating cell's fields become reliable
+ * (src/ProcessGSIS.cpp:1660-1674), in the ProcessDSMC object the step then
+ * reads. Values outside 0..2 are refused and nothing is written. */
+int dsmc_upload_sparse_state(DsmcHandle* h, const unsigned char* sparse_state);
+
 int dsmc_get_counters(DsmcHandle* h, DsmcCounters* out);
 
 /* Tracing check entry (the move kernel's trace on caller-given particles,

@@ -1045,6 +1045,14 @@ void oracle_set_cell_state(OracleCase* o, const double* crmax, const double* rem
     if (rem_inj) memcpy(o->remInj, rem_inj, b);
 }
 
+int oracle_set_sparse_state(OracleCase* o, const unsigned char* sparse_state)
+{
+    for (int c = 0; c < o->ncell; ++c)
+        if (sparse_state[c] > 2) return -1;
+    memcpy(o->sparse, sparse_state, (size_t)o->ncell);
+    return 0;
+}
+
 void oracle_get_counts(const OracleCase* o, int* ppc, double* window_samples, char* window_valid,
                        unsigned char* sparse_state)
 {

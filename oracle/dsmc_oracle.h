@@ -63,6 +63,9 @@ void oracle_get_step_moments(const OracleCase* o, double* out); /* [ncell][18] *
 void oracle_get_acc(const OracleCase* o, double* out);          /* [ncell][54] */
 void oracle_get_cell_state(const OracleCase* o, double* crmax, double* rem_coll, double* rem_inj);
 void oracle_set_cell_state(OracleCase* o, const double* crmax, const double* rem_coll, const double* rem_inj);
+/* dsmc2ns_sparse_state as the host's GSIS exchange writes it back
+ * (src/ProcessGSIS.cpp:1660-1674); values outside 0..2 return -1. */
+int oracle_set_sparse_state(OracleCase* o, const unsigned char* sparse_state);
 void oracle_get_counts(const OracleCase* o, int* ppc, double* window_samples, char* window_valid,
                        unsigned char* sparse_state);
 void oracle_get_wall(const OracleCase* o, double* tally);        /* [nface][6] */

@@ -92,11 +92,12 @@ def trace_finishes(cas: str, mess, x, v, dt, cell, seconds: float) -> bool:
         return False
 
 
-def sample(cas: str, mess, x, v, ir, cell, nsteps: int, ppc: int) -> dict:
+def sample(cas: str, mess, x, v, ir, cell, nsteps: int, ppc: int, host_rule: bool = False) -> dict:
     """statistic_macroPre, then statistic_macro(k) for k = 1..nsteps on the
     particles of each step (the harness's sampledAt rule over the given
-    ones, ppc per cell in input order); the macro arrays and window state
-    after the last step."""
+    ones, ppc per cell in input order), with host_rule the harness's
+    hostRule changes of the sparse states after every exchange step; the
+    macro arrays and window state after the last step."""
     n = int(np.asarray(cell).shape[0])
     with tempfile.TemporaryDirectory() as d:
         pm, pp = os.path.join(d, "mess.bin"), os.path.join(d, "parts.bin")
@@ -104,7 +105,7 @@ def sample(cas: str, mess, x, v, ir, cell, nsteps: int, ppc: int) -> dict:
         _write_particles(pp, x, v, ir, np.zeros(n), cell)
         out = os.path.join(d, "out")
         os.makedirs(out)
-        _run(["sample", cas, pm, pp, out, nsteps, ppc])
+        _run(["sample", cas, pm, pp, out, nsteps, ppc, int(host_rule)])
         res = {k: np.fromfile(os.path.join(out, k + ".bin"), dtype=np.float64).reshape(-1, 18)
                for k in ("local", "record", "final_record")}
         res["window_samples"] = np.fromfile(os.path.join(out, "window_samples.bin"), dtype=np.float64)

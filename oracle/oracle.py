@@ -40,6 +40,8 @@ def load():
         lib.oracle_get_acc.argtypes = [_P, _P]
         lib.oracle_get_cell_state.argtypes = [_P, _P, _P, _P]
         lib.oracle_set_cell_state.argtypes = [_P, _P, _P, _P]
+        lib.oracle_set_sparse_state.restype = C.c_int
+        lib.oracle_set_sparse_state.argtypes = [_P, _P]
         lib.oracle_get_counts.argtypes = [_P, _P, _P, _P, _P]
         lib.oracle_get_wall.argtypes = [_P, _P]
         lib.oracle_counters.argtypes = [_P, _P]
@@ -164,6 +166,11 @@ class Oracle:
         out = np.empty((self.nface, 6))
         self.lib.oracle_get_wall(self.h, _p(out))
         return out
+
+    def set_sparse_state(self, sparse_state):
+        ss = np.ascontiguousarray(sparse_state, dtype=np.uint8)
+        if self.lib.oracle_set_sparse_state(self.h, _p(ss)):
+            raise ValueError("sparse state outside 0..2")
 
     def counters(self):
         out = np.zeros(8, dtype=np.uint64)

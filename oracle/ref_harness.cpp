@@ -49,12 +49,14 @@
  *       FIELDS ([ncell][18] doubles) with MESS as the case constants, into
  *       OUT/fields.dat; the zone declarations (zonemap: id, first, last) go
  *       to OUT/zones.bin (int32).
- *   sample CAS MESS PARTS OUT NSTEPS PPC
+ *   sample CAS MESS PARTS OUT NSTEPS PPC [HOSTRULE]
  *       statistic_macroPre, then for every step k = 1..NSTEPS the buckets
  *       are refilled with the step's particles (sampledAt: PARTS thinned
  *       and scaled by a rule of k, PPC particles per cell in PARTS) and the
- *       public statistic_macro(k) runs; dumps local, record, final_record,
- *       the window samples and validity and the sparse states.
+ *       public statistic_macro(k) runs; with HOSTRULE = 1 the sparse states
+ *       are then changed by hostRule after every exchange step, as the GSIS
+ *       exchange does. Dumps local, record, final_record, the window
+ *       samples and validity and the sparse states.
  *   collide CAS MESS PARTS OUT SEED
  *       Fills the buckets and runs the public collisionDSMC() once from the
  *       initial crmax and remainders (Collision_constant_initial); dumps
@@ -516,9 +518,25 @@ bool sampledAt(int k, std::size_t i, int c, int ppc)
     return true;
 }
 
+// The host rule of the "sample" command (HOSTRULE = 1), standing in for the
+// sparse-state decisions of ProcessGSIS::DSMC2NS (src/ProcessGSIS.cpp:
+// 1660-1674) after exchange step k (k % 100 == 0), j = k / 100: a normal
+// cell c with c % 7 == 3 becomes accumulating when j is odd; an
+// accumulating cell with c % 3 == 0 is released when j is even.
+unsigned char hostRule(unsigned char st, int c, int k)
+{
+    const int j = k / 100;
+    if (st == ProcessDSMC::DSMC2NS_SPARSE_NORMAL && c % 7 == 3 && j % 2 == 1)
+        return ProcessDSMC::DSMC2NS_SPARSE_ACCUMULATING;
+    if (st == ProcessDSMC::DSMC2NS_SPARSE_ACCUMULATING && c % 3 == 0 && j % 2 == 0)
+        return ProcessDSMC::DSMC2NS_SPARSE_RELEASED;
+    return st;
+}
+
 int cmdSample(int argc, char** argv)
 {
     if (argc < 8) return 2;
+    const bool rule = argc > 8 && std::atoi(argv[8]) != 0;
     Rig r;
     if (!buildRig(r, argv[2], argv[3], "-")) return 1;
     Particles P;
@@ -540,6 +558,9 @@ int cmdSample(int argc, char** argv)
         }
         fillBuckets(r, Q);
         p.statistic_macro(k);
+        if (rule && k % 100 == 0)
+            for (std::size_t c = 0; c < p.dsmc2ns_sparse_state.size(); ++c)
+                p.dsmc2ns_sparse_state[c] = hostRule(p.dsmc2ns_sparse_state[c], (int)c, k);
     }
     std::vector<double> wv(p.dsmc2ns_window_valid.begin(), p.dsmc2ns_window_valid.end());
     bool ok = writeFile(out + "/local.bin", p.local.data(), p.local.size() * 8);

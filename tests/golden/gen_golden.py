@@ -49,7 +49,9 @@ outputs:
   sample_pin.npz the reference's statistic_macro over 5,200 steps of a
                  deterministic particle sequence on the 1/8 block mesh
                  (inputs.sampled_at): local, record, final_record, window
-                 samples and validity, sparse states
+                 samples and validity, sparse states; the same with the
+                 sparse states changed after each exchange step by the
+                 harness's host rule (inputs.host_sparse_rule), "rule_" keys
   collide_pin.npz one collisionDSMC of the reference on ragged particle
                  sets (block hexahedra and capsule tets): the NTC remainders,
                  candidate pairs, collisions, how many cells raised crmax,
@@ -323,8 +325,9 @@ def gen_sample(d):
     mess = I.block_mess(dm, SAMPLE_PPC)
     x, v, ir, cell = I.fill_inputs(dm, mess, SAMPLE_PPC, SAMPLE_SEED)
     r = H.sample(cas, mess, x, v, ir, cell, SAMPLE_STEPS, SAMPLE_PPC)
+    rr = H.sample(cas, mess, x, v, ir, cell, SAMPLE_STEPS, SAMPLE_PPC, host_rule=True)
     np.savez_compressed(os.path.join(HERE, "sample_pin.npz"), ppc=SAMPLE_PPC, seed=SAMPLE_SEED, steps=SAMPLE_STEPS,
-                        **r)
+                        **r, **{"rule_" + k: a for k, a in rr.items()})
 
 
 COLLIDE_PPC = (20, 12)        # block hexahedra, capsule tets

@@ -207,6 +207,21 @@ def wall_trace_inputs(dm, mess, n: int, seed: int, wall_tag: int = 6):
     return x, v, np.full(n, float(mess["dtime"])), c
 
 
+def host_sparse_rule(states, k: int):
+    """The harness's hostRule: the sparse-state decisions the GSIS exchange
+    writes back after exchange step k (k % 100 == 0), j = k // 100: normal
+    cells c % 7 == 3 become accumulating (1) when j is odd, accumulating
+    cells c % 3 == 0 are released (2) when j is even."""
+    st = np.array(states, dtype=np.uint8)
+    c = np.arange(len(st))
+    j = k // 100
+    acc = (st == 0) & (c % 7 == 3) & (j % 2 == 1)
+    rel = (st == 1) & (c % 3 == 0) & (j % 2 == 0)
+    st[acc] = 1
+    st[rel] = 2
+    return st
+
+
 def fill_inputs(dm, mess, ppc: int, seed: int):
     """ppc particles per cell from the freestream Maxwellian."""
     rs = np.random.RandomState(seed)

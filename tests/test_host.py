@@ -145,3 +145,30 @@ def test_upload_columns_passes_what_upload_particles_passes():
         case.upload_columns(*cols, ir[:-1], cell)
     assert len(calls) == 3
     case.h = None
+
+
+def test_set_sparse_state_hands_over_one_byte_per_cell():
+    """pydsmc.gpu.Case.set_sparse_state passes dsmc_upload_sparse_state one
+    uint8 per cell, whatever integer type it is given, and refuses a wrong
+    length; checked against a stand-in for the library."""
+    import ctypes as C
+    from pydsmc import gpu
+
+    seen = []
+
+    class FakeLib:
+        def dsmc_upload_sparse_state(self, h, p):
+            seen.append(np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), shape=(5,)).copy())
+            return 0
+
+        def dsmc_destroy(self, h):
+            pass
+
+    case = gpu.Case.__new__(gpu.Case)
+    case.lib, case.h, case.ncell = FakeLib(), 3, 5
+    case.set_sparse_state([0, 1, 2, 1, 0])
+    case.set_sparse_state(np.array([2, 2, 0, 0, 1], dtype=np.int64))
+    assert [s.tolist() for s in seen] == [[0, 1, 2, 1, 0], [2, 2, 0, 0, 1]]
+    with pytest.raises(ValueError):
+        case.set_sparse_state([0, 1])
+    case.h = None

@@ -254,30 +254,36 @@ def test_oracle_sampling_bit_exact_vs_reference(oracle_lib):
     each 100-step window): the step-window average with its exponential
     weight after NSCHEME, the steady average after NSS, the GSIS window
     samples, validity and record, and the sparse-cell state machine, all
-    bit-exact with the reference's."""
+    bit-exact with the reference's; and the same when the host's GSIS
+    exchange writes accumulating and released states back after each
+    exchange step (ProcessGSIS::DSMC2NS, src/ProcessGSIS.cpp:1660-1674)."""
     from pydsmc import gpu
     g = golden("sample_pin.npz")
     raw, dm = I.block_mesh(scale=8)
     ppc = int(g["ppc"])
     mess = I.block_mess(dm, ppc)
     x, v, ir, cell = I.fill_inputs(dm, mess, ppc, int(g["seed"]))
-    o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir(), nss=5000, nscheme=2000, nevery=1,
-                                                 nrepeat=100))
-    o.macro_pre()
-    for k in range(1, int(g["steps"]) + 1):
-        keep, s = I.sampled_at(k, cell, ppc)
-        o.set_particles(x[keep], v[keep] * s, ir[keep] * (s * s), cell[keep])
-        o.step(k, 0x10)
-    for name, which in (("local", gpu.MACRO_LOCAL), ("record", gpu.MACRO_RECORD),
-                        ("final_record", gpu.MACRO_FINAL_RECORD)):
-        assert np.array_equal(o.macro(which), g[name]), name
-    cn = o.counts()
-    for k in ("window_samples", "window_valid", "sparse_state"):
-        assert np.array_equal(cn[k], g[k]), k
-    # the sequence reaches the sparse state and fills every output
-    assert (g["sparse_state"] == 1).sum() > 10 and (g["sparse_state"] == 0).sum() > 10
-    for name in ("local", "record", "final_record"):
-        assert (g[name][:, 0] > 0).all()
+    for pre in ("", "rule_"):
+        o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir(), nss=5000, nscheme=2000, nevery=1,
+                                                     nrepeat=100))
+        o.macro_pre()
+        for k in range(1, int(g["steps"]) + 1):
+            keep, s = I.sampled_at(k, cell, ppc)
+            o.set_particles(x[keep], v[keep] * s, ir[keep] * (s * s), cell[keep])
+            o.step(k, 0x10)
+            if pre and k % 100 == 0:      # the GSIS exchange's write-back (dsmc_upload_sparse_state)
+                o.set_sparse_state(I.host_sparse_rule(o.counts()["sparse_state"], k))
+        for name, which in (("local", gpu.MACRO_LOCAL), ("record", gpu.MACRO_RECORD),
+                            ("final_record", gpu.MACRO_FINAL_RECORD)):
+            assert np.array_equal(o.macro(which), g[pre + name]), pre + name
+        cn = o.counts()
+        for k in ("window_samples", "window_valid", "sparse_state"):
+            assert np.array_equal(cn[k], g[pre + k]), pre + k
+        # the sequence reaches the sparse states and fills every output
+        assert (g[pre + "sparse_state"] == 1).sum() > 10 and (g[pre + "sparse_state"] == 0).sum() > 10
+        for name in ("local", "record", "final_record"):
+            assert (g[pre + name][:, 0] > 0).all()
+    assert (g["rule_sparse_state"] == 2).sum() > 5
 
 
 def test_oracle_ntc_pairs_bit_exact_vs_reference(oracle_lib):
