@@ -12,7 +12,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
+#include <new>
 #include <numeric>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -1562,6 +1565,27 @@ static thread_local std::string g_createError;
         if ((h)->e.device >= 0) cudaSetDevice((h)->e.device);           \
     } while (0)
 
+// No C++ exception crosses the C ABI: the entry points that allocate on the
+// host are function-try-blocks ending in DSMC_CATCH(err), which turns an
+// exception into a status and a message in *err (the handle's, the batch's,
+// or the create error).
+static int host_exception(std::string* err, int code, const char* what) noexcept
+{
+    if (err) {
+        try {
+            *err = what;
+        } catch (...) {
+        }
+    }
+    return code;
+}
+
+#define DSMC_CATCH(err)                                                                              \
+    catch (const std::bad_alloc&) { return host_exception((err), DSMC_E_NOMEM, "host allocation failed"); }  \
+    catch (const std::length_error&) { return host_exception((err), DSMC_E_NOMEM, "host allocation failed"); } \
+    catch (const std::exception& ex) { return host_exception((err), DSMC_E_INVALID, ex.what()); }            \
+    catch (...) { return host_exception((err), DSMC_E_INVALID, "host exception"); }
+
 static int status_of(dsmc::Engine& e, bool ok)
 {
     if (ok) return DSMC_OK;
@@ -1603,20 +1627,19 @@ void dsmc_default_params(DsmcCaseParams* p)
 
 int dsmc_create(const DsmcMeshDesc* mesh, const DsmcMeshMessage* mess, const DsmcCaseParams* params, int device,
                 DsmcHandle** out)
-{
+try {
     if (!out) return DSMC_E_INVALID;
     *out = nullptr;
-    DsmcHandle* h = new (std::nothrow) DsmcHandle();
+    std::unique_ptr<DsmcHandle> h(new (std::nothrow) DsmcHandle());
     if (!h) return DSMC_E_NOMEM;
     if (!h->e.build(mesh, mess, params, device)) {
         g_createError = h->e.err;
-        const int st = status_of(h->e, false);
-        delete h;
-        return st;
+        return status_of(h->e, false);
     }
-    *out = h;
+    *out = h.release();
     return DSMC_OK;
 }
+DSMC_CATCH(&g_createError)
 
 void dsmc_destroy(DsmcHandle* h) { delete h; }
 
@@ -1624,10 +1647,11 @@ const char* dsmc_last_error(const DsmcHandle* h) { return h ? h->e.err.c_str() :
 
 int dsmc_upload_particles(DsmcHandle* h, int64_t n, const double* px, const double* py, const double* pz,
                           const double* vx, const double* vy, const double* vz, const double* ir, const int32_t* cell)
-{
+try {
     DSMC_GUARD(h);
     return status_of(h->e, h->e.uploadParticles(n, px, py, pz, vx, vy, vz, ir, cell));
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 int dsmc_particle_count(DsmcHandle* h, int64_t* n)
 {
@@ -1642,17 +1666,19 @@ int dsmc_particle_count(DsmcHandle* h, int64_t* n)
 
 int dsmc_download_particles(DsmcHandle* h, int64_t n, double* px, double* py, double* pz, double* vx, double* vy,
                             double* vz, double* ir, int32_t* cell, uint32_t* pid)
-{
+try {
     DSMC_GUARD(h);
     if (!h->e.haveParticles) return n == 0 ? DSMC_OK : DSMC_E_STATE;
     return status_of(h->e, h->e.downloadParticles(n, px, py, pz, vx, vy, vz, ir, cell, pid));
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 int dsmc_step(DsmcHandle* h, int32_t istep, uint32_t stages)
-{
+try {
     DSMC_GUARD(h);
     return status_of(h->e, h->e.step(istep, stages));
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 int dsmc_preprocesseffquad(DsmcHandle* h, int32_t istep) { return dsmc_step(h, istep, DSMC_STAGE_INJECT); }
 int dsmc_advection(DsmcHandle* h, int32_t istep) { return dsmc_step(h, istep, DSMC_STAGE_MOVE); }
@@ -1682,7 +1708,7 @@ int dsmc_download_macro(DsmcHandle* h, int32_t which, double* out)
 
 int dsmc_download_counts(DsmcHandle* h, int32_t* ppc, double* window_samples, char* window_valid,
                          unsigned char* sparse_state, double* stepinter_rho, double* steady_rho)
-{
+try {
     DSMC_GUARD(h);
     dsmc::Engine& e = h->e;
     const size_t nc = (size_t)e.ncell;
@@ -1706,6 +1732,7 @@ int dsmc_download_counts(DsmcHandle* h, int32_t* ppc, double* window_samples, ch
     ok = ok && e.cuda(cudaStreamSynchronize(e.stream), "sync");
     return status_of(e, ok);
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 int dsmc_download_step_moments(DsmcHandle* h, double* out)
 {
@@ -1718,7 +1745,7 @@ int dsmc_download_step_moments(DsmcHandle* h, double* out)
 }
 
 int dsmc_download_wall(DsmcHandle* h, double* tally)
-{
+try {
     DSMC_GUARD(h);
     dsmc::Engine& e = h->e;
     if (!tally) return DSMC_E_INVALID;
@@ -1734,6 +1761,7 @@ int dsmc_download_wall(DsmcHandle* h, double* tally)
     }
     return DSMC_OK;
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 int dsmc_download_cell_state(DsmcHandle* h, double* crmax, double* rem_coll, double* rem_inj)
 {
@@ -1806,7 +1834,7 @@ int dsmc_trace(DsmcHandle* h, int64_t n, const double* px, const double* py, con
                int32_t* out_cell, int32_t* out_ifout, int32_t* out_face, int32_t* out_tri, int32_t* out_ncross,
                double* out_px, double* out_py, double* out_pz, double* out_vx, double* out_vy, double* out_vz,
                double* out_dt)
-{
+try {
     DSMC_GUARD(h);
     dsmc::Engine& e = h->e;
     if (n < 0 || n > 0x7fffffff) return DSMC_E_INVALID;
@@ -1816,14 +1844,29 @@ int dsmc_trace(DsmcHandle* h, int64_t n, const double* px, const double* py, con
         if (cell[i] < 0 || cell[i] >= e.ncell) { e.err = "trace: cell id out of range"; return DSMC_E_INVALID; }
     const bool mixed = e.precision == DSMC_PRECISION_MIXED;
     const size_t rs = mixed ? 4 : 8;
-    std::vector<void*> tmp;
-    auto dal = [&](size_t bytes) -> void* {
-        void* p = nullptr;
-        if (cudaMalloc(&p, std::max<size_t>(bytes, 1)) != cudaSuccess) return nullptr;
-        tmp.push_back(p);
-        return p;
-    };
-    auto cleanup = [&]() { for (void* p : tmp) cudaFree(p); };
+    // device scratch of this call: every failed allocation is recorded, and
+    // whatever was allocated is freed on every way out
+    struct DeviceTemps {
+        std::vector<void*> ptrs;
+        bool failed = false;
+        void* alloc(size_t bytes)
+        {
+            ptrs.reserve(ptrs.size() + 1);
+            void* q = nullptr;
+            if (cudaMalloc(&q, std::max<size_t>(bytes, 1)) != cudaSuccess) {
+                failed = true;
+                (void)cudaGetLastError();
+                return nullptr;
+            }
+            ptrs.push_back(q);
+            return q;
+        }
+        ~DeviceTemps()
+        {
+            for (void* q : ptrs) cudaFree(q);
+        }
+    } tmp;
+    auto dal = [&](size_t bytes) -> void* { return tmp.alloc(bytes); };
     void* dIn[6];
     void* dOut[6];
     for (int k = 0; k < 6; ++k) {
@@ -1835,8 +1878,7 @@ int dsmc_trace(DsmcHandle* h, int64_t n, const double* px, const double* py, con
     int* dCell = (int*)dal((size_t)n * 4);
     int* dI[6];
     for (int k = 0; k < 6; ++k) dI[k] = (int*)dal((size_t)n * 4);
-    for (void* p : tmp)
-        if (!p) { cleanup(); e.err = "trace: device allocation failed"; return DSMC_E_NOMEM; }
+    if (tmp.failed) { e.err = "trace: device allocation failed"; return DSMC_E_NOMEM; }
     const double* src[6] = {px, py, pz, vx, vy, vz};
     std::vector<char> hb((size_t)n * 8);
     bool ok = true;
@@ -1885,9 +1927,9 @@ int dsmc_trace(DsmcHandle* h, int64_t n, const double* px, const double* py, con
         }
     }
     if (ok && out_dt) ok = e.cuda(cudaMemcpy(out_dt, dODt, (size_t)n * 8, cudaMemcpyDeviceToHost), "trace dt out");
-    cleanup();
     return status_of(e, ok);
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 int dsmc_set_timing(DsmcHandle* h, int32_t on)
 {
@@ -1937,23 +1979,26 @@ void engine_set_error(DsmcHandle* h, const char* msg) { h->e.err = msg; }
 extern "C" {
 
 int dsmc_fill_freestream(DsmcHandle* h, double ppc_mean, uint64_t seed)
-{
+try {
     DSMC_GUARD(h);
     return status_of(h->e, h->e.fill(ppc_mean, seed, false));
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 int dsmc_fill_initial(DsmcHandle* h, double ppc_mean, uint64_t seed)
-{
+try {
     DSMC_GUARD(h);
     return status_of(h->e, h->e.fill(ppc_mean, seed, true));
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 int dsmc_molecular_velocity_change(DsmcHandle* h, const double* nsresult, const char* accepted,
                                    DsmcGsisReport* report)
-{
+try {
     DSMC_GUARD(h);
     return status_of(h->e, h->e.gsisUpdate(nsresult, accepted, report));
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 // ---------------------------------------------------------------------------
 // launch shapes and the autotuner
@@ -1967,15 +2012,16 @@ int dsmc_get_launch_shape(DsmcHandle* h, DsmcLaunchShape* out)
 }
 
 int dsmc_set_launch_shape(DsmcHandle* h, const DsmcLaunchShape* shape)
-{
+try {
     DSMC_GUARD(h);
     if (!shape) return DSMC_E_INVALID;
     return h->e.setShape(*shape) ? DSMC_OK : DSMC_E_INVALID;
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 int dsmc_autotune(DsmcHandle* h, int32_t first_istep, int32_t trial_steps, int32_t* next_istep,
                   DsmcLaunchShape* chosen)
-{
+try {
     DSMC_GUARD(h);
     int istep = first_istep;
     const bool ok = h->e.autotune(istep, trial_steps);
@@ -1983,6 +2029,7 @@ int dsmc_autotune(DsmcHandle* h, int32_t first_istep, int32_t trial_steps, int32
     if (chosen) *chosen = h->e.getShape();
     return status_of(h->e, ok);
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 // ---------------------------------------------------------------------------
 // batched steps
@@ -2092,7 +2139,7 @@ struct DsmcBatch {
 };
 
 int dsmc_batch_create(DsmcHandle* const* cases, int32_t n, DsmcBatch** out)
-{
+try {
     if (!out) return DSMC_E_INVALID;
     *out = nullptr;
     if (!cases || n < 1) {
@@ -2114,7 +2161,7 @@ int dsmc_batch_create(DsmcHandle* const* cases, int32_t n, DsmcBatch** out)
                 return DSMC_E_INVALID;
             }
     }
-    DsmcBatch* b = new (std::nothrow) DsmcBatch();
+    std::unique_ptr<DsmcBatch> b(new (std::nothrow) DsmcBatch());
     if (!b) return DSMC_E_NOMEM;
     b->cases.assign(cases, cases + n);
     b->device = cases[0]->e.device;
@@ -2127,23 +2174,24 @@ int dsmc_batch_create(DsmcHandle* const* cases, int32_t n, DsmcBatch** out)
         ok = b->cuda(cudaEventCreateWithFlags(&b->join[(size_t)k], cudaEventDisableTiming), "batch event");
     if (!ok) {
         g_createError = b->err;
-        delete b;
         return DSMC_E_CUDA;
     }
-    *out = b;
+    *out = b.release();
     return DSMC_OK;
 }
+DSMC_CATCH(&g_createError)
 
 void dsmc_batch_destroy(DsmcBatch* b) { delete b; }
 
 const char* dsmc_batch_last_error(const DsmcBatch* b) { return b ? b->err.c_str() : g_createError.c_str(); }
 
 int dsmc_batch_step(DsmcBatch* b, int32_t nsteps)
-{
+try {
     if (!b) return DSMC_E_INVALID;
     cudaSetDevice(b->device);
     return b->step(nsteps) ? DSMC_OK : DSMC_E_STATE;
 }
+DSMC_CATCH(b ? &b->err : nullptr)
 
 void* dsmc_batch_stream(DsmcBatch* b) { return b ? (void*)b->stream : nullptr; }
 
@@ -2162,7 +2210,7 @@ int dsmc_batch_sync(DsmcBatch* b)
 // field output (ProcessDSMC::out2dat, outBoundaryStressHeat)
 // ---------------------------------------------------------------------------
 int dsmc_out2dat(DsmcHandle* h, int32_t istep, const DsmcZone* zones, int32_t nzones, const char* path)
-{
+try {
     DSMC_GUARD(h);
     dsmc::Engine& e = h->e;
     const size_t nc = (size_t)e.ncell;
@@ -2183,10 +2231,11 @@ int dsmc_out2dat(DsmcHandle* h, int32_t istep, const DsmcZone* zones, int32_t nz
     if (st != DSMC_OK) e.err = dsmc_meshio_last_error();
     return st;
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 int dsmc_out_boundary_stress_heat(DsmcHandle* h, int32_t istep, const DsmcZone* zones, int32_t nzones,
                                   const char* path)
-{
+try {
     DSMC_GUARD(h);
     dsmc::Engine& e = h->e;
     // EnableBoundaryStressHeatStatistic off: nothing to write
@@ -2199,5 +2248,6 @@ int dsmc_out_boundary_stress_heat(DsmcHandle* h, int32_t istep, const DsmcZone* 
     if (st != DSMC_OK) e.err = dsmc_meshio_last_error();
     return st;
 }
+DSMC_CATCH(h ? &h->e.err : nullptr)
 
 }  // extern "C"

@@ -13,6 +13,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <new>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -36,6 +38,30 @@ int failWith(const std::string& m, int code = DSMC_E_INVALID)
     g_err = m;
     return code;
 }
+
+// No C++ exception crosses the C ABI: the entry points that allocate are
+// function-try-blocks ending in DSMC_MESHIO_CATCH.
+int failNoexcept(const char* m, int code) noexcept
+{
+    try {
+        g_err = m;
+    } catch (...) {
+    }
+    return code;
+}
+
+#define DSMC_MESHIO_CATCH                                                                            \
+    catch (const std::bad_alloc&) { return failNoexcept("host allocation failed", DSMC_E_NOMEM); }  \
+    catch (const std::length_error&) { return failNoexcept("host allocation failed", DSMC_E_NOMEM); } \
+    catch (const std::exception& ex) { return failNoexcept(ex.what(), DSMC_E_INVALID); }            \
+    catch (...) { return failNoexcept("host exception", DSMC_E_INVALID); }
+
+struct FileCloser {
+    void operator()(FILE* f) const
+    {
+        if (f) std::fclose(f);
+    }
+};
 
 // ---------------------------------------------------------------------------
 // lexing
@@ -503,17 +529,17 @@ extern "C" {
 const char* dsmc_meshio_last_error(void) { return g_err.c_str(); }
 
 int dsmc_mesh_read_cas(const char* path, DsmcMeshFile** out)
-{
+try {
     if (!out) return failWith("null output");
     *out = nullptr;
     if (!path) return failWith("null path");
-    FILE* f = std::fopen(path, "rb");
+    std::unique_ptr<FILE, FileCloser> f(std::fopen(path, "rb"));
     if (!f) return failWith(std::string("cannot open ") + path + ": " + std::strerror(errno));
     std::vector<char> buf;
     char chunk[1 << 16];
     size_t n;
-    while ((n = std::fread(chunk, 1, sizeof chunk, f)) > 0) buf.insert(buf.end(), chunk, chunk + n);
-    std::fclose(f);
+    while ((n = std::fread(chunk, 1, sizeof chunk, f.get())) > 0) buf.insert(buf.end(), chunk, chunk + n);
+    f.reset();
     Raw r;
     std::string err;
     if (!parseCas(buf.data(), buf.data() + buf.size(), r, err)) return failWith(std::string(path) + ": " + err);
@@ -522,6 +548,7 @@ int dsmc_mesh_read_cas(const char* path, DsmcMeshFile** out)
     *out = m.release();
     return DSMC_OK;
 }
+DSMC_MESHIO_CATCH
 
 void dsmc_mesh_free(DsmcMeshFile* m) { delete m; }
 
@@ -558,7 +585,7 @@ int dsmc_mesh_get_stats(const DsmcMeshFile* m, double* area_sum, double* min_edg
 
 int dsmc_mesh_message(const DsmcMeshFile* m, double Ma, double Kn, int32_t ppc, double L0, double T_in, double T_wall,
                       double cfl, double cfl_ns, DsmcMeshMessage* out)
-{
+try {
     if (!m || !out) return failWith("null argument");
     if (!(Kn > 0.0) || !(L0 > 0.0) || !(T_in > 0.0) || ppc <= 0) return failWith("Kn, L0, T_in and ppc must be positive");
     DsmcMeshMessage g{};
@@ -634,10 +661,11 @@ int dsmc_mesh_message(const DsmcMeshFile* m, double Ma, double Kn, int32_t ppc, 
     *out = g;
     return DSMC_OK;
 }
+DSMC_MESHIO_CATCH
 
 int dsmc_write_fluent_cells(const char* path, const DsmcMeshMessage* mess, const DsmcZone* zones, int32_t nzones,
                             const double* w, int32_t ncell)
-{
+try {
     if (!path || !mess || !zones || !w) return failWith("null argument");
     int id = 0, first = 0, last = 0;
     if (!findCellZone(zones, nzones, id, first, last)) return failWith("no cell zone with id 2");
@@ -693,11 +721,12 @@ int dsmc_write_fluent_cells(const char* path, const DsmcMeshMessage* mess, const
     if (std::ferror(o.f)) return failWith(std::string("write error on ") + path);
     return DSMC_OK;
 }
+DSMC_MESHIO_CATCH
 
 int dsmc_write_fluent_wall(const char* path, const DsmcMeshMessage* mess, const DsmcCaseParams* params,
                            const DsmcZone* zones, int32_t nzones, const DsmcEdgeRec* edges, int32_t nface,
                            const double* tally, int32_t istep)
-{
+try {
     if (!path || !mess || !params || !edges || !tally || (nzones > 0 && !zones)) return failWith("null argument");
     if (nface <= 0) return failWith("no faces");
     const bool steady = istep > params->nss;
@@ -772,5 +801,6 @@ int dsmc_write_fluent_wall(const char* path, const DsmcMeshMessage* mess, const 
     if (std::ferror(o.f)) return failWith(std::string("write error on ") + path);
     return DSMC_OK;
 }
+DSMC_MESHIO_CATCH
 
 }  // extern "C"
