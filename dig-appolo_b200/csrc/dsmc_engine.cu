@@ -1251,6 +1251,7 @@ struct Engine {
                          const double* vy, const double* vz, const double* ir, const int32_t* cell)
     {
         if (n < 0) return fail("negative particle count");
+        if (n > (int64_t)0x7fffffff - 1) return fail("capacity above 2^31 particles");
         if (n > 0 && (!px || !py || !pz || !vx || !vy || !vz || !ir || !cell)) return fail("null particle array");
         const int nthreads = hostpack::threads_for(n);
         if (!hostpack::cells_in_range(n, cell, ncell, nthreads)) return fail("particle cell id out of range");
