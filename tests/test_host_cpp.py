@@ -55,6 +55,54 @@ def test_hostpack_matches_the_serial_loops(tmp_path):
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
 
 
+def test_host_mesh_file_reads_the_reference_arrays(tmp_path):
+    """The C++ host layer's MeshFile (readCAS + preprocess + DSMC topology
+    through dsmc_mesh_read_cas) on the CPU: the 1/8 block mesh's arrays equal
+    the reference's (tests/golden/mesh_pin.npz), the zone declarations its
+    zonemap (fluent_pin.npz) and the mesh message the pinned restatement;
+    a missing file raises DsmcError (tests/cpp/meshfile_driver.cpp)."""
+    if not shutil.which("g++"):
+        pytest.skip("no g++")
+    if not os.path.exists(os.path.join(LIB_DIR, "libdsmcgpu.so")):
+        pytest.skip("library not built")
+    import inputs as I
+    from conftest import golden
+    from pydsmc import case as CS
+    from pydsmc import mesh as M
+    from pydsmc import meshio as IO
+    exe = os.path.join(str(tmp_path), "meshfile_driver")
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror",
+           "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "dig-appolo_b200", "host"),
+           os.path.join(ROOT, "tests", "cpp", "meshfile_driver.cpp"), "-o", exe,
+           "-L", LIB_DIR, "-ldsmcgpu", f"-Wl,-rpath,{LIB_DIR}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    raw, dm = I.block_mesh(scale=8)
+    cas = str(tmp_path / "b8.cas")
+    M.write_cas(cas, raw)
+    r = subprocess.run([exe, cas, str(tmp_path), str(I.BLOCK_MA), str(I.BLOCK_KN), "20", str(I.BLOCK_L0)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
+    assert "cannot open" in r.stdout
+    g = golden("mesh_pin.npz")
+    cells = np.fromfile(tmp_path / "cells.bin", dtype=M.DSMC_CELL_DTYPE)
+    edges = np.fromfile(tmp_path / "edges.bin", dtype=M.DSMC_EDGE_DTYPE)
+    for f in M.DSMC_CELL_DTYPE.names:
+        if f != "no":
+            assert np.array_equal(cells[f], g["cells"][f]), f
+    for f in M.DSMC_EDGE_DTYPE.names:
+        assert np.array_equal(edges[f], g["edges"][f]), f
+    assert np.array_equal(np.fromfile(tmp_path / "points.bin"), g["points"])
+    assert np.array_equal(np.fromfile(tmp_path / "split.bin", dtype=np.uint8), g["split"])
+    zones = np.fromfile(tmp_path / "zones.bin", dtype=IO.ZONE_DTYPE)
+    fz = golden("fluent_pin.npz")["zones"]
+    assert [(int(z["id"]), int(z["first"]), int(z["last"])) for z in zones] == [tuple(t) for t in fz]
+    mess = np.fromfile(tmp_path / "mess.bin", dtype=CS.MESH_MESSAGE_DTYPE)[0]
+    want = CS.mesh_message(dm, I.BLOCK_MA, I.BLOCK_KN, ppc=20, L0=I.BLOCK_L0)
+    for f in CS.MESH_MESSAGE_DTYPE.names:
+        assert mess[f] == want[f], f
+
+
 def test_host_layer_compiles_and_links(tmp_path):
     if not shutil.which("g++"):
         pytest.skip("no g++")
