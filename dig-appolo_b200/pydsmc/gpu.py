@@ -129,11 +129,12 @@ def lib_path() -> str:
 
 
 def load(path: str | None = None):
-    """Load libdsmcgpu.so (raises OSError if it is not built)."""
+    """Load libdsmcgpu.so, LIB_PATH unless a path is given (raises OSError if
+    it is not built). The library of the default path is loaded once."""
     global _lib
-    if _lib is not None:
+    p = os.path.abspath(path or LIB_PATH)
+    if _lib is not None and path is None and p == os.path.abspath(LIB_PATH):
         return _lib
-    p = path or LIB_PATH
     if not os.path.exists(p):
         raise OSError(f"{p} not built: run __graft_entry__.build()")
     lib = C.CDLL(p)
@@ -141,7 +142,8 @@ def load(path: str | None = None):
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    _lib = lib
+    if path is None:
+        _lib = lib
     return lib
 
 
