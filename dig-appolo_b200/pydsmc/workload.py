@@ -106,26 +106,3 @@ def trace_particles(dm: DsmcMesh, mess, n: int, seed: int, inflow_dir, speed_fac
     v = sigma * rng.standard_normal((n, 3))
     dt = np.full(n, float(mess["dtime"]))
     return {"x": x, "v": v, "dt": dt, "cell": cells}
-
-
-def write_particles(path: str, x, v, ir, dt, cell) -> None:
-    """Particle file of the oracle harness: int64 n; px,py,pz,vx,vy,vz,Ir,dt
-    as float64 arrays; int32 cell ids."""
-    n = int(np.asarray(cell).shape[0])
-    with open(path, "wb") as f:
-        f.write(np.int64(n).tobytes())
-        for k in range(3):
-            f.write(np.ascontiguousarray(x[:, k], dtype=np.float64).tobytes())
-        for k in range(3):
-            f.write(np.ascontiguousarray(v[:, k], dtype=np.float64).tobytes())
-        f.write(np.ascontiguousarray(ir, dtype=np.float64).tobytes())
-        f.write(np.ascontiguousarray(dt, dtype=np.float64).tobytes())
-        f.write(np.ascontiguousarray(cell, dtype=np.int32).tobytes())
-
-
-def read_particles(path: str) -> dict:
-    b = np.fromfile(path, dtype=np.uint8)
-    n = int(b[:8].view(np.int64)[0])
-    d = b[8:8 + n * 64].view(np.float64).reshape(8, n)
-    cell = b[8 + n * 64:8 + n * 68].view(np.int32)
-    return {"x": d[0:3].T.copy(), "v": d[3:6].T.copy(), "ir": d[6].copy(), "dt": d[7].copy(), "cell": cell.copy()}
