@@ -58,11 +58,13 @@ outputs:
                  and the largest per-cell momentum and energy changes
   inject_pin.npz the reference's injection on an empty 1/4 block mesh for
                  40 steps: particles kept per step and per cell, the inflow
-                 remainders, and 6,000 of the kept particles (float32)
+                 remainders, and 6,000 of the kept particles (float32); the
+                 same on the capsule tets ("tet_" keys)
   wall_pin.npz   particles traced near the block's wall (wall_trace_inputs):
                  the reference's first non-interface face of each, and the
                  final velocity (float32) of those whose first hit is the
-                 wall, after its diffuse re-emission
+                 wall, after its diffuse re-emission; the same near the
+                 capsule's wall ("tet_" keys)
   macro_band.npz per-cell mean and seed-to-seed spread of the time-averaged
                  stress and heat-flux fields (writeAveragedMacro's
                  definitions) over the same 8 reference runs as stats_band,
@@ -386,13 +388,18 @@ def gen_inject(d):
     cas = os.path.join(d, "b4i.cas")
     M.write_cas(cas, raw)
     mess = I.block_mess(dm, STATS_PPC)
-    r = H.inject(cas, mess, INJECT_STEPS, INJECT_SEED)
-    sub = np.sort(np.random.RandomState(2).permutation(len(r["cell"]))[:INJECT_SAMPLE])
-    np.savez_compressed(os.path.join(HERE, "inject_pin.npz"), steps=INJECT_STEPS, seed=INJECT_SEED,
-                        per_step=r["per_step"].astype(np.int32), reminj=r["reminj"],
-                        cell_count=np.bincount(r["cell"], minlength=dm.ncell).astype(np.int32),
-                        x=r["x"][sub].astype(np.float32), v=r["v"][sub].astype(np.float32),
-                        ir=r["ir"][sub].astype(np.float32))
+    out = {}
+    rawc, dmc, messc = I.capsule_small()
+    casc = os.path.join(d, "capi.cas")
+    M.write_cas(casc, rawc)
+    for pre, path, m, ms in (("", cas, dm, mess), ("tet_", casc, dmc, messc)):
+        r = H.inject(path, ms, INJECT_STEPS, INJECT_SEED)
+        sub = np.sort(np.random.RandomState(2).permutation(len(r["cell"]))[:INJECT_SAMPLE])
+        out.update({pre + "per_step": r["per_step"].astype(np.int32), pre + "reminj": r["reminj"],
+                    pre + "cell_count": np.bincount(r["cell"], minlength=m.ncell).astype(np.int32),
+                    pre + "x": r["x"][sub].astype(np.float32), pre + "v": r["v"][sub].astype(np.float32),
+                    pre + "ir": r["ir"][sub].astype(np.float32)})
+    np.savez_compressed(os.path.join(HERE, "inject_pin.npz"), steps=INJECT_STEPS, seed=INJECT_SEED, **out)
 
 
 WALL_N = 20000
@@ -404,13 +411,18 @@ def gen_wall(d):
     cas = os.path.join(d, "b4w.cas")
     M.write_cas(cas, raw)
     mess = I.block_mess(dm, STATS_PPC)
-    x, v, dt, c = I.wall_trace_inputs(dm, mess, WALL_N, WALL_SEED)
-    first = H.trace(cas, mess, x, v, dt, c, True)
-    full = H.trace(cas, mess, x, v, dt, c, False)
-    hit = np.nonzero((first["face"] >= 0) & (dm.edges["faceTag"][np.maximum(first["face"], 0)] == 6))[0]
-    np.savez_compressed(os.path.join(HERE, "wall_pin.npz"), n=WALL_N, seed=WALL_SEED,
-                        first_face=first["face"].astype(np.int32), hit=hit.astype(np.int32),
-                        v=full["v"][hit].astype(np.float32))
+    rawc, dmc, messc = I.capsule_small()
+    casc = os.path.join(d, "capw.cas")
+    M.write_cas(casc, rawc)
+    out = {}
+    for pre, path, m, ms, tets in (("", cas, dm, mess, False), ("tet_", casc, dmc, messc, True)):
+        x, v, dt, c = I.wall_trace_inputs(m, ms, WALL_N, WALL_SEED, tets=tets)
+        first = H.trace(path, ms, x, v, dt, c, True)
+        full = H.trace(path, ms, x, v, dt, c, False)
+        hit = np.nonzero((first["face"] >= 0) & (m.edges["faceTag"][np.maximum(first["face"], 0)] == 6))[0]
+        out.update({pre + "first_face": first["face"].astype(np.int32), pre + "hit": hit.astype(np.int32),
+                    pre + "v": full["v"][hit].astype(np.float32)})
+    np.savez_compressed(os.path.join(HERE, "wall_pin.npz"), n=WALL_N, seed=WALL_SEED, **out)
 
 
 DEGEN_CELLS = 20

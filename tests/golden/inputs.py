@@ -192,15 +192,21 @@ def ragged(parts, ncell: int, ppc: int, seed: int):
     return x[keep], v[keep], ir[keep], cell[keep]
 
 
-def wall_trace_inputs(dm, mess, n: int, seed: int, wall_tag: int = 6):
-    """Uniform random points in the hexahedra that touch the wall zone,
-    isotropic velocities with mean speed 3x the freestream speed, one dt."""
+def wall_trace_inputs(dm, mess, n: int, seed: int, wall_tag: int = 6, tets: bool = False):
+    """Uniform random points in the hexahedra (or tetrahedra) that touch the
+    wall zone, isotropic velocities with mean speed 3x the freestream speed,
+    one dt."""
     e = dm.edges
     cells = np.unique(e["faceMap"][e["faceTag"] == wall_tag, 4])
     rs = np.random.RandomState(seed)
     c = rs.choice(cells, n).astype(np.int32)
-    lo, hi = cell_boxes(dm)
-    x = lo[c] + (hi[c] - lo[c]) * rs.random_sample((n, 3))
+    if tets:
+        w = -np.log(rs.random_sample((n, 4)))
+        w /= w.sum(1, keepdims=True)
+        x = np.einsum("nk,nkd->nd", w, dm.points.reshape(-1, 3)[tet_vertices(dm, c)])
+    else:
+        lo, hi = cell_boxes(dm)
+        x = lo[c] + (hi[c] - lo[c]) * rs.random_sample((n, 3))
     u, _, _ = freestream(mess)
     sigma = 3.0 * float(np.linalg.norm(u)) / math.sqrt(8.0 / math.pi)
     v = sigma * rs.standard_normal((n, 3))

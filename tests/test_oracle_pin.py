@@ -314,15 +314,19 @@ def test_oracle_ntc_pairs_bit_exact_vs_reference(oracle_lib):
     assert int(g["tets_pairs"]) > 500000
 
 
-def test_oracle_injection_follows_the_reference(block, oracle_lib):
+@pytest.mark.parametrize("pre", ["", "tet_"])
+def test_oracle_injection_follows_the_reference(block, oracle_lib, pre):
     """preprocesseffquad (src/ProcessDSMC.cpp:2416-2570) on an empty domain
-    for 40 steps: the inflow remainders are bit-exact; the particles that
-    stay in the domain after their r dt trace are as many (within 4
+    for 40 steps, through the block's quad inlet and the capsule's triangle
+    inlet at 30 degrees: the inflow remainders are bit-exact; the particles
+    that stay in the domain after their r dt trace are as many (within 4
     binomial sigma of the share lost), spread over the inlet cells alike
     (chi-squared), and their positions, velocities and Ir have the same
     distributions (KS)."""
-    raw, dm, mess = block
-    g = golden("inject_pin.npz")
+    raw, dm, mess = block if not pre else I.capsule_small()
+    g = {k[len(pre):]: a for k, a in golden("inject_pin.npz").items() if k.startswith(pre)}
+    gg = golden("inject_pin.npz")
+    g["seed"], g["steps"] = gg["seed"], gg["steps"]
     o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir(), seed=int(g["seed"])))
     empty = np.zeros((0, 3))
     xs, vs, irs, cs = [], [], [], []
@@ -347,16 +351,20 @@ def test_oracle_injection_follows_the_reference(block, oracle_lib):
     assert stats.ks_2samp(ir, g["ir"]).pvalue > 1e-3
 
 
-def test_oracle_diffuse_wall_follows_the_reference(block, oracle_lib):
+@pytest.mark.parametrize("pre", ["", "tet_"])
+def test_oracle_diffuse_wall_follows_the_reference(block, oracle_lib, pre):
     """Diffuse re-emission at the wall (CrossboundarySwitch's wall branch,
-    src/ProcessDSMC.cpp:1702-1829): the paths up to the first wall hit are
+    src/ProcessDSMC.cpp:1702-1829), at the block's quad walls and the
+    capsule's triangle walls: the paths up to the first wall hit are
     bit-exact (the first non-interface face of every particle is the
     reference's); the velocities after the hit follow the reference's
     (KS on the normal component, the speed and each component), with the
     flux-weighted Maxwellian's mean normal speed sqrt(Tw / 2) sqrt(pi / 2)."""
-    raw, dm, mess = block
-    g = golden("wall_pin.npz")
-    x, v, dt, c = I.wall_trace_inputs(dm, mess, int(g["n"]), int(g["seed"]))
+    raw, dm, mess = block if not pre else I.capsule_small()
+    gg = golden("wall_pin.npz")
+    g = {k: gg[pre + k] for k in ("first_face", "hit", "v")}
+    g["n"], g["seed"] = gg["n"], gg["seed"]
+    x, v, dt, c = I.wall_trace_inputs(dm, mess, int(g["n"]), int(g["seed"]), tets=bool(pre))
     o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir(), seed=3))
     first = o.trace(x, v, dt, c, stop_at_wall=True)
     assert np.array_equal(first["face"], g["first_face"])
