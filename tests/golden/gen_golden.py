@@ -65,6 +65,10 @@ outputs:
                  final velocity (float32) of those whose first hit is the
                  wall, after its diffuse re-emission; the same near the
                  capsule's wall ("tet_" keys)
+  stats_band_capsule.npz the same band on the capsule tets (Kn 0.01), steps
+                 61-120 of 8 seeded reference runs from 8 particles per
+                 cell: float32 mean and spread of every third cell, and
+                 the particle count of each step of each run
   macro_band.npz per-cell mean and seed-to-seed spread of the time-averaged
                  stress and heat-flux fields (writeAveragedMacro's
                  definitions) over the same 8 reference runs as stats_band,
@@ -425,6 +429,37 @@ def gen_wall(d):
     np.savez_compressed(os.path.join(HERE, "wall_pin.npz"), n=WALL_N, seed=WALL_SEED, **out)
 
 
+CAPBAND_SEEDS = [201, 202, 203, 204, 205, 206, 207, 208]
+CAPBAND_PPC = 8
+CAPBAND_STEPS = 120
+CAPBAND_AVG_FROM = 61
+CAPBAND_EVERY = 3             # cells kept in the fixture: every third
+
+
+def gen_capband(d):
+    """The statistics band on the capsule tets (Kn 0.01: collision-dominated),
+    8 seeded reference runs side by side."""
+    from concurrent.futures import ThreadPoolExecutor
+    raw, dm, mess = I.capsule_small()
+    cas = os.path.join(d, "capb.cas")
+    M.write_cas(cas, raw)
+    x, v, ir, cell = I.fill_inputs_any(dm, mess, CAPBAND_PPC, 3)
+
+    def one(seed):
+        return H.run(cas, mess, x, v, ir, cell, CAPBAND_STEPS, seed, "-", CAPBAND_AVG_FROM)
+
+    with ThreadPoolExecutor(len(CAPBAND_SEEDS)) as ex:
+        runs = list(ex.map(one, CAPBAND_SEEDS))
+    band = np.stack([I.fields_from_moments(r["moments"], CAPBAND_STEPS - CAPBAND_AVG_FROM + 1, dm, mess)
+                     for r in runs])
+    keep = np.arange(0, dm.ncell, CAPBAND_EVERY)
+    np.savez_compressed(os.path.join(HERE, "stats_band_capsule.npz"), cells=keep.astype(np.int32),
+                        mean=band.mean(0)[keep].astype(np.float32),
+                        sd=band.std(0, ddof=1)[keep].astype(np.float32), k=len(CAPBAND_SEEDS),
+                        steps=CAPBAND_STEPS, avg_from=CAPBAND_AVG_FROM, ppc=CAPBAND_PPC,
+                        nparticles=np.stack([r["steps"][:, 0] for r in runs]).astype(np.int32))
+
+
 DEGEN_CELLS = 20
 DEGEN_TET_CELLS = 12
 DEGEN_SEED = 9
@@ -507,9 +542,9 @@ def main():
         raise SystemExit("oracle/_ref/ref_harness missing: make -C oracle ref")
     want = set(sys.argv[1:])
     if want - {"gsis", "fill", "fluent", "pyramid", "prism", "band", "degenerate", "sample", "collide", "inject",
-               "wall", "core"}:
+               "wall", "capband", "core"}:
         raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent, pyramid, "
-                         "prism, band, degenerate, sample, collide, inject, wall")
+                         "prism, band, degenerate, sample, collide, inject, wall, capband")
     with tempfile.TemporaryDirectory() as d:
         if not want or want & {"gsis", "fill"}:
             gen_gsis_fill(d)
@@ -531,6 +566,8 @@ def main():
             gen_inject(d)
         if not want or "wall" in want:
             gen_wall(d)
+        if not want or "capband" in want:
+            gen_capband(d)
         if not want or "core" in want:
             gen_core(d)
     print("fixtures written to", HERE)

@@ -149,6 +149,42 @@ def test_oracle_statistics_within_reference_band(block, oracle_stats_run):
     assert np.all((np.array(counts) >= lo) & (np.array(counts) <= hi))
 
 
+def test_oracle_statistics_on_tets_within_reference_band(oracle_lib):
+    """The same band in the collision-dominated regime: the capsule tets at
+    Kn 0.01 (about a dozen collisions per particle and step), time-averaged
+    rho, u, T, Tr over steps 61-120 against 8 seeded reference runs, every
+    third cell; and the particle count of each step within the runs'
+    spread."""
+    g = golden("stats_band_capsule.npz")
+    raw, dm, mess = I.capsule_small()
+    x, v, ir, cell = I.fill_inputs_any(dm, mess, int(g["ppc"]), 3)
+    o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir(), seed=11))
+    o.set_particles(x, v, ir, cell)
+    acc = np.zeros((dm.ncell, 18))
+    steps, a0 = int(g["steps"]), int(g["avg_from"])
+    counts = []
+    for s in range(1, steps + 1):
+        o.step(s)
+        if s >= a0:
+            acc += o.step_moments()
+        counts.append(int(o.lib.oracle_count(o.h)))
+    f = I.fields_from_moments(acc, steps - a0 + 1, dm, mess)[g["cells"]]
+    K = int(g["k"])
+    mean = g["mean"].astype(float)
+    sd = g["sd"].astype(float) * np.sqrt(1.0 + 1.0 / K)
+    ok = np.isfinite(mean) & np.isfinite(f) & (sd > 0)
+    assert ok.mean() > 0.95
+    z = (f[ok] - mean[ok]) / sd[ok]
+    assert np.mean(np.abs(z) <= 3.0) >= 0.95
+    assert abs(np.mean(z)) < 0.3
+    for j in range(6):
+        zj = (f[ok[:, j], j] - mean[ok[:, j], j]) / sd[ok[:, j], j]
+        assert abs(np.mean(zj)) < 0.3, j
+    ref_n = g["nparticles"].astype(float)
+    lo, hi = ref_n.min(0) * 0.97, ref_n.max(0) * 1.03
+    assert np.all((np.array(counts) >= lo) & (np.array(counts) <= hi))
+
+
 def test_oracle_stress_and_heat_flux_within_reference_band(block, oracle_stats_run):
     """Deviatoric stress, heat flux and rotational heat flux as
     writeAveragedMacro defines them, against the same 8 reference runs."""
