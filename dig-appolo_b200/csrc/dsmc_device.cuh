@@ -60,10 +60,8 @@ struct DevMesh {
     const int* triOffset;        // [ncell+1]
     const double* triD;          // [ntri*9] A, e1=B-A, e2=C-A (absolute FP64)
     const int2* triFT;           // [ntri] face id, triangle tag
-    const float4* triF;          // [ntri*3] A-centre(3) e1(3) e2(3) |e1||e2| face tag (FP32)
     const unsigned char* faceRole;
     const int2* faceCells;       // [nface] c0, c1 (c1 >= ncell: ghost)
-    const float4* faceDelta;     // [nface] centre(c0) - centre(c1) as FP32
     const int* faceWall;         // [nface] wall slot or -1
     const double* wallRot;       // [nwall*2*9] rotation R(n) for tag 1 (or triangle), tag 2
     const float* wallRotF;       // same, FP32
@@ -79,7 +77,9 @@ struct DevMesh {
     const float4* diagF;         // quads: in-plane normal of the diagonal, offset (relative)
     const double* planeD;        // [nrec*8] n(3), d, m(3), md, absolute
     const unsigned char* convex; // [ncell]
-    const float4* nbDeltaF;      // [nrec] FP32 centre shift of a crossing through the record (this - other)
+    const float2* recAux;        // [nrec] x: min |e1 x e2| over the record's triangles (0 when one of them is
+                                 // ill-conditioned), y: the cell's length scale (sum over axes of the
+                                 // largest node offset from the centre)
     int faceStride;              // F when every cell is convex with F records (record k = cell * F + j), else 0
     int allConvex;               // every cell takes the plane path
     // placement tetrahedra of each cell (buildCellInitTets): records
@@ -278,16 +278,11 @@ struct ExitHit {
 // tryCachedCellIntersection, src/ProcessDSMC.cpp:1210-1251. The reference's
 // uncached fallback (intersectFallbackCell, :1484-1524) repeats the same
 // products and sums on the same node coordinates, so it cannot find a hit the
-// cached test missed; a miss here is a miss there.
-//
-// entryFace / posTol serve the mixed path only: its positions carry FP32
-// rounding, so a particle sitting on the face it entered through can see
-// that face again at a tiny positive t that the reference, with exact
-// positions, rejects through its 1e-14 cut. Hits on entryFace closer than
-// posTol / |v.n| are therefore treated as on the face (no hit).
+// cached test missed; a miss here is a miss there. Triangles of the entry face
+// are skipped by the reference's rule (:1229-1233): all of a triangular face,
+// only the same half of a quad.
 __device__ __forceinline__ ExitHit find_exit_exact(const DevMesh& M, int cell, int crossf, int prevTri,
-                                                   const double x[3], const double v[3],
-                                                   int entryFace = -1, double posTol = 0.0)
+                                                   const double x[3], const double v[3])
 {
     ExitHit h{-2, -1, DBL_MAX};
     const int b = M.triOffset[cell];
@@ -297,16 +292,8 @@ __device__ __forceinline__ ExitHit find_exit_exact(const DevMesh& M, int cell, i
         if (ft.x == crossf) {
             if (ft.y <= 0 || (prevTri != 1 && prevTri != 2) || ft.y == prevTri) continue;
         }
-        const double* T = M.triD + (size_t)k * 9;
         double t = DBL_MAX;
-        if (isect_exact(T, x, v, t) && t < h.t) {
-            if (ft.x == entryFace) {
-                const double nx = T[4] * T[8] - T[5] * T[7];
-                const double ny = T[5] * T[6] - T[3] * T[8];
-                const double nz = T[3] * T[7] - T[4] * T[6];
-                const double vn = fabs(v[0] * nx + v[1] * ny + v[2] * nz) / sqrt(nx * nx + ny * ny + nz * nz);
-                if (t * vn <= posTol) continue;
-            }
+        if (isect_exact(M.triD + (size_t)k * 9, x, v, t) && t < h.t) {
             h.t = t;
             h.face = ft.x;
             h.tri = ft.y;
@@ -316,90 +303,9 @@ __device__ __forceinline__ ExitHit find_exit_exact(const DevMesh& M, int cell, i
     return h;
 }
 
-// Guarded FP32 exit search. Positions are relative to the cell centre, so
-// x - A carries no cancellation from the domain's absolute coordinates.
-// Every decision the reference takes (|det| against 1e-14, u/v/u+v against
-// [0,1], t against 1e-14, the smallest t, t against dtleft) is taken in FP32
-// only when the FP32 value is farther from the threshold than an error bound
-// K*eps32/rel_det (rel_det = |det| / (|e1||e2||v|)); otherwise `ambiguous` is
-// set and the caller repeats the step in exact FP64.
-struct ExitHitF {
-    int face;
-    int tri;
-    float t;
-    float terr;
-    bool ambiguous;
-};
-
-constexpr float kGuardK = 256.0f * 5.9604645e-8f;   // 256 ulp(1) of FP32
-
-__device__ __forceinline__ ExitHitF find_exit_f32(const DevMesh& M, int cell, int crossf, int prevTri,
-                                                   const float x[3], const float v[3], float vnorm,
-                                                   int entryFace, float posTol)
-{
-    ExitHitF h{-2, -1, FLT_MAX, 0.0f, false};
-    float second = FLT_MAX, secondErr = 0.0f;
-    const int b = M.triOffset[cell];
-    const int e = M.triOffset[cell + 1];
-    for (int k = b; k < e; ++k) {
-        const float4 r0 = M.triF[(size_t)k * 3 + 0];
-        const float4 r1 = M.triF[(size_t)k * 3 + 1];
-        const float4 r2 = M.triF[(size_t)k * 3 + 2];
-        const int face = __float_as_int(r2.z);
-        const int tag = __float_as_int(r2.w);
-        if (face == crossf) {
-            if (tag <= 0 || (prevTri != 1 && prevTri != 2) || tag == prevTri) continue;
-        }
-        const float ax = r0.x, ay = r0.y, az = r0.z;
-        const float e1x = r0.w, e1y = r1.x, e1z = r1.y;
-        const float e2x = r1.z, e2y = r1.w, e2z = r2.x;
-        const float e12 = r2.y;
-        const float p0 = v[1] * e2z - v[2] * e2y;
-        const float p1 = v[2] * e2x - v[0] * e2z;
-        const float p2 = v[0] * e2y - v[1] * e2x;
-        const float det = e1x * p0 + e1y * p1 + e1z * p2;
-        const float scale = e12 * vnorm;               // |e1||e2||v|
-        const float adet = fabsf(det);
-        if (!(adet > 1e-6f * scale) || adet < 1e-13f) {
-            // near-parallel ray, degenerate triangle or |det| near the
-            // reference's absolute 1e-14 cut: FP32 cannot decide
-            if (scale > 0.0f) h.ambiguous = true;
-            continue;
-        }
-        const float inv = 1.0f / det;
-        const float err = kGuardK * scale * fabsf(inv);  // bound on |u|,|v| errors
-        const float t0 = x[0] - ax, t1 = x[1] - ay, t2 = x[2] - az;
-        const float u = (t0 * p0 + t1 * p1 + t2 * p2) * inv;
-        if (u < -err || u > 1.0f + err) continue;      // certain miss
-        const float q0 = t1 * e1z - t2 * e1y;
-        const float q1 = t2 * e1x - t0 * e1z;
-        const float q2 = t0 * e1y - t1 * e1x;
-        const float w = (v[0] * q0 + v[1] * q1 + v[2] * q2) * inv;
-        if (w < -err || u + w > 1.0f + 2.0f * err) continue;
-        const float t = (e2x * q0 + e2y * q1 + e2z * q2) * inv;
-        // time error: relative err plus the position-scale term
-        const float tErr = err * (fabsf(t) + (fabsf(t0) + fabsf(t1) + fabsf(t2)) / fmaxf(vnorm, 1e-30f));
-        if (t < -tErr) continue;                       // certain miss (behind)
-        // on the entry face: |t| <= posTol/|v.n| <= posTol*|e1||e2|/|det|
-        if (face == entryFace && t <= 2.0f * posTol * e12 * fabsf(inv)) continue;
-        const bool inside = (u > err) && (u < 1.0f - err) && (w > err) && (u + w < 1.0f - 2.0f * err);
-        if (!inside || t <= fmaxf(tErr, 1e-13f)) {
-            h.ambiguous = true;
-            continue;
-        }
-        if (t < h.t) {
-            second = h.t; secondErr = h.terr;
-            h.t = t; h.terr = tErr; h.face = face; h.tri = tag;
-        } else if (t < second) {
-            second = t; secondErr = tErr;
-        }
-    }
-    if (h.face != -2 && second < FLT_MAX && second - h.t <= h.terr + secondErr) h.ambiguous = true;
-    return h;
-}
-
 // ---------------------------------------------------------------------------
-// Plane-based exit search for cells that are convex with planar faces.
+// Plane-based exit search of the FP64 path, for cells that are convex with
+// planar faces.
 //
 // The exit of a ray from inside a convex cell is the face plane it reaches
 // first among those it moves towards: t_f = (d_f - n_f.x) / (v.n_f) for
@@ -413,62 +319,47 @@ __device__ __forceinline__ ExitHitF find_exit_f32(const DevMesh& M, int cell, in
 // triangle search. The entry face (crossf) is never the exit: the particle
 // sits on it and moves away from it.
 // ---------------------------------------------------------------------------
-template <typename Real>
 struct PlaneHit {
     int face;
     int tri;       // -1 triangle face, 1/2 quad half
     int triIdx;    // index of that triangle in the cell's triangle list
-    Real t;
-    Real terr;
+    double t;
     bool ambiguous;
     int nb;        // the record's crossing: the cell on the other side, kNbLost or -(role + 1)
-    float4 delta;  // FP32 path: the record's centre shift
 };
 
-template <typename Real>
-__device__ __forceinline__ PlaneHit<Real> find_exit_planes(const DevMesh& M, int cell, int crossf, const Real x[3],
-                                                           const Real v[3])
+__device__ __forceinline__ PlaneHit find_exit_planes(const DevMesh& M, int cell, int crossf, const double x[3],
+                                                     const double v[3])
 {
-    constexpr Real eps = (sizeof(Real) == 8) ? (Real)1.1102230246251565e-16 : (Real)5.9604645e-8f;
-    constexpr Real K = (sizeof(Real) == 8) ? (Real)64 : (Real)32;
-    PlaneHit<Real> h{-2, -1, -1, (Real)0, (Real)0, false, 0, make_float4(0.f, 0.f, 0.f, 0.f)};
-    const Real vnorm = fabs(v[0]) + fabs(v[1]) + fabs(v[2]);
-    const Real xnorm = fabs(x[0]) + fabs(x[1]) + fabs(x[2]);
-    Real best = (sizeof(Real) == 8) ? (Real)DBL_MAX : (Real)FLT_MAX;
-    Real second = best, bestErr = 0, secondErr = 0;
+    constexpr double eps = 1.1102230246251565e-16;
+    constexpr double K = 64;
+    PlaneHit h{-2, -1, -1, 0.0, false, 0};
+    const double vnorm = fabs(v[0]) + fabs(v[1]) + fabs(v[2]);
+    const double xnorm = fabs(x[0]) + fabs(x[1]) + fabs(x[2]);
+    double best = DBL_MAX, second = DBL_MAX, bestErr = 0, secondErr = 0;
     int bi = -1;
     bool amb = false;
-    float4 bestDelta = make_float4(0.f, 0.f, 0.f, 0.f);
     const int b = M.faceStride ? cell * M.faceStride : M.faceOff[cell];
     const int e = M.faceStride ? b + M.faceStride : M.faceOff[cell + 1];
     for (int k = b; k < e; ++k) {
         const int4 rec = M.faceRec[k];
-        float4 dk = make_float4(0.f, 0.f, 0.f, 0.f);
-        if constexpr (sizeof(Real) == 4) dk = M.nbDeltaF[k];
         if (rec.x == crossf) continue;
-        Real nx, ny, nz, d;
-        if constexpr (sizeof(Real) == 8) {
-            const double* pd = M.planeD + (size_t)k * 8;
-            nx = pd[0]; ny = pd[1]; nz = pd[2]; d = pd[3];
-        } else {
-            const float4 pl = M.planeF[k];
-            nx = pl.x; ny = pl.y; nz = pl.z; d = pl.w;
-        }
-        const Real vn = v[0] * nx + v[1] * ny + v[2] * nz;
-        const Real num = d - (x[0] * nx + x[1] * ny + x[2] * nz);
-        const Real dErr = K * eps * (fabs(d) + xnorm);
-        const Real vErr = K * eps * vnorm;
+        const double* pd = M.planeD + (size_t)k * 8;
+        const double nx = pd[0], ny = pd[1], nz = pd[2], d = pd[3];
+        const double vn = v[0] * nx + v[1] * ny + v[2] * nz;
+        const double num = d - (x[0] * nx + x[1] * ny + x[2] * nz);
+        const double dErr = K * eps * (fabs(d) + xnorm);
+        const double vErr = K * eps * vnorm;
         if (num < -dErr) amb = true;                    // outside this face plane
         if (vn <= vErr) {
             if (vn > -vErr && num <= dErr) amb = true;  // grazing the plane it sits on
             continue;
         }
-        const Real t = num / vn;
-        const Real tErr = (dErr + fabs(t) * vErr) / vn;
+        const double t = num / vn;
+        const double tErr = (dErr + fabs(t) * vErr) / vn;
         if (t < best) {
             second = best; secondErr = bestErr;
             best = t; bestErr = tErr; bi = k;
-            bestDelta = dk;
         } else if (t < second) {
             second = t; secondErr = tErr;
         }
@@ -479,25 +370,17 @@ __device__ __forceinline__ PlaneHit<Real> find_exit_planes(const DevMesh& M, int
     const int4 rec = M.faceRec[bi];
     h.face = rec.x;
     h.t = best;
-    h.terr = bestErr;
     h.tri = -1;
     h.triIdx = rec.y;
     h.nb = rec.w;
-    h.delta = bestDelta;
     if (rec.z == 4) {
-        Real mx, my, mz, md;
-        if constexpr (sizeof(Real) == 8) {
-            const double* pd = M.planeD + (size_t)bi * 8;
-            mx = pd[4]; my = pd[5]; mz = pd[6]; md = pd[7];
-        } else {
-            const float4 dg = M.diagF[bi];
-            mx = dg.x; my = dg.y; mz = dg.z; md = dg.w;
-        }
-        const Real px = x[0] + v[0] * best, py = x[1] + v[1] * best, pz = x[2] + v[2] * best;
-        const Real side = mx * px + my * py + mz * pz - md;
-        const Real sErr = K * eps * (fabs(md) + fabs(px) + fabs(py) + fabs(pz)) + vnorm * bestErr;
+        const double* pd = M.planeD + (size_t)bi * 8;
+        const double mx = pd[4], my = pd[5], mz = pd[6], md = pd[7];
+        const double px = x[0] + v[0] * best, py = x[1] + v[1] * best, pz = x[2] + v[2] * best;
+        const double side = mx * px + my * py + mz * pz - md;
+        const double sErr = K * eps * (fabs(md) + fabs(px) + fabs(py) + fabs(pz)) + vnorm * bestErr;
         if (fabs(side) <= sErr) amb = true;
-        h.tri = side > (Real)0 ? 1 : 2;
+        h.tri = side > 0.0 ? 1 : 2;
         h.triIdx = rec.y + (h.tri == 2 ? 1 : 0);
     }
     h.ambiguous = amb;
@@ -505,11 +388,132 @@ __device__ __forceinline__ PlaneHit<Real> find_exit_planes(const DevMesh& M, int
 }
 
 // ---------------------------------------------------------------------------
+// The mixed path's exit test: FP32 arithmetic that settles, where it can, what
+// the reference's FP64 triangle scan (find_exit_exact) returns, so that the
+// mixed trace takes the same decisions as the FP64 trace.
+//
+// Inputs: the position relative to the cell centre rounded to FP32 from the
+// trace's FP64 position, the FP32 velocity, and the cell's FP32 face planes.
+// Every quantity carries a bound on its error: dErr on a plane distance
+// (32 ulp of the operands' size plus the cell's length scale, five times the
+// worst case of the roundings in x, n, d and the dot product, and far above
+// the reference's own FP64 rounding in absolute coordinates), vErr on v.n.
+// The result is `certain` when:
+//   - every face other than the entry face is either approached (v.n > vErr)
+//     or left behind (v.n < -vErr), with the particle inside its plane by
+//     more than twice its dErr (so no face test can see a hit behind the
+//     particle or at t ~ 0);
+//   - the approached face f reached first is reached, within its interval
+//     [tLo, tHi], before any other approached face could be, with a margin
+//     of one dErr at the hit point on every other face's plane, the entry
+//     face's included: the hit point lies inside f's triangle by more than
+//     the FP64 test's rounding, and no other triangle's hit can come first;
+//   - f is neither grazed (v.n_f below 2^-10 |v|) nor ill-conditioned, and
+//     its triangles' determinants stay above the reference's 1e-14 cut;
+//   - for a quad f, the hit point is clear of the split diagonal (which half),
+//     and after entering through half `tag` of a quad, the position is clear
+//     of that face's diagonal on the side of `tag` (the reference still tests
+//     the other half, :1229-1233; it cannot hit from there).
+// Then the reference's scan returns f (with the half `tri`) at a t inside
+// [tLo, tHi]. Anything else is not certain and the caller runs that scan.
+// ---------------------------------------------------------------------------
+struct CertainExit {
+    bool certain;
+    int face, tri, triIdx;
+    int nb;        // the record's crossing (as PlaneHit::nb)
+    float tLo, tHi;
+};
+
+constexpr float kEps32 = 5.9604645e-8f;   // 2^-24
+
+__device__ __forceinline__ CertainExit certain_exit_f32(const DevMesh& M, int cell, int crossf, int tag,
+                                                        const float x[3], const float v[3], float absScale)
+{
+    CertainExit r{false, -2, -1, -1, 0, 0.0f, 0.0f};
+    const float vnorm = fabsf(v[0]) + fabsf(v[1]) + fabsf(v[2]);
+    const float xnorm = fabsf(x[0]) + fabsf(x[1]) + fabsf(x[2]);
+    const float vErr = 32.0f * kEps32 * vnorm;
+    const float absErr = 0x1p-30f * absScale;
+    const int b = M.faceStride ? cell * M.faceStride : M.faceOff[cell];
+    const int e = M.faceStride ? b + M.faceStride : M.faceOff[cell + 1];
+    int bi = -1;
+    float best = FLT_MAX, bestLo = 0.0f, bestHi = 0.0f, bestTau = 0.0f, bestVn = 0.0f;
+    float tauMin = FLT_MAX;   // latest t_f every other approached face allows
+    float entA = 0.0f, entB = 0.0f;
+    bool ok = true;
+    for (int k = b; k < e; ++k) {
+        const int4 rec = M.faceRec[k];
+        const float4 pl = M.planeF[k];
+        const float lc = M.recAux[k].y;
+        const float vn = v[0] * pl.x + v[1] * pl.y + v[2] * pl.z;
+        const float num = pl.w - (x[0] * pl.x + x[1] * pl.y + x[2] * pl.z);
+        const float dErr = 32.0f * kEps32 * (fabsf(pl.w) + xnorm + lc) + absErr;
+        if (rec.x == crossf) {
+            // entry face: moving away from it; its edge with the exit face is
+            // checked below (slack entA + t_f * entB)
+            if (!(vn < -vErr)) ok = false;
+            entA = num - 2.0f * dErr;
+            entB = -vn - vErr;
+            if (rec.z == 4 && (tag == 1 || tag == 2)) {
+                const float4 dg = M.diagF[k];
+                const float side = dg.x * x[0] + dg.y * x[1] + dg.z * x[2] - dg.w;
+                const float sErr = 2.0f * (32.0f * kEps32 * (fabsf(dg.w) + xnorm + lc) + absErr);
+                if (!(tag == 1 ? side > sErr : side < -sErr)) ok = false;
+            }
+            continue;
+        }
+        if (!(num > 2.0f * dErr) || !(fabsf(vn) > vErr)) { ok = false; continue; }
+        if (vn < 0.0f) continue;   // left behind: never reached
+        const float t = num / vn;
+        const float tLo = (num - dErr) / (vn + vErr);
+        const float tHi = (num + dErr) / (vn - vErr);
+        const float tau = (num - 2.0f * dErr) / (vn + vErr);
+        if (t < best) {
+            if (bi >= 0) tauMin = fminf(tauMin, bestTau);
+            best = t; bestLo = tLo; bestHi = tHi; bestTau = tau; bestVn = vn; bi = k;
+        } else {
+            tauMin = fminf(tauMin, tau);
+        }
+    }
+    if (!ok || bi < 0) return r;
+    if (!(bestHi < tauMin)) return r;
+    if (crossf >= 0 && !(entA + bestLo * entB > 0.0f)) return r;
+    const float2 aux = M.recAux[bi];
+    if (!(bestVn >= 0x1p-10f * vnorm)) return r;            // grazing exit
+    if (!((bestVn - vErr) * aux.x > 2e-14f)) return r;       // |det| near the 1e-14 cut, or ill-conditioned
+    if (!(bestLo > 2e-14f)) return r;                        // the reference's t > 1e-14
+    const int4 rec = M.faceRec[bi];
+    int tri = -1, triIdx = rec.y;
+    if (rec.z == 4) {
+        const float4 dg = M.diagF[bi];
+        const float px = x[0] + v[0] * best, py = x[1] + v[1] * best, pz = x[2] + v[2] * best;
+        const float side = dg.x * px + dg.y * py + dg.z * pz - dg.w;
+        const float sErr = 32.0f * kEps32 * (fabsf(dg.w) + fabsf(px) + fabsf(py) + fabsf(pz) + aux.y) + absErr +
+                           vnorm * (bestHi - bestLo);
+        if (!(fabsf(side) > 2.0f * sErr)) return r;
+        tri = side > 0.0f ? 1 : 2;
+        triIdx = rec.y + (tri == 2 ? 1 : 0);
+    }
+    r.certain = true;
+    r.face = rec.x;
+    r.tri = tri;
+    r.triIdx = triIdx;
+    r.nb = rec.w;
+    r.tLo = bestLo;
+    r.tHi = bestHi;
+    return r;
+}
+
+// ---------------------------------------------------------------------------
 // Particle state in registers and the tracing loop.
 // ---------------------------------------------------------------------------
+// Positions are absolute FP64 while a particle is traced, in both paths: the
+// mixed path stores them in HBM as FP32 offsets from the cell centre and
+// widens them on load (centre + offset, one rounding), so its trace advances
+// exactly the positions the FP64 trace would from the same stored state.
 template <typename Real>
 struct PRegs {
-    Real x[3];   // FP64: absolute; FP32: relative to the centre of `cell`
+    double x[3];
     Real v[3];
     Real ir;
 };
@@ -589,15 +593,13 @@ struct TraceCounts {
     uint32_t removed, dropped, lost, wall, cross, fallback;
 };
 
-// x += v t (scalar_product, src/ProcessDSMC.cpp:1611-1617)
+// x += v t (scalar_product, src/ProcessDSMC.cpp:1611-1617), in FP64 with
+// each operation rounded on its own (an FP32 velocity widens exactly)
 template <typename Real>
-__device__ __forceinline__ void advance(PRegs<Real>& p, Real t)
+__device__ __forceinline__ void advance(PRegs<Real>& p, double t)
 {
-    if constexpr (sizeof(Real) == 8) {
-        for (int d = 0; d < 3; ++d) p.x[d] = da(p.x[d], dm(p.v[d], t));
-    } else {
-        for (int d = 0; d < 3; ++d) p.x[d] += p.v[d] * t;
-    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) p.x[d] = da(p.x[d], dm((double)p.v[d], t));
 }
 
 // The tracing loop's state between two exit searches.
@@ -605,7 +607,6 @@ struct TraceState {
     int ifout;        // outcome so far
     int iter;         // exit searches made
     int crossf, tag;  // the face / triangle the particle entered through
-    int entryFace;    // the face the particle sits on (mixed path)
     bool afterNone;   // the last hit had no handler: use the triangle search
     __device__ __forceinline__ void begin(int crossf0, int tag0)
     {
@@ -613,7 +614,6 @@ struct TraceState {
         iter = 0;
         crossf = crossf0;
         tag = tag0;
-        entryFace = crossf0;
         afterNone = false;
     }
 };
@@ -622,179 +622,150 @@ struct TraceState {
 // 149-221): an exit search from `cell` and either the advance to the end of
 // the step or the crossing with its boundary handling. Returns true when the
 // trace is over, with the outcome in st.ifout.
+//
+// Exit search. FP64 path: the FP64 plane decision confirmed by the
+// reference's test on the chosen triangle, else the reference's triangle
+// scan. Mixed path: certain_exit_f32 on the FP32 offsets; a certain exit
+// beyond the rest of the step needs no FP64 test at all (the particle stays),
+// a certain crossing takes its t from the reference's FP64 test on the one
+// triangle it names, and everything else runs the reference's FP64 triangle
+// scan (counter `fp64_fallbacks`). Positions, dtleft and every decision are
+// then those of the FP64 trace from the same stored state; only wall
+// re-emission draws FP32 velocities.
 template <typename Real>
 __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C, PRegs<Real>& p, int& cell,
-                                           Real& dtleft, TraceState& st, Stream& rng, int istep,
+                                           double& dtleft, TraceState& st, Stream& rng, int istep,
                                            double* wallTally, TraceCounts& cnt, bool stopAtWall, TraceLog* log)
 {
     int& ifout = st.ifout;
     int& crossf = st.crossf;
     int& tag = st.tag;
-    int& entryFace = st.entryFace;
     bool& afterNone = st.afterNone;
-    if (!(dtleft > (Real)0)) return true;
-    {
-        if (st.iter++ >= C.maxCross) { cnt.lost++; dtleft = 0; ifout = kTraceLost; return true; }
-        int face, tri;
-        Real t;
-        bool stays;
-        // a face chosen by the plane search comes with its record's crossing
-        bool hint = false;
-        int hintNb = 0;
-        float4 hintDelta = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!(dtleft > 0.0)) return true;
+    if (st.iter++ >= C.maxCross) { cnt.lost++; dtleft = 0; ifout = kTraceLost; return true; }
+    int face = -2, tri = -1;
+    double t = 0.0;
+    bool decided = false;
+    int hintNb = 0;   // a face chosen from a face record comes with the record's crossing
+    if ((M.allConvex || M.convex[cell]) && !afterNone) {
         if constexpr (sizeof(Real) == 8) {
-            bool decided = false;
-            if ((M.allConvex || M.convex[cell]) && !afterNone) {
-                // plane decision, then the reference's exact test on that one
-                // triangle for the bit-exact t; any doubt runs the full search
-                const PlaneHit<double> ph = find_exit_planes<double>(M, cell, crossf, p.x, p.v);
-                double te = DBL_MAX;
-                if (!ph.ambiguous && isect_exact(M.triD + (size_t)ph.triIdx * 9, p.x, p.v, te)) {
-                    face = ph.face; tri = ph.tri; t = te;
-                    decided = true;
-                    hintNb = ph.nb;
-                    // the other half of a quad entry face stays eligible in
-                    // the reference's skip rule (src/ProcessDSMC.cpp:1229-1233)
-                    if (crossf >= 0 && (tag == 1 || tag == 2)) {
-                        const int b0 = M.triOffset[cell], e0 = M.triOffset[cell + 1];
-                        for (int k = b0; k < e0; ++k) {
-                            const int2 ft = M.triFT[k];
-                            if (ft.x != crossf || ft.y == tag || ft.y <= 0) continue;
-                            double t2 = DBL_MAX;
-                            if (isect_exact(M.triD + (size_t)k * 9, p.x, p.v, t2) && t2 < t) decided = false;
-                        }
+            // plane decision, then the reference's exact test on that one
+            // triangle for the bit-exact t; any doubt runs the full search
+            const PlaneHit ph = find_exit_planes(M, cell, crossf, p.x, p.v);
+            double te = DBL_MAX;
+            if (!ph.ambiguous && isect_exact(M.triD + (size_t)ph.triIdx * 9, p.x, p.v, te)) {
+                face = ph.face; tri = ph.tri; t = te;
+                decided = true;
+                hintNb = ph.nb;
+                // the other half of a quad entry face stays eligible in
+                // the reference's skip rule (src/ProcessDSMC.cpp:1229-1233)
+                if (crossf >= 0 && (tag == 1 || tag == 2)) {
+                    const int b0 = M.triOffset[cell], e0 = M.triOffset[cell + 1];
+                    for (int k = b0; k < e0; ++k) {
+                        const int2 ft = M.triFT[k];
+                        if (ft.x != crossf || ft.y == tag || ft.y <= 0) continue;
+                        double t2 = DBL_MAX;
+                        if (isect_exact(M.triD + (size_t)k * 9, p.x, p.v, t2) && t2 < t) decided = false;
                     }
                 }
             }
-            hint = decided;
-            if (!decided) {
-                const ExitHit h = find_exit_exact(M, cell, crossf, tag, p.x, p.v);
-                if (h.face == -2 || !isfinite(h.t) || h.t <= 0.0) { cnt.dropped++; dtleft = 0; ifout = kTraceDropped; return true; }
-                face = h.face; tri = h.tri; t = h.t;
-            }
-            stays = t >= dtleft;
         } else {
-            const float vnorm = sqrtf(p.v[0] * p.v[0] + p.v[1] * p.v[1] + p.v[2] * p.v[2]);
-            // absolute uncertainty of the FP32 cell-relative position
-            const float posTol = 64.0f * 5.9604645e-8f * (fabsf(p.x[0]) + fabsf(p.x[1]) + fabsf(p.x[2]));
-            ExitHitF h;
-            bool planes = false;
-            if ((M.allConvex || M.convex[cell]) && !afterNone) {
-                const PlaneHit<float> ph = find_exit_planes<float>(M, cell, crossf, p.x, p.v);
-                h = ExitHitF{ph.face, ph.tri, ph.t, ph.terr, ph.ambiguous};
-                planes = true;
-                hintNb = ph.nb;
-                hintDelta = ph.delta;
-            } else {
-                h = find_exit_f32(M, cell, crossf, tag, p.x, p.v, vnorm, entryFace, posTol);
-            }
-            bool amb = h.ambiguous;
-            if (!amb && h.face != -2 &&
-                fabsf(h.t - dtleft) <= h.terr + 4.8e-7f * (dtleft + (float)C.dtime)) amb = true;
-            if (amb) {
-                // Repeat this crossing step in exact FP64 from the same state.
-                cnt.fallback++;
-                const double* cc = M.cellCenter + (size_t)cell * 3;
-                double xa[3] = {cc[0] + (double)p.x[0], cc[1] + (double)p.x[1], cc[2] + (double)p.x[2]};
-                const double va[3] = {(double)p.v[0], (double)p.v[1], (double)p.v[2]};
-                const ExitHit he = find_exit_exact(M, cell, crossf, tag, xa, va, entryFace, (double)posTol);
-                if (he.face == -2 || !isfinite(he.t) || he.t <= 0.0) { cnt.dropped++; dtleft = 0; ifout = kTraceDropped; return true; }
-                face = he.face; tri = he.tri;
-                const double dl = (double)dtleft;
-                if (he.t >= dl) {
-                    for (int d = 0; d < 3; ++d) p.x[d] = (float)(da(xa[d], dm(va[d], dl)) - cc[d]);
+            const double* cc = M.cellCenter + (size_t)cell * 3;
+            const double c0 = cc[0], c1 = cc[1], c2 = cc[2];
+            const float xr[3] = {(float)ds(p.x[0], c0), (float)ds(p.x[1], c1), (float)ds(p.x[2], c2)};
+            const float absScale = (float)(fabs(c0) + fabs(c1) + fabs(c2));
+            const CertainExit ce = certain_exit_f32(M, cell, crossf, tag, xr, p.v, absScale);
+            if (ce.certain) {
+                if (ce.tLo > (float)dtleft * (1.0f + 0x1p-16f)) {
+                    // the reference's scan would return this face at t >= dtleft
+                    advance(p, dtleft);
                     dtleft = 0;
                     return true;
                 }
-                stays = false;
-                t = (float)he.t;
-                if (!(t < dtleft)) t = nextafterf(dtleft, 0.0f);
-            } else {
-                if (h.face == -2 || !(h.t > 0.0f)) { cnt.dropped++; dtleft = 0; ifout = kTraceDropped; return true; }
-                face = h.face; tri = h.tri; t = h.t;
-                stays = t >= dtleft;
-                hint = planes;
-            }
-        }
-        if (stays) {
-            advance(p, dtleft);
-            dtleft = 0;
-            return true;
-        }
-        crossf = face;
-        tag = tri;
-        const int role = !hint ? (int)M.faceRole[face] : (hintNb >= 0 || hintNb == kNbLost) ? kRoleInterface : -(hintNb + 1);
-        if (log && role != kRoleInterface && log->hitFace < 0) {
-            log->hitFace = face;
-            log->hitTri = tri;
-            if (stopAtWall && role == kRoleWall) {
-                advance(p, t);
-                if constexpr (sizeof(Real) == 8) dtleft = ds(dtleft, t); else dtleft -= t;
-                return true;
-            }
-        }
-        cnt.cross++;
-        if (log) log->ncross++;
-        // x += v t (scalar_product, src/ProcessDSMC.cpp:1611-1617) for every
-        // role that has a handler
-        if (role != kRoleNone) advance(p, t);
-        if (role == kRoleInterface) {
-            ifout = kTraceMoved;
-            if constexpr (sizeof(Real) == 8) dtleft = ds(dtleft, t); else dtleft -= t;
-            int next;
-            int2 cc = make_int2(0, 0);
-            if (hint) {
-                next = hintNb;
-            } else {
-                cc = M.faceCells[face];
-                if (cell == cc.x) next = cc.y;
-                else if (cell == cc.y) next = cc.x;
-                else next = cc.x;
-            }
-            if (next < 0 || next >= M.ncell) { cnt.lost++; dtleft = 0; ifout = kTraceLost; return true; }
-            if constexpr (sizeof(Real) == 4) {
-                if (hint) {
-                    p.x[0] += hintDelta.x; p.x[1] += hintDelta.y; p.x[2] += hintDelta.z;
-                } else {
-                    const float4 dl = M.faceDelta[face];
-                    const float sg = (cell == cc.x) ? 1.0f : -1.0f;
-                    p.x[0] += sg * dl.x; p.x[1] += sg * dl.y; p.x[2] += sg * dl.z;
+                const double v64[3] = {(double)p.v[0], (double)p.v[1], (double)p.v[2]};
+                double te = DBL_MAX;
+                if (isect_exact(M.triD + (size_t)ce.triIdx * 9, p.x, v64, te)) {
+                    face = ce.face; tri = ce.tri; t = te;
+                    decided = true;
+                    hintNb = ce.nb;
                 }
             }
-            cell = next;
-            entryFace = face;
-        } else if (role == kRoleInlet || role == kRoleOutlet) {
-            cnt.removed++;
-            dtleft = 0;
-            ifout = kTraceRemoved; return true;
-        } else if (role == kRoleWall) {
-            if constexpr (sizeof(Real) == 8) dtleft = ds(dtleft, t); else dtleft -= t;
-            const int ws = M.faceWall[face];
-            const Real v0 = p.v[0], v1 = p.v[1], v2 = p.v[2], ir0 = p.ir;
-            diffuse_reflect<Real>(M, C, ws, tri, p, rng);
-            cnt.wall++;
-            entryFace = face;
-            if (wallTally && C.wallStats && istep > C.nss) {
-                double* T = wallTally + (size_t)ws * 6;
-                const double a0 = (double)p.v[0], a1 = (double)p.v[1], a2 = (double)p.v[2];
-                const double b0 = (double)v0, b1 = (double)v1, b2 = (double)v2;
-                atomicAdd(T + 0, 1.0);
-                atomicAdd(T + 1, a0 - b0);
-                atomicAdd(T + 2, a1 - b1);
-                atomicAdd(T + 3, a2 - b2);
-                atomicAdd(T + 4, 0.5 * ((a0 * a0 + a1 * a1 + a2 * a2) - (b0 * b0 + b1 * b1 + b2 * b2)));
-                atomicAdd(T + 5, (double)p.ir - (double)ir0);
-            }
-        } else if (role == kRoleSpecular) {
-            if constexpr (sizeof(Real) == 8) dtleft = ds(dtleft, t); else dtleft -= t;
-            specular_reflect<Real>(M, M.faceWall[face], tri, p);
-            cnt.wall++;
-            entryFace = face;
         }
-        // kRoleNone: no handler (src/ProcessDSMC.cpp:1826-1827); the next
-        // search excludes this face and the particle is dropped.
-        afterNone = (role == kRoleNone);
     }
+    if constexpr (sizeof(Real) == 4) {
+        if (!decided) cnt.fallback++;
+    }
+    if (!decided) {
+        const double v64[3] = {(double)p.v[0], (double)p.v[1], (double)p.v[2]};
+        const ExitHit h = find_exit_exact(M, cell, crossf, tag, p.x, v64);
+        if (h.face == -2 || !isfinite(h.t) || h.t <= 0.0) { cnt.dropped++; dtleft = 0; ifout = kTraceDropped; return true; }
+        face = h.face; tri = h.tri; t = h.t;
+    }
+    if (t >= dtleft) {
+        advance(p, dtleft);
+        dtleft = 0;
+        return true;
+    }
+    crossf = face;
+    tag = tri;
+    const int role = !decided ? (int)M.faceRole[face] : (hintNb >= 0 || hintNb == kNbLost) ? kRoleInterface : -(hintNb + 1);
+    if (log && role != kRoleInterface && log->hitFace < 0) {
+        log->hitFace = face;
+        log->hitTri = tri;
+        if (stopAtWall && role == kRoleWall) {
+            advance(p, t);
+            dtleft = ds(dtleft, t);
+            return true;
+        }
+    }
+    cnt.cross++;
+    if (log) log->ncross++;
+    // x += v t (scalar_product, src/ProcessDSMC.cpp:1611-1617) for every
+    // role that has a handler
+    if (role != kRoleNone) advance(p, t);
+    if (role == kRoleInterface) {
+        ifout = kTraceMoved;
+        dtleft = ds(dtleft, t);
+        int next;
+        if (decided) {
+            next = hintNb;
+        } else {
+            const int2 cc = M.faceCells[face];
+            if (cell == cc.x) next = cc.y;
+            else if (cell == cc.y) next = cc.x;
+            else next = cc.x;
+        }
+        if (next < 0 || next >= M.ncell) { cnt.lost++; dtleft = 0; ifout = kTraceLost; return true; }
+        cell = next;
+    } else if (role == kRoleInlet || role == kRoleOutlet) {
+        cnt.removed++;
+        dtleft = 0;
+        ifout = kTraceRemoved; return true;
+    } else if (role == kRoleWall) {
+        dtleft = ds(dtleft, t);
+        const int ws = M.faceWall[face];
+        const Real v0 = p.v[0], v1 = p.v[1], v2 = p.v[2], ir0 = p.ir;
+        diffuse_reflect<Real>(M, C, ws, tri, p, rng);
+        cnt.wall++;
+        if (wallTally && C.wallStats && istep > C.nss) {
+            double* T = wallTally + (size_t)ws * 6;
+            const double a0 = (double)p.v[0], a1 = (double)p.v[1], a2 = (double)p.v[2];
+            const double b0 = (double)v0, b1 = (double)v1, b2 = (double)v2;
+            atomicAdd(T + 0, 1.0);
+            atomicAdd(T + 1, a0 - b0);
+            atomicAdd(T + 2, a1 - b1);
+            atomicAdd(T + 3, a2 - b2);
+            atomicAdd(T + 4, 0.5 * ((a0 * a0 + a1 * a1 + a2 * a2) - (b0 * b0 + b1 * b1 + b2 * b2)));
+            atomicAdd(T + 5, (double)p.ir - (double)ir0);
+        }
+    } else if (role == kRoleSpecular) {
+        dtleft = ds(dtleft, t);
+        specular_reflect<Real>(M, M.faceWall[face], tri, p);
+        cnt.wall++;
+    }
+    // kRoleNone: no handler (src/ProcessDSMC.cpp:1826-1827); the next
+    // search excludes this face and the particle is dropped.
+    afterNone = (role == kRoleNone);
     return false;
 }
 
@@ -804,7 +775,7 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
 // reference's outcome and leaves the final cell in `cell`.
 template <typename Real>
 __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>& p, int& cell,
-                             int crossf, int tag, Real& dtleft, Stream& rng, int istep,
+                             int crossf, int tag, double& dtleft, Stream& rng, int istep,
                              double* wallTally, TraceCounts& cnt, bool stopAtWall, TraceLog* log)
 {
     TraceState st;

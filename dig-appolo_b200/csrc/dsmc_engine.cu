@@ -146,6 +146,7 @@ struct Engine {
     int* cellPairs = nullptr;
     double* cellCons = nullptr;
     int* errorWord = nullptr;
+    int* uploadFlag = nullptr;     // upload_check_kernel's flags
     int* placeFirst = nullptr;     // [nplace] cell-local first particle of each placement tetrahedron (fill)
     // GSIS particle update (allocated on first use)
     double* gsisNs = nullptr;
@@ -172,6 +173,11 @@ struct Engine {
     cudaEvent_t ev[6] = {};
     double stageMs[5] = {0, 0, 0, 0, 0};
     int64_t timedSteps = 0;
+    // pinned host chunks that pageable upload arrays pass through (allocated
+    // on the first such upload), and the events of their last copies
+    static constexpr size_t kHostStage = size_t(64) << 20;
+    void* hostStage[2] = {nullptr, nullptr};
+    cudaEvent_t stageEv[2] = {nullptr, nullptr};
 
     ~Engine() { release(); }
 
@@ -182,6 +188,10 @@ struct Engine {
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
         for (auto& e : ev)
             if (e) { cudaEventDestroy(e); e = nullptr; }
+        for (int b = 0; b < 2; ++b) {
+            if (stageEv[b]) { cudaEventDestroy(stageEv[b]); stageEv[b] = nullptr; }
+            if (hostStage[b]) { cudaFreeHost(hostStage[b]); hostStage[b] = nullptr; }
+        }
         for (void* p : allocs) cudaFree(p);
         allocs.clear();
         if (stream) { cudaStreamDestroy(stream); stream = nullptr; }
@@ -432,7 +442,6 @@ struct Engine {
         std::vector<int> triOffset((size_t)ncell + 1, 0);
         std::vector<double> triD;
         std::vector<int2> triFT;
-        std::vector<float4> triF;
         triD.reserve((size_t)ncell * 8 * 9);
         for (int lc = 0; lc < ncell; ++lc) {
             triOffset[(size_t)lc] = (int)triFT.size();
@@ -447,20 +456,6 @@ struct Engine {
                 for (int d = 0; d < 3; ++d) triD.push_back(e1[d]);
                 for (int d = 0; d < 3; ++d) triD.push_back(e2[d]);
                 triFT.push_back(make_int2(faceid, tag));
-                float ar[3], f1[3], f2[3];
-                for (int d = 0; d < 3; ++d) {
-                    ar[d] = (float)(A[d] - cc[d]);
-                    f1[d] = (float)e1[d];
-                    f2[d] = (float)e2[d];
-                }
-                const double n1 = std::sqrt((double)f1[0] * f1[0] + (double)f1[1] * f1[1] + (double)f1[2] * f1[2]);
-                const double n2 = std::sqrt((double)f2[0] * f2[0] + (double)f2[1] * f2[1] + (double)f2[2] * f2[2]);
-                float fi, ti;
-                std::memcpy(&fi, &faceid, 4);
-                std::memcpy(&ti, &tag, 4);
-                triF.push_back(make_float4(ar[0], ar[1], ar[2], f1[0]));
-                triF.push_back(make_float4(f1[1], f1[2], f2[0], f2[1]));
-                triF.push_back(make_float4(f2[2], (float)(n1 * n2), fi, ti));
             };
             for (int m = 0; m < cl.num && m < 6; ++m) {
                 const int faceid = cl.cell2face[m];
@@ -643,25 +638,17 @@ struct Engine {
 
         // --- face cells / deltas
         std::vector<int2> faceCells((size_t)nface);
-        std::vector<float4> faceDelta((size_t)nface, make_float4(0, 0, 0, 0));
         std::vector<unsigned char> roleU8((size_t)nface);
         for (int f = 0; f < nface; ++f) {
             const int c0 = edges[(size_t)f].faceMap[4], c1 = edges[(size_t)f].faceMap[5];
             faceCells[(size_t)f] = make_int2(c0, c1);
             roleU8[(size_t)f] = (unsigned char)faceRole[(size_t)f];
-            if (c0 >= 0 && c0 < ncell && c1 >= 0 && c1 < ncell) {
-                faceDelta[(size_t)f] = make_float4(
-                    (float)(cellCenterHost[(size_t)c0 * 3] - cellCenterHost[(size_t)c1 * 3]),
-                    (float)(cellCenterHost[(size_t)c0 * 3 + 1] - cellCenterHost[(size_t)c1 * 3 + 1]),
-                    (float)(cellCenterHost[(size_t)c0 * 3 + 2] - cellCenterHost[(size_t)c1 * 3 + 2]), 0.0f);
-            }
         }
 
         // --- what a crossing through each face record needs, kept with the
         //     record so the trace reads no per-face array: the cell on the
         //     other side (interface faces, as the trace picks it) or the
-        //     face's role, and the FP32 centre shift in the crossing's sense
-        std::vector<float4> nbDeltaF(faceRec.size(), make_float4(0, 0, 0, 0));
+        //     face's role
         for (int lc = 0; lc < ncell; ++lc) {
             for (int k = faceOff[(size_t)lc]; k < faceOff[(size_t)lc + 1]; ++k) {
                 const int f = faceRec[(size_t)k].x;
@@ -671,13 +658,48 @@ struct Engine {
                     const int2 fc = faceCells[(size_t)f];
                     const int next = (lc == fc.x) ? fc.y : (lc == fc.y) ? fc.x : fc.x;
                     nb = (next >= 0 && next < ncell) ? next : kNbLost;
-                    const float sg = (lc == fc.x) ? 1.0f : -1.0f;
-                    const float4 dl = faceDelta[(size_t)f];
-                    nbDeltaF[(size_t)k] = make_float4(sg * dl.x, sg * dl.y, sg * dl.z, 0.0f);
                 } else {
                     nb = -(role + 1);
                 }
                 faceRec[(size_t)k].w = nb;
+            }
+        }
+
+        // --- the mixed path's exit test (certain_exit_f32) per record: the
+        //     smallest |e1 x e2| of the record's triangles (the reference's
+        //     determinant is |v.n| times it), 0 when a triangle is so
+        //     ill-conditioned (|e1||e2| / |e1 x e2| > 1024) that its FP64
+        //     test could round far from the plane arithmetic; and the cell's
+        //     length scale
+        std::vector<float2> recAux(faceRec.size(), make_float2(0.0f, 0.0f));
+        for (int lc = 0; lc < ncell; ++lc) {
+            const double* cc = &cellCenterHost[(size_t)lc * 3];
+            double lmax[3] = {0.0, 0.0, 0.0};
+            for (int t = triOffset[(size_t)lc]; t < triOffset[(size_t)lc + 1]; ++t) {
+                const double* T = &triD[(size_t)t * 9];
+                const double P[3][3] = {{T[0], T[1], T[2]},
+                                        {T[0] + T[3], T[1] + T[4], T[2] + T[5]},
+                                        {T[0] + T[6], T[1] + T[7], T[2] + T[8]}};
+                for (int q = 0; q < 3; ++q)
+                    for (int d = 0; d < 3; ++d) lmax[d] = std::max(lmax[d], std::fabs(P[q][d] - cc[d]));
+            }
+            const float lscale = (float)((lmax[0] + lmax[1] + lmax[2]) * (1.0 + 1e-6));
+            for (int k = faceOff[(size_t)lc]; k < faceOff[(size_t)lc + 1]; ++k) {
+                const int4 rec = faceRec[(size_t)k];
+                double detMin = DBL_MAX;
+                for (int q = 0; q < (rec.z == 4 ? 2 : 1); ++q) {
+                    const double* T = &triD[(size_t)(rec.y + q) * 9];
+                    double cr[3];
+                    cross3(T + 3, T + 6, cr);
+                    const double a = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+                    const double l1 = std::sqrt(T[3] * T[3] + T[4] * T[4] + T[5] * T[5]);
+                    const double l2 = std::sqrt(T[6] * T[6] + T[7] * T[7] + T[8] * T[8]);
+                    const double m = (a > 0.0 && l1 * l2 <= 1024.0 * a) ? a : 0.0;
+                    detMin = std::min(detMin, m);
+                }
+                // rounded down: the device bound must not exceed the true value
+                const float df = (float)(detMin * (1.0 - 1e-6));
+                recAux[(size_t)k] = make_float2(df, lscale);
             }
         }
         // every cell convex with the same number of faces: records at cell * F
@@ -739,26 +761,27 @@ struct Engine {
         C.wallStats = params.wall_stats;
 
         // --- device mesh
-        int* dTriOffset; double* dTriD; int2* dTriFT; float4* dTriF; unsigned char* dRole; int2* dFaceCells;
-        float4* dDelta; int* dFaceWall; double* dWallRot; float* dWallRotF; double* dCenter; double* dVol;
+        int* dTriOffset; double* dTriD; int2* dTriFT; unsigned char* dRole; int2* dFaceCells;
+        int* dFaceWall; double* dWallRot; float* dWallRotF; double* dCenter; double* dVol;
         int* dC2c; signed char* dRev;
-        int *dFaceOff; int4* dFaceRec; float4 *dPlaneF, *dDiagF, *dNbDelta; double* dPlaneD; unsigned char* dConvex;
+        int *dFaceOff; int4* dFaceRec; float4 *dPlaneF, *dDiagF; float2* dRecAux; double* dPlaneD;
+        unsigned char* dConvex;
         if (!upload(dFaceOff, faceOff) || !upload(dFaceRec, faceRec) || !upload(dPlaneF, planeF) ||
             !upload(dDiagF, diagF) || !upload(dPlaneD, planeD) || !upload(dConvex, convex) ||
-            !upload(dNbDelta, nbDeltaF))
+            !upload(dRecAux, recAux))
             return false;
         M.faceOff = dFaceOff; M.faceRec = dFaceRec; M.planeF = dPlaneF; M.diagF = dDiagF; M.planeD = dPlaneD;
-        M.convex = dConvex; M.nbDeltaF = dNbDelta;
+        M.convex = dConvex; M.recAux = dRecAux;
         M.faceStride = faceStride;
         M.allConvex = nconvex == ncell ? 1 : 0;
-        if (!upload(dTriOffset, triOffset) || !upload(dTriD, triD) || !upload(dTriFT, triFT) || !upload(dTriF, triF) ||
-            !upload(dRole, roleU8) || !upload(dFaceCells, faceCells) || !upload(dDelta, faceDelta) ||
+        if (!upload(dTriOffset, triOffset) || !upload(dTriD, triD) || !upload(dTriFT, triFT) ||
+            !upload(dRole, roleU8) || !upload(dFaceCells, faceCells) ||
             !upload(dFaceWall, faceWallHost) || !upload(dWallRot, wallRot) || !upload(dWallRotF, wallRotF) ||
             !upload(dCenter, cellCenterHost) || !upload(dVol, vol) || !upload(dC2c, c2c) || !upload(dRev, rev))
             return false;
         M.ncell = ncell; M.nface = nface; M.ntri = ntri; M.nwall = nwall;
-        M.triOffset = dTriOffset; M.triD = dTriD; M.triFT = dTriFT; M.triF = dTriF;
-        M.faceRole = dRole; M.faceCells = dFaceCells; M.faceDelta = dDelta; M.faceWall = dFaceWall;
+        M.triOffset = dTriOffset; M.triD = dTriD; M.triFT = dTriFT;
+        M.faceRole = dRole; M.faceCells = dFaceCells; M.faceWall = dFaceWall;
         M.wallRot = dWallRot; M.wallRotF = dWallRotF; M.cellCenter = dCenter; M.cellVolume = dVol;
         M.cell2cell = dC2c; M.revSlot = dRev;
         {
@@ -783,7 +806,7 @@ struct Engine {
             !alloc(start[0], (size_t)ncell + 1) || !alloc(start[1], (size_t)ncell + 1) || !alloc(ctl, 1) ||
             !alloc(counters, C_COUNT) || !alloc(cellList, (size_t)ncell * 2) || !alloc(cellWork, 8) ||
             !alloc(cellPairs, (size_t)ncell) || !alloc(cellCons, (size_t)ncell) ||
-            !alloc(errorWord, 1))
+            !alloc(errorWord, 1) || !alloc(uploadFlag, 1))
             return false;
         if (params.keep_step_moments && !alloc(stepMom, (size_t)ncell * 18)) return false;
         cudaError_t pe = (precision == DSMC_PRECISION_MIXED) ? prepare_kernels<float>() : prepare_kernels<double>();
@@ -1247,12 +1270,109 @@ struct Engine {
         return true;
     }
 
+    // Whether host memory is page-locked (or registered), so the DMA engine
+    // can read it in place.
+    static bool hostPinned(const void* p)
+    {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return false;
+        }
+        return a.type == cudaMemoryTypeHost;
+    }
+
+    // Host -> device on the handle's stream: pinned memory in one copy;
+    // pageable memory through the two pinned chunks, the host copy of the
+    // next chunk overlapping the transfer of the last. The source may be
+    // reused once the stream has been synchronised.
+    bool h2d(void* dst, const void* src, size_t bytes)
+    {
+        if (bytes == 0) return true;
+        if (hostPinned(src)) return cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "upload");
+        for (int b = 0; b < 2; ++b) {
+            if (!hostStage[b] && !cuda(cudaHostAlloc(&hostStage[b], kHostStage, cudaHostAllocDefault), "pinned staging"))
+                return false;
+            if (!stageEv[b] && !cuda(cudaEventCreateWithFlags(&stageEv[b], cudaEventDisableTiming), "staging event"))
+                return false;
+        }
+        const char* s = static_cast<const char*>(src);
+        char* d = static_cast<char*>(dst);
+        const int nthreads = hostpack::threads_for((int64_t)(kHostStage / 8));
+        size_t j = 0;
+        for (size_t off = 0; off < bytes; off += kHostStage, ++j) {
+            const int b = (int)(j & 1);
+            const size_t len = std::min(kHostStage, bytes - off);
+            if (!cuda(cudaEventSynchronize(stageEv[b]), "staging wait")) return false;
+            hostpack::parallel_copy(hostStage[b], s + off, len, nthreads);
+            if (!cuda(cudaMemcpyAsync(d + off, hostStage[b], len, cudaMemcpyHostToDevice, stream), "upload") ||
+                !cuda(cudaEventRecord(stageEv[b], stream), "staging event"))
+                return false;
+        }
+        return true;
+    }
+
+    // Upload of particles already in cell-major order (the order of the
+    // reference's per-cell buckets, and of dsmc_download_particles): the cell
+    // ids go up first and a kernel checks them and lays out start[]; the
+    // columns then go up unchanged (FP64) or through the other particle
+    // buffer, chunk by chunk, into FP32 offsets from the cell centres (mixed).
+    // Returns 1 when done, 0 when the cells are not in that order (nothing
+    // is kept; the caller orders them on the host), -1 on an error.
+    int uploadCellMajor(int64_t n, const double* const src[7], const int32_t* cell)
+    {
+        int* dCell = static_cast<int*>(buf[cur][7]);
+        if (!h2d(dCell, cell, (size_t)n * sizeof(int))) return -1;
+        if (!cuda(cudaMemsetAsync(uploadFlag, 0, sizeof(int), stream), "upload flag")) return -1;
+        launch_upload_check(dCell, (int)n, ncell, uploadFlag, start[cur], stream);
+        int flags = 0;
+        if (!cuda(cudaGetLastError(), "upload check") ||
+            !cuda(cudaMemcpyAsync(&flags, uploadFlag, sizeof(int), cudaMemcpyDeviceToHost, stream), "upload flag") ||
+            !cuda(cudaStreamSynchronize(stream), "upload check sync"))
+            return -1;
+        if (flags & 1) {
+            fail("particle cell id out of range");
+            return -1;
+        }
+        if (flags & 2) return 0;
+        if (precision != DSMC_PRECISION_MIXED) {
+            for (int k = 0; k < 7; ++k)
+                if (!h2d(buf[cur][k], src[k], (size_t)n * sizeof(double))) return -1;
+            return 1;
+        }
+        // device chunks of the FP64 columns: the x and y arrays of the other
+        // buffer (capacity FP32 slots each, capacity / 2 FP64 values)
+        const int64_t m = std::max<int64_t>(1, capacity / 2);
+        double* dstage[2] = {static_cast<double*>(buf[cur ^ 1][0]), static_cast<double*>(buf[cur ^ 1][1])};
+        int64_t j = 0;
+        for (int k = 0; k < 7; ++k) {
+            float* out = static_cast<float*>(buf[cur][k]);
+            for (int64_t off = 0; off < n; off += m, ++j) {
+                const int64_t len = std::min(m, n - off);
+                double* ds = dstage[j & 1];
+                if (!h2d(ds, src[k] + off, (size_t)len * sizeof(double))) return -1;
+                launch_upload_convert(ds, dCell + off, M.cellCenter, k, out + off, (int)len, stream);
+            }
+        }
+        return cuda(cudaGetLastError(), "upload convert") ? 1 : -1;
+    }
+
     bool uploadParticles(int64_t n, const double* px, const double* py, const double* pz, const double* vx,
                          const double* vy, const double* vz, const double* ir, const int32_t* cell)
     {
         if (n < 0) return fail("negative particle count");
         if (n > (int64_t)0x7fffffff - 1) return fail("capacity above 2^31 particles");
         if (n > 0 && (!px || !py || !pz || !vx || !vy || !vz || !ir || !cell)) return fail("null particle array");
+        const double* src[7] = {px, py, pz, vx, vy, vz, ir};
+        if (n > 0) {
+            const int64_t need = params.capacity > 0 ? params.capacity : std::max<int64_t>(n + n / 2 + (1 << 16), 1 << 20);
+            if (n > need) return fail("more particles than the configured capacity");
+            haveParticles = false;
+            if (!ensureCapacity(need)) return false;
+            const int r = uploadCellMajor(n, src, cell);
+            if (r < 0) return false;
+            if (r == 1) return finishUpload(n);
+        }
         const int nthreads = hostpack::threads_for(n);
         if (!hostpack::cells_in_range(n, cell, ncell, nthreads)) return fail("particle cell id out of range");
         // order: cell-major, input order within a cell
@@ -1264,7 +1384,6 @@ struct Engine {
         haveParticles = false;
         if (!ensureCapacity(need)) return false;
         const bool mixed = precision == DSMC_PRECISION_MIXED;
-        const double* src[7] = {px, py, pz, vx, vy, vz, ir};
         std::vector<char> hb((size_t)n * 8);
         for (int k = 0; k < 7; ++k) {
             if (mixed)
@@ -1283,6 +1402,11 @@ struct Engine {
             return false;
         if (!cuda(cudaMemcpyAsync(start[cur], st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice, stream), "upload start"))
             return false;
+        return finishUpload(n);
+    }
+
+    bool finishUpload(int64_t n)
+    {
         StepCtl h{};
         h.nLive = (int)n;
         h.capacity = (int)capacity;
@@ -1974,7 +2098,15 @@ int engine_precision(const DsmcHandle* h) { return h->e.precision; }
 int engine_device(const DsmcHandle* h) { return h->e.device; }
 cudaStream_t engine_stream(const DsmcHandle* h) { return h->e.stream; }
 unsigned long long* engine_counters(const DsmcHandle* h) { return h->e.counters; }
-void engine_set_error(DsmcHandle* h, const char* msg) { h->e.err = msg; }
+// Sets the handle's message; a failed host allocation leaves the previous
+// one (nothing is thrown across the C ABI).
+void engine_set_error(DsmcHandle* h, const char* msg) noexcept
+{
+    try {
+        h->e.err = msg;
+    } catch (...) {
+    }
+}
 }  // namespace dsmc
 
 extern "C" {

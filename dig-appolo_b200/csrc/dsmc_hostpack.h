@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <cstring>
 #include <thread>
 #include <vector>
 
@@ -135,6 +136,17 @@ void widen(int64_t n, const In* src, const int32_t* cell, const double* shift, i
             if (shift) v = shift[(size_t)cell[j] * 3 + comp] + v;
             dst[j] = v;
         }
+    });
+}
+
+// memcpy split over threads (byte ranges; every thread count gives the same
+// bytes)
+inline void parallel_copy(void* dst, const void* src, size_t bytes, int nthreads)
+{
+    char* d = static_cast<char*>(dst);
+    const char* s = static_cast<const char*>(src);
+    parallel_for((int64_t)bytes, nthreads, [&](int64_t b, int64_t e, int) {
+        if (e > b) std::memcpy(d + b, s + b, (size_t)(e - b));
     });
 }
 

@@ -26,6 +26,38 @@ namespace dsmc {
 constexpr unsigned kFull = 0xffffffffu;
 
 
+// Particle positions between HBM and the trace's FP64 registers: the FP64
+// path stores absolute FP64; the mixed path stores FP32 offsets from the
+// centre of the particle's cell (widened as centre + offset, stored as the
+// FP32 rounding of position - centre).
+template <typename Real>
+__device__ __forceinline__ void load_position(const DevMesh& M, const PBuf<Real>& B, int i, int cell, PRegs<Real>& p)
+{
+    if constexpr (sizeof(Real) == 8) {
+        p.x[0] = B.x[0][i]; p.x[1] = B.x[1][i]; p.x[2] = B.x[2][i];
+    } else {
+        const double* cc = M.cellCenter + (size_t)cell * 3;
+        p.x[0] = da(cc[0], (double)B.x[0][i]);
+        p.x[1] = da(cc[1], (double)B.x[1][i]);
+        p.x[2] = da(cc[2], (double)B.x[2][i]);
+    }
+}
+
+template <typename Real>
+__device__ __forceinline__ void store_position(const DevMesh& M, const PBuf<Real>& B, int i, int cell,
+                                               const PRegs<Real>& p)
+{
+    if constexpr (sizeof(Real) == 8) {
+        B.x[0][i] = p.x[0]; B.x[1][i] = p.x[1]; B.x[2][i] = p.x[2];
+    } else {
+        if (cell < 0 || cell >= M.ncell) return;   // removed: the slot is not read again
+        const double* cc = M.cellCenter + (size_t)cell * 3;
+        B.x[0][i] = (float)ds(p.x[0], cc[0]);
+        B.x[1][i] = (float)ds(p.x[1], cc[1]);
+        B.x[2][i] = (float)ds(p.x[2], cc[2]);
+    }
+}
+
 // ===========================================================================
 // inject
 // ===========================================================================
@@ -173,21 +205,15 @@ __global__ void __launch_bounds__(128) inject_gen_kernel(StepArgs<Real> a)
         for (int d = 0; d < 3; ++d) pos[d] = da(da(G[d], dm(u, G[3 + d])), dm(w, G[6 + d]));
         double vel[3], irv;
         sample_inflow_velocity(gas, R, rs, vel, irv, a.errorWord);
-        const double dtl = rs.uniform64() * a.C.dtime;
+        double dtleft = rs.uniform64() * a.C.dtime;
         PRegs<Real> pr;
         int cell = pcell;
-        if constexpr (sizeof(Real) == 8) {
-            for (int d = 0; d < 3; ++d) pr.x[d] = pos[d];
-        } else {
-            const double* cc = a.M.cellCenter + (size_t)cell * 3;
-            for (int d = 0; d < 3; ++d) pr.x[d] = (float)(pos[d] - cc[d]);
-        }
+        for (int d = 0; d < 3; ++d) pr.x[d] = pos[d];
         for (int d = 0; d < 3; ++d) pr.v[d] = (Real)vel[d];
         pr.ir = (Real)irv;
-        Real dtleft = (Real)dtl;
         const int out = trace_particle<Real>(a.M, a.C, pr, cell, pedge, ptag, dtleft, rs, istep,
                                              a.wallTally, cnt, false, nullptr);
-        a.A.x[0][gi] = pr.x[0]; a.A.x[1][gi] = pr.x[1]; a.A.x[2][gi] = pr.x[2];
+        store_position(a.M, a.A, gi, cell, pr);
         a.A.v[0][gi] = pr.v[0]; a.A.v[1][gi] = pr.v[1]; a.A.v[2][gi] = pr.v[2];
         a.A.ir[gi] = pr.ir;
         a.A.cell[gi] = (out >= 0) ? cell : -1;
@@ -232,13 +258,13 @@ __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
     const int lane = threadIdx.x & 31;
     const unsigned lower = (1u << lane) - 1u;
     TraceCounts cnt{};
-    const Real dt0 = (Real)a.C.dtime;
+    const double dt0 = a.C.dtime;
     int chunkNext = 0, chunkEnd = 0;   // this warp's chunk (warp-uniform)
     bool exhausted = false;            // warp-uniform
     int i = -1;                        // this lane's particle
     PRegs<Real> p;
     int cell = 0;
-    Real dtleft = 0;
+    double dtleft = 0;
     TraceState st;
     Stream rs;
     uint32_t wallBefore = 0;
@@ -260,10 +286,10 @@ __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
             const bool mine = ((want >> lane) & 1u) && __popc(want & lower) < take;
             if (mine) {
                 i = chunkNext + __popc(want & lower);
-                p.x[0] = a.A.x[0][i]; p.x[1] = a.A.x[1][i]; p.x[2] = a.A.x[2][i];
+                cell = a.A.cell[i];
+                load_position(a.M, a.A, i, cell, p);
                 p.v[0] = a.A.v[0][i]; p.v[1] = a.A.v[1][i]; p.v[2] = a.A.v[2][i];
                 p.ir = a.A.ir[i];
-                cell = a.A.cell[i];
                 rs.init((uint32_t)i, (uint32_t)istep, kPurposeWall, a.C.seedLo, a.C.seedHi);
                 dtleft = dt0;
                 st.begin(-1, -1);
@@ -276,7 +302,7 @@ __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
         if (!__any_sync(kFull, active)) break;
         if (active && trace_step<Real>(a.M, a.C, p, cell, dtleft, st, rs, istep, a.wallTally, cnt, false, nullptr)) {
             if (st.ifout >= 0) {
-                a.A.x[0][i] = p.x[0]; a.A.x[1][i] = p.x[1]; a.A.x[2][i] = p.x[2];
+                store_position(a.M, a.A, i, cell, p);
                 if (cnt.wall != wallBefore) {
                     a.A.v[0][i] = p.v[0]; a.A.v[1][i] = p.v[1]; a.A.v[2][i] = p.v[2];
                     a.A.ir[i] = p.ir;
@@ -1590,6 +1616,52 @@ void launch_macro(const DevMesh& M, const DevConsts& C, const double* acc, int s
 }
 
 // ===========================================================================
+// particle upload from cell-major host arrays
+// ===========================================================================
+__global__ void upload_check_kernel(const int* __restrict__ cell, int n, int ncell, int* flags, int* start)
+{
+    int bad = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int c = cell[i];
+        const int prev = i > 0 ? cell[i - 1] : -1;
+        if (c < 0 || c >= ncell) { bad |= 1; continue; }
+        if (prev > c) { bad |= 2; continue; }
+        // cells prev+1 .. c begin at slot i (in range and ordered here; the
+        // host uses start only when no thread flagged anything)
+        const int lo = prev < 0 ? 0 : prev + 1;
+        for (int q = lo; q <= c; ++q) start[q] = i;
+        if (i == n - 1)
+            for (int q = c + 1; q <= ncell; ++q) start[q] = n;
+    }
+    if (bad) atomicOr(flags, bad);
+}
+
+void launch_upload_check(const int* cell, int n, int ncell, int* flags, int* start, cudaStream_t s)
+{
+    int g = (n + 255) / 256;
+    g = g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g);
+    upload_check_kernel<<<g, 256, 0, s>>>(cell, n, ncell, flags, start);
+}
+
+__global__ void upload_convert_kernel(const double* __restrict__ in, const int* __restrict__ cell,
+                                      const double* __restrict__ center, int comp, float* __restrict__ out, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double v = in[i];
+        if (comp < 3) v = v - center[(size_t)cell[i] * 3 + comp];
+        out[i] = (float)v;
+    }
+}
+
+void launch_upload_convert(const double* in, const int* cell, const double* center, int comp, float* out, int n,
+                           cudaStream_t s)
+{
+    int g = (n + 255) / 256;
+    g = g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g);
+    upload_convert_kernel<<<g, 256, 0, s>>>(in, cell, center, comp, out, n);
+}
+
+// ===========================================================================
 // tracing check (dsmc_trace)
 // ===========================================================================
 template <typename Real>
@@ -1602,13 +1674,18 @@ __global__ void trace_check_kernel(DevMesh M, DevConsts C, int n, const Real* px
     TraceCounts cnt{};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         PRegs<Real> p;
-        p.x[0] = px[i]; p.x[1] = py[i]; p.x[2] = pz[i];
+        int c = cell[i];
+        if constexpr (sizeof(Real) == 8) {
+            p.x[0] = px[i]; p.x[1] = py[i]; p.x[2] = pz[i];
+        } else {
+            const double* cc = M.cellCenter + (size_t)c * 3;
+            p.x[0] = da(cc[0], (double)px[i]); p.x[1] = da(cc[1], (double)py[i]); p.x[2] = da(cc[2], (double)pz[i]);
+        }
         p.v[0] = vx[i]; p.v[1] = vy[i]; p.v[2] = vz[i];
         p.ir = (Real)0;
-        int c = cell[i];
         Stream rs;
         rs.init((uint32_t)i, 0u, kPurposeWall, C.seedLo, C.seedHi);
-        Real dtleft = (Real)dt[i];
+        double dtleft = dt[i];
         TraceLog log{-1, 0, 0};
         const int out = trace_particle<Real>(M, C, p, c, -1, -1, dtleft, rs, 0, nullptr, cnt, stopAtWall != 0, &log);
         oCell[i] = (out == kTraceRemoved) ? -1 : c;
@@ -1616,9 +1693,15 @@ __global__ void trace_check_kernel(DevMesh M, DevConsts C, int n, const Real* px
         oFace[i] = log.hitFace;
         oTri[i] = log.hitTri;
         oNcross[i] = log.ncross;
-        ox[i] = p.x[0]; oy[i] = p.x[1]; oz[i] = p.x[2];
+        if constexpr (sizeof(Real) == 8) {
+            ox[i] = p.x[0]; oy[i] = p.x[1]; oz[i] = p.x[2];
+        } else {
+            // relative to the centre of the last cell the particle was in
+            const double* cc = M.cellCenter + (size_t)c * 3;
+            ox[i] = (float)ds(p.x[0], cc[0]); oy[i] = (float)ds(p.x[1], cc[1]); oz[i] = (float)ds(p.x[2], cc[2]);
+        }
         ovx[i] = p.v[0]; ovy[i] = p.v[1]; ovz[i] = p.v[2];
-        odt[i] = (double)dtleft;
+        odt[i] = dtleft;
         oLast[i] = c;   // cell the position is relative to (mixed precision)
     }
     flush_counts(counters, cnt);

@@ -121,6 +121,13 @@ template <typename Real> void launch_gsis_count(const StepArgs<Real>& a, const G
 // B from A: kept, copied, sampled and deleted particles, then the per-cell linear map
 template <typename Real> void launch_gsis_rebuild(const StepArgs<Real>& a, const GsisArgs& g, const LaunchShape& L,
                                                   cudaStream_t s);
+// Particle upload from cell-major host arrays: flags bit 0 a cell id outside
+// [0, ncell), bit 1 a cell id smaller than its predecessor's; when neither
+// is set, start[0..ncell] holds each cell's first slot.
+void launch_upload_check(const int* cell, int n, int ncell, int* flags, int* start, cudaStream_t s);
+// out[i] = (float)(in[i] - center[cell[i] * 3 + comp]) for comp < 3, else (float)in[i]
+void launch_upload_convert(const double* in, const int* cell, const double* center, int comp, float* out, int n,
+                           cudaStream_t s);
 template <typename Real> cudaError_t prepare_kernels();
 void launch_macro(const DevMesh& M, const DevConsts& C, const double* acc, int set, double count,
                   double* out, int ncell, cudaStream_t s);

@@ -65,6 +65,15 @@ outputs:
                  final velocity (float32) of those whose first hit is the
                  wall, after its diffuse re-emission; the same near the
                  capsule's wall ("tet_" keys)
+  trace_full_pin.npz the TRACE configuration: the reference's tracing
+                 check (stop at the first non-interface face) of 10^6
+                 particles on the full 48,640-cell block mesh
+                 (inputs.trace_inputs, seed 1), on the FP64 inputs ("fp64_"
+                 keys) and on the FP32-rounded state the mixed path stores
+                 ("mixed_" keys): SHA-256 digests of every output array
+                 (positions of the mixed run as the FP32 offsets from the
+                 final cell's centre widen back), final per-cell counts,
+                 outcome and hit counts, and 4,096 particles in full
   stats_band_capsule.npz the same band on the capsule tets (Kn 0.01), steps
                  61-120 of 8 seeded reference runs from 8 particles per
                  cell: float32 mean and spread of every third cell, and
@@ -542,9 +551,9 @@ def main():
         raise SystemExit("oracle/_ref/ref_harness missing: make -C oracle ref")
     want = set(sys.argv[1:])
     if want - {"gsis", "fill", "fluent", "pyramid", "prism", "band", "degenerate", "sample", "collide", "inject",
-               "wall", "capband", "core"}:
+               "wall", "capband", "core", "tracefull"}:
         raise SystemExit("fixtures: core (mesh, trace, advect, inflow, stats, tet trace), gsis, fill, fluent, pyramid, "
-                         "prism, band, degenerate, sample, collide, inject, wall, capband")
+                         "prism, band, degenerate, sample, collide, inject, wall, capband, tracefull")
     with tempfile.TemporaryDirectory() as d:
         if not want or want & {"gsis", "fill"}:
             gen_gsis_fill(d)
@@ -570,6 +579,8 @@ def main():
             gen_capband(d)
         if not want or "core" in want:
             gen_core(d)
+        if not want or "tracefull" in want:
+            gen_trace_full(d)
     print("fixtures written to", HERE)
 
 
@@ -638,6 +649,38 @@ def gen_core(d):
     r = H.trace(casc, messc, xt, vt, dtt, ct, True)
     np.savez_compressed(os.path.join(HERE, "tet_trace_pin.npz"), ncell=dmc.ncell,
                         **{k: r[k] for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt")})
+
+
+TRACE_FULL_SAMPLE = 4096
+
+
+def gen_trace_full(d):
+    """The TRACE configuration on the full block mesh, run through the
+    reference's tracing on the FP64 inputs and on their FP32-rounded state."""
+    raw, dm = I.block_mesh(scale=1)
+    cas = os.path.join(d, "b1.cas")
+    M.write_cas(cas, raw)
+    mess = I.block_mess(dm, STATS_PPC)
+    x, v, dt, cell = I.trace_inputs(dm, mess, I.TRACE_FULL_N, seed=I.TRACE_FULL_SEED)
+    x32, v32 = I.fp32_state(dm, x, v, cell)
+    rs = np.random.RandomState(77)
+    pick = np.sort(rs.choice(len(cell), TRACE_FULL_SAMPLE, replace=False)).astype(np.int32)
+    out = dict(ncell=dm.ncell, n=len(cell), seed=I.TRACE_FULL_SEED, pick=pick)
+    for tag, (xi, vi) in (("fp64", (x, v)), ("mixed", (x32, v32))):
+        r = H.trace(cas, mess, xi, vi, dt, cell, True, timeout=3600)
+        for k in ("cell", "ifout", "face", "tri", "ncross", "dt"):
+            out[f"{tag}_{k}_sha"] = np.array(I.digest(r[k]))
+        kept = r["cell"] >= 0
+        if tag == "fp64":
+            out["fp64_x_sha"] = np.array(I.digest(r["x"]))
+        else:
+            out["mixed_x_sha"] = np.array(I.digest(I.fp32_positions(dm, r["x"][kept], r["cell"][kept])))
+        out[f"{tag}_ppc"] = np.bincount(r["cell"][kept], minlength=dm.ncell).astype(np.int32)
+        out[f"{tag}_ifout_counts"] = np.array([np.sum(r["ifout"] == k) for k in (-1, 0, 1)], dtype=np.int64)
+        out[f"{tag}_hits"] = np.int64(np.sum(r["face"] >= 0))
+        for k in ("cell", "ifout", "face", "tri", "ncross", "x", "dt"):
+            out[f"{tag}_sample_{k}"] = r[k][pick]
+    np.savez_compressed(os.path.join(HERE, "trace_full_pin.npz"), **out)
 
 
 if __name__ == "__main__":

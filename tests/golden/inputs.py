@@ -79,6 +79,33 @@ def trace_inputs(dm, mess, n: int, seed: int):
     return x, v, dt, cells
 
 
+TRACE_FULL_N = 1_000_000   # the TRACE configuration: 10^6 particles on the full block mesh, one dt
+TRACE_FULL_SEED = 1
+
+
+def fp32_state(dm, x, v, cell):
+    """The state the mixed path stores for FP64 positions and velocities:
+    FP32 offsets from the cell centre and FP32 velocities, widened back to
+    FP64 the way the trace widens them (centre + offset)."""
+    cc = dm.cells["cellXY"][cell]
+    x32 = cc + (x - cc).astype(np.float32).astype(np.float64)
+    return x32, v.astype(np.float32).astype(np.float64)
+
+
+def fp32_positions(dm, x, cell):
+    """FP64 positions as the mixed path stores and returns them: the FP32
+    rounding of the offset from the centre of `cell`, widened again."""
+    cc = dm.cells["cellXY"][cell]
+    return cc + (x - cc).astype(np.float32).astype(np.float64)
+
+
+def digest(a) -> str:
+    """SHA-256 of an array's bytes (C order), for bit-exact comparisons of
+    outputs too large to store."""
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
 def split_box_trace_inputs(raw, mess, n: int, seed: int):
     """Uniform random points in the cubes of a ``pydsmc.mesh.pyramid_box`` or
     ``prism_box`` mesh, each with the cell of its cube that holds it (the

@@ -1,0 +1,52 @@
+"""Sampling on the B200 against the reference's own statistic_macro
+(tests/golden/sample_pin.npz, made by oracle/_ref/ref_harness's "sample"
+command).
+
+5,200 steps of a particle sequence with no random draws (inputs.sampled_at:
+thinned and rescaled particles; cells that hold one particle on two steps
+of each 100-step window), sampled by the library's statistic_macro stage
+alone: local (exponential window past NSCHEME), record (the GSIS window,
+with the sparse-cell state machine), final_record (steady average past
+NSS), the window samples and validity and the sparse states equal the
+reference's. The second pass writes the host's sparse-state decisions back
+after every exchange step through dsmc_upload_sparse_state (the
+write-back of ProcessGSIS::DSMC2NS, src/ProcessGSIS.cpp:1660-1674; the
+harness's host rule stands in for its decisions), as the coupled loop does.
+"""
+import numpy as np
+import pytest
+
+import inputs as I
+from conftest import golden
+from gpu_util import make_case
+from pydsmc import gpu
+
+pytestmark = pytest.mark.gpu
+
+STAGE_SAMPLE = 0x10
+
+
+@pytest.mark.parametrize("pre", ["", "rule_"])
+def test_sampling_and_sparse_write_back_match_the_reference(pre):
+    g = golden("sample_pin.npz")
+    raw, dm = I.block_mesh(scale=8)
+    ppc = int(g["ppc"])
+    mess = I.block_mess(dm, ppc)
+    x, v, ir, cell = I.fill_inputs(dm, mess, ppc, int(g["seed"]))
+    with make_case(dm, mess, nss=5000, nscheme=2000, nevery=1, nrepeat=100) as case:
+        case.statistic_macroPre()
+        for k in range(1, int(g["steps"]) + 1):
+            keep, s = I.sampled_at(k, cell, ppc)
+            case.upload_particles(x[keep], v[keep] * s, ir[keep] * (s * s), cell[keep])
+            case.step(k, STAGE_SAMPLE)
+            if pre and k % 100 == 0:
+                case.set_sparse_state(I.host_sparse_rule(case.counts()["sparse_state"], k))
+        for name, which in (("local", gpu.MACRO_LOCAL), ("record", gpu.MACRO_RECORD),
+                            ("final_record", gpu.MACRO_FINAL_RECORD)):
+            assert np.array_equal(case.macro(which), g[pre + name]), pre + name
+        cn = case.counts()
+        assert np.array_equal(cn["window_samples"], g[pre + "window_samples"])
+        assert np.array_equal(cn["window_valid"], g[pre + "window_valid"].astype(cn["window_valid"].dtype))
+        assert np.array_equal(cn["sparse_state"], g[pre + "sparse_state"])
+    if pre:
+        assert (g["rule_sparse_state"] == 2).sum() > 5

@@ -233,6 +233,32 @@ def test_oracle_collision_counts_within_reference_band(oracle_stats_run):
     assert mine["collisions"] > 50000
 
 
+def test_oracle_trace_config_full_block(oracle_lib):
+    """The TRACE configuration (10^6 particles on the full 48,640-cell block
+    mesh, one dt, stop at the first non-interface face): the oracle's
+    outputs are bit-exact with the reference's (SHA-256 digests of every
+    array in trace_full_pin.npz), on the FP64 inputs and on the FP32-rounded
+    state the mixed path stores."""
+    g = golden("trace_full_pin.npz")
+    raw, dm = I.block_mesh(scale=1)
+    mess = I.block_mess(dm, 20)
+    assert dm.ncell == int(g["ncell"])
+    x, v, dt, cell = I.trace_inputs(dm, mess, int(g["n"]), seed=int(g["seed"]))
+    o = oracle_lib.Oracle(dm, mess, OracleParams(I.REF_ZONES, I.inflow_dir()))
+    r = o.trace(x, v, dt, cell, stop_at_wall=True)
+    for k in ("cell", "ifout", "face", "tri", "ncross", "dt", "x"):
+        assert I.digest(r[k]) == str(g[f"fp64_{k}_sha"]), k
+    x32, v32 = I.fp32_state(dm, x, v, cell)
+    r = o.trace(x32, v32, dt, cell, stop_at_wall=True)
+    for k in ("cell", "ifout", "face", "tri", "ncross", "dt"):
+        assert I.digest(r[k]) == str(g[f"mixed_{k}_sha"]), k
+    kept = r["cell"] >= 0
+    assert I.digest(I.fp32_positions(dm, r["x"][kept], r["cell"][kept])) == str(g["mixed_x_sha"])
+    assert np.array_equal(np.bincount(r["cell"][kept], minlength=dm.ncell), g["mixed_ppc"])
+    # every outcome and many boundary hits
+    assert np.all(g["fp64_ifout_counts"] > 10000) and int(g["fp64_hits"]) > 10000
+
+
 def test_oracle_degenerate_trace_vs_reference(block, oracle_lib):
     """Exact paths through face centres (on the quads' split diagonals),
     edges and vertices, starts on faces, edges and corners, particles at
