@@ -2,19 +2,18 @@
 // not allocate device memory.
 //
 // Some hosts cannot call cudaMalloc at the point where they want to run a
-// check: a caller that is recording the work into a CUDA graph (allocation
-// calls are not allowed inside a stream capture), a solver that reserved the
-// whole device up front for its own memory pool, or a coupling loop that
-// forbids allocation after start-up so its memory footprint stays fixed.
-// dsmc_trace stages its host arrays in device buffers it allocates for each
-// call; this variant stages them in one file-scope device array instead, so
-// the call itself allocates nothing on the device or the host.
+// check: a solver that reserved the whole device up front for its own memory
+// pool, or a coupling loop that forbids allocation after start-up so its
+// memory footprint stays fixed. dsmc_trace stages its host arrays in device
+// buffers it allocates for each call; this variant stages them in one
+// file-scope device array instead, so the call makes no device allocation.
+// Its messages are formatted into a fixed buffer; no C++ exception leaves it.
 #include "dsmc_gpu.h"
 #include "dsmc_kernels.cuh"
 
+#include <cstdio>
 #include <cstring>
 #include <mutex>
-#include <string>
 
 namespace dsmc {
 DevMesh engine_mesh(const DsmcHandle* h);
@@ -23,7 +22,7 @@ int engine_precision(const DsmcHandle* h);
 int engine_device(const DsmcHandle* h);
 cudaStream_t engine_stream(const DsmcHandle* h);
 unsigned long long* engine_counters(const DsmcHandle* h);
-void engine_set_error(DsmcHandle* h, const char* msg);
+void engine_set_error(DsmcHandle* h, const char* msg) noexcept;
 }  // namespace dsmc
 
 namespace {
@@ -42,13 +41,25 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setupMutex;
 unsigned char* g_scratchPtr[kMaxDevices] = {};
 
+void set_cuda_error(DsmcHandle* h, const char* what, cudaError_t e) noexcept
+{
+    char msg[256];
+    std::snprintf(msg, sizeof msg, "dsmc_trace_noalloc: %s: %s", what, cudaGetErrorString(e));
+    dsmc::engine_set_error(h, msg);
+}
+
 // The address of g_trace_scratch as a device pointer, found once per device
 // with that device current (the host-side name of the array is only a
 // stand-in and must not be passed to a kernel).
-cudaError_t scratch_for_device(int dev, unsigned char** out)
+cudaError_t scratch_for_device(int dev, unsigned char** out) noexcept
 {
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_setupMutex);
+    std::unique_lock<std::mutex> lock(g_setupMutex, std::defer_lock);
+    try {
+        lock.lock();
+    } catch (...) {
+        return cudaErrorUnknown;
+    }
     if (!g_scratchPtr[dev]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_trace_scratch);
@@ -114,11 +125,15 @@ extern "C" int dsmc_trace_noalloc(DsmcHandle* h, int64_t n, const double* px, co
             return DSMC_E_INVALID;
         }
     const int dev = dsmc::engine_device(h);
-    cudaSetDevice(dev);
-    unsigned char* base = nullptr;
-    cudaError_t e = scratch_for_device(dev, &base);
+    cudaError_t e = cudaSetDevice(dev);
     if (e != cudaSuccess) {
-        dsmc::engine_set_error(h, (std::string("dsmc_trace_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e)).c_str());
+        set_cuda_error(h, "cudaSetDevice", e);
+        return DSMC_E_CUDA;
+    }
+    unsigned char* base = nullptr;
+    e = scratch_for_device(dev, &base);
+    if (e != cudaSuccess) {
+        set_cuda_error(h, "cudaGetSymbolAddress", e);
         return DSMC_E_CUDA;
     }
     const int ni = (int)n;
@@ -178,7 +193,7 @@ extern "C" int dsmc_trace_noalloc(DsmcHandle* h, int64_t n, const double* px, co
         if (hd[k]) e = cudaMemcpyAsync(hd[k], dOut + (size_t)k * N, N * 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
-        dsmc::engine_set_error(h, (std::string("dsmc_trace_noalloc: ") + cudaGetErrorString(e)).c_str());
+        set_cuda_error(h, "copy or launch", e);
         return DSMC_E_CUDA;
     }
     return DSMC_OK;

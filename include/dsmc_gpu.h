@@ -339,19 +339,21 @@ int dsmc_trace(DsmcHandle* h, int64_t n,
                double* out_px, double* out_py, double* out_pz,
                double* out_vx, double* out_vy, double* out_vz, double* out_dt);
 
-/* Tracing check for callers that cannot allocate device memory: a caller
- * recording its work into a CUDA graph (allocation is not allowed during a
- * stream capture), or a solver that reserved the whole device for its own
- * memory pool, or a coupling loop that forbids allocation after start-up.
- * Same arguments and results as dsmc_trace, but the host arrays are staged
- * in one static device array of the library instead of in buffers
- * allocated per call: no cudaMalloc, cudaFree or other allocation happens in
- * the call. Limits and caveats:
+/* Tracing check for callers that cannot allocate device memory at the
+ * call site: a solver that reserved the whole device for its own memory
+ * pool, or a coupling loop that forbids allocation after start-up so that
+ * its memory footprint stays fixed. Same arguments and results as
+ * dsmc_trace, but the host arrays are staged in one static device array of
+ * the library instead of in buffers allocated per call: the call makes no
+ * device allocation (no cudaMalloc, cudaFree or allocating library routine);
+ * only its error paths format a message on the host. Limits and caveats:
  *   - n <= DSMC_NOALLOC_MAX_TRACE particles per call (larger n is rejected
- *     with DSMC_E_INVALID); the array takes about 7.3 MB on every GPU that
- *     loads the library, until the process exits.
+ *     with DSMC_E_INVALID); the array takes 7.74 MB (7,737,344 bytes) on
+ *     every GPU that loads the library, until the process exits.
  *   - The first call on a device looks up the array's device address (with
  *     that device current); make that first call before any stream capture.
+ *   - The call copies from and to the caller's host arrays on the handle's
+ *     stream and synchronises that stream before it returns.
  *   - All calls on a device share the array: calls whose work overlaps on the
  *     GPU (other streams, other host threads) race; serialise them.
  * No counterpart in the reference: it is an addition of this library. */
