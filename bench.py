@@ -8,9 +8,13 @@ the library's stream, max over ranks). Mixed precision is the production
 path; the all-FP64 path is timed on the same case for the mixed/FP64 ratio.
 
 Default workload: the capsule case (Ma 5, Kn 0.01, AoA 30 deg) on the
-generated 371,214-tet mesh at 100 particles per cell (37.1M particles);
---workload block runs the 48,640-hex block case (200 particles per cell by
-default).
+generated 372,500-tet mesh at a mean of 100 particles per cell (37.25M
+particles), run for its 2,000 steps with the served sampling rule (NSCHEME
+at 20% of the steps, NSS at 50%) and the wall statistics on; the K timed
+steps follow a spin-up to NSS and the W warm-up steps. Both precisions run
+the whole case from the same host particles; the mixed run's fields are
+compared with the FP64 run's per field. --workload block runs the
+48,640-hex block case (200 particles per cell by default, 500 steps).
 
 Multi-GPU runs are independent replicas (one case per GPU, no collective on
 the data path): value = the sum of all ranks' particle-steps / the slowest
@@ -207,48 +211,142 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # our implementation
 # ---------------------------------------------------------------------------
-def run_case(wl, fill, precision, steps, warmup, seed, timing=False):
+def run_plan(wl, args) -> dict:
+    """The case's run: the configuration's step count (2,000 on the capsule,
+    500 on the block), with the served sampling rule (the exponential window
+    NSCHEME from 20% of the steps, steady sampling NSS from 50%). The timed
+    steps follow a spin-up to NSS and the warm-up steps, so they see the
+    developed flow (shock layer, wake) and every sampler running."""
+    total = args.run_steps if args.run_steps else (2000 if wl["name"] == "capsule" else 500)
+    total = max(total, args.warmup + args.steps)
+    nss, nscheme = total // 2, max(1, total // 5)
+    spin = min(nss, total - args.warmup - args.steps)
+    return {"total": total, "nss": nss, "nscheme": nscheme, "spinup": spin, "exchange_every": 100}
+
+
+def bench_config(wl, plan) -> dict:
+    """The workload as both arms report it."""
+    dm = wl["dm"]
+    return dict(wl["desc"], steps_run=plan["total"], nss=plan["nss"], nscheme=plan["nscheme"], wall_stats=True,
+                particles_nominal=int(round(wl["desc"]["ppc"] * dm.ncell)),
+                l2="inputs larger than L2 (particle state >= 1.2 GB per step)")
+
+
+def case_params(wl, plan, precision, seed):
+    from pydsmc import gpu
+    return gpu.default_params(precision=precision, seed=seed, zones=wl["zones"], inflow_dir=wl["inflow_dir"],
+                              nss=plan["nss"], nscheme=plan["nscheme"], nrepeat=plan["exchange_every"],
+                              wall_stats=1)
+
+
+def pinned_copy(a):
+    """A numpy array in page-locked host memory (the host buffers a caller
+    hands to the C ABI)."""
+    import torch
+    dt = {np.dtype(np.float64): torch.float64, np.dtype(np.int32): torch.int32}[np.asarray(a).dtype]
+    t = torch.empty(np.asarray(a).shape, dtype=dt, pin_memory=True)
+    out = t.numpy()
+    out[...] = a
+    return out
+
+
+def initial_state(wl, plan, args, rank):
+    """The initial particles as host arrays (the reference's fill rule: a mean
+    of ppc per cell in proportion to the cell volumes, freestream
+    velocities; drawn on the device and read back), in pinned memory, and
+    the launch shapes the autotuner keeps on this case."""
     import torch
     from pydsmc import gpu
-    p = gpu.default_params(precision=precision, seed=seed, zones=wl["zones"], inflow_dir=wl["inflow_dir"],
-                           nss=10 ** 9, nscheme=max(1, (steps + warmup) // 5), nrepeat=100)
-    case = gpu.Case(wl["dm"], wl["mess"], p, device=torch.cuda.current_device())
-    if "device" in fill:
-        case.fill_freestream(*fill["device"])
-    else:
-        case.upload_particles(fill["x"], fill["v"], fill["ir"], fill["cell"])
-    case.statistic_macroPre()
-    # launch shapes picked on this case (ordinary steps; results do not
-    # depend on them), then the warm-up steps
-    istep, _ = case.autotune(1, trial_steps=1)
-    istep -= 1
-    for _ in range(warmup):
-        istep += 1
-        case.step(istep)
-    case.sync()
+    case = gpu.Case(wl["dm"], wl["mess"], case_params(wl, plan, gpu.PRECISION_MIXED, 1000 + rank),
+                    device=torch.cuda.current_device())
+    case.fill_freestream(float(args.ppc), 1000 + rank)
+    hx, hv, hir, hcell = case.download_particles()
+    cols = [pinned_copy(np.ascontiguousarray(hx[:, k])) for k in range(3)] + \
+           [pinned_copy(np.ascontiguousarray(hv[:, k])) for k in range(3)] + [pinned_copy(hir), pinned_copy(hcell)]
+    shape = None
+    if not args.no_autotune:
+        case.statistic_macroPre()
+        _, shape = case.autotune(1, trial_steps=1)
+    case.close()
+    return cols, shape
+
+
+def full_run(wl, plan, args, precision, init, shape, rank, barrier, clock_index=None, stage_steps=0):
+    """One run of the case through the C ABI: the host arrays uploaded,
+    steps 1..total, the GSIS hand-off at every exchange step after NSS (the
+    window-averaged `record` fields and the particle count read back), the
+    sampled fields at the end. Wall time of all of it is the run's
+    end-to-end figure; steps spinup+warmup+1 .. +steps are timed on the
+    device with CUDA events (barrier and synchronise on both sides)."""
+    import torch
+    from pydsmc import gpu
+    case = gpu.Case(wl["dm"], wl["mess"], case_params(wl, plan, precision, 1000 + rank),
+                    device=torch.cuda.current_device())
+    if shape:
+        case.set_launch_shape(**shape)
     stream = torch.cuda.ExternalStream(case.lib.dsmc_stream(case.h))
-    n_before = []
-    case.set_timing(timing)
-    case.stage_ms(reset=True)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    counts = []
-    # particle counts are device-resident; read them at the end from the counters
-    c0 = case.counters()
-    n0 = case.particle_count()
-    ev0.record(stream)
-    for _ in range(steps):
-        istep += 1
+    first = plan["spinup"] + args.warmup + 1
+    last = first + args.steps - 1
+    windows, nsamp = [], []
+    h2d = sum(int(c.nbytes) for c in init)
+    d2h = 0
+    res = {}
+    barrier()
+    t0 = time.perf_counter()
+    case.upload_columns(*init)
+    case.statistic_macroPre()
+    n = case.particle_count()
+    nsamp.append((0, n))
+    for istep in range(1, plan["total"] + 1):
+        if istep == first:
+            case.sync()
+            barrier()
+            res["n0"] = case.particle_count()
+            res["c0"] = case.counters()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            clk = ClockSampler(clock_index) if clock_index is not None else None
+            if clk:
+                clk.__enter__()
+            ev0.record(stream)
         case.step(istep)
-    ev1.record(stream)
-    ev1.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    c1 = case.counters()
-    n1 = case.particle_count()
-    stage = case.stage_ms(reset=True) if timing else None
+        if istep == last:
+            ev1.record(stream)
+            ev1.synchronize()
+            if clk:
+                clk.__exit__()
+                res["clocks"] = clk.summary()
+            barrier()
+            res["ms"] = ev0.elapsed_time(ev1)
+            res["n1"] = case.particle_count()
+            res["c1"] = case.counters()
+        if istep % plan["exchange_every"] == 0:
+            n = case.particle_count()
+            nsamp.append((istep, n))
+            d2h += 8
+            if istep > plan["nss"]:
+                windows.append(case.macro(gpu.MACRO_RECORD))
+                d2h += windows[-1].nbytes
+    final = case.macro(gpu.MACRO_FINAL_RECORD)
+    d2h += final.nbytes
     case.sync()
-    res = {"ms": ms, "n0": n0, "n1": n1, "counters0": c0, "counters1": c1, "stage": stage, "istep": istep,
-           "case": case}
+    wall = time.perf_counter() - t0
+    # particle-steps of the run: the inventory read at each exchange, between
+    # two reads the mean of the two
+    ps = 0.0
+    for (sa, na), (sb, nb) in zip(nsamp, nsamp[1:]):
+        ps += 0.5 * (na + nb) * (sb - sa)
+    if nsamp[-1][0] < plan["total"]:
+        ps += nsamp[-1][1] * (plan["total"] - nsamp[-1][0])
+    res.update(case=case, windows=np.stack(windows) if windows else None, final=final, wall_s=wall,
+               particle_steps=ps, h2d=h2d, d2h=d2h, counters_end=case.counters())
+    if stage_steps:
+        case.set_timing(True)
+        case.stage_ms(reset=True)
+        for k in range(stage_steps):
+            case.step(plan["total"] + 1 + k)
+        ms, nst = case.stage_ms(reset=True)
+        case.set_timing(False)
+        res["stage"] = ms / max(nst, 1)
     return res
 
 
@@ -265,16 +363,10 @@ def over_ranks(x: float, op: str, device: str) -> float:
     return float(t.item())
 
 
-def particle_steps(res, steps):
-    # particles at the start of each timed step: n0 + injected - removed... use the
-    # inventory at both ends (the inventory drifts slowly) times the step count
-    return 0.5 * (res["n0"] + res["n1"]) * steps
-
-
 def run_ours(args):
     import torch
     import torch.distributed as dist
-    from pydsmc import gpu
+    from pydsmc import fields, gpu
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -286,10 +378,8 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
     gpu.load()
     wl = make_workload(args.workload, args.ppc)
-    dm, mess = wl["dm"], wl["mess"]
-    # the reference's initial state: a mean of ppc particles per cell in
-    # proportion to the cell volumes, drawn on the device
-    fill = {"device": (float(args.ppc), 1000 + rank)}
+    dm = wl["dm"]
+    plan = run_plan(wl, args)
 
     def barrier():
         if world > 1:
@@ -303,41 +393,34 @@ def run_ours(args):
         return over_ranks(x, "sum", "cuda")
 
     peak, peak_kind = load_peaks()
-    # --- headline: mixed precision, graph replay
-    barrier()
-    with ClockSampler(local) as clk:
-        mixed = run_case(wl, fill, gpu.PRECISION_MIXED, args.steps, args.warmup, seed=1000 + rank)
-    barrier()
+    init, shape = initial_state(wl, plan, args, rank)
+    # --- mixed precision: the full run, the headline steps timed inside it
+    mixed = full_run(wl, plan, args, gpu.PRECISION_MIXED, init, shape, rank, barrier, clock_index=local,
+                     stage_steps=max(3, args.steps // 2))
     ms_mixed = max_over_ranks(mixed["ms"])
-    ps_mixed = sum_over_ranks(particle_steps(mixed, args.steps))
+    ps_mixed = sum_over_ranks(0.5 * (mixed["n0"] + mixed["n1"]) * args.steps)
     value = ps_mixed / (ms_mixed / 1e3)
     case_m = mixed.pop("case")
-    nparts = int(mixed["n0"])
-    # --- the GSIS particle update on the same case (between steps): an NS
-    # state of +-10% density around the current counts, drift and
-    # temperatures perturbed around the freestream; host wall time of the
-    # call (NS upload, count pass and scan, one read-back, rebuild)
+    # --- the GSIS particle update on the developed case (between steps)
     gsis = gsis_timing(case_m, wl, seed=3000 + rank)
-    # --- stage timing pass (events between stages, no graph) for the roofline
-    barrier()
-    tim = run_case(wl, fill, gpu.PRECISION_MIXED, max(3, args.steps // 2), 1, seed=2000 + rank, timing=True)
-    tim.pop("case").close()
-    stage_ms, tsteps = tim["stage"]
-    stage_avg = stage_ms / max(tsteps, 1)
-    # --- FP64 path on the same case
-    barrier()
-    fp64 = run_case(wl, fill, gpu.PRECISION_FP64, args.steps, args.warmup, seed=1000 + rank)
-    fp64.pop("case").close()
-    barrier()
-    ms_fp64 = max_over_ranks(fp64["ms"])
-    ps_fp64 = sum_over_ranks(particle_steps(fp64, args.steps))
-    value_fp64 = ps_fp64 / (ms_fp64 / 1e3)
-    # --- e2e through the C ABI with host buffers
-    barrier()
-    e2e = run_e2e(wl, fill, args, rank)
-    e2e_ms = max_over_ranks(e2e["ms"])
-    e2e_ps = sum_over_ranks(e2e["particle_steps"])
     case_m.close()
+    # --- the all-FP64 path: the same run from the same host particles
+    barrier()
+    fp64 = full_run(wl, plan, args, gpu.PRECISION_FP64, init, None, rank, barrier)
+    fp64.pop("case").close()
+    ms_fp64 = max_over_ranks(fp64["ms"])
+    ps_fp64 = sum_over_ranks(0.5 * (fp64["n0"] + fp64["n1"]) * args.steps)
+    value_fp64 = ps_fp64 / (ms_fp64 / 1e3)
+    field_err = fields.compare_windows(mixed["windows"], fp64["windows"], dm.cells["area"]) \
+        if mixed["windows"] is not None and fp64["windows"] is not None else None
+    # --- end to end over K steps only: upload, K steps, counters every step,
+    # the sampled fields at the end
+    barrier()
+    e2e_k = run_e2e_k(wl, plan, args, init, shape, rank)
+    e2e_full_s = max_over_ranks(mixed["wall_s"])
+    e2e_full_ps = sum_over_ranks(mixed["particle_steps"])
+    e2e_k_s = max_over_ranks(e2e_k["s"])
+    e2e_k_ps = sum_over_ranks(e2e_k["particle_steps"])
 
     tri_per_cell = 12.0 if wl["name"] == "block" else 4.0
     n_mean = 0.5 * (mixed["n0"] + mixed["n1"])
@@ -345,12 +428,15 @@ def run_ours(args):
     names = ["inject", "move", "sort", "collide", "sample"]
     kernels = {"inject": "inject_gen_kernel", "move": "move_kernel", "sort": "gather_kernel",
                "collide": "collide_kernel", "sample": "sample_kernel"}
+    stage_avg = mixed["stage"]
     dom = names[int(np.argmax(stage_avg))]
     dom_ms = float(stage_avg[names.index(dom)])
     dom_bytes = ab.get(dom)
     achieved = (dom_bytes / (dom_ms / 1e3)) / 1e9 if (dom_bytes and dom_ms > 0) else None
     traffic, traffic_src = measured_traffic(kernels[dom], wl["desc"]["workload"] + f"_ppc{args.ppc}", n_mean)
     step_achieved = (ab["step"] / (ms_mixed / args.steps / 1e3)) / 1e9
+    cnt = {k: mixed["c1"][k] - mixed["c0"][k] for k in mixed["c1"]}
+    searches = n_mean * args.steps + cnt["crossings"]
     line = {
         "metric": METRIC,
         "value": value,
@@ -363,11 +449,15 @@ def run_ours(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32+f64acc",
-        "data": "synthetic (generated mesh; device initial fill: the reference's per-cell counts and placement, freestream velocities)",
-        "config": dict(wl["desc"], particles_per_gpu=nparts, parallelism=f"replicas x{world}",
-                       l2="particle state > L2 (126 MB)", precision="mixed"),
+        "data": "synthetic (generated mesh; initial state: the reference's per-cell counts and placement with "
+                "freestream velocities, drawn on the device and handed to the run as host arrays)",
+        "config": bench_config(wl, plan),
+        "timed_steps": [plan["spinup"] + args.warmup + 1, plan["spinup"] + args.warmup + args.steps],
+        "particles": {"at_timed_start": int(mixed["n0"]), "initial": int(init[-1].shape[0]),
+                      "parallelism": f"replicas x{world}"},
         "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / args.steps, "dtype": "f64"},
         "mixed_over_fp64": value / value_fp64 if value_fp64 > 0 else None,
+        "field_error_vs_fp64": field_err,
         "stage_ms_per_step": dict(zip(names, [float(x) for x in stage_avg])),
         "roofline": {"bound": "hbm", "kernel": kernels[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
@@ -375,16 +465,27 @@ def run_ours(args):
                      "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
                      "step": {"algorithmic_bytes": ab["step"], "achieved": step_achieved,
                               "frac": step_achieved / peak}},
-        "e2e": {"value": e2e_ps / (e2e_ms / 1e3), "unit": "particle-steps/s",
-                "h2d_bytes_per_step": e2e["h2d"] / args.steps, "d2h_bytes_per_step": e2e["d2h"] / args.steps},
-        "gpu_launches": None,
+        "e2e": {"value": e2e_full_ps / e2e_full_s, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": mixed["h2d"] / plan["total"], "d2h_bytes_per_step": mixed["d2h"] / plan["total"],
+                "how": f"the whole {plan['total']}-step run through the C ABI: host arrays (pinned) uploaded, every "
+                       f"step, the record fields and the particle count read at every exchange step, the final "
+                       f"fields read; wall time",
+                "k_steps": {"value": e2e_k_ps / e2e_k_s, "steps": args.steps,
+                            "h2d_bytes_per_step": e2e_k["h2d"] / args.steps,
+                            "d2h_bytes_per_step": e2e_k["d2h"] / args.steps,
+                            "how": "upload of the host arrays, K steps with the counters read after each, the "
+                                   "local fields read; wall time"}},
+        "gpu_launches": launches_per_step(wl) * args.steps,
         "gsis_update": gsis,
-        "clocks": clk.summary(),
-        "counters": {k: mixed["counters1"][k] - mixed["counters0"][k] for k in mixed["counters1"]},
+        "clocks": mixed.get("clocks"),
+        "counters": cnt,
+        "fp64_fallback_rate": cnt["fp64_fallbacks"] / searches if searches else None,
     }
-    line["gpu_launches"] = launches_per_step(wl) * args.steps
+    if not args.no_forms:
+        barrier()
+        line["forms"] = short_forms(args, rank)
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(wl, fill, args)
+        line["cpu_baseline"] = cpu_baseline(wl, plan, args)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -421,67 +522,91 @@ def launches_per_step(wl) -> int:
     return 3 + 1 + 6 + 2 + 1
 
 
-def run_e2e(wl, fill, args, rank):
-    """The same step count through the C ABI with host buffers: upload the
-    particles from host memory, run the steps, read each step's counters
-    and the sampled fields (the GSIS hand-off, [cell][18] FP64) back."""
+def run_e2e_k(wl, plan, args, init, shape, rank):
+    """K steps end to end through the C ABI: upload the host arrays
+    (pinned), run the steps, read each step's counters and the sampled
+    fields ([cell][18] FP64) back; wall time. The graphs are warmed by W
+    steps on the same case before the timed region."""
     import torch
     from pydsmc import gpu
-    p = gpu.default_params(precision=gpu.PRECISION_MIXED, seed=3000 + rank, zones=wl["zones"],
-                           inflow_dir=wl["inflow_dir"], nss=10 ** 9, nscheme=100, nrepeat=100)
-    case = gpu.Case(wl["dm"], wl["mess"], p, device=torch.cuda.current_device())
-    # the same initial particles as host arrays (made on the device, read
-    # back before the timed region); the graph is warmed on them
-    case.fill_freestream(*fill["device"])
-    hx, hv, hir, hcell = case.download_particles()
-    # the C ABI's layout: one contiguous column per coordinate
-    cols = [np.ascontiguousarray(hx[:, k]) for k in range(3)] + [np.ascontiguousarray(hv[:, k]) for k in range(3)]
+    case = gpu.Case(wl["dm"], wl["mess"], case_params(wl, plan, gpu.PRECISION_MIXED, 3000 + rank),
+                    device=torch.cuda.current_device())
+    if shape:
+        case.set_launch_shape(**shape)
+    case.upload_columns(*init)
+    case.statistic_macroPre()
     for s in range(1, args.warmup + 1):
         case.step(s)
     case.sync()
     t0 = time.perf_counter()
-    case.upload_columns(*cols, hir, hcell)
+    case.upload_columns(*init)
     n0 = case.particle_count()
-    h2d = int(n0) * (7 * 8 + 4)
+    h2d = sum(int(c.nbytes) for c in init)
     d2h = 0
     total = 0
     for s in range(args.warmup + 1, args.warmup + args.steps + 1):
         case.step(s)
-        c = case.counters()
+        case.counters()
         d2h += 12 * 8
         total += n0
     local = case.macro(gpu.MACRO_LOCAL)
     d2h += local.nbytes
     case.sync()
-    ms = (time.perf_counter() - t0) * 1e3
+    sec = time.perf_counter() - t0
     case.close()
-    return {"ms": ms, "particle_steps": total, "h2d": h2d, "d2h": d2h}
+    return {"s": sec, "particle_steps": total, "h2d": h2d, "d2h": d2h}
 
 
-def cpu_baseline(wl, fill, args):
+def reference_roles(wl) -> str:
+    roles = {1: "interface", 2: "inlet", 3: "outlet", 4: "wall", 5: "none", 0: "none"}
+    return ",".join(f"{t}:{roles[r]}" for t, r, _ in wl["zones"])
+
+
+def reference_bench(wl, args, nproc: int, nsteps: int, seed0: int) -> dict:
+    """The reference's own step (oracle/_ref) on the full case: nproc
+    independent single-rank processes at once, each filling the case with
+    the reference's own initial fill (a mean of ppc particles per cell in
+    proportion to the volumes, moved to the freestream) and running nsteps
+    steps; the first step of each is its warm-up, the rest are timed."""
+    sys.path.insert(0, ROOT)
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import harness as H
+    dm, mess = wl["dm"], wl["mess"]
+    u, _, tN = W.freestream(mess, wl["inflow_dir"])
+    r_arg = reference_roles(wl)
+    with tempfile.TemporaryDirectory() as d:
+        cas = os.path.join(d, "case.cas")
+        M.write_cas(cas, dm.raw)
+        counts = [W.proportional_counts(dm, float(args.ppc), np.random.default_rng(seed0 + k)) for k in range(nproc)]
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=nproc) as ex:
+            futs = [ex.submit(H.bench, cas, mess, counts[k], nsteps, seed0 + k, r_arg, u, tN, 3600)
+                    for k in range(nproc)]
+            res = [f.result() for f in futs]
+        wall = time.perf_counter() - t0
+    rates = []
+    for r in res:
+        sec = r["step_seconds"][1:] if nsteps > 1 else r["step_seconds"]
+        parts = r["step_particles"][1:] if nsteps > 1 else r["step_particles"]
+        rates.append(sum(parts) / sum(sec))
+    return {"value": float(sum(rates)), "per_process": rates, "particles": [r["particles"] for r in res],
+            "fill_s": [r["fill_seconds"] for r in res], "wall_s": wall,
+            "step_s": [r["step_seconds"] for r in res]}
+
+
+def cpu_baseline(wl, plan, args):
     """The reference's own DSMC step (oracle/_ref, one compute rank = one
-    core) on a bounded sample: the same mesh and constants with a reduced
-    particle count, a few steps."""
+    core) on the full case: its own fill, one warm-up step, one timed step."""
     sys.path.insert(0, ROOT)
     from oracle import harness as H
     if not H.available():
         return {"value": None, "unit": "particle-steps/s", "cores": 1, "kind": "reference",
                 "sample": "unavailable: oracle/_ref/ref_harness not built"}
-    dm, mess = wl["dm"], wl["mess"]
-    ppc_s = max(2, min(args.ppc, 10))
-    sub = W.initial_fill(dm, mess, ppc_s, seed=7, inflow_dir=wl["inflow_dir"], proportional=True)
-    nsteps = 5
-    roles = {1: "interface", 2: "inlet", 3: "outlet", 4: "wall", 5: "none", 0: "none"}
-    r_arg = ",".join(f"{t}:{roles[r]}" for t, r, _ in wl["zones"])
-    with tempfile.TemporaryDirectory() as d:
-        cas = os.path.join(d, "case.cas")
-        M.write_cas(cas, wl["dm"].raw)
-        r = H.run(cas, mess, sub["x"], sub["v"], sub["ir"], sub["cell"], nsteps, 1, r_arg, nsteps + 1, timeout=600)
-    t = r["timing"]
-    return {"value": t["particle_steps_per_s"], "unit": "particle-steps/s", "cores": 1, "kind": "reference",
-            "sample": f"{wl['desc']['workload']} mesh, {ppc_s} particles/cell on average in proportion to the cell "
-                      f"volumes ({len(sub['cell'])} particles), "
-                      f"{nsteps} steps, {t['seconds']:.2f} s of one core"}
+    r = reference_bench(wl, args, 1, 2, 7)
+    return {"value": r["value"], "unit": "particle-steps/s", "cores": 1, "kind": "reference",
+            "sample": f"the full {wl['desc']['workload']} case ({r['particles'][0]} particles from the reference's "
+                      f"own fill, moved to the freestream), one warm-up step and one timed step "
+                      f"({r['step_s'][0][-1]:.1f} s) on one core"}
 
 
 # ---------------------------------------------------------------------------
@@ -538,20 +663,16 @@ def make_batch_cases(specs, precision, autotune=True):
     return cases, steps
 
 
-def run_batch(args):
-    """The batched form: args.cases cases (batch_specs), autotuned, advanced
-    (a) one after another, each by its own per-step graph, and (b) together,
-    one CUDA graph per step whose branches are the cases. value = total
-    particle-steps / device time of (b)."""
+def batch_leg(specs, K, W0, autotune=True, clock_index=None) -> dict:
+    """The batched form on the given cases (batch_specs), autotuned,
+    advanced (a) one after another, each by its own per-step graph, and (b)
+    together, one CUDA graph per step whose branches are the cases; device
+    time of each (CUDA events)."""
     import torch
     from pydsmc import gpu
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    gpu.load()
-    specs = batch_specs(args.cases, args.batch_seed)
     t0 = time.perf_counter()
-    cases, steps = make_batch_cases(specs, gpu.PRECISION_MIXED, autotune=not args.no_autotune)
+    cases, steps = make_batch_cases(specs, gpu.PRECISION_MIXED, autotune=autotune)
     setup_s = time.perf_counter() - t0
-    K, W0 = args.steps, args.warmup
     # (a) one after another: device time summed over the cases
     seq_ms, seq_ps = 0.0, 0.0
     for j, case in enumerate(cases):
@@ -576,12 +697,16 @@ def run_batch(args):
     batch.sync()
     bs = torch.cuda.ExternalStream(batch.stream())
     n0 = sum(c.particle_count() for c in cases)
-    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(bs)
-        batch.step(K)
-        e1.record(bs)
-        e1.synchronize()
+    clk = ClockSampler(clock_index) if clock_index is not None else None
+    if clk:
+        clk.__enter__()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(bs)
+    batch.step(K)
+    e1.record(bs)
+    e1.synchronize()
+    if clk:
+        clk.__exit__()
     b_ms = e0.elapsed_time(e1)
     batch.sync()
     n1 = sum(c.particle_count() for c in cases)
@@ -591,23 +716,38 @@ def run_batch(args):
     for c in cases:
         c.close()
     cells = [batch_mesh_cells(sp["k"]) for sp in specs]
+    return {"value": b_ps / (b_ms / 1e3), "ms_per_step": b_ms / K, "particles": int(n0),
+            "sequential": {"value": seq_ps / (seq_ms / 1e3), "ms_per_step": seq_ms / K,
+                           "how": "each case on its own, one after another, its own per-step graph"},
+            "batch_over_sequential": (b_ps / (b_ms / 1e3)) / (seq_ps / (seq_ms / 1e3)),
+            "cases": len(specs), "cells_total": int(sum(cells)), "cells_range": [int(min(cells)), int(max(cells))],
+            "setup_s": setup_s, "move_threads_chosen": sorted({s["move_threads"] for s in shapes}),
+            "clocks": clk.summary() if clk else None}
+
+
+def run_batch(args):
+    """The batched form: args.cases cases (batch_specs). value = total
+    particle-steps / device time of the batched steps."""
+    import torch
+    from pydsmc import gpu
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    gpu.load()
+    specs = batch_specs(args.cases, args.batch_seed)
+    K, W0 = args.steps, args.warmup
+    r = batch_leg(specs, K, W0, autotune=not args.no_autotune, clock_index=int(os.environ.get("LOCAL_RANK", "0")))
     line = {
         "metric": f"DSMC particle-steps/s, {len(specs)}-case batch (one CUDA graph per step, 1 B200)",
-        "value": b_ps / (b_ms / 1e3), "unit": "particle-steps/s", "n_gpus": 1, "steps": K, "warmup": W0,
-        "ms_per_step": b_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "value": r["value"], "unit": "particle-steps/s", "n_gpus": 1, "steps": K, "warmup": W0,
+        "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64acc", "data": "synthetic (seeded cases, device freestream fill)",
-        "sequential": {"value": seq_ps / (seq_ms / 1e3), "ms_per_step": seq_ms / K,
-                       "how": "each case on its own, one after another, its own per-step graph"},
-        "batch_over_sequential": (b_ps / (b_ms / 1e3)) / (seq_ps / (seq_ms / 1e3)),
-        "config": {"workload": f"batch-{len(specs)}", "cases": len(specs), "cells_total": int(sum(cells)),
-                   "particles_total": int(n0), "cells_range": [int(min(cells)), int(max(cells))],
-                   "autotuned": not args.no_autotune, "batch_seed": args.batch_seed, "setup_s": setup_s,
-                   "move_threads_chosen": sorted({s["move_threads"] for s in shapes})},
-        "gpu_launches": None,
-        "gsis_update": gsis,
-        "clocks": clk.summary(),
+        "sequential": r["sequential"], "batch_over_sequential": r["batch_over_sequential"],
+        "config": {"workload": f"batch-{len(specs)}", "cases": len(specs), "cells_total": r["cells_total"],
+                   "particles_total": r["particles"], "cells_range": r["cells_range"],
+                   "autotuned": not args.no_autotune, "batch_seed": args.batch_seed, "setup_s": r["setup_s"],
+                   "move_threads_chosen": r["move_threads_chosen"]},
+        "gpu_launches": launches_per_step(None) * K * len(specs) + K * len(specs),
+        "clocks": r["clocks"],
     }
-    line["gpu_launches"] = launches_per_step(None) * K * len(specs) + K * len(specs)
     print(json.dumps(line), flush=True)
 
 
@@ -622,72 +762,124 @@ def batch_mesh_cells(k: int) -> int:
 SERVE_SCALES = (2.65, 1.8, 1.4, 1.15, 1.0)   # mesh spacing factors: about 20k to 371k tets
 
 
-def serve_pool():
+def serve_pool(scales=None):
     """Capsule meshes at several resolutions (the request stream resamples
     among them)."""
     from pydsmc import capsule
     pool = []
-    for f in SERVE_SCALES:
+    for f in (SERVE_SCALES if scales is None else scales):
         raw = capsule.capsule_mesh(h_fine=0.215 * f, h_coarse=0.60 * f, seed=0)
         pool.append(M.build_dsmc_mesh(raw))
     return pool
 
 
-def run_serve(args):
-    """The served form: args.requests capsule cases arriving as a Poisson
-    stream (args.rate per second), each on a mesh drawn from the pool, with
-    10-100 particles per cell and 200-2000 steps (mixed precision, Ma 5,
-    Kn 0.01, AoA 30 deg); admission by a 160 GB device-memory budget; fields
-    handed to the host every 100 steps; sampling window 20%, steady sampling
-    from 50% of each case's steps."""
+def serve_leg(pool, requests: int, rate: float, seed: int, steps_range=(200, 2001), ppc_range=(10, 100),
+              round_steps: int = 20, clock_index=None) -> dict:
+    """The served form: `requests` capsule cases arriving as a Poisson stream
+    (`rate` per second), each on a mesh drawn from the pool, with particles
+    per cell and steps uniform in the given ranges (mixed precision, Ma 5,
+    Kn 0.01, AoA 30 deg); admission by a 160 GB device-memory budget; rounds
+    of at most `round_steps` steps, arrivals admitted while a round runs;
+    fields handed to the host every 100 steps; sampling window 20%, steady
+    sampling from 50% of each case's steps."""
     import torch
     from pydsmc import capsule, gpu, serve
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    gpu.load()
-    t0 = time.perf_counter()
-    pool = serve_pool()
-    setup_s = time.perf_counter() - t0
-    rs = np.random.default_rng(args.batch_seed)
+    rs = np.random.default_rng(seed)
     zones = [(3, 1, 0), (4, 2, 1), (5, 3, 0), (6, 4, 0)]
     reqs, t = [], 0.0
-    for j in range(args.requests):
-        t += rs.exponential(1.0 / args.rate)
+    for j in range(requests):
+        t += rs.exponential(1.0 / rate)
         dm = pool[int(rs.integers(0, len(pool)))]
-        ppc = float(rs.uniform(10, 100))
-        steps = int(rs.integers(200, 2001))
+        ppc = float(rs.uniform(*ppc_range))
+        steps = int(rs.integers(*steps_range))
         mess = C.mesh_message(dm, 5.0, 0.01, ppc=int(round(ppc)), L0=capsule.L0)
         reqs.append((t, serve.CaseRequest(dm=dm, mess=mess, zones=zones, inflow_dir=C.inflow_direction(30.0),
                                           steps=steps, ppc=ppc, seed=j, precision=gpu.PRECISION_MIXED,
                                           name=f"req{j}")))
     be = serve.GpuBackend(device=torch.cuda.current_device())
-    srv = serve.Server(be, hbm_budget=160e9, max_active=64, handoff_every=100)
-    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
-        start = time.perf_counter()
-        for ta, r in reqs:
-            srv.submit(r, start + ta)
-        srv.run()
+    srv = serve.Server(be, hbm_budget=160e9, max_active=64, handoff_every=100, max_round_steps=round_steps)
+    clk = ClockSampler(clock_index) if clock_index is not None else None
+    if clk:
+        clk.__enter__()
+    start = time.perf_counter()
+    for ta, r in reqs:
+        srv.submit(r, start + ta)
+    srv.run()
+    if clk:
+        clk.__exit__()
     be.close()
     s = srv.summary()
+    return {"value": s["particle_steps_per_s"], "p50_s": s["p50_s"], "p99_s": s["p99_s"],
+            "cases_per_hour": s["cases_per_hour"], "requests": requests, "rate_per_s": rate,
+            "mesh_cells": sorted(int(d.ncell) for d in pool), "ppc": list(ppc_range),
+            "steps": [steps_range[0], steps_range[1] - 1], "hbm_budget_gb": 160, "handoff_every": 100,
+            "round_steps": round_steps, "max_concurrent": s["max_concurrent"],
+            "joined_while_running": s["joined_while_running"], "rounds": s["rounds"], "span_s": s["span_s"],
+            "clocks": clk.summary() if clk else None}
+
+
+def run_serve(args):
+    """The served form (serve_leg) as its own line: args.requests requests
+    at args.rate per second on the full pool of capsule meshes."""
+    import torch
+    from pydsmc import gpu
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    gpu.load()
+    t0 = time.perf_counter()
+    pool = serve_pool()
+    setup_s = time.perf_counter() - t0
+    r = serve_leg(pool, args.requests, args.rate, args.batch_seed, clock_index=int(os.environ.get("LOCAL_RANK", "0")))
     line = {
         "metric": "DSMC served capsule cases (continuous batching, 1 B200): particle-steps/s; p50/p99 time-to-result",
-        "value": s["particle_steps_per_s"], "unit": "particle-steps/s", "n_gpus": 1,
-        "p50_s": s["p50_s"], "p99_s": s["p99_s"], "cases_per_hour": s["cases_per_hour"],
+        "value": r["value"], "unit": "particle-steps/s", "n_gpus": 1,
+        "p50_s": r["p50_s"], "p99_s": r["p99_s"], "cases_per_hour": r["cases_per_hour"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc",
         "data": "synthetic (seeded Poisson request stream, generated meshes, device freestream fill)",
-        "config": {"workload": "serve-capsule", "requests": args.requests, "rate_per_s": args.rate,
-                   "mesh_cells": sorted(int(d.ncell) for d in pool), "ppc": [10, 100], "steps": [200, 2000],
-                   "hbm_budget_gb": 160, "handoff_every": 100, "max_concurrent": s["max_concurrent"],
-                   "rounds": s["rounds"], "span_s": s["span_s"], "mesh_setup_s": setup_s,
-                   "timing": "wall clock from each request's arrival to its result on the host"},
-        "clocks": clk.summary(),
+        "config": dict({k: r[k] for k in ("requests", "rate_per_s", "mesh_cells", "ppc", "steps", "hbm_budget_gb",
+                                          "handoff_every", "round_steps", "max_concurrent", "joined_while_running",
+                                          "rounds", "span_s")},
+                       workload="serve-capsule", mesh_setup_s=setup_s,
+                       timing="wall clock from each request's arrival to its result on the host"),
+        "clocks": r["clocks"],
     }
     print(json.dumps(line), flush=True)
+
+
+def short_forms(args, rank) -> dict:
+    """The batched and served forms, short, for the headline line: 8 seeded
+    batch cases for W + K steps, and 8 served capsule requests (about 20k
+    and 50k tets, 10-60 particles per cell, 200-400 steps) arriving at 4 per
+    second."""
+    out = {}
+    specs = batch_specs(8, 1000 + rank)
+    out["batch"] = batch_leg(specs, args.steps, args.warmup, autotune=not args.no_autotune)
+    pool = serve_pool((2.65, 1.8))
+    out["serve"] = serve_leg(pool, 8, 4.0, 2000 + rank, steps_range=(200, 401), ppc_range=(10, 60))
+    return out
 
 
 # ---------------------------------------------------------------------------
 # reference arm
 # ---------------------------------------------------------------------------
+def mem_available_gb() -> float:
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 8.0
+
+
 def run_reference(args):
+    """The reference arm: the reference's own CPU implementation of the step
+    (oracle/_ref: its sources built against a one-rank MPI stand-in) on the
+    same case as our arm, on the host cores: as many concurrent single-rank
+    processes as the cores and the host memory allow (about 6 GB each at the
+    capsule's 37 million particles), each with the reference's own initial
+    fill, one warm-up step and up to three timed steps (one step takes about
+    14 s of one core). Rank 0 runs it; other ranks exit."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -698,37 +890,22 @@ def run_reference(args):
                           "code built against a one-rank MPI shim) is not built"}))
         return
     wl = make_workload(args.workload, args.ppc)
-    dm, mess = wl["dm"], wl["mess"]
+    plan = run_plan(wl, args)
     cores = os.cpu_count() or 1
-    ppc_s = max(2, min(args.ppc, 10))
-    roles = {1: "interface", 2: "inlet", 3: "outlet", 4: "wall", 5: "none", 0: "none"}
-    r_arg = ",".join(f"{t}:{roles[r]}" for t, r, _ in wl["zones"])
-    nsteps = args.warmup + args.steps
-    with tempfile.TemporaryDirectory() as d:
-        cas = os.path.join(d, "case.cas")
-        M.write_cas(cas, dm.raw)
-        from concurrent.futures import ThreadPoolExecutor
-        fills = [W.initial_fill(dm, mess, ppc_s, seed=100 + k, inflow_dir=wl["inflow_dir"], proportional=True)
-                 for k in range(cores)]
-        t0 = time.perf_counter()
-        with ThreadPoolExecutor(max_workers=cores) as ex:
-            futs = [ex.submit(H.run, cas, mess, f["x"], f["v"], f["ir"], f["cell"], nsteps, 1 + k, r_arg, nsteps + 1, 3600)
-                    for k, f in enumerate(fills)]
-            res = [f.result() for f in futs]
-        wall = time.perf_counter() - t0
-    per = [r["timing"]["particle_steps_per_s"] for r in res]
-    agg = float(sum(per))
-    # n_gpus: the N this arm was launched for (the reference itself runs on
-    # the host cores; "device" says so)
-    line = {"impl": "reference", "metric": METRIC, "value": agg, "unit": "particle-steps/s",
-            "n_gpus": int(os.environ.get("WORLD_SIZE", args.gpus)), "device": f"host ({cores} cores)",
+    per_gb = 8.0 if wl["name"] == "capsule" else 2.0
+    nproc = max(1, min(cores, 16, int(mem_available_gb() // per_gb)))
+    nsteps = min(4, max(2, -(-(args.steps + args.warmup) // nproc)))
+    r = reference_bench(wl, args, nproc, nsteps, 100)
+    line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": "particle-steps/s",
+            "n_gpus": int(os.environ.get("WORLD_SIZE", args.gpus)), "device": f"host ({nproc} of {cores} cores)",
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": wl["desc"],
-            "cpu_baseline": {"value": agg, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
-                             "sample": f"{cores} independent single-rank processes, {ppc_s} particles/cell on "
-                                       f"average each, "
-                                       f"{nsteps} steps each, {wall:.1f} s wall"},
-            "e2e": {"value": agg, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": bench_config(wl, plan),
+            "cpu_baseline": {"value": r["value"], "unit": "particle-steps/s", "cores": nproc, "kind": "reference",
+                             "sample": f"{nproc} concurrent single-rank processes of the reference, each the full "
+                                       f"case ({int(np.mean(r['particles']))} particles on average from its own "
+                                       f"fill, moved to the freestream), 1 warm-up and {nsteps - 1} timed steps "
+                                       f"each, {r['wall_s']:.1f} s wall"},
+            "e2e": {"value": r["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -744,6 +921,10 @@ def main():
     ap.add_argument("--cases", type=int, default=64, help="batch workload: number of cases")
     ap.add_argument("--batch-seed", type=int, default=0)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="leave out the short batched and served legs")
+    ap.add_argument("--run-steps", type=int, default=0,
+                    help="steps of the case's run (default: 2000 capsule, 500 block); the timed steps follow a "
+                         "spin-up to half of it")
     ap.add_argument("--requests", type=int, default=16, help="serve workload: number of requests")
     ap.add_argument("--rate", type=float, default=4.0, help="serve workload: arrivals per second")
     args = ap.parse_args()

@@ -7,7 +7,11 @@ part of its repository; this generator stands in for it. Points come from a
 seeded jittered lattice, finer around the body, in a box of
 6 L0 x 4 L0 x 4 L0 (L0 = 3.912 m), plus points on the body surface; they are
 tetrahedralised with scipy's Delaunay (Qhull) and the tetrahedra whose
-centroid lies inside the body are removed. Faces between kept and removed
+centroid lies inside the body are removed. With ``target_cells`` the count is
+then brought to exactly that number by splitting a few seeded far-field cells:
+a tetrahedron at its centroid (one cell becomes four) and an interior face at
+its centroid (its two cells become six); both keep the mesh conforming and
+every cell's orientation. Faces between kept and removed
 tetrahedra form the diffuse wall (zone 6); box faces whose outward normal
 points against the freestream (or across it) are freestream inlets (zone 4),
 the rest outlets (zone 5).
@@ -89,8 +93,78 @@ def _lattice(lo, hi, h, rng, jitter=0.2):
     return P
 
 
+# the reference's Apollo mesh (mesh/3dapollo372500.cas) has 372,500 cells
+CAP_CELLS = 372500
+
+
+def _split_to_count(pts, tets, target, far, rng):
+    """Split cells of the mask `far` until there are `target` cells: `a`
+    tetrahedra at their centroid (+3 cells each) and `b` interior faces at
+    their centroid (+4 each), 3a + 4b = target - len(tets), on distinct
+    cells. Each new cell is its parent with one vertex moved to the new
+    point, so it keeps the parent's orientation."""
+    extra = target - tets.shape[0]
+    if extra == 0:
+        return pts, tets
+    sol = [(a, (extra - 3 * a) // 4) for a in range(4) if extra - 3 * a >= 0 and (extra - 3 * a) % 4 == 0]
+    if extra < 0 or not sol:
+        raise ValueError(f"cannot reach {target} cells from {tets.shape[0]} by splitting")
+    a, b = sol[0]
+    cand = np.nonzero(far)[0]
+    # interior faces between two candidate cells, in a seeded order
+    fl = np.concatenate([tets[cand][:, [1, 2, 3]], tets[cand][:, [0, 3, 2]],
+                         tets[cand][:, [0, 1, 3]], tets[cand][:, [0, 2, 1]]])
+    own = np.tile(cand, 4)
+    key = np.sort(fl, axis=1)
+    order = np.lexsort((key[:, 2], key[:, 1], key[:, 0]))
+    ks = key[order]
+    dup = np.nonzero(np.all(ks[1:] == ks[:-1], axis=1))[0]
+    pairs = np.column_stack([own[order][dup], own[order][dup + 1]])
+    tris = ks[dup]
+    used = np.zeros(tets.shape[0], dtype=bool)
+    new_pts, new_tets, drop = [], [], []
+    npts = pts.shape[0]
+    for i in rng.permutation(len(pairs)):
+        if b == 0:
+            break
+        c0, c1 = pairs[i]
+        if used[c0] or used[c1]:
+            continue
+        used[c0] = used[c1] = True
+        m = npts + len(new_pts)
+        new_pts.append(pts[tris[i]].mean(axis=0))
+        for c in (c0, c1):
+            t = tets[c]
+            for v in tris[i]:
+                tt = t.copy()
+                tt[tt == v] = m
+                new_tets.append(tt)
+            drop.append(c)
+        b -= 1
+    for c in rng.permutation(cand):
+        if a == 0:
+            break
+        if used[c]:
+            continue
+        used[c] = True
+        g = npts + len(new_pts)
+        new_pts.append(pts[tets[c]].mean(axis=0))
+        for k in range(4):
+            tt = tets[c].copy()
+            tt[k] = g
+            new_tets.append(tt)
+        drop.append(c)
+        a -= 1
+    if a or b:
+        raise ValueError("not enough far-field cells to split")
+    keep = np.ones(tets.shape[0], dtype=bool)
+    keep[np.asarray(drop)] = False
+    tets = np.concatenate([tets[keep], np.asarray(new_tets, dtype=tets.dtype)])
+    return np.concatenate([pts, np.asarray(new_pts)]), tets
+
+
 def capsule_mesh(h_fine: float = 0.215, h_coarse: float = 0.60, seed: int = 0, aoa_deg: float = 30.0,
-                 r_fine: float = 4.2) -> RawMesh:
+                 r_fine: float = 4.2, target_cells: int | None = None) -> RawMesh:
     from scipy.spatial import Delaunay
 
     rng = np.random.default_rng(seed)
@@ -123,6 +197,10 @@ def capsule_mesh(h_fine: float = 0.215, h_coarse: float = 0.60, seed: int = 0, a
     a, b, c_, d_ = (pts[tets[:, k]] for k in range(4))
     v6 = np.einsum("ij,ij->i", b - a, np.cross(c_ - a, d_ - a))
     tets = tets[np.abs(v6) > 1e-12]
+    if target_cells is not None:
+        cent = pts[tets].mean(axis=1)
+        far = np.linalg.norm(cent - body_c, axis=1) > r_fine + 2.0 * h_coarse
+        pts, tets = _split_to_count(pts, tets, int(target_cells), far, np.random.default_rng(seed + 7919))
     ncell = tets.shape[0]
 
     # faces: 4 per tet, matched by sorted node triple
@@ -174,12 +252,13 @@ def capsule_mesh(h_fine: float = 0.215, h_coarse: float = 0.60, seed: int = 0, a
     f2[:, :3] = remap[faces[:, :3]]
     return RawMesh(pts[used], f2, ftype, c0, c1, zone, ncell, 2,
                    meta={"kind": "capsule", "seed": seed, "h_fine": h_fine, "h_coarse": h_coarse,
-                         "aoa_deg": aoa_deg})
+                         "aoa_deg": aoa_deg, "target_cells": target_cells})
 
 
 def capsule_workload(ppc: int = 100, seed: int = 0):
-    """CAP: Ma 5, Kn 0.01 on L0, AoA 30 deg, T_in 142.2 K, T_w 300 K diffuse."""
-    raw = capsule_mesh(seed=seed)
+    """CAP: 372,500 tetrahedra; Ma 5, Kn 0.01 on L0, AoA 30 deg, T_in 142.2 K,
+    T_w 300 K diffuse."""
+    raw = capsule_mesh(seed=seed, target_cells=CAP_CELLS)
     dm = build_dsmc_mesh(raw)
     mess = C.mesh_message(dm, 5.0, 0.01, ppc=ppc, L0=L0)
     zones = [(3, 1, 0), (4, 2, 1), (5, 3, 0), (6, 4, 0)]

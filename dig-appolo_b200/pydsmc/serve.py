@@ -7,9 +7,13 @@ the GPU between steps, and advances all admitted cases together: each round
 is one batched step call (dsmc_batch_step: one CUDA graph per step whose
 branches are the cases). A round stops at the next point where some case
 must hand its sampled fields to the host (every `handoff_every` of its own
-steps, the GSIS exchange of the reference's coupled loop) or finishes; a
-finished case releases its memory and slot before the next admission, so new
-requests join the batch while others are running.
+steps, the GSIS exchange of the reference's coupled loop), finishes, or has
+run `max_round_steps`; a finished case releases its memory and slot before
+the next admission, so new requests join the batch while others are
+running. A backend that can launch a round without waiting for it
+(`launch` / `wait`) lets the server admit the requests that arrive during
+the round while the GPU works: their set-up (mesh upload, device fill) runs
+on their own streams beside the batch, and they join the next round.
 
 Every case keeps its own step count, constants and random streams, and a
 batched step equals the same step taken alone, so a case's result does not
@@ -107,7 +111,8 @@ class GpuBackend:
         case.statistic_macroPre()
         return case
 
-    def step(self, handles, n: int):
+    def launch(self, handles, n: int):
+        """Enqueue n batched steps of these cases and return."""
         if n <= 0 or not handles:
             return
         members = tuple(id(h) for h in handles)
@@ -119,7 +124,15 @@ class GpuBackend:
             self._batch = self.gpu.Batch(handles)
             self._members = members
         self._batch.step(n)
-        self._batch.sync()
+
+    def wait(self):
+        """Wait for the last launched round."""
+        if self._batch is not None:
+            self._batch.sync()
+
+    def step(self, handles, n: int):
+        self.launch(handles, n)
+        self.wait()
 
     def particles(self, handle) -> int:
         return handle.particle_count()
@@ -150,12 +163,14 @@ class Server:
     """Continuous-batching request loop (see the module docstring)."""
 
     def __init__(self, backend, hbm_budget: float = 160e9, max_active: int = 64, handoff_every: int = 100,
-                 clock=time.perf_counter):
+                 clock=time.perf_counter, max_round_steps: int | None = None):
         self.backend = backend
         self.budget = int(hbm_budget)
         self.max_active = max_active
         self.handoff_every = handoff_every
+        self.max_round_steps = max_round_steps
         self.clock = clock
+        self.joined_running = 0     # admissions while other cases were on the GPU
         self._queue = []            # (t_arrival, rid, request)
         self._ids = itertools.count()
         self.active: list[_Active] = []
@@ -164,6 +179,7 @@ class Server:
         self.rounds = 0
         self.max_concurrent = 0
         self.admit_order: list[int] = []
+        self._joining: list[_Active] = []
 
     def submit(self, req: CaseRequest, t_arrival: float | None = None) -> int:
         rid = next(self._ids)
@@ -174,19 +190,22 @@ class Server:
         heapq.heappush(self._queue, (t, rid, req))
         return rid
 
-    def _admit(self, now: float):
+    def _admit(self, now: float, into: list | None = None):
         # arrival order; a case that does not fit blocks the ones behind it
-        while self._queue and self._queue[0][0] <= now and len(self.active) < self.max_active:
+        into = self.active if into is None else into
+        while self._queue and self._queue[0][0] <= now and len(self.active) + len(self._joining) < self.max_active:
             t, rid, req = self._queue[0]
             fp = self.backend.footprint(req)
             if self.used + fp > self.budget:
                 break
             heapq.heappop(self._queue)
+            if self.active:
+                self.joined_running += 1
             handle = self.backend.create(req)
             self.used += fp
-            self.active.append(_Active(rid, req, handle, t, self.clock(), fp))
+            into.append(_Active(rid, req, handle, t, self.clock(), fp))
             self.admit_order.append(rid)
-        self.max_concurrent = max(self.max_concurrent, len(self.active))
+        self.max_concurrent = max(self.max_concurrent, len(self.active) + len(self._joining))
 
     def _round_steps(self) -> int:
         n = None
@@ -195,10 +214,14 @@ class Server:
             to_handoff = self.handoff_every - (a.step % self.handoff_every)
             m = min(to_end, to_handoff)
             n = m if n is None else min(n, m)
+        if n and self.max_round_steps:
+            n = min(n, self.max_round_steps)
         return n or 0
 
     def run(self, sleep=time.sleep):
         """Serve until every submitted request has finished."""
+        overlap = hasattr(self.backend, "launch") and hasattr(self.backend, "wait")
+        self._joining = []
         while self._queue or self.active:
             now = self.clock()
             self._admit(now)
@@ -207,7 +230,13 @@ class Server:
                 continue
             n = self._round_steps()
             counts = [self.backend.particles(a.handle) for a in self.active]
-            self.backend.step([a.handle for a in self.active], n)
+            if overlap:
+                self.backend.launch([a.handle for a in self.active], n)
+                # requests that arrived meanwhile are set up while the round runs
+                self._admit(self.clock(), into=self._joining)
+                self.backend.wait()
+            else:
+                self.backend.step([a.handle for a in self.active], n)
             self.rounds += 1
             still = []
             for a, c in zip(self.active, counts):
@@ -223,7 +252,8 @@ class Server:
                                                      final, local, a.particle_steps, counters)
                 else:
                     still.append(a)
-            self.active = still
+            self.active = still + self._joining
+            self._joining = []
         return self.results
 
     def summary(self) -> dict:
@@ -235,4 +265,5 @@ class Server:
                 "p99_s": float(np.percentile(ttr, 99)) if r else None,
                 "cases_per_hour": len(r) / span * 3600.0 if span > 0 else None,
                 "particle_steps_per_s": ps / span if span > 0 else None, "span_s": span,
-                "rounds": self.rounds, "max_concurrent": self.max_concurrent}
+                "rounds": self.rounds, "max_concurrent": self.max_concurrent,
+                "joined_while_running": self.joined_running}

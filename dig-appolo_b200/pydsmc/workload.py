@@ -74,6 +74,15 @@ def cell_boxes(dm: DsmcMesh):
     return lo, hi
 
 
+def proportional_counts(dm: DsmcMesh, ppc: float, rng: np.random.Generator) -> np.ndarray:
+    """A mean of ``ppc`` particles per cell in proportion to the cell volumes,
+    each cell's count rounded up with probability equal to its fraction
+    (setParticleMessage, src/meshImport.cpp:1399-1421)."""
+    vol = dm.cells["area"].astype(float)
+    ns = vol * (ppc * dm.ncell) / vol.sum()
+    return (np.floor(ns).astype(np.int64) + (rng.random(dm.ncell) < ns - np.floor(ns))).astype(np.int32)
+
+
 def initial_fill(dm: DsmcMesh, mess, ppc: int, seed: int, inflow_dir, proportional: bool = False) -> dict:
     """Particles from the freestream Maxwellian: ``ppc`` in every cell, or
     with ``proportional`` a mean of ``ppc`` per cell in proportion to the
@@ -81,10 +90,7 @@ def initial_fill(dm: DsmcMesh, mess, ppc: int, seed: int, inflow_dir, proportion
     fraction (the reference's initial counts, src/meshImport.cpp:1399-1421)."""
     rng = np.random.default_rng(seed)
     if proportional:
-        vol = dm.cells["area"].astype(float)
-        ns = vol * (ppc * dm.ncell) / vol.sum()
-        n = np.floor(ns).astype(np.int64) + (rng.random(dm.ncell) < ns - np.floor(ns))
-        cells = np.repeat(np.arange(dm.ncell, dtype=np.int32), n)
+        cells = np.repeat(np.arange(dm.ncell, dtype=np.int32), proportional_counts(dm, ppc, rng))
     else:
         cells = np.repeat(np.arange(dm.ncell, dtype=np.int32), ppc)
     x = uniform_positions(dm, cells, rng)

@@ -232,3 +232,17 @@ def fluent(cas: str, mess, fields) -> dict:
             text = fh.read()
         zones = np.fromfile(os.path.join(out, "zones.bin"), dtype=np.int32).reshape(-1, 3)
         return {"text": text, "zones": zones}
+
+
+def bench(cas: str, mess, counts, nsteps: int, seed: int, roles: str, drift, tN: float,
+          timeout: int = 3600) -> dict:
+    """The reference's own initial fill of counts[c] particles per cell,
+    moved to the freestream (drift, temperature tN), then nsteps of its step
+    loop, each timed (the harness's "bench" command); its JSON report."""
+    with tempfile.TemporaryDirectory() as d:
+        pm, pc = os.path.join(d, "mess.bin"), os.path.join(d, "counts.bin")
+        _write_mess(pm, mess)
+        np.ascontiguousarray(counts, dtype=np.int32).tofile(pc)
+        out = _run(["bench", cas, pm, pc, nsteps, seed, roles, float(drift[0]), float(drift[1]), float(drift[2]),
+                    float(tN)], timeout=timeout)
+        return json.loads(out.strip().splitlines()[-1])

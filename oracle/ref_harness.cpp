@@ -69,6 +69,14 @@
  *       stayed in the domain (recv_cache) are collected and the cache is
  *       cleared. Dumps them (OUT/particles.bin), their count per step and
  *       the inflow remainders.
+ *   bench CAS MESS COUNTS NSTEPS SEED ROLES UX UY UZ TN
+ *       The reference's initial fill as in "fill" (COUNTS[c] particles in
+ *       cell c), moved to the freestream the benchmark starts from (the
+ *       fill's unit Maxwellian at rest scaled to temperature TN and shifted
+ *       by the drift U: v <- U + sqrt(TN) v, Ir <- TN Ir), then ProcessDSMC
+ *       over it and NSTEPS steps of the reference's loop (as "run"), each
+ *       timed on its own. Prints one JSON line: particles after the fill,
+ *       fill seconds, per-step seconds and particles, particle-steps/s.
  *   ROLES is "-" or a comma list tag:role with role in
  *       none,interface,inlet,outlet,wall.
  */
@@ -79,6 +87,7 @@
 #include "meshImport.h"
 
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -506,6 +515,75 @@ int cmdFill(int argc, char** argv)
     return ok && writeFile(out + "/np_tri.bin", npTri.data(), npTri.size() * 4) ? 0 : 1;
 }
 
+int cmdBench(int argc, char** argv)
+{
+    if (argc < 12) return 2;
+    Rig r;
+    if (!buildRig(r, argv[2], argv[3], "-", false)) return 1;
+    const int ncell = r.partinit->my_ncell;
+    std::vector<char> cb;
+    if (!readFile(argv[4], cb) || cb.size() != (std::size_t)ncell * 4) return 1;
+    const int nsteps = std::atoi(argv[5]);
+    const unsigned seed = (unsigned)std::strtoul(argv[6], nullptr, 10);
+    const std::string roles = argv[7];
+    const double u[3] = {std::atof(argv[8]), std::atof(argv[9]), std::atof(argv[10])};
+    const double tN = std::atof(argv[11]);
+    const double sq = std::sqrt(tN);
+    r.partinit->thread_rng().seed(seed);
+    std::srand(seed);
+    const auto f0 = std::chrono::steady_clock::now();
+    for (int c = 0; c < ncell; ++c) {
+        int np = 0;
+        std::memcpy(&np, cb.data() + (std::size_t)c * 4, 4);
+        if (np <= 0) continue;
+        std::vector<double> tri;
+        r.partinit->Np_tri_inititial(c, tri, np);
+        if (!tri.empty()) r.partinit->meshfillpar(c, tri);
+    }
+    long long n0 = 0;
+    for (auto& b : r.partinit->cell_particles_curr) {
+        for (std::size_t i = 0; i < b.size(); ++i) {
+            b.vx[i] = u[0] + sq * b.vx[i];
+            b.vy[i] = u[1] + sq * b.vy[i];
+            b.vz[i] = u[2] + sq * b.vz[i];
+            b.p_Ir[i] = tN * b.p_Ir[i];
+        }
+        n0 += (long long)b.size();
+    }
+    const double fillSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - f0).count();
+    r.process = new ProcessDSMC(r.mesh, r.mesh->mess, r.partinit, r.ctx);
+    applyRoles(*r.process, roles);
+    ProcessDSMC& p = *r.process;
+    p.statistic_macroPre();
+    std::vector<double> sec((std::size_t)nsteps);
+    std::vector<long long> parts((std::size_t)nsteps);
+    double total = 0.0;
+    long long particleSteps = 0;
+    for (int istep = 1; istep <= nsteps; ++istep) {
+        long long nBefore = 0;
+        for (const auto& b : r.partinit->cell_particles_curr) nBefore += (long long)b.size();
+        const auto t0 = std::chrono::steady_clock::now();
+        p.preprocesseffquad(istep);
+        p.advection(istep);
+        p.cache2chain();
+        p.collisionDSMC();
+        p.statistic_macro(istep);
+        const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        sec[(std::size_t)istep - 1] = dt;
+        parts[(std::size_t)istep - 1] = nBefore;
+        total += dt;
+        particleSteps += nBefore;
+    }
+    std::printf("{\"particles\": %lld, \"fill_seconds\": %.6f, \"steps\": %d, \"particle_steps\": %lld, "
+                "\"seconds\": %.6f, \"particle_steps_per_s\": %.3f, \"step_seconds\": [",
+                n0, fillSeconds, nsteps, particleSteps, total, total > 0 ? (double)particleSteps / total : 0.0);
+    for (int k = 0; k < nsteps; ++k) std::printf("%s%.6f", k ? ", " : "", sec[(std::size_t)k]);
+    std::printf("], \"step_particles\": [");
+    for (int k = 0; k < nsteps; ++k) std::printf("%s%lld", k ? ", " : "", parts[(std::size_t)k]);
+    std::printf("]}\n");
+    return 0;
+}
+
 // The particles sampled at step k in the "sample" command: particle i of
 // the input (cell c) is present unless c % 5 == 0 and (k % 50 != 0 or
 // i % PPC != 0) (such cells hold one particle on two steps of every
@@ -659,6 +737,7 @@ int main(int argc, char** argv)
     const std::string cmd = argv[1];
     if (cmd == "mesh") return cmdMesh(argc, argv);
     if (cmd == "trace") return cmdTrace(argc, argv);
+    if (cmd == "bench") return cmdBench(argc, argv);
     if (cmd == "advect") return cmdAdvect(argc, argv);
     if (cmd == "run") return cmdRun(argc, argv);
     if (cmd == "gsis") return cmdGsis(argc, argv);

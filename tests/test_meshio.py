@@ -218,3 +218,24 @@ def test_fluent_wall_writer_follows_the_reference_formula(tmp_path, block8_cas):
     out2 = str(tmp_path / "none.dat")
     IO.write_fluent_wall(out2, mess, gpu.default_params(zones=I.NOWALL_ZONES), zones, dm.edges, tally, 25)
     assert not os.path.exists(out2)
+
+
+def test_capsule_mesh_has_the_reference_cell_count():
+    """The CAP mesh: the seeded jittered-lattice Delaunay fill around the
+    capsule, brought to the reference mesh's 372,500 cells by splitting a
+    few far-field cells; every cell keeps a positive volume, every face has
+    one or two cells, and the body wall, inlets and outlets are all there."""
+    from pydsmc import capsule
+    raw = capsule.capsule_mesh(target_cells=capsule.CAP_CELLS)
+    dm = M.build_dsmc_mesh(raw)
+    assert dm.ncell == 372500 == raw.ncell
+    assert np.all(dm.cells["area"] > 0)
+    assert np.all(raw.c0 >= 0)
+    tags = set(np.unique(dm.edges["faceTag"]).tolist())
+    assert {3, 4, 5, 6} <= tags
+    # the split cells lie in the far field: the body and its fine region are
+    # those of the plain fill
+    plain = capsule.capsule_mesh()
+    assert plain.ncell < raw.ncell
+    wall = dm.edges["faceTag"] == 6
+    assert wall.sum() == int((M.build_dsmc_mesh(plain).edges["faceTag"] == 6).sum())

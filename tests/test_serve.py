@@ -140,3 +140,69 @@ def test_served_cases_equal_cases_run_alone():
             assert got.counters[k] == counters[k], k
     s = srv.summary()
     assert s["cases"] == 4 and s["max_concurrent"] == 2 and s["p99_s"] >= s["p50_s"] > 0
+
+
+@pytest.mark.gpu
+def test_cases_arriving_while_others_run_equal_cases_run_alone():
+    """Requests that arrive while another case is on the GPU: the server
+    admits them during the running round (their device fill overlaps it)
+    and they join the next round; every result equals the same case run
+    alone. Time is counted in rounds, so the arrivals fall in mid-run."""
+    from pydsmc import case as CS
+    from pydsmc import gpu
+    raw4, dm4 = I.block_mesh(scale=4)
+    raw8, dm8 = I.block_mesh(scale=8)
+    zones = I.REF_ZONES + [(7, gpu.ROLE_SPECULAR, 0)]
+    specs = [(dm4, 5.0, 0.1, 20, 160, 0.0), (dm8, 7.0, 0.05, 30, 90, 2.5), (dm4, 4.0, 0.3, 15, 70, 5.5)]
+    reqs = []
+    for k, (dm, ma, kn, ppc, steps, _) in enumerate(specs):
+        mess = CS.mesh_message(dm, ma, kn, ppc=ppc, L0=I.BLOCK_L0)
+        reqs.append(serve.CaseRequest(dm=dm, mess=mess, zones=zones, inflow_dir=I.inflow_dir(), steps=steps,
+                                      ppc=float(ppc), seed=200 + k, precision=gpu.PRECISION_MIXED, name=f"a{k}"))
+    class Backend(serve.GpuBackend):
+        in_round = False
+
+        def launch(self, handles, n):
+            super().launch(handles, n)
+            self.in_round = True
+
+        def wait(self):
+            super().wait()
+            self.in_round = False
+
+    be = Backend()
+    alone = []
+    for r in reqs:
+        h = be.create(r)
+        for s in range(1, r.steps + 1):
+            h.step(s)
+        alone.append(be.finish(h))
+
+    class RoundClock:
+        """Rounds done, plus one half while a round is on the GPU."""
+        srv = None
+        slept = 0.0
+
+        def __call__(self):
+            return (self.srv.rounds if self.srv else 0) + (0.5 if be.in_round else 0.0) + self.slept
+
+        def sleep(self, dt):
+            self.slept += dt
+
+    clk = RoundClock()
+    srv = serve.Server(be, max_active=4, max_round_steps=10, clock=clk)
+    clk.srv = srv
+    ids = [srv.submit(r, t) for r, (*_, t) in zip(reqs, specs)]
+    res = srv.run(sleep=clk.sleep)
+    be.close()
+    for rid, (final, local, counters) in zip(ids, alone):
+        got = res[rid]
+        assert np.array_equal(got.final_record, final, equal_nan=True)
+        assert np.array_equal(got.local, local, equal_nan=True)
+        for k in ("injected", "removed", "collisions", "crossings"):
+            assert got.counters[k] == counters[k], k
+    # the later requests were admitted while a round of the first one ran
+    assert srv.joined_running == 2
+    for k in (1, 2):
+        assert res[ids[k]].t_admit % 1.0 == 0.5 and res[ids[k]].t_admit < res[ids[0]].t_done
+    assert srv.max_concurrent == 3
