@@ -769,6 +769,30 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
     return false;
 }
 
+// The first exit search of a particle at rest in `cell` at the start of the
+// step (no entry face), taken only when it settles that the particle stays
+// in its cell for the whole of dtleft: the decision trace_step takes on that
+// search, without the triangle scan. The caller then advances it by dtleft.
+// FP64 path: the plane decision and the reference's test on the chosen
+// triangle; mixed path: certain_exit_f32.
+template <typename Real>
+__device__ __forceinline__ bool stays_for_the_step(const DevMesh& M, int cell, const PRegs<Real>& p, double dtleft)
+{
+    if (!(M.allConvex || M.convex[cell])) return false;
+    if constexpr (sizeof(Real) == 8) {
+        const PlaneHit ph = find_exit_planes(M, cell, -1, p.x, p.v);
+        double te = DBL_MAX;
+        return !ph.ambiguous && isect_exact(M.triD + (size_t)ph.triIdx * 9, p.x, p.v, te) && te >= dtleft;
+    } else {
+        const double* cc = M.cellCenter + (size_t)cell * 3;
+        const double c0 = cc[0], c1 = cc[1], c2 = cc[2];
+        const float xr[3] = {(float)ds(p.x[0], c0), (float)ds(p.x[1], c1), (float)ds(p.x[2], c2)};
+        const float absScale = (float)(fabs(c0) + fabs(c1) + fabs(c2));
+        const CertainExit ce = certain_exit_f32(M, cell, -1, -1, xr, p.v, absScale);
+        return ce.certain && ce.tLo > (float)dtleft * (1.0f + 0x1p-16f);
+    }
+}
+
 // Trace one particle, starting in `cell` having entered through face
 // `crossf` / triangle `tag` (-1/-1 for a particle at rest in its cell), for
 // `dtleft` (updated: the time not flown when the trace stops). Returns the

@@ -17,6 +17,7 @@
 //   sample   statistic_macro (src/ProcessDSMC.cpp:2757-2861): the
 //            18-moment sums of each cell in particle order.
 #include <climits>
+#include <cstddef>
 
 #include "dsmc_kernels.cuh"
 #include "dsmc_macro.cuh"
@@ -237,24 +238,68 @@ void launch_inject(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s
 // ===========================================================================
 // move
 // ===========================================================================
-// Three resident 256-thread blocks per SM (registers capped at 85): the
-// trace is bound by dependent loads, so occupancy pays more than the few
-// registers it spills to L1.
-// Particles are handed to warps in chunks (one atomic per chunk on the
-// step's cursor) and to lanes one at a time: a lane whose particle has
-// finished its trace writes it back and takes the next particle of the
-// chunk, so the lanes of a warp keep doing exit searches instead of waiting
-// for the warp's longest trace (about a quarter of the particles cross a
-// face in a step, a few cross several). Each particle is traced by the same
-// code with its own random stream (particle index, step), so the result
-// does not depend on which lane or warp takes it.
+// Two passes over the particles of the step.
+//
+// Stay pass (move_stay_kernel): one thread per particle, in slot order
+// (coalesced loads, the particles of a cell next to each other, so a warp
+// reads few cells' face records). Most particles stay in their cell for the
+// whole step; where the first exit search settles that (stays_for_the_step)
+// the particle is advanced and stored right there. The others are appended
+// to a work list (warp-aggregated, in the sort's rank array, which is free
+// until the sort).
+//
+// Tracing pass (move_kernel): the listed particles, traced from their start
+// by trace_step. Warps claim chunks of 128 list entries from a cursor in
+// the step control block (one atomic per chunk), and a lane whose particle
+// has finished writes it back and takes the next particle of the chunk, so
+// the lanes keep doing exit searches instead of waiting for the warp's
+// longest trace. Three resident 256-thread blocks per SM (registers capped
+// at 85): the trace is bound by dependent loads, so occupancy pays more than
+// the few registers it spills to L1.
+//
+// Each particle runs the same code with its own random stream (particle
+// index, step), and the stay pass takes exactly the decision the trace's
+// first search takes, so results do not depend on the split, the list
+// order, or which lane or warp traces a particle.
 constexpr int kMoveChunk = 128;
+
+template <typename Real>
+__global__ void __launch_bounds__(256) move_stay_kernel(StepArgs<Real> a)
+{
+    const int n = a.ctl->nLive;
+    const double dt = a.C.dtime;
+    const int lane = threadIdx.x & 31;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const int i = base + (int)threadIdx.x;
+        bool defer = false;
+        if (i < n) {
+            const int cell = a.A.cell[i];
+            PRegs<Real> p;
+            load_position(a.M, a.A, i, cell, p);
+            p.v[0] = a.A.v[0][i]; p.v[1] = a.A.v[1][i]; p.v[2] = a.A.v[2][i];
+            if (stays_for_the_step<Real>(a.M, cell, p, dt)) {
+                advance(p, dt);
+                store_position(a.M, a.A, i, cell, p);
+            } else {
+                defer = true;
+            }
+        }
+        const unsigned m = __ballot_sync(kFull, defer);
+        if (m) {
+            int at = 0;
+            if (lane == 0) at = atomicAdd(&a.ctl->moveList, __popc(m));
+            at = __shfl_sync(kFull, at, 0);
+            if (defer) a.rank[at + __popc(m & ((1u << lane) - 1u))] = i;
+        }
+    }
+}
 
 template <typename Real>
 __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
 {
     const int istep = a.ctl->istep;
-    const int n = a.ctl->nLive;
+    const int n = a.ctl->moveList;
+    const int* __restrict__ list = a.rank;
     const int lane = threadIdx.x & 31;
     const unsigned lower = (1u << lane) - 1u;
     TraceCounts cnt{};
@@ -285,7 +330,7 @@ __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
             const int take = min(chunkEnd - chunkNext, __popc(want));
             const bool mine = ((want >> lane) & 1u) && __popc(want & lower) < take;
             if (mine) {
-                i = chunkNext + __popc(want & lower);
+                i = list[chunkNext + __popc(want & lower)];
                 cell = a.A.cell[i];
                 load_position(a.M, a.A, i, cell, p);
                 p.v[0] = a.A.v[0][i]; p.v[1] = a.A.v[1][i]; p.v[2] = a.A.v[2][i];
@@ -320,7 +365,10 @@ __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
 template <typename Real>
 void launch_move(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s)
 {
-    cudaMemsetAsync(&a.ctl->moveCursor, 0, sizeof(int), s);
+    static_assert(offsetof(StepCtl, moveList) == offsetof(StepCtl, moveCursor) + sizeof(int),
+                  "the move's cursor and list count are reset together");
+    cudaMemsetAsync(&a.ctl->moveCursor, 0, 2 * sizeof(int), s);
+    move_stay_kernel<Real><<<L.smCount * 8, 256, 0, s>>>(a);
     move_kernel<Real><<<L.smCount * L.moveBlocksPerSm, L.moveThreads, 0, s>>>(a);
 }
 

@@ -21,8 +21,9 @@ struct StepCtl {
     int nInj;         // particles injected this step (appended after nLive)
     int nNext;        // particles after the sort
     int capacity;
-    int moveCursor;   // particles handed out by the move kernel (reset before each move)
-    int pad[2];
+    int moveCursor;   // list entries handed out by the tracing pass of the move (reset before each move)
+    int moveList;     // particles the stay pass leaves to the tracing pass (reset before each move)
+    int pad[1];
 };
 
 struct DevPatches {

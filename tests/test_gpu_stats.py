@@ -14,13 +14,23 @@ cell, the reference's boundary roles).
 - Mixed against FP64 (the all-FP64 GPU oracle), per cell: the two runs
   within 3 sigma of each other (sigma from the reference spread, times
   sqrt 2 for two independent runs) for at least 95% of (cell, field).
+- The deviatoric stress, heat flux and rotational heat flux of the same
+  runs (writeAveragedMacro's definitions) against the reference's band
+  (tests/golden/macro_band.npz).
+- The capsule tets at Kn 0.01 (collision-dominated), FP64 and mixed,
+  against the band of 8 reference runs there
+  (tests/golden/stats_band_capsule.npz).
 - Mixed against FP64 on the full block case (48,640 cells, 50 particles per
   cell, fields averaged over steps 201-400): domain-integrated density,
   velocity, temperature and rotational temperature within 0.5%. At this
   size the seed-to-seed spread is below 0.1% (1.3% for the temperature on
   the 1/4-resolution case above, which has 1/160 of the particles and half
   the averaging steps), so the bound measures the precision path, not the
-  sampling noise.
+  sampling noise. Per cell and per field, all 18 of them, over ten 20-step
+  windows: the two runs' window means within 3 standard errors of each
+  other (batch means) for at least 95% of the cells, and every field's
+  mass-weighted domain difference within 0.5% of its scale; the per-cell
+  noise the comparison resolves is printed with it.
 """
 import numpy as np
 import pytest
@@ -84,6 +94,65 @@ def test_statistics_within_reference_band(runs, name):
     assert np.all((counts >= lo) & (counts <= hi))
 
 
+@pytest.mark.parametrize("name", ["fp64", "mixed"])
+def test_stress_and_heat_flux_within_reference_band(runs, name):
+    dm, mess, g0, out = runs
+    g = golden("macro_band.npz")
+    acc, counts, nsteps = out[name]
+    assert nsteps == int(g["steps"]) - int(g["avg_from"]) + 1
+    f = I.macro_from_moments(acc, nsteps, dm, mess)[:, g["columns"]]
+    K = int(g["k"])
+    sd = g["sd"] * np.sqrt(1.0 + 1.0 / K)
+    ok = np.isfinite(f) & np.isfinite(g["mean"]) & (sd > 0)
+    assert ok.mean() > 0.9
+    z = (f[ok] - g["mean"][ok]) / sd[ok]
+    assert np.mean(np.abs(z) <= 3.0) >= 0.95
+    assert abs(np.mean(z)) < 0.3
+    for j in range(f.shape[1]):
+        zj = (f[ok[:, j], j] - g["mean"][ok[:, j], j]) / sd[ok[:, j], j]
+        assert abs(np.mean(zj)) < 0.3, (int(g["columns"][j]), float(np.mean(zj)))
+
+
+@pytest.mark.parametrize("name,prec", [("fp64", gpu.PRECISION_FP64), ("mixed", gpu.PRECISION_MIXED)])
+def test_capsule_statistics_within_reference_band(name, prec):
+    """rho, u, T, Tr over steps 61-120 on the capsule tets at Kn 0.01 from 8
+    particles per cell, every third cell, against the 8 reference runs; the
+    particle count of every step within their spread."""
+    g = golden("stats_band_capsule.npz")
+    raw, dm, mess = I.capsule_small()
+    x, v, ir, cell = I.fill_inputs_any(dm, mess, int(g["ppc"]), 3)
+    steps, a0 = int(g["steps"]), int(g["avg_from"])
+    acc = np.zeros((dm.ncell, 18))
+    counts = []
+    with make_case(dm, mess, precision=prec, seed=13, keep_step_moments=1) as case:
+        case.upload_particles(x, v, ir, cell)
+        case.statistic_macroPre()
+        for s in range(1, steps + 1):
+            case.step(s)
+            if s >= a0:
+                acc += case.step_moments()
+            counts.append(case.particle_count())
+        c = case.counters()
+    assert c["lost"] == 0 and c["overflow"] == 0
+    f = I.fields_from_moments(acc, steps - a0 + 1, dm, mess)[g["cells"]]
+    K = int(g["k"])
+    mean = g["mean"].astype(float)
+    sd = g["sd"].astype(float) * np.sqrt(1.0 + 1.0 / K)
+    ok = np.isfinite(mean) & np.isfinite(f) & (sd > 0)
+    assert ok.mean() > 0.95
+    z = (f[ok] - mean[ok]) / sd[ok]
+    frac = float(np.mean(np.abs(z) <= 3.0))
+    print(f"capsule band, {name}: {frac:.4f} of (cell, field) within 3 sigma, mean z {np.mean(z):+.3f}")
+    assert frac >= 0.95
+    assert abs(np.mean(z)) < 0.3
+    for j in range(6):
+        zj = (f[ok[:, j], j] - mean[ok[:, j], j]) / sd[ok[:, j], j]
+        assert abs(np.mean(zj)) < 0.3, j
+    ref_n = g["nparticles"].astype(float)
+    lo, hi = ref_n.min(0) * 0.97, ref_n.max(0) * 1.03
+    assert np.all((np.array(counts) >= lo) & (np.array(counts) <= hi))
+
+
 def test_mixed_cells_within_fp64_band(runs):
     dm, mess, g, out = runs
     fr = I.fields_from_moments(out["fp64"][0], out["fp64"][2], dm, mess)
@@ -103,21 +172,36 @@ def test_mixed_domain_fields_within_half_percent_of_fp64():
     dm, mess = wl["dm"], wl["mess"]
     from pydsmc import workload as W
     fill = W.initial_fill(dm, mess, 50, seed=0, inflow_dir=wl["inflow_dir"])
-    dom = {}
+    dom, win = {}, {}
     for name, prec, seed in (("fp64", gpu.PRECISION_FP64, 21), ("mixed", gpu.PRECISION_MIXED, 22)):
         p = gpu.default_params(precision=prec, seed=seed, zones=wl["zones"], inflow_dir=wl["inflow_dir"],
                                keep_step_moments=1)
         acc = np.zeros((dm.ncell, 18))
+        wacc = np.zeros((dm.ncell, 18))
+        windows = []
         with gpu.Case(dm, mess, p, device=0) as case:
             case.upload_particles(fill["x"], fill["v"], fill["ir"], fill["cell"])
             case.statistic_macroPre()
             for s in range(1, 401):
                 case.step(s)
                 if s > 200:
-                    acc += case.step_moments()
+                    m = case.step_moments()
+                    acc += m
+                    wacc += m
+                    if s % 20 == 0:
+                        windows.append(I.macro_from_moments(wacc, 20, dm, mess))
+                        wacc[:] = 0.0
             c = case.counters()
         assert c["lost"] == 0 and c["overflow"] == 0
         dom[name] = _domain_fields(acc, float(mess["dr"]))
+        win[name] = np.stack(windows)
+    from pydsmc import fields
+    cmp = fields.compare_windows(win["mixed"], win["fp64"], dm.cells["area"])
+    print("mixed vs FP64 per field (domain_rel, within_3se, rel_noise):",
+          {k: tuple(round(x, 5) for x in v.values()) for k, v in cmp["fields"].items()})
+    assert cmp["windows"] == 10 and cmp["cells"] > 0.9 * dm.ncell
+    assert cmp["worst_within_3se"] >= 0.95, cmp["worst_within_3se"]
+    assert cmp["worst_domain_rel"] <= 5e-3, cmp["worst_domain_rel"]
     ref, mix = dom["fp64"], dom["mixed"]
     speed = np.linalg.norm(ref[1:4])
     assert abs(mix[0] - ref[0]) <= 5e-3 * ref[0], (mix[0], ref[0])
