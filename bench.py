@@ -307,11 +307,14 @@ def full_run(wl, plan, args, precision, init, shape, rank, barrier, clock_index=
             clk = ClockSampler(clock_index) if clock_index is not None else None
             if clk:
                 clk.__enter__()
+            # a named range around the timed steps, for profilers
+            torch.cuda.nvtx.range_push(f"timed-{'mixed' if precision == gpu.PRECISION_MIXED else 'fp64'}")
             ev0.record(stream)
         case.step(istep)
         if istep == last:
             ev1.record(stream)
             ev1.synchronize()
+            torch.cuda.nvtx.range_pop()
             if clk:
                 clk.__exit__()
                 res["clocks"] = clk.summary()

@@ -313,8 +313,9 @@ __device__ __forceinline__ ExitHit find_exit_exact(const DevMesh& M, int cell, i
 // triangle test per triangle. The result is only trusted when it is clear of
 // every tie the triangle tests could resolve differently: a second plane
 // reached within the error bound (edge or vertex), a tiny or negative t, a
-// plane grazed while the particle sits on it, a position outside a face
-// plane, and for quads a hit point within the bound of the split diagonal
+// position on, outside or within twice the error bound of any face plane
+// other than the entry face's, and for quads a hit point within the bound of
+// the split diagonal
 // (which sub-triangle). Otherwise `ambiguous` is set and the caller runs the
 // triangle search. The entry face (crossf) is never the exit: the particle
 // sits on it and moves away from it.
@@ -350,11 +351,11 @@ __device__ __forceinline__ PlaneHit find_exit_planes(const DevMesh& M, int cell,
         const double num = d - (x[0] * nx + x[1] * ny + x[2] * nz);
         const double dErr = K * eps * (fabs(d) + xnorm);
         const double vErr = K * eps * vnorm;
-        if (num < -dErr) amb = true;                    // outside this face plane
-        if (vn <= vErr) {
-            if (vn > -vErr && num <= dErr) amb = true;  // grazing the plane it sits on
-            continue;
-        }
+        // on, outside or within the error bound of a face it did not enter
+        // through: the reference's test of that face's triangles can see a
+        // hit at t ~ 0 (a start on a vertex, an edge or a face)
+        if (num <= 2.0 * dErr) amb = true;
+        if (vn <= vErr) continue;
         const double t = num / vn;
         const double tErr = (dErr + fabs(t) * vErr) / vn;
         if (t < best) {

@@ -82,7 +82,9 @@ def test_mixed_trace_bit_exact(block):
     rate = _fallback_rate(c, len(cell))
     print(f"mixed block trace: {c['fp64_fallbacks']} FP64 scans in {len(cell) + c['crossings']} exit searches "
           f"({rate:.2e})")
-    assert 0 < c["fp64_fallbacks"] and rate < 0.05
+    # the side faces (zone 7) have no role in the reference's table: every
+    # search after such a hit is the FP64 scan, as in the reference
+    assert 0 < c["fp64_fallbacks"] and rate < 0.1
 
 
 @pytest.fixture(scope="module")
