@@ -1558,12 +1558,92 @@ __global__ void __launch_bounds__(128) sample_kernel(StepArgs<Real> a, int pre)
     }
 }
 
+// Mixed path: a segmented warp reduction. Cells are taken in groups of 32
+// consecutive cells (by index, so the grouping does not depend on the
+// launch); lane j of the warp that takes a group keeps the running moment
+// sums of the group's cell j. The warp walks the group's particles 32 slots
+// at a time: every lane forms its particle's 18 terms in FP64 (each
+// operation rounded on its own, as cell_moments), a segmented scan by cell
+// over the warp (a fixed shuffle tree) leaves each cell's sum over the chunk
+// in the cell's last lane, and each owner lane adds its cell's chunk sum.
+// The order of additions depends only on the cells' particle counts, so the
+// result does not depend on the launch shape. At the end every owner lane
+// folds its cell's moments into the accumulators (sample_cell), empty cells
+// included.
+__global__ void __launch_bounds__(128) sample_seg_kernel(StepArgs<float> a, int pre)
+{
+    const int istep = a.ctl->istep;
+    const int lane = threadIdx.x & 31;
+    const int ncell = a.M.ncell;
+    const int ngroups = (ncell + 31) >> 5;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngroups; g += warps) {
+        const int c0 = g << 5;
+        const int myc = c0 + lane;
+        const int cEnd = min(c0 + 32, ncell);
+        const int gs = a.startA[c0];
+        const int ge = a.startA[cEnd];
+        const int ms = myc < ncell ? a.startA[myc] : ge;
+        const int me = myc < ncell ? a.startA[myc + 1] : ge;
+        double tot[18];
+#pragma unroll
+        for (int k = 0; k < 18; ++k) tot[k] = 0.0;
+        for (int base = gs; base < ge; base += 32) {
+            const int sidx = base + lane;
+            const bool live = sidx < ge;
+            const int cell = live ? a.A.cell[sidx] : -1;
+            double t[18];
+            {
+                const double x = live ? (double)a.A.v[0][sidx] : 0.0;
+                const double y = live ? (double)a.A.v[1][sidx] : 0.0;
+                const double z = live ? (double)a.A.v[2][sidx] : 0.0;
+                const double I = live ? (double)a.A.ir[sidx] : 0.0;
+                const double v2 = da(da(dm(x, x), dm(y, y)), dm(z, z));
+                t[0] = live ? 1.0 : 0.0; t[1] = x; t[2] = y; t[3] = z; t[4] = v2;
+                t[5] = dm(x, x); t[6] = dm(x, y); t[7] = dm(y, y); t[8] = dm(y, z); t[9] = dm(z, z); t[10] = dm(z, x);
+                t[11] = dm(x, v2); t[12] = dm(y, v2); t[13] = dm(z, v2);
+                t[14] = I; t[15] = dm(x, I); t[16] = dm(y, I); t[17] = dm(z, I);
+            }
+            // segmented inclusive scan: a lane adds what the lane o below it
+            // holds when both belong to the same cell
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int co = __shfl_up_sync(kFull, cell, o);
+                const bool same = lane >= o && co == cell;
+#pragma unroll
+                for (int k = 0; k < 18; ++k) {
+                    const double y = __shfl_up_sync(kFull, t[k], o);
+                    if (same) t[k] = da(t[k], y);
+                }
+            }
+            // the owner of each cell takes the sum from the cell's last lane
+            // in this chunk
+            const int lo = max(ms, base), hi = min(me, base + 32);
+            const bool has = hi > lo;
+            const int src = has ? hi - 1 - base : 0;
+#pragma unroll
+            for (int k = 0; k < 18; ++k) {
+                const double y = __shfl_sync(kFull, t[k], src);
+                if (has) tot[k] = da(tot[k], y);
+            }
+        }
+        if (myc < ncell) sample_cell<float>(a, myc, tot, istep, pre != 0);
+    }
+}
+
 template <typename Real>
 void launch_sample(const StepArgs<Real>& a, bool pre, const LaunchShape& L, cudaStream_t s)
 {
-    int g = (a.M.ncell + 127) / 128;
-    if (g > L.smCount * 16) g = L.smCount * 16;
-    sample_kernel<Real><<<g > 0 ? g : 1, 128, 0, s>>>(a, pre ? 1 : 0);
+    if constexpr (sizeof(Real) == 4) {
+        const int groups = (a.M.ncell + 31) / 32;
+        int g = (groups + 3) / 4;
+        if (g > L.smCount * 16) g = L.smCount * 16;
+        sample_seg_kernel<<<g > 0 ? g : 1, 128, 0, s>>>(a, pre ? 1 : 0);
+    } else {
+        int g = (a.M.ncell + 127) / 128;
+        if (g > L.smCount * 16) g = L.smCount * 16;
+        sample_kernel<Real><<<g > 0 ? g : 1, 128, 0, s>>>(a, pre ? 1 : 0);
+    }
 }
 
 // ===========================================================================

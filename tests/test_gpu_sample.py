@@ -52,3 +52,29 @@ def test_sampling_and_sparse_write_back_match_the_reference(pre):
         assert np.array_equal(cn["sparse_state"], g[pre + "sparse_state"])
     if pre:
         assert (g["rule_sparse_state"] == 2).sum() > 5
+
+
+def test_mixed_sampling_sums_every_particle_once(block):
+    """The mixed path samples by a segmented warp reduction: every cell's 18
+    raw moments are the sums over exactly its particles (ragged cells, empty
+    ones included), within FP64 rounding of numpy's sums of the same FP32
+    state."""
+    raw, dm, mess = block
+    x, v, ir, cell = I.ragged(I.fill_inputs(dm, mess, 70, seed=41), dm.ncell, 70, seed=42)
+    with make_case(dm, mess, precision=gpu.PRECISION_MIXED, keep_step_moments=1) as case:
+        case.upload_particles(x, v, ir, cell)
+        case.statistic_macroPre()
+        case.step(1, STAGE_SAMPLE)
+        got = case.step_moments()
+    vf = v.astype(np.float32).astype(np.float64)
+    irf = ir.astype(np.float32).astype(np.float64)
+    X, Y, Z = vf[:, 0], vf[:, 1], vf[:, 2]
+    v2 = X * X + Y * Y + Z * Z
+    terms = np.stack([np.ones_like(X), X, Y, Z, v2, X * X, X * Y, Y * Y, Y * Z, Z * Z, Z * X,
+                      X * v2, Y * v2, Z * v2, irf, X * irf, Y * irf, Z * irf], 1)
+    want = np.zeros((dm.ncell, 18))
+    np.add.at(want, cell, terms)
+    assert (want[:, 0] == 0).any() and want[:, 0].max() > 32      # empty cells and cells over a warp
+    assert np.array_equal(got[:, 0], want[:, 0])
+    scale = np.abs(terms).max(0) * np.maximum(want[:, :1], 1.0)
+    assert np.all(np.abs(got - want) <= 1e-12 * scale)
