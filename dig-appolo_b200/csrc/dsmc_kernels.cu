@@ -246,7 +246,9 @@ void launch_inject(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s
 // whole step; where the first exit search settles that (stays_for_the_step)
 // the particle is advanced and stored right there. The others are appended
 // to a work list (warp-aggregated, in the sort's rank array, which is free
-// until the sort).
+// until the sort), with the crossing that search settled, if any (mixed
+// path, in the sort's idx array beside it), so that the tracing pass starts
+// from it instead of searching again.
 //
 // Tracing pass (move_kernel): the listed particles, traced from their start
 // by trace_step. Warps claim chunks of 128 list entries from a cursor in
@@ -272,12 +274,13 @@ __global__ void __launch_bounds__(256) move_stay_kernel(StepArgs<Real> a)
     for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const int i = base + (int)threadIdx.x;
         bool defer = false;
+        int known = -1;
         if (i < n) {
             const int cell = a.A.cell[i];
             PRegs<Real> p;
             load_position(a.M, a.A, i, cell, p);
             p.v[0] = a.A.v[0][i]; p.v[1] = a.A.v[1][i]; p.v[2] = a.A.v[2][i];
-            if (stays_for_the_step<Real>(a.M, cell, p, dt)) {
+            if (stays_for_the_step<Real>(a.M, cell, p, dt, &known)) {
                 advance(p, dt);
                 store_position(a.M, a.A, i, cell, p);
             } else {
@@ -289,7 +292,11 @@ __global__ void __launch_bounds__(256) move_stay_kernel(StepArgs<Real> a)
             int at = 0;
             if (lane == 0) at = atomicAdd(&a.ctl->moveList, __popc(m));
             at = __shfl_sync(kFull, at, 0);
-            if (defer) a.rank[at + __popc(m & ((1u << lane) - 1u))] = i;
+            if (defer) {
+                const int pos = at + __popc(m & ((1u << lane) - 1u));
+                a.rank[pos] = i;
+                if constexpr (sizeof(Real) == 4) a.idx[pos] = known;
+            }
         }
     }
 }
@@ -330,14 +337,15 @@ __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
             const int take = min(chunkEnd - chunkNext, __popc(want));
             const bool mine = ((want >> lane) & 1u) && __popc(want & lower) < take;
             if (mine) {
-                i = list[chunkNext + __popc(want & lower)];
+                const int pos = chunkNext + __popc(want & lower);
+                i = list[pos];
                 cell = a.A.cell[i];
                 load_position(a.M, a.A, i, cell, p);
                 p.v[0] = a.A.v[0][i]; p.v[1] = a.A.v[1][i]; p.v[2] = a.A.v[2][i];
                 p.ir = a.A.ir[i];
                 rs.init((uint32_t)i, (uint32_t)istep, kPurposeWall, a.C.seedLo, a.C.seedHi);
                 dtleft = dt0;
-                st.begin(-1, -1);
+                st.begin(-1, -1, sizeof(Real) == 4 ? a.idx[pos] : -1);
                 wallBefore = cnt.wall;
             }
             chunkNext += take;
