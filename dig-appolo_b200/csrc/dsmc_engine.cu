@@ -1137,11 +1137,14 @@ struct Engine {
         if (s.move_blocks_per_sm < 1 || s.move_blocks_per_sm > 32 || s.sort_blocks_per_sm < 1 ||
             s.sort_blocks_per_sm > 32 || s.collide_blocks_per_sm < 1 || s.collide_blocks_per_sm > 32)
             return fail("launch shape: blocks per SM outside [1, 32]");
+        if (s.stay_per_thread != 1 && s.stay_per_thread != 2 && s.stay_per_thread != 4)
+            return fail("launch shape: stay_per_thread must be 1, 2 or 4");
         // work already queued keeps the shape it was launched with
         shape.moveThreads = s.move_threads;
         shape.moveBlocksPerSm = s.move_blocks_per_sm;
         shape.sortBlocksPerSm = s.sort_blocks_per_sm;
         shape.collideBlocksPerSm = s.collide_blocks_per_sm;
+        shape.stayPerThread = s.stay_per_thread;
         dropGraphs();
         return true;
     }
@@ -1153,13 +1156,15 @@ struct Engine {
         s.move_blocks_per_sm = shape.moveBlocksPerSm;
         s.sort_blocks_per_sm = shape.sortBlocksPerSm;
         s.collide_blocks_per_sm = shape.collideBlocksPerSm;
+        s.stay_per_thread = shape.stayPerThread;
         return s;
     }
 
     // The autotuner: runs full steps of this case from step `istep` on,
     // timing each stage with events, and keeps per stage the fastest of a
-    // few launch shapes (move: block size x blocks per SM; rank / scatter /
-    // gather: blocks per SM; collide: blocks per SM). Since no kernel's
+    // few launch shapes (move: block size x blocks per SM, particles per
+    // thread of the stay pass; rank / scatter / gather: blocks per SM;
+    // collide: blocks per SM). Since no kernel's
     // result depends on its launch shape, the steps it runs are ordinary
     // steps of the case; on return `istep` is the next step to run.
     bool autotune(int& istep, int trialSteps)
@@ -1192,6 +1197,15 @@ struct Engine {
                 ok = trial(c, 1, ms);
                 if (ok && ms < bestMs) { bestMs = ms; best = c; }
             }
+        const int perThread[3] = {1, 2, 4};
+        for (int k = 0; ok && k < 3; ++k) {
+            DsmcLaunchShape c = best;
+            c.stay_per_thread = perThread[k];
+            if (c.stay_per_thread == best.stay_per_thread) continue;
+            double ms = 0.0;
+            ok = trial(c, 1, ms);
+            if (ok && ms < bestMs) { bestMs = ms; best = c; }
+        }
         if (ok) ok = trial(best, 2, bestMs);
         for (int b = 0; ok && b < 4; ++b) {
             DsmcLaunchShape c = best;

@@ -265,37 +265,54 @@ void launch_inject(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s
 // order, or which lane or warp traces a particle.
 constexpr int kMoveChunk = 128;
 
-template <typename Real>
+// K particles per thread (K x 256 consecutive slots per block and round):
+// the loads of all K are issued before the first decision.
+template <typename Real, int K>
 __global__ void __launch_bounds__(256) move_stay_kernel(StepArgs<Real> a)
 {
     const int n = a.ctl->nLive;
     const double dt = a.C.dtime;
     const int lane = threadIdx.x & 31;
-    for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const int i = base + (int)threadIdx.x;
-        bool defer = false;
-        int known = -1;
-        if (i < n) {
-            const int cell = a.A.cell[i];
-            PRegs<Real> p;
-            load_position(a.M, a.A, i, cell, p);
-            p.v[0] = a.A.v[0][i]; p.v[1] = a.A.v[1][i]; p.v[2] = a.A.v[2][i];
-            if (stays_for_the_step<Real>(a.M, cell, p, dt, &known)) {
-                advance(p, dt);
-                store_position(a.M, a.A, i, cell, p);
-            } else {
-                defer = true;
+    const int tile = K * (int)blockDim.x;
+    for (int base = blockIdx.x * tile; base < n; base += gridDim.x * tile) {
+        int cell[K];
+        PRegs<Real> p[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int i = base + k * (int)blockDim.x + (int)threadIdx.x;
+            cell[k] = i < n ? a.A.cell[i] : -1;
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int i = base + k * (int)blockDim.x + (int)threadIdx.x;
+            if (cell[k] >= 0) {
+                load_position(a.M, a.A, i, cell[k], p[k]);
+                p[k].v[0] = a.A.v[0][i]; p[k].v[1] = a.A.v[1][i]; p[k].v[2] = a.A.v[2][i];
             }
         }
-        const unsigned m = __ballot_sync(kFull, defer);
-        if (m) {
-            int at = 0;
-            if (lane == 0) at = atomicAdd(&a.ctl->moveList, __popc(m));
-            at = __shfl_sync(kFull, at, 0);
-            if (defer) {
-                const int pos = at + __popc(m & ((1u << lane) - 1u));
-                a.rank[pos] = i;
-                if constexpr (sizeof(Real) == 4) a.idx[pos] = known;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int i = base + k * (int)blockDim.x + (int)threadIdx.x;
+            bool defer = false;
+            int known = -1;
+            if (cell[k] >= 0) {
+                if (stays_for_the_step<Real>(a.M, cell[k], p[k], dt, &known)) {
+                    advance(p[k], dt);
+                    store_position(a.M, a.A, i, cell[k], p[k]);
+                } else {
+                    defer = true;
+                }
+            }
+            const unsigned m = __ballot_sync(kFull, defer);
+            if (m) {
+                int at = 0;
+                if (lane == 0) at = atomicAdd(&a.ctl->moveList, __popc(m));
+                at = __shfl_sync(kFull, at, 0);
+                if (defer) {
+                    const int pos = at + __popc(m & ((1u << lane) - 1u));
+                    a.rank[pos] = i;
+                    if constexpr (sizeof(Real) == 4) a.idx[pos] = known;
+                }
             }
         }
     }
@@ -376,7 +393,12 @@ void launch_move(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s)
     static_assert(offsetof(StepCtl, moveList) == offsetof(StepCtl, moveCursor) + sizeof(int),
                   "the move's cursor and list count are reset together");
     cudaMemsetAsync(&a.ctl->moveCursor, 0, 2 * sizeof(int), s);
-    move_stay_kernel<Real><<<L.smCount * 8, 256, 0, s>>>(a);
+    if (L.stayPerThread == 4)
+        move_stay_kernel<Real, 4><<<L.smCount * 8, 256, 0, s>>>(a);
+    else if (L.stayPerThread == 2)
+        move_stay_kernel<Real, 2><<<L.smCount * 8, 256, 0, s>>>(a);
+    else
+        move_stay_kernel<Real, 1><<<L.smCount * 8, 256, 0, s>>>(a);
     move_kernel<Real><<<L.smCount * L.moveBlocksPerSm, L.moveThreads, 0, s>>>(a);
 }
 
@@ -1566,92 +1588,12 @@ __global__ void __launch_bounds__(128) sample_kernel(StepArgs<Real> a, int pre)
     }
 }
 
-// Mixed path: a segmented warp reduction. Cells are taken in groups of 32
-// consecutive cells (by index, so the grouping does not depend on the
-// launch); lane j of the warp that takes a group keeps the running moment
-// sums of the group's cell j. The warp walks the group's particles 32 slots
-// at a time: every lane forms its particle's 18 terms in FP64 (each
-// operation rounded on its own, as cell_moments), a segmented scan by cell
-// over the warp (a fixed shuffle tree) leaves each cell's sum over the chunk
-// in the cell's last lane, and each owner lane adds its cell's chunk sum.
-// The order of additions depends only on the cells' particle counts, so the
-// result does not depend on the launch shape. At the end every owner lane
-// folds its cell's moments into the accumulators (sample_cell), empty cells
-// included.
-__global__ void __launch_bounds__(128) sample_seg_kernel(StepArgs<float> a, int pre)
-{
-    const int istep = a.ctl->istep;
-    const int lane = threadIdx.x & 31;
-    const int ncell = a.M.ncell;
-    const int ngroups = (ncell + 31) >> 5;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngroups; g += warps) {
-        const int c0 = g << 5;
-        const int myc = c0 + lane;
-        const int cEnd = min(c0 + 32, ncell);
-        const int gs = a.startA[c0];
-        const int ge = a.startA[cEnd];
-        const int ms = myc < ncell ? a.startA[myc] : ge;
-        const int me = myc < ncell ? a.startA[myc + 1] : ge;
-        double tot[18];
-#pragma unroll
-        for (int k = 0; k < 18; ++k) tot[k] = 0.0;
-        for (int base = gs; base < ge; base += 32) {
-            const int sidx = base + lane;
-            const bool live = sidx < ge;
-            const int cell = live ? a.A.cell[sidx] : -1;
-            double t[18];
-            {
-                const double x = live ? (double)a.A.v[0][sidx] : 0.0;
-                const double y = live ? (double)a.A.v[1][sidx] : 0.0;
-                const double z = live ? (double)a.A.v[2][sidx] : 0.0;
-                const double I = live ? (double)a.A.ir[sidx] : 0.0;
-                const double v2 = da(da(dm(x, x), dm(y, y)), dm(z, z));
-                t[0] = live ? 1.0 : 0.0; t[1] = x; t[2] = y; t[3] = z; t[4] = v2;
-                t[5] = dm(x, x); t[6] = dm(x, y); t[7] = dm(y, y); t[8] = dm(y, z); t[9] = dm(z, z); t[10] = dm(z, x);
-                t[11] = dm(x, v2); t[12] = dm(y, v2); t[13] = dm(z, v2);
-                t[14] = I; t[15] = dm(x, I); t[16] = dm(y, I); t[17] = dm(z, I);
-            }
-            // segmented inclusive scan: a lane adds what the lane o below it
-            // holds when both belong to the same cell
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int co = __shfl_up_sync(kFull, cell, o);
-                const bool same = lane >= o && co == cell;
-#pragma unroll
-                for (int k = 0; k < 18; ++k) {
-                    const double y = __shfl_up_sync(kFull, t[k], o);
-                    if (same) t[k] = da(t[k], y);
-                }
-            }
-            // the owner of each cell takes the sum from the cell's last lane
-            // in this chunk
-            const int lo = max(ms, base), hi = min(me, base + 32);
-            const bool has = hi > lo;
-            const int src = has ? hi - 1 - base : 0;
-#pragma unroll
-            for (int k = 0; k < 18; ++k) {
-                const double y = __shfl_sync(kFull, t[k], src);
-                if (has) tot[k] = da(tot[k], y);
-            }
-        }
-        if (myc < ncell) sample_cell<float>(a, myc, tot, istep, pre != 0);
-    }
-}
-
 template <typename Real>
 void launch_sample(const StepArgs<Real>& a, bool pre, const LaunchShape& L, cudaStream_t s)
 {
-    if constexpr (sizeof(Real) == 4) {
-        const int groups = (a.M.ncell + 31) / 32;
-        int g = (groups + 3) / 4;
-        if (g > L.smCount * 16) g = L.smCount * 16;
-        sample_seg_kernel<<<g > 0 ? g : 1, 128, 0, s>>>(a, pre ? 1 : 0);
-    } else {
-        int g = (a.M.ncell + 127) / 128;
-        if (g > L.smCount * 16) g = L.smCount * 16;
-        sample_kernel<Real><<<g > 0 ? g : 1, 128, 0, s>>>(a, pre ? 1 : 0);
-    }
+    int g = (a.M.ncell + 127) / 128;
+    if (g > L.smCount * 16) g = L.smCount * 16;
+    sample_kernel<Real><<<g > 0 ? g : 1, 128, 0, s>>>(a, pre ? 1 : 0);
 }
 
 // ===========================================================================

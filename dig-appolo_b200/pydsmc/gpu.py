@@ -69,7 +69,8 @@ class GsisReport(C.Structure):
 
 class LaunchShape(C.Structure):
     _fields_ = [("move_threads", C.c_int32), ("move_blocks_per_sm", C.c_int32),
-                ("sort_blocks_per_sm", C.c_int32), ("collide_blocks_per_sm", C.c_int32)]
+                ("sort_blocks_per_sm", C.c_int32), ("collide_blocks_per_sm", C.c_int32),
+                ("stay_per_thread", C.c_int32)]
 
     def as_dict(self):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}

@@ -393,6 +393,7 @@ typedef struct DsmcLaunchShape {
     int32_t move_blocks_per_sm;    /* move grid = SMs x this, 1..32 (particles per thread follow) */
     int32_t sort_blocks_per_sm;    /* rank / scatter / gather grids = SMs x this, 1..32 */
     int32_t collide_blocks_per_sm; /* cap on the collision grid per SM, 1..32 (at most the resident blocks) */
+    int32_t stay_per_thread;       /* particles per thread of the move's stay pass: 1, 2 or 4 */
 } DsmcLaunchShape;
 
 int dsmc_get_launch_shape(DsmcHandle* h, DsmcLaunchShape* out);
@@ -401,7 +402,8 @@ int dsmc_set_launch_shape(DsmcHandle* h, const DsmcLaunchShape* shape);
 
 /* Runs full steps first_istep, first_istep+1, ... of the case, timing each
  * stage, and keeps per stage the fastest of a few shapes (move: block size
- * x blocks per SM; sort: blocks per SM; collide: blocks per SM). The steps
+ * x blocks per SM, particles per thread of the stay pass; sort: blocks per
+ * SM; collide: blocks per SM). The steps
  * are ordinary steps of the case (about 20 x trial_steps of them);
  * *next_istep receives the next step to run, *chosen the shape kept. */
 int dsmc_autotune(DsmcHandle* h, int32_t first_istep, int32_t trial_steps, int32_t* next_istep,

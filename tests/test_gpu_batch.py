@@ -42,9 +42,12 @@ def _same(a, b):
         assert a["counters"][k] == b["counters"][k], k
 
 
-SHAPES = [dict(move_threads=128, move_blocks_per_sm=3, sort_blocks_per_sm=1, collide_blocks_per_sm=1),
-          dict(move_threads=128, move_blocks_per_sm=2, sort_blocks_per_sm=16, collide_blocks_per_sm=5),
-          dict(move_threads=256, move_blocks_per_sm=32, sort_blocks_per_sm=3, collide_blocks_per_sm=9)]
+SHAPES = [dict(move_threads=128, move_blocks_per_sm=3, sort_blocks_per_sm=1, collide_blocks_per_sm=1,
+               stay_per_thread=1),
+          dict(move_threads=128, move_blocks_per_sm=2, sort_blocks_per_sm=16, collide_blocks_per_sm=5,
+               stay_per_thread=4),
+          dict(move_threads=256, move_blocks_per_sm=32, sort_blocks_per_sm=3, collide_blocks_per_sm=9,
+               stay_per_thread=2)]
 
 
 @pytest.mark.parametrize("precision", [gpu.PRECISION_FP64, gpu.PRECISION_MIXED])

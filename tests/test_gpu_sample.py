@@ -55,9 +55,9 @@ def test_sampling_and_sparse_write_back_match_the_reference(pre):
 
 
 def test_mixed_sampling_sums_every_particle_once(block):
-    """The mixed path samples by a segmented warp reduction: every cell's 18
-    raw moments are the sums over exactly its particles (ragged cells, empty
-    ones included), within FP64 rounding of numpy's sums of the same FP32
+    """Mixed path: every cell's 18 raw moments are the sums over exactly its
+    particles (ragged cells, empty ones and cells longer than a warp
+    included), within FP64 rounding of numpy's sums of the same FP32
     state."""
     raw, dm, mess = block
     x, v, ir, cell = I.ragged(I.fill_inputs(dm, mess, 70, seed=41), dm.ncell, 70, seed=42)

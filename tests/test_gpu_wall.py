@@ -60,7 +60,7 @@ def _compare_with_oracle(dm, mess, x, v, ir, cell, steps, exact_hits, rtol):
 
 def test_wall_tallies_match_the_oracle_block(block):
     raw, dm, mess = block
-    x, v, ir, cell = I.fill_inputs(dm, mess, 20, seed=31)
+    x, v, ir, cell = I.fill_inputs(dm, mess, 60, seed=31)
     _compare_with_oracle(dm, mess, x, v, ir, cell, 1, True, 1e-10)
     _compare_with_oracle(dm, mess, x, v, ir, cell, 3, False, 1e-6)
 
