@@ -521,6 +521,29 @@ __device__ __forceinline__ CertainExit unpack_exit(const DevMesh& M, int packed)
     return CertainExit{true, rec.x, tri, rec.y + (tri == 2 ? 1 : 0), rec.w, k, 0.0f, 0.0f};
 }
 
+// A hint to bring the line holding p into L1 (no effect on results).
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// The records the next exit search in cell `nb` reads, fetched ahead while
+// the crossing into it is being computed (meshes whose cells all have F
+// face records).
+template <typename Real>
+__device__ __forceinline__ void prefetch_cell(const DevMesh& M, int nb)
+{
+    if (nb < 0 || nb >= M.ncell || !M.faceStride) return;
+    const int kb = nb * M.faceStride;
+    prefetch_l1(M.faceRec + kb);
+    if constexpr (sizeof(Real) == 8) {
+        prefetch_l1(M.planeD + (size_t)kb * 8);
+        prefetch_l1(M.planeD + (size_t)(kb + M.faceStride) * 8 - 1);
+    } else {
+        prefetch_l1(M.planeF + kb);
+        prefetch_l1(M.recAux + kb);
+        prefetch_l1(M.cellCenter + (size_t)nb * 3);
+        prefetch_l1(M.cellCenter + (size_t)nb * 3 + 2);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Particle state in registers and the tracing loop.
 // ---------------------------------------------------------------------------
@@ -672,6 +695,7 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
             // triangle for the bit-exact t; any doubt runs the full search
             const PlaneHit ph = find_exit_planes(M, cell, crossf, p.x, p.v);
             double te = DBL_MAX;
+            if (!ph.ambiguous) prefetch_cell<Real>(M, ph.nb);
             if (!ph.ambiguous && isect_exact(M.triD + (size_t)ph.triIdx * 9, p.x, p.v, te)) {
                 face = ph.face; tri = ph.tri; t = te;
                 decided = true;
@@ -710,6 +734,7 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
                 }
                 const double v64[3] = {(double)p.v[0], (double)p.v[1], (double)p.v[2]};
                 double te = DBL_MAX;
+                prefetch_cell<Real>(M, ce.nb);
                 if (isect_exact(M.triD + (size_t)ce.triIdx * 9, p.x, v64, te)) {
                     face = ce.face; tri = ce.tri; t = te;
                     decided = true;
