@@ -456,6 +456,7 @@ def run_ours(args):
                 "freestream velocities, drawn on the device and handed to the run as host arrays)",
         "config": bench_config(wl, plan),
         "timed_steps": [plan["spinup"] + args.warmup + 1, plan["spinup"] + args.warmup + args.steps],
+        "launch_shape": shape,
         "particles": {"at_timed_start": int(mixed["n0"]), "initial": int(init[-1].shape[0]),
                       "parallelism": f"replicas x{world}"},
         "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / args.steps, "dtype": "f64"},
