@@ -253,8 +253,7 @@ def pinned_copy(a):
 def initial_state(wl, plan, args, rank):
     """The initial particles as host arrays (the reference's fill rule: a mean
     of ppc per cell in proportion to the cell volumes, freestream
-    velocities; drawn on the device and read back), in pinned memory, and
-    the launch shapes the autotuner keeps on this case."""
+    velocities; drawn on the device and read back), in pinned memory."""
     import torch
     from pydsmc import gpu
     case = gpu.Case(wl["dm"], wl["mess"], case_params(wl, plan, gpu.PRECISION_MIXED, 1000 + rank),
@@ -263,21 +262,20 @@ def initial_state(wl, plan, args, rank):
     hx, hv, hir, hcell = case.download_particles()
     cols = [pinned_copy(np.ascontiguousarray(hx[:, k])) for k in range(3)] + \
            [pinned_copy(np.ascontiguousarray(hv[:, k])) for k in range(3)] + [pinned_copy(hir), pinned_copy(hcell)]
-    shape = None
-    if not args.no_autotune:
-        case.statistic_macroPre()
-        _, shape = case.autotune(1, trial_steps=1)
     case.close()
-    return cols, shape
+    return cols
 
 
-def full_run(wl, plan, args, precision, init, shape, rank, barrier, clock_index=None, stage_steps=0):
+def full_run(wl, plan, args, precision, init, shape, rank, barrier, clock_index=None, stage_steps=0, tune=False):
     """One run of the case through the C ABI: the host arrays uploaded,
     steps 1..total, the GSIS hand-off at every exchange step after NSS (the
     window-averaged `record` fields and the particle count read back), the
     sampled fields at the end. Wall time of all of it is the run's
     end-to-end figure; steps spinup+warmup+1 .. +steps are timed on the
-    device with CUDA events (barrier and synchronise on both sides)."""
+    device with CUDA events (barrier and synchronise on both sides). With
+    `tune`, the autotuner picks the launch shapes on about 20 ordinary steps
+    of the run ending some 20 steps before the warm-up, on the developed
+    flow the timed steps see."""
     import torch
     from pydsmc import gpu
     case = gpu.Case(wl["dm"], wl["mess"], case_params(wl, plan, precision, 1000 + rank),
@@ -297,7 +295,18 @@ def full_run(wl, plan, args, precision, init, shape, rank, barrier, clock_index=
     case.statistic_macroPre()
     n = case.particle_count()
     nsamp.append((0, n))
-    for istep in range(1, plan["total"] + 1):
+    # the autotuner takes about 20 steps: tune where that ends well before
+    # the warm-up, or not at all on runs too short for it
+    tune_at = -1
+    if tune:
+        tune_at = plan["spinup"] - 40 if plan["spinup"] > 40 else (1 if first > 30 else -1)
+    istep = 0
+    while istep < plan["total"]:
+        istep += 1
+        if istep == tune_at:
+            nxt, res["launch_shape"] = case.autotune(istep, trial_steps=1)
+            istep = nxt - 1
+            continue
         if istep == first:
             case.sync()
             barrier()
@@ -396,10 +405,11 @@ def run_ours(args):
         return over_ranks(x, "sum", "cuda")
 
     peak, peak_kind = load_peaks()
-    init, shape = initial_state(wl, plan, args, rank)
+    init = initial_state(wl, plan, args, rank)
     # --- mixed precision: the full run, the headline steps timed inside it
-    mixed = full_run(wl, plan, args, gpu.PRECISION_MIXED, init, shape, rank, barrier, clock_index=local,
-                     stage_steps=max(3, args.steps // 2))
+    mixed = full_run(wl, plan, args, gpu.PRECISION_MIXED, init, None, rank, barrier, clock_index=local,
+                     stage_steps=max(3, args.steps // 2), tune=not args.no_autotune)
+    shape = mixed.get("launch_shape")
     ms_mixed = max_over_ranks(mixed["ms"])
     ps_mixed = sum_over_ranks(0.5 * (mixed["n0"] + mixed["n1"]) * args.steps)
     value = ps_mixed / (ms_mixed / 1e3)
@@ -409,7 +419,7 @@ def run_ours(args):
     case_m.close()
     # --- the all-FP64 path: the same run from the same host particles
     barrier()
-    fp64 = full_run(wl, plan, args, gpu.PRECISION_FP64, init, None, rank, barrier)
+    fp64 = full_run(wl, plan, args, gpu.PRECISION_FP64, init, None, rank, barrier, tune=not args.no_autotune)
     fp64.pop("case").close()
     ms_fp64 = max_over_ranks(fp64["ms"])
     ps_fp64 = sum_over_ranks(0.5 * (fp64["n0"] + fp64["n1"]) * args.steps)
@@ -459,7 +469,8 @@ def run_ours(args):
         "launch_shape": shape,
         "particles": {"at_timed_start": int(mixed["n0"]), "initial": int(init[-1].shape[0]),
                       "parallelism": f"replicas x{world}"},
-        "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / args.steps, "dtype": "f64"},
+        "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / args.steps, "dtype": "f64",
+                 "launch_shape": fp64.get("launch_shape")},
         "mixed_over_fp64": value / value_fp64 if value_fp64 > 0 else None,
         "field_error_vs_fp64": field_err,
         "stage_ms_per_step": dict(zip(names, [float(x) for x in stage_avg])),
