@@ -1134,15 +1134,11 @@ constexpr int kArena = 512;                   // staged particles per warp
 constexpr int kSmallSlots = 32 * kSmallMax;
 static_assert(kSmallSlots <= kArena, "small-cell slots must fit in the arena");
 
-// accepted pairs waiting for a full warp: a ring of kQueue entries (at most
-// 31 left over plus the 64 a round can add)
-constexpr int kQueue = 96;
-
-// per-warp shared memory: Real arena[4][kArena]; int claim[kArena]; int4 queue[kQueue]
+// per-warp shared memory: Real arena[4][kArena]; int claim[kArena]; int4 queue[64]
 template <typename Real>
 __host__ __device__ constexpr size_t warp_smem_bytes()
 {
-    return (size_t)kArena * (4 * sizeof(Real) + sizeof(int)) + kQueue * sizeof(int4);
+    return (size_t)kArena * (4 * sizeof(Real) + sizeof(int)) + 64 * sizeof(int4);
 }
 template <typename Real>
 __host__ __device__ constexpr size_t cell_smem_bytes()
@@ -1212,14 +1208,10 @@ __device__ __forceinline__ void copy_cell(const PBuf<Real>& buf, int s0, int n, 
 // waits until that one is done. Each channel runs the sliding window of
 // collide_cell (one pending pair per lane, claims by pair index); the pairs
 // that go in a round are tested for acceptance by their own lanes, and the
-// accepted ones, from both channels, join a ring queue in shared memory. An
-// accepted pair keeps the claims on its two particles until it is carried
-// out, so no later pair that shares a particle can be tested before it; the
-// queued pairs share no particle and run in any order. The queue is carried
-// out 32 pairs at a time, one per lane (the costly half of a collision on a
-// full warp), or whatever it holds when no pair could go this round or a
-// channel has handed out and settled all its pairs. A channel whose pairs are
-// done writes its cell back and takes the next. *item holds a cell item
+// accepted ones, from both channels, are queued in shared memory and carried
+// out by consecutive lanes, so the costly half of a collision runs once per
+// round with most lanes busy. A channel whose pairs are done writes its
+// cell back and takes the next. *item holds a cell item
 // already taken from the list, or -1.
 template <typename Real>
 __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& dst, const int* start, Real* arena,
@@ -1237,7 +1229,6 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
     uint32_t sw2[2] = {0u, 0u}, sw3[2] = {0u, 0u};
     int held = item;      // an item taken but not yet placed
     bool more = true;
-    int qHead = 0, qLen = 0;   // the ring queue of accepted pairs (warp-uniform)
     for (;;) {
 #pragma unroll
         for (int ch = 0; ch < 2; ++ch) {
@@ -1327,49 +1318,30 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
         }
         const unsigned m0 = __ballot_sync(kFull, acc[0]);
         const unsigned m1 = __ballot_sync(kFull, acc[1]);
-        const unsigned anyGo = __ballot_sync(kFull, go[0] || go[1]);
-        {
-            const int at0 = qHead + qLen + __popc(m0 & below);
-            if (acc[0]) queue[at0 % kQueue] = make_int4(sk1[0] - cbase[0], sk2[0] - cbase[0], sj[0], (int)sw3[0]);
-            const int at1 = qHead + qLen + __popc(m0) + __popc(m1 & below);
-            if (acc[1])
-                queue[at1 % kQueue] = make_int4(sk1[1] - cbase[1], sk2[1] - cbase[1], sj[1] | (1 << 30), (int)sw3[1]);
+        if (acc[0]) queue[__popc(m0 & below)] = make_int4(sk1[0] - cbase[0], sk2[0] - cbase[0], sj[0], (int)sw3[0]);
+        if (acc[1])
+            queue[__popc(m0) + __popc(m1 & below)] =
+                make_int4(sk1[1] - cbase[1], sk2[1] - cbase[1], sj[1] | (1 << 30), (int)sw3[1]);
+        __syncwarp();
+        const int total = __popc(m0) + __popc(m1);
+        for (int e = lane; e < total; e += 32) {
+            const int4 q = queue[e];
+            const int ch = q.z >> 30;
+            const int base = ch ? cbase[1] : cbase[0];
+            Real* b = arena + base;
+            pair_execute<Real>(b, b + N, b + 2 * N, b + 3 * N, 1, q.x, q.y, ch ? cc[1] : cc[0], istep,
+                               q.z & 0x3fffffff, (uint32_t)q.w, a.C);
         }
-        qLen += __popc(m0) + __popc(m1);
-        if (lane == 0) colls += (uint32_t)(__popc(m0) + __popc(m1));
-        // a pair that went and was not accepted releases its particles now
+        if (lane == 0) colls += (uint32_t)total;
+        __syncwarp();
 #pragma unroll
         for (int ch = 0; ch < 2; ++ch)
             if (go[ch]) {
-                if (!acc[ch]) {
-                    sclaim[sk1[ch]] = INT_MAX;
-                    sclaim[sk2[ch]] = INT_MAX;
-                }
+                sclaim[sk1[ch]] = INT_MAX;
+                sclaim[sk2[ch]] = INT_MAX;
                 sj[ch] = -1;
             }
         __syncwarp();
-        // carry out the queue: a full warp's worth, or all of it when nothing
-        // could go or a channel is about to finish its cell
-        bool flush = anyGo == 0u;
-#pragma unroll
-        for (int ch = 0; ch < 2; ++ch)
-            if (cc[ch] >= 0 && cnext[ch] >= cnp[ch] && __ballot_sync(kFull, sj[ch] >= 0) == 0u) flush = true;
-        while (qLen >= 32 || (flush && qLen > 0)) {
-            const int take = qLen < 32 ? qLen : 32;
-            if (lane < take) {
-                const int4 q = queue[(qHead + lane) % kQueue];
-                const int ch = q.z >> 30;
-                const int base = ch ? cbase[1] : cbase[0];
-                Real* b = arena + base;
-                pair_execute<Real>(b, b + N, b + 2 * N, b + 3 * N, 1, q.x, q.y, ch ? cc[1] : cc[0], istep,
-                                   q.z & 0x3fffffff, (uint32_t)q.w, a.C);
-                sclaim[base + q.x] = INT_MAX;
-                sclaim[base + q.y] = INT_MAX;
-            }
-            qHead = (qHead + take) % kQueue;
-            qLen -= take;
-            __syncwarp();
-        }
         // a channel whose pairs are all done finishes its cell
 #pragma unroll
         for (int ch = 0; ch < 2; ++ch) {
