@@ -276,18 +276,18 @@ __global__ void __launch_bounds__(256) move_stay_kernel(StepArgs<Real> a)
     const int tile = K * (int)blockDim.x;
     for (int base = blockIdx.x * tile; base < n; base += gridDim.x * tile) {
         int cell[K];
+        Real xs[K][3];
         PRegs<Real> p[K];
+        // the slot's own loads first, all of them independent of each other
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const int i = base + k * (int)blockDim.x + (int)threadIdx.x;
-            cell[k] = i < n ? a.A.cell[i] : -1;
-        }
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int i = base + k * (int)blockDim.x + (int)threadIdx.x;
-            if (cell[k] >= 0) {
-                load_position(a.M, a.A, i, cell[k], p[k]);
+            if (i < n) {
+                cell[k] = a.A.cell[i];
+                xs[k][0] = a.A.x[0][i]; xs[k][1] = a.A.x[1][i]; xs[k][2] = a.A.x[2][i];
                 p[k].v[0] = a.A.v[0][i]; p[k].v[1] = a.A.v[1][i]; p[k].v[2] = a.A.v[2][i];
+            } else {
+                cell[k] = -1;
             }
         }
 #pragma unroll
@@ -296,6 +296,15 @@ __global__ void __launch_bounds__(256) move_stay_kernel(StepArgs<Real> a)
             bool defer = false;
             int known = -1;
             if (cell[k] >= 0) {
+                // the position as load_position widens it
+                if constexpr (sizeof(Real) == 8) {
+                    p[k].x[0] = xs[k][0]; p[k].x[1] = xs[k][1]; p[k].x[2] = xs[k][2];
+                } else {
+                    const double* cc = a.M.cellCenter + (size_t)cell[k] * 3;
+                    p[k].x[0] = da(cc[0], (double)xs[k][0]);
+                    p[k].x[1] = da(cc[1], (double)xs[k][1]);
+                    p[k].x[2] = da(cc[2], (double)xs[k][2]);
+                }
                 if (stays_for_the_step<Real>(a.M, cell[k], p[k], dt, &known)) {
                     advance(p[k], dt);
                     store_position(a.M, a.A, i, cell[k], p[k]);
