@@ -186,6 +186,40 @@ struct Stream {
 template <> __device__ __forceinline__ double Stream::uniform<double>() { return uniform64(); }
 template <> __device__ __forceinline__ float Stream::uniform<float>() { return uniform32(); }
 
+// The four uniforms of one wall re-emission from a Stream, in order.
+template <typename Real>
+__device__ __forceinline__ void draw4(Stream& s, const DevConsts&, Real u[4])
+{
+#pragma unroll
+    for (int k = 0; k < 4; ++k) u[k] = s.uniform<Real>();
+}
+
+// A stream over counter (id, step, purpose, n) that is only ever drawn a
+// whole wall re-emission at a time, starting block-aligned: the same words
+// as a Stream drawn the same way (FP32: one block of four words; FP64: two
+// blocks, a 53-bit uniform from each pair), kept in one register (n).
+struct BlockStream {
+    uint32_t id, step, purpose, n;
+    __device__ __forceinline__ void init(uint32_t id_, uint32_t step_, uint32_t purpose_)
+    {
+        id = id_; step = step_; purpose = purpose_; n = 0;
+    }
+};
+template <typename Real>
+__device__ __forceinline__ void draw4(BlockStream& s, const DevConsts& C, Real u[4])
+{
+    if constexpr (sizeof(Real) == 8) {
+        const U4 a = philox4x32_10(U4{s.id, s.step, s.purpose, s.n}, C.seedLo, C.seedHi);
+        const U4 b = philox4x32_10(U4{s.id, s.step, s.purpose, s.n + 1}, C.seedLo, C.seedHi);
+        s.n += 2;
+        u[0] = unit64(a.x, a.y); u[1] = unit64(a.z, a.w); u[2] = unit64(b.x, b.y); u[3] = unit64(b.z, b.w);
+    } else {
+        const U4 a = philox4x32_10(U4{s.id, s.step, s.purpose, s.n}, C.seedLo, C.seedHi);
+        s.n += 1;
+        u[0] = unit32(a.x); u[1] = unit32(a.y); u[2] = unit32(a.z); u[3] = unit32(a.w);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Exact FP64 arithmetic helpers: each operation rounded on its own, as the
 // reference's x86-64 build evaluates them (no fused multiply-add).
@@ -571,15 +605,14 @@ struct WallTally {
 // Diffuse re-emission at a wall (CrossboundarySwitch Wall case,
 // src/ProcessDSMC.cpp:1793-1825): Maxwellian at Twall_ref in the local frame
 // of the wall normal, rotational energy -ln(r) Tw / 2.
-template <typename Real>
+template <typename Real, typename Rng>
 __device__ __forceinline__ void diffuse_reflect(const DevMesh& M, const DevConsts& C, int wslot, int tag,
-                                                PRegs<Real>& p, Stream& rng)
+                                                PRegs<Real>& p, Rng& rng)
 {
     const int which = (tag == 2) ? 1 : 0;
-    const Real r1 = rng.uniform<Real>();
-    const Real r2 = rng.uniform<Real>();
-    const Real al = rng.uniform<Real>();
-    const Real r3 = rng.uniform<Real>();
+    Real u[4];
+    draw4<Real>(rng, C, u);
+    const Real r1 = u[0], r2 = u[1], al = u[2], r3 = u[3];
     Real s, c;
     if constexpr (sizeof(Real) == 8) {
         sincospi(2.0 * al, &s, &c);
@@ -674,9 +707,9 @@ struct TraceState {
 // scan (counter `fp64_fallbacks`). Positions, dtleft and every decision are
 // then those of the FP64 trace from the same stored state; only wall
 // re-emission draws FP32 velocities.
-template <typename Real>
+template <typename Real, typename Rng>
 __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C, PRegs<Real>& p, int& cell,
-                                           double& dtleft, TraceState& st, Stream& rng, int istep,
+                                           double& dtleft, TraceState& st, Rng& rng, int istep,
                                            double* wallTally, TraceCounts& cnt, bool stopAtWall, TraceLog* log)
 {
     int& ifout = st.ifout;
@@ -796,7 +829,7 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
         dtleft = ds(dtleft, t);
         const int ws = M.faceWall[face];
         const Real v0 = p.v[0], v1 = p.v[1], v2 = p.v[2], ir0 = p.ir;
-        diffuse_reflect<Real>(M, C, ws, tri, p, rng);
+        diffuse_reflect<Real, Rng>(M, C, ws, tri, p, rng);
         cnt.wall++;
         if (wallTally && C.wallStats && istep > C.nss) {
             double* T = wallTally + (size_t)ws * 6;
@@ -861,7 +894,7 @@ __device__ int trace_particle(const DevMesh& M, const DevConsts& C, PRegs<Real>&
 {
     TraceState st;
     st.begin(crossf, tag);
-    while (!trace_step<Real>(M, C, p, cell, dtleft, st, rng, istep, wallTally, cnt, stopAtWall, log)) {
+    while (!trace_step<Real, Stream>(M, C, p, cell, dtleft, st, rng, istep, wallTally, cnt, stopAtWall, log)) {
     }
     return st.ifout;
 }

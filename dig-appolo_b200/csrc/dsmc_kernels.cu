@@ -18,6 +18,7 @@
 //            18-moment sums of each cell in particle order.
 #include <climits>
 #include <cstddef>
+#include <type_traits>
 
 #include "dsmc_kernels.cuh"
 #include "dsmc_macro.cuh"
@@ -344,7 +345,10 @@ __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
     int cell = 0;
     double dtleft = 0;
     TraceState st;
-    Stream rs;
+    // the particle's wall draws; the mixed path's in one register (drawn a
+    // re-emission at a time, from block 0)
+    using Rng = typename std::conditional<sizeof(Real) == 4, BlockStream, Stream>::type;
+    Rng rs;
     uint32_t wallBefore = 0;
     for (;;) {
         unsigned want = __ballot_sync(kFull, i < 0);
@@ -369,7 +373,8 @@ __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
                 load_position(a.M, a.A, i, cell, p);
                 p.v[0] = a.A.v[0][i]; p.v[1] = a.A.v[1][i]; p.v[2] = a.A.v[2][i];
                 p.ir = a.A.ir[i];
-                rs.init((uint32_t)i, (uint32_t)istep, kPurposeWall, a.C.seedLo, a.C.seedHi);
+                if constexpr (sizeof(Real) == 4) rs.init((uint32_t)i, (uint32_t)istep, kPurposeWall);
+                else rs.init((uint32_t)i, (uint32_t)istep, kPurposeWall, a.C.seedLo, a.C.seedHi);
                 dtleft = dt0;
                 st.begin(-1, -1, sizeof(Real) == 4 ? a.idx[pos] : -1);
                 wallBefore = cnt.wall;
@@ -379,7 +384,7 @@ __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
         }
         const bool active = i >= 0;
         if (!__any_sync(kFull, active)) break;
-        if (active && trace_step<Real>(a.M, a.C, p, cell, dtleft, st, rs, istep, a.wallTally, cnt, false, nullptr)) {
+        if (active && trace_step<Real, Rng>(a.M, a.C, p, cell, dtleft, st, rs, istep, a.wallTally, cnt, false, nullptr)) {
             if (st.ifout >= 0) {
                 store_position(a.M, a.A, i, cell, p);
                 if (cnt.wall != wallBefore) {
