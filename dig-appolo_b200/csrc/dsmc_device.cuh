@@ -456,21 +456,15 @@ struct CertainExit {
     bool certain;
     int face, tri, triIdx;
     int nb;        // the record's crossing (as PlaneHit::nb)
-    int rec;       // the face record
     float tLo, tHi;
 };
-
-// A certain exit carried from the move's stay pass to its tracing pass:
-// the face record and the quad half, packed (record << 2 | (tri + 1)), or
-// -1 for none.
-__device__ __forceinline__ int pack_exit(const CertainExit& ce) { return ce.certain ? (ce.rec << 2) | (ce.tri + 1) : -1; }
 
 constexpr float kEps32 = 5.9604645e-8f;   // 2^-24
 
 __device__ __forceinline__ CertainExit certain_exit_f32(const DevMesh& M, int cell, int crossf, int tag,
                                                         const float x[3], const float v[3], float absScale)
 {
-    CertainExit r{false, -2, -1, -1, 0, -1, 0.0f, 0.0f};
+    CertainExit r{false, -2, -1, -1, 0, 0.0f, 0.0f};
     const float vnorm = fabsf(v[0]) + fabsf(v[1]) + fabsf(v[2]);
     const float xnorm = fabsf(x[0]) + fabsf(x[1]) + fabsf(x[2]);
     const float vErr = 32.0f * kEps32 * vnorm;
@@ -540,42 +534,9 @@ __device__ __forceinline__ CertainExit certain_exit_f32(const DevMesh& M, int ce
     r.tri = tri;
     r.triIdx = triIdx;
     r.nb = rec.w;
-    r.rec = bi;
     r.tLo = bestLo;
     r.tHi = bestHi;
     return r;
-}
-
-// The certain exit a packed record stands for (its t interval is not kept).
-__device__ __forceinline__ CertainExit unpack_exit(const DevMesh& M, int packed)
-{
-    const int k = packed >> 2;
-    const int tri = (packed & 3) - 1;
-    const int4 rec = M.faceRec[k];
-    return CertainExit{true, rec.x, tri, rec.y + (tri == 2 ? 1 : 0), rec.w, k, 0.0f, 0.0f};
-}
-
-// A hint to bring the line holding p into L1 (no effect on results).
-__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
-
-// The records the next exit search in cell `nb` reads, fetched ahead while
-// the crossing into it is being computed (meshes whose cells all have F
-// face records).
-template <typename Real>
-__device__ __forceinline__ void prefetch_cell(const DevMesh& M, int nb)
-{
-    if (nb < 0 || nb >= M.ncell || !M.faceStride) return;
-    const int kb = nb * M.faceStride;
-    prefetch_l1(M.faceRec + kb);
-    if constexpr (sizeof(Real) == 8) {
-        prefetch_l1(M.planeD + (size_t)kb * 8);
-        prefetch_l1(M.planeD + (size_t)(kb + M.faceStride) * 8 - 1);
-    } else {
-        prefetch_l1(M.planeF + kb);
-        prefetch_l1(M.recAux + kb);
-        prefetch_l1(M.cellCenter + (size_t)nb * 3);
-        prefetch_l1(M.cellCenter + (size_t)nb * 3 + 2);
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -680,15 +641,13 @@ struct TraceState {
     int ifout;        // outcome so far
     int iter;         // exit searches made
     int crossf, tag;  // the face / triangle the particle entered through
-    int known;        // mixed path: the next search's certain crossing, packed (pack_exit), or -1
     bool afterNone;   // the last hit had no handler: use the triangle search
-    __device__ __forceinline__ void begin(int crossf0, int tag0, int known0 = -1)
+    __device__ __forceinline__ void begin(int crossf0, int tag0)
     {
         ifout = kTraceStay;
         iter = 0;
         crossf = crossf0;
         tag = tag0;
-        known = known0;
         afterNone = false;
     }
 };
@@ -728,7 +687,6 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
             // triangle for the bit-exact t; any doubt runs the full search
             const PlaneHit ph = find_exit_planes(M, cell, crossf, p.x, p.v);
             double te = DBL_MAX;
-            if (!ph.ambiguous) prefetch_cell<Real>(M, ph.nb);
             if (!ph.ambiguous && isect_exact(M.triD + (size_t)ph.triIdx * 9, p.x, p.v, te)) {
                 face = ph.face; tri = ph.tri; t = te;
                 decided = true;
@@ -746,18 +704,11 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
                 }
             }
         } else {
-            CertainExit ce;
-            if (st.known >= 0) {
-                // settled by the stay pass from this very state: a crossing
-                ce = unpack_exit(M, st.known);
-                st.known = -1;
-            } else {
-                const double* cc = M.cellCenter + (size_t)cell * 3;
-                const double c0 = cc[0], c1 = cc[1], c2 = cc[2];
-                const float xr[3] = {(float)ds(p.x[0], c0), (float)ds(p.x[1], c1), (float)ds(p.x[2], c2)};
-                const float absScale = (float)(fabs(c0) + fabs(c1) + fabs(c2));
-                ce = certain_exit_f32(M, cell, crossf, tag, xr, p.v, absScale);
-            }
+            const double* cc = M.cellCenter + (size_t)cell * 3;
+            const double c0 = cc[0], c1 = cc[1], c2 = cc[2];
+            const float xr[3] = {(float)ds(p.x[0], c0), (float)ds(p.x[1], c1), (float)ds(p.x[2], c2)};
+            const float absScale = (float)(fabs(c0) + fabs(c1) + fabs(c2));
+            const CertainExit ce = certain_exit_f32(M, cell, crossf, tag, xr, p.v, absScale);
             if (ce.certain) {
                 if (ce.tLo > (float)dtleft * (1.0f + 0x1p-16f)) {
                     // the reference's scan would return this face at t >= dtleft
@@ -767,7 +718,6 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
                 }
                 const double v64[3] = {(double)p.v[0], (double)p.v[1], (double)p.v[2]};
                 double te = DBL_MAX;
-                prefetch_cell<Real>(M, ce.nb);
                 if (isect_exact(M.triD + (size_t)ce.triIdx * 9, p.x, v64, te)) {
                     face = ce.face; tri = ce.tri; t = te;
                     decided = true;
@@ -859,13 +809,9 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
 // search, without the triangle scan. The caller then advances it by dtleft.
 // FP64 path: the plane decision and the reference's test on the chosen
 // triangle; mixed path: certain_exit_f32.
-// Mixed path: a certain crossing found on the way goes to *known (packed),
-// so the tracing pass does not search again.
 template <typename Real>
-__device__ __forceinline__ bool stays_for_the_step(const DevMesh& M, int cell, const PRegs<Real>& p, double dtleft,
-                                                   int* known)
+__device__ __forceinline__ bool stays_for_the_step(const DevMesh& M, int cell, const PRegs<Real>& p, double dtleft)
 {
-    *known = -1;
     if (!(M.allConvex || M.convex[cell])) return false;
     if constexpr (sizeof(Real) == 8) {
         const PlaneHit ph = find_exit_planes(M, cell, -1, p.x, p.v);
@@ -877,9 +823,7 @@ __device__ __forceinline__ bool stays_for_the_step(const DevMesh& M, int cell, c
         const float xr[3] = {(float)ds(p.x[0], c0), (float)ds(p.x[1], c1), (float)ds(p.x[2], c2)};
         const float absScale = (float)(fabs(c0) + fabs(c1) + fabs(c2));
         const CertainExit ce = certain_exit_f32(M, cell, -1, -1, xr, p.v, absScale);
-        if (ce.certain && ce.tLo > (float)dtleft * (1.0f + 0x1p-16f)) return true;
-        *known = pack_exit(ce);
-        return false;
+        return ce.certain && ce.tLo > (float)dtleft * (1.0f + 0x1p-16f);
     }
 }
 
