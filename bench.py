@@ -273,9 +273,9 @@ def full_run(wl, plan, args, precision, init, shape, rank, barrier, clock_index=
     sampled fields at the end. Wall time of all of it is the run's
     end-to-end figure; steps spinup+warmup+1 .. +steps are timed on the
     device with CUDA events (barrier and synchronise on both sides). With
-    `tune`, the autotuner picks the launch shapes on about 20 ordinary steps
-    of the run ending some 20 steps before the warm-up, on the developed
-    flow the timed steps see."""
+    `tune`, the autotuner picks the launch shapes on 29 ordinary steps of
+    the run ending some 30 steps before the warm-up, on the developed flow
+    the timed steps see."""
     import torch
     from pydsmc import gpu
     case = gpu.Case(wl["dm"], wl["mess"], case_params(wl, plan, precision, 1000 + rank),
@@ -295,16 +295,17 @@ def full_run(wl, plan, args, precision, init, shape, rank, barrier, clock_index=
     case.statistic_macroPre()
     n = case.particle_count()
     nsamp.append((0, n))
-    # the autotuner takes about 20 steps: tune where that ends well before
-    # the warm-up, or not at all on runs too short for it
+    # the autotuner runs 29 steps (14 shapes, two steps each, and one to
+    # warm up): tune where that ends well before the warm-up, or not at all
+    # on runs too short for it
     tune_at = -1
     if tune:
-        tune_at = plan["spinup"] - 40 if plan["spinup"] > 40 else (1 if first > 30 else -1)
+        tune_at = plan["spinup"] - 60 if plan["spinup"] > 60 else (1 if first > 45 else -1)
     istep = 0
     while istep < plan["total"]:
         istep += 1
         if istep == tune_at:
-            nxt, res["launch_shape"] = case.autotune(istep, trial_steps=1)
+            nxt, res["launch_shape"] = case.autotune(istep, trial_steps=2)
             istep = nxt - 1
             continue
         if istep == first:
@@ -532,9 +533,10 @@ def gsis_timing(case, wl, seed: int, repeats: int = 3) -> dict:
 
 
 def launches_per_step(wl) -> int:
-    # inject: count, scan, generate; move; sort: rank, scan x2, scatter,
-    # far-slot order, gather; collide: classify, collide; sample
-    return 3 + 1 + 6 + 2 + 1
+    # inject: count, scan, generate; move: stay pass, tracing pass; sort:
+    # rank, scan x2, scatter, far-slot order, gather; collide: classify,
+    # collide; sample
+    return 3 + 2 + 6 + 2 + 1
 
 
 def run_e2e_k(wl, plan, args, init, shape, rank):

@@ -461,6 +461,13 @@ struct CertainExit {
 
 constexpr float kEps32 = 5.9604645e-8f;   // 2^-24
 
+// kAtRest: the search of a particle at rest in its cell (crossf -1, as in
+// the stay pass), which has no entry face and reads no face records in its
+// loop; the same result as the general form with crossf -1.
+// kFaces > 0: the mesh's face records sit at cell * kFaces (faceStride ==
+// kFaces, checked by the caller), and the face loop is unrolled with its
+// loads issued together.
+template <bool kAtRest = false, int kFaces = 0>
 __device__ __forceinline__ CertainExit certain_exit_f32(const DevMesh& M, int cell, int crossf, int tag,
                                                         const float x[3], const float v[3], float absScale)
 {
@@ -469,21 +476,25 @@ __device__ __forceinline__ CertainExit certain_exit_f32(const DevMesh& M, int ce
     const float xnorm = fabsf(x[0]) + fabsf(x[1]) + fabsf(x[2]);
     const float vErr = 32.0f * kEps32 * vnorm;
     const float absErr = 0x1p-30f * absScale;
-    const int b = M.faceStride ? cell * M.faceStride : M.faceOff[cell];
-    const int e = M.faceStride ? b + M.faceStride : M.faceOff[cell + 1];
+    const int b = kFaces ? cell * kFaces : (M.faceStride ? cell * M.faceStride : M.faceOff[cell]);
+    const int e = kFaces ? b + kFaces : (M.faceStride ? b + M.faceStride : M.faceOff[cell + 1]);
     int bi = -1;
     float best = FLT_MAX, bestLo = 0.0f, bestHi = 0.0f, bestTau = 0.0f, bestVn = 0.0f;
     float tauMin = FLT_MAX;   // latest t_f every other approached face allows
     float entA = 0.0f, entB = 0.0f;
     bool ok = true;
+    // the length scale is the cell's (the same in each of its records)
+    const float lc = b < e ? M.recAux[b].y : 0.0f;
+    const float dErr0 = 32.0f * kEps32 * (xnorm + lc) + absErr;
+#pragma unroll(kFaces > 0 ? kFaces : 1)
     for (int k = b; k < e; ++k) {
-        const int4 rec = M.faceRec[k];
+        int4 rec = make_int4(-1, 0, 0, 0);
+        if constexpr (!kAtRest) rec = M.faceRec[k];
         const float4 pl = M.planeF[k];
-        const float lc = M.recAux[k].y;
         const float vn = v[0] * pl.x + v[1] * pl.y + v[2] * pl.z;
         const float num = pl.w - (x[0] * pl.x + x[1] * pl.y + x[2] * pl.z);
-        const float dErr = 32.0f * kEps32 * (fabsf(pl.w) + xnorm + lc) + absErr;
-        if (rec.x == crossf) {
+        const float dErr = 32.0f * kEps32 * fabsf(pl.w) + dErr0;
+        if (!kAtRest && rec.x == crossf) {
             // entry face: moving away from it; its edge with the exit face is
             // checked below (slack entA + t_f * entB)
             if (!(vn < -vErr)) ok = false;
@@ -499,10 +510,12 @@ __device__ __forceinline__ CertainExit certain_exit_f32(const DevMesh& M, int ce
         }
         if (!(num > 2.0f * dErr) || !(fabsf(vn) > vErr)) { ok = false; continue; }
         if (vn < 0.0f) continue;   // left behind: never reached
-        const float t = num / vn;
-        const float tLo = (num - dErr) / (vn + vErr);
-        const float tHi = (num + dErr) / (vn - vErr);
-        const float tau = (num - 2.0f * dErr) / (vn + vErr);
+        // fast divisions (a few ulp, well inside dErr's margin), each bound
+        // then moved outwards by 2^-21 of itself
+        const float t = __fdividef(num, vn);
+        const float tLo = __fdividef(num - dErr, vn + vErr) * (1.0f - 0x1p-21f);
+        const float tHi = __fdividef(num + dErr, vn - vErr) * (1.0f + 0x1p-21f);
+        const float tau = __fdividef(num - 2.0f * dErr, vn + vErr) * (1.0f - 0x1p-21f);
         if (t < best) {
             if (bi >= 0) tauMin = fminf(tauMin, bestTau);
             best = t; bestLo = tLo; bestHi = tHi; bestTau = tau; bestVn = vn; bi = k;
@@ -708,7 +721,9 @@ __device__ __forceinline__ bool trace_step(const DevMesh& M, const DevConsts& C,
             const double c0 = cc[0], c1 = cc[1], c2 = cc[2];
             const float xr[3] = {(float)ds(p.x[0], c0), (float)ds(p.x[1], c1), (float)ds(p.x[2], c2)};
             const float absScale = (float)(fabs(c0) + fabs(c1) + fabs(c2));
-            const CertainExit ce = certain_exit_f32(M, cell, crossf, tag, xr, p.v, absScale);
+            const CertainExit ce = M.faceStride == 4
+                                       ? certain_exit_f32<false, 4>(M, cell, crossf, tag, xr, p.v, absScale)
+                                       : certain_exit_f32<false, 0>(M, cell, crossf, tag, xr, p.v, absScale);
             if (ce.certain) {
                 if (ce.tLo > (float)dtleft * (1.0f + 0x1p-16f)) {
                     // the reference's scan would return this face at t >= dtleft
@@ -822,7 +837,8 @@ __device__ __forceinline__ bool stays_for_the_step(const DevMesh& M, int cell, c
         const double c0 = cc[0], c1 = cc[1], c2 = cc[2];
         const float xr[3] = {(float)ds(p.x[0], c0), (float)ds(p.x[1], c1), (float)ds(p.x[2], c2)};
         const float absScale = (float)(fabs(c0) + fabs(c1) + fabs(c2));
-        const CertainExit ce = certain_exit_f32(M, cell, -1, -1, xr, p.v, absScale);
+        const CertainExit ce = M.faceStride == 4 ? certain_exit_f32<true, 4>(M, cell, -1, -1, xr, p.v, absScale)
+                                                 : certain_exit_f32<true, 0>(M, cell, -1, -1, xr, p.v, absScale);
         return ce.certain && ce.tLo > (float)dtleft * (1.0f + 0x1p-16f);
     }
 }

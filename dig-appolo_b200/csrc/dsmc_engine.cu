@@ -142,6 +142,8 @@ struct Engine {
     StepCtl* ctl = nullptr;
     unsigned long long* counters = nullptr;
     int* cellList = nullptr;
+    int4* cellItem = nullptr;
+    double2* cellItemC = nullptr;
     int* cellWork = nullptr;
     int* cellPairs = nullptr;
     double* cellCons = nullptr;
@@ -806,6 +808,7 @@ struct Engine {
             !alloc(start[0], (size_t)ncell + 1) || !alloc(start[1], (size_t)ncell + 1) || !alloc(ctl, 1) ||
             !alloc(counters, C_COUNT) || !alloc(cellList, (size_t)ncell * 2) || !alloc(cellWork, 8) ||
             !alloc(cellPairs, (size_t)ncell) || !alloc(cellCons, (size_t)ncell) ||
+            !alloc(cellItem, (size_t)ncell) || !alloc(cellItemC, (size_t)ncell) ||
             !alloc(errorWord, 1) || !alloc(uploadFlag, 1))
             return false;
         if (params.keep_step_moments && !alloc(stepMom, (size_t)ncell * 18)) return false;
@@ -1033,6 +1036,7 @@ struct Engine {
         a.windowValid = windowValid; a.wallTally = wallTally; a.ctl = ctl; a.counters = counters;
         a.cellList = cellList; a.cellWork = cellWork; a.errorWord = errorWord;
         a.cellPairs = cellPairs; a.cellCons = cellCons;
+        a.cellItem = cellItem; a.cellItemC = cellItemC;
         return a;
     }
 
@@ -1163,8 +1167,8 @@ struct Engine {
     // The autotuner: runs full steps of this case from step `istep` on,
     // timing each stage with events, and keeps per stage the fastest of a
     // few launch shapes (move: block size x blocks per SM, particles per
-    // thread of the stay pass; rank / scatter / gather: blocks per SM;
-    // collide: blocks per SM). Since no kernel's
+    // thread of the stay pass; rank / scatter / gather: blocks per SM).
+    // Since no kernel's
     // result depends on its launch shape, the steps it runs are ordinary
     // steps of the case; on return `istep` is the next step to run.
     bool autotune(int& istep, int trialSteps)
@@ -1215,16 +1219,9 @@ struct Engine {
             ok = trial(c, 2, ms);
             if (ok && ms < bestMs) { bestMs = ms; best = c; }
         }
-        if (ok) ok = trial(best, 3, bestMs);
-        const int cblocks[3] = {3, 6, 9};
-        for (int b = 0; ok && b < 3; ++b) {
-            DsmcLaunchShape c = best;
-            c.collide_blocks_per_sm = cblocks[b];
-            if (c.collide_blocks_per_sm == best.collide_blocks_per_sm) continue;
-            double ms = 0.0;
-            ok = trial(c, 3, ms);
-            if (ok && ms < bestMs) { bestMs = ms; best = c; }
-        }
+        // collide keeps its grid cap (the resident-block maximum by
+        // default): fewer blocks per SM were slower in every timed run, and
+        // single-step trials of them picked them by noise
         timing = wasTiming;
         for (double& v : stageMs) v = 0.0;
         timedSteps = 0;

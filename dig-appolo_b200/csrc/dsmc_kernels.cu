@@ -394,18 +394,29 @@ __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
     flush_counts(a.counters, cnt);
 }
 
+// resident blocks per SM of the stay pass (1, 2, 4 particles per thread),
+// set by prepare_kernels
+template <typename Real>
+struct StayOcc {
+    static int blocks[3];
+};
+template <typename Real>
+int StayOcc<Real>::blocks[3] = {4, 4, 4};
+
 template <typename Real>
 void launch_move(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s)
 {
     static_assert(offsetof(StepCtl, moveList) == offsetof(StepCtl, moveCursor) + sizeof(int),
                   "the move's cursor and list count are reset together");
     cudaMemsetAsync(&a.ctl->moveCursor, 0, 2 * sizeof(int), s);
+    // one wave: every block resident (the blocks split the slots evenly, so
+    // a second, partial wave would run at a fraction of the occupancy)
     if (L.stayPerThread == 4)
-        move_stay_kernel<Real, 4><<<L.smCount * 8, 256, 0, s>>>(a);
+        move_stay_kernel<Real, 4><<<L.smCount * StayOcc<Real>::blocks[2], 256, 0, s>>>(a);
     else if (L.stayPerThread == 2)
-        move_stay_kernel<Real, 2><<<L.smCount * 8, 256, 0, s>>>(a);
+        move_stay_kernel<Real, 2><<<L.smCount * StayOcc<Real>::blocks[1], 256, 0, s>>>(a);
     else
-        move_stay_kernel<Real, 1><<<L.smCount * 8, 256, 0, s>>>(a);
+        move_stay_kernel<Real, 1><<<L.smCount * StayOcc<Real>::blocks[0], 256, 0, s>>>(a);
     move_kernel<Real><<<L.smCount * L.moveBlocksPerSm, L.moveThreads, 0, s>>>(a);
 }
 
@@ -1167,12 +1178,16 @@ __global__ void classify_kernel(StepArgs<Real> a, int stageMax)
     int* work = a.cellWork;
     for (int base = blockIdx.x * blockDim.x; base < ncell; base += gridDim.x * blockDim.x) {
         const int c = base + threadIdx.x;
-        const int n = c < ncell ? start[c + 1] - start[c] : -1;
+        const int s0 = c < ncell ? start[c] : 0;
+        const int n = c < ncell ? start[c + 1] - s0 : -1;
         // the cell's candidate pair count, one thread per cell (the
-        // collision kernels read it back with pair_fetch)
+        // collision kernels read it back with pair_fetch, or from the
+        // cell's item record)
+        int np = 0;
+        double consCrm = 0.0, crm0 = 0.0;
         if (n > 1) {
-            double consCrm, crm0;
-            a.cellPairs[c] = pair_count(a, c, n, consCrm, crm0);
+            np = pair_count(a, c, n, consCrm, crm0);
+            a.cellPairs[c] = np;
             a.cellCons[c] = consCrm;
         }
         const int cls = n < 0 ? -1 : (n > stageMax ? 0 : (n > kSmallMax ? 1 : 2));
@@ -1186,9 +1201,14 @@ __global__ void classify_kernel(StepArgs<Real> a, int stageMax)
             b = __shfl_sync(kFull, b, leader);
             if (cls == k) {
                 const int pos = b + __popc(m & ((1u << lane) - 1u));
-                if (k == 0) list[pos] = c;
-                else if (k == 1) list[ncell - 1 - pos] = c;
-                else list[ncell + pos] = c;
+                if (k == 2) {
+                    list[ncell + pos] = c;
+                } else {
+                    const int slot = k == 0 ? pos : ncell - 1 - pos;
+                    list[slot] = c;
+                    a.cellItem[slot] = make_int4(c, s0, n, np);
+                    a.cellItemC[slot] = make_double2(consCrm, crm0);
+                }
             }
         }
     }
@@ -1236,23 +1256,32 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
     uint32_t sw2[2] = {0u, 0u}, sw3[2] = {0u, 0u};
     int held = item;      // an item taken but not yet placed
     bool more = true;
+    // the next item index, taken one item ahead (lane 0): the atomic's
+    // round trip overlaps the rounds of the cells in work. Indices are
+    // handed out in increasing order and the loop runs until it sees one
+    // past the end, so an index taken ahead is always used.
+    int ahead = 0;
+    if (lane == 0) ahead = atomicAdd(a.cellWork + 3, 1);
     for (;;) {
 #pragma unroll
         for (int ch = 0; ch < 2; ++ch) {
             while (cc[ch] < 0 && (more || held >= 0)) {
                 int it = held;
                 if (it < 0) {
-                    if (lane == 0) it = atomicAdd(a.cellWork + 3, 1);
-                    it = __shfl_sync(kFull, it, 0);
+                    it = __shfl_sync(kFull, ahead, 0);
+                    if (lane == 0 && it < nItems) ahead = atomicAdd(a.cellWork + 3, 1);
                 }
                 held = -1;
                 if (it >= nItems) {
                     more = false;
                     break;
                 }
-                const int c = it < nHuge ? a.cellList[it] : a.cellList[ncell - 1 - (it - nHuge)];
-                const int s0 = start[c];
-                const int n = start[c + 1] - s0;
+                // the item's record (classify pass): one load instead of the
+                // list, the starts and the pair count one after another
+                const int slot = it < nHuge ? it : ncell - 1 - (it - nHuge);
+                const int4 rec = a.cellItem[slot];
+                const double2 rc = a.cellItemC[slot];
+                const int c = rec.x, s0 = rec.y, n = rec.z;
                 if (n > N) {   // never reached (huge items precede these): flag rather than overflow the arena
                     if (lane == 0) atomicOr(a.errorWord, kErrStageCell);
                     continue;
@@ -1265,15 +1294,9 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
                 Real* const v[4] = {arena + base, arena + N + base, arena + 2 * N + base, arena + 3 * N + base};
                 copy_cell<Real, false>(dst, s0, n, v, 1);
                 __syncwarp();
-                double consCrm = 0.0, crm0 = 0.0;
-                int np = 0;
-                if (lane == 0 && n > 1) {
-                    np = pair_fetch(a, c, consCrm, crm0);
-                    pairs += (uint32_t)np;
-                }
-                np = __shfl_sync(kFull, np, 0);
-                consCrm = __shfl_sync(kFull, consCrm, 0);
-                crm0 = __shfl_sync(kFull, crm0, 0);
+                const int np = n > 1 ? rec.w : 0;
+                const double consCrm = rc.x, crm0 = rc.y;
+                if (lane == 0) pairs += (uint32_t)np;
                 if (!(consCrm > 0.0) || np <= 0) {   // nothing changes: no write-back
                     __syncwarp();
                     continue;
@@ -1477,6 +1500,13 @@ cudaError_t prepare_kernels()
                                                       cell_smem_bytes<Real>());
     if (e != cudaSuccess) return e;
     CellOcc<Real>::blocks = nb > 0 ? nb : 1;
+    const void* stay[3] = {(const void*)move_stay_kernel<Real, 1>, (const void*)move_stay_kernel<Real, 2>,
+                           (const void*)move_stay_kernel<Real, 4>};
+    for (int k = 0; k < 3; ++k) {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stay[k], 256, 0);
+        if (e != cudaSuccess) return e;
+        StayOcc<Real>::blocks[k] = nb > 0 ? nb : 1;
+    }
     return cudaSuccess;
 }
 
@@ -1516,36 +1546,31 @@ __device__ __forceinline__ void cell_moments(const PBuf<Real>& b, int s0, int n,
     }
 }
 
-// Fold one step's moments of cell c into its accumulators, by one thread:
-// statistic_macro, src/ProcessDSMC.cpp:2784-2859 (statistic_macroPre,
-// :3312-3326, when pre).
+// updateStepWindowMoments, :3106-3113, for moment k of a cell: the
+// exponential window (local), the steady sum past NSS (final_record) and the
+// GSIS window sum (every NEVERY steps)
+// (s, sSteady, sWindow: the three accumulators' values before the step).
 template <typename Real>
-__device__ __forceinline__ void sample_cell(const StepArgs<Real>& a, int c, const double* mom, int istep, bool pre)
+__device__ __forceinline__ void fold_moment(const StepArgs<Real>& a, double* acc, int k, double v, int istep,
+                                            double s, double sSteady, double sWindow)
 {
-    const double S = a.M.cellVolume[c];
-    if (a.stepMom)
-        for (int k = 0; k < 18; ++k) a.stepMom[(size_t)c * 18 + k] = mom[k];
-    if (pre) {
-        double out[18];
-        local_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
-        for (int k = 0; k < 18; ++k) a.local[(size_t)c * 18 + k] = out[k];
-        record_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
-        for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
-        return;
-    }
-    double* acc = a.acc + (size_t)c * 54;
     const bool every = (istep % a.C.nevery) == 0;
-    // updateStepWindowMoments, :3106-3113
     const double na = (double)a.C.nscheme;
     const double w = (istep <= a.C.nscheme) ? 1.0 : dd(ds(na, 1.0), na);
     const bool steady = istep > a.C.nss;
-    for (int k = 0; k < 18; ++k) {
-        const double v = mom[k];
-        const double s = acc[k];
-        acc[k] = (w == 1.0) ? da(s, v) : da(dm(w, s), v);
-        if (steady) acc[18 + k] = da(acc[18 + k], v);
-        if (every) acc[36 + k] = da(acc[36 + k], v);
-    }
+    acc[k] = (w == 1.0) ? da(s, v) : da(dm(w, s), v);
+    if (steady) acc[18 + k] = da(sSteady, v);
+    if (every) acc[36 + k] = da(sWindow, v);
+}
+
+// The rest of statistic_macro for cell c once its moments are folded in:
+// the sparse-cell state machine and, at an exchange step, the record fields
+// from the GSIS window.
+template <typename Real>
+__device__ __forceinline__ void sample_cell_tail(const StepArgs<Real>& a, int c, double* acc, int istep)
+{
+    const double S = a.M.cellVolume[c];
+    const bool every = (istep % a.C.nevery) == 0;
     const int ngsis = a.C.nevery * a.C.nrepeat;
     unsigned char st = a.sparseState[c];
     int accum = a.sparseAccum[c];
@@ -1581,6 +1606,29 @@ __device__ __forceinline__ void sample_cell(const StepArgs<Real>& a, int c, cons
     a.sparseAccum[c] = accum;
 }
 
+// Fold one step's moments of cell c into its accumulators, by one thread:
+// statistic_macro, src/ProcessDSMC.cpp:2784-2859 (statistic_macroPre,
+// :3312-3326, when pre).
+template <typename Real>
+__device__ __forceinline__ void sample_cell(const StepArgs<Real>& a, int c, const double* mom, int istep, bool pre)
+{
+    const double S = a.M.cellVolume[c];
+    if (a.stepMom)
+        for (int k = 0; k < 18; ++k) a.stepMom[(size_t)c * 18 + k] = mom[k];
+    if (pre) {
+        double out[18];
+        local_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
+        for (int k = 0; k < 18; ++k) a.local[(size_t)c * 18 + k] = out[k];
+        record_macro_pre(mom, S, a.C.neff, a.C.nref, a.C.dr, out);
+        for (int k = 0; k < 18; ++k) a.record[(size_t)c * 18 + k] = out[k];
+        return;
+    }
+    double* acc = a.acc + (size_t)c * 54;
+    for (int k = 0; k < 18; ++k) fold_moment(a, acc, k, mom[k], istep, acc[k], acc[18 + k], acc[36 + k]);
+    sample_cell_tail(a, c, acc, istep);
+}
+
+
 // statistic_macro / statistic_macroPre over the sorted buffer: one thread
 // per cell.
 template <typename Real>
@@ -1595,9 +1643,86 @@ __global__ void __launch_bounds__(128) sample_kernel(StepArgs<Real> a, int pre)
     }
 }
 
+// statistic_macro of the mixed path, one warp per cell: the lanes sum the
+// cell's particles 32 apart (coalesced loads), lane q < 18 then adds up
+// moment q of the 32 lanes (four groups of eight, through shared memory)
+// and folds it into the cell's accumulators, and lane 0 runs the rest. Its FP64 sums
+// run in another order than the one-thread sums, which the FP64 path keeps
+// (they are the reference's order).
+constexpr int kSampleWarps = 8;
+
+__global__ void __launch_bounds__(kSampleWarps * 32, 3) sample_warp_kernel(StepArgs<float> a)
+{
+    __shared__ double part[kSampleWarps][18][33];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int istep = a.ctl->istep;
+    double (*mine)[33] = part[wib];
+    for (int c = blockIdx.x * kSampleWarps + wib; c < a.M.ncell; c += gridDim.x * kSampleWarps) {
+        const int s0 = a.startA[c];
+        const int e = a.startA[c + 1];
+        double* acc = a.acc + (size_t)c * 54;
+        // the accumulators' old values, loaded while the particles are summed
+        double o0 = 0.0, o1 = 0.0, o2 = 0.0;
+        if (lane < 18) {
+            o0 = acc[lane]; o1 = acc[18 + lane]; o2 = acc[36 + lane];
+        }
+        double m[18];
+#pragma unroll
+        for (int q = 0; q < 18; ++q) m[q] = 0.0;
+        auto add = [&](float fx, float fy, float fz, float fi) {
+            const double x = (double)fx, y = (double)fy, z = (double)fz, I = (double)fi;
+            const double v2 = da(da(dm(x, x), dm(y, y)), dm(z, z));
+            m[0] = da(m[0], 1.0); m[1] = da(m[1], x); m[2] = da(m[2], y); m[3] = da(m[3], z); m[4] = da(m[4], v2);
+            m[5] = da(m[5], dm(x, x)); m[6] = da(m[6], dm(x, y)); m[7] = da(m[7], dm(y, y));
+            m[8] = da(m[8], dm(y, z)); m[9] = da(m[9], dm(z, z)); m[10] = da(m[10], dm(z, x));
+            m[11] = da(m[11], dm(x, v2)); m[12] = da(m[12], dm(y, v2)); m[13] = da(m[13], dm(z, v2));
+            m[14] = da(m[14], I); m[15] = da(m[15], dm(x, I)); m[16] = da(m[16], dm(y, I)); m[17] = da(m[17], dm(z, I));
+        };
+        // two particles per lane and iteration, their loads issued first
+        int k = s0 + lane;
+        for (; k + 32 < e; k += 64) {
+            const float x1 = a.A.v[0][k], y1 = a.A.v[1][k], z1 = a.A.v[2][k], i1 = a.A.ir[k];
+            const float x2 = a.A.v[0][k + 32], y2 = a.A.v[1][k + 32], z2 = a.A.v[2][k + 32], i2 = a.A.ir[k + 32];
+            add(x1, y1, z1, i1);
+            add(x2, y2, z2, i2);
+        }
+        if (k < e) add(a.A.v[0][k], a.A.v[1][k], a.A.v[2][k], a.A.ir[k]);
+#pragma unroll
+        for (int q = 0; q < 18; ++q) mine[q][lane] = m[q];
+        __syncwarp();
+        double mq = 0.0;
+        if (lane < 18) {
+            // four partial sums of eight lanes each, then their pairs
+            double t[4];
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+                t[g] = mine[lane][8 * g];
+#pragma unroll
+                for (int l = 1; l < 8; ++l) t[g] = da(t[g], mine[lane][8 * g + l]);
+            }
+            mq = da(da(t[0], t[1]), da(t[2], t[3]));
+        }
+        __syncwarp();   // the rows are reused for the next cell
+        if (lane < 18) {
+            if (a.stepMom) a.stepMom[(size_t)c * 18 + lane] = mq;
+            fold_moment(a, acc, lane, mq, istep, o0, o1, o2);
+        }
+        __syncwarp();   // lane 0 reads the folded window sums
+        if (lane == 0) sample_cell_tail(a, c, acc, istep);
+    }
+}
+
 template <typename Real>
 void launch_sample(const StepArgs<Real>& a, bool pre, const LaunchShape& L, cudaStream_t s)
 {
+    if constexpr (sizeof(Real) == 4) {
+        if (!pre) {
+            int g = (a.M.ncell + kSampleWarps - 1) / kSampleWarps;
+            if (g > L.smCount * 32) g = L.smCount * 32;
+            sample_warp_kernel<<<g > 0 ? g : 1, kSampleWarps * 32, 0, s>>>(a);
+            return;
+        }
+    }
     int g = (a.M.ncell + 127) / 128;
     if (g > L.smCount * 16) g = L.smCount * 16;
     sample_kernel<Real><<<g > 0 ? g : 1, 128, 0, s>>>(a, pre ? 1 : 0);

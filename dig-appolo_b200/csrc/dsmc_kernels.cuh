@@ -71,6 +71,8 @@ struct StepArgs {
     int* cellPairs;           // [ncell] candidate pair count of the step (classify pass)
     double* cellCons;         // [ncell] majorant term of the pair count (classify pass)
     int* cellList;            // [2*ncell] work lists of the cell pass
+    int4* cellItem;           // [ncell] huge / large items at their list slot: cell, start, count, pairs
+    double2* cellItemC;       // [ncell] the same items' majorant term and crmax
     int* cellWork;            // [8] list lengths and hand-out counters of the cell pass
     int* errorWord;
 };
@@ -84,9 +86,9 @@ struct LaunchShape {
     int smCount = 148;
     int moveThreads = 256;        // threads per block of the move kernel: 128 or 256
     int moveBlocksPerSm = 8;      // move grid = smCount x this
-    int sortBlocksPerSm = 8;      // rank, scatter, gather grids = smCount x this
+    int sortBlocksPerSm = 16;     // rank, scatter, gather grids = smCount x this
     int collideBlocksPerSm = 9;   // collide grid cap per SM (at most the resident blocks)
-    int stayPerThread = 2;        // particles per thread of the move's stay pass: 1, 2 or 4
+    int stayPerThread = 1;        // particles per thread of the move's stay pass: 1, 2 or 4
 };
 
 template <typename Real> void launch_inject(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s);

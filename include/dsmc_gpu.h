@@ -403,8 +403,8 @@ int dsmc_set_launch_shape(DsmcHandle* h, const DsmcLaunchShape* shape);
 /* Runs full steps first_istep, first_istep+1, ... of the case, timing each
  * stage, and keeps per stage the fastest of a few shapes (move: block size
  * x blocks per SM, particles per thread of the stay pass; sort: blocks per
- * SM; collide: blocks per SM). The steps
- * are ordinary steps of the case (about 20 x trial_steps of them);
+ * SM; collide keeps its cap). The steps
+ * are ordinary steps of the case (about 15 x trial_steps of them);
  * *next_istep receives the next step to run, *chosen the shape kept. */
 int dsmc_autotune(DsmcHandle* h, int32_t first_istep, int32_t trial_steps, int32_t* next_istep,
                   DsmcLaunchShape* chosen);
