@@ -23,7 +23,7 @@ import math
 import numpy as np
 
 from . import case as C
-from .mesh import ZONE_INLET, ZONE_INTERIOR, ZONE_OUTLET, ZONE_WALL, RawMesh, _order_by_zone, build_dsmc_mesh
+from .mesh import ZONE_INLET, ZONE_INTERIOR, ZONE_OUTLET, ZONE_WALL, RawMesh, _order_by_zone, build_dsmc_mesh, morton_order
 
 L0 = 3.912
 NOSE_RADIUS = 4.7
@@ -164,7 +164,7 @@ def _split_to_count(pts, tets, target, far, rng):
 
 
 def capsule_mesh(h_fine: float = 0.215, h_coarse: float = 0.60, seed: int = 0, aoa_deg: float = 30.0,
-                 r_fine: float = 4.2, target_cells: int | None = None) -> RawMesh:
+                 r_fine: float = 4.2, target_cells: int | None = None, morton: bool = False) -> RawMesh:
     from scipy.spatial import Delaunay
 
     rng = np.random.default_rng(seed)
@@ -201,6 +201,10 @@ def capsule_mesh(h_fine: float = 0.215, h_coarse: float = 0.60, seed: int = 0, a
         cent = pts[tets].mean(axis=1)
         far = np.linalg.norm(cent - body_c, axis=1) > r_fine + 2.0 * h_coarse
         pts, tets = _split_to_count(pts, tets, int(target_cells), far, np.random.default_rng(seed + 7919))
+    if morton:
+        # cells numbered along a Morton curve of their centroids (the
+        # triangulator's order scatters neighbours across the numbering)
+        tets = tets[morton_order(pts[tets].mean(axis=1))]
     ncell = tets.shape[0]
 
     # faces: 4 per tet, matched by sorted node triple
@@ -258,7 +262,7 @@ def capsule_mesh(h_fine: float = 0.215, h_coarse: float = 0.60, seed: int = 0, a
 def capsule_workload(ppc: int = 100, seed: int = 0):
     """CAP: 372,500 tetrahedra; Ma 5, Kn 0.01 on L0, AoA 30 deg, T_in 142.2 K,
     T_w 300 K diffuse."""
-    raw = capsule_mesh(seed=seed, target_cells=CAP_CELLS)
+    raw = capsule_mesh(seed=seed, target_cells=CAP_CELLS, morton=True)
     dm = build_dsmc_mesh(raw)
     mess = C.mesh_message(dm, 5.0, 0.01, ppc=ppc, L0=L0)
     zones = [(3, 1, 0), (4, 2, 1), (5, 3, 0), (6, 4, 0)]

@@ -80,6 +80,23 @@ class RawMesh:
         return int(self.points.shape[0])
 
 
+def morton_order(points: np.ndarray, bits: int = 21) -> np.ndarray:
+    """Order of `points` (n x 3) along a Morton (Z-order) curve of their
+    bounding box, 2^bits cells per axis: the permutation that numbers
+    nearby points nearby, as mesh tools renumber cells for locality."""
+    p = np.asarray(points, dtype=np.float64)
+    if len(p) == 0:
+        return np.zeros(0, dtype=np.int64)
+    lo, hi = p.min(axis=0), p.max(axis=0)
+    span = np.where(hi > lo, hi - lo, 1.0)
+    q = np.minimum(((p - lo) / span * (1 << bits)).astype(np.uint64), np.uint64((1 << bits) - 1))
+    key = np.zeros(len(p), dtype=np.uint64)
+    for b in range(bits):
+        for a in range(3):
+            key |= ((q[:, a] >> np.uint64(b)) & np.uint64(1)) << np.uint64(3 * b + a)
+    return np.argsort(key, kind="stable")
+
+
 def _order_by_zone(faces, ftype, c0, c1, zone, order=(ZONE_INTERIOR, ZONE_INLET, ZONE_OUTLET, ZONE_WALL, ZONE_SIDE)):
     idx = np.concatenate([np.nonzero(zone == z)[0] for z in order])
     assert idx.size == zone.size

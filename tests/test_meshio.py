@@ -239,3 +239,29 @@ def test_capsule_mesh_has_the_reference_cell_count():
     assert plain.ncell < raw.ncell
     wall = dm.edges["faceTag"] == 6
     assert wall.sum() == int((M.build_dsmc_mesh(plain).edges["faceTag"] == 6).sum())
+
+
+def test_morton_numbering_keeps_the_mesh_and_brings_neighbours_close():
+    """Cells numbered along a Morton curve of their centroids (the bench's
+    CAP mesh): the same cells and faces, renumbered; on a point lattice the
+    order is the Z-order curve; neighbour ids lie closer in the numbering
+    than in the triangulator's order."""
+    from pydsmc import capsule
+    g = np.stack(np.meshgrid(np.arange(4), np.arange(4), np.arange(4), indexing="ij"), -1).reshape(-1, 3)
+    order = M.morton_order(g.astype(float))
+    assert sorted(order.tolist()) == list(range(64))
+    first = g[order[:8]]                                  # the first octant's 2x2x2 block, x fastest
+    assert np.array_equal(first, [[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0],
+                                  [0, 0, 1], [1, 0, 1], [0, 1, 1], [1, 1, 1]])
+    raw0 = capsule.capsule_mesh(h_fine=0.5, h_coarse=1.0)
+    raw1 = capsule.capsule_mesh(h_fine=0.5, h_coarse=1.0, morton=True)
+    dm0, dm1 = M.build_dsmc_mesh(raw0), M.build_dsmc_mesh(raw1)
+    assert dm0.ncell == dm1.ncell and len(dm0.edges) == len(dm1.edges)
+    assert np.isclose(dm0.cells["area"].sum(), dm1.cells["area"].sum(), rtol=1e-12)
+    assert np.array_equal(np.sort(dm0.cells["area"]), np.sort(dm1.cells["area"]))
+
+    def spread(dm):
+        c2c = dm.cells["cell2cell"][:, :4]
+        d = np.abs(c2c - np.arange(dm.ncell)[:, None])[c2c >= 0]
+        return np.percentile(d, 90)
+    assert spread(dm1) < spread(dm0)
