@@ -129,8 +129,9 @@ def measured_traffic(kernel: str, workload: str, particles: float):
     ncu summaries (profiles/<kernel>_<mesh>_ppc<N>.md, lines
     'dram_bytes_per_launch: B' and 'particles: P'): the summary of this very
     workload if there is one, else one of the same mesh at another particle
-    count, scaled to this launch by the particle ratio (full captures are
-    taken on a smaller case). Returns (bytes or None, source note)."""
+    count (full captures are taken on a smaller case), scaled to this launch
+    by the particle ratio (the captured steps hold a slightly different
+    count than the timed ones). Returns (bytes or None, source note)."""
     mesh, _, _ = workload.rpartition("_ppc")
     pdir = os.path.join(ROOT, "profiles")
 
@@ -152,7 +153,7 @@ def measured_traffic(kernel: str, workload: str, particles: float):
         if "dram_bytes_per_launch" not in vals:
             continue
         rel = os.path.relpath(path, ROOT)
-        if path == exact or "particles" not in vals:
+        if "particles" not in vals:
             return vals["dram_bytes_per_launch"], rel
         scale = particles / vals["particles"]
         return vals["dram_bytes_per_launch"] * scale, f"{rel}, scaled by particles x{scale:.3f}"
