@@ -247,8 +247,11 @@ void launch_inject(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s
 // whole step; where the first exit search settles that (stays_for_the_step)
 // the particle is advanced and stored right there. The others are appended
 // to a work list (warp-aggregated, in the sort's rank array, which is free
-// until the sort). (Handing the crossing that search settled to the tracing
-// pass through the work list was measured slower: 2.37 against 2.17 ms.)
+// until the sort), with their state copied to the same positions of the
+// other particle buffer (free until the sort too): the tracing pass then
+// reads its particles in list order instead of gathering them from sparse
+// slots (move 2.18 -> 2.08 ms). (Handing the crossing that search settled
+// to the tracing pass as well was measured slower: 2.37 against 2.17 ms.)
 //
 // Tracing pass (move_kernel): the listed particles, traced from their start
 // by trace_step. Warps claim chunks of 128 list entries from a cursor in
@@ -316,7 +319,17 @@ __global__ void __launch_bounds__(256) move_stay_kernel(StepArgs<Real> a)
                 int at = 0;
                 if (lane == 0) at = atomicAdd(&a.ctl->moveList, __popc(m));
                 at = __shfl_sync(kFull, at, 0);
-                if (defer) a.rank[at + __popc(m & ((1u << lane) - 1u))] = i;
+                if (defer) {
+                    // the entry: the slot, and the particle's state in the
+                    // other buffer (free until the sort) at the same
+                    // position, so the tracing pass reads it in list order
+                    const int j = at + __popc(m & ((1u << lane) - 1u));
+                    a.rank[j] = i;
+                    a.B.cell[j] = cell[k];
+                    a.B.x[0][j] = xs[k][0]; a.B.x[1][j] = xs[k][1]; a.B.x[2][j] = xs[k][2];
+                    a.B.v[0][j] = p[k].v[0]; a.B.v[1][j] = p[k].v[1]; a.B.v[2][j] = p[k].v[2];
+                    a.B.ir[j] = a.A.ir[i];
+                }
             }
         }
     }
@@ -361,11 +374,13 @@ __global__ void __launch_bounds__(256, 3) move_kernel(StepArgs<Real> a)
             const int take = min(chunkEnd - chunkNext, __popc(want));
             const bool mine = ((want >> lane) & 1u) && __popc(want & lower) < take;
             if (mine) {
-                i = list[chunkNext + __popc(want & lower)];
-                cell = a.A.cell[i];
-                load_position(a.M, a.A, i, cell, p);
-                p.v[0] = a.A.v[0][i]; p.v[1] = a.A.v[1][i]; p.v[2] = a.A.v[2][i];
-                p.ir = a.A.ir[i];
+                // the entry's slot and state, as the stay pass wrote them
+                const int j = chunkNext + __popc(want & lower);
+                i = list[j];
+                cell = a.B.cell[j];
+                load_position(a.M, a.B, j, cell, p);
+                p.v[0] = a.B.v[0][j]; p.v[1] = a.B.v[1][j]; p.v[2] = a.B.v[2][j];
+                p.ir = a.B.ir[j];
                 if constexpr (sizeof(Real) == 4) rs.init((uint32_t)i, (uint32_t)istep, kPurposeWall);
                 else rs.init((uint32_t)i, (uint32_t)istep, kPurposeWall, a.C.seedLo, a.C.seedHi);
                 dtleft = dt0;
