@@ -87,7 +87,7 @@ struct LaunchShape {
     int moveThreads = 256;        // threads per block of the move kernel: 128 or 256
     int moveBlocksPerSm = 8;      // move grid = smCount x this
     int sortBlocksPerSm = 16;     // rank, scatter, gather grids = smCount x this
-    int collideBlocksPerSm = 9;   // collide grid cap per SM (at most the resident blocks)
+    int collideBlocksPerSm = 32;  // collide grid cap per SM (at most the resident blocks)
     int stayPerThread = 1;        // particles per thread of the move's stay pass: 1, 2 or 4
 };
 
