@@ -466,30 +466,43 @@ __global__ void __launch_bounds__(256) rank_kernel(StepArgs<Real> a)
             slotQ[j + 1] = __shfl_sync(kFull, rvL, j) + 1;
             runQ[j + 1] = 0;
         }
-        for (int base = b; base < e; base += 32) {
-            const int i = base + lane;
-            const bool valid = i < e;
-            const int d = valid ? a.A.cell[i] : -1;
-            int q = -1;
-            if (d >= 0) {
-                if (d == s) q = 0;
-                else {
+        // the cell ids of up to 128 particles loaded first, then ranked 32 at
+        // a time
+        for (int base4 = b; base4 < e; base4 += 128) {
+            int dq[4];
 #pragma unroll
-                    for (int j = 5; j >= 0; --j)
-                        if (d == nbr[j]) q = j + 1;
+            for (int u = 0; u < 4; ++u) {
+                const int i = base4 + 32 * u + lane;
+                dq[u] = i < e ? a.A.cell[i] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int base = base4 + 32 * u;
+                if (base >= e) break;
+                const int i = base + lane;
+                const bool valid = i < e;
+                const int d = dq[u];
+                int q = -1;
+                if (d >= 0) {
+                    if (d == s) q = 0;
+                    else {
+#pragma unroll
+                        for (int j = 5; j >= 0; --j)
+                            if (d == nbr[j]) q = j + 1;
+                    }
                 }
-            }
-            int packed = -1;
+                int packed = -1;
 #pragma unroll
-            for (int qq = 0; qq < 7; ++qq) {
-                const unsigned m = __ballot_sync(kFull, q == qq);
-                if (q == qq) packed = (slotQ[qq] << 24) | (runQ[qq] + __popc(m & lt));
-                runQ[qq] += __popc(m);
+                for (int qq = 0; qq < 7; ++qq) {
+                    const unsigned m = __ballot_sync(kFull, q == qq);
+                    if (q == qq) packed = (slotQ[qq] << 24) | (runQ[qq] + __popc(m & lt));
+                    runQ[qq] += __popc(m);
+                }
+                // multi-cell hops (a few percent): a slot each; their order is
+                // made canonical after the scatter
+                if (d >= 0 && q < 0) packed = (kFarSlot << 24) | atomicAdd(a.countSlot + (size_t)d * kSlots + kFarSlot, 1);
+                if (valid) a.rank[i] = packed;
             }
-            // multi-cell hops (a few percent): a slot each; their order is
-            // made canonical after the scatter
-            if (d >= 0 && q < 0) packed = (kFarSlot << 24) | atomicAdd(a.countSlot + (size_t)d * kSlots + kFarSlot, 1);
-            if (valid) a.rank[i] = packed;
         }
         int myRun = 0;
 #pragma unroll
@@ -1230,18 +1243,36 @@ __global__ void classify_kernel(StepArgs<Real> a, int stageMax)
 }
 
 // copy a cell's velocities and internal energies between the buffer (at s0)
-// and v[comp][k * stride], whole warp
+// and v[comp][k * stride], whole warp. Into shared memory, the loads of up
+// to 128 particles are issued before their stores (one round trip to
+// memory for most cells instead of one per 32 particles).
 template <typename Real, bool kToBuffer>
 __device__ __forceinline__ void copy_cell(const PBuf<Real>& buf, int s0, int n, Real* const (&v)[4], int stride)
 {
     const int lane = threadIdx.x & 31;
     Real* b[4] = {buf.v[0] + s0, buf.v[1] + s0, buf.v[2] + s0, buf.ir + s0};
-    for (int k = lane; k < n; k += 32)
+    if constexpr (kToBuffer) {
+        for (int k = lane; k < n; k += 32)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (kToBuffer) b[q][k] = v[q][k * stride];
-            else v[q][k * stride] = b[q][k];
+            for (int q = 0; q < 4; ++q) b[q][k] = v[q][k * stride];
+    } else {
+        for (int k0 = lane; k0 < n; k0 += 128) {
+            Real t[4][4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + 32 * u;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) t[u][q] = k < n ? b[q][k] : (Real)0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + 32 * u;
+                if (k < n)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) v[q][k * stride] = t[u][q];
+            }
         }
+    }
 }
 
 // Collisions of staged large cells, two cells per warp at a time, both in
@@ -1305,17 +1336,14 @@ __device__ void collide_two_channels(const StepArgs<Real>& a, const PBuf<Real>& 
                     held = it;
                     break;
                 }
+                const int np = n > 1 ? rec.w : 0;
+                const double consCrm = rc.x, crm0 = rc.y;
+                if (lane == 0) pairs += (uint32_t)np;
+                if (!(consCrm > 0.0) || np <= 0) continue;   // nothing changes: not staged
                 const int base = ch == 0 ? 0 : N - n;
                 Real* const v[4] = {arena + base, arena + N + base, arena + 2 * N + base, arena + 3 * N + base};
                 copy_cell<Real, false>(dst, s0, n, v, 1);
                 __syncwarp();
-                const int np = n > 1 ? rec.w : 0;
-                const double consCrm = rc.x, crm0 = rc.y;
-                if (lane == 0) pairs += (uint32_t)np;
-                if (!(consCrm > 0.0) || np <= 0) {   // nothing changes: no write-back
-                    __syncwarp();
-                    continue;
-                }
                 for (int k = lane; k < n; k += 32) sclaim[base + k] = INT_MAX;
                 __syncwarp();
                 cc[ch] = c; cbase[ch] = base; cs0[ch] = s0; cn[ch] = n; cnp[ch] = np; cnext[ch] = 0;

@@ -78,3 +78,32 @@ def test_mixed_sampling_sums_every_particle_once(block):
     assert np.array_equal(got[:, 0], want[:, 0])
     scale = np.abs(terms).max(0) * np.maximum(want[:, :1], 1.0)
     assert np.all(np.abs(got - want) <= 1e-12 * scale)
+
+
+def test_mixed_full_step_moments_sum_every_particle_once(block):
+    """Mixed path, full steps: the moments the sampling pass folds (made by
+    the collide pass for the cells it staged, summed from the particles for
+    the others) are the sums over exactly each cell's particles after the
+    step, within FP64 rounding of numpy's sums of the same FP32 state."""
+    raw, dm, mess = block
+    x, v, ir, cell = I.ragged(I.fill_inputs(dm, mess, 70, seed=43), dm.ncell, 70, seed=44)
+    with make_case(dm, mess, precision=gpu.PRECISION_MIXED, keep_step_moments=1) as case:
+        case.upload_particles(x, v, ir, cell)
+        case.statistic_macroPre()
+        for s in (1, 2):
+            case.step(s)
+        got = case.step_moments()
+        _, vd, ird, celld = case.download_particles()
+        c = case.counters()
+    assert c["collisions"] > 0
+    X, Y, Z = vd[:, 0], vd[:, 1], vd[:, 2]
+    v2 = X * X + Y * Y + Z * Z
+    terms = np.stack([np.ones_like(X), X, Y, Z, v2, X * X, X * Y, Y * Y, Y * Z, Z * Z, Z * X,
+                      X * v2, Y * v2, Z * v2, ird, X * ird, Y * ird, Z * ird], 1)
+    want = np.zeros((dm.ncell, 18))
+    np.add.at(want, celld, terms)
+    n = want[:, 0]
+    assert (n > 16).sum() > 100 and (n <= 16).any()          # cells of the two-cell collide path and others
+    assert np.array_equal(got[:, 0], n)
+    scale = np.abs(terms).max(0) * np.maximum(want[:, :1], 1.0)
+    assert np.all(np.abs(got - want) <= 1e-12 * scale)
