@@ -88,7 +88,7 @@ struct LaunchShape {
     int moveBlocksPerSm = 8;      // move grid = smCount x this
     int sortBlocksPerSm = 16;     // rank, scatter, gather grids = smCount x this
     int collideBlocksPerSm = 32;  // collide grid cap per SM (at most the resident blocks)
-    int stayPerThread = 1;        // particles per thread of the move's stay pass: 1, 2 or 4
+    int stayPerThread = 4;        // particles per thread of the move's stay pass: 1, 2 or 4
 };
 
 template <typename Real> void launch_inject(const StepArgs<Real>& a, const LaunchShape& L, cudaStream_t s);
