@@ -124,6 +124,20 @@ def algorithmic_bytes(n_particles: float, ncell: int, ntri_per_cell: float, mixe
             "per_particle_state": sp, "geom_per_cell": geom}
 
 
+def stage_rooflines(ab: dict, stage_ms, names, kernels: dict, peak: float) -> dict:
+    """Algorithmic bytes over the event-timed stage time, for every stage
+    with a byte model (the dominant one is the line's `roofline`)."""
+    out = {}
+    for k, name in enumerate(names):
+        b = ab.get(name)
+        ms = float(stage_ms[k])
+        if not b or ms <= 0:
+            continue
+        gbs = (b / (ms / 1e3)) / 1e9
+        out[name] = {"kernel": kernels[name], "ms": ms, "algorithmic_bytes": b, "achieved": gbs, "frac": gbs / peak}
+    return out
+
+
 def measured_traffic(kernel: str, workload: str, particles: float):
     """DRAM bytes per launch of a kernel on this workload from the committed
     ncu summaries (profiles/<kernel>_<mesh>_ppc<N>.md, lines
@@ -442,7 +456,7 @@ def run_ours(args):
     ab = algorithmic_bytes(n_mean, dm.ncell, tri_per_cell, mixed=True)
     names = ["inject", "move", "sort", "collide", "sample"]
     kernels = {"inject": "inject_gen_kernel", "move": "move_kernel", "sort": "gather_kernel",
-               "collide": "collide_kernel", "sample": "sample_kernel"}
+               "collide": "collide_kernel", "sample": "sample_warp_kernel"}
     stage_avg = mixed["stage"]
     dom = names[int(np.argmax(stage_avg))]
     dom_ms = float(stage_avg[names.index(dom)])
@@ -481,7 +495,8 @@ def run_ours(args):
                      "traffic_source": traffic_src, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
                      "step": {"algorithmic_bytes": ab["step"], "achieved": step_achieved,
-                              "frac": step_achieved / peak}},
+                              "frac": step_achieved / peak},
+                     "stages": stage_rooflines(ab, stage_avg, names, kernels, peak)},
         "e2e": {"value": e2e_full_ps / e2e_full_s, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": mixed["h2d"] / plan["total"], "d2h_bytes_per_step": mixed["d2h"] / plan["total"],
                 "how": f"the whole {plan['total']}-step run through the C ABI: host arrays (pinned) uploaded, every "
