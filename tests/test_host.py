@@ -103,6 +103,25 @@ def test_bench_reads_and_scales_profile_traffic(tmp_path, monkeypatch):
     assert b == 7000.0 and src == os.path.join("profiles", "move_kernel_meshA_ppc100.md")
     assert bench.measured_traffic("move_kernel", "meshB_ppc100", 2500.0) == (None, None)
     assert bench.measured_traffic("collide_kernel", "meshA_ppc100", 2500.0) == (None, None)
+    # the workload's own summary with its particle count: scaled to the timed count
+    (prof / "move_kernel_meshA_ppc100.md").write_text("dram_bytes_per_launch: 7000\nparticles: 2000\n")
+    b, src = bench.measured_traffic("move_kernel", "meshA_ppc100", 2500.0)
+    assert b == 8750.0 and "scaled by particles x1.250" in src
+
+
+def test_bench_stage_rooflines():
+    """Every stage with a byte model gets its algorithmic bytes over its
+    event-timed stage time as a fraction of the peak; stages without one
+    (inject) or without a time are left out."""
+    import numpy as np
+    import bench
+    names = ["inject", "move", "sort", "collide", "sample"]
+    kernels = {k: k + "_kernel" for k in names}
+    ab = {"inject": None, "move": 2.0e9, "sort": 3.0e9, "collide": 1.0e9, "sample": 0.5e9}
+    st = bench.stage_rooflines(ab, np.array([0.1, 2.0, 1.0, 0.0, 0.5]), names, kernels, 4000.0)
+    assert set(st) == {"move", "sort", "sample"}
+    assert st["move"]["achieved"] == 1000.0 and st["move"]["frac"] == 0.25
+    assert st["sort"]["achieved"] == 3000.0 and st["sample"]["kernel"] == "sample_kernel"
 
 
 def test_upload_columns_passes_what_upload_particles_passes():
