@@ -1689,9 +1689,9 @@ __global__ void __launch_bounds__(128) sample_kernel(StepArgs<Real> a, int pre)
 // statistic_macro of the mixed path, one warp per cell: the lanes sum the
 // cell's particles 32 apart (coalesced loads), lane q < 18 then adds up
 // moment q of the 32 lanes (four groups of eight, through shared memory)
-// and folds it into the cell's accumulators, and lane 0 runs the rest. Its FP64 sums
-// run in another order than the one-thread sums, which the FP64 path keeps
-// (they are the reference's order).
+// and folds it into the cell's accumulators, and lane 0 runs the rest. Its
+// FP64 sums run in another order than the one-thread sums, which the FP64
+// path keeps (they are the reference's order).
 constexpr int kSampleWarps = 8;
 
 __global__ void __launch_bounds__(kSampleWarps * 32, 3) sample_warp_kernel(StepArgs<float> a)
