@@ -392,8 +392,8 @@ typedef struct DsmcLaunchShape {
     int32_t move_threads;          /* threads per block of the move kernel: 128 or 256 */
     int32_t move_blocks_per_sm;    /* move grid = SMs x this, 1..32 (particles per thread follow) */
     int32_t sort_blocks_per_sm;    /* rank / scatter / gather grids = SMs x this, 1..32 */
-    int32_t collide_blocks_per_sm; /* cap on the collision grid per SM, 1..32 (at most the resident blocks) */
-    int32_t stay_per_thread;       /* particles per thread of the move's stay pass: 1, 2 or 4 */
+    int32_t collide_blocks_per_sm; /* cap on the collision grid per SM, 1..32 (at most the resident blocks; default 32) */
+    int32_t stay_per_thread;       /* particles per thread of the move's stay pass: 1, 2 or 4 (default 4) */
 } DsmcLaunchShape;
 
 int dsmc_get_launch_shape(DsmcHandle* h, DsmcLaunchShape* out);
